@@ -1,0 +1,165 @@
+// sfgpu_internal.cuh -- device-side lattice descriptor and the per-site
+// stencils of the SFbox hot path, shared by all kernels of libsfgpu.
+//
+// Layout in HBM: every profile is a full lattice vector of M doubles
+// including SFbox's boundary layers, last gradient fastest (Lat3D.cpp:59-68).
+// Boundary entries always hold SetBoundaries copies (Lat3D.cpp:1510-1562),
+// so stencils on interior sites read their neighbours directly.  Second-order
+// propagators stack the six direction components k*M + z
+// (k: 0=+x 1=+y 2=+z 3=-z 4=-y 5=-x, Lat3D2ndO.cpp:70-82).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "../../include/sfgpu.h"
+
+#ifndef SFGPU_MAX_SEG
+#define SFGPU_MAX_SEG 8          // segment types per system (chi held in kernel params)
+#endif
+
+struct DLat {
+    int grad, cyl, order;
+    int M;
+    int Md[3];                 // layers incl. boundaries (1 for unused gradients)
+    int st[3];                 // strides
+    int bc_lo[3], bc_hi[3];    // SFGPU_BOUND_*
+    int map_lo[3], map_hi[3];  // coordinate copied into 0 / Md-1
+    double l1, l1chi;
+    const double *lam_m, *lam_p;   // cylinder tables by x (device)
+};
+
+struct ChiTable {              // passed by value: small interaction tables
+    int nseg;
+    double chi[SFGPU_MAX_SEG * SFGPU_MAX_SEG];
+};
+
+__host__ __device__ inline void lat_coords(const DLat &L, int z, int c[3]) {
+    if (L.grad == 1) { c[0] = z; c[1] = 0; c[2] = 0; return; }
+    if (L.grad == 2) { c[0] = z / L.st[0]; c[1] = z - c[0] * L.st[0]; c[2] = 0; return; }
+    c[0] = z / L.st[0];
+    int r = z - c[0] * L.st[0];
+    c[1] = r / L.st[1];
+    c[2] = r - c[1] * L.st[1];
+}
+
+__host__ __device__ inline bool lat_interior(const DLat &L, const int c[3]) {
+    for (int d = 0; d < L.grad; d++)
+        if (c[d] == 0 || c[d] == L.Md[d] - 1) return false;
+    return true;
+}
+
+// Site whose value boundary site z copies (z itself for interior sites and for
+// surface layers); *swap gets one bit per mirrored gradient.
+__host__ __device__ inline int lat_map(const DLat &L, int z, int *swap = nullptr) {
+    int c[3];
+    lat_coords(L, z, c);
+    int m = 0;
+    bool bnd = false;
+    for (int d = 0; d < L.grad; d++) {
+        if (c[d] == 0) {
+            bnd = true; c[d] = L.map_lo[d];
+            if (L.bc_lo[d] == SFGPU_BOUND_MIRROR1 || L.bc_lo[d] == SFGPU_BOUND_MIRROR2) m |= 1 << d;
+        } else if (c[d] == L.Md[d] - 1) {
+            bnd = true; c[d] = L.map_hi[d];
+            if (L.bc_hi[d] == SFGPU_BOUND_MIRROR1 || L.bc_hi[d] == SFGPU_BOUND_MIRROR2) m |= 1 << d;
+        }
+    }
+    if (swap) *swap = m;
+    if (!bnd) return z;
+    return c[0] * L.st[0] + c[1] * L.st[1] + c[2] * L.st[2];
+}
+
+__device__ inline int swap_dir(int k, int sw) {
+    if (sw & 1) { if (k == 0) k = 5; else if (k == 5) k = 0; }
+    if (sw & 2) { if (k == 1) k = 4; else if (k == 4) k = 1; }
+    if (sw & 4) { if (k == 2) k = 3; else if (k == 3) k = 2; }
+    return k;
+}
+
+// First-order step at interior site t: G(t) * stencil(gin) in SFbox's
+// operation order (Lat1DFlat1stO.cpp:44-47, Lat2DFlat1stO.cpp:40-46,
+// Lat2DCyl1stO.cpp:24-33, Lat3D1stO.cpp:151-157).  The library is compiled
+// without FMA contraction so the rounding sequence matches the CPU code.
+__device__ __forceinline__ double stencil1(const DLat &L, const double *__restrict__ gin, double g, int t) {
+    if (L.grad == 1) {
+        double a = gin[t - 1], b = gin[t], c = gin[t + 1];
+        return g * (b + L.l1 * (a - b - b + c));
+    } else if (L.grad == 2) {
+        int MY = L.st[0];
+        double a = gin[t - 1], b = gin[t], c = gin[t + 1];
+        double u = gin[t - MY], d = gin[t + MY];
+        if (L.cyl) {
+            int x = t / MY;
+            return g * (b + L.lam_m[x] * (u - b) + L.lam_p[x] * (d - b) + L.l1 * (a + c - b - b));
+        }
+        double l0 = 1 - 4 * L.l1;
+        return g * (l0 * b + L.l1 * (a + c) + L.l1 * (u + d));
+    } else {
+        int jx = L.st[0], jy = L.st[1];
+        double acc = gin[t - jx] * g;
+        acc += gin[t + jx] * g;
+        acc += gin[t - jy] * g;
+        acc += gin[t + jy] * g;
+        acc += gin[t - 1] * g;
+        acc += gin[t + 1] * g;
+        return acc * (1.0 / 6.0);
+    }
+}
+
+// Contact average <phi>(z) at any site (SideFraction, Lat1DFlat.cpp:511-524,
+// Lat2DFlat.cpp:996-1109, Lat2DCylinder.cpp:205-320; Sides with removed
+// boundaries in 3D, Lat3D.cpp:1729-1785).  p must carry boundary copies.
+__device__ inline double side_fraction(const DLat &L, const double *__restrict__ p, int z) {
+    int c[3];
+    lat_coords(L, z, c);
+    if (L.grad == 3) {
+        if (!lat_interior(L, c)) return 0.0;
+        int jx = L.st[0], jy = L.st[1];
+        const double l1 = 1.0 / 6.0;
+        double acc = 0 * p[z];
+        acc += l1 * p[z + jx]; acc += l1 * p[z - jx];
+        acc += l1 * p[z + jy]; acc += l1 * p[z - jy];
+        acc += l1 * p[z + 1];  acc += l1 * p[z - 1];
+        return acc;
+    }
+    double l = L.l1chi;
+    if (L.grad == 1) {
+        int zz = z;
+        if (z == 0) {
+            if (L.bc_lo[0] == SFGPU_BOUND_SURFACE) return p[0] + l * (-p[0] - p[0] + p[1]);
+            zz = L.map_lo[0];
+        } else if (z == L.M - 1) {
+            if (L.bc_hi[0] == SFGPU_BOUND_SURFACE) return p[z] + l * (-p[z] - p[z] + p[z - 1]);
+            zz = L.map_hi[0];
+        }
+        return p[zz] + l * (p[zz - 1] - p[zz] - p[zz] + p[zz + 1]);
+    }
+    int MX = L.Md[0], MY = L.Md[1];
+    bool onsurf = (c[0] == 0 && L.bc_lo[0] == SFGPU_BOUND_SURFACE) ||
+                  (c[0] == MX - 1 && L.bc_hi[0] == SFGPU_BOUND_SURFACE) ||
+                  (c[1] == 0 && L.bc_lo[1] == SFGPU_BOUND_SURFACE) ||
+                  (c[1] == MY - 1 && L.bc_hi[1] == SFGPU_BOUND_SURFACE);
+    int x = c[0], zz = z;
+    if (!onsurf) { zz = lat_map(L, z); x = zz / MY; }
+    double lm = L.cyl ? L.lam_m[x] : l, lp = L.cyl ? L.lam_p[x] : l;
+    if (!onsurf) {
+        if (L.cyl)
+            return p[zz] + lp * (p[zz + MY] - p[zz]) + lm * (p[zz - MY] - p[zz]) + l * (p[zz - 1] + p[zz + 1] - p[zz] - p[zz]);
+        double l0 = 1 - 2 * l - lm - lp;
+        return l0 * p[zz] + l * (p[zz - MY] + p[zz + MY]) + l * (p[zz - 1] + p[zz + 1]);
+    }
+    double l0 = 1 - 2 * l - lm - lp;
+    double acc = l0 * p[z];
+    if (c[0] > 0) acc += lm * p[z - MY];
+    if (c[0] < MX - 1) acc += lp * p[z + MY];
+    if (c[1] > 0) acc += l * p[z - 1];
+    if (c[1] < MY - 1) acc += l * p[z + 1];
+    return acc;
+}
+
+#define SFGPU_CUDA_TRY(expr)                                          \
+    do {                                                              \
+        cudaError_t _e = (expr);                                      \
+        if (_e != cudaSuccess) { sfgpu_set_error(_e, #expr, __FILE__, __LINE__); return SFGPU_ERR_CUDA; } \
+    } while (0)
+
+void sfgpu_set_error(cudaError_t e, const char *what, const char *file, int line);

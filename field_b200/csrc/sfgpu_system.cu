@@ -1,0 +1,705 @@
+// sfgpu_system.cu -- one SF-SCF system on one GPU: set-up of the lattice and
+// molecules, the residual evaluation x -> f (SF_Solve::residuals,
+// SF_Solve.cpp:647-651), free energy, the Lattice-level entry points and the
+// host-driven Pure_DIIS iteration (the plain GPU form).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include "sfgpu_kernels.cuh"
+#include "sfgpu_system.h"
+
+static thread_local char g_errmsg[512] = "";
+
+void sfgpu_set_error(cudaError_t e, const char *what, const char *file, int line) {
+    snprintf(g_errmsg, sizeof(g_errmsg), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+static int fail(int code, const char *msg) {
+    snprintf(g_errmsg, sizeof(g_errmsg), "%s", msg);
+    return code;
+}
+
+extern "C" const char *sfgpu_last_error(void) { return g_errmsg; }
+
+using namespace sfk;
+
+static int grid_for(long n) {
+    long b = (n + kBlock - 1) / kBlock;
+    return (int)std::max(1L, std::min(b, 148L * 16));
+}
+
+// ---------------------------------------------------------------------------
+// lattice set-up (Lat1DFlat.cpp:4-149, Lat2DFlat.cpp:35-220,
+// Lat2DCylinder.cpp:7-55, Lat3D.cpp:44-236)
+// ---------------------------------------------------------------------------
+static int map_lo_of(int bc, int n) {
+    switch (bc) {
+        case SFGPU_BOUND_SURFACE: return 0;
+        case SFGPU_BOUND_MIRROR1: return 1;
+        case SFGPU_BOUND_MIRROR2: return 2;
+        case SFGPU_BOUND_PERIODIC: return n;
+    }
+    return -1;
+}
+static int map_hi_of(int bc, int n) {
+    switch (bc) {
+        case SFGPU_BOUND_SURFACE: return n + 1;
+        case SFGPU_BOUND_MIRROR1: return n;
+        case SFGPU_BOUND_MIRROR2: return n - 1;
+        case SFGPU_BOUND_PERIODIC: return 1;
+    }
+    return -1;
+}
+
+int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
+    DLat &L = H->L;
+    memset(&L, 0, sizeof(L));
+    L.grad = d->gradients;
+    L.order = d->order;
+    L.cyl = (d->gradients == 2 && d->geometry == SFGPU_GEOM_CYLINDRICAL);
+    if (L.grad < 1 || L.grad > 3) return fail(SFGPU_ERR_INVALID, "gradients must be 1, 2 or 3");
+    if (d->geometry == SFGPU_GEOM_CYLINDRICAL && L.grad != 2)
+        return fail(SFGPU_ERR_UNSUPPORTED, "cylindrical geometry needs 2 gradients");
+    if (L.order == 2 && L.grad != 3) return fail(SFGPU_ERR_UNSUPPORTED, "second order is implemented for 3 gradients");
+    if (L.order != 1 && L.order != 2) return fail(SFGPU_ERR_INVALID, "order must be 1 or 2");
+    for (int k = 0; k < 3; k++) L.Md[k] = 1;
+    for (int k = 0; k < L.grad; k++) {
+        int n = d->n_layers[k];
+        if (n < 1) return fail(SFGPU_ERR_INVALID, "n_layers must be positive");
+        if (L.grad == 3 && n < 3) return fail(SFGPU_ERR_INVALID, "3D lattices need at least 3 layers per gradient");
+        int lo = d->bound_lo[k], hi = d->bound_hi[k];
+        if (lo < 1 || lo > 4 || hi < 1 || hi > 4) return fail(SFGPU_ERR_INVALID, "unknown boundary condition");
+        if ((lo == SFGPU_BOUND_PERIODIC) != (hi == SFGPU_BOUND_PERIODIC))
+            return fail(SFGPU_ERR_INVALID, "periodic boundaries must be periodic on both sides");
+        if ((lo == SFGPU_BOUND_MIRROR2 || hi == SFGPU_BOUND_MIRROR2) && n < 2)
+            return fail(SFGPU_ERR_INVALID, "mirror2 needs at least 2 layers");
+        if (L.grad == 3 && (lo == SFGPU_BOUND_SURFACE || hi == SFGPU_BOUND_SURFACE))
+            return fail(SFGPU_ERR_INVALID, "the 3D lattice has no surface boundary");
+        L.Md[k] = n + 2;
+        L.bc_lo[k] = lo; L.bc_hi[k] = hi;
+        L.map_lo[k] = map_lo_of(lo, n);
+        L.map_hi[k] = map_hi_of(hi, n);
+    }
+    L.M = L.Md[0] * L.Md[1] * L.Md[2];
+    if (L.grad == 1) { L.st[0] = 1; L.st[1] = 0; L.st[2] = 0; }
+    else if (L.grad == 2) { L.st[0] = L.Md[1]; L.st[1] = 1; L.st[2] = 0; }
+    else { L.st[0] = L.Md[1] * L.Md[2]; L.st[1] = L.Md[2]; L.st[2] = 1; }
+    L.l1 = (L.grad == 3) ? 1.0 / 6.0 : d->lambda;
+    if (L.grad != 3 && !(d->lambda > 0 && d->lambda <= 0.5)) return fail(SFGPU_ERR_INVALID, "lambda must be in (0, 0.5]");
+    L.l1chi = (L.grad == 1 && d->lambda_chi >= 0) ? d->lambda_chi : L.l1;
+    double ladj = (L.grad == 1 && d->layer_adjustment > 0) ? d->layer_adjustment : 1.0;
+
+    int MX = L.Md[0];
+    H->lam_m.assign(MX, 0.0); H->lam_p.assign(MX, 0.0); H->Lx.assign(MX, 1.0);
+    if (L.cyl) {
+        const double PI_ = 4.0 * atan(1.0);
+        double off = d->offset_first_layer;
+        double D = (d->dimensions > 0 ? d->dimensions : 3.0) - 1;
+        std::vector<double> V(MX + 1, 0), S(MX + 1, 0), lm(MX + 1, 0), lp(MX + 1, 0), LL(MX + 1, 0);
+        S[1] = off * PI_ * 2; V[1] = off * off * PI_; LL[1] = V[1];
+        for (int z = 2; z <= MX; z++) {
+            double x = z + off - 2 + 1.0;
+            V[z] = (PI_ * pow(2, (D - 1)) / D) * pow(x, D);
+            LL[z] = V[z] - V[z - 1];
+            S[z] = pow(2, (D - 1)) * PI_ * pow(x, (D - 1));
+            lm[z] = L.l1 * S[z - 1] / LL[z];
+            lp[z] = L.l1 * S[z] / LL[z];
+        }
+        lp[MX] = 0;
+        if (LL[1] > PI_) LL[1] = V[1] - (off - 1) * (off - 1) * PI_;
+        if (LL[1] > 0) lp[1] = LL[2] * lm[2] / LL[1];
+        for (int x = 0; x < MX; x++) { H->lam_m[x] = lm[x + 1]; H->lam_p[x] = lp[x + 1]; H->Lx[x] = LL[x + 1]; }
+    }
+    // weights of lnGN sums and of the free energy (SubtractBoundaries +
+    // MultiplyWithLatticeSites)
+    H->w_gn.assign(L.M, 0.0); H->w_f.assign(L.M, 0.0);
+    for (int z = 0; z < L.M; z++) {
+        int c[3];
+        lat_coords(L, z, c);
+        double w = 1.0;
+        bool keep = true, interior = true;
+        for (int k = 0; k < L.grad; k++) {
+            int last = L.Md[k] - 1;
+            if (c[k] == 0) { interior = false; if (L.bc_lo[k] != SFGPU_BOUND_SURFACE) keep = false; }
+            else if (c[k] == last) { interior = false; if (L.bc_hi[k] != SFGPU_BOUND_SURFACE) keep = false; }
+            else {
+                if (c[k] == 1 && L.bc_lo[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
+                else if (c[k] == last - 1 && L.bc_hi[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
+            }
+        }
+        if (L.cyl) w *= H->Lx[c[0]];
+        if (L.grad == 1) {
+            if (z == 1) w *= ladj;
+            if (z == L.M - 2 && L.M > 3) w *= (2 - ladj);
+        }
+        H->w_f[z] = keep ? w : 0.0;
+        H->w_gn[z] = interior ? w : 0.0;
+    }
+    return SFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// system
+// ---------------------------------------------------------------------------
+template <class T> static int dalloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) { sfgpu_set_error(e, "cudaMalloc", __FILE__, __LINE__); return SFGPU_ERR_NOMEM; }
+    return SFGPU_OK;
+}
+
+static bool chi_cols_equal(const std::vector<double> &chi, int ns, int a, int b) {
+    for (int i = 0; i < ns; i++)
+        if (chi[i * ns + a] != chi[i * ns + b]) return false;
+    return true;
+}
+
+sfgpu_system::~sfgpu_system() {
+    for (void *p : allocs) cudaFree(p);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+int sfgpu_system::alloc_d(double **p, size_t n) {
+    int rc = dalloc(p, n);
+    if (rc == SFGPU_OK) allocs.push_back(*p);
+    return rc;
+}
+int sfgpu_system::alloc_i(int **p, size_t n) {
+    int rc = dalloc(p, n);
+    if (rc == SFGPU_OK) allocs.push_back(*p);
+    return rc;
+}
+
+int sfgpu_system::setup(const sfgpu_system_desc *d) {
+    int rc = sfgpu_build_lattice(&d->lattice, &H);
+    if (rc) return rc;
+    DLat &L = H.L;
+    M = L.M;
+    K = (L.order == 2) ? 6 : 1;
+    nseg = d->n_segments;
+    if (nseg < 1 || nseg > SFGPU_MAX_SEG) return fail(SFGPU_ERR_UNSUPPORTED, "1 to 8 segment types are supported");
+    nmol = d->n_molecules;
+    if (nmol < 1 || nmol > SFGPU_MAX_SEG) return fail(SFGPU_ERR_UNSUPPORTED, "1 to 8 molecules are supported");
+    chi.assign(nseg * nseg, 0.0);
+    pf.assign(nseg * nseg, 0.2);
+    freedom.resize(nseg);
+    range_h.assign((size_t)nseg * M, 0.0);
+    for (int i = 0; i < nseg; i++) {
+        freedom[i] = d->segments[i].freedom;
+        if (freedom[i] < SFGPU_SEG_FREE || freedom[i] > SFGPU_SEG_PINNED) return fail(SFGPU_ERR_UNSUPPORTED, "segment freedom");
+        if (freedom[i] != SFGPU_SEG_FREE) {
+            if (!d->segments[i].range) return fail(SFGPU_ERR_INVALID, "frozen/pinned segment without range");
+            memcpy(&range_h[(size_t)i * M], d->segments[i].range, sizeof(double) * M);
+        }
+        for (int j = 0; j < nseg; j++) {
+            chi[i * nseg + j] = d->chi ? d->chi[i * nseg + j] : 0.0;
+            pf[i * nseg + j] = d->pf ? d->pf[i * nseg + j] : 0.2;
+        }
+    }
+    for (int i = 0; i < nseg; i++)
+        for (int j = 0; j < nseg; j++)
+            if (chi[i * nseg + j] != chi[j * nseg + i]) return fail(SFGPU_ERR_INVALID, "chi must be symmetric");
+    memset(&ct, 0, sizeof(ct));
+    ct.nseg = nseg;
+    for (int i = 0; i < nseg; i++)
+        for (int j = 0; j < nseg; j++) ct.chi[i * SFGPU_MAX_SEG + j] = chi[i * nseg + j];
+
+    // molecules
+    mols.resize(nmol);
+    solvent = -1;
+    for (int m = 0; m < nmol; m++) {
+        const sfgpu_molecule_desc &md = d->molecules[m];
+        HMol &o = mols[m];
+        o.seg.clear();
+        if (md.n_blocks < 1) return fail(SFGPU_ERR_INVALID, "molecule without blocks");
+        for (int b = 0; b < md.n_blocks; b++) {
+            if (md.block_length[b] < 1) return fail(SFGPU_ERR_INVALID, "block length must be positive");
+            for (int q = 0; q < md.block_length[b]; q++) o.seg.push_back(md.block_segment[b]);
+        }
+        o.N = (int)o.seg.size();
+        o.count.assign(nseg, 0);
+        for (int sg : o.seg) {
+            if (sg < 0 || sg >= nseg) return fail(SFGPU_ERR_INVALID, "segment index out of range");
+            if (freedom[sg] == SFGPU_SEG_FROZEN) return fail(SFGPU_ERR_INVALID, "frozen segment inside a molecule");
+            o.count[sg]++;
+        }
+        o.used.clear();
+        o.pinned = 0;
+        for (int i = 0; i < nseg; i++)
+            if (o.count[i]) { o.used.push_back(i); if (freedom[i] == SFGPU_SEG_PINNED) o.pinned = 1; }
+        o.type = (o.N == 1) ? 0 : (o.used.size() == 1 ? 1 : 2);
+        o.sym = (o.type == 1 && K == 1);
+        o.freedom = md.freedom;
+        o.phibulk = md.phibulk;
+        o.theta = md.theta;
+        if (o.freedom == SFGPU_MOL_SOLVENT) {
+            if (solvent >= 0) return fail(SFGPU_ERR_INVALID, "more than one solvent molecule");
+            solvent = m;
+        } else if (o.freedom == SFGPU_MOL_RESTRICTED) {
+            if (!(o.theta > 0)) return fail(SFGPU_ERR_INVALID, "restricted molecule needs theta > 0");
+        } else if (o.freedom == SFGPU_MOL_FREE) {
+            if (!(o.phibulk > 0 && o.phibulk < 1)) return fail(SFGPU_ERR_INVALID, "free molecule needs 0 < phibulk < 1");
+        } else {
+            return fail(SFGPU_ERR_UNSUPPORTED, "molecule freedom");
+        }
+        double cr = 0;   // SF_MolStructure.cpp:411-423
+        for (int a : o.used) {
+            double inner = 0;
+            for (int b : o.used) inner += chi[a * nseg + b] * ((double)o.count[b] / o.N);
+            cr += ((double)o.count[a] / o.N) * inner;
+        }
+        o.chemintref = cr / 2;
+    }
+    if (solvent < 0) return fail(SFGPU_ERR_INVALID, "a solvent molecule is required");
+
+    // classes of liquid states (SF_Solve.cpp:37-86)
+    std::vector<int> q;
+    for (int i = 0; i < nseg; i++) if (freedom[i] != SFGPU_SEG_FROZEN) q.push_back(i);
+    int nl = (int)q.size();
+    if (nl == 0) return fail(SFGPU_ERR_INVALID, "no liquid segments");
+    for (int i = 0; i < nl; i++) {
+        int s1 = q[i];
+        for (int j = i + 1; j < nl; j++)
+            if (chi_cols_equal(chi, nseg, s1, q[j])) {
+                if (j != i + 1) std::swap(q[i + 1], q[j]);
+                i++;
+            }
+    }
+    class_of.assign(nseg, -1);
+    rep_of_class.clear();
+    for (int i = 0; i < nl; i++) {
+        int s1 = q[i];
+        int c = (int)rep_of_class.size();
+        class_of[s1] = c;
+        rep_of_class.push_back(s1);
+        for (int j = i + 1; j < nl; j++)
+            if (chi_cols_equal(chi, nseg, s1, q[j])) { i++; class_of[q[i]] = c; rep_of_class[c] = q[i]; }
+    }
+    nclass = (int)rep_of_class.size();
+    // sites with iteration variables (SF_Solve.cpp:129-150)
+    std::vector<int> jmap(M, -1);
+    sites_h.clear();
+    for (int z = 0; z < M; z++) {
+        int c[3];
+        lat_coords(L, z, c);
+        if (!lat_interior(L, c)) continue;
+        bool ok = true;
+        for (int i = 0; i < nseg; i++)
+            if (freedom[i] == SFGPU_SEG_FROZEN && range_h[(size_t)i * M + z] > 0.999) ok = false;
+        if (ok) { jmap[z] = (int)sites_h.size(); sites_h.push_back(z); }
+    }
+    nsites = (int)sites_h.size();
+    nvar = (size_t)nsites * nclass;
+    if (nsites == 0) return fail(SFGPU_ERR_INVALID, "no sites carry iteration variables");
+
+    // device buffers
+    if ((rc = alloc_d(&d_lam_m, M > 0 ? L.Md[0] : 1))) return rc;
+    if ((rc = alloc_d(&d_lam_p, L.Md[0]))) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpy(d_lam_m, H.lam_m.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
+    SFGPU_CUDA_TRY(cudaMemcpy(d_lam_p, H.lam_p.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
+    L.lam_m = d_lam_m; L.lam_p = d_lam_p;
+    if ((rc = alloc_d(&d_wgn, M)) || (rc = alloc_d(&d_wf, M))) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpy(d_wgn, H.w_gn.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+    SFGPU_CUDA_TRY(cudaMemcpy(d_wf, H.w_f.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+    if ((rc = alloc_i(&d_jmap, M)) || (rc = alloc_i(&d_sites, nsites))) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpy(d_jmap, jmap.data(), sizeof(int) * M, cudaMemcpyHostToDevice));
+    SFGPU_CUDA_TRY(cudaMemcpy(d_sites, sites_h.data(), sizeof(int) * nsites, cudaMemcpyHostToDevice));
+    d_range.assign(nseg, nullptr); d_gfull.assign(nseg, nullptr); d_gseg.assign(nseg, nullptr); d_phi.assign(nseg, nullptr);
+    for (int i = 0; i < nseg; i++) {
+        if ((rc = alloc_d(&d_phi[i], M))) return rc;
+        if (freedom[i] != SFGPU_SEG_FREE) {
+            if ((rc = alloc_d(&d_range[i], M))) return rc;
+            SFGPU_CUDA_TRY(cudaMemcpy(d_range[i], &range_h[(size_t)i * M], sizeof(double) * M, cudaMemcpyHostToDevice));
+        }
+        if (freedom[i] == SFGPU_SEG_FROZEN) {
+            // phi of a frozen state: its range values with boundary copies (SF_Segment.cpp:428-433)
+            std::vector<double> p(range_h.begin() + (size_t)i * M, range_h.begin() + (size_t)(i + 1) * M);
+            for (int z = 0; z < M; z++) { int t = lat_map(L, z); if (t != z) p[z] = range_h[(size_t)i * M + t]; }
+            SFGPU_CUDA_TRY(cudaMemcpy(d_phi[i], p.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+            continue;
+        }
+        if ((rc = alloc_d(&d_gfull[i], M))) return rc;
+        if (freedom[i] == SFGPU_SEG_PINNED) { if ((rc = alloc_d(&d_gseg[i], M))) return rc; }
+        else d_gseg[i] = d_gfull[i];
+    }
+    size_t store = 0;
+    for (auto &o : mols) {
+        o.d_phi.assign(nseg, nullptr);
+        for (int i : o.used) if ((rc = alloc_d(&o.d_phi[i], M))) return rc;
+        size_t need = (o.type == 0) ? 0 : (size_t)(o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
+        store = std::max(store, need);
+    }
+    if ((rc = alloc_d(&d_gi, store))) return rc;
+    if ((rc = alloc_d(&d_ginv[0], (size_t)K * M)) || (rc = alloc_d(&d_ginv[1], (size_t)K * M))) return rc;
+    nblocks_red = grid_for(M);
+    if ((rc = alloc_d(&d_partial, (size_t)std::max(nblocks_red, 64) * 64))) return rc;
+    if ((rc = alloc_d((double **)&d_scal, 4 * (size_t)nmol))) return rc;
+    if ((rc = alloc_d(&d_phib, nseg)) || (rc = alloc_d(&d_chib, nclass)) || (rc = alloc_d(&d_misc, 64))) return rc;
+    if ((rc = alloc_d(&d_x, nvar)) || (rc = alloc_d(&d_f, nvar))) return rc;
+    SFGPU_CUDA_TRY(cudaMemset(d_scal, 0, sizeof(MolScal) * nmol));
+
+    // bulk parameters
+    memset(&bp, 0, sizeof(bp));
+    bp.nseg = nseg; bp.nmol = nmol; bp.nclass = nclass;
+    for (int c = 0; c < nclass; c++) bp.rep[c] = rep_of_class[c];
+    for (int i = 0; i < nseg; i++)
+        for (int m = 0; m < nmol; m++) bp.frac[i * SFGPU_MAX_SEG + m] = (double)mols[m].count[i] / mols[m].N;
+    return SFGPU_OK;
+}
+
+// propagation of one molecule (SF_Monomer1stO::Matrix1, SF_Homopol1stO::Matrix1,
+// SF_Copol1stO::Matrix1, SF_Homopol2ndO::Matrix1, SF_Copol2ndO::Matrix1)
+int sfgpu_system::molecule_phi(int m) {
+    HMol &o = mols[m];
+    const DLat &L = H.L;
+    const int g = grid_for(M);
+    cudaStream_t s = stream;
+    MolParam p;
+    p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = o.sym; p.K = K;
+    p.pinned = o.pinned; p.solvent = (m == solvent); p.nmol = nmol;
+    p.phibulk_in = o.phibulk; p.theta = o.theta;
+    MolScal *scal = (MolScal *)d_scal;
+    const size_t KM = (size_t)K * M;
+    if (o.type == 0) {
+        int i = o.seg[0];
+        // lnGN of the end-point distribution G itself (all K components equal)
+        wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, d_gseg[i], d_wgn, d_partial);
+        MolParam p1 = p; p1.K = 1;
+        mol_scalars<<<1, 1, 0, s>>>(p1, nblocks_red, d_partial, scal, m);
+        finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], scal, m, 1);
+        return SFGPU_OK;
+    }
+    for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_phi[i], 0, sizeof(double) * M, s));
+    double *ginv = d_ginv[0], *tmp = d_ginv[1];
+    if (o.sym) {
+        const int i = o.seg[0];
+        const double *G = d_gseg[i];
+        const int N = o.N, half = N / 2;
+        double *phi = o.d_phi[i];
+        SFGPU_CUDA_TRY(cudaMemcpyAsync(d_gi, G, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+        for (int t = 1; t < half; t++)
+            step1<<<g, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * M, G, d_gi + (size_t)t * M, nullptr, nullptr, COMP_NONE);
+        const double *cur = d_gi + (size_t)(half - 1) * M;
+        if (N % 2 == 1) {
+            step1<<<g, kBlock, 0, s>>>(L, cur, G, ginv, nullptr, phi, COMP_CENTRE);
+            cur = ginv; std::swap(ginv, tmp);
+        }
+        for (int sp = (N + 3) / 2; sp <= N; sp++) {
+            int sinv = N - sp + 1;
+            step1<<<g, kBlock, 0, s>>>(L, cur, G, ginv, d_gi + (size_t)(sinv - 1) * M, phi, COMP_ACC);
+            cur = ginv; std::swap(ginv, tmp);
+        }
+        wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, cur, d_wgn, d_partial);
+        mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, scal, m);
+        finalize_phi<<<g, kBlock, 0, s>>>(M, G, phi, scal, m, 0);
+        return SFGPU_OK;
+    }
+    // full storage: copolymers and all second-order chains
+    const int N = o.N;
+    replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[0]], d_gi);
+    if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, d_gi);
+    for (int t = 1; t < N; t++) {
+        int sg = o.seg[t];
+        if (K == 1)
+            step1<<<g, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
+        else
+            step2<<<g, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
+                                       d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0);
+    }
+    replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[N - 1]], ginv);
+    if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, ginv);
+    connect<<<g, kBlock, 0, s>>>(M, K, ginv, d_gi + (size_t)(N - 1) * KM, o.d_phi[o.seg[N - 1]]);
+    const double *cur = ginv;
+    std::swap(ginv, tmp);
+    for (int t = N - 2; t >= 0; t--) {
+        int sg = o.seg[t];
+        if (K == 1)
+            step1<<<g, kBlock, 0, s>>>(L, cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
+        else
+            step2<<<g, kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv, d_gi + (size_t)t * KM,
+                                       o.d_phi[sg], COMP_ACC, 1);
+        cur = ginv; std::swap(ginv, tmp);
+    }
+    wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, cur, d_wgn, d_partial);
+    mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, scal, m);
+    for (int i : o.used) finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], scal, m, 0);
+    return SFGPU_OK;
+}
+
+int sfgpu_system::residual_async(const double *x, double *f) {
+    const DLat &L = H.L;
+    const int g = grid_for(M);
+    cudaStream_t s = stream;
+    // segment weighting factors
+    for (int i = 0; i < nseg; i++) {
+        if (freedom[i] == SFGPU_SEG_FROZEN) continue;
+        swf_update<<<g, kBlock, 0, s>>>(L, x, d_jmap, nclass, class_of[i], d_range[i],
+                                        freedom[i] == SFGPU_SEG_PINNED, d_gfull[i], d_gseg[i]);
+    }
+    // molecules, solvent last (SF_MolList1stO.cpp:274-291)
+    for (int m = 0; m < nmol; m++) {
+        if (m == solvent) continue;
+        int rc = molecule_phi(m);
+        if (rc) return rc;
+    }
+    int rc = molecule_phi(solvent);
+    if (rc) return rc;
+    // state profiles
+    for (int i = 0; i < nseg; i++) {
+        if (freedom[i] == SFGPU_SEG_FROZEN) continue;
+        PtrList pl; pl.n = 0;
+        for (auto &o : mols) if (o.count[i]) pl.p[pl.n++] = o.d_phi[i];
+        sum_profiles<<<g, kBlock, 0, s>>>(M, pl, d_phi[i]);
+    }
+    bulk_scalars<<<1, 1, 0, s>>>(bp, ct, (const MolScal *)d_scal, d_phib, d_chib);
+    ResParam rp;
+    memset(&rp, 0, sizeof(rp));
+    rp.nsites = nsites; rp.nclass = nclass; rp.nseg = nseg;
+    for (int c = 0; c < nclass; c++) { rp.rep[c] = rep_of_class[c]; rp.gfull[c] = d_gfull[rep_of_class[c]]; }
+    for (int i = 0; i < nseg; i++) rp.phi[i] = d_phi[i];
+    residual<<<grid_for(nsites), kBlock, 0, s>>>(L, rp, ct, d_sites, d_chib, f);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+int sfgpu_system::free_energy(double *F) {
+    FreeParam fp;
+    memset(&fp, 0, sizeof(fp));
+    fp.nseg = nseg; fp.nmol = nmol;
+    for (int i = 0; i < nseg; i++) { fp.phi[i] = d_phi[i]; fp.gseg[i] = d_gseg[i] ? d_gseg[i] : d_phi[i]; }
+    for (int m = 0; m < nmol; m++) {
+        fp.invN[m] = 1.0 / mols[m].N;
+        fp.lnN[m] = log((double)mols[m].N);
+        fp.chemintref[m] = mols[m].chemintref;
+        for (int i : mols[m].used) fp.mphi[m * SFGPU_MAX_SEG + i] = mols[m].d_phi[i];
+    }
+    free_energy_partial<<<nblocks_red, kBlock, 0, stream>>>(H.L, fp, ct, d_wf, (const MolScal *)d_scal, d_partial);
+    finish_sums<<<1, 32, 0, stream>>>(1, nblocks_red, d_partial, d_misc);
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(F, d_misc, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(stream));
+    return SFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+#define CHECK_SYS(s) do { if (!(s)) return fail(SFGPU_ERR_INVALID, "null system"); } while (0)
+
+extern "C" int sfgpu_device_count(int *count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) { *count = 0; cudaGetLastError(); return SFGPU_ERR_NODEVICE; }
+    *count = n;
+    return n > 0 ? SFGPU_OK : SFGPU_ERR_NODEVICE;
+}
+
+extern "C" int sfgpu_system_create(const sfgpu_system_desc *desc, sfgpu_system **out) {
+    if (!desc || !out) return fail(SFGPU_ERR_INVALID, "null argument");
+    *out = nullptr;
+    int n = 0;
+    if (sfgpu_device_count(&n) != SFGPU_OK) return fail(SFGPU_ERR_NODEVICE, "no CUDA device");
+    sfgpu_system *s = new sfgpu_system();
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete s; sfgpu_set_error(e, "cudaStreamCreate", __FILE__, __LINE__); return SFGPU_ERR_CUDA; }
+    s->own_stream = true;
+    int rc = s->setup(desc);
+    if (rc) { delete s; return rc; }
+    *out = s;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_destroy(sfgpu_system *s) {
+    if (!s) return SFGPU_OK;
+    cudaStreamSynchronize(s->stream);
+    delete s;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_info(sfgpu_system *s, int *M, int *nvar, int *nclass, int *nsites) {
+    CHECK_SYS(s);
+    if (M) *M = s->M;
+    if (nvar) *nvar = (int)s->nvar;
+    if (nclass) *nclass = s->nclass;
+    if (nsites) *nsites = s->nsites;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_stream(sfgpu_system *s, void **stream) {
+    CHECK_SYS(s);
+    *stream = (void *)s->stream;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_residual(sfgpu_system *s, const double *x_dev, double *f_dev) {
+    CHECK_SYS(s);
+    return s->residual_async(x_dev, f_dev);
+}
+
+extern "C" int sfgpu_residual_host(sfgpu_system *s, const double *x, double *f) {
+    CHECK_SYS(s);
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(s->d_x, x, sizeof(double) * s->nvar, cudaMemcpyHostToDevice, s->stream));
+    int rc = s->residual_async(s->d_x, s->d_f);
+    if (rc) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(f, s->d_f, sizeof(double) * s->nvar, cudaMemcpyDeviceToHost, s->stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_set_stream(sfgpu_system *s, void *stream) {
+    CHECK_SYS(s);
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    s->own_stream = false;
+    s->stream = (cudaStream_t)stream;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_synchronize(sfgpu_system *s) {
+    CHECK_SYS(s);
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_get_phi(sfgpu_system *s, int seg, double *phi) {
+    CHECK_SYS(s);
+    if (seg < 0 || seg >= s->nseg) return fail(SFGPU_ERR_INVALID, "segment index");
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(phi, s->d_phi[seg], sizeof(double) * s->M, cudaMemcpyDeviceToHost, s->stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_get_mol_phi(sfgpu_system *s, int mol, int seg, double *phi) {
+    CHECK_SYS(s);
+    if (mol < 0 || mol >= s->nmol || seg < 0 || seg >= s->nseg) return fail(SFGPU_ERR_INVALID, "index");
+    const double *p = s->mols[mol].d_phi[seg];
+    if (!p) { memset(phi, 0, sizeof(double) * s->M); return SFGPU_OK; }
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(phi, p, sizeof(double) * s->M, cudaMemcpyDeviceToHost, s->stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_get_mol_scalars(sfgpu_system *s, int mol, double *lngn, double *phibulk, double *lnc) {
+    CHECK_SYS(s);
+    if (mol < 0 || mol >= s->nmol) return fail(SFGPU_ERR_INVALID, "molecule index");
+    MolScal v;
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(&v, (MolScal *)s->d_scal + mol, sizeof(v), cudaMemcpyDeviceToHost, s->stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (lngn) *lngn = v.lngn;
+    if (phibulk) *phibulk = v.phibulk;
+    if (lnc) *lnc = v.lnc;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_get_swf(sfgpu_system *s, int seg, double *g) {
+    CHECK_SYS(s);
+    if (seg < 0 || seg >= s->nseg || !s->d_gseg[seg]) return fail(SFGPU_ERR_INVALID, "segment index");
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(g, s->d_gseg[seg], sizeof(double) * s->M, cudaMemcpyDeviceToHost, s->stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_free_energy(sfgpu_system *s, double *F) {
+    CHECK_SYS(s);
+    return s->free_energy(F);
+}
+
+// Lattice-level entry points (Lat1stO::PropagateG, Lat2ndO::PropagateF/B,
+// Lattice::SideFraction/Sides, Lat1stO::ComputeLnGN) on device vectors
+extern "C" int sfgpu_lat_propagate(sfgpu_system *s, const double *gin, const double *g, double *gout,
+                                   double S, int backward) {
+    CHECK_SYS(s);
+    if (gin == gout) return fail(SFGPU_ERR_INVALID, "gin and gout must differ");
+    int gr = grid_for(s->M);
+    if (s->K == 1)
+        step1<<<gr, kBlock, 0, s->stream>>>(s->H.L, gin, g, gout, nullptr, nullptr, COMP_NONE);
+    else
+        step2<<<gr, kBlock, 0, s->stream>>>(s->H.L, gin, g, S, gout, nullptr, nullptr, COMP_NONE, backward);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_lat_set_boundaries(sfgpu_system *s, double *p, int components) {
+    CHECK_SYS(s);
+    if (components != 1 && components != 6) return fail(SFGPU_ERR_INVALID, "components must be 1 or 6");
+    set_boundaries<<<grid_for(s->M), kBlock, 0, s->stream>>>(s->H.L, components, p);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_lat_side_fraction(sfgpu_system *s, const double *phi, double *rho) {
+    CHECK_SYS(s);
+    side_kernel<<<grid_for(s->M), kBlock, 0, s->stream>>>(s->H.L, phi, rho);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_lat_lngn(sfgpu_system *s, const double *g, int components, double *lngn) {
+    CHECK_SYS(s);
+    if (components != 1 && components != 6) return fail(SFGPU_ERR_INVALID, "components must be 1 or 6");
+    wsum_partial<<<s->nblocks_red, kBlock, 0, s->stream>>>(s->M, components, g, s->d_wgn, s->d_partial);
+    finish_sums<<<1, 32, 0, s->stream>>>(1, s->nblocks_red, s->d_partial, s->d_misc);
+    double v = 0;
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(&v, s->d_misc, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (components == 6) v /= 6.0;
+    *lngn = log(v);
+    return SFGPU_OK;
+}
+
+// Timing of the dominant kernels on this system's buffers: reps launches of
+// a forward step and of a backward step with fused composition, bracketed by
+// CUDA events on the system stream.  Algorithmic bytes per launch follow the
+// per-site counts of the step: forward 8*(K+1+K) (read G(s-1), G, write
+// G(s)), backward 8*(K+1+K+K+2) (also read Gf(s), read and write phi).
+extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fwd, double *ms_bwd,
+                                        double *bytes_fwd, double *bytes_bwd) {
+    CHECK_SYS(s);
+    if (reps < 1) return fail(SFGPU_ERR_INVALID, "reps must be positive");
+    int mol = -1;
+    for (int m = 0; m < s->nmol; m++) if (s->mols[m].type != 0) { mol = m; break; }
+    if (mol < 0) return fail(SFGPU_ERR_INVALID, "no chain molecule to time");
+    const HMol &o = s->mols[mol];
+    const int K = s->K, M = s->M;
+    const size_t KM = (size_t)K * M;
+    size_t nslices = (size_t)(o.sym ? std::max(1, o.N / 2) : o.N);
+    if (nslices < 2) return fail(SFGPU_ERR_INVALID, "chain too short to time");
+    const double *G = s->d_gseg[o.seg[0]];
+    double *phi = o.d_phi[o.seg[0]];
+    const int g = grid_for(M);
+    cudaEvent_t e0, e1, e2;
+    SFGPU_CUDA_TRY(cudaEventCreate(&e0));
+    SFGPU_CUDA_TRY(cudaEventCreate(&e1));
+    SFGPU_CUDA_TRY(cudaEventCreate(&e2));
+    SFGPU_CUDA_TRY(cudaEventRecord(e0, s->stream));
+    for (int r = 0; r < reps; r++) {
+        size_t t = 1 + (size_t)r % (nslices - 1);
+        if (K == 1)
+            step1<<<g, kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE);
+        else
+            step2<<<g, kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, 0.2, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE, 0);
+    }
+    SFGPU_CUDA_TRY(cudaEventRecord(e1, s->stream));
+    for (int r = 0; r < reps; r++) {
+        size_t t = (size_t)r % nslices;
+        const double *src = s->d_ginv[r & 1];
+        double *dst = s->d_ginv[(r + 1) & 1];
+        if (K == 1)
+            step1<<<g, kBlock, 0, s->stream>>>(s->H.L, src, G, dst, s->d_gi + t * KM, phi, COMP_ACC);
+        else
+            step2<<<g, kBlock, 0, s->stream>>>(s->H.L, src, G, 0.2, dst, s->d_gi + t * KM, phi, COMP_ACC, 1);
+    }
+    SFGPU_CUDA_TRY(cudaEventRecord(e2, s->stream));
+    SFGPU_CUDA_TRY(cudaEventSynchronize(e2));
+    float a = 0, b = 0;
+    SFGPU_CUDA_TRY(cudaEventElapsedTime(&a, e0, e1));
+    SFGPU_CUDA_TRY(cudaEventElapsedTime(&b, e1, e2));
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    if (ms_fwd) *ms_fwd = a / reps;
+    if (ms_bwd) *ms_bwd = b / reps;
+    if (bytes_fwd) *bytes_fwd = 8.0 * (2 * K + 1) * M;
+    if (bytes_bwd) *bytes_bwd = 8.0 * (3 * K + 3) * M;
+    return SFGPU_OK;
+}

@@ -1,0 +1,47 @@
+// sfgpu_system.h -- host object behind the opaque sfgpu_system handle.
+#pragma once
+#include <vector>
+#include "sfgpu_kernels.cuh"
+
+struct HostLat {
+    DLat L;
+    std::vector<double> lam_m, lam_p, Lx, w_gn, w_f;
+};
+int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H);
+
+struct HMol {
+    int N = 0, type = 0, sym = 0, freedom = 0, pinned = 0;
+    double phibulk = 0, theta = 0, chemintref = 0;
+    std::vector<int> seg, used, count;
+    std::vector<double *> d_phi;      // per segment (used ones)
+};
+
+struct sfgpu_system {
+    HostLat H;
+    int M = 0, K = 1, nseg = 0, nmol = 0, nclass = 0, nsites = 0, solvent = -1;
+    size_t nvar = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<double> chi, pf, range_h;
+    std::vector<int> freedom, class_of, rep_of_class, sites_h;
+    std::vector<HMol> mols;
+    sfk::BulkParam bp;
+    ChiTable ct;
+    // device buffers
+    double *d_lam_m = nullptr, *d_lam_p = nullptr, *d_wgn = nullptr, *d_wf = nullptr;
+    int *d_jmap = nullptr, *d_sites = nullptr;
+    std::vector<double *> d_range, d_gfull, d_gseg, d_phi;
+    double *d_gi = nullptr, *d_ginv[2] = {nullptr, nullptr};
+    double *d_partial = nullptr, *d_scal = nullptr, *d_phib = nullptr, *d_chib = nullptr, *d_misc = nullptr;
+    double *d_x = nullptr, *d_f = nullptr;
+    int nblocks_red = 1;
+    std::vector<void *> allocs;
+
+    ~sfgpu_system();
+    int alloc_d(double **p, size_t n);
+    int alloc_i(int **p, size_t n);
+    int setup(const sfgpu_system_desc *d);
+    int molecule_phi(int m);
+    int residual_async(const double *x, double *f);
+    int free_energy(double *F);
+};

@@ -1,0 +1,225 @@
+"""System descriptions shared by the CUDA library and its checkers.
+
+``SystemSpec`` is the host-side picture of one SFbox calculation restricted to
+the SCF hot path: a lattice (``lat``), segment types (``mon``), a chi matrix,
+persistence factors (2nd order) and molecules (``mol``).  ``to_c()`` packs it
+into the ``sfgpu_system_desc`` C struct declared in ``include/sfgpu.h``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+BOUND_SURFACE, BOUND_MIRROR1, BOUND_MIRROR2, BOUND_PERIODIC = 1, 2, 3, 4
+GEOM_FLAT, GEOM_CYLINDRICAL = 0, 1
+SEG_FREE, SEG_FROZEN, SEG_PINNED = 0, 1, 2
+MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT = 0, 1, 2
+
+BOUND_NAMES = {"surface": BOUND_SURFACE, "mirror1": BOUND_MIRROR1,
+               "mirror2": BOUND_MIRROR2, "periodic": BOUND_PERIODIC}
+
+
+class LatticeDesc(C.Structure):
+    _fields_ = [("gradients", C.c_int), ("geometry", C.c_int), ("order", C.c_int),
+                ("n_layers", C.c_int * 3), ("bound_lo", C.c_int * 3), ("bound_hi", C.c_int * 3),
+                ("lam", C.c_double), ("lambda_chi", C.c_double),
+                ("layer_adjustment", C.c_double), ("dimensions", C.c_double),
+                ("offset_first_layer", C.c_double)]
+
+
+class SegmentDesc(C.Structure):
+    _fields_ = [("freedom", C.c_int), ("range", C.POINTER(C.c_double))]
+
+
+class MoleculeDesc(C.Structure):
+    _fields_ = [("n_blocks", C.c_int), ("block_segment", C.POINTER(C.c_int)),
+                ("block_length", C.POINTER(C.c_int)), ("freedom", C.c_int),
+                ("phibulk", C.c_double), ("theta", C.c_double)]
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [("lattice", LatticeDesc), ("n_segments", C.c_int),
+                ("segments", C.POINTER(SegmentDesc)), ("chi", C.POINTER(C.c_double)),
+                ("pf", C.POINTER(C.c_double)), ("n_molecules", C.c_int),
+                ("molecules", C.POINTER(MoleculeDesc))]
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def iptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+@dataclass
+class Lattice:
+    gradients: int
+    n_layers: Sequence[int]
+    bound_lo: Sequence[int]
+    bound_hi: Sequence[int]
+    geometry: int = GEOM_FLAT
+    order: int = 1
+    lam: float = 1.0 / 6.0
+    lambda_chi: float = -1.0
+    layer_adjustment: float = 1.0
+    dimensions: float = 3.0
+    offset_first_layer: float = 0.0
+
+    @property
+    def shape(self):
+        return tuple(int(n) + 2 for n in self.n_layers[: self.gradients])
+
+    @property
+    def M(self) -> int:
+        return int(np.prod(self.shape))
+
+    def to_c(self) -> LatticeDesc:
+        d = LatticeDesc()
+        d.gradients, d.geometry, d.order = self.gradients, self.geometry, self.order
+        for k in range(3):
+            d.n_layers[k] = int(self.n_layers[k]) if k < self.gradients else 0
+            d.bound_lo[k] = int(self.bound_lo[k]) if k < self.gradients else 0
+            d.bound_hi[k] = int(self.bound_hi[k]) if k < self.gradients else 0
+        d.lam, d.lambda_chi = self.lam, self.lambda_chi
+        d.layer_adjustment, d.dimensions = self.layer_adjustment, self.dimensions
+        d.offset_first_layer = self.offset_first_layer
+        return d
+
+
+@dataclass
+class Segment:
+    name: str
+    freedom: int = SEG_FREE
+    range: Optional[np.ndarray] = None      # M range values (frozen/pinned)
+
+
+@dataclass
+class Molecule:
+    name: str
+    blocks: List[tuple]                     # [(segment index, length), ...]
+    freedom: int = MOL_FREE
+    phibulk: float = 0.0
+    theta: float = 0.0
+
+    @property
+    def N(self) -> int:
+        return int(sum(n for _, n in self.blocks))
+
+
+@dataclass
+class SystemSpec:
+    lattice: Lattice
+    segments: List[Segment]
+    chi: np.ndarray
+    molecules: List[Molecule]
+    pf: Optional[np.ndarray] = None
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def M(self) -> int:
+        return self.lattice.M
+
+    def segment_index(self, name: str) -> int:
+        for i, s in enumerate(self.segments):
+            if s.name == name:
+                return i
+        raise KeyError(name)
+
+    def to_c(self) -> SystemDesc:
+        keep = []
+        ns = len(self.segments)
+        segs = (SegmentDesc * ns)()
+        for i, s in enumerate(self.segments):
+            segs[i].freedom = s.freedom
+            if s.range is not None:
+                r = np.ascontiguousarray(s.range, dtype=np.float64)
+                if r.size != self.M:
+                    raise ValueError(f"range of segment {s.name} has {r.size} values, lattice has {self.M}")
+                keep.append(r)
+                segs[i].range = dptr(r)
+            else:
+                segs[i].range = C.POINTER(C.c_double)()
+        chi = np.ascontiguousarray(self.chi, dtype=np.float64).reshape(ns, ns)
+        keep.append(chi)
+        mols = (MoleculeDesc * len(self.molecules))()
+        for m, mol in enumerate(self.molecules):
+            bs = np.array([b[0] for b in mol.blocks], dtype=np.int32)
+            bl = np.array([b[1] for b in mol.blocks], dtype=np.int32)
+            keep += [bs, bl]
+            mols[m].n_blocks = len(mol.blocks)
+            mols[m].block_segment, mols[m].block_length = iptr(bs), iptr(bl)
+            mols[m].freedom, mols[m].phibulk, mols[m].theta = mol.freedom, mol.phibulk, mol.theta
+        d = SystemDesc()
+        d.lattice = self.lattice.to_c()
+        d.n_segments = ns
+        d.segments = C.cast(segs, C.POINTER(SegmentDesc))
+        d.chi = dptr(chi)
+        if self.pf is not None:
+            pf = np.ascontiguousarray(self.pf, dtype=np.float64).reshape(ns, ns)
+            keep.append(pf)
+            d.pf = dptr(pf)
+        else:
+            d.pf = C.POINTER(C.c_double)()
+        d.n_molecules = len(self.molecules)
+        d.molecules = C.cast(mols, C.POINTER(MoleculeDesc))
+        keep += [segs, mols]
+        self._keep = keep
+        return d
+
+    # ---- helpers on the iteration-variable packing -----------------------
+    def class_layout(self):
+        """Classes of liquid segments with equal chi rows, in SFbox's order
+        (SF_Solve.cpp:53-86).  Returns (class_of_segment, n_classes)."""
+        ns = len(self.segments)
+        chi = np.asarray(self.chi, dtype=np.float64).reshape(ns, ns)
+        q = [i for i, s in enumerate(self.segments) if s.freedom != SEG_FROZEN]
+        n = len(q)
+        i = 0
+        while i < n:
+            s1 = q[i]
+            j = i + 1
+            while j < n:
+                if np.array_equal(chi[:, s1], chi[:, q[j]]):
+                    if j != i + 1:
+                        q[i + 1], q[j] = q[j], q[i + 1]
+                    i += 1
+                j += 1
+            i += 1
+        cls = [-1] * ns
+        nc = 0
+        i = 0
+        while i < n:
+            s1 = q[i]
+            cls[s1] = nc
+            j = i + 1
+            while j < n:
+                if np.array_equal(chi[:, s1], chi[:, q[j]]):
+                    i += 1
+                    cls[q[i]] = nc
+                j += 1
+            nc += 1
+            i += 1
+        return cls, nc
+
+    def itvar_sites(self) -> np.ndarray:
+        """Sites carrying iteration variables (SF_Solve.cpp:129-150)."""
+        shape = self.lattice.shape
+        interior = np.ones(shape, dtype=bool)
+        for d in range(len(shape)):
+            sl = [slice(None)] * len(shape)
+            sl[d] = 0
+            interior[tuple(sl)] = False
+            sl[d] = shape[d] - 1
+            interior[tuple(sl)] = False
+        ok = interior.reshape(-1).copy()
+        for s in self.segments:
+            if s.freedom == SEG_FROZEN and s.range is not None:
+                ok &= ~(np.asarray(s.range).reshape(-1) > 0.999)
+        return np.nonzero(ok)[0].astype(np.int64)
+
+    def n_itvar(self) -> int:
+        return len(self.itvar_sites()) * self.class_layout()[1]

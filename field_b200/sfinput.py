@@ -1,0 +1,226 @@
+"""SFbox input files: ``class : name : parameter : value`` lines.
+
+Restates the reader of SFbox's ``Input`` class (Input.cpp:20-102): one
+statement per line, four fields separated by ':', ``//`` and ``#`` start a
+comment, a line ``start`` closes a calculation, and every calculation starts
+from the values of the previous one (later statements override earlier ones).
+
+``build_system`` turns one calculation into a :class:`SystemSpec` restricted
+to the SCF hot path (``lat``, ``mon``, ``mol``, ``sys`` and ``newton``
+statements).  Unsupported features raise ``ValueError`` naming the statement.
+"""
+from __future__ import annotations
+
+import re
+from dataclasses import dataclass
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from .desc import (BOUND_NAMES, BOUND_MIRROR1, BOUND_PERIODIC, GEOM_CYLINDRICAL, GEOM_FLAT,
+                   Lattice, Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, Segment,
+                   SEG_FREE, SEG_FROZEN, SEG_PINNED, SystemSpec)
+
+Key = Tuple[str, str, str]
+
+
+def parse_input(text: str) -> List[Dict[Key, str]]:
+    """Split an input text into calculations (Input.cpp:36-102)."""
+    calcs: List[Dict[Key, str]] = []
+    cur: Dict[Key, str] = {}
+    dirty = False
+    for lineno, raw in enumerate(text.splitlines(), 1):
+        line = raw
+        for mark in ("//", "#"):
+            p = line.find(mark)
+            if p >= 0:
+                line = line[:p]
+        line = line.strip()
+        if not line:
+            continue
+        if line == "start":
+            if dirty:
+                calcs.append(dict(cur))
+                dirty = False
+            continue
+        parts = [p.strip() for p in line.split(":")]
+        if len(parts) > 4:
+            # values such as ranges never contain ':'; more fields is an error
+            raise ValueError(f"line {lineno}: line contains too many elements")
+        if len(parts) < 4 or any(p == "" for p in parts):
+            raise ValueError(f"line {lineno}: statement missing")
+        cur[(parts[0], parts[1], parts[2])] = parts[3]
+        dirty = True
+    if dirty:
+        calcs.append(dict(cur))
+    return calcs
+
+
+def _names(calc: Dict[Key, str], cls: str) -> List[str]:
+    out: List[str] = []
+    for (c, n, _p) in calc:
+        if c == cls and n not in out:
+            out.append(n)
+    return out
+
+
+def _get(calc, cls, name, param, default=None):
+    return calc.get((cls, name, param), default)
+
+
+def parse_composition(text: str) -> List[Tuple[str, int]]:
+    """Linear compositions '(A)20(B)20' (SF_MolStructure); branches are not
+    on this path."""
+    blocks = re.findall(r"\(([^()]+)\)(\d+)", text.replace(" ", ""))
+    if not blocks or "".join(f"({a}){b}" for a, b in blocks) != text.replace(" ", ""):
+        raise ValueError(f"composition '{text}' is not a linear block sequence")
+    return [(a, int(b)) for a, b in blocks]
+
+
+@dataclass
+class SolverSettings:
+    method: str = "Pure_DIIS"
+    tolerance: float = 1e-7
+    iterationlimit: int = 5000
+    m: int = 5
+    deltamax: float = 0.1
+    initial_guess_file: Optional[str] = None
+
+
+def _range_mask(lat: Lattice, text: str) -> np.ndarray:
+    """Lattice ranges (Lat1DFlat.cpp:300-388, Lat2DFlat.cpp:419-609,
+    Lat3D.cpp:596-862): 'low;high' boxes of layer coordinates (0 is the lower
+    boundary layer; 'lowerbound', 'upperbound', 'lastlayer' allowed in 1D) or
+    point lists '=(x,y,z)(x,y,z)...'."""
+    shape = lat.shape
+    mask = np.zeros(shape, dtype=np.float64)
+    t = text.replace(" ", "")
+    if t.startswith("="):
+        pts = re.findall(r"\(([^()]*)\)", t)
+        for p in pts:
+            c = tuple(int(v) for v in p.split(","))
+            if len(c) != len(shape):
+                raise ValueError(f"point '{p}' does not match {len(shape)} gradients")
+            mask[c] = 1.0
+        return mask.reshape(-1)
+    parts = t.split(";")
+    if len(parts) == 1:
+        parts = parts * 2
+    if len(parts) != 2:
+        raise ValueError(f"range '{text}'")
+
+    def coord(s: str):
+        if len(shape) == 1:
+            M = shape[0]
+            if s == "lowerbound":
+                return (0,)
+            if s == "upperbound":
+                return (M - 1,)
+            if s == "lastlayer":
+                return (M - 2,)
+        return tuple(int(v) for v in s.split(","))
+
+    lo, hi = coord(parts[0]), coord(parts[1])
+    if len(lo) != len(shape) or len(hi) != len(shape):
+        raise ValueError(f"range '{text}' does not match {len(shape)} gradients")
+    sl = tuple(slice(min(a, b), max(a, b) + 1) for a, b in zip(lo, hi))
+    mask[sl] = 1.0
+    return mask.reshape(-1)
+
+
+def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
+    lats = _names(calc, "lat")
+    if len(lats) != 1:
+        raise ValueError("exactly one 'lat' is supported")
+    ln = lats[0]
+    g = int(_get(calc, "lat", ln, "gradients", "1"))
+    geom = _get(calc, "lat", ln, "geometry", "flat")
+    if geom not in ("flat", "cylindrical"):
+        raise ValueError(f"lat : {ln} : geometry : {geom} is not on this path")
+    order = 1
+    for sysname in _names(calc, "sys"):
+        if _get(calc, "sys", sysname, "matrix_approach", "first_order") == "second_order":
+            order = 2
+    ltype = _get(calc, "lat", ln, "latticetype", "standard")
+    if ltype != "standard":
+        raise ValueError(f"lat : {ln} : latticetype : {ltype} is not on this path")
+    if g == 1:
+        n = [int(_get(calc, "lat", ln, "n_layers"))]
+        lo = [BOUND_NAMES[_get(calc, "lat", ln, "lowerbound", "mirror1")]]
+        hi = [BOUND_NAMES[_get(calc, "lat", ln, "upperbound", "mirror1")]]
+        if lo[0] == BOUND_PERIODIC or hi[0] == BOUND_PERIODIC:
+            lo = hi = [BOUND_PERIODIC]
+    else:
+        axes = "xyz"[:g]
+        n = [int(_get(calc, "lat", ln, f"n_layers_{a}")) for a in axes]
+        default = "periodic" if g == 3 else "mirror1"
+        lo, hi = [], []
+        for a in axes:
+            l = BOUND_NAMES[_get(calc, "lat", ln, f"lowerbound_{a}", default)]
+            h = BOUND_NAMES[_get(calc, "lat", ln, f"upperbound_{a}", default)]
+            if BOUND_PERIODIC in (l, h):
+                l = h = BOUND_PERIODIC
+            lo.append(l)
+            hi.append(h)
+    lam = float(_get(calc, "lat", ln, "lambda", repr(1.0 / 6.0)))
+    lat = Lattice(gradients=g, n_layers=n + [0] * (3 - g), bound_lo=lo + [0] * (3 - g),
+                  bound_hi=hi + [0] * (3 - g),
+                  geometry=GEOM_CYLINDRICAL if geom == "cylindrical" else GEOM_FLAT,
+                  order=order, lam=lam,
+                  lambda_chi=float(_get(calc, "lat", ln, "lambda_chi", "-1")),
+                  layer_adjustment=float(_get(calc, "lat", ln, "layer_adjustment", "1")),
+                  dimensions=float(_get(calc, "lat", ln, "dimensions", "3")),
+                  offset_first_layer=float(_get(calc, "lat", ln, "offset_first_layer_x", "0")))
+    # segments
+    seg_names = _names(calc, "mon")
+    segs: List[Segment] = []
+    for sn in seg_names:
+        fr = _get(calc, "mon", sn, "freedom", "free")
+        if fr == "free":
+            segs.append(Segment(sn, SEG_FREE))
+        elif fr == "frozen":
+            segs.append(Segment(sn, SEG_FROZEN, _range_mask(lat, _get(calc, "mon", sn, "frozen_range"))))
+        elif fr == "pinned":
+            segs.append(Segment(sn, SEG_PINNED, _range_mask(lat, _get(calc, "mon", sn, "pinned_range"))))
+        else:
+            raise ValueError(f"mon : {sn} : freedom : {fr} is not on this path")
+    ns = len(segs)
+    chi = np.zeros((ns, ns))
+    pf = np.full((ns, ns), 0.2)
+    for i, a in enumerate(seg_names):
+        for j, b in enumerate(seg_names):
+            v = _get(calc, "mon", a, f"chi - {b}")
+            if v is not None:
+                chi[i, j] = chi[j, i] = float(v)
+            v = _get(calc, "mon", a, f"Pf - {b}")
+            if v is not None:
+                pf[i, j] = pf[j, i] = float(v)
+    mols: List[Molecule] = []
+    for mn in _names(calc, "mol"):
+        comp = parse_composition(_get(calc, "mol", mn, "composition"))
+        blocks = [(seg_names.index(a), n_) for a, n_ in comp]
+        fr = _get(calc, "mol", mn, "freedom", "free")
+        if fr == "free":
+            mols.append(Molecule(mn, blocks, MOL_FREE, phibulk=float(_get(calc, "mol", mn, "phibulk"))))
+        elif fr == "restricted":
+            th = _get(calc, "mol", mn, "theta")
+            if th is None:
+                nn = _get(calc, "mol", mn, "n")
+                if nn is None:
+                    raise ValueError(f"mol : {mn} needs theta or n")
+                th = float(nn) * sum(b for _, b in blocks)
+            mols.append(Molecule(mn, blocks, MOL_RESTRICTED, theta=float(th)))
+        elif fr == "solvent":
+            mols.append(Molecule(mn, blocks, MOL_SOLVENT))
+        else:
+            raise ValueError(f"mol : {mn} : freedom : {fr} is not on this path")
+    spec = SystemSpec(lat, segs, chi, mols, pf=pf if order == 2 else None)
+    st = SolverSettings()
+    for nn in _names(calc, "newton"):
+        st.method = _get(calc, "newton", nn, "method", st.method)
+        st.tolerance = float(_get(calc, "newton", nn, "tolerance", st.tolerance))
+        st.iterationlimit = int(_get(calc, "newton", nn, "iterationlimit", st.iterationlimit))
+        st.m = int(_get(calc, "newton", nn, "m", st.m))
+        st.deltamax = float(_get(calc, "newton", nn, "deltamax", st.deltamax))
+        st.initial_guess_file = _get(calc, "newton", nn, "initial_guess_input_file")
+    return spec, st

@@ -1,0 +1,160 @@
+"""Host-side mirror of SFbox's solver-facing API over the C ABI.
+
+``System`` owns one SF-SCF system on the GPU (``sfgpu_system``).  Its methods
+map onto the reference interfaces: ``residual`` is ``SF_Solve::residuals``
+(SF_Solve.cpp:647), ``phi``/``mol_phi`` read ``SF_State::GetPhi`` /
+``SF_Molecule::GetPhi`` results, ``free_energy`` is
+``SF_MolList1stO::GetFreeEnergy`` (SF_MolList1stO.cpp:606) and ``solve`` runs
+``SFNewton::PlainLBFGSDIIS`` (sfnewton.cpp:566) on the device.  The
+Lattice-level methods (``propagate``, ``side_fraction``, ``lngn``) take torch
+CUDA tensors and mirror ``Lat1stO::PropagateG`` / ``Lat2ndO::PropagateF/B``,
+``Lattice::SideFraction`` and ``Lat1stO::ComputeLnGN``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as nat
+from .desc import SystemSpec
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+@dataclass
+class SolveResult:
+    x: np.ndarray
+    status: int
+    iterations: int
+    error: float
+
+    @property
+    def converged(self) -> bool:
+        return self.status == 0
+
+
+class System:
+    def __init__(self, spec: SystemSpec):
+        self.lib = nat.load()
+        self.spec = spec
+        self._desc = spec.to_c()
+        h = C.c_void_p()
+        nat.check(self.lib.sfgpu_system_create(C.byref(self._desc), C.byref(h)), "sfgpu_system_create")
+        self.h = h
+        M, nv, nc, ns = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        nat.check(self.lib.sfgpu_system_info(h, C.byref(M), C.byref(nv), C.byref(nc), C.byref(ns)), "info")
+        self.M, self.nvar, self.nclass, self.nsites = M.value, nv.value, nc.value, ns.value
+        self.K = 6 if spec.lattice.order == 2 else 1
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sfgpu_system_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- SF_Solve-level ----------------------------------------------------
+    def residual(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != self.nvar:
+            raise ValueError(f"x has {x.size} values, system has {self.nvar} iteration variables")
+        f = np.empty(self.nvar)
+        nat.check(self.lib.sfgpu_residual_host(self.h, _d(x), _d(f)), "sfgpu_residual_host")
+        return f
+
+    def residual_device(self, x_ptr: int, f_ptr: int):
+        """x -> f on device pointers, asynchronous on the system's stream."""
+        nat.check(self.lib.sfgpu_residual(self.h, C.c_void_p(x_ptr), C.c_void_p(f_ptr)), "sfgpu_residual")
+
+    def use_stream(self, stream_handle: int):
+        """Launch on a caller-owned CUDA stream (e.g. torch's current stream)."""
+        nat.check(self.lib.sfgpu_system_set_stream(self.h, C.c_void_p(stream_handle)), "set_stream")
+
+    def synchronize(self):
+        nat.check(self.lib.sfgpu_synchronize(self.h), "sfgpu_synchronize")
+
+    def phi(self, seg: int) -> np.ndarray:
+        out = np.empty(self.M)
+        nat.check(self.lib.sfgpu_get_phi(self.h, seg, _d(out)), "sfgpu_get_phi")
+        return out
+
+    def mol_phi(self, mol: int, seg: int) -> np.ndarray:
+        out = np.empty(self.M)
+        nat.check(self.lib.sfgpu_get_mol_phi(self.h, mol, seg, _d(out)), "sfgpu_get_mol_phi")
+        return out
+
+    def swf(self, seg: int) -> np.ndarray:
+        out = np.empty(self.M)
+        nat.check(self.lib.sfgpu_get_swf(self.h, seg, _d(out)), "sfgpu_get_swf")
+        return out
+
+    def mol_scalars(self, mol: int):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        nat.check(self.lib.sfgpu_get_mol_scalars(self.h, mol, C.byref(a), C.byref(b), C.byref(c)),
+                  "sfgpu_get_mol_scalars")
+        return {"lngn": a.value, "phibulk": b.value, "lnc": c.value}
+
+    def free_energy(self) -> float:
+        F = C.c_double()
+        nat.check(self.lib.sfgpu_free_energy(self.h, C.byref(F)), "sfgpu_free_energy")
+        return F.value
+
+    def solve(self, x0=None, tol=1e-7, maxit=5000, m=5, eta=0.1) -> SolveResult:
+        x = np.zeros(self.nvar) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+        it, err = C.c_int(), C.c_double()
+        rc = self.lib.sfgpu_solve_diis(self.h, _d(x), tol, maxit, m, eta, C.byref(it), C.byref(err))
+        if rc not in (0, 5, 4):
+            nat.check(rc, "sfgpu_solve_diis")
+        return SolveResult(x, rc, it.value, err.value)
+
+    def profile_propagator(self, reps: int = 200):
+        a, b, c, d = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        nat.check(self.lib.sfgpu_profile_propagator(self.h, reps, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
+                  "sfgpu_profile_propagator")
+        return {"ms_fwd": a.value, "ms_bwd": b.value, "bytes_fwd": c.value, "bytes_bwd": d.value}
+
+    # ---- Lattice-level (torch CUDA tensors) -------------------------------
+    def _sync_torch(self):
+        import torch
+        torch.cuda.synchronize()
+
+    def propagate(self, gin, g, S: float = 0.2, backward: bool = False):
+        import torch
+        out = torch.empty_like(gin)
+        self._sync_torch()
+        nat.check(self.lib.sfgpu_lat_propagate(self.h, C.c_void_p(gin.data_ptr()), C.c_void_p(g.data_ptr()),
+                                               C.c_void_p(out.data_ptr()), float(S), int(backward)),
+                  "sfgpu_lat_propagate")
+        self.synchronize()
+        return out
+
+    def side_fraction(self, phi):
+        import torch
+        out = torch.empty_like(phi)
+        self._sync_torch()
+        nat.check(self.lib.sfgpu_lat_side_fraction(self.h, C.c_void_p(phi.data_ptr()), C.c_void_p(out.data_ptr())),
+                  "sfgpu_lat_side_fraction")
+        self.synchronize()
+        return out
+
+    def set_boundaries(self, p):
+        self._sync_torch()
+        comps = p.numel() // self.M
+        nat.check(self.lib.sfgpu_lat_set_boundaries(self.h, C.c_void_p(p.data_ptr()), comps), "set_boundaries")
+        self.synchronize()
+        return p
+
+    def lngn(self, g) -> float:
+        self._sync_torch()
+        v = C.c_double()
+        nat.check(self.lib.sfgpu_lat_lngn(self.h, C.c_void_p(g.data_ptr()), g.numel() // self.M, C.byref(v)),
+                  "sfgpu_lat_lngn")
+        return v.value

@@ -1,0 +1,206 @@
+/*
+ * sfgpu.h -- C ABI of the B200-native Scheutjens-Fleer SCF hot path.
+ *
+ * The library (field_b200/libsfgpu.so) replaces the propagation, composition,
+ * segment-potential update and residual steps of SFbox 2.1 (the Wageningen
+ * SF-SCF lattice program).  Every entry point is plain C: scalars, raw
+ * pointers and sizes, no C++ or torch types.  Device pointers are CUDA
+ * global-memory pointers on the current device; host pointers are ordinary
+ * process memory.  Every call returns an int status (SFGPU_OK == 0).
+ *
+ * Index conventions follow SFbox: a lattice with n interior layers per
+ * gradient carries one boundary layer on each side, so M = prod(n_i + 2).
+ * Site z (0-based here, 1-based in SFbox) is ordered with the LAST gradient
+ * fastest: 2D z = x*MY + y, 3D z = x*MY*MZ + y*MZ + z (Lat2DFlat.cpp:43-46,
+ * Lat3D.cpp:59-68).  Iteration variables use SFbox's packing: for every site
+ * that carries iteration variables, in site order, one value per class of
+ * liquid segments with identical interaction parameters
+ * (SF_Solve.cpp:53-86, 129-163, 794-812).
+ *
+ * Reference interfaces replaced (file:line in SFbox):
+ *   Lat1stO  PropagateG/ConnectG/CorrectDoubleCountG/ComputeLnGN/NormPhi*  Lat1stO.h:7-50
+ *   Lat2ndO  PropagateF/PropagateB/ConnectG(PHI)                            Lat2ndO.h:7-66
+ *   SF_Molecule::ComputePhi (Matrix1 / CudaMatrix1)                         SF_Molecule.h:16
+ *   SF_Solve::residuals / UpdateSWF / GetResiduals                          SF_Solve.cpp:647,794,527
+ *   SFNewton::iterate (Pure_DIIS, LBFGS, TN)                                sfnewton.cpp:566,844
+ *   Cuda_tools.h free functions (Forward/Backward/Composition/...)          Cuda_tools.h:4-27
+ */
+#ifndef SFGPU_H
+#define SFGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SFGPU_OK               0
+#define SFGPU_ERR_INVALID      1   /* bad argument or unsupported combination */
+#define SFGPU_ERR_NOMEM        2   /* device or host allocation failed */
+#define SFGPU_ERR_CUDA         3   /* a CUDA runtime call failed */
+#define SFGPU_ERR_NONFINITE    4   /* NaN/Inf met in a residual or norm */
+#define SFGPU_ERR_NOTCONVERGED 5   /* iteration limit reached */
+#define SFGPU_ERR_TIMEOUT      6   /* a bounded device wait gave up */
+#define SFGPU_ERR_UNSUPPORTED  7   /* feature outside the implemented path */
+#define SFGPU_ERR_NODEVICE     8   /* no CUDA device present */
+
+/* ---- enumerations (values equal SFbox's input-choice indices) ---------- */
+/* lowerbound/upperbound choices, Lat1DFlat.cpp:26-31, Lat2DFlat.cpp:47-52.
+ * The 3D lattice has no 'surface' choice (Lat3D.cpp:68-72); pass MIRROR1,
+ * MIRROR2 or PERIODIC there. */
+#define SFGPU_BOUND_SURFACE   1
+#define SFGPU_BOUND_MIRROR1   2
+#define SFGPU_BOUND_MIRROR2   3
+#define SFGPU_BOUND_PERIODIC  4
+
+#define SFGPU_GEOM_FLAT        0
+#define SFGPU_GEOM_CYLINDRICAL 1
+
+/* segment freedom, SF_Segment.cpp:61-65 ('grafted' is not on this path) */
+#define SFGPU_SEG_FREE    0
+#define SFGPU_SEG_FROZEN  1
+#define SFGPU_SEG_PINNED  2
+
+/* molecule freedom, SF_Molecule.cpp:47-54 (free, restricted, solvent) */
+#define SFGPU_MOL_FREE       0
+#define SFGPU_MOL_RESTRICTED 1
+#define SFGPU_MOL_SOLVENT    2
+
+/* solver methods */
+#define SFGPU_METHOD_DIIS      1   /* SFNewton::PlainLBFGSDIIS, sfnewton.cpp:566-664 */
+#define SFGPU_METHOD_ANDERSON  2   /* DIIS on residual history (project addition) */
+#define SFGPU_METHOD_NK        3   /* Newton-Krylov with exact tangent J*v */
+
+/* ---- system description ------------------------------------------------ */
+typedef struct {
+    int    gradients;          /* 1, 2 or 3 */
+    int    geometry;           /* SFGPU_GEOM_*; cylindrical only with 2 gradients */
+    int    order;              /* 1 = first-order chains, 2 = semiflexible (3D) */
+    int    n_layers[3];        /* interior layers per gradient (unused entries 0) */
+    int    bound_lo[3];        /* SFGPU_BOUND_* per gradient */
+    int    bound_hi[3];
+    double lambda;             /* a-priori step probability l1 (1D/2D); 3D uses 1/6 */
+    double lambda_chi;         /* l1 used in contact averages; < 0 means lambda */
+    double layer_adjustment;   /* 1D only (Lat1DFlat.cpp:139); 1 = none */
+    double dimensions;         /* cylinder: spatial dimensions D (default 3) */
+    double offset_first_layer; /* cylinder: offset_first_layer_x (default 0) */
+} sfgpu_lattice_desc;
+
+typedef struct {
+    int           freedom;     /* SFGPU_SEG_* */
+    const double *range;       /* host array of M range values for frozen and
+                                  pinned segments (1 inside the range), else NULL */
+} sfgpu_segment_desc;
+
+typedef struct {
+    int        n_blocks;       /* composition (A)n1(B)n2... as blocks */
+    const int *block_segment;  /* segment index of each block */
+    const int *block_length;   /* length of each block */
+    int        freedom;        /* SFGPU_MOL_* */
+    double     phibulk;        /* free molecules */
+    double     theta;          /* restricted molecules */
+} sfgpu_molecule_desc;
+
+typedef struct {
+    sfgpu_lattice_desc         lattice;
+    int                        n_segments;
+    const sfgpu_segment_desc  *segments;
+    const double              *chi;   /* n_segments*n_segments, row-major, symmetric */
+    const double              *pf;    /* n_segments*n_segments persistence factors
+                                         S for 2nd order (NULL: 0.2 everywhere,
+                                         SF_Copol2ndO.cpp:234-247) */
+    int                        n_molecules;
+    const sfgpu_molecule_desc *molecules;
+} sfgpu_system_desc;
+
+typedef struct sfgpu_system sfgpu_system;   /* opaque handle, owns device buffers */
+
+/* ---- library ------------------------------------------------------------ */
+/* Message of the last failed call on this host thread.  SFbox prints GPU
+ * errors and continues (Cuda_tools.cu:174-175); here every call returns a
+ * status and the text is kept for the caller. */
+const char *sfgpu_last_error(void);
+/* Number of CUDA devices (SFGPU_ERR_NODEVICE when none).
+ * Replaces GPU_present(), Cuda_tools.h:4. */
+int sfgpu_device_count(int *count);
+
+/* ---- system lifetime ---------------------------------------------------- */
+/* Build the lattice, segment/state tables, molecule chains and device
+ * buffers of one system on the current device.  Takes the place of the
+ * construction in SF_System::SF_System (SF_System.cpp:13-100) for the hot
+ * path and of the per-call cudaMalloc of SF_Homopol1stO::CudaMatrix1
+ * (SF_Homopol1stO.cpp:639-643): buffers are allocated once here. */
+int sfgpu_system_create(const sfgpu_system_desc *desc, sfgpu_system **out);
+int sfgpu_system_destroy(sfgpu_system *sys);
+/* M (sites incl. boundaries), number of iteration variables, classes and
+ * sites carrying iteration variables (SF_Solve.cpp:129-163). */
+int sfgpu_system_info(sfgpu_system *sys, int *M, int *nvar, int *nclass, int *nsites);
+/* CUDA stream (cudaStream_t) all work of this system is queued on. */
+int sfgpu_system_stream(sfgpu_system *sys, void **stream);
+/* Queue all further work of this system on the caller's stream (for example
+ * torch.cuda.current_stream().cuda_stream); the caller keeps it alive. */
+int sfgpu_system_set_stream(sfgpu_system *sys, void *stream);
+int sfgpu_synchronize(sfgpu_system *sys);
+
+/* ---- SF_Solve-level ----------------------------------------------------- */
+/* f = residuals(x) on device pointers, asynchronous on the system stream:
+ * UpdateSWF + MolQ->ComputePhi + GetResiduals, SF_Solve::residuals
+ * (SF_Solve.cpp:647-651). */
+int sfgpu_residual(sfgpu_system *sys, const double *x_dev, double *f_dev);
+/* same on host arrays, copies included, synchronous */
+int sfgpu_residual_host(sfgpu_system *sys, const double *x, double *f);
+/* Results of the last residual evaluation (host copies, synchronous):
+ * state profile phi (SF_State::GetPhi, SF_State.cpp:302), the profile of one
+ * segment type inside one molecule (SF_MolSegment::GetPhi), the segment
+ * weighting factor G (SF_MolSegment::GetSWF) and the molecule scalars lnGN,
+ * phibulk and ln C (SF_Molecule::GetLnGN/GetPhiBulk/GetLnNormFree). */
+int sfgpu_get_phi(sfgpu_system *sys, int segment, double *phi);
+int sfgpu_get_mol_phi(sfgpu_system *sys, int molecule, int segment, double *phi);
+int sfgpu_get_swf(sfgpu_system *sys, int segment, double *g);
+int sfgpu_get_mol_scalars(sfgpu_system *sys, int molecule, double *lngn, double *phibulk, double *lnc);
+/* Helmholtz free energy of the last evaluation,
+ * SF_MolList1stO::GetFreeEnergy (SF_MolList1stO.cpp:606-635). */
+int sfgpu_free_energy(sfgpu_system *sys, double *F);
+
+/* ---- Lattice-level (device vectors of M or 6*M doubles) ----------------- */
+/* gout = one propagator step of gin with segment weights g.  First order:
+ * Lat1stO::PropagateG(Gi, G, Gout) (Lat1stO.h:22; Lat1DFlat1stO.cpp:101-113,
+ * Lat2DCyl1stO.cpp:72-97, Lat3D1stO.cpp:51-90).  Second order:
+ * Lat2ndO::PropagateF (backward = 0) / PropagateB (backward = 1) with
+ * persistence factor S (Lat3D2ndO.cpp:65-152, :597-678).  Boundary entries of
+ * gout hold SetBoundaries copies. */
+int sfgpu_lat_propagate(sfgpu_system *sys, const double *gin, const double *g, double *gout,
+                        double S, int backward);
+/* Lattice::SetBoundaries on 1 or 6 components (Lat3D.cpp:1510-1562; the six
+ * components swap direction at mirrors, Lat3D2ndO.cpp:84-89) */
+int sfgpu_lat_set_boundaries(sfgpu_system *sys, double *p, int components);
+/* rho(z) = contact average of phi: Lattice::SideFraction for 1 and 2
+ * gradients (Lat1DFlat.cpp:511-524, Lat2DCylinder.cpp:205-320), Sides for 3
+ * (Lat3D.cpp:1729-1785) */
+int sfgpu_lat_side_fraction(sfgpu_system *sys, const double *phi, double *rho);
+/* Lat1stO::ComputeLnGN (Lat1DFlat1stO.cpp:301-316, Lat3D1stO.cpp:344-370,
+ * Lat3D2ndO.cpp:995-1025) of an end-point distribution */
+int sfgpu_lat_lngn(sfgpu_system *sys, const double *g, int components, double *lngn);
+
+/* ---- measurement ------------------------------------------------------- */
+/* Average device time of one forward propagator step and of one backward
+ * step with fused composition on this system's buffers (reps launches each,
+ * CUDA events on the system stream), with their algorithmic bytes per launch
+ * (8 bytes per value read or written once).  Propagator contents are
+ * overwritten; call before the next residual. */
+int sfgpu_profile_propagator(sfgpu_system *sys, int reps, double *ms_fwd, double *ms_bwd,
+                             double *bytes_fwd, double *bytes_bwd);
+
+/* ---- iterations ------------------------------------------------------- */
+/* Pure_DIIS: SFNewton::PlainLBFGSDIIS (sfnewton.cpp:566-664) on the device,
+ * coefficients as SFNewton::Ax (sfnewton.cpp:531-557).  x is a host array,
+ * in: initial guess, out: last iterate.  Returns SFGPU_ERR_NOTCONVERGED when
+ * maxit is reached, SFGPU_ERR_NONFINITE on a NaN/Inf residual. */
+int sfgpu_solve_diis(sfgpu_system *sys, double *x, double tol, int maxit, int m, double eta,
+                     int *iterations, double *final_error);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SFGPU_H */

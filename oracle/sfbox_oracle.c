@@ -1,0 +1,928 @@
+/*
+ * sfbox_oracle.c -- TEST INFRASTRUCTURE ONLY: the checker for the CUDA
+ * library, never linked into it, never the thing measured or shipped.
+ *
+ * A plain-C restatement of the SFbox 2.1 SF-SCF hot path (lattice
+ * propagators, Gf*Gb/G composition, normalisation, segment-potential update,
+ * residual, free energy and the Pure_DIIS iteration).  Every function cites
+ * the reference lines it follows.  Arrays are 0-based; SFbox's 1-based site
+ * z corresponds to index z-1 here.
+ *
+ * Parity unpinned: SFbox has no tests or golden files for this path and it
+ * cannot be built in this environment (it needs the absent 'fenk' container
+ * library and CLAPACK), so this file is validated by known-answer tests
+ * derived from the equations.
+ *
+ * Where SFbox leaves boundary-site values unspecified (3D propagator slices
+ * keep stale scratch values on the boundary planes, Lat3D1stO.cpp:151-157;
+ * contact averages on mirror boundary rows, Lat2DCylinder.cpp:205-320), this
+ * file writes the SetBoundaries copy instead.  Those values never reach an
+ * interior residual, lnGN or the free energy.
+ */
+#include "sfbox_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdio.h>
+
+/* ------------------------------------------------------------------------ */
+/* lattice                                                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int grad, cyl, order;
+    int n[3];          /* interior layers */
+    int Md[3];         /* layers incl. the two boundary layers (1 if unused) */
+    int M;
+    int st[3];         /* strides, last gradient fastest */
+    int bc_lo[3], bc_hi[3];     /* SFGPU_BOUND_* */
+    int map_lo[3], map_hi[3];   /* coordinate copied into 0 / Md-1 */
+    double l1, l1chi, ladj;
+    double *lam_m, *lam_p, *Lx; /* cylinder tables by 0-based x (0..MX-1) */
+    double *w_gn;      /* weights of interior sites in lnGN sums */
+    double *w_f;       /* weights in the free-energy sum (surfaces included) */
+} olat;
+
+static int map_lo_of(int bc, int n) {
+    /* Lat1DFlat.cpp:81-88, Lat2DFlat.cpp:140-145, Lat3D.cpp:205-210 */
+    switch (bc) {
+        case SFGPU_BOUND_SURFACE: return 0;
+        case SFGPU_BOUND_MIRROR1: return 1;
+        case SFGPU_BOUND_MIRROR2: return 2;
+        case SFGPU_BOUND_PERIODIC: return n;
+    }
+    return -1;
+}
+static int map_hi_of(int bc, int n) {
+    switch (bc) {
+        case SFGPU_BOUND_SURFACE: return n + 1;
+        case SFGPU_BOUND_MIRROR1: return n;
+        case SFGPU_BOUND_MIRROR2: return n - 1;
+        case SFGPU_BOUND_PERIODIC: return 1;
+    }
+    return -1;
+}
+
+static void coords(const olat *L, int z, int c[3]) {
+    c[0] = c[1] = c[2] = 0;
+    if (L->grad == 1) { c[0] = z; return; }
+    if (L->grad == 2) { c[0] = z / L->Md[1]; c[1] = z % L->Md[1]; return; }
+    c[0] = z / L->st[0]; c[1] = (z % L->st[0]) / L->st[1]; c[2] = z % L->st[1];
+}
+static int site(const olat *L, const int c[3]) {
+    return c[0] * L->st[0] + c[1] * L->st[1] + c[2] * L->st[2];
+}
+static int is_interior(const olat *L, int z) {
+    int c[3]; coords(L, z, c);
+    for (int d = 0; d < L->grad; d++) if (c[d] == 0 || c[d] == L->Md[d] - 1) return 0;
+    return 1;
+}
+/* site whose value a boundary site copies (the site itself if interior or on
+   a surface); swapmask gets one bit per mirrored gradient */
+static int mapped_site(const olat *L, int z, int *swapmask) {
+    int c[3]; coords(L, z, c);
+    int m = 0;
+    for (int d = 0; d < L->grad; d++) {
+        if (c[d] == 0) {
+            c[d] = L->map_lo[d];
+            if (L->bc_lo[d] == SFGPU_BOUND_MIRROR1 || L->bc_lo[d] == SFGPU_BOUND_MIRROR2) m |= 1 << d;
+        } else if (c[d] == L->Md[d] - 1) {
+            c[d] = L->map_hi[d];
+            if (L->bc_hi[d] == SFGPU_BOUND_MIRROR1 || L->bc_hi[d] == SFGPU_BOUND_MIRROR2) m |= 1 << d;
+        }
+    }
+    if (swapmask) *swapmask = m;
+    return site(L, c);
+}
+
+/* SetBoundaries: Lat1DFlat.cpp:396-399, Lat2DFlat.cpp:619-666, Lat3D.cpp:1510-1562 */
+static void olat_set_boundaries(const olat *L, double *P) {
+    for (int z = 0; z < L->M; z++) {
+        if (is_interior(L, z)) continue;
+        int m = mapped_site(L, z, NULL);
+        if (m != z) P[z] = P[m];
+    }
+}
+
+/* direction swap of the 2nd-order components at mirror boundaries,
+   Lat3D2ndO.cpp:84-89 with Lat3D.cpp:1276-1290 (k: 0=+x 1=+y 2=+z 3=-z 4=-y 5=-x) */
+static void olat_set_boundaries6(const olat *L, double *P) {
+    for (int z = 0; z < L->M; z++) {
+        if (is_interior(L, z)) continue;
+        int sw;
+        int m = mapped_site(L, z, &sw);
+        if (m == z) continue;
+        for (int k = 0; k < 6; k++) {
+            int kk = k;
+            if (sw & 1) { if (kk == 0) kk = 5; else if (kk == 5) kk = 0; }
+            if (sw & 2) { if (kk == 1) kk = 4; else if (kk == 4) kk = 1; }
+            if (sw & 4) { if (kk == 2) kk = 3; else if (kk == 3) kk = 2; }
+            P[k * L->M + z] = P[kk * L->M + m];
+        }
+    }
+}
+
+static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
+    memset(L, 0, sizeof(*L));
+    L->grad = d->gradients;
+    L->order = d->order;
+    L->cyl = (d->gradients == 2 && d->geometry == SFGPU_GEOM_CYLINDRICAL);
+    if (L->grad < 1 || L->grad > 3) return SFGPU_ERR_INVALID;
+    if (d->geometry == SFGPU_GEOM_CYLINDRICAL && d->gradients != 2) return SFGPU_ERR_UNSUPPORTED;
+    if (L->order == 2 && L->grad != 3) return SFGPU_ERR_UNSUPPORTED;
+    for (int k = 0; k < 3; k++) { L->Md[k] = 1; }
+    for (int k = 0; k < L->grad; k++) {
+        L->n[k] = d->n_layers[k];
+        if (L->n[k] < 1) return SFGPU_ERR_INVALID;
+        L->Md[k] = L->n[k] + 2;
+        int lo = d->bound_lo[k], hi = d->bound_hi[k];
+        if (lo < 1 || lo > 4 || hi < 1 || hi > 4) return SFGPU_ERR_INVALID;
+        if ((lo == SFGPU_BOUND_PERIODIC) != (hi == SFGPU_BOUND_PERIODIC)) return SFGPU_ERR_INVALID;
+        if (L->grad == 3 && (lo == SFGPU_BOUND_SURFACE || hi == SFGPU_BOUND_SURFACE)) return SFGPU_ERR_INVALID;
+        if ((lo == SFGPU_BOUND_MIRROR2 || hi == SFGPU_BOUND_MIRROR2) && L->n[k] < 2) return SFGPU_ERR_INVALID;
+        L->bc_lo[k] = lo; L->bc_hi[k] = hi;
+        L->map_lo[k] = map_lo_of(lo, L->n[k]);
+        L->map_hi[k] = map_hi_of(hi, L->n[k]);
+    }
+    L->M = L->Md[0] * L->Md[1] * L->Md[2];
+    L->st[2] = 1; L->st[1] = L->Md[2]; L->st[0] = L->Md[1] * L->Md[2];
+    if (L->grad == 1) { L->st[0] = 1; L->st[1] = L->st[2] = 0; }
+    if (L->grad == 2) { L->st[0] = L->Md[1]; L->st[1] = 1; L->st[2] = 0; }
+    L->l1 = (L->grad == 3) ? 1.0 / 6.0 : d->lambda;   /* Lat3D.cpp:231-236 */
+    L->l1chi = (d->lambda_chi >= 0 && L->grad == 1) ? d->lambda_chi : L->l1;
+    L->ladj = (L->grad == 1 && d->layer_adjustment > 0) ? d->layer_adjustment : 1.0;
+
+    int MX = L->Md[0];
+    if (L->cyl) {
+        /* Lat2DCylinder.cpp:7-55 (tables indexed 1..MX there, 0..MX-1 here) */
+        const double PI_ = 4.0 * atan(1.0);
+        double off = d->offset_first_layer;
+        double D = (d->dimensions > 0 ? d->dimensions : 3.0) - 1;
+        double ladj = 1.0;
+        double *V = calloc(MX + 1, sizeof(double)), *S = calloc(MX + 1, sizeof(double));
+        double *lm = calloc(MX + 1, sizeof(double)), *lp = calloc(MX + 1, sizeof(double));
+        double *LL = calloc(MX + 1, sizeof(double));
+        S[1] = off * PI_ * 2; V[1] = off * off * PI_; LL[1] = V[1];
+        for (int z = 2; z <= MX; z++) {
+            double x = z + off - 2 + ladj;
+            V[z] = (PI_ * pow(2, (D - 1)) / D) * pow(x, D);
+            LL[z] = V[z] - V[z - 1];
+            S[z] = pow(2, (D - 1)) * PI_ * pow(x, (D - 1));
+            lm[z] = L->l1 * S[z - 1] / LL[z];
+            lp[z] = L->l1 * S[z] / LL[z];
+        }
+        lp[MX] = 0;
+        if (LL[1] > PI_) LL[1] = V[1] - (off - 1) * (off - 1) * PI_;
+        if (LL[1] > 0) lp[1] = LL[2] * lm[2] / LL[1];
+        L->lam_m = calloc(MX, sizeof(double)); L->lam_p = calloc(MX, sizeof(double));
+        L->Lx = calloc(MX, sizeof(double));
+        for (int x = 0; x < MX; x++) { L->lam_m[x] = lm[x + 1]; L->lam_p[x] = lp[x + 1]; L->Lx[x] = LL[x + 1]; }
+        free(V); free(S); free(lm); free(lp); free(LL);
+    }
+
+    /* site weights: SubtractBoundaries + MultiplyWithLatticeSites
+       (Lat1DFlat.cpp:266-269,410-415; Lat2DFlat.cpp:716-731; Lat2DCylinder.cpp:156-164;
+        Lat3D.cpp:1591-1633) */
+    L->w_gn = calloc(L->M, sizeof(double));
+    L->w_f = calloc(L->M, sizeof(double));
+    for (int z = 0; z < L->M; z++) {
+        int c[3]; coords(L, z, c);
+        double w = 1.0; int keep = 1, interior = 1;
+        for (int k = 0; k < L->grad; k++) {
+            int last = L->Md[k] - 1;
+            if (c[k] == 0) { interior = 0; if (L->bc_lo[k] != SFGPU_BOUND_SURFACE) keep = 0; }
+            else if (c[k] == last) { interior = 0; if (L->bc_hi[k] != SFGPU_BOUND_SURFACE) keep = 0; }
+            else {
+                if (c[k] == 1 && L->bc_lo[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
+                else if (c[k] == last - 1 && L->bc_hi[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
+            }
+        }
+        if (L->cyl) w *= L->Lx[c[0]];
+        if (L->grad == 1) {
+            if (z == 1) w *= L->ladj;
+            if (z == L->M - 2 && L->M > 3) w *= (2 - L->ladj);
+        }
+        L->w_f[z] = keep ? w : 0.0;
+        L->w_gn[z] = interior ? w : 0.0;
+    }
+    return SFGPU_OK;
+}
+
+static void olat_free(olat *L) {
+    free(L->lam_m); free(L->lam_p); free(L->Lx); free(L->w_gn); free(L->w_f);
+}
+
+/* one first-order step gout = G * stencil(gin); gin must carry valid
+   boundary copies.  Op order as in Lat1DFlat1stO.cpp:37-50,
+   Lat2DFlat1stO.cpp:32-53, Lat2DCyl1stO.cpp:17-39, Lat3D1stO.cpp:134-163 */
+static void olat_prop1(const olat *L, const double *gin, const double *G, double *gout) {
+    int M = L->M;
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(L, z)) continue;
+        double g = G[z], r;
+        if (L->grad == 1) {
+            double a = gin[z - 1], b = gin[z], c = gin[z + 1];
+            r = g * (b + L->l1 * (a - b - b + c));
+        } else if (L->grad == 2) {
+            int MY = L->Md[1];
+            double a = gin[z - 1], b = gin[z], c = gin[z + 1];
+            double u = gin[z - MY], dn = gin[z + MY];
+            if (L->cyl) {
+                int x = z / MY;
+                r = g * (b + L->lam_m[x] * (u - b) + L->lam_p[x] * (dn - b) + L->l1 * (a + c - b - b));
+            } else {
+                double l0 = 1 - 4 * L->l1;
+                r = g * (l0 * b + L->l1 * (a + c) + L->l1 * (u + dn));
+            }
+        } else {
+            int jx = L->st[0], jy = L->st[1];
+            double acc = gin[z - jx] * g;
+            acc += gin[z + jx] * g;
+            acc += gin[z - jy] * g;
+            acc += gin[z + jy] * g;
+            acc += gin[z - 1] * g;
+            acc += gin[z + 1] * g;
+            r = acc * (1.0 / 6.0);
+        }
+        gout[z] = r;
+    }
+    /* boundary: copy of the mapped site; surface layers keep their value */
+    for (int z = 0; z < M; z++) {
+        if (is_interior(L, z)) continue;
+        int m = mapped_site(L, z, NULL);
+        gout[z] = is_interior(L, m) ? gout[m] : gin[m];
+    }
+}
+
+/* second-order steps, Lat3D2ndO.cpp:65-152 (forward) and :597-678 (backward) */
+static const int OPP[6] = {5, 4, 3, 2, 1, 0};
+static void olat_prop2(const olat *L, const double *gin, const double *G, double S,
+                       double *gout, int backward) {
+    int M = L->M, jx = L->st[0], jy = L->st[1];
+    int e[6] = {jx, jy, 1, -1, -jy, -jx};
+    double Lw = (1.0 - S) / 4.0;
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(L, z)) continue;
+        double gS = G[z] * S, gL = G[z] * Lw;
+        for (int k = 0; k < 6; k++) {
+            double acc = 0; int first = 1;
+            if (!backward) {
+                int src = z - e[k];
+                for (int kp = 0; kp < 6; kp++) {
+                    if (kp == OPP[k]) continue;
+                    double t = gin[kp * M + src] * (kp == k ? gS : gL);
+                    if (first) { acc = t; first = 0; } else acc += t;
+                }
+            } else {
+                for (int kp = 5; kp >= 0; kp--) {
+                    if (kp == OPP[k]) continue;
+                    double t = gin[kp * M + z + e[kp]] * (kp == k ? gS : gL);
+                    if (first) { acc = t; first = 0; } else acc += t;
+                }
+            }
+            gout[k * M + z] = acc;
+        }
+    }
+    olat_set_boundaries6(L, gout);
+}
+
+/* lnGN of an end-point distribution: Lat1DFlat1stO.cpp:301-316,
+   Lat2DFlat1stO.cpp:293-342, Lat2DCyl1stO.cpp:388-438, Lat3D1stO.cpp:344-370,
+   Lat3D2ndO.cpp:995-1025 (sum of the six components over 6) */
+static double olat_lngn(const olat *L, const double *G) {
+    double v = 0;
+    int K = (L->order == 2) ? 6 : 1;
+    for (int k = 0; k < K; k++)
+        for (int z = 0; z < L->M; z++) v += L->w_gn[z] * G[k * L->M + z];
+    if (K == 6) v /= 6.0;
+    return log(v);
+}
+
+/* contact average <phi>: Lat1DFlat.cpp:511-524, Lat2DFlat.cpp:996-1109,
+   Lat2DCylinder.cpp:205-320 (surface rows drop the missing neighbour),
+   Lat3D.cpp:1729-1785 (Sides, boundary values removed) */
+static void olat_side(const olat *L, const double *phi_in, double *rho) {
+    int M = L->M;
+    double *p = malloc(sizeof(double) * M);
+    memcpy(p, phi_in, sizeof(double) * M);
+    olat_set_boundaries(L, p);   /* SF_SegmentList.cpp:524-525 */
+    double l = L->l1chi;
+    for (int z = 0; z < M; z++) {
+        int c[3]; coords(L, z, c);
+        if (L->grad == 3) {
+            if (!is_interior(L, z)) { rho[z] = 0; continue; }
+            int jx = L->st[0], jy = L->st[1];
+            double l1 = 1.0 / 6.0, acc = 0 * p[z];
+            acc += l1 * p[z + jx]; acc += l1 * p[z - jx];
+            acc += l1 * p[z + jy]; acc += l1 * p[z - jy];
+            acc += l1 * p[z + 1]; acc += l1 * p[z - 1];
+            rho[z] = acc;
+            continue;
+        }
+        if (L->grad == 1) {
+            int zz = z;
+            if (z == 0) {
+                if (L->bc_lo[0] == SFGPU_BOUND_SURFACE) { rho[z] = p[0] + l * (-p[0] - p[0] + p[1]); continue; }
+                zz = L->map_lo[0];
+            } else if (z == M - 1) {
+                if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) { rho[z] = p[z] + l * (-p[z] - p[z] + p[z - 1]); continue; }
+                zz = L->map_hi[0];
+            }
+            rho[z] = p[zz] + l * (p[zz - 1] - p[zz] - p[zz] + p[zz + 1]);
+            continue;
+        }
+        /* 2 gradients */
+        int MX = L->Md[0], MY = L->Md[1];
+        int onsurf = 0;
+        if ((c[0] == 0 && L->bc_lo[0] == SFGPU_BOUND_SURFACE) || (c[0] == MX - 1 && L->bc_hi[0] == SFGPU_BOUND_SURFACE) ||
+            (c[1] == 0 && L->bc_lo[1] == SFGPU_BOUND_SURFACE) || (c[1] == MY - 1 && L->bc_hi[1] == SFGPU_BOUND_SURFACE))
+            onsurf = 1;
+        int x = c[0], zz = z;
+        if (!onsurf) zz = mapped_site(L, z, NULL), x = zz / MY;
+        double lm = L->cyl ? L->lam_m[x] : l, lp = L->cyl ? L->lam_p[x] : l;
+        double l0 = 1 - 2 * l - lm - lp;
+        if (!onsurf) {
+            if (L->cyl)
+                rho[z] = p[zz] + lp * (p[zz + MY] - p[zz]) + lm * (p[zz - MY] - p[zz]) + l * (p[zz - 1] + p[zz + 1] - p[zz] - p[zz]);
+            else
+                rho[z] = l0 * p[zz] + l * (p[zz - MY] + p[zz + MY]) + l * (p[zz - 1] + p[zz + 1]);
+        } else {
+            double acc = l0 * p[z];
+            if (c[0] > 0) acc += lm * p[z - MY];
+            if (c[0] < MX - 1) acc += lp * p[z + MY];
+            if (c[1] > 0) acc += l * p[z - 1];
+            if (c[1] < MY - 1) acc += l * p[z + 1];
+            rho[z] = acc;
+        }
+    }
+    free(p);
+}
+
+/* ------------------------------------------------------------------------ */
+/* system                                                                    */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int N, type;          /* type: 0 monomer, 1 homopolymer, 2 copolymer */
+    int *seg;             /* segment of each chain position, N entries */
+    int freedom;
+    double phibulk, theta;
+    int nseg_used;        /* number of distinct segments */
+    int *used;            /* list of distinct segments */
+    int *count;           /* per segment (n_segments): occurrences */
+    int pinned;
+    double lngn, lnc, chemintref;
+    double *phi;          /* n_segments * M (only used ones nonzero) */
+} omol;
+
+struct orc_system {
+    olat L;
+    int nseg;
+    int *freedom;
+    double *range;        /* nseg*M (zeros for free) */
+    double *chi, *pf;
+    int nmol, solvent;
+    omol *mol;
+    /* iteration variables, SF_Solve.cpp:37-163 */
+    int nliq, nclass;
+    int *stateQ;          /* liquid states in SFbox's reordered order */
+    int *class_of;        /* per segment, -1 for frozen */
+    int *rep_of_class;    /* last state of each class (SF_Solve.cpp:563-564) */
+    int nsites; int *sites;
+    int nvar;
+    /* work */
+    double *swf_full;     /* nseg*M, state level G = exp(-x) */
+    double *swf;          /* nseg*M, segment level (pinned mask) */
+    double *phi;          /* nseg*M, state phi */
+    double *rho;          /* nseg*M */
+    double *phib;         /* nseg */
+    int evaluated;
+};
+
+static int chi_rows_equal(const orc_system *s, int a, int b) {
+    for (int i = 0; i < s->nseg; i++)
+        if (s->chi[i * s->nseg + a] != s->chi[i * s->nseg + b]) return 0;
+    return 1;
+}
+
+int orc_create(const sfgpu_system_desc *d, orc_system **out) {
+    *out = NULL;
+    orc_system *s = calloc(1, sizeof(orc_system));
+    int rc = olat_init(&s->L, &d->lattice);
+    if (rc) { free(s); return rc; }
+    int M = s->L.M, ns = d->n_segments;
+    s->nseg = ns;
+    s->freedom = calloc(ns, sizeof(int));
+    s->range = calloc((size_t)ns * M, sizeof(double));
+    s->chi = calloc((size_t)ns * ns, sizeof(double));
+    s->pf = calloc((size_t)ns * ns, sizeof(double));
+    for (int i = 0; i < ns; i++) {
+        s->freedom[i] = d->segments[i].freedom;
+        if (s->freedom[i] != SFGPU_SEG_FREE && d->segments[i].range)
+            memcpy(s->range + (size_t)i * M, d->segments[i].range, sizeof(double) * M);
+        for (int j = 0; j < ns; j++) {
+            s->chi[i * ns + j] = d->chi ? d->chi[i * ns + j] : 0.0;
+            s->pf[i * ns + j] = d->pf ? d->pf[i * ns + j] : 0.2;
+        }
+    }
+    /* molecules */
+    s->nmol = d->n_molecules;
+    s->mol = calloc(s->nmol, sizeof(omol));
+    s->solvent = -1;
+    for (int m = 0; m < s->nmol; m++) {
+        const sfgpu_molecule_desc *md = &d->molecules[m];
+        omol *o = &s->mol[m];
+        int N = 0;
+        for (int b = 0; b < md->n_blocks; b++) N += md->block_length[b];
+        if (N < 1) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+        o->N = N; o->seg = calloc(N, sizeof(int)); o->count = calloc(ns, sizeof(int));
+        int p = 0;
+        for (int b = 0; b < md->n_blocks; b++)
+            for (int q = 0; q < md->block_length[b]; q++) o->seg[p++] = md->block_segment[b];
+        for (int q = 0; q < N; q++) {
+            if (o->seg[q] < 0 || o->seg[q] >= ns || s->freedom[o->seg[q]] == SFGPU_SEG_FROZEN) {
+                orc_destroy(s); return SFGPU_ERR_INVALID;
+            }
+            o->count[o->seg[q]]++;
+        }
+        o->used = calloc(ns, sizeof(int));
+        for (int i = 0; i < ns; i++) if (o->count[i]) {
+            o->used[o->nseg_used++] = i;
+            if (s->freedom[i] == SFGPU_SEG_PINNED) o->pinned = 1;
+        }
+        o->type = (N == 1) ? 0 : (o->nseg_used == 1 ? 1 : 2);
+        o->freedom = md->freedom; o->phibulk = md->phibulk; o->theta = md->theta;
+        if (o->freedom == SFGPU_MOL_SOLVENT) {
+            if (s->solvent >= 0) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+            s->solvent = m;
+        }
+        /* chemIntRef, SF_MolStructure.cpp:411-423 */
+        double cr = 0;
+        for (int a = 0; a < o->nseg_used; a++) {
+            int i = o->used[a];
+            double inner = 0;
+            for (int bb = 0; bb < o->nseg_used; bb++) {
+                int j = o->used[bb];
+                inner += s->chi[i * ns + j] * ((double)o->count[j] / N);
+            }
+            cr += ((double)o->count[i] / N) * inner;
+        }
+        o->chemintref = cr / 2;
+        o->phi = calloc((size_t)ns * M, sizeof(double));
+    }
+    if (s->solvent < 0) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+
+    /* liquid states and their classes, SF_Solve.cpp:37-86 */
+    s->stateQ = calloc(ns, sizeof(int));
+    s->class_of = calloc(ns, sizeof(int));
+    s->rep_of_class = calloc(ns, sizeof(int));
+    for (int i = 0; i < ns; i++) if (s->freedom[i] != SFGPU_SEG_FROZEN) s->stateQ[s->nliq++] = i;
+    for (int i = 0; i < s->nliq; i++) {
+        int s1 = s->stateQ[i];
+        for (int j = i + 1; j < s->nliq; j++) {
+            if (chi_rows_equal(s, s1, s->stateQ[j])) {
+                if (j != i + 1) { int t = s->stateQ[i + 1]; s->stateQ[i + 1] = s->stateQ[j]; s->stateQ[j] = t; }
+                i++;
+            }
+        }
+    }
+    for (int i = 0; i < ns; i++) s->class_of[i] = -1;
+    s->nclass = 0;
+    for (int i = 0; i < s->nliq; i++) {
+        int s1 = s->stateQ[i];
+        int c = s->nclass++;
+        s->class_of[s1] = c; s->rep_of_class[c] = s1;
+        for (int j = i + 1; j < s->nliq; j++) {
+            if (chi_rows_equal(s, s1, s->stateQ[j])) {
+                i++; s->class_of[s->stateQ[i]] = c; s->rep_of_class[c] = s->stateQ[i];
+            }
+        }
+    }
+    /* itvar sites, SF_Solve.cpp:129-150 */
+    s->sites = calloc(M, sizeof(int));
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(&s->L, z)) continue;
+        int ok = 1;
+        for (int i = 0; i < ns; i++)
+            if (s->freedom[i] == SFGPU_SEG_FROZEN && s->range[(size_t)i * M + z] > 0.999) ok = 0;
+        if (ok) s->sites[s->nsites++] = z;
+    }
+    s->nvar = s->nsites * s->nclass;
+    s->swf_full = calloc((size_t)ns * M, sizeof(double));
+    s->swf = calloc((size_t)ns * M, sizeof(double));
+    s->phi = calloc((size_t)ns * M, sizeof(double));
+    s->rho = calloc((size_t)ns * M, sizeof(double));
+    s->phib = calloc(ns, sizeof(double));
+    *out = s;
+    return SFGPU_OK;
+}
+
+void orc_destroy(orc_system *s) {
+    if (!s) return;
+    olat_free(&s->L);
+    for (int m = 0; m < s->nmol; m++) {
+        free(s->mol[m].seg); free(s->mol[m].count); free(s->mol[m].used); free(s->mol[m].phi);
+    }
+    free(s->mol); free(s->freedom); free(s->range); free(s->chi); free(s->pf);
+    free(s->stateQ); free(s->class_of); free(s->rep_of_class); free(s->sites);
+    free(s->swf_full); free(s->swf); free(s->phi); free(s->rho); free(s->phib);
+    free(s);
+}
+
+int orc_num_sites(const orc_system *s) { return s->L.M; }
+int orc_num_itvar(const orc_system *s) { return s->nvar; }
+int orc_num_classes(const orc_system *s) { return s->nclass; }
+int orc_itvar_sites(const orc_system *s, int *sites) { memcpy(sites, s->sites, sizeof(int) * s->nsites); return s->nsites; }
+int orc_class_of_segment(const orc_system *s, int seg) { return s->class_of[seg]; }
+
+/* SF_Solve::UpdateSWF (SF_Solve.cpp:794-852) + SF_State/SF_MolState::UpdateSWF
+   (SF_State.cpp:281-287, SF_MolState.cpp:147-151) */
+static void update_swf(orc_system *s, const double *x) {
+    int M = s->L.M, nc = s->nclass;
+    for (int i = 0; i < s->nseg; i++) {
+        double *gf = s->swf_full + (size_t)i * M;
+        memset(gf, 0, sizeof(double) * M);
+        int c = s->class_of[i];
+        if (c < 0) continue;
+        for (int j = 0; j < s->nsites; j++) gf[s->sites[j]] = exp(-x[j * nc + c]);
+        olat_set_boundaries(&s->L, gf);
+        double *g = s->swf + (size_t)i * M;
+        if (s->freedom[i] == SFGPU_SEG_PINNED) {
+            const double *r = s->range + (size_t)i * M;
+            for (int z = 0; z < M; z++) g[z] = (r[z] > 0) ? gf[z] : 0.0;
+            olat_set_boundaries(&s->L, g);   /* SF_Homopol1stO.cpp:105-106, SF_Copol1stO.cpp:123-127 */
+        } else {
+            memcpy(g, gf, sizeof(double) * M);
+        }
+    }
+}
+
+static void propagate_any(const orc_system *s, const double *gin, const double *G, double S, double *gout, int backward) {
+    if (s->L.order == 2) olat_prop2(&s->L, gin, G, S, gout, backward);
+    else olat_prop1(&s->L, gin, G, gout);
+}
+
+/* one molecule: SF_Monomer1stO::Matrix1 (SF_Monomer1stO.cpp:99-130),
+   SF_Homopol1stO::Matrix1 (SF_Homopol1stO.cpp:553-622),
+   SF_Copol1stO::Matrix1 (SF_Copol1stO.cpp:1187-1281),
+   SF_Homopol2ndO::Matrix1 (SF_Homopol2ndO.cpp:153-207),
+   SF_Copol2ndO::Matrix1 (SF_Copol2ndO.cpp:250-356) */
+static void molecule_phi(orc_system *s, omol *o) {
+    olat *L = &s->L;
+    int M = L->M, N = o->N, K = (L->order == 2) ? 6 : 1;
+    size_t KM = (size_t)K * M;
+    for (int a = 0; a < o->nseg_used; a++) memset(o->phi + (size_t)o->used[a] * M, 0, sizeof(double) * M);
+    if (o->type == 0) {
+        int i = o->seg[0];
+        const double *G = s->swf + (size_t)i * M;
+        double *phi = o->phi + (size_t)i * M;
+        memcpy(phi, G, sizeof(double) * M);
+        double *Gk = malloc(sizeof(double) * KM);
+        for (int k = 0; k < K; k++) memcpy(Gk + (size_t)k * M, G, sizeof(double) * M);
+        o->lngn = olat_lngn(L, Gk);
+        free(Gk);
+        if (o->freedom == SFGPU_MOL_RESTRICTED) {
+            o->lnc = log(o->theta) - o->lngn;
+            double norm = o->theta / exp(o->lngn);
+            for (int z = 0; z < M; z++) phi[z] *= norm;
+            o->phibulk = o->theta / exp(o->lngn);
+        } else {
+            o->lnc = log(o->phibulk);
+            for (int z = 0; z < M; z++) phi[z] *= o->phibulk;
+        }
+        return;
+    }
+    if (o->type == 1 && K == 1) {
+        /* symmetric half chain */
+        int i = o->seg[0];
+        const double *G = s->swf + (size_t)i * M;
+        double *phi = o->phi + (size_t)i * M;
+        int half = N / 2;
+        double *Gi = malloc(sizeof(double) * M * (size_t)half);
+        double *Ginv = malloc(sizeof(double) * M), *tmp = malloc(sizeof(double) * M);
+        memcpy(Gi, G, sizeof(double) * M);
+        for (int t = 1; t < half; t++) olat_prop1(L, Gi + (size_t)(t - 1) * M, G, Gi + (size_t)t * M);
+        memcpy(Ginv, Gi + (size_t)(half - 1) * M, sizeof(double) * M);
+        if (N % 2 == 1) {
+            olat_prop1(L, Ginv, G, tmp); memcpy(Ginv, tmp, sizeof(double) * M);
+            for (int z = 0; z < M; z++) phi[z] += Ginv[z] * Ginv[z];
+            for (int z = 0; z < M; z++) phi[z] *= 0.5;
+        }
+        for (int sp = (N + 3) / 2; sp <= N; sp++) {
+            int sinv = N - sp + 1;
+            olat_prop1(L, Ginv, G, tmp); memcpy(Ginv, tmp, sizeof(double) * M);
+            const double *Gb = Gi + (size_t)(sinv - 1) * M;
+            for (int z = 0; z < M; z++) phi[z] += Ginv[z] * Gb[z];
+        }
+        for (int z = 0; z < M; z++) { if (G[z] > 0) phi[z] /= G[z]; else phi[z] = 0; }
+        o->lngn = olat_lngn(L, Ginv);
+        if (o->freedom == SFGPU_MOL_RESTRICTED) {
+            o->lnc = log(o->theta) - o->lngn - log(1.0 * N);
+            double norm = (2 * o->theta / N) / exp(olat_lngn(L, Ginv));
+            for (int z = 0; z < M; z++) phi[z] *= norm;
+            o->phibulk = o->theta / exp(o->lngn);
+        } else {
+            double norm = 2 * o->phibulk / N;
+            for (int z = 0; z < M; z++) phi[z] *= norm;
+            o->lnc = log(o->phibulk / N);
+        }
+        free(Gi); free(Ginv); free(tmp);
+        return;
+    }
+    /* copolymer (1st order) and every 2nd-order chain: full storage */
+    double *Gi = malloc(sizeof(double) * KM * (size_t)N);
+    double *Ginv = malloc(sizeof(double) * KM), *tmp = malloc(sizeof(double) * KM);
+    const double *G1 = s->swf + (size_t)o->seg[0] * M;
+    for (int k = 0; k < K; k++) memcpy(Gi + (size_t)k * M, G1, sizeof(double) * M);
+    if (K == 6) olat_set_boundaries6(L, Gi);
+    for (int t = 1; t < N; t++) {
+        int sg = o->seg[t];
+        double S = s->pf[o->seg[t - 1] * s->nseg + sg];
+        propagate_any(s, Gi + (size_t)(t - 1) * KM, s->swf + (size_t)sg * M, S, Gi + (size_t)t * KM, 0);
+    }
+    const double *GN = s->swf + (size_t)o->seg[N - 1] * M;
+    for (int k = 0; k < K; k++) memcpy(Ginv + (size_t)k * M, GN, sizeof(double) * M);
+    if (K == 6) olat_set_boundaries6(L, Ginv);
+    {
+        double *phi = o->phi + (size_t)o->seg[N - 1] * M;
+        const double *Gf = Gi + (size_t)(N - 1) * KM;
+        for (int k = 0; k < K; k++)
+            for (int z = 0; z < M; z++) phi[z] += Ginv[(size_t)k * M + z] * Gf[(size_t)k * M + z];
+    }
+    for (int t = N - 2; t >= 0; t--) {
+        int sg = o->seg[t];
+        double S = s->pf[sg * s->nseg + o->seg[t + 1]];
+        propagate_any(s, Ginv, s->swf + (size_t)sg * M, S, tmp, 1);
+        memcpy(Ginv, tmp, sizeof(double) * KM);
+        double *phi = o->phi + (size_t)sg * M;
+        const double *Gf = Gi + (size_t)t * KM;
+        for (int k = 0; k < K; k++)
+            for (int z = 0; z < M; z++) phi[z] += Ginv[(size_t)k * M + z] * Gf[(size_t)k * M + z];
+    }
+    o->lngn = olat_lngn(L, Ginv);
+    for (int a = 0; a < o->nseg_used; a++) {
+        int i = o->used[a];
+        double *phi = o->phi + (size_t)i * M;
+        const double *G = s->swf + (size_t)i * M;
+        for (int z = 0; z < M; z++) { if (G[z] > 0) phi[z] /= G[z]; else phi[z] = 0; }
+    }
+    double norm;
+    if (o->freedom == SFGPU_MOL_RESTRICTED) {
+        o->lnc = log(o->theta) - o->lngn - log(1.0 * N);
+        o->phibulk = o->theta / exp(o->lngn);
+        norm = (o->theta / N) / (K == 6 ? 6.0 * exp(o->lngn) : exp(o->lngn));
+    } else {
+        o->lnc = log(o->phibulk / N);
+        norm = o->phibulk / (K == 6 ? 6.0 * N : (double)N);
+    }
+    for (int a = 0; a < o->nseg_used; a++) {
+        double *phi = o->phi + (size_t)o->used[a] * M;
+        for (int z = 0; z < M; z++) phi[z] *= norm;
+    }
+    free(Gi); free(Ginv); free(tmp);
+}
+
+/* SF_MolList1stO::ComputePhi (SF_MolList1stO.cpp:246-295) */
+static void compute_phi(orc_system *s) {
+    int M = s->L.M;
+    double phib_solv = 1.0;
+    for (int m = 0; m < s->nmol; m++) {
+        if (m == s->solvent) continue;
+        omol *o = &s->mol[m];
+        molecule_phi(s, o);
+        if (o->pinned) o->phibulk = 0;   /* SF_Homopol1stO.cpp:124-125 */
+        phib_solv -= o->phibulk;
+    }
+    s->mol[s->solvent].phibulk = phib_solv;
+    molecule_phi(s, &s->mol[s->solvent]);
+    /* state phi and bulk values */
+    for (int i = 0; i < s->nseg; i++) {
+        double *p = s->phi + (size_t)i * M;
+        s->phib[i] = 0;
+        if (s->freedom[i] == SFGPU_SEG_FROZEN) {
+            memcpy(p, s->range + (size_t)i * M, sizeof(double) * M);
+            olat_set_boundaries(&s->L, p);   /* SF_Segment.cpp:428-433 */
+            continue;
+        }
+        memset(p, 0, sizeof(double) * M);
+        for (int m = 0; m < s->nmol; m++) {
+            omol *o = &s->mol[m];
+            if (!o->count[i]) continue;
+            const double *q = o->phi + (size_t)i * M;
+            for (int z = 0; z < M; z++) p[z] += q[z];
+            s->phib[i] += o->phibulk * ((double)o->count[i] / o->N);
+        }
+    }
+}
+
+/* SF_Solve::GetResiduals (SF_Solve.cpp:527-591) with PutSides/ChemInt/
+   ChemIntBulk/GetPhiTotal (SF_SegmentList.cpp:512-744) */
+static void get_residuals(orc_system *s, double *f) {
+    int M = s->L.M, ns = s->nseg, nc = s->nclass;
+    for (int i = 0; i < ns; i++) olat_side(&s->L, s->phi + (size_t)i * M, s->rho + (size_t)i * M);
+    double *upr = malloc(sizeof(double) * nc);
+    for (int j = 0; j < s->nsites; j++) {
+        int z = s->sites[j];
+        double phit = 0;
+        for (int i = 0; i < ns; i++) phit += s->phi[(size_t)i * M + z];
+        double av = 0;
+        for (int c = 0; c < nc; c++) {
+            int st = s->rep_of_class[c];
+            double u = -log(s->swf_full[(size_t)st * M + z]);
+            double ci = 0, cb = 0;
+            for (int i = 0; i < ns; i++) {
+                double x = s->chi[st * ns + i];
+                if (x != 0) { ci += x * s->rho[(size_t)i * M + z]; cb += x * s->phib[i]; }
+            }
+            u -= ci / phit;
+            u += cb;
+            upr[c] = u; av += u;
+        }
+        av /= nc;
+        for (int c = 0; c < nc; c++) f[j * nc + c] = -1.0 + 1.0 / phit + upr[c] - av;
+    }
+    free(upr);
+}
+
+int orc_residual(orc_system *s, const double *x, double *f) {
+    update_swf(s, x);
+    compute_phi(s);
+    get_residuals(s, f);
+    s->evaluated = 1;
+    return SFGPU_OK;
+}
+
+int orc_get_phi(const orc_system *s, int seg, double *phi) {
+    if (seg < 0 || seg >= s->nseg) return SFGPU_ERR_INVALID;
+    memcpy(phi, s->phi + (size_t)seg * s->L.M, sizeof(double) * s->L.M);
+    return SFGPU_OK;
+}
+int orc_get_mol_phi(const orc_system *s, int mol, int seg, double *phi) {
+    if (mol < 0 || mol >= s->nmol || seg < 0 || seg >= s->nseg) return SFGPU_ERR_INVALID;
+    memcpy(phi, s->mol[mol].phi + (size_t)seg * s->L.M, sizeof(double) * s->L.M);
+    return SFGPU_OK;
+}
+double orc_get_lngn(const orc_system *s, int mol) { return s->mol[mol].lngn; }
+double orc_get_phibulk(const orc_system *s, int mol) { return s->mol[mol].phibulk; }
+int orc_get_swf(const orc_system *s, int seg, double *g) {
+    memcpy(g, s->swf + (size_t)seg * s->L.M, sizeof(double) * s->L.M);
+    return SFGPU_OK;
+}
+
+/* SF_MolList1stO::GetFreeEnergy (SF_MolList1stO.cpp:606-635) with
+   GetEntropyProfile (:827-911) and GetContactInteractionsProfile (:914-940) */
+double orc_free_energy(orc_system *s) {
+    if (!s->evaluated) return NAN;
+    int M = s->L.M, ns = s->nseg;
+    double F = 0;
+    for (int z = 0; z < M; z++) {
+        double w = s->L.w_f[z];
+        if (w == 0) continue;
+        double entropy = 0, contact = 0;
+        for (int m = 0; m < s->nmol; m++) {
+            omol *o = &s->mol[m];
+            double phim = 0;
+            for (int a = 0; a < o->nseg_used; a++) phim += o->phi[(size_t)o->used[a] * M + z];
+            entropy -= (phim / o->N) * (log((double)o->N) + o->lnc);
+            contact -= phim * o->chemintref;
+        }
+        for (int m = 0; m < s->nmol; m++) {
+            omol *o = &s->mol[m];
+            for (int a = 0; a < o->nseg_used; a++) {
+                int i = o->used[a];
+                double G = s->swf[(size_t)i * M + z];
+                if (G > 0) entropy -= o->phi[(size_t)i * M + z] * log(G);
+            }
+        }
+        for (int i = 0; i < ns; i++) {
+            double ci = 0;
+            for (int j = 0; j < ns; j++) {
+                double x = s->chi[i * ns + j];
+                if (x != 0) ci += x * s->rho[(size_t)j * M + z];
+            }
+            contact += 0.5 * s->phi[(size_t)i * M + z] * ci;
+        }
+        F += w * (-entropy + contact);
+    }
+    return F;
+}
+
+int orc_propagate(const orc_system *s, const double *gin, const double *g, double *gout, double S, int backward) {
+    int M = s->L.M, K = (s->L.order == 2) ? 6 : 1;
+    double *tmp = malloc(sizeof(double) * K * M);
+    memcpy(tmp, gin, sizeof(double) * K * M);
+    if (K == 6) olat_set_boundaries6(&s->L, tmp); else olat_set_boundaries(&s->L, tmp);
+    propagate_any(s, tmp, g, S, gout, backward);
+    free(tmp);
+    return SFGPU_OK;
+}
+int orc_side(const orc_system *s, const double *phi, double *rho) { olat_side(&s->L, phi, rho); return SFGPU_OK; }
+int orc_site_weights(const orc_system *s, double *w) { memcpy(w, s->L.w_gn, sizeof(double) * s->L.M); return SFGPU_OK; }
+int orc_set_boundaries(const orc_system *s, double *p) { olat_set_boundaries(&s->L, p); return SFGPU_OK; }
+
+/* ------------------------------------------------------------------------ */
+/* Pure_DIIS                                                                 */
+/* ------------------------------------------------------------------------ */
+/* cyclic Jacobi eigen-decomposition of a small symmetric matrix (Golub and
+   Van Loan, Matrix Computations, 4th ed., sec. 8.5): A = Q diag(ev) Q^T */
+static void jacobi_eig(int n, double *A, double *Q, double *ev) {
+    for (int i = 0; i < n; i++) for (int j = 0; j < n; j++) Q[i * n + j] = (i == j);
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0, tot = 0;
+        for (int i = 0; i < n; i++) for (int j = 0; j < n; j++) {
+            tot += A[i * n + j] * A[i * n + j];
+            if (i != j) off += A[i * n + j] * A[i * n + j];
+        }
+        if (off <= 1e-30 * tot || off == 0) break;
+        for (int p = 0; p < n; p++) for (int q = p + 1; q < n; q++) {
+            double apq = A[p * n + q];
+            if (apq == 0) continue;
+            double theta = (A[q * n + q] - A[p * n + p]) / (2 * apq);
+            double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+            double c = 1 / sqrt(t * t + 1), sn = t * c;
+            for (int k = 0; k < n; k++) {
+                double akp = A[k * n + p], akq = A[k * n + q];
+                A[k * n + p] = c * akp - sn * akq; A[k * n + q] = sn * akp + c * akq;
+            }
+            for (int k = 0; k < n; k++) {
+                double apk = A[p * n + k], aqk = A[q * n + k];
+                A[p * n + k] = c * apk - sn * aqk; A[q * n + k] = sn * apk + c * aqk;
+            }
+            for (int k = 0; k < n; k++) {
+                double qkp = Q[k * n + p], qkq = Q[k * n + q];
+                Q[k * n + p] = c * qkp - sn * qkq; Q[k * n + q] = sn * qkp + c * qkq;
+            }
+        }
+    }
+    for (int i = 0; i < n; i++) ev[i] = A[i * n + i];
+}
+
+/* coefficients c = A^-1 * 1 of the DIIS Gram matrix (SFNewton::Ax,
+   sfnewton.cpp:531-557, which forms V S^-1 U^T 1 from an SVD) */
+static void diis_coeff(int n, const double *A, double *c) {
+    double *B = malloc(sizeof(double) * n * n), *Q = malloc(sizeof(double) * n * n), *ev = malloc(sizeof(double) * n);
+    memcpy(B, A, sizeof(double) * n * n);
+    jacobi_eig(n, B, Q, ev);
+    for (int i = 0; i < n; i++) c[i] = 0;
+    for (int k = 0; k < n; k++) {
+        double proj = 0;
+        for (int i = 0; i < n; i++) proj += Q[i * n + k];
+        double t = proj / ev[k];
+        for (int i = 0; i < n; i++) c[i] += Q[i * n + k] * t;
+    }
+    free(B); free(Q); free(ev);
+}
+
+static double dot(const double *a, const double *b, int n) {
+    double r = 0; for (int i = 0; i < n; i++) r += a[i] * b[i]; return r;
+}
+
+/* SFNewton::PlainLBFGSDIIS, sfnewton.cpp:566-664 */
+int orc_solve_diis(orc_system *s, double *x, double tol, int maxit, int m, double eta,
+                   int *iterations, double *final_error) {
+    int iv = s->nvar;
+    double *g = malloc(sizeof(double) * iv), *x0 = malloc(sizeof(double) * iv);
+    double *XR = malloc(sizeof(double) * iv * (size_t)m), *XX0 = malloc(sizeof(double) * iv * (size_t)m);
+    double *Aij = calloc((size_t)m * m, sizeof(double)), *Ap = calloc((size_t)m * m, sizeof(double));
+    double *C = calloc(m, sizeof(double));
+    int k = 0, it = 0, kd = 1, rc = SFGPU_OK;
+    orc_residual(s, x, g);
+    memcpy(x0, x, sizeof(double) * iv);
+    for (int i = 0; i < iv; i++) x[i] = -eta * g[i];
+    for (int i = 0; i < iv; i++) XX0[i] = x[i] - x0[i];
+    memcpy(XR, x, sizeof(double) * iv);
+    double err = sqrt(dot(g, g, iv));
+    while (tol < err && it < maxit) {
+        it++;
+        memcpy(x0, x, sizeof(double) * iv);
+        orc_residual(s, x, g);
+        for (int i = 0; i < iv; i++) x[i] -= g[i] * eta;
+        k = it % m; kd++;
+        memcpy(XR + (size_t)k * iv, x, sizeof(double) * iv);
+        for (int i = 0; i < iv; i++) XX0[(size_t)k * iv + i] = x[i] - x0[i];
+        if (kd > m) {
+            kd = m;
+            for (int i = 1; i < m; i++) for (int j = 1; j < m; j++) Aij[m * (i - 1) + j - 1] = Aij[m * i + j];
+        }
+        for (int i = 0; i < kd; i++) {
+            int posi = k - kd + 1 + i; if (posi < 0) posi += m;
+            Aij[i + m * (kd - 1)] = Aij[kd - 1 + m * i] = dot(XX0 + (size_t)posi * iv, XX0 + (size_t)k * iv, iv);
+        }
+        for (int i = 0; i < kd; i++) for (int j = 0; j < kd; j++) Ap[j + kd * i] = Aij[j + m * i];
+        diis_coeff(kd, Ap, C);
+        double nc = 0;
+        for (int i = 0; i < kd; i++) nc += C[i];
+        for (int i = 0; i < kd; i++) C[i] /= nc;
+        int posi = k - kd + 1; if (posi < 0) posi += m;
+        for (int i = 0; i < iv; i++) x[i] = C[0] * XR[(size_t)posi * iv + i];
+        for (int q = 1; q < kd; q++) {
+            posi = k - kd + 1 + q; if (posi < 0) posi += m;
+            for (int i = 0; i < iv; i++) x[i] += C[q] * XR[(size_t)posi * iv + i];
+        }
+        err = sqrt(dot(g, g, iv));
+        if (!isfinite(err)) { rc = SFGPU_ERR_NONFINITE; break; }
+    }
+    if (rc == SFGPU_OK && err > tol) rc = SFGPU_ERR_NOTCONVERGED;
+    if (iterations) *iterations = it;
+    if (final_error) *final_error = err;
+    free(g); free(x0); free(XR); free(XX0); free(Aij); free(Ap); free(C);
+    return rc;
+}

@@ -1,0 +1,142 @@
+"""CUDA path vs the CPU oracle on identical seeded inputs, through the C ABI.
+
+Tolerances (FP64 throughout): single propagator steps and contact averages
+agree to 1e-14 relative (the library is built without FMA contraction and
+keeps SFbox's operation order); whole residual evaluations to 1e-11
+relative (reductions and exp/log differ in the last bits); converged
+profiles to 1e-10 in phi and 1e-9 in the free energy.
+"""
+import numpy as np
+import pytest
+import torch
+
+from cases import CASES, random_x
+from field_b200.system import System
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-14
+TOL_EVAL = 1e-11
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_propagator_step(gpu_lib, case):
+    spec = CASES[case]()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    rng = np.random.default_rng(3)
+    K = sys_.K
+    gin = o.set_boundaries(rng.uniform(0.2, 2.0, o.M)) if K == 1 else rng.uniform(0.2, 2.0, K * o.M)
+    g = o.set_boundaries(rng.uniform(0.1, 1.5, o.M))
+    for backward in ([0] if K == 1 else [0, 1]):
+        want = o.propagate(gin, g, S=0.35, backward=backward)
+        gin_t = torch.tensor(gin, device="cuda")
+        if K == 6:
+            sys_.set_boundaries(gin_t)
+        got = sys_.propagate(gin_t, torch.tensor(g, device="cuda"), S=0.35, backward=bool(backward)).cpu().numpy()
+        assert rel(got, want) <= TOL_STEP, (case, backward, rel(got, want))
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_side_fraction(gpu_lib, case):
+    spec = CASES[case]()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    rng = np.random.default_rng(4)
+    phi = o.set_boundaries(rng.uniform(0.0, 1.0, o.M))
+    want = o.side(phi)
+    got = sys_.side_fraction(torch.tensor(phi, device="cuda")).cpu().numpy()
+    assert rel(got, want) <= TOL_STEP
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_residual_and_profiles(gpu_lib, case):
+    spec = CASES[case]()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    assert sys_.nvar == o.nvar and sys_.M == o.M
+    x = random_x(spec)
+    f_gpu = sys_.residual(x)
+    f_cpu = o.residual(x)
+    assert np.all(np.isfinite(f_gpu))
+    assert rel(f_gpu, f_cpu) <= TOL_EVAL, rel(f_gpu, f_cpu)
+    for i, seg in enumerate(spec.segments):
+        assert rel(sys_.phi(i), o.phi(i)) <= TOL_EVAL, (seg.name, rel(sys_.phi(i), o.phi(i)))
+    for m in range(len(spec.molecules)):
+        sc = sys_.mol_scalars(m)
+        assert abs(sc["lngn"] - o.lngn(m)) <= 1e-12 * max(1.0, abs(o.lngn(m)))
+        assert abs(sc["phibulk"] - o.phibulk(m)) <= 1e-12 * max(1e-300, abs(o.phibulk(m))) + 1e-300
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_free_energy(gpu_lib, case):
+    spec = CASES[case]()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    x = random_x(spec, seed=11, scale=0.2)
+    sys_.residual(x)
+    o.residual(x)
+    Fg, Fc = sys_.free_energy(), o.free_energy()
+    assert abs(Fg - Fc) <= 1e-11 * max(1.0, abs(Fc)), (Fg, Fc)
+
+
+def test_edge_single_layer_and_short_chains(gpu_lib):
+    """Smallest lattices and chains: one interior layer, N = 1, 2, 3."""
+    from field_b200 import configs
+    for n, N in [(1, 2), (2, 3), (3, 1), (5, 2)]:
+        spec, _ = configs.flat_adsorption(n=n, N=N)
+        sys_ = System(spec)
+        o = Oracle(spec)
+        x = random_x(spec, seed=n * 10 + N)
+        assert rel(sys_.residual(x), o.residual(x)) <= TOL_EVAL
+
+
+def test_solve_c1_converged_parity(gpu_lib):
+    """Config C1 converged by the device Pure_DIIS and by the oracle's: same
+    algorithm, so the profiles agree to 1e-10 and the free energy to 1e-9."""
+    from field_b200 import configs
+    spec, x0 = configs.flat_adsorption()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    rg = sys_.solve(x0, tol=1e-10, maxit=5000, m=10, eta=0.5)
+    xc, rc, it, err = o.solve_diis(x0, tol=1e-10, maxit=5000, m=10, eta=0.5)
+    assert rg.converged and rc == 0
+    sys_.residual(rg.x)
+    o.residual(xc)
+    for i in range(3):
+        np.testing.assert_allclose(sys_.phi(i), o.phi(i), rtol=1e-10, atol=1e-12)
+    assert abs(sys_.free_energy() - o.free_energy()) <= 1e-9
+    # the converged residual of the GPU iterate is below tolerance on the oracle too
+    assert np.linalg.norm(o.residual(rg.x)) < 1e-9
+
+
+def test_full_size_c2_residual(gpu_lib):
+    """Config C2 (Lat2DCyl1stO 128x128, A20B20, seeded micelle) at full size."""
+    from field_b200 import configs
+    spec, x0 = configs.cyl_micelle()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    f_gpu, f_cpu = sys_.residual(x0), o.residual(x0)
+    assert rel(f_gpu, f_cpu) <= TOL_EVAL
+    assert abs(sys_.free_energy() - o.free_energy()) <= 1e-10 * max(1.0, abs(o.free_energy()))
+
+
+def test_full_size_c3_residual(gpu_lib):
+    """Config C3 (Lat3D1stO 128^3 periodic, A50B50 melt) at full size: one
+    residual against the oracle plus the sum rule sum_z phi = phibulk * GN."""
+    from field_b200 import configs
+    spec, x0 = configs.melt3d()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    f_gpu, f_cpu = sys_.residual(x0), o.residual(x0)
+    assert rel(f_gpu, f_cpu) <= TOL_EVAL
+    sites = spec.itvar_sites()
+    tot = (sys_.phi(0) + sys_.phi(1))[sites].sum()
+    gn = np.exp(sys_.mol_scalars(0)["lngn"])
+    assert abs(tot - gn) < 1e-10 * gn

@@ -1,0 +1,82 @@
+"""SFbox input-file reader and system builder (host logic, no GPU)."""
+import numpy as np
+import pytest
+
+from field_b200 import configs
+from field_b200.desc import BOUND_MIRROR1, BOUND_SURFACE, MOL_FREE, MOL_SOLVENT, SEG_FROZEN
+from field_b200.sfinput import build_system, parse_composition, parse_input
+
+
+def test_parse_c1_input():
+    text = configs.C1_INPUT.format(n=100, N=100, phib=0.01, chi_aw=0.5, chi_as=-1.0)
+    calcs = parse_input(text)
+    assert len(calcs) == 1
+    spec, st = build_system(calcs[0])
+    assert spec.lattice.M == 102
+    assert spec.lattice.bound_lo[0] == BOUND_SURFACE and spec.lattice.bound_hi[0] == BOUND_MIRROR1
+    assert [s.name for s in spec.segments] == ["S", "A", "W"]
+    assert spec.segments[0].freedom == SEG_FROZEN and spec.segments[0].range[0] == 1.0
+    assert spec.segments[0].range[1:].sum() == 0
+    assert spec.chi[1, 2] == 0.5 and spec.chi[2, 1] == 0.5 and spec.chi[0, 1] == -1.0
+    assert spec.molecules[0].N == 100 and spec.molecules[0].freedom == MOL_FREE
+    assert spec.molecules[1].freedom == MOL_SOLVENT
+    assert spec.n_itvar() == 200
+    assert st.tolerance == 1e-7 and st.method == "Pure_DIIS"
+
+
+def test_start_blocks_inherit_and_override():
+    text = """lat : l : gradients : 1
+lat : l : n_layers : 10
+lat : l : lambda : 0.2
+mon : A : freedom : free
+mon : W : freedom : free
+mol : p : composition : (A)5
+mol : p : freedom : free
+mol : p : phibulk : 0.1
+mol : w : composition : (W)1
+mol : w : freedom : solvent
+start
+mol : p : phibulk : 0.2   // second calculation changes one value
+start
+"""
+    calcs = parse_input(text)
+    assert len(calcs) == 2
+    s1, _ = build_system(calcs[0])
+    s2, _ = build_system(calcs[1])
+    assert s1.molecules[0].phibulk == 0.1 and s2.molecules[0].phibulk == 0.2
+    assert s2.lattice.n_layers[0] == 10
+
+
+def test_malformed_lines_rejected():
+    with pytest.raises(ValueError):
+        parse_input("lat : a : gradients\n")
+    with pytest.raises(ValueError):
+        parse_input("lat : a : b : c : d\n")
+
+
+def test_composition():
+    assert parse_composition("(A)20(B)20") == [("A", 20), ("B", 20)]
+    assert parse_composition("(X)1(A)199") == [("X", 1), ("A", 199)]
+    with pytest.raises(ValueError):
+        parse_composition("A20")
+
+
+def test_class_layout_groups_equal_chemistry():
+    spec, _ = configs.cyl_micelle(nx=8, ny=8)
+    cls, nc = spec.class_layout()
+    assert nc == 3 and sorted(cls) == [0, 1, 2]
+    # B and W equal when chi_BW equals chi_AW... here B has chi 0 with all, W does not
+    spec2, _ = configs.melt3d(n=4, nA=2, nB=2, chi_ab=0.0)
+    cls2, nc2 = spec2.class_layout()
+    assert nc2 == 1 and cls2 == [0, 0]
+
+
+def test_synthetic_configs_shapes():
+    spec, x = configs.cyl_micelle()
+    assert spec.lattice.shape == (130, 130) and x.size == spec.n_itvar() == 128 * 128 * 3
+    spec, x = configs.melt3d(n=16)
+    assert x.size == 16 ** 3 * 2 and np.all(np.abs(x) <= 0.05)
+    inst = configs.sweep1d(count=8)
+    assert len(inst) == 8 and all(50 <= s.lattice.n_layers[0] <= 400 for s, _ in inst)
+    spec, x = configs.brush3d(n=12, N=20, sigma=0.05)
+    assert spec.segments[0].range.sum() == round(0.05 * 144)
