@@ -165,12 +165,44 @@ def run_reference(a, rank, world):
 
 
 # ---------------------------------------------------------------------------
+def plain_form(insts, stream, steps=1):
+    """Per-instance host-driven Pure_DIIS with one launch per propagator step
+    (the plain GPU form); returns solves/s."""
+    import torch
+    from field_b200.system import System
+    systems = [System(s) for s, _ in insts]
+    for s in systems:
+        s.use_stream(stream.cuda_stream)
+    x_host = [torch.from_numpy(x0).pin_memory() for _, x0 in insts]
+
+    def run():
+        conv, iters = 0, 0
+        for s, xh in zip(systems, x_host):
+            r = s.solve(xh.numpy(), tol=TOL, maxit=MAXIT, m=DIIS_M, eta=DIIS_ETA)
+            conv += r.converged
+            iters += r.iterations
+        return conv, iters
+    run()
+    torch.cuda.synchronize()
+    t = 0.0
+    conv = iters = 0
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        c, it = run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1) / 1000.0
+        conv += c
+        iters += it
+    return conv / t, systems[0], iters
+
+
 def run_ours(a, rank, world, local_rank):
     import numpy as np
     import torch
     import torch.distributed as dist
     from field_b200 import batch as fbatch
-    from field_b200.system import System
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -179,56 +211,49 @@ def run_ours(a, rank, world, local_rank):
     insts = instances(rank, B)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > 126 MB L2
 
-    if a.form == "plain":
-        systems = [System(s) for s, _ in insts]
-        for s in systems:
-            s.use_stream(stream.cuda_stream)
-        x_host = [torch.from_numpy(x0).pin_memory() for _, x0 in insts]
-
-        def step():
-            conv, iters = 0, 0
-            for s, xh in zip(systems, x_host):
-                r = s.solve(xh.numpy(), tol=TOL, maxit=MAXIT, m=DIIS_M, eta=DIIS_ETA)
-                conv += r.converged
-                iters += r.iterations
-            return conv, iters
-        launches_per_iter = None
-        prof_sys = systems[0]
-    else:
-        solver = fbatch.BatchSolver([s for s, _ in insts], method="diis", m=DIIS_M, eta=DIIS_ETA)
-        solver.use_stream(stream.cuda_stream)
-        x_host = torch.from_numpy(np.concatenate([x for _, x in insts])).pin_memory()
-
-        def step():
-            res = solver.solve(x_host.numpy(), tol=TOL, maxit=MAXIT)
-            return int(res.converged.sum()), int(res.iterations.sum())
-        prof_sys = System(insts[0][0])
-        prof_sys.use_stream(stream.cuda_stream)
-
     def barrier():
         if world > 1:
             dist.barrier()
 
-    for _ in range(a.warmup):
-        step()
+    solver = None
+    if a.form == "chosen":
+        solver = fbatch.BatchSolver([s for s, _ in insts], method="diis", m=DIIS_M, eta=DIIS_ETA)
+        solver.use_stream(stream.cuda_stream)
+        x_all = np.concatenate([x for _, x in insts])
+        x_pinned = torch.from_numpy(x_all).pin_memory()
+        y_pinned = torch.empty_like(x_pinned).pin_memory()
+        for _ in range(a.warmup):
+            solver.load(x_all)
+            solver.solve_resident(TOL, MAXIT)
+            solver.results()
     torch.cuda.synchronize()
+
     sampler = ClockSampler(local_rank) if rank == 0 else None
-    times, conv_total, iters_total = [], 0, 0
+    times, conv_total, iters_total, kms = [], 0, 0, []
     barrier()
     torch.cuda.synchronize()
     if sampler:
         sampler.start()
-    for _ in range(a.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        c, it = step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1) / 1000.0)
-        conv_total += c
-        iters_total += it
+    if a.form == "chosen":
+        for _ in range(a.steps):
+            flush.zero_()
+            solver.load(x_all)                 # inputs resident in HBM before the timed region
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.solve_resident(TOL, MAXIT)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1000.0)
+            res = solver.results()
+            conv_total += int(res.converged.sum())
+            iters_total += int(res.iterations.sum())
+            kms.append(solver.kernel_ms())
+        last_iters = res.iterations
+    else:
+        v, prof_sys, iters_total = plain_form(insts, stream, steps=a.steps)
+        conv_total = len(insts) * a.steps
+        times = [conv_total / v]
     barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop() if sampler else None
@@ -240,17 +265,44 @@ def run_ours(a, rank, world, local_rank):
     t_max = local.item()
     value = solved.item() / t_max
 
-    # e2e through the public API: pinned host inputs copied in, converged
-    # iteration variables copied out, every step
+    # e2e through the public API: pinned host guesses in, iterates out, every step
     h2d = sum(x.size for _, x in insts) * 8
-    d2h = h2d
-    e2e = {"value": value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "note": "the solve call takes host arrays: the copies are inside every timed step"}
+    if a.form == "chosen":
+        et, econv = 0.0, 0
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = solver.solve(x_pinned.numpy(), tol=TOL, maxit=MAXIT, out=y_pinned.numpy())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            et += e0.elapsed_time(e1) / 1000.0
+            econv += int(r.converged.sum())
+        el = torch.tensor([et], device=dev, dtype=torch.float64)
+        ec = torch.tensor([float(econv)], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(el, op=dist.ReduceOp.MAX)
+            dist.all_reduce(ec, op=dist.ReduceOp.SUM)
+        e2e_value = ec.item() / el.item()
+    else:
+        e2e_value = value
+    e2e = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
+           "note": "sfgpu_batch_solve / sfgpu_solve_diis on pinned host arrays; copies inside every timed step"}
 
-    # roofline of the dominant kernel (propagator step), timed live
+    # plain GPU form on a few instances of the same workload, same run
+    plain = None
+    if a.form == "chosen":
+        pv, prof_sys, _ = plain_form(instances(rank, 2), stream, steps=1)
+        plain = {"value": pv, "unit": "solves/s", "instances": 2,
+                 "form": "per-instance host-driven Pure_DIIS, one launch per propagator step"}
+        kp_bytes = solver.algorithmic_bytes(last_iters)
+        solver.kernel_profile = {"kernel": "batch_diis_kernel (persistent, one launch per batch solve)",
+                                 "bytes": kp_bytes, "ms": statistics.median(kms), "traffic": None}
     prof = prof_sys.profile_propagator(reps=400)
-    from field_b200 import batch as fb
-    roof = fb.roofline(prof, a.form, solver if a.form == "chosen" else None)
+    roof = fbatch.roofline(prof, a.form, solver)
+    if a.form == "chosen":
+        roof["per_step_kernel"] = fbatch.roofline(prof, "plain", None)
 
     if rank == 0:
         cpu = cpu_baseline(a.cpu_sample)
@@ -258,12 +310,13 @@ def run_ours(a, rank, world, local_rank):
                 "warmup": a.warmup, "ms_per_step": 1000 * t_max / a.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "form": a.form, "instances_per_rank_per_step": B,
-                           "method": "Pure_DIIS" if a.form == "plain" else "batched DIIS",
+                           "method": "Pure_DIIS, m=%d, eta=%g" % (DIIS_M, DIIS_ETA),
                            "tolerance": TOL, "converged": int(solved.item()),
                            "mean_iterations": iters_total / max(1, conv_total),
-                           "l2": "256 MB buffer written between timed steps", "parallelism": f"instances x{world}"},
-                "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-                "gpu_launches": fb.launch_count(a.form, iters_total, insts, solver if a.form == "chosen" else None)}
+                           "l2": "256 MB buffer written between timed steps",
+                           "parallelism": f"instances x{world}"},
+                "e2e": e2e, "roofline": roof, "plain_gpu_form": plain, "cpu_baseline": cpu, "clocks": clocks,
+                "gpu_launches": fbatch.launch_count(a.form, iters_total, insts, solver)}
         print(json.dumps(line), flush=True)
 
 

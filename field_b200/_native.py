@@ -37,6 +37,16 @@ PROTOTYPES = {
     "sfgpu_lat_lngn": (i32, [vp, vp, i32, dp]),
     "sfgpu_solve_diis": (i32, [vp, dp, f64, i32, i32, f64, ip, dp]),
     "sfgpu_profile_propagator": (i32, [vp, i32, dp, dp, dp, dp]),
+    "sfgpu_batch_create": (i32, [i32, vp, i32, C.POINTER(vp)]),
+    "sfgpu_batch_destroy": (i32, [vp]),
+    "sfgpu_batch_info": (i32, [vp, ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "sfgpu_batch_set_stream": (i32, [vp, vp]),
+    "sfgpu_batch_solve": (i32, [vp, dp, dp, f64, i32, f64, ip, ip, dp]),
+    "sfgpu_batch_get_phi": (i32, [vp, i32, i32, dp]),
+    "sfgpu_batch_load": (i32, [vp, dp]),
+    "sfgpu_batch_solve_resident": (i32, [vp, f64, i32, f64]),
+    "sfgpu_batch_results": (i32, [vp, dp, ip, ip, dp]),
+    "sfgpu_batch_kernel_ms": (i32, [vp, dp]),
 }
 
 _lib = None

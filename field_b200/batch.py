@@ -2,8 +2,15 @@
 by bench.py (roofline figures and launch counts)."""
 from __future__ import annotations
 
+import ctypes as C
 import json
 import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as nat
+from .desc import SystemDesc
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -67,3 +74,139 @@ def roofline(prof: dict, form: str, solver=None) -> dict:
             "bytes_per_launch": prof["bytes_bwd"], "ms_per_launch": prof["ms_bwd"],
             "forward_step": {"bytes": prof["bytes_fwd"], "ms": prof["ms_fwd"],
                              "achieved": prof["bytes_fwd"] / (prof["ms_fwd"] / 1e3) / 1e9}}
+
+
+@dataclass
+class BatchResult:
+    x: np.ndarray
+    status: np.ndarray
+    iterations: np.ndarray
+    errors: np.ndarray
+
+    @property
+    def converged(self) -> np.ndarray:
+        return self.status == 0
+
+
+def residual_bytes(spec) -> float:
+    """Algorithmic bytes of one residual evaluation's propagation: forward
+    step 8*(K+1+K) per site, backward step with composition 8*(3K+3) per site
+    (read Gb(s+1), G, Gf(s), phi; write Gb(s), phi), per molecule."""
+    K = 6 if spec.lattice.order == 2 else 1
+    M = spec.M
+    tot = 0.0
+    for mol in spec.molecules:
+        N = mol.N
+        used = len({b[0] for b in mol.blocks})
+        if N == 1:
+            continue
+        if used == 1 and K == 1:
+            nf, nb = N // 2 - 1, N - N // 2
+        else:
+            nf, nb = N - 1, N - 1
+        tot += nf * 8.0 * (2 * K + 1) * M + nb * 8.0 * (3 * K + 3) * M
+    return tot
+
+
+class BatchSolver:
+    """Many independent instances solved by Pure_DIIS in one persistent
+    kernel launch (sfgpu_batch_solve)."""
+
+    def __init__(self, specs, method: str = "diis", m: int = 10, eta: float = 0.1):
+        if method != "diis":
+            raise ValueError("the batched path implements Pure_DIIS")
+        self.lib = nat.load()
+        self.specs = list(specs)
+        self.m, self.eta = m, eta
+        descs = (SystemDesc * len(self.specs))()
+        for i, sp in enumerate(self.specs):
+            descs[i] = sp.to_c()
+        self._descs = descs
+        h = C.c_void_p()
+        nat.check(self.lib.sfgpu_batch_create(len(self.specs), descs, m, C.byref(h)), "sfgpu_batch_create")
+        self.h = h
+        n, tot = C.c_int(), C.c_longlong()
+        offs = (C.c_longlong * len(self.specs))()
+        nat.check(self.lib.sfgpu_batch_info(h, C.byref(n), C.byref(tot), offs), "sfgpu_batch_info")
+        self.n, self.total = n.value, tot.value
+        self.offsets = np.array(list(offs), dtype=np.int64)
+        self.launches_in_last_solve_total = 0
+        self.kernel_profile = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sfgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def use_stream(self, stream_handle: int):
+        nat.check(self.lib.sfgpu_batch_set_stream(self.h, C.c_void_p(stream_handle)), "sfgpu_batch_set_stream")
+
+    def split(self, x):
+        ends = list(self.offsets[1:]) + [self.total]
+        return [x[a:b] for a, b in zip(self.offsets, ends)]
+
+    def solve(self, x0, tol=1e-7, maxit=2000, out=None) -> BatchResult:
+        """Host API: guesses in, iterates out (``out`` may be a caller-owned,
+        e.g. pinned, float64 array; by default a new array)."""
+        x = np.ascontiguousarray(x0, dtype=np.float64)
+        if x.size != self.total:
+            raise ValueError(f"x has {x.size} values, batch has {self.total}")
+        y = np.empty(self.total) if out is None else out
+        st = np.zeros(self.n, dtype=np.int32)
+        it = np.zeros(self.n, dtype=np.int32)
+        er = np.zeros(self.n)
+        dp = C.POINTER(C.c_double)
+        nat.check(self.lib.sfgpu_batch_solve(self.h, x.ctypes.data_as(dp), y.ctypes.data_as(dp), tol, maxit,
+                                             self.eta, st.ctypes.data_as(C.POINTER(C.c_int)),
+                                             it.ctypes.data_as(C.POINTER(C.c_int)), er.ctypes.data_as(dp)),
+                  "sfgpu_batch_solve")
+        self.launches_in_last_solve_total += 1
+        return BatchResult(y, st, it, er)
+
+    def load(self, x0):
+        x = np.ascontiguousarray(x0, dtype=np.float64)
+        if x.size != self.total:
+            raise ValueError(f"x has {x.size} values, batch has {self.total}")
+        nat.check(self.lib.sfgpu_batch_load(self.h, x.ctypes.data_as(C.POINTER(C.c_double))), "sfgpu_batch_load")
+
+    def solve_resident(self, tol=1e-7, maxit=2000):
+        """Launch the solve on the device-resident iterate (asynchronous)."""
+        nat.check(self.lib.sfgpu_batch_solve_resident(self.h, tol, maxit, self.eta), "sfgpu_batch_solve_resident")
+        self.launches_in_last_solve_total += 1
+
+    def results(self, want_x: bool = False) -> BatchResult:
+        st = np.zeros(self.n, dtype=np.int32)
+        it = np.zeros(self.n, dtype=np.int32)
+        er = np.zeros(self.n)
+        x = np.empty(self.total) if want_x else None
+        xp = x.ctypes.data_as(C.POINTER(C.c_double)) if want_x else C.POINTER(C.c_double)()
+        nat.check(self.lib.sfgpu_batch_results(self.h, xp, st.ctypes.data_as(C.POINTER(C.c_int)),
+                                               it.ctypes.data_as(C.POINTER(C.c_int)),
+                                               er.ctypes.data_as(C.POINTER(C.c_double))), "sfgpu_batch_results")
+        return BatchResult(x, st, it, er)
+
+    def kernel_ms(self) -> float:
+        v = C.c_double()
+        nat.check(self.lib.sfgpu_batch_kernel_ms(self.h, C.byref(v)), "sfgpu_batch_kernel_ms")
+        return v.value
+
+    def phi(self, inst: int, seg: int) -> np.ndarray:
+        out = np.empty(self.specs[inst].M)
+        nat.check(self.lib.sfgpu_batch_get_phi(self.h, inst, seg, out.ctypes.data_as(C.POINTER(C.c_double))),
+                  "sfgpu_batch_get_phi")
+        return out
+
+    def algorithmic_bytes(self, iterations) -> float:
+        """Propagator bytes plus DIIS vector traffic of one batch solve."""
+        tot = 0.0
+        for sp, it in zip(self.specs, iterations):
+            nv = sp.n_itvar()
+            tot += (int(it) + 1) * residual_bytes(sp)
+            tot += int(it) * 8.0 * nv * (self.m + 7)
+        return tot

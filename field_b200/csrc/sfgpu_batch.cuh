@@ -1,0 +1,348 @@
+// sfgpu_batch.cuh -- one SF-SCF instance evaluated and iterated by ONE
+// thread block.  The persistent batch kernel gives every block an instance
+// from a work queue and the block runs the whole Pure_DIIS iteration
+// (SFNewton::PlainLBFGSDIIS, sfnewton.cpp:566-664) on it: segment weighting
+// factors, chain propagation with fused composition, normalisation, residual,
+// Gram products and the DIIS combination, with __syncthreads between the
+// propagator steps and no host round trip.  Uneven instances of a parameter
+// sweep (Vary.cpp:127) therefore share the GPU without per-step launches.
+#pragma once
+#include "sfgpu_kernels.cuh"
+
+namespace sfb {
+
+constexpr int kMaxMol = SFGPU_MAX_SEG;
+constexpr int kMaxHist = 16;        // DIIS memory m supported by the batch path
+
+struct IMol {
+    int N, type, sym, freedom, pinned, solvent, nused;
+    int used[SFGPU_MAX_SEG];
+    const int *seg;                 // device: segment of each chain position
+    double *phi[SFGPU_MAX_SEG];     // per segment, nullptr when unused
+    double phibulk, theta;
+};
+
+struct InstDesc {
+    DLat L;
+    int M, nseg, nmol, nclass, nsites, solvent;
+    long long nvar;
+    int freedom[SFGPU_MAX_SEG];
+    int class_of[SFGPU_MAX_SEG];
+    int rep[SFGPU_MAX_SEG];
+    ChiTable ct;
+    double frac[SFGPU_MAX_SEG * SFGPU_MAX_SEG];     // [seg][mol] = count/N
+    const int *jmap, *sites;
+    const double *w_gn;
+    const double *range[SFGPU_MAX_SEG];
+    double *gfull[SFGPU_MAX_SEG], *gseg[SFGPU_MAX_SEG], *phi[SFGPU_MAX_SEG];
+    IMol mol[kMaxMol];
+    double *gi, *ginv0, *ginv1;
+    // iteration work
+    double *x, *x0, *g, *XR, *XX0;
+};
+
+struct BlockShared {
+    double red[32 * (kMaxHist + 2)];
+    double val[kMaxHist + 2];
+    sfk::MolScal scal[kMaxMol];
+    double phib[SFGPU_MAX_SEG], chib[SFGPU_MAX_SEG];
+    double gram[kMaxHist * kMaxHist];
+    double coef[kMaxHist];
+    int pos[kMaxHist];
+    int inst;
+};
+
+// Sum of nv per-thread values over the block in a fixed order
+// (warp shuffle tree, then warps in index order); result in sh.val[0..nv).
+__device__ inline void block_sums(const double *v, int nv, BlockShared &sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    for (int i = 0; i < nv; i++) {
+        double a = v[i];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) sh.red[i * 32 + warp] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        double a = 0;
+        for (int w = 0; w < nw; w++) a += sh.red[threadIdx.x * 32 + w];
+        sh.val[threadIdx.x] = a;
+    }
+    __syncthreads();
+}
+
+__device__ inline void mol_scalars_block(const InstDesc &I, int m, double wsum, BlockShared &sh) {
+    const IMol &o = I.mol[m];
+    sfk::MolScal s;
+    s.lngn = log(wsum);
+    double phib = o.phibulk;
+    if (o.solvent) {
+        phib = 1.0;
+        for (int q = 0; q < I.nmol; q++)
+            if (q != m) phib -= sh.scal[q].phibulk;
+    }
+    const double N = (double)o.N;
+    double gn = exp(s.lngn);
+    if (o.freedom == SFGPU_MOL_RESTRICTED) {
+        if (o.type == 0) { s.lnc = log(o.theta) - s.lngn; s.norm = o.theta / gn; }
+        else {
+            s.lnc = log(o.theta) - s.lngn - log(1.0 * o.N);
+            s.norm = (o.sym ? 2 * o.theta / N : o.theta / N) / gn;
+        }
+        s.phibulk = o.theta / gn;
+    } else {
+        s.phibulk = phib;
+        if (o.type == 0) { s.lnc = log(phib); s.norm = phib; }
+        else { s.lnc = log(phib / N); s.norm = o.sym ? 2 * phib / N : phib / N; }
+    }
+    if (o.pinned) s.phibulk = 0;
+    sh.scal[m] = s;
+}
+
+// lnGN sum, scalars and normalised phi of molecule m; cur = end-point
+// distribution (Gi_inv after the backward pass)
+__device__ inline void finish_molecule(const InstDesc &I, int m, const double *cur, BlockShared &sh) {
+    const IMol &o = I.mol[m];
+    double acc = 0;
+    for (int r = threadIdx.x; r < I.M; r += blockDim.x) {
+        double w = I.w_gn[r];
+        if (w != 0) acc += w * cur[r];
+    }
+    block_sums(&acc, 1, sh);
+    if (threadIdx.x == 0) mol_scalars_block(I, m, sh.val[0], sh);
+    __syncthreads();
+    const double norm = sh.scal[m].norm;
+    for (int a = 0; a < o.nused; a++) {
+        int i = o.used[a];
+        const double *G = I.gseg[i];
+        double *phi = o.phi[i];
+        for (int r = threadIdx.x; r < I.M; r += blockDim.x) {
+            double p;
+            if (o.type == 0) p = G[r];
+            else { double g = G[r]; p = (g > 0) ? phi[r] / g : 0.0; }
+            phi[r] = p * norm;
+        }
+    }
+}
+
+// SF_Homopol1stO::Matrix1 / SF_Copol1stO::Matrix1 / SF_Monomer1stO::Matrix1
+// inside one block (first-order lattices)
+__device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared &sh) {
+    const IMol &o = I.mol[m];
+    const DLat &L = I.L;
+    const int M = I.M;
+    if (o.type == 0) { finish_molecule(I, m, I.gseg[o.seg[0]], sh); return; }
+    for (int a = 0; a < o.nused; a++) {
+        double *phi = o.phi[o.used[a]];
+        for (int r = threadIdx.x; r < M; r += blockDim.x) phi[r] = 0.0;
+    }
+    double *gi = I.gi;
+    double *bufA = I.ginv0, *bufB = I.ginv1;
+    if (o.sym) {
+        const int sg = o.seg[0];
+        const double *G = I.gseg[sg];
+        double *phi = o.phi[sg];
+        const int N = o.N, half = N / 2;
+        for (int r = threadIdx.x; r < M; r += blockDim.x) gi[r] = G[r];
+        __syncthreads();
+        for (int t = 1; t < half; t++) {
+            const double *src = gi + (size_t)(t - 1) * M;
+            double *dst = gi + (size_t)t * M;
+            for (int r = threadIdx.x; r < M; r += blockDim.x) dst[r] = prop1_site(L, src, G, r);
+            __syncthreads();
+        }
+        const double *cur = gi + (size_t)(half - 1) * M;
+        if (N % 2 == 1) {
+            for (int r = threadIdx.x; r < M; r += blockDim.x) {
+                double out = prop1_site(L, cur, G, r);
+                bufA[r] = out;
+                phi[r] = (phi[r] + out * out) * 0.5;
+            }
+            __syncthreads();
+            cur = bufA; double *t = bufA; bufA = bufB; bufB = t;
+        }
+        for (int sp = (N + 3) / 2; sp <= N; sp++) {
+            const double *other = gi + (size_t)(N - sp) * M;
+            for (int r = threadIdx.x; r < M; r += blockDim.x) {
+                double out = prop1_site(L, cur, G, r);
+                bufA[r] = out;
+                phi[r] += out * other[r];
+            }
+            __syncthreads();
+            cur = bufA; double *t = bufA; bufA = bufB; bufB = t;
+        }
+        finish_molecule(I, m, cur, sh);
+        return;
+    }
+    const int N = o.N;
+    {
+        const double *G1 = I.gseg[o.seg[0]];
+        for (int r = threadIdx.x; r < M; r += blockDim.x) gi[r] = G1[r];
+        __syncthreads();
+    }
+    for (int t = 1; t < N; t++) {
+        const double *src = gi + (size_t)(t - 1) * M;
+        double *dst = gi + (size_t)t * M;
+        const double *G = I.gseg[o.seg[t]];
+        for (int r = threadIdx.x; r < M; r += blockDim.x) dst[r] = prop1_site(L, src, G, r);
+        __syncthreads();
+    }
+    {
+        const int sN = o.seg[N - 1];
+        const double *GN = I.gseg[sN];
+        const double *gf = gi + (size_t)(N - 1) * M;
+        double *phi = o.phi[sN];
+        for (int r = threadIdx.x; r < M; r += blockDim.x) {
+            double g = GN[r];
+            bufA[r] = g;
+            phi[r] += g * gf[r];
+        }
+        __syncthreads();
+    }
+    const double *cur = bufA;
+    { double *t = bufA; bufA = bufB; bufB = t; }
+    for (int t = N - 2; t >= 0; t--) {
+        const int sg = o.seg[t];
+        const double *G = I.gseg[sg];
+        const double *gf = gi + (size_t)t * M;
+        double *phi = o.phi[sg];
+        for (int r = threadIdx.x; r < M; r += blockDim.x) {
+            double out = prop1_site(L, cur, G, r);
+            bufA[r] = out;
+            phi[r] += out * gf[r];
+        }
+        __syncthreads();
+        cur = bufA; double *tt = bufA; bufA = bufB; bufB = tt;
+    }
+    finish_molecule(I, m, cur, sh);
+}
+
+// x -> f for one instance (SF_Solve::residuals, SF_Solve.cpp:647-651)
+__device__ inline void residual_block(const InstDesc &I, const double *x, double *f, BlockShared &sh) {
+    const DLat &L = I.L;
+    const int M = I.M;
+    for (int i = 0; i < I.nseg; i++) {
+        if (I.freedom[i] == SFGPU_SEG_FROZEN) continue;
+        const int cls = I.class_of[i];
+        const bool pinned = I.freedom[i] == SFGPU_SEG_PINNED;
+        double *gf = I.gfull[i], *gs = I.gseg[i];
+        const double *range = I.range[i];
+        for (int r = threadIdx.x; r < M; r += blockDim.x) {
+            int t = lat_map(L, r);
+            int j = I.jmap[t];
+            double v = (j >= 0) ? exp(-x[(size_t)j * I.nclass + cls]) : 0.0;
+            gf[r] = v;
+            gs[r] = pinned ? (range[t] > 0 ? v : 0.0) : v;
+        }
+    }
+    __syncthreads();
+    for (int m = 0; m < I.nmol; m++) {
+        if (m == I.solvent) continue;
+        molecule_phi_block(I, m, sh);
+        __syncthreads();
+    }
+    molecule_phi_block(I, I.solvent, sh);
+    __syncthreads();
+    for (int i = 0; i < I.nseg; i++) {
+        if (I.freedom[i] == SFGPU_SEG_FROZEN) continue;
+        double *p = I.phi[i];
+        for (int r = threadIdx.x; r < M; r += blockDim.x) {
+            double acc = 0;
+            for (int m = 0; m < I.nmol; m++) {
+                const double *q = I.mol[m].phi[i];
+                if (q) acc += q[r];
+            }
+            p[r] = acc;
+        }
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < I.nseg; i++) {
+            double v = 0;
+            for (int m = 0; m < I.nmol; m++) v += sh.scal[m].phibulk * I.frac[i * SFGPU_MAX_SEG + m];
+            sh.phib[i] = v;
+        }
+        for (int c = 0; c < I.nclass; c++) {
+            int st = I.rep[c];
+            double v = 0;
+            for (int j = 0; j < I.nseg; j++) {
+                double xx = I.ct.chi[st * SFGPU_MAX_SEG + j];
+                if (xx != 0) v += xx * sh.phib[j];
+            }
+            sh.chib[c] = v;
+        }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < I.nsites; j += blockDim.x) {
+        int z = I.sites[j];
+        double phit = 0;
+        double rho[SFGPU_MAX_SEG];
+        for (int i = 0; i < I.nseg; i++) { phit += I.phi[i][z]; rho[i] = 0; }
+        for (int i = 0; i < I.nseg; i++) {
+            bool need = false;
+            for (int c = 0; c < I.nclass; c++) need |= I.ct.chi[I.rep[c] * SFGPU_MAX_SEG + i] != 0;
+            if (need) rho[i] = side_fraction(L, I.phi[i], z);
+        }
+        double u[SFGPU_MAX_SEG];
+        double av = 0;
+        for (int c = 0; c < I.nclass; c++) {
+            int st = I.rep[c];
+            double v = -log(I.gfull[st][z]);
+            double ci = 0;
+            for (int i = 0; i < I.nseg; i++) {
+                double xx = I.ct.chi[st * SFGPU_MAX_SEG + i];
+                if (xx != 0) ci += xx * rho[i];
+            }
+            v -= ci / phit;
+            v += sh.chib[c];
+            u[c] = v;
+            av += v;
+        }
+        av /= I.nclass;
+        for (int c = 0; c < I.nclass; c++) f[(size_t)j * I.nclass + c] = -1.0 + 1.0 / phit + u[c] - av;
+    }
+    __syncthreads();
+}
+
+// DIIS coefficients c = A^-1 1 by cyclic Jacobi (one thread; k <= kMaxHist)
+__device__ inline void diis_coeff_thread(int n, double *A, double *c) {
+    double Q[kMaxHist * kMaxHist], ev[kMaxHist];
+    for (int i = 0; i < n; i++) for (int j = 0; j < n; j++) Q[i * n + j] = (i == j);
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0, tot = 0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                tot += A[i * n + j] * A[i * n + j];
+                if (i != j) off += A[i * n + j] * A[i * n + j];
+            }
+        if (off <= 1e-30 * tot || off == 0) break;
+        for (int p = 0; p < n; p++)
+            for (int q = p + 1; q < n; q++) {
+                double apq = A[p * n + q];
+                if (apq == 0) continue;
+                double theta = (A[q * n + q] - A[p * n + p]) / (2 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+                double cs = 1 / sqrt(t * t + 1), sn = t * cs;
+                for (int k = 0; k < n; k++) {
+                    double akp = A[k * n + p], akq = A[k * n + q];
+                    A[k * n + p] = cs * akp - sn * akq; A[k * n + q] = sn * akp + cs * akq;
+                }
+                for (int k = 0; k < n; k++) {
+                    double apk = A[p * n + k], aqk = A[q * n + k];
+                    A[p * n + k] = cs * apk - sn * aqk; A[q * n + k] = sn * apk + cs * aqk;
+                }
+                for (int k = 0; k < n; k++) {
+                    double qkp = Q[k * n + p], qkq = Q[k * n + q];
+                    Q[k * n + p] = cs * qkp - sn * qkq; Q[k * n + q] = sn * qkp + cs * qkq;
+                }
+            }
+    }
+    for (int i = 0; i < n; i++) ev[i] = A[i * n + i];
+    for (int i = 0; i < n; i++) c[i] = 0;
+    for (int k = 0; k < n; k++) {
+        double proj = 0;
+        for (int i = 0; i < n; i++) proj += Q[i * n + k];
+        double t = proj / ev[k];
+        for (int i = 0; i < n; i++) c[i] += Q[i * n + k] * t;
+    }
+}
+
+}  // namespace sfb

@@ -105,6 +105,20 @@ __device__ __forceinline__ double stencil1(const DLat &L, const double *__restri
     }
 }
 
+// Value of site r after one first-order step: interior sites by the stencil;
+// boundary sites copy their mapped site (UpdateBoundaries), and a site on a
+// surface layer (or a corner reached through one) keeps its value.
+__device__ __forceinline__ double prop1_site(const DLat &L, const double *__restrict__ gin,
+                                             const double *__restrict__ G, int r) {
+    int c[3];
+    lat_coords(L, r, c);
+    if (lat_interior(L, c)) return stencil1(L, gin, G[r], r);
+    int t = lat_map(L, r);
+    int ct[3];
+    lat_coords(L, t, ct);
+    return lat_interior(L, ct) ? stencil1(L, gin, G[t], t) : gin[t];
+}
+
 // Contact average <phi>(z) at any site (SideFraction, Lat1DFlat.cpp:511-524,
 // Lat2DFlat.cpp:996-1109, Lat2DCylinder.cpp:205-320; Sides with removed
 // boundaries in 3D, Lat3D.cpp:1729-1785).  p must carry boundary copies.

@@ -42,19 +42,7 @@ static __global__ void step1(DLat L, const double *__restrict__ gin, const doubl
                       double *__restrict__ gout, const double *__restrict__ other,
                       double *__restrict__ phi, int mode) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < L.M; r += gridDim.x * blockDim.x) {
-        int c[3];
-        lat_coords(L, r, c);
-        double out;
-        if (lat_interior(L, c)) {
-            out = stencil1(L, gin, G[r], r);
-        } else {
-            // boundary: the value of the mapped site; a site on a surface
-            // layer (also a corner reached through a surface) keeps its value
-            int t = lat_map(L, r);
-            int ct[3];
-            lat_coords(L, t, ct);
-            out = lat_interior(L, ct) ? stencil1(L, gin, G[t], t) : gin[t];
-        }
+        double out = prop1_site(L, gin, G, r);
         gout[r] = out;
         if (mode == COMP_ACC) phi[r] += out * other[r];
         else if (mode == COMP_CENTRE) phi[r] = (phi[r] + out * out) * 0.5;

@@ -200,6 +200,37 @@ int sfgpu_profile_propagator(sfgpu_system *sys, int reps, double *ms_fwd, double
 int sfgpu_solve_diis(sfgpu_system *sys, double *x, double tol, int maxit, int m, double eta,
                      int *iterations, double *final_error);
 
+/* ---- batched instances (parameter sweeps) --------------------------------- */
+/* Many independent first-order systems -- the calculations of a 'var :'
+ * sweep, which SFbox runs one after another (Vary::NextCalculation,
+ * Vary.cpp:127; SF_Box.cpp:145-177) -- solved together.  m is the DIIS
+ * memory (1..16). */
+typedef struct sfgpu_batch sfgpu_batch;
+int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, sfgpu_batch **out);
+int sfgpu_batch_destroy(sfgpu_batch *batch);
+/* number of instances, total iteration variables and the start of every
+ * instance in the concatenated x vector */
+int sfgpu_batch_info(sfgpu_batch *batch, int *n, long long *total_nvar, long long *offsets);
+int sfgpu_batch_set_stream(sfgpu_batch *batch, void *stream);
+/* Pure_DIIS (SFNewton::PlainLBFGSDIIS, sfnewton.cpp:566-664) on every
+ * instance in one persistent kernel launch: thread blocks take instances
+ * from a work queue and iterate them to |f| <= tol on the device.  x_in is
+ * the concatenated host vector of initial guesses, x_out (may be NULL, may
+ * equal x_in) receives the last iterates; status[i] is SFGPU_OK,
+ * SFGPU_ERR_NOTCONVERGED or SFGPU_ERR_NONFINITE. */
+int sfgpu_batch_solve(sfgpu_batch *batch, const double *x_in, double *x_out, double tol, int maxit,
+                      double eta, int *status, int *iterations, double *errors);
+/* the same in three parts: load guesses (host -> device), launch the solve
+ * on the device-resident iterate (asynchronous), read results back (x may
+ * be NULL to leave the iterates on the device) */
+int sfgpu_batch_load(sfgpu_batch *batch, const double *x);
+int sfgpu_batch_solve_resident(sfgpu_batch *batch, double tol, int maxit, double eta);
+int sfgpu_batch_results(sfgpu_batch *batch, double *x, int *status, int *iterations, double *errors);
+/* device time of the last solve launch (CUDA events around the kernel) */
+int sfgpu_batch_kernel_ms(sfgpu_batch *batch, double *ms);
+/* state profile of one instance after the solve (its last evaluation) */
+int sfgpu_batch_get_phi(sfgpu_batch *batch, int instance, int segment, double *phi);
+
 #ifdef __cplusplus
 }
 #endif
