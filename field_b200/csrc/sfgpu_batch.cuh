@@ -122,6 +122,20 @@ __device__ inline void finish_molecule(const InstDesc &I, int m, const double *c
             phi[r] = p * norm;
         }
     }
+    if (o.type == 0) return;
+    // boundary entries of phi: copies of the mapped sites (row-wise steps
+    // leave them untouched)
+    __syncthreads();
+    for (int a = 0; a < o.nused; a++) {
+        double *phi = o.phi[o.used[a]];
+        for (int r = threadIdx.x; r < I.M; r += blockDim.x) {
+            int c[3];
+            lat_coords(I.L, r, c);
+            if (lat_interior(I.L, c)) continue;
+            int t = lat_map(I.L, r);
+            if (t != r) phi[r] = phi[t];
+        }
+    }
 }
 
 // SF_Homopol1stO::Matrix1 / SF_Copol1stO::Matrix1 / SF_Monomer1stO::Matrix1
@@ -147,26 +161,32 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         for (int t = 1; t < half; t++) {
             const double *src = gi + (size_t)(t - 1) * M;
             double *dst = gi + (size_t)t * M;
-            for (int r = threadIdx.x; r < M; r += blockDim.x) dst[r] = prop1_site(L, src, G, r);
+            for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+                dst[R.base + k] = prop1_row(L, R, src, G, k, nlast);
+            });
             __syncthreads();
         }
         const double *cur = gi + (size_t)(half - 1) * M;
         if (N % 2 == 1) {
-            for (int r = threadIdx.x; r < M; r += blockDim.x) {
-                double out = prop1_site(L, cur, G, r);
-                bufA[r] = out;
-                phi[r] = (phi[r] + out * out) * 0.5;
-            }
+            double *dst = bufA;
+            for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+                const int z = R.base + k;
+                double out = prop1_row(L, R, cur, G, k, nlast);
+                dst[z] = out;
+                phi[z] = (phi[z] + out * out) * 0.5;
+            });
             __syncthreads();
             cur = bufA; double *t = bufA; bufA = bufB; bufB = t;
         }
         for (int sp = (N + 3) / 2; sp <= N; sp++) {
             const double *other = gi + (size_t)(N - sp) * M;
-            for (int r = threadIdx.x; r < M; r += blockDim.x) {
-                double out = prop1_site(L, cur, G, r);
-                bufA[r] = out;
-                phi[r] += out * other[r];
-            }
+            double *dst = bufA;
+            for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+                const int z = R.base + k;
+                double out = prop1_row(L, R, cur, G, k, nlast);
+                dst[z] = out;
+                phi[z] += out * other[z];
+            });
             __syncthreads();
             cur = bufA; double *t = bufA; bufA = bufB; bufB = t;
         }
@@ -183,7 +203,9 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         const double *src = gi + (size_t)(t - 1) * M;
         double *dst = gi + (size_t)t * M;
         const double *G = I.gseg[o.seg[t]];
-        for (int r = threadIdx.x; r < M; r += blockDim.x) dst[r] = prop1_site(L, src, G, r);
+        for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+            dst[R.base + k] = prop1_row(L, R, src, G, k, nlast);
+        });
         __syncthreads();
     }
     {
@@ -205,11 +227,13 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         const double *G = I.gseg[sg];
         const double *gf = gi + (size_t)t * M;
         double *phi = o.phi[sg];
-        for (int r = threadIdx.x; r < M; r += blockDim.x) {
-            double out = prop1_site(L, cur, G, r);
-            bufA[r] = out;
-            phi[r] += out * gf[r];
-        }
+        double *dst = bufA;
+        for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+            const int z = R.base + k;
+            double out = prop1_row(L, R, cur, G, k, nlast);
+            dst[z] = out;
+            phi[z] += out * gf[z];
+        });
         __syncthreads();
         cur = bufA; double *tt = bufA; bufA = bufB; bufB = tt;
     }

@@ -119,6 +119,103 @@ __device__ __forceinline__ double prop1_site(const DLat &L, const double *__rest
     return lat_interior(L, ct) ? stencil1(L, gin, G[t], t) : gin[t];
 }
 
+// ---------------------------------------------------------------------------
+// Row-wise first-order steps.  The interior of the lattice is walked as rows
+// along the fastest gradient; a row knows the (mapped) offsets of its
+// neighbour rows, and only the two ends of a row need the mapped left/right
+// neighbour, so no per-site division or branch remains.  Boundary entries
+// of the output are not written: every neighbour read goes to the site a
+// boundary entry would copy (SetBoundaries), and surface layers (which keep
+// their value, always 0 for a propagator) are read in place.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline int lat_mapc(const DLat &L, int d, int c) {
+    if (c == 0) return L.map_lo[d];
+    if (c == L.Md[d] - 1) return L.map_hi[d];
+    return c;
+}
+
+__host__ __device__ inline int lat_nrows(const DLat &L) {
+    if (L.grad == 1) return 1;
+    if (L.grad == 2) return L.Md[0] - 2;
+    return (L.Md[0] - 2) * (L.Md[1] - 2);
+}
+
+struct RowInfo {
+    int base;        // site index of the row's element 0 (boundary position)
+    int up, dn;      // offsets of the first-gradient neighbour rows (2D/3D)
+    int up2, dn2;    // offsets of the second-gradient neighbour rows (3D)
+    int x;           // first-gradient coordinate (cylinder tables)
+};
+
+__device__ __forceinline__ RowInfo lat_row(const DLat &L, int row) {
+    RowInfo R;
+    R.up = R.dn = R.up2 = R.dn2 = 0;
+    if (L.grad == 1) { R.base = 0; R.x = 0; return R; }
+    if (L.grad == 2) {
+        int x = row + 1;
+        R.x = x;
+        R.base = x * L.st[0];
+        R.up = (lat_mapc(L, 0, x - 1) - x) * L.st[0];
+        R.dn = (lat_mapc(L, 0, x + 1) - x) * L.st[0];
+        return R;
+    }
+    int ny = L.Md[1] - 2;
+    int x = row / ny + 1, y = row - (x - 1) * ny + 1;
+    R.x = x;
+    R.base = x * L.st[0] + y * L.st[1];
+    R.up = (lat_mapc(L, 0, x - 1) - x) * L.st[0];
+    R.dn = (lat_mapc(L, 0, x + 1) - x) * L.st[0];
+    R.up2 = (lat_mapc(L, 1, y - 1) - y) * L.st[1];
+    R.dn2 = (lat_mapc(L, 1, y + 1) - y) * L.st[1];
+    return R;
+}
+
+// new value at interior position k (1..n_last) of row R, same operation
+// order as stencil1
+__device__ __forceinline__ double prop1_row(const DLat &L, const RowInfo &R, const double *__restrict__ gin,
+                                            const double *__restrict__ G, int k, int nlast) {
+    const int d = L.grad - 1;
+    const int t = R.base + k;
+    const int km = (k == 1) ? L.map_lo[d] : k - 1;
+    const int kp = (k == nlast) ? L.map_hi[d] : k + 1;
+    const double g = G[t];
+    const double a = gin[R.base + km], b = gin[t], c = gin[R.base + kp];
+    if (L.grad == 1) return g * (b + L.l1 * (a - b - b + c));
+    if (L.grad == 2) {
+        const double u = gin[t + R.up], dd = gin[t + R.dn];
+        if (L.cyl) return g * (b + L.lam_m[R.x] * (u - b) + L.lam_p[R.x] * (dd - b) + L.l1 * (a + c - b - b));
+        double l0 = 1 - 4 * L.l1;
+        return g * (l0 * b + L.l1 * (a + c) + L.l1 * (u + dd));
+    }
+    double acc = gin[t + R.up] * g;
+    acc += gin[t + R.dn] * g;
+    acc += gin[t + R.up2] * g;
+    acc += gin[t + R.dn2] * g;
+    acc += a * g;
+    acc += c * g;
+    return acc * (1.0 / 6.0);
+}
+
+// Visit the interior sites assigned to this thread: for 1 gradient threads
+// stride over the single row; otherwise warps take rows and lanes take the
+// positions along the row.  worker = thread index among nworkers threads.
+template <class F>
+__device__ __forceinline__ void for_interior(const DLat &L, int worker, int nworkers, F &&f) {
+    const int d = L.grad - 1;
+    const int nlast = L.Md[d] - 2;
+    if (L.grad == 1) {
+        RowInfo R = lat_row(L, 0);
+        for (int k = worker + 1; k <= nlast; k += nworkers) f(R, k, nlast);
+        return;
+    }
+    const int lane = worker & 31, warp = worker >> 5, nw = nworkers >> 5;
+    const int nrows = lat_nrows(L);
+    for (int row = warp; row < nrows; row += nw) {
+        RowInfo R = lat_row(L, row);
+        for (int k = lane + 1; k <= nlast; k += 32) f(R, k, nlast);
+    }
+}
+
 // Contact average <phi>(z) at any site (SideFraction, Lat1DFlat.cpp:511-524,
 // Lat2DFlat.cpp:996-1109, Lat2DCylinder.cpp:205-320; Sides with removed
 // boundaries in 3D, Lat3D.cpp:1729-1785).  p must carry boundary copies.

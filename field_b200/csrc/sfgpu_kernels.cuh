@@ -49,6 +49,22 @@ static __global__ void step1(DLat L, const double *__restrict__ gin, const doubl
     }
 }
 
+// The same step over interior sites only (row-wise, see for_interior); the
+// path used inside residual evaluations.  Boundary entries of gout and phi
+// are left untouched.
+static __global__ void step1_rows(DLat L, const double *__restrict__ gin, const double *__restrict__ G,
+                                  double *__restrict__ gout, const double *__restrict__ other,
+                                  double *__restrict__ phi, int mode) {
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const double out = prop1_row(L, R, gin, G, k, nlast);
+        const int t = R.base + k;
+        gout[t] = out;
+        if (mode == COMP_ACC) phi[t] += out * other[t];
+        else if (mode == COMP_CENTRE) phi[t] = (phi[t] + out * out) * 0.5;
+    });
+}
+
 // One second-order step (Lat3D2ndO::PropagateF, Lat3D2ndO.cpp:65-152, and
 // PropagateB, :597-678) for the six direction components, with boundary
 // components swapped at mirrors (SetBx1(gz0,gz5)..., Lat3D2ndO.cpp:84-89) and

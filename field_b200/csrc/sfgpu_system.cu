@@ -30,6 +30,14 @@ static int grid_for(long n) {
     return (int)std::max(1L, std::min(b, 148L * 16));
 }
 
+// blocks for a row-wise kernel: one warp per interior row (1D: one thread
+// per interior site)
+static int grid_rows(const DLat &L) {
+    long threads = (L.grad == 1) ? (long)(L.Md[0] - 2) : 32L * lat_nrows(L);
+    long b = (threads + kBlock - 1) / kBlock;
+    return (int)std::max(1L, std::min(b, 148L * 32));
+}
+
 // ---------------------------------------------------------------------------
 // lattice set-up (Lat1DFlat.cpp:4-149, Lat2DFlat.cpp:35-220,
 // Lat2DCylinder.cpp:7-55, Lat3D.cpp:44-236)
@@ -334,6 +342,11 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     }
     if ((rc = alloc_d(&d_gi, store))) return rc;
     if ((rc = alloc_d(&d_ginv[0], (size_t)K * M)) || (rc = alloc_d(&d_ginv[1], (size_t)K * M))) return rc;
+    // row-wise steps never write boundary entries; surface layers are read
+    // in place and must hold the propagator's value there, 0
+    SFGPU_CUDA_TRY(cudaMemset(d_gi, 0, sizeof(double) * std::max<size_t>(store, 1)));
+    SFGPU_CUDA_TRY(cudaMemset(d_ginv[0], 0, sizeof(double) * K * M));
+    SFGPU_CUDA_TRY(cudaMemset(d_ginv[1], 0, sizeof(double) * K * M));
     nblocks_red = grid_for(M);
     if ((rc = alloc_d(&d_partial, (size_t)std::max(nblocks_red, 64) * 64))) return rc;
     if ((rc = alloc_d((double **)&d_scal, 4 * (size_t)nmol))) return rc;
@@ -356,6 +369,7 @@ int sfgpu_system::molecule_phi(int m) {
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_for(M);
+    const int gr = grid_rows(L);
     cudaStream_t s = stream;
     MolParam p;
     p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = o.sym; p.K = K;
@@ -381,20 +395,21 @@ int sfgpu_system::molecule_phi(int m) {
         double *phi = o.d_phi[i];
         SFGPU_CUDA_TRY(cudaMemcpyAsync(d_gi, G, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
         for (int t = 1; t < half; t++)
-            step1<<<g, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * M, G, d_gi + (size_t)t * M, nullptr, nullptr, COMP_NONE);
+            step1_rows<<<gr, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * M, G, d_gi + (size_t)t * M, nullptr, nullptr, COMP_NONE);
         const double *cur = d_gi + (size_t)(half - 1) * M;
         if (N % 2 == 1) {
-            step1<<<g, kBlock, 0, s>>>(L, cur, G, ginv, nullptr, phi, COMP_CENTRE);
+            step1_rows<<<gr, kBlock, 0, s>>>(L, cur, G, ginv, nullptr, phi, COMP_CENTRE);
             cur = ginv; std::swap(ginv, tmp);
         }
         for (int sp = (N + 3) / 2; sp <= N; sp++) {
             int sinv = N - sp + 1;
-            step1<<<g, kBlock, 0, s>>>(L, cur, G, ginv, d_gi + (size_t)(sinv - 1) * M, phi, COMP_ACC);
+            step1_rows<<<gr, kBlock, 0, s>>>(L, cur, G, ginv, d_gi + (size_t)(sinv - 1) * M, phi, COMP_ACC);
             cur = ginv; std::swap(ginv, tmp);
         }
         wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, cur, d_wgn, d_partial);
         mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, scal, m);
         finalize_phi<<<g, kBlock, 0, s>>>(M, G, phi, scal, m, 0);
+        set_boundaries<<<g, kBlock, 0, s>>>(L, 1, phi);
         return SFGPU_OK;
     }
     // full storage: copolymers and all second-order chains
@@ -404,7 +419,7 @@ int sfgpu_system::molecule_phi(int m) {
     for (int t = 1; t < N; t++) {
         int sg = o.seg[t];
         if (K == 1)
-            step1<<<g, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
+            step1_rows<<<gr, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
         else
             step2<<<g, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
                                        d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0);
@@ -417,7 +432,7 @@ int sfgpu_system::molecule_phi(int m) {
     for (int t = N - 2; t >= 0; t--) {
         int sg = o.seg[t];
         if (K == 1)
-            step1<<<g, kBlock, 0, s>>>(L, cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
+            step1_rows<<<gr, kBlock, 0, s>>>(L, cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
         else
             step2<<<g, kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv, d_gi + (size_t)t * KM,
                                        o.d_phi[sg], COMP_ACC, 1);
@@ -425,7 +440,10 @@ int sfgpu_system::molecule_phi(int m) {
     }
     wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, cur, d_wgn, d_partial);
     mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, scal, m);
-    for (int i : o.used) finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], scal, m, 0);
+    for (int i : o.used) {
+        finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], scal, m, 0);
+        if (K == 1) set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_phi[i]);
+    }
     return SFGPU_OK;
 }
 
@@ -677,7 +695,7 @@ extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fw
     for (int r = 0; r < reps; r++) {
         size_t t = 1 + (size_t)r % (nslices - 1);
         if (K == 1)
-            step1<<<g, kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE);
+            step1_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE);
         else
             step2<<<g, kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, 0.2, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE, 0);
     }
@@ -687,7 +705,7 @@ extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fw
         const double *src = s->d_ginv[r & 1];
         double *dst = s->d_ginv[(r + 1) & 1];
         if (K == 1)
-            step1<<<g, kBlock, 0, s->stream>>>(s->H.L, src, G, dst, s->d_gi + t * KM, phi, COMP_ACC);
+            step1_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, src, G, dst, s->d_gi + t * KM, phi, COMP_ACC);
         else
             step2<<<g, kBlock, 0, s->stream>>>(s->H.L, src, G, 0.2, dst, s->d_gi + t * KM, phi, COMP_ACC, 1);
     }
