@@ -47,6 +47,7 @@ PROTOTYPES = {
     "sfgpu_batch_solve_resident": (i32, [vp, f64, i32, f64]),
     "sfgpu_batch_results": (i32, [vp, dp, ip, ip, dp]),
     "sfgpu_batch_kernel_ms": (i32, [vp, dp]),
+    "sfgpu_chain_phi_noalloc": (i32, [vp, i32, ip, i32, C.POINTER(vp), C.POINTER(vp), vp, vp]),
 }
 
 _lib = None

@@ -231,6 +231,38 @@ int sfgpu_batch_kernel_ms(sfgpu_batch *batch, double *ms);
 /* state profile of one instance after the solve (its last evaluation) */
 int sfgpu_batch_get_phi(sfgpu_batch *batch, int instance, int segment, double *phi);
 
+/* ---- allocation-free chain propagation -------------------------------- */
+/* No counterpart in SFbox: an addition of this library.
+ *
+ * For callers that cannot allocate device memory -- code running inside
+ * another application's memory pool, a process whose device memory is
+ * reserved up front, or anything that must not change the device's
+ * allocation state while it runs -- and so cannot create an sfgpu_system
+ * (which allocates its buffers once at creation).  This call propagates one
+ * first-order chain (N segments, segment index seg_of_s[s] per position, a
+ * host array) on the lattice *lat with the caller's device arrays G[i] (M
+ * segment weighting factors per segment type i, boundary layers set) and
+ * writes, into the caller's device arrays phi[i], the unnormalised volume
+ * fraction sum_s Gf(z,s) Gb(z,s) / G(z) of every segment type used, plus
+ * lnGN into the caller's device double *lngn.  Multiply phi by phibulk/N
+ * (free) or theta/(N exp(lnGN)) (restricted) to normalise.  G and phi are
+ * host arrays of nseg device pointers.
+ *
+ * It calls no cudaMalloc, cudaFree or other allocating routine: all
+ * intermediates live in one array inside the library of 2*1024*1024 doubles
+ * (16 MiB), which every GPU that loads the library keeps until the process
+ * exits.  The chain must satisfy 2*MX + 3*M + 1024 + N*M <= 2097152 (MX =
+ * layers of the first gradient incl. boundaries); larger chains are
+ * rejected with SFGPU_ERR_INVALID before any work is queued.  The first call
+ * on a device looks up the array's device address (once per device, with
+ * that device current); make that first call before any stream capture.
+ * All work is queued on `stream` (0 = legacy default stream).  Every call
+ * uses the same array and overwrites it, and nothing in it has to start at
+ * zero (phi is cleared by the call); two calls that overlap on the GPU, on
+ * different streams or devices sharing a context, race on it. */
+int sfgpu_chain_phi_noalloc(const sfgpu_lattice_desc *lat, int N, const int *seg_of_s, int nseg,
+                            const double *const *G, double *const *phi, double *lngn, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
