@@ -45,11 +45,8 @@ def parse():
 
 def instances(rank: int, count: int):
     from field_b200 import configs
-    out = []
-    for i in range(count):
-        spec, x0 = configs.cyl_micelle(seed=configs.BASE_SEED + 2 + 1000 * rank + i)
-        out.append((spec, x0))
-    return out
+    from field_b200.shard import instance_seeds
+    return [configs.cyl_micelle(seed=sd) for sd in instance_seeds(rank, count, configs.BASE_SEED + 2)]
 
 
 # ---------------------------------------------------------------------------
@@ -257,13 +254,9 @@ def run_ours(a, rank, world, local_rank):
     barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop() if sampler else None
-    local = torch.tensor([sum(times)], device=dev, dtype=torch.float64)
-    solved = torch.tensor([float(conv_total)], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(local, op=dist.ReduceOp.MAX)
-        dist.all_reduce(solved, op=dist.ReduceOp.SUM)
-    t_max = local.item()
-    value = solved.item() / t_max
+    from field_b200.shard import aggregate
+    t_max, solved_all = aggregate(sum(times), conv_total, world, dev)
+    value = solved_all / t_max
 
     # e2e through the public API: pinned host guesses in, iterates out, every step
     h2d = sum(x.size for _, x in insts) * 8
@@ -279,12 +272,8 @@ def run_ours(a, rank, world, local_rank):
             torch.cuda.synchronize()
             et += e0.elapsed_time(e1) / 1000.0
             econv += int(r.converged.sum())
-        el = torch.tensor([et], device=dev, dtype=torch.float64)
-        ec = torch.tensor([float(econv)], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(el, op=dist.ReduceOp.MAX)
-            dist.all_reduce(ec, op=dist.ReduceOp.SUM)
-        e2e_value = ec.item() / el.item()
+        el, ec = aggregate(et, econv, world, dev)
+        e2e_value = ec / el
     else:
         e2e_value = value
     e2e = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
@@ -311,7 +300,7 @@ def run_ours(a, rank, world, local_rank):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "form": a.form, "instances_per_rank_per_step": B,
                            "method": "Pure_DIIS, m=%d, eta=%g" % (DIIS_M, DIIS_ETA),
-                           "tolerance": TOL, "converged": int(solved.item()),
+                           "tolerance": TOL, "converged": int(solved_all),
                            "mean_iterations": iters_total / max(1, conv_total),
                            "l2": "256 MB buffer written between timed steps",
                            "parallelism": f"instances x{world}"},

@@ -37,6 +37,14 @@ PROTOTYPES = {
     "sfgpu_lat_lngn": (i32, [vp, vp, i32, dp]),
     "sfgpu_solve_diis": (i32, [vp, dp, f64, i32, i32, f64, ip, dp]),
     "sfgpu_profile_propagator": (i32, [vp, i32, dp, dp, dp, dp]),
+    "sfgpu_system_set_tile": (i32, [vp, i32]),
+    "sfgpu_jvp": (i32, [vp, vp, vp, vp, vp]),
+    "sfgpu_jvp_host": (i32, [vp, dp, dp, dp, dp]),
+    "sfgpu_solve_nk": (i32, [vp, dp, f64, i32, i32, ip, ip, dp]),
+    "sfgpu_vjp": (i32, [vp, vp, vp, vp, vp]),
+    "sfgpu_vjp_host": (i32, [vp, dp, dp, dp, dp]),
+    "sfgpu_solve_lbfgs": (i32, [vp, dp, f64, i32, i32, ip, ip, dp]),
+    "sfgpu_system_autotune": (i32, [vp, i32, ip, dp]),
     "sfgpu_batch_create": (i32, [i32, vp, i32, C.POINTER(vp)]),
     "sfgpu_batch_destroy": (i32, [vp]),
     "sfgpu_batch_info": (i32, [vp, ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),

@@ -161,32 +161,34 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         for (int t = 1; t < half; t++) {
             const double *src = gi + (size_t)(t - 1) * M;
             double *dst = gi + (size_t)t * M;
-            for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
-                dst[R.base + k] = prop1_row(L, R, src, G, k, nlast);
-            });
+            for_interior4(L, threadIdx.x, blockDim.x,
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, src, G, k, nlast); },
+                [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
             __syncthreads();
         }
         const double *cur = gi + (size_t)(half - 1) * M;
         if (N % 2 == 1) {
             double *dst = bufA;
-            for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
-                const int z = R.base + k;
-                double out = prop1_row(L, R, cur, G, k, nlast);
-                dst[z] = out;
-                phi[z] = (phi[z] + out * out) * 0.5;
-            });
+            for_interior4(L, threadIdx.x, blockDim.x,
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, cur, G, k, nlast); },
+                [&](const RowInfo &R, int k, double out) {
+                    const int z = R.base + k;
+                    dst[z] = out;
+                    phi[z] = (phi[z] + out * out) * 0.5;
+                });
             __syncthreads();
             cur = bufA; double *t = bufA; bufA = bufB; bufB = t;
         }
         for (int sp = (N + 3) / 2; sp <= N; sp++) {
             const double *other = gi + (size_t)(N - sp) * M;
             double *dst = bufA;
-            for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
-                const int z = R.base + k;
-                double out = prop1_row(L, R, cur, G, k, nlast);
-                dst[z] = out;
-                phi[z] += out * other[z];
-            });
+            for_interior4(L, threadIdx.x, blockDim.x,
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, cur, G, k, nlast); },
+                [&](const RowInfo &R, int k, double out) {
+                    const int z = R.base + k;
+                    dst[z] = out;
+                    phi[z] += out * other[z];
+                });
             __syncthreads();
             cur = bufA; double *t = bufA; bufA = bufB; bufB = t;
         }
@@ -203,9 +205,9 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         const double *src = gi + (size_t)(t - 1) * M;
         double *dst = gi + (size_t)t * M;
         const double *G = I.gseg[o.seg[t]];
-        for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
-            dst[R.base + k] = prop1_row(L, R, src, G, k, nlast);
-        });
+        for_interior4(L, threadIdx.x, blockDim.x,
+            [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, src, G, k, nlast); },
+            [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
         __syncthreads();
     }
     {
@@ -228,12 +230,13 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         const double *gf = gi + (size_t)t * M;
         double *phi = o.phi[sg];
         double *dst = bufA;
-        for_interior(L, threadIdx.x, blockDim.x, [&](const RowInfo &R, int k, int nlast) {
-            const int z = R.base + k;
-            double out = prop1_row(L, R, cur, G, k, nlast);
-            dst[z] = out;
-            phi[z] += out * gf[z];
-        });
+        for_interior4(L, threadIdx.x, blockDim.x,
+            [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, cur, G, k, nlast); },
+            [&](const RowInfo &R, int k, double out) {
+                const int z = R.base + k;
+                dst[z] = out;
+                phi[z] += out * gf[z];
+            });
         __syncthreads();
         cur = bufA; double *tt = bufA; bufA = bufB; bufB = tt;
     }

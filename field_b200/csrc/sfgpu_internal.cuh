@@ -144,12 +144,13 @@ struct RowInfo {
     int base;        // site index of the row's element 0 (boundary position)
     int up, dn;      // offsets of the first-gradient neighbour rows (2D/3D)
     int up2, dn2;    // offsets of the second-gradient neighbour rows (3D)
-    int x;           // first-gradient coordinate (cylinder tables)
+    int x, y;        // coordinates of the row (x: cylinder tables)
 };
 
 __device__ __forceinline__ RowInfo lat_row(const DLat &L, int row) {
     RowInfo R;
     R.up = R.dn = R.up2 = R.dn2 = 0;
+    R.y = 0;
     if (L.grad == 1) { R.base = 0; R.x = 0; return R; }
     if (L.grad == 2) {
         int x = row + 1;
@@ -162,6 +163,7 @@ __device__ __forceinline__ RowInfo lat_row(const DLat &L, int row) {
     int ny = L.Md[1] - 2;
     int x = row / ny + 1, y = row - (x - 1) * ny + 1;
     R.x = x;
+    R.y = y;
     R.base = x * L.st[0] + y * L.st[1];
     R.up = (lat_mapc(L, 0, x - 1) - x) * L.st[0];
     R.dn = (lat_mapc(L, 0, x + 1) - x) * L.st[0];
@@ -213,6 +215,51 @@ __device__ __forceinline__ void for_interior(const DLat &L, int worker, int nwor
     for (int row = warp; row < nrows; row += nw) {
         RowInfo R = lat_row(L, row);
         for (int k = lane + 1; k <= nlast; k += 32) f(R, k, nlast);
+    }
+}
+
+// Same walk, four positions per lane at a time: all four stencils are
+// computed (every load issued) before any result is stored, so one thread
+// keeps four rows' worth of loads in flight instead of waiting on each.
+// compute(R, k, nlast) -> double, store(R, k, value).
+template <class C, class S>
+__device__ __forceinline__ void for_interior4(const DLat &L, int worker, int nworkers, C &&compute, S &&store) {
+    const int d = L.grad - 1;
+    const int nlast = L.Md[d] - 2;
+    if (L.grad == 1) {
+        RowInfo R = lat_row(L, 0);
+        for (int k0 = worker + 1; k0 <= nlast; k0 += 4 * nworkers) {
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                int k = k0 + u * nworkers;
+                v[u] = (k <= nlast) ? compute(R, k, nlast) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                int k = k0 + u * nworkers;
+                if (k <= nlast) store(R, k, v[u]);
+            }
+        }
+        return;
+    }
+    const int lane = worker & 31, warp = worker >> 5, nw = nworkers >> 5;
+    const int nrows = lat_nrows(L);
+    for (int row = warp; row < nrows; row += nw) {
+        RowInfo R = lat_row(L, row);
+        for (int k0 = lane + 1; k0 <= nlast; k0 += 128) {
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                int k = k0 + 32 * u;
+                v[u] = (k <= nlast) ? compute(R, k, nlast) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                int k = k0 + 32 * u;
+                if (k <= nlast) store(R, k, v[u]);
+            }
+        }
     }
 }
 

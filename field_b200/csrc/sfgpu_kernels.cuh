@@ -56,13 +56,87 @@ static __global__ void step1_rows(DLat L, const double *__restrict__ gin, const 
                                   double *__restrict__ gout, const double *__restrict__ other,
                                   double *__restrict__ phi, int mode) {
     const int worker = blockIdx.x * blockDim.x + threadIdx.x;
-    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
-        const double out = prop1_row(L, R, gin, G, k, nlast);
-        const int t = R.base + k;
-        gout[t] = out;
-        if (mode == COMP_ACC) phi[t] += out * other[t];
-        else if (mode == COMP_CENTRE) phi[t] = (phi[t] + out * out) * 0.5;
-    });
+    for_interior4(L, worker, gridDim.x * blockDim.x,
+        [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, gin, G, k, nlast); },
+        [&](const RowInfo &R, int k, double out) {
+            const int t = R.base + k;
+            gout[t] = out;
+            if (mode == COMP_ACC) phi[t] += out * other[t];
+            else if (mode == COMP_CENTRE) phi[t] = (phi[t] + out * out) * 0.5;
+        });
+}
+
+// First-order step on a 3D lattice, x-marching: a block owns a 32 (z) x 8
+// (y) tile of columns and walks `xc` consecutive x planes.  The x-1/x/x+1
+// values of a column stay in registers, the y/z neighbours come from the
+// current plane staged in shared memory, so every value of gin is read from
+// L2/HBM about once (plus a 1-plane overlap per chunk and the tile halos).
+// Neighbour coordinates 0 and n+1 read the site their boundary entry would
+// copy; boundary entries are neither read nor written.  Operation order as
+// stencil1 (Lat3D1stO.cpp:151-157).
+constexpr int kTZ = 32, kTY = 8;
+static __global__ void __launch_bounds__(kTZ * kTY)
+step3d_march(DLat L, const double *__restrict__ gin, const double *__restrict__ G,
+             double *__restrict__ gout, const double *__restrict__ other, double *__restrict__ phi,
+             int mode, int xc) {
+    __shared__ double tile[kTY + 2][kTZ + 2];
+    const int nx = L.Md[0] - 2, ny = L.Md[1] - 2, nz = L.Md[2] - 2;
+    const int jx = L.st[0], jy = L.st[1];
+    const int tz = threadIdx.x % kTZ, ty = threadIdx.x / kTZ;
+    const int z = blockIdx.x * kTZ + tz + 1;
+    const int y = blockIdx.y * kTY + ty + 1;
+    const int x0 = blockIdx.z * xc + 1;
+    if (x0 > nx) return;
+    const int x1 = min(x0 + xc - 1, nx);
+    const bool act = (z <= nz) && (y <= ny);
+    const int zm = lat_mapc(L, 2, z - 1), zp = lat_mapc(L, 2, z + 1);
+    const int ym = lat_mapc(L, 1, y - 1), yp = lat_mapc(L, 1, y + 1);
+    const bool hz0 = (tz == 0), hz1 = (tz == kTZ - 1) || (z == nz);
+    const bool hy0 = (ty == 0), hy1 = (ty == kTY - 1) || (y == ny);
+    const int col = y * jy + z;
+    double vprev = 0, vcur = 0;
+    if (act) {
+        vprev = gin[lat_mapc(L, 0, x0 - 1) * jx + col];
+        vcur = gin[x0 * jx + col];
+    }
+    for (int x = x0; x <= x1; x++) {
+        double vnext = 0, g = 0, hz_lo = 0, hz_hi = 0, hy_lo = 0, hy_hi = 0;
+        const int base = x * jx;
+        if (act) {
+            vnext = gin[lat_mapc(L, 0, x + 1) * jx + col];
+            g = G[base + col];
+            if (hz0) hz_lo = gin[base + y * jy + zm];
+            if (hz1) hz_hi = gin[base + y * jy + zp];
+            if (hy0) hy_lo = gin[base + ym * jy + z];
+            if (hy1) hy_hi = gin[base + yp * jy + z];
+        }
+        __syncthreads();
+        if (act) {
+            // only active columns write their own slot: in a partial tile the
+            // slot right of the last column is that column's halo
+            tile[ty + 1][tz + 1] = vcur;
+            if (hz0) tile[ty + 1][0] = hz_lo;
+            if (hz1) tile[ty + 1][tz + 2] = hz_hi;
+            if (hy0) tile[0][tz + 1] = hy_lo;
+            if (hy1) tile[ty + 2][tz + 1] = hy_hi;
+        }
+        __syncthreads();
+        if (act) {
+            double acc = vprev * g;
+            acc += vnext * g;
+            acc += tile[ty][tz + 1] * g;
+            acc += tile[ty + 2][tz + 1] * g;
+            acc += tile[ty + 1][tz] * g;
+            acc += tile[ty + 1][tz + 2] * g;
+            const double out = acc * (1.0 / 6.0);
+            const int t = base + col;
+            gout[t] = out;
+            if (mode == COMP_ACC) phi[t] += out * other[t];
+            else if (mode == COMP_CENTRE) phi[t] = (phi[t] + out * out) * 0.5;
+        }
+        vprev = vcur;
+        vcur = vnext;
+    }
 }
 
 // One second-order step (Lat3D2ndO::PropagateF, Lat3D2ndO.cpp:65-152, and
@@ -118,6 +192,94 @@ static __global__ void step2(DLat L, const double *__restrict__ gin, const doubl
             phi[r] = p;
         }
     }
+}
+
+// Second-order steps over interior sites only (row-wise).  A neighbour on a
+// boundary plane is read at its mapped site, with the x/y/z direction pair
+// swapped when that boundary is a mirror (the SetBx1(gz0,gz5) ... copies of
+// Lat3D2ndO.cpp:84-89).  Forward: component k at t collects the five allowed
+// components at t - e_k (Lat3D2ndO.cpp:109-143); backward: component k' at t
+// collects component k at t + e_k (:634-668).  Same weights and summation
+// order as comp2.
+__device__ __forceinline__ bool is_mirror(int bc) {
+    return bc == SFGPU_BOUND_MIRROR1 || bc == SFGPU_BOUND_MIRROR2;
+}
+static __global__ void step2_rows(DLat L, const double *__restrict__ gin, const double *__restrict__ G, double S,
+                                  double *__restrict__ gout, const double *__restrict__ other,
+                                  double *__restrict__ phi, int mode, int backward) {
+    const int M = L.M;
+    const double Lw = (1.0 - S) / 4.0;
+    const int nx = L.Md[0] - 2, ny = L.Md[1] - 2;
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const int t = R.base + k;
+        // neighbour offsets and mirror swaps by direction: [0]=-x [1]=+x [2]=-y [3]=+y [4]=-z [5]=+z
+        const int zm = (k == 1) ? L.map_lo[2] : k - 1;
+        const int zp = (k == nlast) ? L.map_hi[2] : k + 1;
+        const int off[6] = {R.up, R.dn, R.up2, R.dn2, zm - k, zp - k};
+        const bool sw[6] = {R.x == 1 && is_mirror(L.bc_lo[0]), R.x == nx && is_mirror(L.bc_hi[0]),
+                            R.y == 1 && is_mirror(L.bc_lo[1]), R.y == ny && is_mirror(L.bc_hi[1]),
+                            k == 1 && is_mirror(L.bc_lo[2]), k == nlast && is_mirror(L.bc_hi[2])};
+        const double g = G[t];
+        const double gS = g * S, gL = g * Lw;
+        double out[6];
+        if (!backward) {
+            // source of component kk is t - e_kk: kk=0 -> -x, 5 -> +x, 1 -> -y, 4 -> +y, 2 -> -z, 3 -> +z
+            const int dir_of[6] = {0, 2, 4, 5, 3, 1};
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++) {
+                const int dd = dir_of[kk];
+                const int src = t + off[dd];
+                const int axis = dd >> 1;
+                const bool s = sw[dd];
+                double acc = 0;
+                bool first = true;
+#pragma unroll
+                for (int kp = 0; kp < 6; kp++) {
+                    if (kp == 5 - kk) continue;
+                    int c = kp;
+                    if (s) {
+                        if (axis == 0 && (kp == 0 || kp == 5)) c = 5 - kp;
+                        if (axis == 1 && (kp == 1 || kp == 4)) c = 5 - kp;
+                        if (axis == 2 && (kp == 2 || kp == 3)) c = 5 - kp;
+                    }
+                    double v = gin[(size_t)c * M + src] * (kp == kk ? gS : gL);
+                    if (first) { acc = v; first = false; } else acc += v;
+                }
+                out[kk] = acc;
+            }
+        } else {
+            // component k is read at t + e_k: 0 -> +x, 5 -> -x, 1 -> +y, 4 -> -y, 2 -> +z, 3 -> -z
+            const int dir_of[6] = {1, 3, 5, 4, 2, 0};
+            double v[6];
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++) {
+                const int dd = dir_of[kk];
+                const int c = sw[dd] ? 5 - kk : kk;
+                v[kk] = gin[(size_t)c * M + t + off[dd]];
+            }
+#pragma unroll
+            for (int kq = 0; kq < 6; kq++) {
+                double acc = 0;
+                bool first = true;
+#pragma unroll
+                for (int kp = 5; kp >= 0; kp--) {
+                    if (kp == 5 - kq) continue;
+                    double w = v[kp] * (kp == kq ? gS : gL);
+                    if (first) { acc = w; first = false; } else acc += w;
+                }
+                out[kq] = acc;
+            }
+        }
+#pragma unroll
+        for (int kk = 0; kk < 6; kk++) gout[(size_t)kk * M + t] = out[kk];
+        if (mode == COMP_ACC) {
+            double p = phi[t];
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++) p += out[kk] * other[(size_t)kk * M + t];
+            phi[t] = p;
+        }
+    });
 }
 
 // phi += a * b over all K*M entries summed per site (copolymer end segment,

@@ -38,6 +38,20 @@ static int grid_rows(const DLat &L) {
     return (int)std::max(1L, std::min(b, 148L * 32));
 }
 
+// first-order step inside a residual evaluation: x-marching tiles in 3D,
+// row-wise otherwise
+int sfgpu_system::launch_step1(const double *gin, const double *G, double *gout, const double *other, double *phi,
+                               int mode) {
+    const DLat &L = H.L;
+    if (L.grad == 3) {
+        dim3 grid((L.Md[2] - 2 + kTZ - 1) / kTZ, (L.Md[1] - 2 + kTY - 1) / kTY, (L.Md[0] - 2 + tile_xc - 1) / tile_xc);
+        step3d_march<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, tile_xc);
+    } else {
+        step1_rows<<<grid_rows(L), kBlock, 0, stream>>>(L, gin, G, gout, other, phi, mode);
+    }
+    return SFGPU_OK;
+}
+
 // ---------------------------------------------------------------------------
 // lattice set-up (Lat1DFlat.cpp:4-149, Lat2DFlat.cpp:35-220,
 // Lat2DCylinder.cpp:7-55, Lat3D.cpp:44-236)
@@ -369,7 +383,6 @@ int sfgpu_system::molecule_phi(int m) {
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_for(M);
-    const int gr = grid_rows(L);
     cudaStream_t s = stream;
     MolParam p;
     p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = o.sym; p.K = K;
@@ -395,15 +408,15 @@ int sfgpu_system::molecule_phi(int m) {
         double *phi = o.d_phi[i];
         SFGPU_CUDA_TRY(cudaMemcpyAsync(d_gi, G, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
         for (int t = 1; t < half; t++)
-            step1_rows<<<gr, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * M, G, d_gi + (size_t)t * M, nullptr, nullptr, COMP_NONE);
+            launch_step1(d_gi + (size_t)(t - 1) * M, G, d_gi + (size_t)t * M, nullptr, nullptr, COMP_NONE);
         const double *cur = d_gi + (size_t)(half - 1) * M;
         if (N % 2 == 1) {
-            step1_rows<<<gr, kBlock, 0, s>>>(L, cur, G, ginv, nullptr, phi, COMP_CENTRE);
+            launch_step1(cur, G, ginv, nullptr, phi, COMP_CENTRE);
             cur = ginv; std::swap(ginv, tmp);
         }
         for (int sp = (N + 3) / 2; sp <= N; sp++) {
             int sinv = N - sp + 1;
-            step1_rows<<<gr, kBlock, 0, s>>>(L, cur, G, ginv, d_gi + (size_t)(sinv - 1) * M, phi, COMP_ACC);
+            launch_step1(cur, G, ginv, d_gi + (size_t)(sinv - 1) * M, phi, COMP_ACC);
             cur = ginv; std::swap(ginv, tmp);
         }
         wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, cur, d_wgn, d_partial);
@@ -419,9 +432,9 @@ int sfgpu_system::molecule_phi(int m) {
     for (int t = 1; t < N; t++) {
         int sg = o.seg[t];
         if (K == 1)
-            step1_rows<<<gr, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
+            launch_step1(d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
         else
-            step2<<<g, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
+            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
                                        d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0);
     }
     replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[N - 1]], ginv);
@@ -432,17 +445,17 @@ int sfgpu_system::molecule_phi(int m) {
     for (int t = N - 2; t >= 0; t--) {
         int sg = o.seg[t];
         if (K == 1)
-            step1_rows<<<gr, kBlock, 0, s>>>(L, cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
+            launch_step1(cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
         else
-            step2<<<g, kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv, d_gi + (size_t)t * KM,
-                                       o.d_phi[sg], COMP_ACC, 1);
+            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv,
+                                       d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC, 1);
         cur = ginv; std::swap(ginv, tmp);
     }
     wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, cur, d_wgn, d_partial);
     mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, scal, m);
     for (int i : o.used) {
         finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], scal, m, 0);
-        if (K == 1) set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_phi[i]);
+        set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_phi[i]);
     }
     return SFGPU_OK;
 }
@@ -695,9 +708,9 @@ extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fw
     for (int r = 0; r < reps; r++) {
         size_t t = 1 + (size_t)r % (nslices - 1);
         if (K == 1)
-            step1_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE);
+            s->launch_step1(s->d_gi + (t - 1) * KM, G, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE);
         else
-            step2<<<g, kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, 0.2, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE, 0);
+            step2_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, 0.2, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE, 0);
     }
     SFGPU_CUDA_TRY(cudaEventRecord(e1, s->stream));
     for (int r = 0; r < reps; r++) {
@@ -705,9 +718,9 @@ extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fw
         const double *src = s->d_ginv[r & 1];
         double *dst = s->d_ginv[(r + 1) & 1];
         if (K == 1)
-            step1_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, src, G, dst, s->d_gi + t * KM, phi, COMP_ACC);
+            s->launch_step1(src, G, dst, s->d_gi + t * KM, phi, COMP_ACC);
         else
-            step2<<<g, kBlock, 0, s->stream>>>(s->H.L, src, G, 0.2, dst, s->d_gi + t * KM, phi, COMP_ACC, 1);
+            step2_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, src, G, 0.2, dst, s->d_gi + t * KM, phi, COMP_ACC, 1);
     }
     SFGPU_CUDA_TRY(cudaEventRecord(e2, s->stream));
     SFGPU_CUDA_TRY(cudaEventSynchronize(e2));
@@ -719,5 +732,40 @@ extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fw
     if (ms_bwd) *ms_bwd = b / reps;
     if (bytes_fwd) *bytes_fwd = 8.0 * (2 * K + 1) * M;
     if (bytes_bwd) *bytes_bwd = 8.0 * (3 * K + 3) * M;
+    return SFGPU_OK;
+}
+
+// Pick the x-chunk depth of the 3D first-order step by timing each candidate
+// on this system's buffers (CUDA events, `reps` forward + backward steps
+// each); the fastest is kept for all later evaluations.  Other lattices have
+// nothing to tune.
+extern "C" int sfgpu_system_autotune(sfgpu_system *s, int reps, int *chosen_xc, double *best_ms) {
+    CHECK_SYS(s);
+    if (reps < 1) return fail(SFGPU_ERR_INVALID, "reps must be positive");
+    if (s->H.L.grad != 3 || s->K != 1) {
+        if (chosen_xc) *chosen_xc = s->tile_xc;
+        if (best_ms) *best_ms = 0;
+        return SFGPU_OK;
+    }
+    const int cand[] = {2, 4, 8, 16, 32};
+    double best = 1e30;
+    int bestx = s->tile_xc;
+    for (int c : cand) {
+        s->tile_xc = c;
+        double f = 0, b = 0;
+        int rc = sfgpu_profile_propagator(s, reps, &f, &b, nullptr, nullptr);
+        if (rc) return rc;
+        if (f + b < best) { best = f + b; bestx = c; }
+    }
+    s->tile_xc = bestx;
+    if (chosen_xc) *chosen_xc = bestx;
+    if (best_ms) *best_ms = best;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_set_tile(sfgpu_system *s, int xc) {
+    CHECK_SYS(s);
+    if (xc < 1 || xc > 1024) return fail(SFGPU_ERR_INVALID, "tile depth must be in 1..1024");
+    s->tile_xc = xc;
     return SFGPU_OK;
 }

@@ -14,6 +14,7 @@ struct HMol {
     double phibulk = 0, theta = 0, chemintref = 0;
     std::vector<int> seg, used, count;
     std::vector<double *> d_phi;      // per segment (used ones)
+    std::vector<double *> d_dphi;     // tangents (allocated on first J*v)
 };
 
 struct sfgpu_system {
@@ -35,6 +36,26 @@ struct sfgpu_system {
     double *d_partial = nullptr, *d_scal = nullptr, *d_phib = nullptr, *d_chib = nullptr, *d_misc = nullptr;
     double *d_x = nullptr, *d_f = nullptr;
     int nblocks_red = 1;
+    int tile_xc = 8;          // x planes per block of the 3D first-order step
+    // forward-mode tangent buffers, allocated on the first J*v
+    bool t_ready = false;
+    std::vector<double *> dgfull, dgseg, dphi;
+    double *d_dgi = nullptr, *d_dginv[2] = {nullptr, nullptr};
+    double *d_tscal = nullptr, *d_dpartial = nullptr, *d_dphib = nullptr, *d_dchib = nullptr;
+    double *d_v = nullptr, *d_jv = nullptr;
+    int ensure_tangent();
+    int molecule_phi_t(int m);
+    int jvp_async(const double *x, const double *v, double *f, double *jv);
+    // reverse-mode (adjoint) buffers, allocated on the first J^T w
+    bool a_ready = false;
+    double *a_gf = nullptr, *a_gb = nullptr, *a_cot[2] = {nullptr, nullptr};
+    std::vector<double *> a_phibar, a_gbar, a_phibar_raw;
+    double *a_scal = nullptr, *a_chibbar = nullptr, *a_qbar = nullptr, *a_w = nullptr, *a_xbar = nullptr;
+    int ensure_adjoint();
+    int molecule_phi_store(int m);
+    int molecule_adjoint(int m);
+    int vjp_async(const double *x, const double *w, double *f, double *xbar);
+    int launch_step1(const double *gin, const double *G, double *gout, const double *other, double *phi, int mode);
     std::vector<void *> allocs;
 
     ~sfgpu_system();

@@ -25,6 +25,7 @@ def main():
     ap.add_argument("--case", default="c3", choices=["c2", "c3", "c5"])
     ap.add_argument("--reps", type=int, default=50)
     ap.add_argument("--n", type=int, default=0, help="lattice size override")
+    ap.add_argument("--tile", type=int, default=0, help="3D x-chunk depth (0: autotune)")
     a = ap.parse_args()
     if a.case == "c2":
         spec, x = configs.cyl_micelle(**({"nx": a.n, "ny": a.n} if a.n else {}))
@@ -34,9 +35,14 @@ def main():
         spec, x = configs.brush3d(**({"n": a.n} if a.n else {}))
     s = System(spec)
     s.residual(x)
+    tune = None
+    if a.tile:
+        s.set_tile(a.tile)
+    else:
+        tune = s.autotune(reps=max(5, a.reps // 5))
     p = s.profile_propagator(reps=a.reps)
     peak, kind = measured_peaks()
-    out = {"case": a.case, "M": s.M, "K": s.K, "reps": a.reps, **p,
+    out = {"case": a.case, "M": s.M, "K": s.K, "reps": a.reps, "tile": a.tile or tune, **p,
            "gbs_fwd": p["bytes_fwd"] / (p["ms_fwd"] / 1e3) / 1e9,
            "gbs_bwd": p["bytes_bwd"] / (p["ms_bwd"] / 1e3) / 1e9, "peak_gbs": peak, "peak_kind": kind}
     out["frac_fwd"] = out["gbs_fwd"] / peak

@@ -115,11 +115,59 @@ class System:
             nat.check(rc, "sfgpu_solve_diis")
         return SolveResult(x, rc, it.value, err.value)
 
+    def jvp(self, x, v):
+        """(f(x), J(x) v) with the exact forward-mode tangent."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        f = np.empty(self.nvar)
+        jv = np.empty(self.nvar)
+        nat.check(self.lib.sfgpu_jvp_host(self.h, _d(x), _d(v), _d(f), _d(jv)), "sfgpu_jvp_host")
+        return f, jv
+
+    def vjp(self, x, w):
+        """(f(x), J(x)^T w) from the adjoint sweep (first-order lattices)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        f = np.empty(self.nvar)
+        xb = np.empty(self.nvar)
+        nat.check(self.lib.sfgpu_vjp_host(self.h, _d(x), _d(w), _d(f), _d(xb)), "sfgpu_vjp_host")
+        return f, xb
+
+    def solve_lbfgs(self, x0=None, tol=1e-7, maxit=2000, m=10) -> SolveResult:
+        """L-BFGS on |f|^2/2 with the adjoint gradient (sfgpu_solve_lbfgs)."""
+        x = np.zeros(self.nvar) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+        it, ne, err = C.c_int(), C.c_int(), C.c_double()
+        rc = self.lib.sfgpu_solve_lbfgs(self.h, _d(x), tol, maxit, m, C.byref(it), C.byref(ne), C.byref(err))
+        if rc not in (0, 4, 5):
+            nat.check(rc, "sfgpu_solve_lbfgs")
+        r = SolveResult(x, rc, it.value, err.value)
+        r.evaluations = ne.value
+        return r
+
+    def solve_nk(self, x0=None, tol=1e-7, maxit=50, krylov=30) -> SolveResult:
+        """Newton-Krylov with exact J*v (sfgpu_solve_nk)."""
+        x = np.zeros(self.nvar) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+        it, nj, err = C.c_int(), C.c_int(), C.c_double()
+        rc = self.lib.sfgpu_solve_nk(self.h, _d(x), tol, maxit, krylov, C.byref(it), C.byref(nj), C.byref(err))
+        if rc not in (0, 4, 5):
+            nat.check(rc, "sfgpu_solve_nk")
+        r = SolveResult(x, rc, it.value, err.value)
+        r.jvps = nj.value
+        return r
+
     def profile_propagator(self, reps: int = 200):
         a, b, c, d = C.c_double(), C.c_double(), C.c_double(), C.c_double()
         nat.check(self.lib.sfgpu_profile_propagator(self.h, reps, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
                   "sfgpu_profile_propagator")
         return {"ms_fwd": a.value, "ms_bwd": b.value, "bytes_fwd": c.value, "bytes_bwd": d.value}
+
+    def autotune(self, reps: int = 20):
+        x, ms = C.c_int(), C.c_double()
+        nat.check(self.lib.sfgpu_system_autotune(self.h, reps, C.byref(x), C.byref(ms)), "sfgpu_system_autotune")
+        return {"tile_xc": x.value, "ms_fwd_plus_bwd": ms.value}
+
+    def set_tile(self, xc: int):
+        nat.check(self.lib.sfgpu_system_set_tile(self.h, xc), "sfgpu_system_set_tile")
 
     # ---- Lattice-level (torch CUDA tensors) -------------------------------
     def _sync_torch(self):

@@ -183,6 +183,42 @@ int sfgpu_lat_side_fraction(sfgpu_system *sys, const double *phi, double *rho);
  * Lat3D2ndO.cpp:995-1025) of an end-point distribution */
 int sfgpu_lat_lngn(sfgpu_system *sys, const double *g, int components, double *lngn);
 
+/* ---- derivatives ------------------------------------------------------- */
+/* f = residuals(x) and jv = J(x) v with J the exact Jacobian df/dx, by a
+ * forward-mode (tangent) sweep through UpdateSWF, both propagator sweeps, the
+ * composition, the lnGN/phibulk normalisations and GetResiduals.  SFbox forms
+ * J*v only by finite differences of residuals (SFNewton::Hp,
+ * sfnewton.cpp:1662-1688).  f equals sfgpu_residual's bit for bit.  Device
+ * pointers, asynchronous; the _host variant copies and synchronises.  The
+ * first call allocates the tangent buffers (about the size of the
+ * propagator storage). */
+int sfgpu_jvp(sfgpu_system *sys, const double *x_dev, const double *v_dev, double *f_dev, double *jv_dev);
+int sfgpu_jvp_host(sfgpu_system *sys, const double *x, const double *v, double *f, double *jv);
+/* Newton-Krylov iteration on residuals(x) = 0: GMRES(krylov) with exact J*v
+ * (Eisenstat-Walker forcing, backtracking line search on |f|), the
+ * replacement of SFNewton's numerical-Hessian and truncated-Newton methods
+ * (sfnewton.cpp:1627-1688, 1809-1944).  x is a host array (in: guess, out:
+ * last iterate; the system's profiles are those of the returned x). */
+int sfgpu_solve_nk(sfgpu_system *sys, double *x, double tol, int maxit, int krylov,
+                   int *iterations, int *jvps, double *final_error);
+
+/* f = residuals(x) and xbar = J(x)^T w by a reverse (adjoint) sweep:
+ * cotangents flow from GetResiduals through the contact averages, the
+ * normalisations (lnGN, restricted and solvent phibulk), CorrectDoubleCountG
+ * and the two propagator recursions (adjoint propagators run against their
+ * primal direction over stored Gf and Gb) to UpdateSWF.  First-order
+ * lattices (SFGPU_ERR_UNSUPPORTED for second order).  The first call
+ * allocates 2*N*M doubles for the stored propagators.  SFbox has no
+ * counterpart: its L-BFGS and truncated Newton use finite differences. */
+int sfgpu_vjp(sfgpu_system *sys, const double *x_dev, const double *w_dev, double *f_dev, double *xbar_dev);
+int sfgpu_vjp_host(sfgpu_system *sys, const double *x, const double *w, double *f, double *xbar);
+/* L-BFGS (Nocedal 1980 two-loop recursion, m pairs, Armijo backtracking) on
+ * |f(x)|^2 / 2 with the exact gradient J^T f from the adjoint sweep; SFbox's
+ * LBFGS method (SFNewton::L_BFGS, sfnewton.cpp:1770-1807) iterates on the
+ * residual itself.  x is a host array (in: guess, out: last iterate). */
+int sfgpu_solve_lbfgs(sfgpu_system *sys, double *x, double tol, int maxit, int m,
+                      int *iterations, int *evaluations, double *final_error);
+
 /* ---- measurement ------------------------------------------------------- */
 /* Average device time of one forward propagator step and of one backward
  * step with fused composition on this system's buffers (reps launches each,
@@ -191,6 +227,13 @@ int sfgpu_lat_lngn(sfgpu_system *sys, const double *g, int components, double *l
  * overwritten; call before the next residual. */
 int sfgpu_profile_propagator(sfgpu_system *sys, int reps, double *ms_fwd, double *ms_bwd,
                              double *bytes_fwd, double *bytes_bwd);
+
+/* Tile shape of the 3D first-order step (x planes walked per thread block):
+ * set it, or let the library time the candidates 2..32 on this system's own
+ * buffers and keep the fastest (reps forward + backward steps each; the
+ * propagator contents are overwritten).  Other lattices ignore it. */
+int sfgpu_system_set_tile(sfgpu_system *sys, int xc);
+int sfgpu_system_autotune(sfgpu_system *sys, int reps, int *chosen_xc, double *best_ms);
 
 /* ---- iterations ------------------------------------------------------- */
 /* Pure_DIIS: SFNewton::PlainLBFGSDIIS (sfnewton.cpp:566-664) on the device,

@@ -140,3 +140,32 @@ def test_full_size_c3_residual(gpu_lib):
     tot = (sys_.phi(0) + sys_.phi(1))[sites].sum()
     gn = np.exp(sys_.mol_scalars(0)["lngn"])
     assert abs(tot - gn) < 1e-10 * gn
+
+
+def test_brush_2nd_order_residual_48(gpu_lib):
+    """Config C5 shape (Lat3D2ndO, grafted (X)1(A)199 brush, mirror walls,
+    bending S=0.5) on a 48^3 lattice: residual, profiles and lnGN."""
+    from field_b200 import configs
+    spec, _ = configs.brush3d(n=48, N=200, sigma=0.05, S=0.5)
+    rng = np.random.default_rng(77)
+    x = rng.normal(0.0, 0.05, spec.n_itvar())
+    sys_ = System(spec)
+    o = Oracle(spec)
+    f_gpu, f_cpu = sys_.residual(x), o.residual(x)
+    assert rel(f_gpu, f_cpu) <= TOL_EVAL
+    for i in range(len(spec.segments)):
+        assert rel(sys_.phi(i), o.phi(i)) <= TOL_EVAL
+    assert abs(sys_.mol_scalars(0)["lngn"] - o.lngn(0)) <= 1e-12 * abs(o.lngn(0))
+
+
+def test_autotuned_tile_keeps_results(gpu_lib):
+    """The 3D tile depth changes the launch shape only, not the numbers."""
+    from field_b200 import configs
+    spec, x0 = configs.melt3d(n=20, nA=6, nB=5)
+    s = System(spec)
+    f_ref = s.residual(x0)
+    for xc in (1, 3, 7, 32):
+        s.set_tile(xc)
+        assert np.array_equal(s.residual(x0), f_ref)
+    s.autotune(reps=3)
+    assert np.array_equal(s.residual(x0), f_ref)
