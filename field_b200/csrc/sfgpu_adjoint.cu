@@ -159,12 +159,38 @@ int sfgpu_system::ensure_adjoint() {
     return SFGPU_OK;
 }
 
-// primal evaluation that keeps Gf and Gb of every segment (full chains, also
-// for homopolymers) for the reverse sweep
-int sfgpu_system::molecule_phi_store(int m) {
+// Gf and Gb of every position of molecule m's chain (full chains, also for
+// symmetric homopolymers) into a_gf / a_gb; with compose, the backward sweep
+// also accumulates Gf.Gb into the molecule's (zeroed) phi
+int sfgpu_system::store_chains(int m, bool compose) {
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_a(M), gr = grid_rows_a(L);
+    cudaStream_t s = stream;
+    const int N = o.N;
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(a_gf, d_gseg[o.seg[0]], sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+    for (int t = 1; t < N; t++)
+        step1_rows<<<gr, kBlock, 0, s>>>(L, a_gf + (size_t)(t - 1) * M, d_gseg[o.seg[t]], a_gf + (size_t)t * M,
+                                         nullptr, nullptr, COMP_NONE);
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(a_gb + (size_t)(N - 1) * M, d_gseg[o.seg[N - 1]], sizeof(double) * M,
+                                   cudaMemcpyDeviceToDevice, s));
+    if (compose)
+        connect<<<g, kBlock, 0, s>>>(M, 1, a_gb + (size_t)(N - 1) * M, a_gf + (size_t)(N - 1) * M,
+                                     o.d_phi[o.seg[N - 1]]);
+    for (int t = N - 2; t >= 0; t--) {
+        int sg = o.seg[t];
+        step1_rows<<<gr, kBlock, 0, s>>>(L, a_gb + (size_t)(t + 1) * M, d_gseg[sg], a_gb + (size_t)t * M,
+                                         compose ? a_gf + (size_t)t * M : nullptr, compose ? o.d_phi[sg] : nullptr,
+                                         compose ? COMP_ACC : COMP_NONE);
+    }
+    return SFGPU_OK;
+}
+
+// primal evaluation of molecule m through store_chains
+int sfgpu_system::molecule_phi_store(int m) {
+    HMol &o = mols[m];
+    const DLat &L = H.L;
+    const int g = grid_a(M);
     cudaStream_t s = stream;
     MolParam p;
     p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = 0; p.K = 1;
@@ -179,20 +205,8 @@ int sfgpu_system::molecule_phi_store(int m) {
         return SFGPU_OK;
     }
     for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_phi[i], 0, sizeof(double) * M, s));
-    const int N = o.N;
-    SFGPU_CUDA_TRY(cudaMemcpyAsync(a_gf, d_gseg[o.seg[0]], sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
-    for (int t = 1; t < N; t++)
-        step1_rows<<<gr, kBlock, 0, s>>>(L, a_gf + (size_t)(t - 1) * M, d_gseg[o.seg[t]], a_gf + (size_t)t * M,
-                                         nullptr, nullptr, COMP_NONE);
-    SFGPU_CUDA_TRY(cudaMemcpyAsync(a_gb + (size_t)(N - 1) * M, d_gseg[o.seg[N - 1]], sizeof(double) * M,
-                                   cudaMemcpyDeviceToDevice, s));
-    connect<<<g, kBlock, 0, s>>>(M, 1, a_gb + (size_t)(N - 1) * M, a_gf + (size_t)(N - 1) * M, o.d_phi[o.seg[N - 1]]);
-    for (int t = N - 2; t >= 0; t--) {
-        int sg = o.seg[t];
-        step1_rows<<<gr, kBlock, 0, s>>>(L, a_gb + (size_t)(t + 1) * M, d_gseg[sg], a_gb + (size_t)t * M,
-                                         a_gf + (size_t)t * M, o.d_phi[sg], COMP_ACC);
-    }
-    p.sym = 0;
+    int rc = store_chains(m, true);
+    if (rc) return rc;
     wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, a_gb, d_wgn, d_partial);
     mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, scal, m);
     for (int i : o.used) {
@@ -298,10 +312,20 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
     ap.chibbar = a_chibbar;
     adj_residual<<<grid_a(nsites), kBlock, 0, s>>>(L, rp, ct, d_sites, w, ap, xbar);
     adj_bulk<<<1, 1, 0, s>>>(bp, ct, a_chibbar, (AdjScal *)a_scal);
-    // molecules in reverse order of the primal (the solvent first)
+    // molecules in reverse order of the primal (the solvent first).  The
+    // chain storage holds one molecule: the last polymer the primal
+    // propagated keeps its chains, every other polymer is propagated again.
+    int held = (mols[solvent].type != 0) ? solvent : -1;
+    if (held < 0)
+        for (int m = nmol - 1; m >= 0 && held < 0; m--)
+            if (m != solvent && mols[m].type != 0) held = m;
     if ((rc = molecule_adjoint(solvent))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
+        if (mols[m].type != 0 && m != held) {
+            if ((rc = store_chains(m, false))) return rc;
+            held = m;
+        }
         if ((rc = molecule_adjoint(m))) return rc;
     }
     SwfAdj sa;

@@ -52,6 +52,7 @@ struct sfgpu_system {
     std::vector<double *> a_phibar, a_gbar, a_phibar_raw;
     double *a_scal = nullptr, *a_chibbar = nullptr, *a_qbar = nullptr, *a_w = nullptr, *a_xbar = nullptr;
     int ensure_adjoint();
+    int store_chains(int m, bool compose);
     int molecule_phi_store(int m);
     int molecule_adjoint(int m);
     int vjp_async(const double *x, const double *w, double *f, double *xbar);

@@ -226,10 +226,6 @@ extern "C" int sfgpu_jvp_host(sfgpu_system *s, const double *x, const double *v,
 // ---------------------------------------------------------------------------
 namespace {
 
-__global__ void k_axpy(size_t n, double a, const double *__restrict__ x, double *__restrict__ y) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        y[i] += a * x[i];
-}
 __global__ void k_scale_copy(size_t n, double a, const double *__restrict__ x, double *__restrict__ y) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         y[i] = a * x[i];

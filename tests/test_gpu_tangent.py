@@ -123,7 +123,7 @@ def test_newton_krylov_agrees_with_pure_diis_on_sweep(gpu_lib):
         xd, rc, _, _ = o.solve_diis(x0, tol=1e-10, maxit=3000, m=5, eta=0.1)
         if rc != 0:
             continue
-        r = System(spec).solve_nk(x0, tol=1e-10, maxit=60, krylov=40)
+        r = System(spec).solve_nk(x0, tol=1e-10, maxit=120, krylov=40)
         assert r.converged, (i, r.status, r.error, r.iterations)
         assert np.linalg.norm(o.residual(r.x)) < 1e-8, i
         phi_nk = [o.phi(k).copy() for k in range(len(spec.segments))]
