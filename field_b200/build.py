@@ -5,6 +5,7 @@ propagator arithmetic rounds like SFbox's separate multiply/add CPU loops.
 """
 from __future__ import annotations
 
+import glob
 import os
 import subprocess
 import sys
@@ -29,6 +30,7 @@ def needs_build() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = _sources() + [os.path.join(CSRC, h) for h in HEADERS]
+    deps += glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
     return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
 
 

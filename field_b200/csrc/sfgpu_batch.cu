@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(1024) batch_diis_kernel(const InstDesc *__rest
             XX0[r] = v - xi;
             acc += g[r] * g[r];
         }
-        block_sums(&acc, 1, sh);
+        block_sum1(acc, sh);
         double err = sqrt(sh.val[0]);
         int k = 0, it = 0, kd = 1, st = ST_CONVERGED;
         if (threadIdx.x == 0)
@@ -91,19 +91,26 @@ __global__ void __launch_bounds__(1024) batch_diis_kernel(const InstDesc *__rest
             double *xr = XR + (size_t)k * iv, *xx = XX0 + (size_t)k * iv;
             // x -= eta*g; XR[k] = x; XX0[k] = x - x0; Gram row and |g|^2 in one pass
             double part[kMaxHist + 1];
-            for (int i = 0; i <= kd; i++) part[i] = 0;
+            int slot[kMaxHist + 1];
+#pragma unroll
+            for (int i = 0; i <= kMaxHist; i++) {
+                part[i] = 0;
+                slot[i] = (i < kd) ? i : (i == kMaxHist ? kd : -1);
+            }
             for (long long r = threadIdx.x; r < iv; r += blockDim.x) {
-                double v = x[r] - g[r] * eta;
-                double d = v - x0[r];
+                const double v = x[r] - g[r] * eta;
+                const double d = v - x0[r];
                 x[r] = v; xr[r] = v; xx[r] = d;
-                part[kd] += g[r] * g[r];
-                for (int i = 0; i < kd; i++) {
+                part[kMaxHist] += g[r] * g[r];
+#pragma unroll
+                for (int i = 0; i < kMaxHist; i++) {
+                    if (i >= kd) continue;
                     int posi = k - kd + 1 + i;
                     if (posi < 0) posi += m;
                     part[i] += XX0[(size_t)posi * iv + r] * d;
                 }
             }
-            block_sums(part, kd + 1, sh);
+            block_sums_slots<kMaxHist + 1>(part, slot, sh);
             if (threadIdx.x == 0) {
                 // shift out the oldest row/column when the memory is full
                 // (sfnewton.cpp:624-628), then write the new row
@@ -112,17 +119,21 @@ __global__ void __launch_bounds__(1024) batch_diis_kernel(const InstDesc *__rest
                         for (int j = 1; j < m; j++) sh.gram[m * (i - 1) + j - 1] = sh.gram[m * i + j];
                 }
                 for (int i = 0; i < kd; i++) sh.gram[i + m * (kd - 1)] = sh.gram[kd - 1 + m * i] = sh.val[i];
-                double A[kMaxHist * kMaxHist], c[kMaxHist];
-                for (int i = 0; i < kd; i++)
-                    for (int j = 0; j < kd; j++) A[j + kd * i] = sh.gram[j + m * i];
-                diis_coeff_thread(kd, A, c);
-                double nc = 0;
-                for (int i = 0; i < kd; i++) nc += c[i];
-                for (int i = 0; i < kd; i++) {
-                    sh.coef[i] = c[i] / nc;
-                    int posi = k - kd + 1 + i;
-                    if (posi < 0) posi += m;
-                    sh.pos[i] = posi;
+            }
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                for (int e = threadIdx.x; e < kd * kd; e += 32) sh.A[e] = sh.gram[(e % kd) + m * (e / kd)];
+                __syncwarp();
+                diis_coeff_warp(kd, sh.A, sh.Q, sh.coef);
+                if (threadIdx.x == 0) {
+                    double nc = 0;
+                    for (int i = 0; i < kd; i++) nc += sh.coef[i];
+                    for (int i = 0; i < kd; i++) {
+                        sh.coef[i] = sh.coef[i] / nc;
+                        int posi = k - kd + 1 + i;
+                        if (posi < 0) posi += m;
+                        sh.pos[i] = posi;
+                    }
                 }
             }
             __syncthreads();
@@ -164,6 +175,7 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
         sfgpu_system *s = new sfgpu_system();
         s->stream = b->stream;
         rc = s->setup(&descs[i]);
+        if (!rc && (s->nseg > kResMax || s->nclass > kResMax)) rc = SFGPU_ERR_UNSUPPORTED;   // site_residual registers
         if (rc) { delete s; break; }
         b->sys.push_back(s);
         b->offset[i] = b->total;

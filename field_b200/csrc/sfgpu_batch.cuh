@@ -47,19 +47,27 @@ struct BlockShared {
     sfk::MolScal scal[kMaxMol];
     double phib[SFGPU_MAX_SEG], chib[SFGPU_MAX_SEG];
     double gram[kMaxHist * kMaxHist];
+    double A[kMaxHist * kMaxHist], Q[kMaxHist * kMaxHist];   // DIIS eigen-solve work
     double coef[kMaxHist];
     int pos[kMaxHist];
     int inst;
 };
 
-// Sum of nv per-thread values over the block in a fixed order
-// (warp shuffle tree, then warps in index order); result in sh.val[0..nv).
-__device__ inline void block_sums(const double *v, int nv, BlockShared &sh) {
+// Sum of per-thread values over the block in a fixed order (warp shuffle
+// tree, then warps in index order): sh.val[slot[i]] = block sum of v[i] for
+// every i < NMAX with slot[i] >= 0.  v is a register array, indexed only
+// with compile-time constants so that it never goes to local memory.
+template <int NMAX>
+__device__ __forceinline__ void block_sums_slots(const double (&v)[NMAX], const int (&slot)[NMAX], BlockShared &sh) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-    for (int i = 0; i < nv; i++) {
+    int nv = 0;
+#pragma unroll
+    for (int i = 0; i < NMAX; i++) {
+        if (slot[i] < 0) continue;
         double a = v[i];
         for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-        if (lane == 0) sh.red[i * 32 + warp] = a;
+        if (lane == 0) sh.red[slot[i] * 32 + warp] = a;
+        nv = max(nv, slot[i] + 1);
     }
     __syncthreads();
     if (threadIdx.x < nv) {
@@ -68,6 +76,12 @@ __device__ inline void block_sums(const double *v, int nv, BlockShared &sh) {
         sh.val[threadIdx.x] = a;
     }
     __syncthreads();
+}
+// one value per thread: sh.val[0]
+__device__ __forceinline__ void block_sum1(double v, BlockShared &sh) {
+    const double a[1] = {v};
+    const int sl[1] = {0};
+    block_sums_slots<1>(a, sl, sh);
 }
 
 __device__ inline void mol_scalars_block(const InstDesc &I, int m, double wsum, BlockShared &sh) {
@@ -107,7 +121,7 @@ __device__ inline void finish_molecule(const InstDesc &I, int m, const double *c
         double w = I.w_gn[r];
         if (w != 0) acc += w * cur[r];
     }
-    block_sums(&acc, 1, sh);
+    block_sum1(acc, sh);
     if (threadIdx.x == 0) mol_scalars_block(I, m, sh.val[0], sh);
     __syncthreads();
     const double norm = sh.scal[m].norm;
@@ -243,6 +257,56 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
     finish_molecule(I, m, cur, sh);
 }
 
+// f at iteration site j (lattice site z) of SF_Solve::GetResiduals
+// (SF_Solve.cpp:527-591) once phi and the bulk terms (sh.chib) are known.
+// Segment types and classes are bounded by kResMax so that the per-site
+// contact averages and potentials stay in registers; the sums run in the
+// same order as the single-system kernel.
+constexpr int kResMax = 8;
+__device__ __forceinline__ void site_residual(const InstDesc &I, const BlockShared &sh, int j, double *f) {
+    const DLat &L = I.L;
+    const int z = I.sites[j];
+    const int nseg = I.nseg, ncl = I.nclass;
+    double phit = 0;
+    double rho[kResMax];
+#pragma unroll
+    for (int i = 0; i < kResMax; i++) {
+        rho[i] = 0;
+        if (i < nseg) phit += I.phi[i][z];
+    }
+#pragma unroll
+    for (int i = 0; i < kResMax; i++) {
+        if (i >= nseg) continue;
+        bool need = false;
+        for (int c = 0; c < ncl; c++) need |= I.ct.chi[I.rep[c] * SFGPU_MAX_SEG + i] != 0;
+        if (need) rho[i] = side_fraction(L, I.phi[i], z);
+    }
+    double u[kResMax];
+    double av = 0;
+#pragma unroll
+    for (int c = 0; c < kResMax; c++) {
+        u[c] = 0;
+        if (c >= ncl) continue;
+        const int st = I.rep[c];
+        double v = -log(I.gfull[st][z]);
+        double ci = 0;
+#pragma unroll
+        for (int i = 0; i < kResMax; i++) {
+            if (i >= nseg) continue;
+            const double xx = I.ct.chi[st * SFGPU_MAX_SEG + i];
+            if (xx != 0) ci += xx * rho[i];
+        }
+        v -= ci / phit;
+        v += sh.chib[c];
+        u[c] = v;
+        av += v;
+    }
+    av /= ncl;
+#pragma unroll
+    for (int c = 0; c < kResMax; c++)
+        if (c < ncl) f[(size_t)j * ncl + c] = -1.0 + 1.0 / phit + u[c] - av;
+}
+
 // x -> f for one instance (SF_Solve::residuals, SF_Solve.cpp:647-651)
 __device__ inline void residual_block(const InstDesc &I, const double *x, double *f, BlockShared &sh) {
     const DLat &L = I.L;
@@ -298,78 +362,69 @@ __device__ inline void residual_block(const InstDesc &I, const double *x, double
         }
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < I.nsites; j += blockDim.x) {
-        int z = I.sites[j];
-        double phit = 0;
-        double rho[SFGPU_MAX_SEG];
-        for (int i = 0; i < I.nseg; i++) { phit += I.phi[i][z]; rho[i] = 0; }
-        for (int i = 0; i < I.nseg; i++) {
-            bool need = false;
-            for (int c = 0; c < I.nclass; c++) need |= I.ct.chi[I.rep[c] * SFGPU_MAX_SEG + i] != 0;
-            if (need) rho[i] = side_fraction(L, I.phi[i], z);
-        }
-        double u[SFGPU_MAX_SEG];
-        double av = 0;
-        for (int c = 0; c < I.nclass; c++) {
-            int st = I.rep[c];
-            double v = -log(I.gfull[st][z]);
-            double ci = 0;
-            for (int i = 0; i < I.nseg; i++) {
-                double xx = I.ct.chi[st * SFGPU_MAX_SEG + i];
-                if (xx != 0) ci += xx * rho[i];
-            }
-            v -= ci / phit;
-            v += sh.chib[c];
-            u[c] = v;
-            av += v;
-        }
-        av /= I.nclass;
-        for (int c = 0; c < I.nclass; c++) f[(size_t)j * I.nclass + c] = -1.0 + 1.0 / phit + u[c] - av;
-    }
+    for (int j = threadIdx.x; j < I.nsites; j += blockDim.x) site_residual(I, sh, j, f);
     __syncthreads();
 }
 
-// DIIS coefficients c = A^-1 1 by cyclic Jacobi (one thread; k <= kMaxHist)
-__device__ inline void diis_coeff_thread(int n, double *A, double *c) {
-    double Q[kMaxHist * kMaxHist], ev[kMaxHist];
-    for (int i = 0; i < n; i++) for (int j = 0; j < n; j++) Q[i * n + j] = (i == j);
+// DIIS coefficients c = A^-1 1 through the eigen-decomposition of the
+// symmetric Gram matrix by cyclic Jacobi (the oracle's jacobi_eig: same
+// rotation order, same per-element expressions), run by one warp on A and Q
+// in shared memory: lane k owns row / column k of each rotation, lane 0 takes
+// the convergence sums in the serial order, so the result is bit-identical
+// to the serial form (n <= kMaxHist <= 32).
+__device__ inline void diis_coeff_warp(int n, double *A, double *Q, double *c) {
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    for (int i = lane; i < n * n; i += 32) Q[i] = (i / n == i % n);
+    __syncwarp();
     for (int sweep = 0; sweep < 100; sweep++) {
         double off = 0, tot = 0;
-        for (int i = 0; i < n; i++)
-            for (int j = 0; j < n; j++) {
-                tot += A[i * n + j] * A[i * n + j];
-                if (i != j) off += A[i * n + j] * A[i * n + j];
-            }
+        if (lane == 0) {
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) {
+                    tot += A[i * n + j] * A[i * n + j];
+                    if (i != j) off += A[i * n + j] * A[i * n + j];
+                }
+        }
+        off = __shfl_sync(full, off, 0);
+        tot = __shfl_sync(full, tot, 0);
         if (off <= 1e-30 * tot || off == 0) break;
         for (int p = 0; p < n; p++)
             for (int q = p + 1; q < n; q++) {
-                double apq = A[p * n + q];
+                const double apq = A[p * n + q];
                 if (apq == 0) continue;
-                double theta = (A[q * n + q] - A[p * n + p]) / (2 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
-                double cs = 1 / sqrt(t * t + 1), sn = t * cs;
-                for (int k = 0; k < n; k++) {
-                    double akp = A[k * n + p], akq = A[k * n + q];
+                const double theta = (A[q * n + q] - A[p * n + p]) / (2 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1));
+                const double cs = 1 / sqrt(t * t + 1), sn = t * cs;
+                __syncwarp();
+                if (lane < n) {
+                    const int k = lane;
+                    const double akp = A[k * n + p], akq = A[k * n + q];
                     A[k * n + p] = cs * akp - sn * akq; A[k * n + q] = sn * akp + cs * akq;
-                }
-                for (int k = 0; k < n; k++) {
-                    double apk = A[p * n + k], aqk = A[q * n + k];
-                    A[p * n + k] = cs * apk - sn * aqk; A[q * n + k] = sn * apk + cs * aqk;
-                }
-                for (int k = 0; k < n; k++) {
-                    double qkp = Q[k * n + p], qkq = Q[k * n + q];
+                    const double qkp = Q[k * n + p], qkq = Q[k * n + q];
                     Q[k * n + p] = cs * qkp - sn * qkq; Q[k * n + q] = sn * qkp + cs * qkq;
                 }
+                __syncwarp();
+                if (lane < n) {
+                    const int k = lane;
+                    const double apk = A[p * n + k], aqk = A[q * n + k];
+                    A[p * n + k] = cs * apk - sn * aqk; A[q * n + k] = sn * apk + cs * aqk;
+                }
+                __syncwarp();
             }
     }
-    for (int i = 0; i < n; i++) ev[i] = A[i * n + i];
-    for (int i = 0; i < n; i++) c[i] = 0;
-    for (int k = 0; k < n; k++) {
-        double proj = 0;
-        for (int i = 0; i < n; i++) proj += Q[i * n + k];
-        double t = proj / ev[k];
-        for (int i = 0; i < n; i++) c[i] += Q[i * n + k] * t;
+    if (lane < n) {
+        const int i = lane;
+        double ci = 0;
+        for (int k = 0; k < n; k++) {
+            double proj = 0;
+            for (int j = 0; j < n; j++) proj += Q[j * n + k];
+            const double t = proj / A[k * n + k];
+            ci += Q[i * n + k] * t;
+        }
+        c[i] = ci;
     }
+    __syncwarp();
 }
 
 }  // namespace sfb
