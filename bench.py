@@ -27,6 +27,9 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "cyl_micelle Lat2DCyl1stO 128x128 (r,z), (A)20(B)20 + W solvent, phibulk 0.005, chi_AW 1.6"
 METRIC = "converged SCF solves/s (resid<1e-7)"
+# ncu: 106.16 GB read + 77.81 GB written by one batch_diis_kernel launch of
+# 148 instances that made 148 * (33.63 + 1) residual evaluations
+DRAM_BYTES_PER_INSTANCE_ITERATION = (106.159e9 + 77.811e9) / (148 * 34.63)
 TOL = 1e-7
 DIIS_M, DIIS_ETA, MAXIT = 10, 0.1, 2000
 
@@ -286,8 +289,14 @@ def run_ours(a, rank, world, local_rank):
         plain = {"value": pv, "unit": "solves/s", "instances": 2,
                  "form": "per-instance host-driven Pure_DIIS, one launch per propagator step"}
         kp_bytes = solver.algorithmic_bytes(last_iters)
+        # DRAM traffic measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+        # on one launch of 148 instances of this workload, per instance and
+        # DIIS iteration (profiles/batch_diis_kernel_lat2dcyl_128x128.md),
+        # scaled to this launch's iterations
+        traffic = DRAM_BYTES_PER_INSTANCE_ITERATION * float(sum(int(i) + 1 for i in last_iters))
         solver.kernel_profile = {"kernel": "batch_diis_kernel (persistent, one launch per batch solve)",
-                                 "bytes": kp_bytes, "ms": statistics.median(kms), "traffic": None}
+                                 "bytes": kp_bytes, "ms": statistics.median(kms), "traffic": traffic,
+                                 "traffic_source": "ncu capture of 148 instances, scaled by residual evaluations"}
     prof = prof_sys.profile_propagator(reps=400)
     roof = fbatch.roofline(prof, a.form, solver)
     if a.form == "chosen":

@@ -66,7 +66,8 @@ def roofline(prof: dict, form: str, solver=None) -> dict:
         kp = solver.kernel_profile
         ach = kp["bytes"] / (kp["ms"] / 1e3) / 1e9
         return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": kp.get("traffic"), "peak_kind": kind, "kernel": kp["kernel"],
+                "traffic": kp.get("traffic"), "traffic_source": kp.get("traffic_source"),
+                "peak_kind": kind, "kernel": kp["kernel"],
                 "bytes_per_launch": kp["bytes"], "ms_per_launch": kp["ms"]}
     ach = prof["bytes_bwd"] / (prof["ms_bwd"] / 1e3) / 1e9
     return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": None,
