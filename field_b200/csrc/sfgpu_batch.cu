@@ -21,6 +21,7 @@ struct sfgpu_batch {
     std::vector<long long> offset;      // start of each instance in the concatenated x
     long long total = 0;
     int m = 10, block = 256;
+    size_t stage_bytes = 0;         // dynamic shared memory per block (staged G)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -232,6 +233,33 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
     if (!rc) rc = balloc(b, (void **)&b->d_err, sizeof(double) * n);
     if (rc) { delete b; return rc; }
     b->block = maxM >= 4096 ? 1024 : (maxM >= 1024 ? 512 : 256);
+    // stage G in shared memory for every instance whose lattice fits next to
+    // the static descriptor and reduction space
+    {
+        int dev = 0, optin = 0;
+        cudaFuncAttributes fa;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+            cudaFuncGetAttributes(&fa, batch_diis_kernel) != cudaSuccess) {
+            delete b;
+            return SFGPU_ERR_CUDA;
+        }
+        const size_t fixed = fa.sharedSizeBytes + 1024;   // 1 KB the system reserves per block
+        const size_t room = (size_t)optin > fixed ? (size_t)optin - fixed : 0;
+        size_t need = 0;
+        for (int i = 0; i < n; i++) {
+            const size_t bytes = sizeof(double) * (size_t)b->sys[i]->M;
+            b->desc_h[i].gstage = bytes <= room ? 1 : 0;
+            if (bytes <= room) need = std::max(need, bytes);
+        }
+        if (cudaMemcpy(b->d_desc, b->desc_h.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaFuncSetAttribute(batch_diis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) !=
+                cudaSuccess) {
+            delete b;
+            return SFGPU_ERR_CUDA;
+        }
+        b->stage_bytes = need;
+    }
     *out = b;
     return SFGPU_OK;
 }
@@ -281,14 +309,14 @@ extern "C" int sfgpu_batch_solve_resident(sfgpu_batch *b, double tol, int maxit,
     SFGPU_CUDA_TRY(cudaGetDevice(&dev));
     SFGPU_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     int per_sm = 1;
-    SFGPU_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_diis_kernel, b->block, 0));
+    SFGPU_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_diis_kernel, b->block, b->stage_bytes));
     int grid = std::max(1, std::min(n, nsm * std::max(1, per_sm)));
     if (!b->ev0) {
         SFGPU_CUDA_TRY(cudaEventCreate(&b->ev0));
         SFGPU_CUDA_TRY(cudaEventCreate(&b->ev1));
     }
     SFGPU_CUDA_TRY(cudaEventRecord(b->ev0, st));
-    batch_diis_kernel<<<grid, b->block, 0, st>>>(b->d_desc, n, b->d_queue, b->m, eta, tol, maxit,
+    batch_diis_kernel<<<grid, b->block, b->stage_bytes, st>>>(b->d_desc, n, b->d_queue, b->m, eta, tol, maxit,
                                                   b->d_status, b->d_iters, b->d_err);
     SFGPU_CUDA_TRY(cudaGetLastError());
     SFGPU_CUDA_TRY(cudaEventRecord(b->ev1, st));

@@ -25,6 +25,7 @@ struct IMol {
 struct InstDesc {
     DLat L;
     int M, nseg, nmol, nclass, nsites, solvent;
+    int gstage;                     // G of the running segment staged in shared memory
     long long nvar;
     int freedom[SFGPU_MAX_SEG];
     int class_of[SFGPU_MAX_SEG];
@@ -154,11 +155,29 @@ __device__ inline void finish_molecule(const InstDesc &I, int m, const double *c
 
 // SF_Homopol1stO::Matrix1 / SF_Copol1stO::Matrix1 / SF_Monomer1stO::Matrix1
 // inside one block (first-order lattices)
+//
+// G of a run of equal segments is constant over the run's steps, so when the
+// lattice fits (I.gstage) it is copied once per run into the block's dynamic
+// shared memory and the steps read it there instead of streaming it from L2
+// in every step.
 __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared &sh) {
+    extern __shared__ double g_stage[];
     const IMol &o = I.mol[m];
     const DLat &L = I.L;
     const int M = I.M;
     if (o.type == 0) { finish_molecule(I, m, I.gseg[o.seg[0]], sh); return; }
+    int staged = -1;   // segment whose G is in g_stage (block-uniform)
+    auto gof = [&](int sg) -> const double * {
+        if (!I.gstage) return I.gseg[sg];
+        if (sg != staged) {
+            __syncthreads();
+            const double *src = I.gseg[sg];
+            for (int r = threadIdx.x; r < M; r += blockDim.x) g_stage[r] = src[r];
+            __syncthreads();
+            staged = sg;
+        }
+        return g_stage;
+    };
     for (int a = 0; a < o.nused; a++) {
         double *phi = o.phi[o.used[a]];
         for (int r = threadIdx.x; r < M; r += blockDim.x) phi[r] = 0.0;
@@ -167,7 +186,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
     double *bufA = I.ginv0, *bufB = I.ginv1;
     if (o.sym) {
         const int sg = o.seg[0];
-        const double *G = I.gseg[sg];
+        const double *G = gof(sg);
         double *phi = o.phi[sg];
         const int N = o.N, half = N / 2;
         for (int r = threadIdx.x; r < M; r += blockDim.x) gi[r] = G[r];
@@ -218,7 +237,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
     for (int t = 1; t < N; t++) {
         const double *src = gi + (size_t)(t - 1) * M;
         double *dst = gi + (size_t)t * M;
-        const double *G = I.gseg[o.seg[t]];
+        const double *G = gof(o.seg[t]);
         for_interior4(L, threadIdx.x, blockDim.x,
             [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, src, G, k, nlast); },
             [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
@@ -240,7 +259,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
     { double *t = bufA; bufA = bufB; bufB = t; }
     for (int t = N - 2; t >= 0; t--) {
         const int sg = o.seg[t];
-        const double *G = I.gseg[sg];
+        const double *G = gof(sg);
         const double *gf = gi + (size_t)t * M;
         double *phi = o.phi[sg];
         double *dst = bufA;
