@@ -136,53 +136,194 @@ __global__ void adj_swf(int nsites, SwfAdj sa, const int *__restrict__ sites, do
 
 }  // namespace
 
-int sfgpu_system::ensure_adjoint() {
-    if (a_ready) return SFGPU_OK;
-    if (K != 1) return SFGPU_ERR_UNSUPPORTED;
+// cotangent vectors and scalars of the reverse sweep (any lattice order)
+int sfgpu_system::ensure_adjoint_misc() {
     int rc;
-    size_t store = 1;
-    for (auto &o : mols) if (o.type != 0) store = std::max(store, (size_t)o.N * M);
-    if ((rc = alloc_d(&a_gf, store)) || (rc = alloc_d(&a_gb, store))) return rc;
-    SFGPU_CUDA_TRY(cudaMemset(a_gf, 0, sizeof(double) * store));
-    SFGPU_CUDA_TRY(cudaMemset(a_gb, 0, sizeof(double) * store));
-    a_phibar.assign(nseg, nullptr); a_gbar.assign(nseg, nullptr); a_phibar_raw.assign(nseg, nullptr);
-    for (int i = 0; i < nseg; i++) {
-        if ((rc = alloc_d(&a_phibar[i], M)) || (rc = alloc_d(&a_gbar[i], M)) || (rc = alloc_d(&a_phibar_raw[i], M)))
+    if (!a_misc) {
+        a_phibar.assign(nseg, nullptr); a_gbar.assign(nseg, nullptr); a_phibar_raw.assign(nseg, nullptr);
+        for (int i = 0; i < nseg; i++) {
+            if ((rc = alloc_d(&a_phibar[i], M)) || (rc = alloc_d(&a_gbar[i], M)) ||
+                (rc = alloc_d(&a_phibar_raw[i], M)))
+                return rc;
+        }
+        if ((rc = alloc_d(&a_cot[0], (size_t)K * M)) || (rc = alloc_d(&a_cot[1], (size_t)K * M))) return rc;
+        if ((rc = alloc_d(&a_scal, 4 * (size_t)nmol)) || (rc = alloc_d(&a_chibbar, SFGPU_MAX_SEG)) ||
+            (rc = alloc_d(&a_qbar, 1)))
             return rc;
+        if ((rc = alloc_d(&a_w, nvar)) ||
+            (rc = alloc_d(&a_xbar, std::max((size_t)nvar, (size_t)nseg * nseg))))
+            return rc;
+        a_misc = true;
     }
-    if ((rc = alloc_d(&a_cot[0], M)) || (rc = alloc_d(&a_cot[1], M))) return rc;
-    if ((rc = alloc_d(&a_scal, 4 * (size_t)nmol)) || (rc = alloc_d(&a_chibbar, SFGPU_MAX_SEG)) ||
-        (rc = alloc_d(&a_qbar, 1)))
-        return rc;
-    if ((rc = alloc_d(&a_w, nvar)) || (rc = alloc_d(&a_xbar, nvar))) return rc;
-    a_ready = true;
     return SFGPU_OK;
+}
+
+int sfgpu_system::ensure_adjoint() {
+    int rc = ensure_adjoint_misc();
+    if (rc) return rc;
+    if (!a_store) {
+        int nmax = 1;
+        for (auto &o : mols) if (o.type != 0) nmax = std::max(nmax, o.N);
+        size_t slices;
+        if (a_stride == 0) {
+            slices = 2 * (size_t)nmax;
+        } else {
+            const size_t nq = (size_t)(nmax + a_stride - 1) / a_stride;
+            slices = 2 * nq + 2 * (size_t)a_stride + 1;
+        }
+        const size_t KM = (size_t)K * M;
+        cudaError_t e = cudaMalloc((void **)&a_store, sizeof(double) * slices * KM);
+        if (e != cudaSuccess) {
+            a_store = nullptr;
+            sfgpu_set_error(e, "cudaMalloc (reverse-sweep chain storage)", __FILE__, __LINE__);
+            return SFGPU_ERR_NOMEM;
+        }
+        // boundary entries of the slices are read only on surface layers, where
+        // propagators are 0: start from zeros
+        SFGPU_CUDA_TRY(cudaMemset(a_store, 0, sizeof(double) * slices * KM));
+        if (a_stride == 0) {
+            a_gf = a_store;
+            a_gb = a_store + (size_t)nmax * KM;
+        } else {
+            const size_t nq = (size_t)(nmax + a_stride - 1) / a_stride;
+            a_ckF = a_store;
+            a_ckB = a_ckF + nq * KM;
+            a_bufF = a_ckB + nq * KM;
+            a_bufB = a_bufF + (size_t)a_stride * KM;   // a_stride + 1 slices: the last is the carry
+            a_gf = a_gb = nullptr;
+        }
+        a_qseg = -1;
+    }
+    return SFGPU_OK;
+}
+
+int sfgpu_system::set_checkpoint(int stride) {
+    if (stride < 0) return SFGPU_ERR_INVALID;
+    if (stride == a_stride && a_store) return SFGPU_OK;
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (a_store) SFGPU_CUDA_TRY(cudaFree(a_store));
+    a_store = nullptr;
+    a_stride = stride;
+    return SFGPU_OK;
+}
+
+// Steps of molecule o's chain on K-component slices: the start slice (G in
+// every component), forward step t (Gf(t) from Gf(t-1)), backward step t
+// (Gb(t) from Gb(t+1), composing Gb(t).Gf(t) into phi when other != nullptr).
+void sfgpu_system::adj_start(const double *G, double *dst) {
+    const int g = grid_a(M);
+    replicate<<<g, kBlock, 0, stream>>>(M, K, G, dst);
+    if (K == 6) set_boundaries<<<g, kBlock, 0, stream>>>(H.L, 6, dst);
+}
+void sfgpu_system::adj_fstep(const HMol &o, int t, const double *src, double *dst) {
+    const DLat &L = H.L;
+    const int sg = o.seg[t];
+    if (K == 1)
+        step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, nullptr, nullptr, COMP_NONE);
+    else
+        step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], dst,
+                                                          nullptr, nullptr, COMP_NONE, 0);
+}
+void sfgpu_system::adj_bstep(const HMol &o, int t, const double *src, double *dst, const double *other,
+                             double *phi) {
+    const DLat &L = H.L;
+    const int sg = o.seg[t];
+    const int mode = other ? COMP_ACC : COMP_NONE;
+    if (K == 1)
+        step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, other, phi, mode);
+    else
+        step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], dst,
+                                                          other, phi, mode, 1);
 }
 
 // Gf and Gb of every position of molecule m's chain (full chains, also for
 // symmetric homopolymers) into a_gf / a_gb; with compose, the backward sweep
-// also accumulates Gf.Gb into the molecule's (zeroed) phi
-int sfgpu_system::store_chains(int m, bool compose) {
+// also accumulates Gf.Gb into the molecule's (zeroed) phi.  *gb0 = Gb(0).
+int sfgpu_system::store_chains(int m, bool compose, const double **gb0) {
+    if (a_stride > 0) return store_chains_ck(m, compose, gb0);
     HMol &o = mols[m];
-    const DLat &L = H.L;
-    const int g = grid_a(M), gr = grid_rows_a(L);
+    const int g = grid_a(M);
     cudaStream_t s = stream;
     const int N = o.N;
-    SFGPU_CUDA_TRY(cudaMemcpyAsync(a_gf, d_gseg[o.seg[0]], sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
-    for (int t = 1; t < N; t++)
-        step1_rows<<<gr, kBlock, 0, s>>>(L, a_gf + (size_t)(t - 1) * M, d_gseg[o.seg[t]], a_gf + (size_t)t * M,
-                                         nullptr, nullptr, COMP_NONE);
-    SFGPU_CUDA_TRY(cudaMemcpyAsync(a_gb + (size_t)(N - 1) * M, d_gseg[o.seg[N - 1]], sizeof(double) * M,
-                                   cudaMemcpyDeviceToDevice, s));
+    const size_t KM = (size_t)K * M;
+    adj_start(d_gseg[o.seg[0]], a_gf);
+    for (int t = 1; t < N; t++) adj_fstep(o, t, a_gf + (size_t)(t - 1) * KM, a_gf + (size_t)t * KM);
+    adj_start(d_gseg[o.seg[N - 1]], a_gb + (size_t)(N - 1) * KM);
     if (compose)
-        connect<<<g, kBlock, 0, s>>>(M, 1, a_gb + (size_t)(N - 1) * M, a_gf + (size_t)(N - 1) * M,
+        connect<<<g, kBlock, 0, s>>>(M, K, a_gb + (size_t)(N - 1) * KM, a_gf + (size_t)(N - 1) * KM,
                                      o.d_phi[o.seg[N - 1]]);
-    for (int t = N - 2; t >= 0; t--) {
-        int sg = o.seg[t];
-        step1_rows<<<gr, kBlock, 0, s>>>(L, a_gb + (size_t)(t + 1) * M, d_gseg[sg], a_gb + (size_t)t * M,
-                                         compose ? a_gf + (size_t)t * M : nullptr, compose ? o.d_phi[sg] : nullptr,
-                                         compose ? COMP_ACC : COMP_NONE);
+    for (int t = N - 2; t >= 0; t--)
+        adj_bstep(o, t, a_gb + (size_t)(t + 1) * KM, a_gb + (size_t)t * KM, compose ? a_gf + (size_t)t * KM : nullptr,
+                  compose ? o.d_phi[o.seg[t]] : nullptr);
+    if (gb0) *gb0 = a_gb;
+    return SFGPU_OK;
+}
+
+// The same with checkpoints: Gf at the first and Gb at the last position of
+// every segment of a_stride positions, each segment's slices recomputed by
+// load_segment when a sweep needs them.  The backward sweep walks the
+// segments downwards, recomputing each segment's Gf for the composition;
+// a_bufB's last slice carries Gb from one segment to the next.
+int sfgpu_system::store_chains_ck(int m, bool compose, const double **gb0) {
+    HMol &o = mols[m];
+    const int g = grid_a(M);
+    cudaStream_t s = stream;
+    const int N = o.N, k = a_stride, nq = (N + k - 1) / k;
+    const size_t KM = (size_t)K * M, bytes = sizeof(double) * KM;
+    auto F = [&](int j) { return a_bufF + (size_t)j * KM; };
+    auto B = [&](int j) { return a_bufB + (size_t)j * KM; };
+    double *carry = B(k);
+    // forward: checkpoints at t = qk, the others in two alternating slices
+    adj_start(d_gseg[o.seg[0]], a_ckF);
+    const double *prev = a_ckF;
+    for (int t = 1; t < N; t++) {
+        double *dst = (t % k == 0) ? a_ckF + (size_t)(t / k) * KM : F(t & 1);
+        adj_fstep(o, t, prev, dst);
+        prev = dst;
     }
+    a_qseg = -1;
+    // backward, segments downwards
+    for (int q = nq - 1; q >= 0; q--) {
+        const int s0 = q * k, e = std::min(s0 + k, N) - 1;
+        if (compose) {   // Gf of this segment
+            SFGPU_CUDA_TRY(cudaMemcpyAsync(F(0), a_ckF + (size_t)q * KM, bytes, cudaMemcpyDeviceToDevice, s));
+            for (int j = 1; j <= e - s0; j++) adj_fstep(o, s0 + j, F(j - 1), F(j));
+        }
+        for (int t = e; t >= s0; t--) {
+            double *dst = B(t - s0);
+            const int sg = o.seg[t];
+            if (t == N - 1) {
+                adj_start(d_gseg[sg], dst);
+                if (compose) connect<<<g, kBlock, 0, s>>>(M, K, dst, F(t - s0), o.d_phi[sg]);
+            } else {
+                const double *src = (t == e) ? carry : B(t + 1 - s0);
+                adj_bstep(o, t, src, dst, compose ? F(t - s0) : nullptr, compose ? o.d_phi[sg] : nullptr);
+            }
+            if (t == e)
+                SFGPU_CUDA_TRY(cudaMemcpyAsync(a_ckB + (size_t)q * KM, dst, bytes, cudaMemcpyDeviceToDevice, s));
+        }
+        SFGPU_CUDA_TRY(cudaMemcpyAsync(carry, B(0), bytes, cudaMemcpyDeviceToDevice, s));
+    }
+    if (gb0) *gb0 = B(0);
+    return SFGPU_OK;
+}
+
+// Gf and Gb of segment q (positions qk .. min(qk + k, N) - 1) of molecule m
+// into a_bufF / a_bufB from its checkpoints
+int sfgpu_system::load_segment(int m, int q) {
+    if (a_stride == 0 || q == a_qseg) return SFGPU_OK;
+    HMol &o = mols[m];
+    cudaStream_t s = stream;
+    const int N = o.N, k = a_stride;
+    const int s0 = q * k, e = std::min(s0 + k, N) - 1;
+    const size_t KM = (size_t)K * M, bytes = sizeof(double) * KM;
+    auto F = [&](int j) { return a_bufF + (size_t)j * KM; };
+    auto B = [&](int j) { return a_bufB + (size_t)j * KM; };
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(F(0), a_ckF + (size_t)q * KM, bytes, cudaMemcpyDeviceToDevice, s));
+    for (int j = 1; j <= e - s0; j++) adj_fstep(o, s0 + j, F(j - 1), F(j));
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(B(e - s0), a_ckB + (size_t)q * KM, bytes, cudaMemcpyDeviceToDevice, s));
+    for (int t = e - 1; t >= s0; t--) adj_bstep(o, t, B(t + 1 - s0), B(t - s0), nullptr, nullptr);
+    a_qseg = q;
     return SFGPU_OK;
 }
 
@@ -193,21 +334,24 @@ int sfgpu_system::molecule_phi_store(int m) {
     const int g = grid_a(M);
     cudaStream_t s = stream;
     MolParam p;
-    p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = 0; p.K = 1;
+    p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = 0; p.K = K;
     p.pinned = o.pinned; p.solvent = (m == solvent); p.nmol = nmol;
     p.phibulk_in = o.phibulk; p.theta = o.theta;
     MolScal *scal = (MolScal *)d_scal;
     if (o.type == 0) {
         int i = o.seg[0];
+        MolParam p1 = p;
+        p1.K = 1;   // a monomer's end distribution is G itself
         wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, d_gseg[i], d_wgn, d_partial);
-        mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, scal, m);
+        mol_scalars<<<1, 1, 0, s>>>(p1, nblocks_red, d_partial, scal, m);
         finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], scal, m, 1);
         return SFGPU_OK;
     }
     for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_phi[i], 0, sizeof(double) * M, s));
-    int rc = store_chains(m, true);
+    const double *gb0 = nullptr;
+    int rc = store_chains(m, true, &gb0);
     if (rc) return rc;
-    wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, a_gb, d_wgn, d_partial);
+    wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, gb0, d_wgn, d_partial);
     mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, scal, m);
     for (int i : o.used) {
         finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], scal, m, 0);
@@ -241,30 +385,59 @@ int sfgpu_system::molecule_adjoint(int m) {
     if (o.type == 0) {
         // Q = sum w G enters restricted monomers: Gbar += qbar w
         adj_qbar_scale<<<1, 1, 0, s>>>(as, m, a_qbar);
-        adj_axpy_interior<<<g, kBlock, 0, s>>>(L, d_wgn, a_qbar, a_gbar[o.seg[0]]);
+        adj_axpy_interior<<<g, kBlock, 0, s>>>(L, 1, d_wgn, a_qbar, 1.0, a_gbar[o.seg[0]]);
         return SFGPU_OK;
     }
     const int N = o.N;
     double *cot = a_cot[0], *nxt = a_cot[1];
-    // descending sweep over the forward recursion
-    adj_init<<<g, kBlock, 0, s>>>(L, a_phibar_raw[o.seg[N - 1]], a_gb + (size_t)(N - 1) * M, cot);
+    // slices of position t: stored, or recomputed segment by segment
+    a_qseg = -1;
+    int rcs = SFGPU_OK;
+    auto at = [&](int t) {
+        if (a_stride == 0) return t;
+        const int q = t / a_stride;
+        if (!rcs) rcs = load_segment(m, q);
+        return t - q * a_stride;
+    };
+    const size_t KM = (size_t)K * M;
+    auto GF = [&](int j) -> const double * { return (a_stride ? a_bufF : a_gf) + (size_t)j * KM; };
+    auto GB = [&](int j) -> const double * { return (a_stride ? a_bufB : a_gb) + (size_t)j * KM; };
+    // one reverse step: gbar(seg t) += cot . A p; nxt += A^T (G_t cot)
+    auto rstep = [&](int t, const double *p, double S, int backward) {
+        const int sg = o.seg[t];
+        if (K == 1)
+            adj_chain_step<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[sg], p, a_gbar[sg], nxt);
+        else
+            adj_step2<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[sg], p, S, backward, a_gbar[sg], nxt);
+    };
+    // descending sweep over the forward recursion (step t used S(t-1, t))
+    {
+        const int j = at(N - 1);
+        adj_init<<<g, kBlock, 0, s>>>(L, K, a_phibar_raw[o.seg[N - 1]], GB(j), cot);
+    }
     for (int t = N - 1; t >= 1; t--) {
-        adj_init<<<g, kBlock, 0, s>>>(L, a_phibar_raw[o.seg[t - 1]], a_gb + (size_t)(t - 1) * M, nxt);
-        adj_chain_step<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[o.seg[t]], a_gf + (size_t)(t - 1) * M, a_gbar[o.seg[t]], nxt);
+        const int j = at(t - 1);
+        adj_init<<<g, kBlock, 0, s>>>(L, K, a_phibar_raw[o.seg[t - 1]], GB(j), nxt);
+        rstep(t, GF(j), K == 6 ? pf[o.seg[t - 1] * nseg + o.seg[t]] : 0.0, 0);
         std::swap(cot, nxt);
     }
-    adj_add_interior<<<g, kBlock, 0, s>>>(L, cot, a_gbar[o.seg[0]]);
-    // ascending sweep over the backward recursion (Q = sum w Gb(1) adds qbar * w)
-    adj_init<<<g, kBlock, 0, s>>>(L, a_phibar_raw[o.seg[0]], a_gf, cot);
+    adj_add_interior<<<g, kBlock, 0, s>>>(L, K, cot, a_gbar[o.seg[0]]);
+    // ascending sweep over the backward recursion (step t used S(t, t+1));
+    // lnGN = ln(sum w sum_k Gb_k(1) / K) adds qbar / K * w to every component
+    {
+        const int j = at(0);
+        adj_init<<<g, kBlock, 0, s>>>(L, K, a_phibar_raw[o.seg[0]], GF(j), cot);
+    }
     adj_qbar_scale<<<1, 1, 0, s>>>(as, m, a_qbar);
-    adj_axpy_interior<<<g, kBlock, 0, s>>>(L, d_wgn, a_qbar, cot);
+    adj_axpy_interior<<<g, kBlock, 0, s>>>(L, K, d_wgn, a_qbar, 1.0 / K, cot);
     for (int t = 0; t < N - 1; t++) {
-        adj_init<<<g, kBlock, 0, s>>>(L, a_phibar_raw[o.seg[t + 1]], a_gf + (size_t)(t + 1) * M, nxt);
-        adj_chain_step<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[o.seg[t]], a_gb + (size_t)(t + 1) * M, a_gbar[o.seg[t]], nxt);
+        const int j = at(t + 1);
+        adj_init<<<g, kBlock, 0, s>>>(L, K, a_phibar_raw[o.seg[t + 1]], GF(j), nxt);
+        rstep(t, GB(j), K == 6 ? pf[o.seg[t] * nseg + o.seg[t + 1]] : 0.0, 1);
         std::swap(cot, nxt);
     }
-    adj_add_interior<<<g, kBlock, 0, s>>>(L, cot, a_gbar[o.seg[N - 1]]);
-    return SFGPU_OK;
+    adj_add_interior<<<g, kBlock, 0, s>>>(L, K, cot, a_gbar[o.seg[N - 1]]);
+    return rcs;
 }
 
 int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double *xbar) {
@@ -323,7 +496,7 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
         if (mols[m].type != 0 && m != held) {
-            if ((rc = store_chains(m, false))) return rc;
+            if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }
         if ((rc = molecule_adjoint(m))) return rc;
@@ -346,6 +519,34 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
 extern "C" int sfgpu_vjp(sfgpu_system *s, const double *x_dev, const double *w_dev, double *f_dev, double *xbar_dev) {
     if (!s) return SFGPU_ERR_INVALID;
     return s->vjp_async(x_dev, w_dev, f_dev, xbar_dev);
+}
+
+extern "C" int sfgpu_vjp_chi(sfgpu_system *s, const double *x, const double *w, double *dchi) {
+    if (!s || !x || !w || !dchi) return SFGPU_ERR_INVALID;
+    int rc = s->ensure_adjoint_misc();
+    if (rc) return rc;
+    cudaStream_t st = s->stream;
+    const size_t nv = s->nvar;
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(s->d_x, x, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(s->a_w, w, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+    if ((rc = s->residual_async(s->d_x, s->d_f))) return rc;
+    const int ns = s->nseg;
+    SFGPU_CUDA_TRY(cudaMemsetAsync(s->a_xbar, 0, sizeof(double) * (size_t)ns * ns, st));
+    ResParam rp;
+    memset(&rp, 0, sizeof(rp));
+    rp.nsites = s->nsites; rp.nclass = s->nclass; rp.nseg = ns;
+    for (int c = 0; c < s->nclass; c++) rp.rep[c] = s->rep_of_class[c];
+    for (int i = 0; i < ns; i++) rp.phi[i] = s->d_phi[i];
+    adj_chi<<<grid_a(s->nsites), kBlock, 0, st>>>(s->H.L, rp, s->d_sites, s->a_w, s->d_phib, s->a_xbar);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(dchi, s->a_xbar, sizeof(double) * (size_t)ns * ns, cudaMemcpyDeviceToHost, st));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_set_checkpoint(sfgpu_system *s, int stride) {
+    if (!s) return SFGPU_ERR_INVALID;
+    return s->set_checkpoint(stride);
 }
 
 extern "C" int sfgpu_vjp_host(sfgpu_system *s, const double *x, const double *w, double *f, double *xbar) {

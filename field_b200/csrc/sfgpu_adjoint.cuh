@@ -62,34 +62,131 @@ static __global__ void adj_chain_step(DLat L, const double *__restrict__ cot, co
     });
 }
 
-// out[t] = phibar_raw[t] * q[t] on interior sites (0 elsewhere)
-static __global__ void adj_init(DLat L, const double *__restrict__ phibar_raw, const double *__restrict__ q,
+// out[k][t] = phibar_raw[t] * q[k][t] on interior sites (0 elsewhere), K components
+static __global__ void adj_init(DLat L, int K, const double *__restrict__ phibar_raw, const double *__restrict__ q,
                                 double *__restrict__ out) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < L.M; r += gridDim.x * blockDim.x) {
         int c[3];
         lat_coords(L, r, c);
-        out[r] = lat_interior(L, c) ? phibar_raw[r] * q[r] : 0.0;
+        const bool in = lat_interior(L, c);
+        for (int k = 0; k < K; k++)
+            out[(size_t)k * L.M + r] = in ? phibar_raw[r] * q[(size_t)k * L.M + r] : 0.0;
     }
 }
 
-// gbar[t] += cot[t] on interior sites (slice 1 / slice N equal G itself)
-static __global__ void adj_add_interior(DLat L, const double *__restrict__ cot, double *__restrict__ gbar) {
+// gbar[t] += sum_k cot[k][t] on interior sites (slice 1 / slice N hold G in
+// every component)
+static __global__ void adj_add_interior(DLat L, int K, const double *__restrict__ cot, double *__restrict__ gbar) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < L.M; r += gridDim.x * blockDim.x) {
         int c[3];
         lat_coords(L, r, c);
-        if (lat_interior(L, c)) gbar[r] += cot[r];
+        if (!lat_interior(L, c)) continue;
+        double a = 0;
+        for (int k = 0; k < K; k++) a += cot[(size_t)k * L.M + r];
+        gbar[r] += a;
     }
 }
 
-// out[t] += s * w[t] (interior)
-static __global__ void adj_axpy_interior(DLat L, const double *__restrict__ w, const double *__restrict__ sptr,
-                                         double *__restrict__ out) {
-    const double s = *sptr;
+// out[k][t] += s * w[t] (interior, every component); s = *sptr * scale
+static __global__ void adj_axpy_interior(DLat L, int K, const double *__restrict__ w,
+                                         const double *__restrict__ sptr, double scale, double *__restrict__ out) {
+    const double s = *sptr * scale;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < L.M; r += gridDim.x * blockDim.x) {
         int c[3];
         lat_coords(L, r, c);
-        if (lat_interior(L, c)) out[r] += s * w[r];
+        if (!lat_interior(L, c)) continue;
+        for (int k = 0; k < K; k++) out[(size_t)k * L.M + r] += s * w[r];
     }
+}
+
+// One reverse second-order step (the transpose of step2_rows): with
+// new = G * A(S) p, gbar[t] += sum_k cot[k][t] * (A(S) p)[k][t] and
+// out += A(S)^T (G * cot), scattered with FP64 atomics to the (mapped,
+// component-swapped) sources each output component read.
+static __global__ void adj_step2(DLat L, const double *__restrict__ cot, const double *__restrict__ G,
+                                 const double *__restrict__ p, double S, int backward, double *__restrict__ gbar,
+                                 double *__restrict__ out) {
+    const int M = L.M;
+    const double Lw = (1.0 - S) / 4.0;
+    const int nx = L.Md[0] - 2, ny = L.Md[1] - 2;
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const int t = R.base + k;
+        double c[6];
+        bool any = false;
+#pragma unroll
+        for (int kk = 0; kk < 6; kk++) {
+            c[kk] = cot[(size_t)kk * M + t];
+            any |= c[kk] != 0.0;
+        }
+        if (!any) return;
+        const int zm = (k == 1) ? L.map_lo[2] : k - 1;
+        const int zp = (k == nlast) ? L.map_hi[2] : k + 1;
+        const int off[6] = {R.up, R.dn, R.up2, R.dn2, zm - k, zp - k};
+        const bool sw[6] = {R.x == 1 && is_mirror(L.bc_lo[0]), R.x == nx && is_mirror(L.bc_hi[0]),
+                            R.y == 1 && is_mirror(L.bc_lo[1]), R.y == ny && is_mirror(L.bc_hi[1]),
+                            k == 1 && is_mirror(L.bc_lo[2]), k == nlast && is_mirror(L.bc_hi[2])};
+        const double g = G[t];
+        double raw[6];
+        if (!backward) {
+            const int dir_of[6] = {0, 2, 4, 5, 3, 1};
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++) {
+                const int dd = dir_of[kk];
+                const int src = t + off[dd];
+                const int axis = dd >> 1;
+                const bool s = sw[dd];
+                const double y = g * c[kk];
+                double acc = 0;
+#pragma unroll
+                for (int kp = 0; kp < 6; kp++) {
+                    if (kp == 5 - kk) continue;
+                    int cc = kp;
+                    if (s) {
+                        if (axis == 0 && (kp == 0 || kp == 5)) cc = 5 - kp;
+                        if (axis == 1 && (kp == 1 || kp == 4)) cc = 5 - kp;
+                        if (axis == 2 && (kp == 2 || kp == 3)) cc = 5 - kp;
+                    }
+                    const double wgt = (kp == kk) ? S : Lw;
+                    acc += p[(size_t)cc * M + src] * wgt;
+                    if (y != 0.0) atomicAdd(out + (size_t)cc * M + src, y * wgt);
+                }
+                raw[kk] = acc;
+            }
+        } else {
+            const int dir_of[6] = {1, 3, 5, 4, 2, 0};
+            double v[6], vbar[6];
+            size_t at[6];
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++) {
+                const int dd = dir_of[kk];
+                const int cc = sw[dd] ? 5 - kk : kk;
+                at[kk] = (size_t)cc * M + t + off[dd];
+                v[kk] = p[at[kk]];
+                vbar[kk] = 0.0;
+            }
+#pragma unroll
+            for (int kq = 0; kq < 6; kq++) {
+                const double y = g * c[kq];
+                double acc = 0;
+#pragma unroll
+                for (int kp = 0; kp < 6; kp++) {
+                    if (kp == 5 - kq) continue;
+                    const double wgt = (kp == kq) ? S : Lw;
+                    acc += v[kp] * wgt;
+                    vbar[kp] += y * wgt;
+                }
+                raw[kq] = acc;
+            }
+#pragma unroll
+            for (int kp = 0; kp < 6; kp++)
+                if (vbar[kp] != 0.0) atomicAdd(out + at[kp], vbar[kp]);
+        }
+        double gb = 0;
+#pragma unroll
+        for (int kk = 0; kk < 6; kk++) gb += c[kk] * raw[kk];
+        gbar[t] += gb;
+    });
 }
 
 // residual adjoint: x-direct terms, phi-state cotangents (with the
@@ -170,6 +267,29 @@ static __global__ void adj_residual(DLat L, ResParam rp, ChiTable ct, const int 
         for (int i = 0; i < rp.nseg; i++) {
             atomicAdd(ap.phibar[i] + z, phitbar);
             if (rhobar[i] != 0) side_scatter(L, z, rhobar[i], ap.phibar[i]);
+        }
+    }
+}
+
+// d(w . f)/d chi at fixed x: chi enters f only through the contact averages
+// and the bulk terms of u' (SF_Solve.cpp:527-591), so for class c with
+// representative state a = rep(c), d f_c' / d chi(a, i) = (delta_cc' - 1/n_class)
+// (phib_i - <phi_i>/phi_T).  dchi[a * nseg + i] accumulates over sites.
+static __global__ void adj_chi(DLat L, ResParam rp, const int *__restrict__ sites, const double *__restrict__ w,
+                               const double *__restrict__ phib, double *__restrict__ dchi) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < rp.nsites; j += gridDim.x * blockDim.x) {
+        const int z = sites[j];
+        double phit = 0;
+        for (int i = 0; i < rp.nseg; i++) phit += rp.phi[i][z];
+        double mean = 0;
+        for (int c = 0; c < rp.nclass; c++) mean += w[(size_t)j * rp.nclass + c];
+        mean /= rp.nclass;
+        for (int i = 0; i < rp.nseg; i++) {
+            const double term = phib[i] - side_fraction(L, rp.phi[i], z) / phit;
+            for (int c = 0; c < rp.nclass; c++) {
+                const double ub = w[(size_t)j * rp.nclass + c] - mean;
+                atomicAdd(dchi + rp.rep[c] * rp.nseg + i, ub * term);
+            }
         }
     }
 }

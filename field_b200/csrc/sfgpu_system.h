@@ -49,10 +49,24 @@ struct sfgpu_system {
     // reverse-mode (adjoint) buffers, allocated on the first J^T w
     bool a_ready = false;
     double *a_gf = nullptr, *a_gb = nullptr, *a_cot[2] = {nullptr, nullptr};
+    // chain storage of the reverse sweep: every slice (a_stride 0) or
+    // checkpoints every a_stride positions plus two segment buffers
+    int a_stride = 0;
+    bool a_misc = false;
+    double *a_store = nullptr;
+    double *a_ckF = nullptr, *a_ckB = nullptr, *a_bufF = nullptr, *a_bufB = nullptr;
+    int a_qseg = -1;                        // segment held in a_bufF / a_bufB
     std::vector<double *> a_phibar, a_gbar, a_phibar_raw;
     double *a_scal = nullptr, *a_chibbar = nullptr, *a_qbar = nullptr, *a_w = nullptr, *a_xbar = nullptr;
     int ensure_adjoint();
-    int store_chains(int m, bool compose);
+    int ensure_adjoint_misc();
+    int store_chains(int m, bool compose, const double **gb0);
+    int store_chains_ck(int m, bool compose, const double **gb0);
+    int load_segment(int m, int q);
+    void adj_start(const double *G, double *dst);
+    void adj_fstep(const HMol &o, int t, const double *src, double *dst);
+    void adj_bstep(const HMol &o, int t, const double *src, double *dst, const double *other, double *phi);
+    int set_checkpoint(int stride);
     int molecule_phi_store(int m);
     int molecule_adjoint(int m);
     int vjp_async(const double *x, const double *w, double *f, double *xbar);

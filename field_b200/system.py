@@ -133,6 +133,20 @@ class System:
         nat.check(self.lib.sfgpu_vjp_host(self.h, _d(x), _d(w), _d(f), _d(xb)), "sfgpu_vjp_host")
         return f, xb
 
+    def vjp_chi(self, x, w) -> np.ndarray:
+        """d (w . f(x)) / d chi at fixed x, as an nseg x nseg array (sfgpu_vjp_chi)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        ns = len(self.spec.segments)
+        out = np.zeros(ns * ns)
+        nat.check(self.lib.sfgpu_vjp_chi(self.h, _d(x), _d(w), _d(out)), "sfgpu_vjp_chi")
+        return out.reshape(ns, ns)
+
+    def set_checkpoint(self, stride: int):
+        """Reverse-sweep memory: 0 stores every slice, k > 0 keeps checkpoints
+        every k positions and recomputes segments (sfgpu_system_set_checkpoint)."""
+        nat.check(self.lib.sfgpu_system_set_checkpoint(self.h, int(stride)), "sfgpu_system_set_checkpoint")
+
     def solve_lbfgs(self, x0=None, tol=1e-7, maxit=2000, m=10) -> SolveResult:
         """L-BFGS on |f|^2/2 with the adjoint gradient (sfgpu_solve_lbfgs)."""
         x = np.zeros(self.nvar) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()

@@ -206,12 +206,31 @@ int sfgpu_solve_nk(sfgpu_system *sys, double *x, double tol, int maxit, int kryl
  * cotangents flow from GetResiduals through the contact averages, the
  * normalisations (lnGN, restricted and solvent phibulk), CorrectDoubleCountG
  * and the two propagator recursions (adjoint propagators run against their
- * primal direction over stored Gf and Gb) to UpdateSWF.  First-order
- * lattices (SFGPU_ERR_UNSUPPORTED for second order).  The first call
- * allocates 2*N*M doubles for the stored propagators.  SFbox has no
- * counterpart: its L-BFGS and truncated Newton use finite differences. */
+ * primal direction over stored Gf and Gb) to UpdateSWF.  First- and
+ * second-order lattices (second order: the transposed six-direction step,
+ * with the component swaps at mirrors, scattered by FP64 atomics).  The
+ * first call allocates 2*N*K*M doubles for the stored propagators (K = 1 or
+ * 6; see sfgpu_system_set_checkpoint for less).  SFbox has no counterpart:
+ * its L-BFGS and truncated Newton use finite differences. */
 int sfgpu_vjp(sfgpu_system *sys, const double *x_dev, const double *w_dev, double *f_dev, double *xbar_dev);
 int sfgpu_vjp_host(sfgpu_system *sys, const double *x, const double *w, double *f, double *xbar);
+/* Memory of the reverse sweep: stride 0 (default) stores every forward and
+ * backward slice of the longest chain (2 N M doubles); stride k > 0 stores
+ * the slices at every k-th position (checkpoints) and recomputes the k
+ * slices of one segment at a time when the sweep reaches it, in
+ * (2 ceil(N/k) + 2k + 1) M doubles -- k near sqrt(N) is smallest -- for
+ * about 1.75x the propagation work.  Results are identical for every
+ * stride (the recomputed slices are computed by the same kernels).  The
+ * storage is reallocated at the next sfgpu_vjp. */
+int sfgpu_system_set_checkpoint(sfgpu_system *sys, int stride);
+/* Sensitivity of the residual to the Flory-Huggins parameters at fixed x
+ * (first and second order): dchi[a * nseg + i] = d (w . f(x)) / d chi(a, i)
+ * over the entries the residual reads (a = the representative state of a
+ * class, SF_Solve.cpp:563-564), 0 elsewhere.  x, w: nvar host values; dchi:
+ * nseg * nseg host values.  For a symmetric change of chi(a,b) = chi(b,a)
+ * add dchi[a][b] + dchi[b][a].  With the adjoint solution w of J^T w = dL/dx
+ * at a converged x, dL/dchi = -(that sum).  No counterpart in SFbox. */
+int sfgpu_vjp_chi(sfgpu_system *sys, const double *x, const double *w, double *dchi);
 /* L-BFGS (Nocedal 1980 two-loop recursion, m pairs, Armijo backtracking) on
  * |f(x)|^2 / 2 with the exact gradient J^T f from the adjoint sweep; SFbox's
  * LBFGS method (SFNewton::L_BFGS, sfnewton.cpp:1770-1807) iterates on the
