@@ -29,6 +29,7 @@ struct AdjScal {
     double phibbar;     // cotangent of phibulk (accumulated from bulk terms and the solvent)
     double lngnbar;     // cotangent of lnGN
     double qbar;        // cotangent of Q = exp(lnGN)
+    double lncbar;      // cotangent of ln C (free energy)
 };
 
 __global__ void adj_bulk(BulkParam b, ChiTable ct, const double *__restrict__ chibbar, AdjScal *__restrict__ as) {
@@ -46,7 +47,7 @@ __global__ void adj_bulk(BulkParam b, ChiTable ct, const double *__restrict__ ch
         double v = 0;
         for (int j = 0; j < b.nseg; j++) v += phibbar_seg[j] * b.frac[j * SFGPU_MAX_SEG + m];
         as[m].phibbar = v;
-        as[m].cbar = as[m].lngnbar = as[m].qbar = 0;
+        as[m].cbar = as[m].lngnbar = as[m].qbar = as[m].lncbar = 0;
     }
 }
 
@@ -79,9 +80,10 @@ __global__ void adj_mol_scalar(MolParam p, int nparts, const double *__restrict_
     if (p.freedom == SFGPU_MOL_RESTRICTED) {
         lngnbar += -a.cbar * s.norm;                                   // C = c0 exp(-lnGN)
         if (!p.pinned) lngnbar += -a.phibbar * (p.theta / exp(s.lngn));  // phibulk = theta exp(-lnGN)
+        lngnbar += -a.lncbar;                                          // ln C = ln(theta [/N]) - lnGN
     } else if (p.solvent) {
         double phib = s.phibulk;
-        double pbar = a.phibbar + ((phib != 0) ? a.cbar * s.norm / phib : 0.0);
+        double pbar = a.phibbar + ((phib != 0) ? (a.cbar * s.norm + a.lncbar) / phib : 0.0);  // ln C = ln(phib [/N])
         for (int m = 0; m < p.nmol; m++)
             if (m != self) as[m].phibbar -= pbar;                       // phib_solv = 1 - sum others
     }
@@ -109,6 +111,20 @@ __global__ void adj_phi_cd(DLat L, const double *__restrict__ phibar, const doub
             phibar_raw[r] = 0;
         }
     }
+}
+
+// free-energy scalars: zero every molecule's cotangents, then
+// lncbar of molecule m = invN sum_z wf p_m (block partials of its profiles)
+__global__ void fe_zero_scal(int nmol, AdjScal *__restrict__ as) {
+    if (threadIdx.x == 0 && blockIdx.x == 0)
+        for (int m = 0; m < nmol; m++) as[m].cbar = as[m].phibbar = as[m].lngnbar = as[m].qbar = as[m].lncbar = 0;
+}
+__global__ void fe_set_lncbar(int nparts, const double *__restrict__ partial, double invN, AdjScal *__restrict__ as,
+                              int mol) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double v = 0;
+    for (int b = 0; b < nparts; b++) v += partial[b];
+    as[mol].lncbar = invN * v;
 }
 
 __global__ void adj_qbar_scale(const AdjScal *__restrict__ as, int mol, double *__restrict__ out) {
@@ -147,7 +163,7 @@ int sfgpu_system::ensure_adjoint_misc() {
                 return rc;
         }
         if ((rc = alloc_d(&a_cot[0], (size_t)K * M)) || (rc = alloc_d(&a_cot[1], (size_t)K * M))) return rc;
-        if ((rc = alloc_d(&a_scal, 4 * (size_t)nmol)) || (rc = alloc_d(&a_chibbar, SFGPU_MAX_SEG)) ||
+        if ((rc = alloc_d(&a_scal, sizeof(AdjScal) / sizeof(double) * (size_t)nmol)) || (rc = alloc_d(&a_chibbar, SFGPU_MAX_SEG)) ||
             (rc = alloc_d(&a_qbar, 1)))
             return rc;
         if ((rc = alloc_d(&a_w, nvar)) ||
@@ -198,7 +214,12 @@ int sfgpu_system::ensure_adjoint() {
 }
 
 int sfgpu_system::set_checkpoint(int stride) {
-    if (stride < 0) return SFGPU_ERR_INVALID;
+    if (stride < -1) return SFGPU_ERR_INVALID;
+    if (stride == -1) {   // the memory-optimal stride for the longest chain
+        int nmax = 1;
+        for (auto &o : mols) if (o.type != 0) nmax = std::max(nmax, o.N);
+        stride = std::max(1, (int)std::ceil(std::sqrt((double)nmax)));
+    }
     if (stride == a_stride && a_store) return SFGPU_OK;
     SFGPU_CUDA_TRY(cudaStreamSynchronize(stream));
     if (a_store) SFGPU_CUDA_TRY(cudaFree(a_store));
@@ -361,7 +382,7 @@ int sfgpu_system::molecule_phi_store(int m) {
 }
 
 // reverse sweep of one molecule; state phi cotangents in a_phibar
-int sfgpu_system::molecule_adjoint(int m) {
+int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_a(M), gr = grid_rows_a(L);
@@ -376,11 +397,11 @@ int sfgpu_system::molecule_adjoint(int m) {
     const int np = nblocks_red;
     for (size_t a = 0; a < o.used.size(); a++) {
         int i = o.used[a];
-        adj_dot_partial<<<np, kBlock, 0, s>>>(M, a_phibar[i], o.d_phi[i], d_partial + a * np);
+        adj_dot_partial<<<np, kBlock, 0, s>>>(M, phibar_src[i], o.d_phi[i], d_partial + a * np);
     }
     adj_mol_scalar<<<1, 1, 0, s>>>(p, np * (int)o.used.size(), d_partial, scal, as, m);
     for (int i : o.used)
-        adj_phi_cd<<<g, kBlock, 0, s>>>(L, a_phibar[i], o.d_phi[i], d_gseg[i], scal, m, o.type == 0,
+        adj_phi_cd<<<g, kBlock, 0, s>>>(L, phibar_src[i], o.d_phi[i], d_gseg[i], scal, m, o.type == 0,
                                          a_phibar_raw[i], a_gbar[i]);
     if (o.type == 0) {
         // Q = sum w G enters restricted monomers: Gbar += qbar w
@@ -440,13 +461,14 @@ int sfgpu_system::molecule_adjoint(int m) {
     return rcs;
 }
 
-int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double *xbar) {
-    int rc = ensure_adjoint();
-    if (rc) return rc;
+// primal residual evaluation that keeps what the reverse sweep reads:
+// G of every state, every molecule's profiles and scalars, the state phi,
+// the bulk terms, and the chains of the last polymer propagated
+int sfgpu_system::primal_store(const double *x, double *f) {
+    int rc;
     const DLat &L = H.L;
     const int g = grid_a(M);
     cudaStream_t s = stream;
-    // primal with stored propagators
     for (int i = 0; i < nseg; i++) {
         if (freedom[i] == SFGPU_SEG_FROZEN) continue;
         swf_update<<<g, kBlock, 0, s>>>(L, x, d_jmap, nclass, class_of[i], d_range[i],
@@ -471,6 +493,20 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
     for (int c = 0; c < nclass; c++) { rp.rep[c] = rep_of_class[c]; rp.gfull[c] = d_gfull[rep_of_class[c]]; }
     for (int i = 0; i < nseg; i++) rp.phi[i] = d_phi[i];
     residual<<<grid_a(nsites), kBlock, 0, s>>>(L, rp, ct, d_sites, d_chib, f);
+    return SFGPU_OK;
+}
+
+int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double *xbar) {
+    int rc = ensure_adjoint();
+    if (rc) return rc;
+    const DLat &L = H.L;
+    cudaStream_t s = stream;
+    if ((rc = primal_store(x, f))) return rc;
+    ResParam rp;
+    memset(&rp, 0, sizeof(rp));
+    rp.nsites = nsites; rp.nclass = nclass; rp.nseg = nseg;
+    for (int c = 0; c < nclass; c++) { rp.rep[c] = rep_of_class[c]; rp.gfull[c] = d_gfull[rep_of_class[c]]; }
+    for (int i = 0; i < nseg; i++) rp.phi[i] = d_phi[i];
     if (!w) w = f;   // gradient of |f|^2 / 2
     // reverse
     for (int i = 0; i < nseg; i++) {
@@ -492,14 +528,14 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
             if (m != solvent && mols[m].type != 0) held = m;
-    if ((rc = molecule_adjoint(solvent))) return rc;
+    if ((rc = molecule_adjoint(solvent, a_phibar.data()))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
         if (mols[m].type != 0 && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }
-        if ((rc = molecule_adjoint(m))) return rc;
+        if ((rc = molecule_adjoint(m, a_phibar.data()))) return rc;
     }
     SwfAdj sa;
     memset(&sa, 0, sizeof(sa));
@@ -513,6 +549,88 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
     }
     adj_swf<<<grid_a(nsites), kBlock, 0, s>>>(nsites, sa, d_sites, xbar);
     SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+// F(x) and dF/dx by the reverse sweep: the free energy's direct
+// cotangents (fe_contact_adj, fe_mol_phibar, fe_gbar, lncbar) feed the same
+// molecule and SWF adjoints as the residual's.  x, xbar on the device.
+int sfgpu_system::free_energy_grad(const double *x, double *F, double *xbar) {
+    int rc = ensure_adjoint();
+    if (rc) return rc;
+    if (a_phibar_m.empty()) {
+        a_phibar_m.assign(nseg, nullptr);
+        for (int i = 0; i < nseg; i++)
+            if ((rc = alloc_d(&a_phibar_m[i], M))) return rc;
+    }
+    const DLat &L = H.L;
+    const int g = grid_a(M), np = nblocks_red;
+    cudaStream_t s = stream;
+    if ((rc = primal_store(x, d_f))) return rc;
+    if ((rc = free_energy(F))) return rc;
+    for (int i = 0; i < nseg; i++) {
+        SFGPU_CUDA_TRY(cudaMemsetAsync(a_phibar[i], 0, sizeof(double) * M, s));
+        SFGPU_CUDA_TRY(cudaMemsetAsync(a_gbar[i], 0, sizeof(double) * M, s));
+    }
+    FeAdjParam fp;
+    memset(&fp, 0, sizeof(fp));
+    fp.nseg = nseg;
+    for (int i = 0; i < nseg; i++) { fp.phi[i] = d_phi[i]; fp.phibar[i] = a_phibar[i]; }
+    fe_contact_adj<<<g, kBlock, 0, s>>>(L, fp, ct, d_wf);
+    AdjScal *as = (AdjScal *)a_scal;
+    const MolScal *scal = (const MolScal *)d_scal;
+    fe_zero_scal<<<1, 1, 0, s>>>(nmol, as);
+    for (int m = 0; m < nmol; m++) {
+        HMol &o = mols[m];
+        for (size_t a = 0; a < o.used.size(); a++)
+            adj_dot_partial<<<np, kBlock, 0, s>>>(M, d_wf, o.d_phi[o.used[a]], d_partial + a * np);
+        fe_set_lncbar<<<1, 1, 0, s>>>(np * (int)o.used.size(), d_partial, 1.0 / o.N, as, m);
+        for (int i : o.used) fe_gbar<<<g, kBlock, 0, s>>>(M, o.d_phi[i], d_wf, d_gseg[i], a_gbar[i]);
+    }
+    auto mol_adj = [&](int m) -> int {
+        HMol &o = mols[m];
+        for (int i : o.used)
+            fe_mol_phibar<<<g, kBlock, 0, s>>>(M, a_phibar[i], d_wf, d_gseg[i], 1.0 / o.N, log((double)o.N),
+                                               o.chemintref, scal, m, a_phibar_m[i]);
+        return molecule_adjoint(m, a_phibar_m.data());
+    };
+    int held = (mols[solvent].type != 0) ? solvent : -1;
+    if (held < 0)
+        for (int m = nmol - 1; m >= 0 && held < 0; m--)
+            if (m != solvent && mols[m].type != 0) held = m;
+    if ((rc = mol_adj(solvent))) return rc;
+    for (int m = nmol - 1; m >= 0; m--) {
+        if (m == solvent) continue;
+        if (mols[m].type != 0 && m != held) {
+            if ((rc = store_chains(m, false, nullptr))) return rc;
+            held = m;
+        }
+        if ((rc = mol_adj(m))) return rc;
+    }
+    SFGPU_CUDA_TRY(cudaMemsetAsync(xbar, 0, sizeof(double) * nvar, s));
+    SwfAdj sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.nseg = nseg; sa.nclass = nclass;
+    for (int i = 0; i < nseg; i++) {
+        sa.cls[i] = class_of[i];
+        sa.pinned[i] = freedom[i] == SFGPU_SEG_PINNED;
+        sa.gbar[i] = a_gbar[i];
+        sa.gfull[i] = d_gfull[i];
+        sa.range[i] = d_range[i];
+    }
+    adj_swf<<<grid_a(nsites), kBlock, 0, s>>>(nsites, sa, d_sites, xbar);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_free_energy_grad(sfgpu_system *s, const double *x, double *F, double *xbar) {
+    if (!s || !x || !F || !xbar) return SFGPU_ERR_INVALID;
+    int rc = s->ensure_adjoint();
+    if (rc) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(s->d_x, x, sizeof(double) * s->nvar, cudaMemcpyHostToDevice, s->stream));
+    if ((rc = s->free_energy_grad(s->d_x, F, s->a_xbar))) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(xbar, s->a_xbar, sizeof(double) * s->nvar, cudaMemcpyDeviceToHost, s->stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return SFGPU_OK;
 }
 

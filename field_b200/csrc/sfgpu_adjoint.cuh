@@ -294,4 +294,137 @@ static __global__ void adj_chi(DLat L, ResParam rp, const int *__restrict__ site
     }
 }
 
+// out[idx] += v for a value side_fraction read at idx: a boundary entry that
+// holds a copy of another site (SetBoundaries) passes v on to that site;
+// surface layers keep it
+__device__ __forceinline__ void side_put(const DLat &L, int idx, double v, double *__restrict__ out) {
+    atomicAdd(out + lat_map(L, idx), v);
+}
+
+// Transpose of side_fraction(L, p, z) at any site z (surface layers
+// included): out += y * d<p>(z)/dp, branch by branch as side_fraction reads.
+__device__ inline void side_fraction_adj(const DLat &L, int z, double y, double *__restrict__ out) {
+    if (y == 0.0) return;
+    int c[3];
+    lat_coords(L, z, c);
+    if (L.grad == 3) {
+        if (!lat_interior(L, c)) return;
+        const int jx = L.st[0], jy = L.st[1];
+        const double q = y * (1.0 / 6.0);
+        side_put(L, z + jx, q, out); side_put(L, z - jx, q, out);
+        side_put(L, z + jy, q, out); side_put(L, z - jy, q, out);
+        side_put(L, z + 1, q, out);  side_put(L, z - 1, q, out);
+        return;
+    }
+    const double l = L.l1chi;
+    if (L.grad == 1) {
+        int zz = z;
+        if (z == 0) {
+            if (L.bc_lo[0] == SFGPU_BOUND_SURFACE) {
+                side_put(L, 0, (1.0 - 2.0 * l) * y, out);
+                side_put(L, 1, l * y, out);
+                return;
+            }
+            zz = L.map_lo[0];
+        } else if (z == L.M - 1) {
+            if (L.bc_hi[0] == SFGPU_BOUND_SURFACE) {
+                side_put(L, z, (1.0 - 2.0 * l) * y, out);
+                side_put(L, z - 1, l * y, out);
+                return;
+            }
+            zz = L.map_hi[0];
+        }
+        side_put(L, zz, (1.0 - 2.0 * l) * y, out);
+        side_put(L, zz - 1, l * y, out);
+        side_put(L, zz + 1, l * y, out);
+        return;
+    }
+    const int MX = L.Md[0], MY = L.Md[1];
+    const bool onsurf = (c[0] == 0 && L.bc_lo[0] == SFGPU_BOUND_SURFACE) ||
+                        (c[0] == MX - 1 && L.bc_hi[0] == SFGPU_BOUND_SURFACE) ||
+                        (c[1] == 0 && L.bc_lo[1] == SFGPU_BOUND_SURFACE) ||
+                        (c[1] == MY - 1 && L.bc_hi[1] == SFGPU_BOUND_SURFACE);
+    int x = c[0], zz = z;
+    if (!onsurf) { zz = lat_map(L, z); x = zz / MY; }
+    const double lm = L.cyl ? L.lam_m[x] : l, lp = L.cyl ? L.lam_p[x] : l;
+    if (!onsurf) {
+        if (L.cyl) {
+            side_put(L, zz, (1.0 - lp - lm - 2.0 * l) * y, out);
+            side_put(L, zz + MY, lp * y, out);
+            side_put(L, zz - MY, lm * y, out);
+        } else {
+            side_put(L, zz, (1.0 - 2.0 * l - lm - lp) * y, out);
+            side_put(L, zz - MY, l * y, out);
+            side_put(L, zz + MY, l * y, out);
+        }
+        side_put(L, zz - 1, l * y, out);
+        side_put(L, zz + 1, l * y, out);
+        return;
+    }
+    side_put(L, z, (1.0 - 2.0 * l - lm - lp) * y, out);
+    if (c[0] > 0) side_put(L, z - MY, lm * y, out);
+    if (c[0] < MX - 1) side_put(L, z + MY, lp * y, out);
+    if (c[1] > 0) side_put(L, z - 1, l * y, out);
+    if (c[1] < MY - 1) side_put(L, z + 1, l * y, out);
+}
+
+// Free energy F = sum_z wf [sum_m p_m (ln(N_m) + lnC_m)/N_m - p_m chemintref_m
+// + sum_(m,i) q_mi ln G_i + 1/2 sum_(i,j) chi_ij phi_i <phi_j>] (the form of
+// free_energy_partial).  Contact part of the state cotangents:
+// phibar_i += 1/2 wf sum_j chi_ij <phi_j> directly and, through the
+// averages, the transpose of SideFraction applied to 1/2 wf sum_i chi_ij phi_i.
+struct FeAdjParam {
+    int nseg;
+    const double *phi[SFGPU_MAX_SEG];
+    double *phibar[SFGPU_MAX_SEG];
+};
+static __global__ void fe_contact_adj(DLat L, FeAdjParam fp, ChiTable ct, const double *__restrict__ wf) {
+    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < L.M; z += gridDim.x * blockDim.x) {
+        const double w = wf[z];
+        if (w == 0) continue;
+        for (int i = 0; i < fp.nseg; i++) {
+            double ci = 0;
+            for (int j = 0; j < fp.nseg; j++) {
+                const double x = ct.chi[i * SFGPU_MAX_SEG + j];
+                if (x != 0) ci += x * side_fraction(L, fp.phi[j], z);
+            }
+            if (ci != 0) atomicAdd(fp.phibar[i] + z, 0.5 * w * ci);
+        }
+        for (int j = 0; j < fp.nseg; j++) {
+            double yj = 0;
+            for (int i = 0; i < fp.nseg; i++) {
+                const double x = ct.chi[i * SFGPU_MAX_SEG + j];
+                if (x != 0) yj += x * fp.phi[i][z];
+            }
+            side_fraction_adj(L, z, 0.5 * w * yj, fp.phibar[j]);
+        }
+    }
+}
+
+// cotangent of molecule m's profile of segment i: the state part plus
+// wf ((ln N + lnC)/N - chemintref + ln G_i)
+static __global__ void fe_mol_phibar(int M, const double *__restrict__ state_bar, const double *__restrict__ wf,
+                                     const double *__restrict__ G, double invN, double lnN, double chemintref,
+                                     const MolScal *__restrict__ scal, int mol, double *__restrict__ out) {
+    const double a = invN * (lnN + scal[mol].lnc) - chemintref;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+        const double w = wf[r];
+        double v = state_bar[r];
+        if (w != 0) {
+            const double g = G[r];
+            v += w * (a + (g > 0 ? log(g) : 0.0));
+        }
+        out[r] = v;
+    }
+}
+
+// Gbar_i += wf q_mi / G_i where G_i > 0 (the q ln G term), for one molecule profile
+static __global__ void fe_gbar(int M, const double *__restrict__ q, const double *__restrict__ wf,
+                               const double *__restrict__ G, double *__restrict__ gbar) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+        const double w = wf[r], g = G[r];
+        if (w != 0 && g > 0) gbar[r] += w * q[r] / g;
+    }
+}
+
 }  // namespace sfa

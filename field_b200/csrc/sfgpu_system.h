@@ -68,7 +68,10 @@ struct sfgpu_system {
     void adj_bstep(const HMol &o, int t, const double *src, double *dst, const double *other, double *phi);
     int set_checkpoint(int stride);
     int molecule_phi_store(int m);
-    int molecule_adjoint(int m);
+    int molecule_adjoint(int m, double *const *phibar_src);
+    int primal_store(const double *x, double *f);
+    int free_energy_grad(const double *x, double *F, double *xbar);
+    std::vector<double *> a_phibar_m;
     int vjp_async(const double *x, const double *w, double *f, double *xbar);
     int launch_step1(const double *gin, const double *G, double *gout, const double *other, double *phi, int mode);
     std::vector<void *> allocs;

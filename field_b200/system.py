@@ -142,6 +142,14 @@ class System:
         nat.check(self.lib.sfgpu_vjp_chi(self.h, _d(x), _d(w), _d(out)), "sfgpu_vjp_chi")
         return out.reshape(ns, ns)
 
+    def free_energy_grad(self, x):
+        """(F(x), dF/dx) with the exact gradient from the reverse sweep (sfgpu_free_energy_grad)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        F = C.c_double()
+        g = np.empty(self.nvar)
+        nat.check(self.lib.sfgpu_free_energy_grad(self.h, _d(x), C.byref(F), _d(g)), "sfgpu_free_energy_grad")
+        return F.value, g
+
     def set_checkpoint(self, stride: int):
         """Reverse-sweep memory: 0 stores every slice, k > 0 keeps checkpoints
         every k positions and recomputes segments (sfgpu_system_set_checkpoint)."""

@@ -219,9 +219,10 @@ int sfgpu_vjp_host(sfgpu_system *sys, const double *x, const double *w, double *
  * the slices at every k-th position (checkpoints) and recomputes the k
  * slices of one segment at a time when the sweep reaches it, in
  * (2 ceil(N/k) + 2k + 1) M doubles -- k near sqrt(N) is smallest -- for
- * about 1.75x the propagation work.  Results are identical for every
- * stride (the recomputed slices are computed by the same kernels).  The
- * storage is reallocated at the next sfgpu_vjp. */
+ * about 1.75x the propagation work; stride -1 picks ceil(sqrt(N)) of the
+ * longest chain, the stride of least memory.  Results are identical for
+ * every stride (the recomputed slices are computed by the same kernels).
+ * The storage is reallocated at the next sfgpu_vjp. */
 int sfgpu_system_set_checkpoint(sfgpu_system *sys, int stride);
 /* Sensitivity of the residual to the Flory-Huggins parameters at fixed x
  * (first and second order): dchi[a * nseg + i] = d (w . f(x)) / d chi(a, i)
@@ -231,6 +232,11 @@ int sfgpu_system_set_checkpoint(sfgpu_system *sys, int stride);
  * add dchi[a][b] + dchi[b][a].  With the adjoint solution w of J^T w = dL/dx
  * at a converged x, dL/dchi = -(that sum).  No counterpart in SFbox. */
 int sfgpu_vjp_chi(sfgpu_system *sys, const double *x, const double *w, double *dchi);
+/* Free energy F(x) (as sfgpu_free_energy after a residual at x,
+ * SF_MolList1stO::GetFreeEnergy, SF_MolList1stO.cpp:606-635) and its exact
+ * gradient dF/dx by the reverse sweep (first and second order).  x, xbar:
+ * nvar host values; F: one host value.  No counterpart in SFbox. */
+int sfgpu_free_energy_grad(sfgpu_system *sys, const double *x, double *F, double *xbar);
 /* L-BFGS (Nocedal 1980 two-loop recursion, m pairs, Armijo backtracking) on
  * |f(x)|^2 / 2 with the exact gradient J^T f from the adjoint sweep; SFbox's
  * LBFGS method (SFNewton::L_BFGS, sfnewton.cpp:1770-1807) iterates on the
