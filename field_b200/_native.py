@@ -46,6 +46,7 @@ PROTOTYPES = {
     "sfgpu_system_set_checkpoint": (i32, [vp, i32]),
     "sfgpu_vjp_chi": (i32, [vp, dp, dp, dp]),
     "sfgpu_free_energy_grad": (i32, [vp, dp, dp, dp]),
+    "sfgpu_phi_sensitivity_chi": (i32, [vp, dp, dp, dp, f64, i32, i32, dp]),
     "sfgpu_solve_lbfgs": (i32, [vp, dp, f64, i32, i32, ip, ip, dp]),
     "sfgpu_system_autotune": (i32, [vp, i32, ip, dp]),
     "sfgpu_batch_create": (i32, [i32, vp, i32, C.POINTER(vp)]),

@@ -623,6 +623,62 @@ int sfgpu_system::free_energy_grad(const double *x, double *F, double *xbar) {
     return SFGPU_OK;
 }
 
+// xbar = (d phi / dx)^T omega at fixed chi, for L = sum_i sum_z omega_i(z)
+// phi_i(z) of the state profiles (omega: nseg device vectors of M)
+int sfgpu_system::phi_vjp_async(const double *x, const double *const *omega, double *xbar) {
+    int rc = ensure_adjoint();
+    if (rc) return rc;
+    cudaStream_t s = stream;
+    if ((rc = primal_store(x, d_f))) return rc;
+    for (int i = 0; i < nseg; i++) {
+        SFGPU_CUDA_TRY(cudaMemcpyAsync(a_phibar[i], omega[i], sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+        SFGPU_CUDA_TRY(cudaMemsetAsync(a_gbar[i], 0, sizeof(double) * M, s));
+    }
+    fe_zero_scal<<<1, 1, 0, s>>>(nmol, (AdjScal *)a_scal);
+    int held = (mols[solvent].type != 0) ? solvent : -1;
+    if (held < 0)
+        for (int m = nmol - 1; m >= 0 && held < 0; m--)
+            if (m != solvent && mols[m].type != 0) held = m;
+    if ((rc = molecule_adjoint(solvent, a_phibar.data()))) return rc;
+    for (int m = nmol - 1; m >= 0; m--) {
+        if (m == solvent) continue;
+        if (mols[m].type != 0 && m != held) {
+            if ((rc = store_chains(m, false, nullptr))) return rc;
+            held = m;
+        }
+        if ((rc = molecule_adjoint(m, a_phibar.data()))) return rc;
+    }
+    SFGPU_CUDA_TRY(cudaMemsetAsync(xbar, 0, sizeof(double) * nvar, s));
+    SwfAdj sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.nseg = nseg; sa.nclass = nclass;
+    for (int i = 0; i < nseg; i++) {
+        sa.cls[i] = class_of[i];
+        sa.pinned[i] = freedom[i] == SFGPU_SEG_PINNED;
+        sa.gbar[i] = a_gbar[i];
+        sa.gfull[i] = d_gfull[i];
+        sa.range[i] = d_range[i];
+    }
+    adj_swf<<<grid_a(nsites), kBlock, 0, s>>>(nsites, sa, d_sites, xbar);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+// dchi = d (w . f(x)) / d chi at fixed x, nseg * nseg device values
+int sfgpu_system::chi_vjp_async(const double *x, const double *w, double *dchi) {
+    int rc = residual_async(x, d_f);
+    if (rc) return rc;
+    SFGPU_CUDA_TRY(cudaMemsetAsync(dchi, 0, sizeof(double) * (size_t)nseg * nseg, stream));
+    ResParam rp;
+    memset(&rp, 0, sizeof(rp));
+    rp.nsites = nsites; rp.nclass = nclass; rp.nseg = nseg;
+    for (int c = 0; c < nclass; c++) rp.rep[c] = rep_of_class[c];
+    for (int i = 0; i < nseg; i++) rp.phi[i] = d_phi[i];
+    adj_chi<<<grid_a(nsites), kBlock, 0, stream>>>(H.L, rp, d_sites, w, d_phib, dchi);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
 extern "C" int sfgpu_free_energy_grad(sfgpu_system *s, const double *x, double *F, double *xbar) {
     if (!s || !x || !F || !xbar) return SFGPU_ERR_INVALID;
     int rc = s->ensure_adjoint();

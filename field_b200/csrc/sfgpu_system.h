@@ -71,6 +71,8 @@ struct sfgpu_system {
     int molecule_adjoint(int m, double *const *phibar_src);
     int primal_store(const double *x, double *f);
     int free_energy_grad(const double *x, double *F, double *xbar);
+    int phi_vjp_async(const double *x, const double *const *omega, double *xbar);
+    int chi_vjp_async(const double *x, const double *w, double *dchi);
     std::vector<double *> a_phibar_m;
     int vjp_async(const double *x, const double *w, double *f, double *xbar);
     int launch_step1(const double *gin, const double *G, double *gout, const double *other, double *phi, int mode);

@@ -3,6 +3,7 @@
 // built on them (GMRES with exact J*v in place of the finite-difference
 // products of SFNewton's truncated Newton, sfnewton.cpp:1662-1688).
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -410,4 +411,135 @@ extern "C" int sfgpu_solve_nk(sfgpu_system *s, double *x_host, double tol, int m
     if (final_error) *final_error = fn;
     if (!std::isfinite(fn)) return SFGPU_ERR_NONFINITE;
     return (fn <= tol) ? SFGPU_OK : SFGPU_ERR_NOTCONVERGED;
+}
+
+// Restarted GMRES(krylov) on A y = b from y = 0, A applied by op (CGS2
+// orthogonalisation, Givens rotations), until |b - A y| <= rtol |b| or
+// maxcycles restarts.  V: n (krylov + 1) doubles; w, r: n doubles.
+static int gmres_solve(NKWork &W, const std::function<int(const double *, double *)> &op, const double *b,
+                       double *y, double rtol, int krylov, int maxcycles, double *V, double *w, double *r,
+                       double *relres, int *nops) {
+    sfgpu_system *s = W.s;
+    const size_t n = W.n;
+    const int gv = W.gb;
+    cudaStream_t st = s->stream;
+    int rc;
+    double bn;
+    if ((rc = W.norm(b, &bn))) return rc;
+    SFGPU_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(double) * n, st));
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    std::vector<double> H((size_t)(krylov + 1) * krylov), cs(krylov), sn(krylov), g(krylov + 1), yk(krylov);
+    double rn = bn;
+    *nops = 0;
+    for (int cycle = 0; cycle < maxcycles && rn > rtol * bn && bn > 0; cycle++) {
+        const double beta = rn;
+        k_scale_copy<<<gv, kBlock, 0, st>>>(n, 1.0 / beta, r, V);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int kdim = 0;
+        for (int j = 0; j < krylov; j++) {
+            if ((rc = op(V + (size_t)j * n, w))) return rc;
+            (*nops)++;
+            std::vector<const double *> va(j + 1), wb(j + 1, w);
+            for (int i = 0; i <= j; i++) va[i] = V + (size_t)i * n;
+            std::vector<double> h1(j + 1), h2(j + 1);
+            if ((rc = W.dots(j + 1, va.data(), wb.data(), h1.data()))) return rc;
+            HCoef c;
+            c.n = j + 1;
+            for (int i = 0; i <= j; i++) c.h[i] = h1[i];
+            k_subtract_basis<<<gv, kBlock, 0, st>>>(n, c, V, w);
+            if ((rc = W.dots(j + 1, va.data(), wb.data(), h2.data()))) return rc;
+            for (int i = 0; i <= j; i++) c.h[i] = h2[i];
+            k_subtract_basis<<<gv, kBlock, 0, st>>>(n, c, V, w);
+            double hn;
+            if ((rc = W.norm(w, &hn))) return rc;
+            for (int i = 0; i <= j; i++) H[(size_t)i * krylov + j] = h1[i] + h2[i];
+            H[(size_t)(j + 1) * krylov + j] = hn;
+            for (int i = 0; i < j; i++) {
+                const double a = H[(size_t)i * krylov + j], bb = H[(size_t)(i + 1) * krylov + j];
+                H[(size_t)i * krylov + j] = cs[i] * a + sn[i] * bb;
+                H[(size_t)(i + 1) * krylov + j] = -sn[i] * a + cs[i] * bb;
+            }
+            const double a = H[(size_t)j * krylov + j], bb = H[(size_t)(j + 1) * krylov + j];
+            const double rr = sqrt(a * a + bb * bb);
+            cs[j] = (rr > 0) ? a / rr : 1.0;
+            sn[j] = (rr > 0) ? bb / rr : 0.0;
+            H[(size_t)j * krylov + j] = rr;
+            H[(size_t)(j + 1) * krylov + j] = 0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            kdim = j + 1;
+            if (hn > 0) k_scale_copy<<<gv, kBlock, 0, st>>>(n, 1.0 / hn, w, V + (size_t)(j + 1) * n);
+            if (fabs(g[j + 1]) <= rtol * bn || !(hn > 0)) break;
+        }
+        for (int i = kdim - 1; i >= 0; i--) {
+            double acc = g[i];
+            for (int k = i + 1; k < kdim; k++) acc -= H[(size_t)i * krylov + k] * yk[k];
+            yk[i] = acc / H[(size_t)i * krylov + i];
+        }
+        HCoef c;
+        c.n = kdim;
+        for (int i = 0; i < kdim; i++) c.h[i] = yk[i];
+        k_add_basis<<<gv, kBlock, 0, st>>>(n, c, V, y);
+        // true residual r = b - A y
+        if ((rc = op(y, w))) return rc;
+        (*nops)++;
+        k_lincomb<<<gv, kBlock, 0, st>>>(n, b, -1.0, w, r);
+        if ((rc = W.norm(r, &rn))) return rc;
+    }
+    *relres = (bn > 0) ? rn / bn : 0.0;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_phi_sensitivity_chi(sfgpu_system *s, const double *x_host, const double *omega_host,
+                                         double *dchi_host, double rtol, int krylov, int maxcycles,
+                                         double *relres) {
+    if (!s || !x_host || !omega_host || !dchi_host || krylov < 1 || krylov > 60 || maxcycles < 1 || !(rtol > 0))
+        return SFGPU_ERR_INVALID;
+    int rc = s->ensure_adjoint();
+    if (rc) return rc;
+    const size_t n = s->nvar, M = s->M;
+    const int ns = s->nseg;
+    cudaStream_t st = s->stream;
+    std::vector<void *> mine;
+    auto get = [&](double **p, size_t cnt) -> int {
+        cudaError_t e = cudaMalloc((void **)p, sizeof(double) * (cnt ? cnt : 1));
+        if (e != cudaSuccess) { sfgpu_set_error(e, "cudaMalloc", __FILE__, __LINE__); return SFGPU_ERR_NOMEM; }
+        mine.push_back(*p);
+        return SFGPU_OK;
+    };
+    auto cleanup = [&]() { for (void *p : mine) cudaFree(p); };
+    NKWork W;
+    W.s = s;
+    W.n = n;
+    W.gb = (int)std::max<size_t>(1, std::min<size_t>((n + kBlock - 1) / kBlock, 148 * 8));
+    double *x, *b, *lam, *V, *w, *r, *om, *dchi;
+    if ((rc = get(&x, n)) || (rc = get(&b, n)) || (rc = get(&lam, n)) || (rc = get(&V, n * (krylov + 1))) ||
+        (rc = get(&w, n)) || (rc = get(&r, n)) || (rc = get(&om, (size_t)ns * M)) ||
+        (rc = get(&dchi, (size_t)ns * ns)) || (rc = get(&W.partial, (size_t)W.gb * 64)) || (rc = get(&W.sums, 64))) {
+        cleanup();
+        return rc;
+    }
+#define SCTRY(e) do { cudaError_t _e = (e); if (_e != cudaSuccess) { sfgpu_set_error(_e, #e, __FILE__, __LINE__); cleanup(); return SFGPU_ERR_CUDA; } } while (0)
+#define SCRC(e) do { int _r = (e); if (_r) { cleanup(); return _r; } } while (0)
+    SCTRY(cudaMemcpyAsync(x, x_host, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    SCTRY(cudaMemcpyAsync(om, omega_host, sizeof(double) * ns * M, cudaMemcpyHostToDevice, st));
+    std::vector<const double *> omp(ns);
+    for (int i = 0; i < ns; i++) omp[i] = om + (size_t)i * M;
+    SCRC(s->phi_vjp_async(x, omp.data(), b));   // b = dL/dx at fixed chi
+    int nops = 0;
+    double rr = 0;
+    // J^T lam = b
+    SCRC(gmres_solve(W, [&](const double *v, double *out) { return s->vjp_async(x, v, s->d_f, out); }, b, lam,
+                     rtol, krylov, maxcycles, V, w, r, &rr, &nops));
+    SCRC(s->chi_vjp_async(x, lam, dchi));
+    std::vector<double> h((size_t)ns * ns);
+    SCTRY(cudaMemcpyAsync(h.data(), dchi, sizeof(double) * ns * ns, cudaMemcpyDeviceToHost, st));
+    SCTRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < ns * ns; i++) dchi_host[i] = -h[i];
+    if (relres) *relres = rr;
+    cleanup();
+#undef SCTRY
+#undef SCRC
+    return SFGPU_OK;
 }

@@ -150,6 +150,21 @@ class System:
         nat.check(self.lib.sfgpu_free_energy_grad(self.h, _d(x), C.byref(F), _d(g)), "sfgpu_free_energy_grad")
         return F.value, g
 
+    def phi_sensitivity_chi(self, x, omega, rtol=1e-10, krylov=40, maxcycles=20):
+        """dL/d chi at a solution x for L = sum omega . phi (nseg x M weights),
+        through the solution's dependence on chi (sfgpu_phi_sensitivity_chi).
+        Returns (nseg x nseg array, relative residual of the adjoint solve)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        om = np.ascontiguousarray(omega, dtype=np.float64).reshape(-1)
+        ns = len(self.spec.segments)
+        if om.size != ns * self.M:
+            raise ValueError(f"omega has {om.size} values, expected {ns} x {self.M}")
+        out = np.zeros(ns * ns)
+        rr = C.c_double()
+        nat.check(self.lib.sfgpu_phi_sensitivity_chi(self.h, _d(x), _d(om), _d(out), rtol, krylov, maxcycles,
+                                                     C.byref(rr)), "sfgpu_phi_sensitivity_chi")
+        return out.reshape(ns, ns), rr.value
+
     def set_checkpoint(self, stride: int):
         """Reverse-sweep memory: 0 stores every slice, k > 0 keeps checkpoints
         every k positions and recomputes segments (sfgpu_system_set_checkpoint)."""

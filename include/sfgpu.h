@@ -237,6 +237,16 @@ int sfgpu_vjp_chi(sfgpu_system *sys, const double *x, const double *w, double *d
  * gradient dF/dx by the reverse sweep (first and second order).  x, xbar:
  * nvar host values; F: one host value.  No counterpart in SFbox. */
 int sfgpu_free_energy_grad(sfgpu_system *sys, const double *x, double *F, double *xbar);
+/* Sensitivity of the converged profiles to chi.  x: a solution of
+ * residuals(x) = 0 (host, nvar); omega: nseg * M host weights defining
+ * L = sum_i sum_z omega[i * M + z] phi_i(z).  Returns dchi[a * nseg + i] =
+ * dL / d chi(a, i) through the solution's dependence on chi (implicit
+ * function theorem: J^T lam = dL/dx solved by restarted GMRES(krylov) to
+ * rtol with the reverse sweep as operator, then dL/dchi = -lam^T df/dchi);
+ * for a symmetric change of chi(a,b) = chi(b,a) add both entries.  relres:
+ * the relative residual reached (may be NULL).  No counterpart in SFbox. */
+int sfgpu_phi_sensitivity_chi(sfgpu_system *sys, const double *x, const double *omega, double *dchi, double rtol,
+                              int krylov, int maxcycles, double *relres);
 /* L-BFGS (Nocedal 1980 two-loop recursion, m pairs, Armijo backtracking) on
  * |f(x)|^2 / 2 with the exact gradient J^T f from the adjoint sweep; SFbox's
  * LBFGS method (SFNewton::L_BFGS, sfnewton.cpp:1770-1807) iterates on the

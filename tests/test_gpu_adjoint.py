@@ -230,3 +230,41 @@ def test_free_energy_gradient(gpu_lib, case):
         d = rng.normal(size=s.nvar)
         fd = (F_at(x + h * d) - F_at(x - h * d)) / (2 * h)
         assert abs(fd - g @ d) <= 1e-7 * np.linalg.norm(g) * np.linalg.norm(d) + 1e-9 * abs(F), (fd, g @ d)
+
+
+def test_phi_sensitivity_to_chi(gpu_lib):
+    """dL/dchi for L = omega . phi_A at a converged C1-shaped solution,
+    through the solution's dependence on chi (adjoint GMRES on J^T), against
+    central differences of L between solutions re-converged (Newton-Krylov,
+    |f| < 1e-12) with chi(a,b) = chi(b,a) changed by +-1e-4."""
+    def build(dchi=None):
+        spec, x0 = configs.flat_adsorption(n=40, N=20)
+        if dchi is not None:
+            a, b, h = dchi
+            spec.chi = np.array(spec.chi, dtype=float).copy()
+            spec.chi[a, b] += h
+            spec.chi[b, a] += h
+        return spec, x0
+
+    spec, x0 = build()
+    s = System(spec)
+    r = s.solve_nk(x0, tol=1e-12, maxit=100, krylov=40)
+    assert r.converged
+    iA = spec.segment_index("A")
+    omega = np.zeros((len(spec.segments), s.M))
+    omega[iA] = np.random.default_rng(111).normal(size=s.M)
+    d, relres = s.phi_sensitivity_chi(r.x, omega, rtol=1e-11)
+    assert relres < 1e-10
+    h = 1e-4
+    for other in ("W", "S"):
+        j = spec.segment_index(other)
+        vals = []
+        for sgn in (1, -1):
+            sp, _ = build((iA, j, sgn * h))
+            s2 = System(sp)
+            r2 = s2.solve_nk(r.x, tol=1e-12, maxit=100, krylov=40)
+            assert r2.converged
+            vals.append(float(np.sum(omega[iA] * s2.phi(iA))))
+        fd = (vals[0] - vals[1]) / (2 * h)
+        got = d[iA, j] + d[j, iA]
+        assert abs(fd - got) <= 1e-5 * max(abs(fd), 1e-8), (other, fd, got)
