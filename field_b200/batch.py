@@ -33,7 +33,7 @@ def launches_per_residual(spec) -> int:
     """Kernel launches of one single-system residual evaluation
     (sfgpu_system::residual_async): SWF updates, per-molecule propagation,
     state sums, bulk scalars and the residual kernel."""
-    K = 6 if spec.lattice.order == 2 else 1
+    K = spec.lattice.components
     n = 0
     for s in spec.segments:
         if s.freedom != 1:
@@ -93,7 +93,7 @@ def residual_bytes(spec) -> float:
     """Algorithmic bytes of one residual evaluation's propagation: forward
     step 8*(K+1+K) per site, backward step with composition 8*(3K+3) per site
     (read Gb(s+1), G, Gf(s), phi; write Gb(s), phi), per molecule."""
-    K = 6 if spec.lattice.order == 2 else 1
+    K = spec.lattice.components
     M = spec.M
     tot = 0.0
     for mol in spec.molecules:

@@ -25,6 +25,12 @@ struct DLat {
     int map_lo[3], map_hi[3];  // coordinate copied into 0 / Md-1
     double l1, l1chi;
     const double *lam_m, *lam_p;   // cylinder tables by x (device)
+    // second order: direction components (6 in 3D; 1D and 2D lump the
+    // directions along the homogeneous gradients: 3 and 5), and whether a
+    // step that reads across the lower / upper boundary of gradient d swaps
+    // the +d and -d components
+    int K;
+    int sw_lo[3], sw_hi[3];
 };
 
 struct ChiTable {              // passed by value: small interaction tables
@@ -321,3 +327,4 @@ __device__ inline double side_fraction(const DLat &L, const double *__restrict__
     } while (0)
 
 void sfgpu_set_error(cudaError_t e, const char *what, const char *file, int line);
+int fail_unsupported(const char *what);   // records the message, returns SFGPU_ERR_UNSUPPORTED

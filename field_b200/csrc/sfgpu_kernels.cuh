@@ -282,13 +282,151 @@ static __global__ void step2_rows(DLat L, const double *__restrict__ gin, const 
     });
 }
 
+// Second-order steps of the flat 1D and 2D lattices, whose homogeneous
+// gradients lump their bond directions into one component each (Lat1D2ndO:
+// +x, lateral x4, -x, Lat1D2ndO.cpp:33-147; Lat2D2ndO: +x, +y, z x2, -y, -x,
+// Lat2D2ndO.cpp:32-230).  W[kk][kp] = the weight of a bond in direction kk
+// after one in kp summed over kp's group: S for the same direction (plus
+// 2L for the 1D lateral group's two perpendicular members), 0 for the
+// opposite direction, mult[kp] L otherwise.  The forward step reads every
+// component at t - e_kk, the backward step reads component kp at t + e_kp;
+// a read across a boundary goes to the mapped site and, where the lattice
+// swaps there (sw_lo / sw_hi), takes the opposite component of that axis
+// (at a surface, the site itself, only the + component does).
+struct Lump2 {
+    int K;
+    int axis[5], sgn[5];
+    double mult[5];
+};
+__host__ __device__ inline Lump2 lump2_of(int grad) {
+    Lump2 q;
+    if (grad == 1) {
+        q.K = 3;
+        const int ax[3] = {0, -1, 0}, sg[3] = {1, 0, -1};
+        const double mu[3] = {1, 4, 1};
+        for (int k = 0; k < 3; k++) { q.axis[k] = ax[k]; q.sgn[k] = sg[k]; q.mult[k] = mu[k]; }
+        q.axis[3] = q.axis[4] = -1; q.sgn[3] = q.sgn[4] = 0; q.mult[3] = q.mult[4] = 0;
+    } else {
+        q.K = 5;
+        const int ax[5] = {0, 1, -1, 1, 0}, sg[5] = {1, 1, 0, -1, -1};
+        const double mu[5] = {1, 1, 2, 1, 1};
+        for (int k = 0; k < 5; k++) { q.axis[k] = ax[k]; q.sgn[k] = sg[k]; q.mult[k] = mu[k]; }
+    }
+    return q;
+}
+__host__ __device__ inline double lump2_w(const Lump2 &q, int kk, int kp, double S, double Lw) {
+    if (kk == kp) return (q.K == 3 && kk == 1) ? S + 2 * Lw : S;
+    if (q.axis[kk] >= 0 && q.axis[kk] == q.axis[kp] && q.sgn[kk] == -q.sgn[kp]) return 0.0;
+    return q.mult[kp] * Lw;
+}
+// the component of the opposite direction along kp's axis (kp itself for a lumped one)
+__host__ __device__ inline int lump2_swap(const Lump2 &q, int kp) {
+    if (q.axis[kp] < 0) return kp;
+    for (int k = 0; k < q.K; k++)
+        if (q.axis[k] == q.axis[kp] && q.sgn[k] == -q.sgn[kp]) return k;
+    return kp;
+}
+
+// site and swap mode (0 none, 1 swap, 2 surface) of a read one step from
+// interior site (x, y) along axis a in direction d (+1 / -1); 1D: x is the
+// position, y = 0
+__device__ __forceinline__ int lump2_nb(const DLat &L, int x, int y, int a, int d, int &sm) {
+    int c[2] = {x, y};
+    int v = c[a] + d;
+    sm = 0;
+    if (v == 0) { sm = L.sw_lo[a]; v = L.map_lo[a]; }
+    else if (v == L.Md[a] - 1) { sm = L.sw_hi[a]; v = L.map_hi[a]; }
+    c[a] = v;
+    return (L.grad == 1) ? c[0] : c[0] * L.st[0] + c[1];
+}
+// the component read for kp across a boundary of axis a with swap mode sm:
+// components of other axes are plain copies; a swap reads the opposite
+// direction; at a surface only the + direction reads the - one
+__host__ __device__ inline int lump2_read(const Lump2 &q, int kp, int a, int sm) {
+    if (sm == 0 || q.axis[kp] != a) return kp;
+    if (sm == 1 || q.sgn[kp] > 0) return lump2_swap(q, kp);
+    return kp;
+}
+
+static __global__ void step2l_rows(DLat L, const double *__restrict__ gin, const double *__restrict__ G, double S,
+                                   double *__restrict__ gout, const double *__restrict__ other,
+                                   double *__restrict__ phi, int mode, int backward) {
+    const int M = L.M;
+    const Lump2 q = lump2_of(L.grad);
+    const double Lw = (1.0 - S) / 4.0;
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const int t = R.base + k;
+        const int x = (L.grad == 1) ? k : R.x, y = (L.grad == 1) ? 0 : k;
+        const double g = G[t];
+        double out[5];
+        if (!backward) {
+            for (int kk = 0; kk < q.K; kk++) {
+                int src = t;
+                int sm = 0;
+                if (q.axis[kk] >= 0) src = lump2_nb(L, x, y, q.axis[kk], -q.sgn[kk], sm);
+                double acc = 0;
+                bool first = true;
+                for (int kp = 0; kp < q.K; kp++) {
+                    const double w = lump2_w(q, kk, kp, S, Lw);
+                    if (w == 0.0) continue;
+                    const int c = lump2_read(q, kp, q.axis[kk], sm);
+                    const double v = w * gin[(size_t)c * M + src];
+                    if (first) { acc = v; first = false; } else acc += v;
+                }
+                out[kk] = acc * g;
+            }
+        } else {
+            double v[5];
+            for (int kp = 0; kp < q.K; kp++) {
+                int src = t;
+                int sm = 0;
+                if (q.axis[kp] >= 0) src = lump2_nb(L, x, y, q.axis[kp], q.sgn[kp], sm);
+                const int c = lump2_read(q, kp, q.axis[kp], sm);
+                v[kp] = gin[(size_t)c * M + src];
+            }
+            for (int kq = 0; kq < q.K; kq++) {
+                double acc = 0;
+                bool first = true;
+                for (int kp = 0; kp < q.K; kp++) {
+                    const double w = lump2_w(q, kq, kp, S, Lw);
+                    if (w == 0.0) continue;
+                    const double u = w * v[kp];
+                    if (first) { acc = u; first = false; } else acc += u;
+                }
+                out[kq] = acc * g;
+            }
+        }
+        for (int kk = 0; kk < q.K; kk++) gout[(size_t)kk * M + t] = out[kk];
+        if (mode == COMP_ACC) {
+            double p = phi[t];
+            for (int kk = 0; kk < q.K; kk++) {
+                const double a = out[kk] * other[(size_t)kk * M + t];
+                p += (q.mult[kk] == 1.0) ? a : a * q.mult[kk];
+            }
+            phi[t] = p;
+        }
+    });
+}
+
+// multiplicity of direction component k of a K-component slice
+__host__ __device__ inline double comp_mult(int K, int k) {
+    if (K == 3 && k == 1) return 4.0;
+    if (K == 5 && k == 2) return 2.0;
+    return 1.0;
+}
+
 // phi += a * b over all K*M entries summed per site (copolymer end segment,
 // SF_Copol1stO.cpp:1218-1222; Lat3D2ndO::ConnectG over six components)
 static __global__ void connect(int M, int K, const double *__restrict__ a, const double *__restrict__ b,
                         double *__restrict__ phi) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
         double p = phi[r];
-        for (int k = 0; k < K; k++) p += a[(size_t)k * M + r] * b[(size_t)k * M + r];
+        for (int k = 0; k < K; k++) {
+            const double v = a[(size_t)k * M + r] * b[(size_t)k * M + r];
+            const double mu = comp_mult(K, k);
+            p += (mu == 1.0) ? v : v * mu;
+        }
         phi[r] = p;
     }
 }
@@ -308,7 +446,10 @@ static __global__ void wsum_partial(int M, int K, const double *__restrict__ g, 
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
         double wr = w[r];
         if (wr != 0)
-            for (int k = 0; k < K; k++) acc += wr * g[(size_t)k * M + r];
+            for (int k = 0; k < K; k++) {
+                const double mu = comp_mult(K, k);
+                acc += (mu == 1.0) ? wr * g[(size_t)k * M + r] : wr * (g[(size_t)k * M + r] * mu);
+            }
     }
     sh[threadIdx.x] = acc;
     __syncthreads();
@@ -332,7 +473,7 @@ static __global__ void mol_scalars(MolParam p, int nblocks, const double *__rest
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double v = 0;
     for (int b = 0; b < nblocks; b++) v += partial[b];
-    if (p.K == 6) v /= 6.0;
+    if (p.K > 1) v /= 6.0;   // six bond directions (lumped or not)
     MolScal s;
     s.lngn = log(v);
     double phib = p.phibulk_in;
@@ -350,7 +491,7 @@ static __global__ void mol_scalars(MolParam p, int nblocks, const double *__rest
         } else {
             s.lnc = log(p.theta) - s.lngn - log(1.0 * p.N);
             double c = (p.sym ? 2 * p.theta / N : p.theta / N);
-            s.norm = (p.K == 6) ? c / (6.0 * gn) : c / gn;
+            s.norm = (p.K > 1) ? c / (6.0 * gn) : c / gn;
         }
         s.phibulk = p.theta / gn;
     } else {
@@ -360,7 +501,7 @@ static __global__ void mol_scalars(MolParam p, int nblocks, const double *__rest
             s.norm = phib;
         } else {
             s.lnc = log(phib / N);
-            s.norm = p.sym ? 2 * phib / N : (p.K == 6 ? phib / (6 * N) : phib / N);
+            s.norm = p.sym ? 2 * phib / N : (p.K > 1 ? phib / (6 * N) : phib / N);
         }
     }
     if (p.pinned) s.phibulk = 0;   // SF_Homopol1stO.cpp:124-125
@@ -517,7 +658,8 @@ static __global__ void side_kernel(DLat L, const double *__restrict__ p, double 
         rho[z] = side_fraction(L, p, z);
 }
 
-// SetBoundaries on a profile (K components, with mirror swaps when K == 6)
+// SetBoundaries on a profile of K components: 6 swap at mirrors (3D); the
+// lumped 1D/2D components swap where the lattice's sw_lo / sw_hi say so
 static __global__ void set_boundaries(DLat L, int K, double *__restrict__ p) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < L.M; r += gridDim.x * blockDim.x) {
         int c[3];
@@ -525,9 +667,34 @@ static __global__ void set_boundaries(DLat L, int K, double *__restrict__ p) {
         if (lat_interior(L, c)) continue;
         int sw = 0;
         int t = lat_map(L, r, &sw);
-        if (t == r) continue;
+        if (t == r) {
+            // a surface site of a lumped lattice: the + component of each
+            // surface axis takes the - one's value (SetBx1(P,Q) with the
+            // boundary as its own copy layer)
+            if (K == 3 || K == 5) {
+                const Lump2 q = lump2_of(L.grad);
+                for (int k = 0; k < K; k++) {
+                    const int a = q.axis[k];
+                    if (a < 0 || q.sgn[k] < 0) continue;
+                    const int sm = (c[a] == 0) ? L.sw_lo[a] : (c[a] == L.Md[a] - 1 ? L.sw_hi[a] : 0);
+                    if (sm == 2) p[(size_t)k * L.M + r] = p[(size_t)lump2_swap(q, k) * L.M + r];
+                }
+            }
+            continue;
+        }
+        int swl = 0;   // axes whose boundary this site lies on and swaps, lumped lattices
+        if (K == 3 || K == 5)
+            for (int d = 0; d < L.grad; d++) {
+                if (c[d] == 0 && L.sw_lo[d]) swl |= 1 << d;
+                if (c[d] == L.Md[d] - 1 && L.sw_hi[d]) swl |= 1 << d;
+            }
         for (int k = 0; k < K; k++) {
-            int ks = (K == 6) ? swap_dir(k, sw) : k;
+            int ks = k;
+            if (K == 6) ks = swap_dir(k, sw);
+            else if (K == 3 || K == 5) {
+                const Lump2 q = lump2_of(L.grad);
+                if (q.axis[k] >= 0 && (swl >> q.axis[k]) & 1) ks = lump2_swap(q, k);
+            }
             p[(size_t)k * L.M + r] = p[(size_t)ks * L.M + t];
         }
     }

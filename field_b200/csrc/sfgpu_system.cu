@@ -21,6 +21,11 @@ static int fail(int code, const char *msg) {
     return code;
 }
 
+int fail_unsupported(const char *what) {
+    snprintf(g_errmsg, sizeof(g_errmsg), "not implemented: %s", what);
+    return SFGPU_ERR_UNSUPPORTED;
+}
+
 extern "C" const char *sfgpu_last_error(void) { return g_errmsg; }
 
 using namespace sfk;
@@ -84,8 +89,8 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
     if (L.grad < 1 || L.grad > 3) return fail(SFGPU_ERR_INVALID, "gradients must be 1, 2 or 3");
     if (d->geometry == SFGPU_GEOM_CYLINDRICAL && L.grad != 2)
         return fail(SFGPU_ERR_UNSUPPORTED, "cylindrical geometry needs 2 gradients");
-    if (L.order == 2 && L.grad != 3) return fail(SFGPU_ERR_UNSUPPORTED, "second order is implemented for 3 gradients");
     if (L.order != 1 && L.order != 2) return fail(SFGPU_ERR_INVALID, "order must be 1 or 2");
+    if (L.order == 2 && L.cyl) return fail(SFGPU_ERR_UNSUPPORTED, "second order is implemented for flat lattices");
     for (int k = 0; k < 3; k++) L.Md[k] = 1;
     for (int k = 0; k < L.grad; k++) {
         int n = d->n_layers[k];
@@ -103,7 +108,26 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
         L.bc_lo[k] = lo; L.bc_hi[k] = hi;
         L.map_lo[k] = map_lo_of(lo, n);
         L.map_hi[k] = map_hi_of(hi, n);
+        // component swaps of second-order steps across a boundary: 3D swaps
+        // at both mirror kinds (Lat3D::SetBx1(P,Q), Lat3D.cpp:1276-1289).  The
+        // flat 1D/2D lattices swap where the 1-based copy layer (surface 1 /
+        // n+2, mirror1 2 / n+1, mirror2 3 / n, periodic n+1 / 2) is <= 2 below
+        // (Lat1DFlat.cpp:658-666, Lat2DFlat.cpp:1382-1393) or >= n - 1 above
+        // (Lat1DFlat.cpp:673-680, Lat2DFlat.cpp:1401-1413), assigning P = Q',
+        // Q = P' in that order; at a surface the copy layer is the boundary
+        // itself, so the + component takes the - one's value and the - one
+        // keeps its own (swap mode 2)
+        if (L.grad == 3) {
+            L.sw_lo[k] = (lo == SFGPU_BOUND_MIRROR1 || lo == SFGPU_BOUND_MIRROR2);
+            L.sw_hi[k] = (hi == SFGPU_BOUND_MIRROR1 || hi == SFGPU_BOUND_MIRROR2);
+        } else {
+            const int copy_lo = (lo == SFGPU_BOUND_PERIODIC) ? n + 1 : lo;
+            const int copy_hi = (hi == SFGPU_BOUND_PERIODIC) ? 2 : (n + 2) - hi + 1;
+            L.sw_lo[k] = (copy_lo <= 2) ? (lo == SFGPU_BOUND_SURFACE ? 2 : 1) : 0;
+            L.sw_hi[k] = (copy_hi >= n - 1) ? (hi == SFGPU_BOUND_SURFACE ? 2 : 1) : 0;
+        }
     }
+    L.K = (L.order == 2) ? (L.grad == 1 ? 3 : (L.grad == 2 ? 5 : 6)) : 1;
     L.M = L.Md[0] * L.Md[1] * L.Md[2];
     if (L.grad == 1) { L.st[0] = 1; L.st[1] = 0; L.st[2] = 0; }
     else if (L.grad == 2) { L.st[0] = L.Md[1]; L.st[1] = 1; L.st[2] = 0; }
@@ -158,6 +182,9 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
         }
         H->w_f[z] = keep ? w : 0.0;
         H->w_gn[z] = interior ? w : 0.0;
+        // Lat1D2ndO::ComputeLnGN sums the interior without mirror2 halves or
+        // layer adjustment (Lat1D2ndO.cpp:275-285)
+        if (L.order == 2 && L.grad == 1) H->w_gn[z] = interior ? 1.0 : 0.0;
     }
     return SFGPU_OK;
 }
@@ -201,7 +228,7 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     if (rc) return rc;
     DLat &L = H.L;
     M = L.M;
-    K = (L.order == 2) ? 6 : 1;
+    K = L.K;
     nseg = d->n_segments;
     if (nseg < 1 || nseg > SFGPU_MAX_SEG) return fail(SFGPU_ERR_UNSUPPORTED, "1 to 8 segment types are supported");
     nmol = d->n_molecules;
@@ -434,9 +461,12 @@ int sfgpu_system::molecule_phi(int m) {
         int sg = o.seg[t];
         if (K == 1)
             launch_step1(d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
-        else
+        else if (K == 6)
             step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
                                        d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0);
+        else
+            step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
+                                        d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0);
     }
     replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[N - 1]], ginv);
     if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, ginv);
@@ -447,9 +477,12 @@ int sfgpu_system::molecule_phi(int m) {
         int sg = o.seg[t];
         if (K == 1)
             launch_step1(cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
-        else
+        else if (K == 6)
             step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv,
                                        d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC, 1);
+        else
+            step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv,
+                                        d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC, 1);
         cur = ginv; std::swap(ginv, tmp);
     }
     wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, cur, d_wgn, d_partial);
@@ -647,15 +680,18 @@ extern "C" int sfgpu_lat_propagate(sfgpu_system *s, const double *gin, const dou
     int gr = grid_for(s->M);
     if (s->K == 1)
         step1<<<gr, kBlock, 0, s->stream>>>(s->H.L, gin, g, gout, nullptr, nullptr, COMP_NONE);
-    else
+    else if (s->K == 6)
         step2<<<gr, kBlock, 0, s->stream>>>(s->H.L, gin, g, S, gout, nullptr, nullptr, COMP_NONE, backward);
+    else
+        step2l_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, gin, g, S, gout, nullptr, nullptr, COMP_NONE,
+                                                                backward);
     SFGPU_CUDA_TRY(cudaGetLastError());
     return SFGPU_OK;
 }
 
 extern "C" int sfgpu_lat_set_boundaries(sfgpu_system *s, double *p, int components) {
     CHECK_SYS(s);
-    if (components != 1 && components != 6) return fail(SFGPU_ERR_INVALID, "components must be 1 or 6");
+    if (components != 1 && components != s->K) return fail(SFGPU_ERR_INVALID, "components must be 1 or the lattice's K");
     set_boundaries<<<grid_for(s->M), kBlock, 0, s->stream>>>(s->H.L, components, p);
     SFGPU_CUDA_TRY(cudaGetLastError());
     return SFGPU_OK;
@@ -670,13 +706,13 @@ extern "C" int sfgpu_lat_side_fraction(sfgpu_system *s, const double *phi, doubl
 
 extern "C" int sfgpu_lat_lngn(sfgpu_system *s, const double *g, int components, double *lngn) {
     CHECK_SYS(s);
-    if (components != 1 && components != 6) return fail(SFGPU_ERR_INVALID, "components must be 1 or 6");
+    if (components != 1 && components != s->K) return fail(SFGPU_ERR_INVALID, "components must be 1 or the lattice's K");
     wsum_partial<<<s->nblocks_red, kBlock, 0, s->stream>>>(s->M, components, g, s->d_wgn, s->d_partial);
     finish_sums<<<1, 32, 0, s->stream>>>(1, s->nblocks_red, s->d_partial, s->d_misc);
     double v = 0;
     SFGPU_CUDA_TRY(cudaMemcpyAsync(&v, s->d_misc, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
-    if (components == 6) v /= 6.0;
+    if (components > 1) v /= 6.0;
     *lngn = log(v);
     return SFGPU_OK;
 }

@@ -77,6 +77,15 @@ class Lattice:
     def M(self) -> int:
         return int(np.prod(self.shape))
 
+    @property
+    def components(self) -> int:
+        """Direction components of a propagator: 1 (first order); second order
+        6 in 3D, and 3 (1D) / 5 (2D), which lump the bond directions along the
+        homogeneous gradients (Lat1D2ndO, Lat2D2ndO)."""
+        if self.order != 2:
+            return 1
+        return {1: 3, 2: 5, 3: 6}[self.gradients]
+
     def to_c(self) -> LatticeDesc:
         d = LatticeDesc()
         d.gradients, d.geometry, d.order = self.gradients, self.geometry, self.order

@@ -48,7 +48,7 @@ class System:
         M, nv, nc, ns = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         nat.check(self.lib.sfgpu_system_info(h, C.byref(M), C.byref(nv), C.byref(nc), C.byref(ns)), "info")
         self.M, self.nvar, self.nclass, self.nsites = M.value, nv.value, nc.value, ns.value
-        self.K = 6 if spec.lattice.order == 2 else 1
+        self.K = spec.lattice.components
 
     def close(self):
         if getattr(self, "h", None):
@@ -125,7 +125,7 @@ class System:
         return f, jv
 
     def vjp(self, x, w):
-        """(f(x), J(x)^T w) from the adjoint sweep (first-order lattices)."""
+        """(f(x), J(x)^T w) from the adjoint sweep (first-order lattices and Lat3D2ndO)."""
         x = np.ascontiguousarray(x, dtype=np.float64)
         w = np.ascontiguousarray(w, dtype=np.float64)
         f = np.empty(self.nvar)

@@ -168,8 +168,10 @@ int sfgpu_free_energy(sfgpu_system *sys, double *F);
  * Lat1stO::PropagateG(Gi, G, Gout) (Lat1stO.h:22; Lat1DFlat1stO.cpp:101-113,
  * Lat2DCyl1stO.cpp:72-97, Lat3D1stO.cpp:51-90).  Second order:
  * Lat2ndO::PropagateF (backward = 0) / PropagateB (backward = 1) with
- * persistence factor S (Lat3D2ndO.cpp:65-152, :597-678).  Boundary entries of
- * gout hold SetBoundaries copies. */
+ * persistence factor S (Lat3D2ndO.cpp:65-152, :597-678; lumped 1D/2D:
+ * Lat1D2ndO.cpp:33-147, Lat2D2ndO.cpp:32-230).  Boundary entries of gout hold
+ * SetBoundaries copies, except on the lumped 1D/2D lattices, whose step
+ * writes the interior entries only. */
 int sfgpu_lat_propagate(sfgpu_system *sys, const double *gin, const double *g, double *gout,
                         double S, int backward);
 /* Lattice::SetBoundaries on 1 or 6 components (Lat3D.cpp:1510-1562; the six

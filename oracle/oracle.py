@@ -74,7 +74,7 @@ class Oracle:
         self.M = lib().orc_num_sites(h)
         self.nvar = lib().orc_num_itvar(h)
         self.nclass = lib().orc_num_classes(h)
-        self.K = 6 if spec.lattice.order == 2 else 1
+        self.K = spec.lattice.components
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -40,6 +40,8 @@ typedef struct {
     double *lam_m, *lam_p, *Lx; /* cylinder tables by 0-based x (0..MX-1) */
     double *w_gn;      /* weights of interior sites in lnGN sums */
     double *w_f;       /* weights in the free-energy sum (surfaces included) */
+    int K;             /* 2nd-order direction components: 3 (1D), 5 (2D), 6 (3D); 1 first order */
+    int sw_lo[3], sw_hi[3];   /* 2nd order: +/- components swap at a boundary copy */
 } olat;
 
 static int map_lo_of(int bc, int n) {
@@ -128,7 +130,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
     L->cyl = (d->gradients == 2 && d->geometry == SFGPU_GEOM_CYLINDRICAL);
     if (L->grad < 1 || L->grad > 3) return SFGPU_ERR_INVALID;
     if (d->geometry == SFGPU_GEOM_CYLINDRICAL && d->gradients != 2) return SFGPU_ERR_UNSUPPORTED;
-    if (L->order == 2 && L->grad != 3) return SFGPU_ERR_UNSUPPORTED;
+    if (L->order == 2 && L->cyl) return SFGPU_ERR_UNSUPPORTED;
     for (int k = 0; k < 3; k++) { L->Md[k] = 1; }
     for (int k = 0; k < L->grad; k++) {
         L->n[k] = d->n_layers[k];
@@ -142,7 +144,22 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
         L->bc_lo[k] = lo; L->bc_hi[k] = hi;
         L->map_lo[k] = map_lo_of(lo, L->n[k]);
         L->map_hi[k] = map_hi_of(hi, L->n[k]);
+        /* SetBx1(P,Q) / SetBxm(P,Q) swap the two components of an axis when
+           the 1-based copy layer is <= 2 (lower side) or >= n - 1 (upper
+           side): Lat3D.cpp:1276-1289 (codes mirror1 1, mirror2 2);
+           Lat1DFlat.cpp:33-58 and :658-680, Lat2DFlat.cpp:1343-1413 (lower:
+           surface 1, mirror1 2, mirror2 3, periodic M-1; upper: M - code + 1,
+           periodic 2), i.e. the 0-based copy index map_lo <= 1 or
+           map_hi >= n - 2 */
+        if (L->grad == 3) {
+            L->sw_lo[k] = (lo == SFGPU_BOUND_MIRROR1 || lo == SFGPU_BOUND_MIRROR2);
+            L->sw_hi[k] = (hi == SFGPU_BOUND_MIRROR1 || hi == SFGPU_BOUND_MIRROR2);
+        } else {
+            L->sw_lo[k] = L->map_lo[k] <= 1;
+            L->sw_hi[k] = L->map_hi[k] >= L->n[k] - 2;
+        }
     }
+    L->K = (L->order == 2) ? (L->grad == 1 ? 3 : (L->grad == 2 ? 5 : 6)) : 1;
     L->M = L->Md[0] * L->Md[1] * L->Md[2];
     L->st[2] = 1; L->st[1] = L->Md[2]; L->st[0] = L->Md[1] * L->Md[2];
     if (L->grad == 1) { L->st[0] = 1; L->st[1] = L->st[2] = 0; }
@@ -203,6 +220,9 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
         }
         L->w_f[z] = keep ? w : 0.0;
         L->w_gn[z] = interior ? w : 0.0;
+        /* Lat1D2ndO::ComputeLnGN: interior sum without mirror2 halves or layer
+           adjustment (Lat1D2ndO.cpp:275-285) */
+        if (L->order == 2 && L->grad == 1) L->w_gn[z] = interior ? 1.0 : 0.0;
     }
     return SFGPU_OK;
 }
@@ -285,15 +305,112 @@ static void olat_prop2(const olat *L, const double *gin, const double *G, double
     olat_set_boundaries6(L, gout);
 }
 
+/* 2nd-order steps of the flat 1D and 2D lattices, whose homogeneous
+   gradients lump their bond directions: Lat1D2ndO (k: 0 = +x, 1 = lateral x4,
+   2 = -x), Lat1D2ndO.cpp:33-147; Lat2D2ndO (0 = +x, 1 = +y, 2 = z x2, 3 = -y,
+   4 = -x), Lat2D2ndO.cpp:32-230.  Boundary copies first (SetBx1/SetBxm/
+   SetBy1/SetBym on the input, swapping the two components of an axis where
+   the lattice does), then gx[kk](z) = sum_kp W[kk][kp] gin[kp](z - e_kk)
+   forward, gx[kq](z) = sum_kp W[kq][kp] gin[kp](z + e_kp) backward, times
+   G(z).  W: S for the same direction (+2L for the 1D lateral group), 0 for
+   the opposite one, mult[kp] L otherwise. */
+static const int LUMP_AXIS[2][5] = {{0, -1, 0, -1, -1}, {0, 1, -1, 1, 0}};
+static const int LUMP_SGN[2][5] = {{1, 0, -1, 0, 0}, {1, 1, 0, -1, -1}};
+static const double LUMP_MULT[2][5] = {{1, 4, 1, 0, 0}, {1, 1, 2, 1, 1}};
+static double lump_w(int g, int kk, int kp, double S, double Lw) {
+    if (kk == kp) return (g == 0 && kk == 1) ? S + 2 * Lw : S;
+    if (LUMP_AXIS[g][kk] >= 0 && LUMP_AXIS[g][kk] == LUMP_AXIS[g][kp] && LUMP_SGN[g][kk] == -LUMP_SGN[g][kp]) return 0.0;
+    return LUMP_MULT[g][kp] * Lw;
+}
+/* one SetBx1 / SetBxm / SetBy1 / SetBym call (Lat1DFlat.cpp:654-681,
+   Lat2DFlat.cpp:1336-1413) on the boundary line of axis a (upper side when
+   hi): every entry of P (and Q) on the line copies the copy layer's; where
+   the side swaps, P = Q' then Q = P' site by site, so at a surface (the
+   boundary is its own copy layer) both end with Q's value */
+static void lump_setb(const olat *L, double *P, double *Q, int a, int hi) {
+    int b = hi ? L->Md[a] - 1 : 0;
+    int src = hi ? L->map_hi[a] : L->map_lo[a];
+    int sw = hi ? L->sw_hi[a] : L->sw_lo[a];
+    for (int z = 0; z < L->M; z++) {
+        int c[3]; coords(L, z, c);
+        if (c[a] != b) continue;
+        c[a] = src;
+        int zs = site(L, c);
+        if (Q && sw) { P[z] = Q[zs]; Q[z] = P[zs]; }
+        else { P[z] = P[zs]; if (Q) Q[z] = Q[zs]; }
+    }
+}
+/* the boundary calls of Lat1D2ndO::PropagateF/B (Lat1D2ndO.cpp:43-44):
+   SetBx1(g0,g2) SetBx1(g1) SetBxm(g0,g2) SetBxm(g1); of Lat2D2ndO
+   (Lat2D2ndO.cpp:48-51): x below on (g0,g4) then g1..g3, y below on (g1,g3)
+   then g0, g2, g4, x above, y above */
+static void olat_set_boundaries_lumped(const olat *L, double *P) {
+    size_t M = (size_t)L->M;
+    double *g[5];
+    for (int k = 0; k < L->K; k++) g[k] = P + k * M;
+    for (int hi = 0; hi < 2; hi++) {
+        if (L->grad == 1) {
+            lump_setb(L, g[0], g[2], 0, hi);
+            lump_setb(L, g[1], NULL, 0, hi);
+        } else {
+            lump_setb(L, g[0], g[4], 0, hi);
+            for (int k = 1; k <= 3; k++) lump_setb(L, g[k], NULL, 0, hi);
+            lump_setb(L, g[1], g[3], 1, hi);
+            lump_setb(L, g[0], NULL, 1, hi);
+            lump_setb(L, g[2], NULL, 1, hi);
+            lump_setb(L, g[4], NULL, 1, hi);
+        }
+    }
+}
+static void olat_prop2l(const olat *L, const double *gin_, const double *G, double S, double *gout, int backward) {
+    int g = L->grad - 1, K = L->K, M = L->M;
+    int e[2] = {L->st[0], L->grad == 2 ? L->st[1] : 0};
+    double Lw = (1.0 - S) / 4.0;
+    double *gin = malloc(sizeof(double) * K * M);
+    memcpy(gin, gin_, sizeof(double) * K * M);
+    olat_set_boundaries_lumped(L, gin);
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(L, z)) continue;
+        for (int kk = 0; kk < K; kk++) {
+            double acc = 0; int first = 1;
+            for (int kp = 0; kp < K; kp++) {
+                double w = lump_w(g, kk, kp, S, Lw);
+                if (w == 0.0) continue;
+                int src;
+                if (!backward) src = (LUMP_AXIS[g][kk] >= 0) ? z - LUMP_SGN[g][kk] * e[LUMP_AXIS[g][kk]] : z;
+                else src = (LUMP_AXIS[g][kp] >= 0) ? z + LUMP_SGN[g][kp] * e[LUMP_AXIS[g][kp]] : z;
+                double t = w * gin[(size_t)kp * M + src];
+                if (first) { acc = t; first = 0; } else acc += t;
+            }
+            gout[(size_t)kk * M + z] = acc * G[z];
+        }
+    }
+    /* boundary entries: surface layers keep their (boundary-set) value, 0
+       for a propagator; the others copy as the next step's SetB calls do */
+    for (int z = 0; z < M; z++)
+        if (!is_interior(L, z) && mapped_site(L, z, NULL) == z)
+            for (int k = 0; k < K; k++) gout[(size_t)k * M + z] = gin[(size_t)k * M + z];
+    olat_set_boundaries_lumped(L, gout);
+    free(gin);
+}
+static double comp_mult(int K, int k) {
+    if (K == 3 && k == 1) return 4.0;
+    if (K == 5 && k == 2) return 2.0;
+    return 1.0;
+}
+
 /* lnGN of an end-point distribution: Lat1DFlat1stO.cpp:301-316,
    Lat2DFlat1stO.cpp:293-342, Lat2DCyl1stO.cpp:388-438, Lat3D1stO.cpp:344-370,
    Lat3D2ndO.cpp:995-1025 (sum of the six components over 6) */
 static double olat_lngn(const olat *L, const double *G) {
     double v = 0;
-    int K = (L->order == 2) ? 6 : 1;
-    for (int k = 0; k < K; k++)
-        for (int z = 0; z < L->M; z++) v += L->w_gn[z] * G[k * L->M + z];
-    if (K == 6) v /= 6.0;
+    int K = L->K;
+    for (int k = 0; k < K; k++) {
+        double mu = comp_mult(K, k);
+        for (int z = 0; z < L->M; z++)
+            v += (mu == 1.0) ? L->w_gn[z] * G[k * L->M + z] : L->w_gn[z] * (G[k * L->M + z] * mu);
+    }
+    if (K > 1) v /= 6.0;   /* six bond directions, lumped or not */
     return log(v);
 }
 
@@ -556,7 +673,8 @@ static void update_swf(orc_system *s, const double *x) {
 }
 
 static void propagate_any(const orc_system *s, const double *gin, const double *G, double S, double *gout, int backward) {
-    if (s->L.order == 2) olat_prop2(&s->L, gin, G, S, gout, backward);
+    if (s->L.order == 2 && s->L.grad == 3) olat_prop2(&s->L, gin, G, S, gout, backward);
+    else if (s->L.order == 2) olat_prop2l(&s->L, gin, G, S, gout, backward);
     else olat_prop1(&s->L, gin, G, gout);
 }
 
@@ -567,7 +685,7 @@ static void propagate_any(const orc_system *s, const double *gin, const double *
    SF_Copol2ndO::Matrix1 (SF_Copol2ndO.cpp:250-356) */
 static void molecule_phi(orc_system *s, omol *o) {
     olat *L = &s->L;
-    int M = L->M, N = o->N, K = (L->order == 2) ? 6 : 1;
+    int M = L->M, N = o->N, K = L->K;
     size_t KM = (size_t)K * M;
     for (int a = 0; a < o->nseg_used; a++) memset(o->phi + (size_t)o->used[a] * M, 0, sizeof(double) * M);
     if (o->type == 0) {
@@ -644,8 +762,13 @@ static void molecule_phi(orc_system *s, omol *o) {
     {
         double *phi = o->phi + (size_t)o->seg[N - 1] * M;
         const double *Gf = Gi + (size_t)(N - 1) * KM;
-        for (int k = 0; k < K; k++)
-            for (int z = 0; z < M; z++) phi[z] += Ginv[(size_t)k * M + z] * Gf[(size_t)k * M + z];
+        for (int k = 0; k < K; k++) {
+            double mu = comp_mult(K, k);
+            for (int z = 0; z < M; z++) {
+                double v = Ginv[(size_t)k * M + z] * Gf[(size_t)k * M + z];
+                phi[z] += (mu == 1.0) ? v : v * mu;
+            }
+        }
     }
     for (int t = N - 2; t >= 0; t--) {
         int sg = o->seg[t];
@@ -654,8 +777,13 @@ static void molecule_phi(orc_system *s, omol *o) {
         memcpy(Ginv, tmp, sizeof(double) * KM);
         double *phi = o->phi + (size_t)sg * M;
         const double *Gf = Gi + (size_t)t * KM;
-        for (int k = 0; k < K; k++)
-            for (int z = 0; z < M; z++) phi[z] += Ginv[(size_t)k * M + z] * Gf[(size_t)k * M + z];
+        for (int k = 0; k < K; k++) {
+            double mu = comp_mult(K, k);
+            for (int z = 0; z < M; z++) {
+                double v = Ginv[(size_t)k * M + z] * Gf[(size_t)k * M + z];
+                phi[z] += (mu == 1.0) ? v : v * mu;
+            }
+        }
     }
     o->lngn = olat_lngn(L, Ginv);
     for (int a = 0; a < o->nseg_used; a++) {
@@ -668,10 +796,10 @@ static void molecule_phi(orc_system *s, omol *o) {
     if (o->freedom == SFGPU_MOL_RESTRICTED) {
         o->lnc = log(o->theta) - o->lngn - log(1.0 * N);
         o->phibulk = o->theta / exp(o->lngn);
-        norm = (o->theta / N) / (K == 6 ? 6.0 * exp(o->lngn) : exp(o->lngn));
+        norm = (o->theta / N) / (K > 1 ? 6.0 * exp(o->lngn) : exp(o->lngn));
     } else {
         o->lnc = log(o->phibulk / N);
-        norm = o->phibulk / (K == 6 ? 6.0 * N : (double)N);
+        norm = o->phibulk / (K > 1 ? 6.0 * N : (double)N);
     }
     for (int a = 0; a < o->nseg_used; a++) {
         double *phi = o->phi + (size_t)o->used[a] * M;
@@ -806,10 +934,12 @@ double orc_free_energy(orc_system *s) {
 }
 
 int orc_propagate(const orc_system *s, const double *gin, const double *g, double *gout, double S, int backward) {
-    int M = s->L.M, K = (s->L.order == 2) ? 6 : 1;
+    int M = s->L.M, K = s->L.K;
     double *tmp = malloc(sizeof(double) * K * M);
     memcpy(tmp, gin, sizeof(double) * K * M);
-    if (K == 6) olat_set_boundaries6(&s->L, tmp); else olat_set_boundaries(&s->L, tmp);
+    if (K == 6) olat_set_boundaries6(&s->L, tmp);
+    else if (K > 1) olat_set_boundaries_lumped(&s->L, tmp);
+    else olat_set_boundaries(&s->L, tmp);
     propagate_any(s, tmp, g, S, gout, backward);
     free(tmp);
     return SFGPU_OK;

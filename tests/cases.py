@@ -49,6 +49,51 @@ def _flat1d_mirror2_layeradj():
     return spec
 
 
+def _flat1d_2nd():
+    """Lat1D2ndO: surface with an adsorbing frozen layer below, mirror2 above
+    (the upper side swaps the +x/-x components there, the lower side does not
+    for mirror2), stiff A chains (S = 0.5) in solvent."""
+    lat = Lattice(1, [24, 0, 0], [BOUND_SURFACE, 0, 0], [BOUND_MIRROR2, 0, 0], order=2, lam=1 / 6)
+    M = lat.M
+    surf = np.zeros(M)
+    surf[0] = 1.0
+    segs = [Segment("S", SEG_FROZEN, surf), Segment("A"), Segment("W")]
+    chi = np.zeros((3, 3))
+    chi[0, 1] = chi[1, 0] = -1.2
+    chi[1, 2] = chi[2, 1] = 0.6
+    pf = np.full((3, 3), 0.2)
+    pf[1, 1] = 0.5
+    mols = [Molecule("A", [(1, 15)], MOL_FREE, phibulk=0.02), Molecule("W", [(2, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols, pf=pf)
+
+
+def _flat2d_2nd():
+    """Lat2D2ndO: mirror2 below in x (no swap) and mirror1 above, surface and
+    mirror2 in y; an AB copolymer with stiffness across the junction, a
+    restricted homopolymer and solvent."""
+    lat = Lattice(2, [11, 9, 0], [BOUND_MIRROR2, BOUND_SURFACE, 0], [BOUND_MIRROR1, BOUND_MIRROR2, 0], order=2,
+                  lam=1 / 6)
+    segs = [Segment("A"), Segment("B"), Segment("W")]
+    chi = np.array([[0, 0.4, 1.0], [0.4, 0, 0.1], [1.0, 0.1, 0]])
+    pf = np.full((3, 3), 0.2)
+    pf[0, 0], pf[0, 1], pf[1, 0] = 0.45, 0.3, 0.3
+    mols = [Molecule("AB", [(0, 6), (1, 5)], MOL_FREE, phibulk=0.05),
+            Molecule("h", [(1, 7)], MOL_RESTRICTED, theta=4.0),
+            Molecule("W", [(2, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols, pf=pf)
+
+
+def _flat2d_2nd_periodic():
+    """Lat2D2ndO with periodic x (no swaps) and surface/mirror1 y."""
+    lat = Lattice(2, [8, 7, 0], [BOUND_PERIODIC, BOUND_SURFACE, 0], [BOUND_PERIODIC, BOUND_MIRROR1, 0], order=2,
+                  lam=1 / 6)
+    segs = [Segment("A"), Segment("W")]
+    chi = np.array([[0, 0.8], [0.8, 0]])
+    pf = np.full((2, 2), 0.3)
+    mols = [Molecule("A", [(0, 9)], MOL_FREE, phibulk=0.04), Molecule("W", [(1, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols, pf=pf)
+
+
 CASES = {
     "1d_surface": lambda: configs.flat_adsorption(n=40, N=21)[0],
     "1d_surface_even": lambda: configs.flat_adsorption(n=17, N=30, phib=0.002, chi_aw=0.2, chi_as=-2.0)[0],
@@ -59,7 +104,13 @@ CASES = {
     "3d_periodic_melt": lambda: configs.melt3d(n=9, nA=7, nB=6)[0],
     "3d_mirror_mix": _melt_mirror,
     "3d_2nd_brush": lambda: configs.brush3d(n=6, N=15, sigma=0.2, S=0.5)[0],
+    "1d_2nd_lumped": _flat1d_2nd,
+    "2d_2nd_lumped": _flat2d_2nd,
+    "2d_2nd_lumped_periodic": _flat2d_2nd_periodic,
 }
+
+# cases whose derivatives (forward and reverse mode) are implemented
+DIFFERENTIABLE = sorted(k for k in CASES if "lumped" not in k)
 
 
 def random_x(spec, seed=7, scale=0.3):

@@ -131,3 +131,120 @@ def test_second_order_isotropic_limit_reduces_to_first_order_walk_count():
     w = o.site_weights() > 0
     for k in range(6):
         np.testing.assert_allclose(out[k * o.M:(k + 1) * o.M][w], 1.0, rtol=1e-15)
+
+
+def _lumped_and_3d(grad, bx, by=None, n=(7, 6), N=8, S=0.45, seed=5):
+    """The same free chain (S stiffness) in solvent on a lumped 1D/2D
+    second-order lattice and on the 3D six-direction lattice made homogeneous
+    along the lumped gradients (periodic, 3 layers), with potentials that
+    depend on the modelled coordinates only."""
+    from field_b200.desc import Lattice, Molecule, MOL_FREE, MOL_SOLVENT, Segment, SystemSpec
+    segs = [Segment("A"), Segment("W")]
+    chi = np.array([[0, 0.7], [0.7, 0]])
+    pf = np.full((2, 2), 0.2)
+    pf[0, 0] = S
+    mols = [Molecule("A", [(0, N)], MOL_FREE, phibulk=0.05), Molecule("W", [(1, 1)], MOL_SOLVENT)]
+    P = BOUND_PERIODIC
+    if grad == 1:
+        lo, hi = [bx[0], 0, 0], [bx[1], 0, 0]
+        lat = Lattice(1, [n[0], 0, 0], lo, hi, order=2, lam=1 / 6)
+        lat3 = Lattice(3, [n[0], 3, 3], [bx[0], P, P], [bx[1], P, P], order=2)
+    else:
+        lat = Lattice(2, [n[0], n[1], 0], [bx[0], by[0], 0], [bx[1], by[1], 0], order=2, lam=1 / 6)
+        lat3 = Lattice(3, [n[0], n[1], 3], [bx[0], by[0], P], [bx[1], by[1], P], order=2)
+    s1 = SystemSpec(lat, segs, chi, mols, pf=pf)
+    s3 = SystemSpec(lat3, segs, chi, mols, pf=pf)
+    o1, o3 = Oracle(s1), Oracle(s3)
+    nc = s1.class_layout()[1]
+    x1 = np.random.default_rng(seed).normal(0.0, 0.2, o1.nvar)
+    # the 3D sites' potentials: those of the same modelled coordinates
+    sites1, sites3 = s1.itvar_sites(), s3.itvar_sites()
+    sh1, sh3 = lat.shape, lat3.shape
+    key1 = {tuple(np.unravel_index(z, sh1)): j for j, z in enumerate(sites1)}
+    x3 = np.empty(o3.nvar)
+    for j, z in enumerate(sites3):
+        c = np.unravel_index(z, sh3)
+        j1 = key1[tuple(c[:grad])]
+        x3[j * nc:(j + 1) * nc] = x1[j1 * nc:(j1 + 1) * nc]
+    return s1, s3, o1, o3, x1, x3
+
+
+@pytest.mark.parametrize("grad,bx,by", [(1, (BOUND_MIRROR1, BOUND_MIRROR1), None),
+                                        (1, (BOUND_PERIODIC, BOUND_PERIODIC), None),
+                                        (2, (BOUND_MIRROR1, BOUND_MIRROR1), (BOUND_PERIODIC, BOUND_PERIODIC)),
+                                        (2, (BOUND_PERIODIC, BOUND_PERIODIC), (BOUND_MIRROR1, BOUND_MIRROR1))])
+def test_lumped_second_order_equals_3d(grad, bx, by):
+    """Lat1D2ndO / Lat2D2ndO lump the bond directions along homogeneous
+    gradients (lateral x4, z x2).  On a 3D lattice homogeneous along those
+    gradients the six-direction model must give the same profiles, residual
+    and free energy per site, and lnGN larger by ln(sites per modelled
+    site) -- an independent check of the lumped weights, multiplicities and
+    mirror swaps."""
+    s1, s3, o1, o3, x1, x3 = _lumped_and_3d(grad, bx, by)
+    f1, f3 = o1.residual(x1), o3.residual(x3)
+    sh1, sh3 = s1.lattice.shape, s3.lattice.shape
+    reps = 3 ** (3 - grad)   # 3D sites per modelled site
+    for i in range(2):
+        p1 = o1.phi(i).reshape(sh1)
+        p3 = o3.phi(i).reshape(sh3)
+        inner1 = p1[(slice(1, -1),) * grad]
+        for idx in np.ndindex(*sh3[grad:]):
+            if any(v == 0 or v == sh3[grad + k] - 1 for k, v in enumerate(idx)):
+                continue
+            inner3 = p3[(slice(1, -1),) * grad + idx]
+            np.testing.assert_allclose(inner3, inner1, rtol=1e-12, atol=1e-15)
+    for m in range(2):
+        assert o3.lngn(m) == pytest.approx(o1.lngn(m) + np.log(reps), rel=1e-12, abs=1e-12)
+    # residual of every 3D site equals that of its modelled site
+    nc = s1.class_layout()[1]
+    sites1, sites3 = s1.itvar_sites(), s3.itvar_sites()
+    key1 = {tuple(np.unravel_index(z, sh1)): j for j, z in enumerate(sites1)}
+    for j, z in enumerate(sites3):
+        j1 = key1[tuple(np.unravel_index(z, sh3)[:grad])]
+        np.testing.assert_allclose(f3[j * nc:(j + 1) * nc], f1[j1 * nc:(j1 + 1) * nc], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("grad", [1, 2])
+def test_lumped_second_order_step_conserves_weight(grad):
+    """G = 1 and every component 1: each W row sums to S + 4L = 1, so one
+    step (forward and backward) keeps every interior component at 1 on a
+    periodic lattice."""
+    from field_b200.desc import Lattice, Molecule, MOL_SOLVENT, Segment, SystemSpec
+    P = BOUND_PERIODIC
+    lat = Lattice(grad, [6, 5, 0][:3], [P, P if grad == 2 else 0, 0], [P, P if grad == 2 else 0, 0], order=2)
+    spec = SystemSpec(lat, [Segment("W")], np.zeros((1, 1)), [Molecule("W", [(0, 1)], MOL_SOLVENT)])
+    o = Oracle(spec)
+    K = lat.components
+    sh = lat.shape
+    for bw in (0, 1):
+        out = o.propagate(np.ones(K * o.M), np.ones(o.M), S=0.37, backward=bw).reshape((K,) + sh)
+        inner = out[(slice(None),) + (slice(1, -1),) * grad]
+        np.testing.assert_allclose(inner, 1.0, rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("grad", [1, 2])
+@pytest.mark.parametrize("freedom", ["free", "restricted"])
+def test_lumped_second_order_mass_sum_rule(grad, freedom):
+    """With a surface below and mirror1 above (and periodic y in 2D) every
+    bond direction is counted once: sum_z w phi_A = phibulk * GN for a free
+    chain and = theta for a restricted one.  Surface layers of the stored
+    propagators stay 0, so the sum is finite and exact."""
+    from field_b200.desc import (Lattice, Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, Segment, SystemSpec,
+                                 BOUND_SURFACE)
+    if grad == 1:
+        lat = Lattice(1, [9, 0, 0], [BOUND_SURFACE, 0, 0], [BOUND_MIRROR1, 0, 0], order=2, lam=1 / 6)
+    else:
+        lat = Lattice(2, [9, 7, 0], [BOUND_SURFACE, BOUND_PERIODIC, 0], [BOUND_MIRROR1, BOUND_PERIODIC, 0],
+                      order=2, lam=1 / 6)
+    segs = [Segment("A"), Segment("W")]
+    chi = np.array([[0, 0.7], [0.7, 0]])
+    pf = np.full((2, 2), 0.3)
+    a = (Molecule("A", [(0, 12)], MOL_FREE, phibulk=0.05) if freedom == "free"
+         else Molecule("A", [(0, 12)], MOL_RESTRICTED, theta=3.0))
+    spec = SystemSpec(lat, segs, chi, [a, Molecule("W", [(1, 1)], MOL_SOLVENT)], pf=pf)
+    o = Oracle(spec)
+    f = o.residual(np.random.default_rng(1).normal(0.0, 0.3, o.nvar))
+    assert np.all(np.isfinite(f))
+    tot = float((o.phi(0) * o.site_weights()).sum())
+    want = o.phibulk(0) * np.exp(o.lngn(0)) if freedom == "free" else 3.0
+    assert tot == pytest.approx(want, rel=1e-13)
