@@ -431,6 +431,35 @@ static __global__ void connect(int M, int K, const double *__restrict__ a, const
     }
 }
 
+// Bond-orientation composition, the OUT/PHI argument of the second-order
+// ConnectG (Lat3D2ndO.cpp:905-918, Lat2D2ndO.cpp:285-304,
+// Lat1D2ndO.cpp:215-227): the product of component k of the two propagators
+// is added to the slot of k's bond axis.  3D: +-x -> 0, +-y -> 1, +-z -> 2.
+// 1D: +-x -> 0, the lateral group (times 4) -> 1.  2D follows SFbox's slot
+// selection as written: k = 3 (-y) keeps the slot of k = 2 and k = 4 (-x)
+// goes to slot 1, and the z group's product is added to slot 2 a second
+// time after the loop.  Interior sites only; boundary entries stay 0.
+__host__ __device__ inline int orient_slot(int K, int k) {
+    if (K == 6) { const int s6[6] = {0, 1, 2, 2, 1, 0}; return s6[k]; }
+    if (K == 5) { const int s5[5] = {0, 1, 2, 2, 1}; return s5[k]; }
+    return (k == 1) ? 1 : 0;
+}
+static __global__ void orient_acc(DLat L, const double *__restrict__ a, const double *__restrict__ b,
+                                  double *__restrict__ out) {
+    const int M = L.M, K = L.K;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+        int c[3];
+        lat_coords(L, r, c);
+        if (!lat_interior(L, c)) continue;
+        for (int k = 0; k < K; k++) {
+            double v = a[(size_t)k * M + r] * b[(size_t)k * M + r];
+            if (K == 3 && k == 1) v = v * 4.0;
+            out[(size_t)orient_slot(K, k) * M + r] += v;
+        }
+        if (K == 5) out[2 * (size_t)M + r] += a[2 * (size_t)M + r] * b[2 * (size_t)M + r];
+    }
+}
+
 // copy a full lattice vector into K components (Gi[.][1] = G, Gi_inv = G)
 static __global__ void replicate(int M, int K, const double *__restrict__ g, double *__restrict__ out) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x)

@@ -471,6 +471,11 @@ int sfgpu_system::molecule_phi(int m) {
     replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[N - 1]], ginv);
     if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, ginv);
     connect<<<g, kBlock, 0, s>>>(M, K, ginv, d_gi + (size_t)(N - 1) * KM, o.d_phi[o.seg[N - 1]]);
+    const bool ori = orient && K > 1;
+    if (ori) {
+        for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_ori[i], 0, sizeof(double) * mphi() * M, s));
+        orient_acc<<<g, kBlock, 0, s>>>(L, ginv, d_gi + (size_t)(N - 1) * KM, o.d_ori[o.seg[N - 1]]);
+    }
     const double *cur = ginv;
     std::swap(ginv, tmp);
     for (int t = N - 2; t >= 0; t--) {
@@ -483,6 +488,7 @@ int sfgpu_system::molecule_phi(int m) {
         else
             step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv,
                                         d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC, 1);
+        if (ori) orient_acc<<<g, kBlock, 0, s>>>(L, ginv, d_gi + (size_t)t * KM, o.d_ori[sg]);
         cur = ginv; std::swap(ginv, tmp);
     }
     wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, cur, d_wgn, d_partial);
@@ -490,7 +496,32 @@ int sfgpu_system::molecule_phi(int m) {
     for (int i : o.used) {
         finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], scal, m, 0);
         set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_phi[i]);
+        // CorrectDoubleCountG / NormPhi* on the orientation slots
+        // (Lat3D2ndO.cpp:986-993, :1031-1046)
+        if (ori)
+            for (int a = 0; a < mphi(); a++)
+                finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_ori[i] + (size_t)a * M, scal, m, 0);
     }
+    return SFGPU_OK;
+}
+
+// Bond-orientation profiles (SF_Homopol2ndO::GetBondOrientation,
+// SF_Homopol2ndO.cpp:82-90; SF_Copol2ndO.cpp:108-116): per molecule and
+// segment type mphi profiles, filled by the residual evaluations that follow.
+int sfgpu_system::set_orientation(int enable) {
+    if (K == 1) return fail(SFGPU_ERR_UNSUPPORTED, "bond orientation needs a second-order lattice");
+    if (enable && !d_ori_sum) {
+        int rc = alloc_d(&d_ori_sum, M);
+        if (rc) return rc;
+        for (auto &o : mols) {
+            o.d_ori.assign(nseg, nullptr);
+            for (int i : o.used) {
+                if ((rc = alloc_d(&o.d_ori[i], (size_t)mphi() * M))) return rc;
+                SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_ori[i], 0, sizeof(double) * mphi() * M, stream));
+            }
+        }
+    }
+    orient = enable != 0;
     return SFGPU_OK;
 }
 
@@ -655,6 +686,27 @@ extern "C" int sfgpu_get_mol_scalars(sfgpu_system *s, int mol, double *lngn, dou
     if (lngn) *lngn = v.lngn;
     if (phibulk) *phibulk = v.phibulk;
     if (lnc) *lnc = v.lnc;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_set_bond_orientation(sfgpu_system *s, int enable) {
+    CHECK_SYS(s);
+    return s->set_orientation(enable);
+}
+
+extern "C" int sfgpu_get_bond_orientation(sfgpu_system *s, int mol, int axis, double *out) {
+    CHECK_SYS(s);
+    if (!out) return fail(SFGPU_ERR_INVALID, "null output");
+    if (!s->orient) return fail(SFGPU_ERR_INVALID, "bond orientation is not enabled");
+    if (mol < 0 || mol >= s->nmol) return fail(SFGPU_ERR_INVALID, "molecule index");
+    if (axis < 0 || axis >= s->mphi()) return fail(SFGPU_ERR_INVALID, "axis out of range for this lattice");
+    const HMol &o = s->mols[mol];
+    PtrList pl; pl.n = 0;
+    for (int i : o.used) pl.p[pl.n++] = o.d_ori[i] + (size_t)axis * s->M;
+    sum_profiles<<<grid_for(s->M), kBlock, 0, s->stream>>>(s->M, pl, s->d_ori_sum);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(out, s->d_ori_sum, sizeof(double) * s->M, cudaMemcpyDeviceToHost, s->stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return SFGPU_OK;
 }
 

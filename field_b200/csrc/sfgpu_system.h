@@ -15,6 +15,7 @@ struct HMol {
     std::vector<int> seg, used, count;
     std::vector<double *> d_phi;      // per segment (used ones)
     std::vector<double *> d_dphi;     // tangents (allocated on first J*v)
+    std::vector<double *> d_ori;      // bond orientation per segment, mphi*M (when enabled)
 };
 
 struct sfgpu_system {
@@ -37,6 +38,11 @@ struct sfgpu_system {
     double *d_x = nullptr, *d_f = nullptr;
     int nblocks_red = 1;
     int tile_xc = 8;          // x planes per block of the 3D first-order step
+    // bond-orientation profiles of second-order lattices (off by default)
+    bool orient = false;
+    double *d_ori_sum = nullptr;
+    int mphi() const { return K == 3 ? 2 : 3; }
+    int set_orientation(int enable);
     // forward-mode tangent buffers, allocated on the first J*v
     bool t_ready = false;
     std::vector<double *> dgfull, dgseg, dphi;

@@ -102,6 +102,21 @@ class System:
                   "sfgpu_get_mol_scalars")
         return {"lngn": a.value, "phibulk": b.value, "lnc": c.value}
 
+    def set_bond_orientation(self, enable: bool = True):
+        """Fill bond-orientation profiles in the following evaluations
+        (second-order lattices; Lat2ndO::ConnectG with PHI)."""
+        nat.check(self.lib.sfgpu_system_set_bond_orientation(self.h, int(bool(enable))),
+                  "sfgpu_system_set_bond_orientation")
+
+    def bond_orientation(self, mol: int, axis: int) -> np.ndarray:
+        """Molecule mol's bond-orientation profile along axis 0 (x), 1 (y, yz
+        in 1D) or 2 (z), summed over its segment types
+        (SF_Copol2ndO::GetBondOrientation)."""
+        out = np.empty(self.M)
+        nat.check(self.lib.sfgpu_get_bond_orientation(self.h, int(mol), int(axis), _d(out)),
+                  "sfgpu_get_bond_orientation")
+        return out
+
     def free_energy(self) -> float:
         F = C.c_double()
         nat.check(self.lib.sfgpu_free_energy(self.h, C.byref(F)), "sfgpu_free_energy")

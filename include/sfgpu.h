@@ -76,7 +76,8 @@ extern "C" {
 typedef struct {
     int    gradients;          /* 1, 2 or 3 */
     int    geometry;           /* SFGPU_GEOM_*; cylindrical only with 2 gradients */
-    int    order;              /* 1 = first-order chains, 2 = semiflexible (3D) */
+    int    order;              /* 1 = first-order chains, 2 = semiflexible (3D,
+                                  and flat 1D/2D with lumped directions) */
     int    n_layers[3];        /* interior layers per gradient (unused entries 0) */
     int    bound_lo[3];        /* SFGPU_BOUND_* per gradient */
     int    bound_hi[3];
@@ -159,6 +160,20 @@ int sfgpu_get_phi(sfgpu_system *sys, int segment, double *phi);
 int sfgpu_get_mol_phi(sfgpu_system *sys, int molecule, int segment, double *phi);
 int sfgpu_get_swf(sfgpu_system *sys, int segment, double *g);
 int sfgpu_get_mol_scalars(sfgpu_system *sys, int molecule, double *lngn, double *phibulk, double *lnc);
+/* Bond-orientation profiles of second-order lattices: the orientation-
+ * resolved composition of Lat2ndO::ConnectG(..., PHI) (Lat2ndO.h:7-66;
+ * Lat3D2ndO.cpp:905-918, Lat2D2ndO.cpp:285-304, Lat1D2ndO.cpp:215-227),
+ * divided by G and normalised like phi (CorrectDoubleCountG / NormPhi* with
+ * PHI, Lat3D2ndO.cpp:986-993, :1031-1046).  Enabling makes every following
+ * evaluation also fill, per molecule and segment type, mphi = 3 profiles
+ * (2 on Lat1D2ndO) at 2K*8 extra bytes read per site and chain position.
+ * sfgpu_get_bond_orientation copies to host (M doubles) the molecule's
+ * profile of axis 0 = x_dir, 1 = y_dir (yz_dir in 1D), 2 = z_dir, summed
+ * over its segment types as SF_Copol2ndO::GetBondOrientation does
+ * (SF_Copol2ndO.cpp:108-116).  Boundary entries are 0.  First-order
+ * lattices: SFGPU_ERR_UNSUPPORTED. */
+int sfgpu_system_set_bond_orientation(sfgpu_system *sys, int enable);
+int sfgpu_get_bond_orientation(sfgpu_system *sys, int molecule, int axis, double *host_out);
 /* Helmholtz free energy of the last evaluation,
  * SF_MolList1stO::GetFreeEnergy (SF_MolList1stO.cpp:606-635). */
 int sfgpu_free_energy(sfgpu_system *sys, double *F);

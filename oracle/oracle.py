@@ -45,6 +45,7 @@ def lib():
         l.orc_get_phibulk.argtypes = [vp, C.c_int]
         l.orc_get_phibulk.restype = C.c_double
         l.orc_get_swf.argtypes = [vp, C.c_int, dp]
+        l.orc_bond_orientation.argtypes = [vp, C.c_int, C.c_int, dp]
         l.orc_free_energy.argtypes = [vp]
         l.orc_free_energy.restype = C.c_double
         l.orc_propagate.argtypes = [vp, dp, dp, dp, C.c_double, C.c_int]
@@ -99,6 +100,13 @@ class Oracle:
 
     def lngn(self, mol):
         return lib().orc_get_lngn(self.h, mol)
+
+    def bond_orientation(self, mol, axis):
+        out = np.empty(self.M)
+        rc = lib().orc_bond_orientation(self.h, mol, axis, _d(out))
+        if rc:
+            raise ValueError(f"orc_bond_orientation failed with status {rc}")
+        return out
 
     def phibulk(self, mol):
         return lib().orc_get_phibulk(self.h, mol)

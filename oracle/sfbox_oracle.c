@@ -488,6 +488,7 @@ typedef struct {
     int pinned;
     double lngn, lnc, chemintref;
     double *phi;          /* n_segments * M (only used ones nonzero) */
+    double *ori;          /* 2nd order: n_segments * 3 * M bond-orientation slots */
 } omol;
 
 struct orc_system {
@@ -584,6 +585,7 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
         }
         o->chemintref = cr / 2;
         o->phi = calloc((size_t)ns * M, sizeof(double));
+        o->ori = calloc((size_t)ns * 3 * M, sizeof(double));
     }
     if (s->solvent < 0) { orc_destroy(s); return SFGPU_ERR_INVALID; }
 
@@ -636,7 +638,7 @@ void orc_destroy(orc_system *s) {
     if (!s) return;
     olat_free(&s->L);
     for (int m = 0; m < s->nmol; m++) {
-        free(s->mol[m].seg); free(s->mol[m].count); free(s->mol[m].used); free(s->mol[m].phi);
+        free(s->mol[m].seg); free(s->mol[m].count); free(s->mol[m].used); free(s->mol[m].phi); free(s->mol[m].ori);
     }
     free(s->mol); free(s->freedom); free(s->range); free(s->chi); free(s->pf);
     free(s->stateQ); free(s->class_of); free(s->rep_of_class); free(s->sites);
@@ -676,6 +678,28 @@ static void propagate_any(const orc_system *s, const double *gin, const double *
     if (s->L.order == 2 && s->L.grad == 3) olat_prop2(&s->L, gin, G, S, gout, backward);
     else if (s->L.order == 2) olat_prop2l(&s->L, gin, G, S, gout, backward);
     else olat_prop1(&s->L, gin, G, gout);
+}
+
+/* bond-orientation composition, Lat2ndO::ConnectG(..., PHI):
+   Lat3D2ndO.cpp:905-918 (+-x -> 0, +-y -> 1, +-z -> 2), Lat1D2ndO.cpp:215-227
+   (+-x -> 0, lateral group times 4 -> 1), Lat2D2ndO.cpp:285-304 (slot kk of
+   k = 0..4 is 0, 1, 2, then 2 again for k = 3 since kk is not reassigned, and
+   1 for k = 4; the z group is added to slot 2 once more after the loop).
+   Interior sites only (Lat1D2ndO::ConnectG removes the boundaries first). */
+static void orient_acc(const olat *L, const double *a, const double *b, double *out) {
+    static const int s6[6] = {0, 1, 2, 2, 1, 0}, s5[5] = {0, 1, 2, 2, 1}, s3[3] = {0, 1, 0};
+    int M = L->M, K = L->K;
+    const int *sl = (K == 6) ? s6 : (K == 5) ? s5 : s3;
+    for (int k = 0; k < K; k++)
+        for (int z = 0; z < M; z++) {
+            if (!is_interior(L, z)) continue;
+            double v = a[(size_t)k * M + z] * b[(size_t)k * M + z];
+            if (K == 3 && k == 1) v = v * 4.0;
+            out[(size_t)sl[k] * M + z] += v;
+        }
+    if (K == 5)
+        for (int z = 0; z < M; z++)
+            if (is_interior(L, z)) out[2 * (size_t)M + z] += a[2 * (size_t)M + z] * b[2 * (size_t)M + z];
 }
 
 /* one molecule: SF_Monomer1stO::Matrix1 (SF_Monomer1stO.cpp:99-130),
@@ -759,6 +783,10 @@ static void molecule_phi(orc_system *s, omol *o) {
     const double *GN = s->swf + (size_t)o->seg[N - 1] * M;
     for (int k = 0; k < K; k++) memcpy(Ginv + (size_t)k * M, GN, sizeof(double) * M);
     if (K == 6) olat_set_boundaries6(L, Ginv);
+    if (K > 1) {
+        for (int a = 0; a < o->nseg_used; a++) memset(o->ori + (size_t)o->used[a] * 3 * M, 0, sizeof(double) * 3 * M);
+        orient_acc(L, Ginv, Gi + (size_t)(N - 1) * KM, o->ori + (size_t)o->seg[N - 1] * 3 * M);
+    }
     {
         double *phi = o->phi + (size_t)o->seg[N - 1] * M;
         const double *Gf = Gi + (size_t)(N - 1) * KM;
@@ -775,6 +803,7 @@ static void molecule_phi(orc_system *s, omol *o) {
         double S = s->pf[sg * s->nseg + o->seg[t + 1]];
         propagate_any(s, Ginv, s->swf + (size_t)sg * M, S, tmp, 1);
         memcpy(Ginv, tmp, sizeof(double) * KM);
+        if (K > 1) orient_acc(L, Ginv, Gi + (size_t)t * KM, o->ori + (size_t)sg * 3 * M);
         double *phi = o->phi + (size_t)sg * M;
         const double *Gf = Gi + (size_t)t * KM;
         for (int k = 0; k < K; k++) {
@@ -805,6 +834,18 @@ static void molecule_phi(orc_system *s, omol *o) {
         double *phi = o->phi + (size_t)o->used[a] * M;
         for (int z = 0; z < M; z++) phi[z] *= norm;
     }
+    /* CorrectDoubleCountG / NormPhi* on the orientation slots
+       (Lat3D2ndO.cpp:986-993, :1031-1046; Lat1D2ndO.cpp:281-289, :309-327) */
+    if (K > 1)
+        for (int a = 0; a < o->nseg_used; a++) {
+            const double *G = s->swf + (size_t)o->used[a] * M;
+            double *ori = o->ori + (size_t)o->used[a] * 3 * M;
+            for (int sl = 0; sl < 3; sl++)
+                for (int z = 0; z < M; z++) {
+                    double v = ori[(size_t)sl * M + z];
+                    ori[(size_t)sl * M + z] = ((G[z] > 0) ? v / G[z] : 0.0) * norm;
+                }
+        }
     free(Gi); free(Ginv); free(tmp);
 }
 
@@ -1055,4 +1096,21 @@ int orc_solve_diis(orc_system *s, double *x, double tol, int maxit, int m, doubl
     if (final_error) *final_error = err;
     free(g); free(x0); free(XR); free(XX0); free(Aij); free(Ap); free(C);
     return rc;
+}
+
+/* SF_Homopol2ndO::GetBondOrientation (SF_Homopol2ndO.cpp:82-90) and
+   SF_Copol2ndO::GetBondOrientation (SF_Copol2ndO.cpp:108-116): slot axis of
+   the molecule, summed over its segment types */
+int orc_bond_orientation(const orc_system *s, int mol, int axis, double *out) {
+    if (s->L.K == 1 || mol < 0 || mol >= s->nmol) return SFGPU_ERR_INVALID;
+    if (axis < 0 || axis >= (s->L.K == 3 ? 2 : 3)) return SFGPU_ERR_INVALID;
+    const omol *o = &s->mol[mol];
+    int M = s->L.M;
+    for (int z = 0; z < M; z++) out[z] = 0;
+    if (o->type == 0) return SFGPU_OK;
+    for (int a = 0; a < o->nseg_used; a++) {
+        const double *src = o->ori + ((size_t)o->used[a] * 3 + axis) * M;
+        for (int z = 0; z < M; z++) out[z] += src[z];
+    }
+    return SFGPU_OK;
 }

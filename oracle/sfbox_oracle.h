@@ -32,6 +32,7 @@ int    orc_residual(orc_system *s, const double *x, double *f);
 int    orc_get_phi(const orc_system *s, int seg, double *phi);         /* state phi, M */
 int    orc_get_mol_phi(const orc_system *s, int mol, int seg, double *phi);
 double orc_get_lngn(const orc_system *s, int mol);
+int    orc_bond_orientation(const orc_system *s, int mol, int axis, double *out);  /* 2nd order, M */
 double orc_get_phibulk(const orc_system *s, int mol);
 int    orc_get_swf(const orc_system *s, int seg, double *g);           /* segment G (masked) */
 double orc_free_energy(orc_system *s);                                 /* SF_MolList1stO.cpp:606 */

@@ -208,3 +208,38 @@ def test_lumped_derivatives_report_unsupported(gpu_lib):
         assert e.value.code == 7
     # the primal path stays usable afterwards
     assert np.all(np.isfinite(sys_.residual(x)))
+
+
+@pytest.mark.parametrize("case", ["3d_2nd_brush", "1d_2nd_lumped", "2d_2nd_lumped", "2d_2nd_lumped_periodic"])
+def test_bond_orientation(gpu_lib, case):
+    """Bond-orientation profiles of the second-order lattices against the
+    oracle, per molecule and axis."""
+    spec = CASES[case]()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    x = random_x(spec, seed=21)
+    sys_.set_bond_orientation(True)
+    sys_.residual(x)
+    o.residual(x)
+    na = 2 if sys_.K == 3 else 3
+    for m in range(len(spec.molecules)):
+        for a in range(na):
+            want = o.bond_orientation(m, a)
+            got = sys_.bond_orientation(m, a)
+            assert np.max(np.abs(got - want)) <= TOL_EVAL * max(np.max(np.abs(want)), 1e-300), (m, a)
+    from field_b200._native import SfgpuError
+    with pytest.raises(SfgpuError):
+        sys_.bond_orientation(0, na)
+
+
+def test_bond_orientation_errors(gpu_lib):
+    """First-order lattices have no bond orientation; a second-order system
+    reports it only once enabled."""
+    from field_b200._native import SfgpuError
+    s1 = System(CASES["1d_surface"]())
+    with pytest.raises(SfgpuError) as e:
+        s1.set_bond_orientation(True)
+    assert e.value.code == 7
+    s2 = System(CASES["3d_2nd_brush"]())
+    with pytest.raises(SfgpuError):
+        s2.bond_orientation(0, 0)

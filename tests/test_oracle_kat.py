@@ -248,3 +248,43 @@ def test_lumped_second_order_mass_sum_rule(grad, freedom):
     tot = float((o.phi(0) * o.site_weights()).sum())
     want = o.phibulk(0) * np.exp(o.lngn(0)) if freedom == "free" else 3.0
     assert tot == pytest.approx(want, rel=1e-13)
+
+
+@pytest.mark.parametrize("case", ["3d_2nd_brush", "1d_2nd_lumped", "2d_2nd_lumped"])
+def test_bond_orientation_slots_sum_to_phi(case):
+    """Every direction component lands in one orientation slot (the 2D slot
+    selection included), so on interior sites the slots add up to the
+    molecule's phi; boundary entries are 0."""
+    from cases import CASES, random_x
+    spec = CASES[case]()
+    o = Oracle(spec)
+    o.residual(random_x(spec))
+    inner = np.zeros(spec.lattice.shape, bool)
+    inner[(slice(1, -1),) * spec.lattice.gradients] = True
+    inner = inner.ravel()
+    na = 2 if spec.lattice.components == 3 else 3
+    for m, mol in enumerate(spec.molecules):
+        if sum(n for _, n in mol.blocks) == 1:
+            continue
+        tot = sum(o.bond_orientation(m, a) for a in range(na))
+        phim = sum(o.mol_phi(m, i) for i in sorted({b[0] for b in mol.blocks}))
+        np.testing.assert_allclose(tot[inner], phim[inner], rtol=1e-13, atol=1e-16)
+        assert not np.any(tot[~inner])
+
+
+def test_bond_orientation_isotropic_melt():
+    """u = 0 on a periodic 3D second-order lattice: every bond direction is
+    equally likely, so each of the three axis slots holds phi / 3."""
+    from field_b200.desc import Lattice, Molecule, MOL_FREE, MOL_SOLVENT, Segment, SystemSpec
+    P = BOUND_PERIODIC
+    lat = Lattice(3, [5, 4, 6], [P, P, P], [P, P, P], order=2)
+    spec = SystemSpec(lat, [Segment("A"), Segment("W")], np.zeros((2, 2)),
+                      [Molecule("A", [(0, 7)], MOL_FREE, phibulk=0.3), Molecule("W", [(1, 1)], MOL_SOLVENT)],
+                      pf=np.full((2, 2), 0.35))
+    o = Oracle(spec)
+    o.residual(np.zeros(o.nvar))
+    inner = np.zeros(lat.shape, bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    inner = inner.ravel()
+    for a in range(3):
+        np.testing.assert_allclose(o.bond_orientation(0, a)[inner], 0.1, rtol=1e-13)
