@@ -23,6 +23,13 @@ __device__ __forceinline__ void scatter1(const DLat &L, const RowInfo &R, int k,
     const int km = R.base + ((k == 1) ? L.map_lo[d] : k - 1);
     const int kp = R.base + ((k == nlast) ? L.map_hi[d] : k + 1);
     if (L.grad == 1) {
+        if (L.cyl) {
+            const double lm = L.lam_m[t], lp = L.lam_p[t];
+            atomicAdd(out + t, (1.0 - lm - lp) * y);
+            atomicAdd(out + km, lm * y);
+            atomicAdd(out + kp, lp * y);
+            return;
+        }
         atomicAdd(out + t, (1.0 - 2.0 * L.l1) * y);
         atomicAdd(out + km, L.l1 * y);
         atomicAdd(out + kp, L.l1 * y);
@@ -217,6 +224,13 @@ __device__ __forceinline__ void side_scatter(const DLat &L, int z, double y, dou
         return;
     }
     const double l = L.l1chi;
+    if (L.grad == 1 && L.cyl) {
+        const double lm = L.lamc_m[z], lp = L.lamc_p[z];
+        atomicAdd(out + z, (1.0 - lp - lm) * y);
+        atomicAdd(out + at(c[0] + 1, 0, 0), lp * y);
+        atomicAdd(out + at(c[0] - 1, 0, 0), lm * y);
+        return;
+    }
     if (L.grad == 1) {
         atomicAdd(out + z, (1.0 - 2.0 * l) * y);
         atomicAdd(out + at(c[0] - 1, 0, 0), l * y);
@@ -317,6 +331,31 @@ __device__ inline void side_fraction_adj(const DLat &L, int z, double y, double 
         return;
     }
     const double l = L.l1chi;
+    if (L.grad == 1 && L.cyl) {
+        int zz = z;
+        if (z == 0) {
+            if (L.bc_lo[0] == SFGPU_BOUND_SURFACE) {
+                const double lp = L.lamc_p[0];
+                side_put(L, 0, (1.0 - 2.0 * lp) * y, out);
+                side_put(L, 1, lp * y, out);
+                return;
+            }
+            zz = L.map_lo[0];
+        } else if (z == L.M - 1) {
+            if (L.bc_hi[0] == SFGPU_BOUND_SURFACE) {
+                const double lm = L.lamc_m[z];
+                side_put(L, z, (1.0 - 2.0 * lm) * y, out);
+                side_put(L, z - 1, lm * y, out);
+                return;
+            }
+            zz = L.map_hi[0];
+        }
+        const double lm = L.lamc_m[zz], lp = L.lamc_p[zz];
+        side_put(L, zz, (1.0 - lp - lm) * y, out);
+        side_put(L, zz + 1, lp * y, out);
+        side_put(L, zz - 1, lm * y, out);
+        return;
+    }
     if (L.grad == 1) {
         int zz = z;
         if (z == 0) {

@@ -24,7 +24,11 @@ struct DLat {
     int bc_lo[3], bc_hi[3];    // SFGPU_BOUND_*
     int map_lo[3], map_hi[3];  // coordinate copied into 0 / Md-1
     double l1, l1chi;
-    const double *lam_m, *lam_p;   // cylinder tables by x (device)
+    // curved lattices (2D cylinder; 1D cylinder and sphere): step
+    // probabilities to the inner / outer neighbour by radial coordinate x,
+    // for propagators (lam_*) and contact averages (lamc_*, lambda_chi)
+    const double *lam_m, *lam_p;
+    const double *lamc_m, *lamc_p;
     // second order: direction components (6 in 3D; 1D and 2D lump the
     // directions along the homogeneous gradients: 3 and 5), and whether a
     // step that reads across the lower / upper boundary of gradient d swaps
@@ -88,6 +92,7 @@ __device__ inline int swap_dir(int k, int sw) {
 __device__ __forceinline__ double stencil1(const DLat &L, const double *__restrict__ gin, double g, int t) {
     if (L.grad == 1) {
         double a = gin[t - 1], b = gin[t], c = gin[t + 1];
+        if (L.cyl) return g * (b + L.lam_m[t] * (a - b) + L.lam_p[t] * (c - b));   // Lat1DCyl1stO.cpp:21-22
         return g * (b + L.l1 * (a - b - b + c));
     } else if (L.grad == 2) {
         int MY = L.st[0];
@@ -188,7 +193,10 @@ __device__ __forceinline__ double prop1_row(const DLat &L, const RowInfo &R, con
     const int kp = (k == nlast) ? L.map_hi[d] : k + 1;
     const double g = G[t];
     const double a = gin[R.base + km], b = gin[t], c = gin[R.base + kp];
-    if (L.grad == 1) return g * (b + L.l1 * (a - b - b + c));
+    if (L.grad == 1) {
+        if (L.cyl) return g * (b + L.lam_m[t] * (a - b) + L.lam_p[t] * (c - b));
+        return g * (b + L.l1 * (a - b - b + c));
+    }
     if (L.grad == 2) {
         const double u = gin[t + R.up], dd = gin[t + R.dn];
         if (L.cyl) return g * (b + L.lam_m[R.x] * (u - b) + L.lam_p[R.x] * (dd - b) + L.l1 * (a + c - b - b));
@@ -286,6 +294,18 @@ __device__ inline double side_fraction(const DLat &L, const double *__restrict__
         return acc;
     }
     double l = L.l1chi;
+    if (L.grad == 1 && L.cyl) {
+        // Lat1DCylinder::SideFraction (Lat1DCylinder.cpp:159-171)
+        int zz = z;
+        if (z == 0) {
+            if (L.bc_lo[0] == SFGPU_BOUND_SURFACE) return p[0] + L.lamc_p[0] * (-p[0] - p[0] + p[1]);
+            zz = L.map_lo[0];
+        } else if (z == L.M - 1) {
+            if (L.bc_hi[0] == SFGPU_BOUND_SURFACE) return p[z] + L.lamc_m[z] * (-p[z] - p[z] + p[z - 1]);
+            zz = L.map_hi[0];
+        }
+        return p[zz] + L.lamc_p[zz] * (p[zz + 1] - p[zz]) + L.lamc_m[zz] * (p[zz - 1] - p[zz]);
+    }
     if (L.grad == 1) {
         int zz = z;
         if (z == 0) {

@@ -108,6 +108,8 @@ extern "C" int sfgpu_chain_phi_noalloc(const sfgpu_lattice_desc *lat, int N, con
     DLat L = H.L;
     L.lam_m = lam_m;
     L.lam_p = lam_p;
+    L.lamc_m = lam_m;   // contact tables are not read on this path
+    L.lamc_p = lam_p;
     const int g = (int)nblocks;
     std::vector<int> used(nseg, 0);
     for (int s = 0; s < N; s++) used[seg_of_s[s]] = 1;

@@ -85,10 +85,14 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
     memset(&L, 0, sizeof(L));
     L.grad = d->gradients;
     L.order = d->order;
-    L.cyl = (d->gradients == 2 && d->geometry == SFGPU_GEOM_CYLINDRICAL);
+    // curved lattices: Lat2DCylinder, Lat1DCylinder, Lat1DSphere (the radial
+    // coordinate is the first gradient); SF_System.cpp:434-519
+    L.cyl = (d->geometry == SFGPU_GEOM_CYLINDRICAL && (d->gradients == 1 || d->gradients == 2)) ||
+            (d->geometry == SFGPU_GEOM_SPHERICAL && d->gradients == 1);
     if (L.grad < 1 || L.grad > 3) return fail(SFGPU_ERR_INVALID, "gradients must be 1, 2 or 3");
-    if (d->geometry == SFGPU_GEOM_CYLINDRICAL && L.grad != 2)
-        return fail(SFGPU_ERR_UNSUPPORTED, "cylindrical geometry needs 2 gradients");
+    if (d->geometry < SFGPU_GEOM_FLAT || d->geometry > SFGPU_GEOM_SPHERICAL) return fail(SFGPU_ERR_INVALID, "unknown geometry");
+    if (d->geometry != SFGPU_GEOM_FLAT && !L.cyl)
+        return fail(SFGPU_ERR_UNSUPPORTED, "cylindrical geometry needs 1 or 2 gradients, spherical 1");
     if (L.order != 1 && L.order != 2) return fail(SFGPU_ERR_INVALID, "order must be 1 or 2");
     if (L.order == 2 && L.cyl) return fail(SFGPU_ERR_UNSUPPORTED, "second order is implemented for flat lattices");
     for (int k = 0; k < 3; k++) L.Md[k] = 1;
@@ -139,7 +143,44 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
 
     int MX = L.Md[0];
     H->lam_m.assign(MX, 0.0); H->lam_p.assign(MX, 0.0); H->Lx.assign(MX, 1.0);
-    if (L.cyl) {
+    if (L.cyl && L.grad == 1) {
+        // Lat1DCylinder::calculateLambdas (Lat1DCylinder.cpp:375-415; D =
+        // dimensions - 1) and Lat1DSphere::calculateLambdas
+        // (Lat1DSphere.cpp:240-286; D = dimensions), with layer_adjustment in
+        // the radius of the first layer and removed again from the last one
+        // (adjustOuterLayer), and separate contact tables for lambda_chi
+        const double PI_ = 4.0 * atan(1.0);
+        const bool sph = d->geometry == SFGPU_GEOM_SPHERICAL;
+        const double off = d->offset_first_layer;
+        if (off <= 0 && d->bound_lo[0] == SFGPU_BOUND_SURFACE)
+            return fail(SFGPU_ERR_INVALID, "a surface at the lower bound of a curved lattice needs offset_first_layer");
+        const double dim = d->dimensions > 0 ? d->dimensions : 3.0;
+        const double D = sph ? dim : dim - 1;
+        std::vector<double> V(MX + 1, 0), S(MX + 1, 0), LL(MX + 1, 0);
+        std::vector<double> lm(MX + 1, 0), lp(MX + 1, 0), lcm(MX + 1, 0), lcp(MX + 1, 0);
+        if (sph) { S[1] = off * off * PI_ * 4; V[1] = (4.0 / 3.0) * pow(off, 3) * PI_; }
+        else { S[1] = off * PI_ * 2; V[1] = off * off * PI_; }
+        LL[1] = V[1];
+        for (int z = 2; z <= MX; z++) {
+            double x = z + off - 2 + ladj;
+            if (z == MX - 1 && ladj != 1.0) x += -ladj + 1;
+            V[z] = (PI_ * pow(2, (D - 1)) / D) * pow(x, D);
+            LL[z] = V[z] - V[z - 1];
+            S[z] = pow(2, (D - 1)) * PI_ * pow(x, (D - 1));
+            lm[z] = L.l1 * S[z - 1] / LL[z];
+            lp[z] = L.l1 * S[z] / LL[z];
+            lcm[z] = L.l1chi * S[z - 1] / LL[z];
+            lcp[z] = L.l1chi * S[z] / LL[z];
+        }
+        if (sph) { if (LL[1] > 4.0 * PI_ / 3.0) LL[1] = V[1] - pow((off - 1), 3) * PI_ * 4.0 / 3.0; }
+        else if (LL[1] > PI_) LL[1] = V[1] - (off - 1) * (off - 1) * PI_;
+        if (LL[1] > 0) { lp[1] = LL[2] * lm[2] / LL[1]; lcp[1] = LL[2] * lcm[2] / LL[1]; }
+        H->lamc_m.assign(MX, 0.0); H->lamc_p.assign(MX, 0.0);
+        for (int x = 0; x < MX; x++) {
+            H->lam_m[x] = lm[x + 1]; H->lam_p[x] = lp[x + 1]; H->Lx[x] = LL[x + 1];
+            H->lamc_m[x] = lcm[x + 1]; H->lamc_p[x] = lcp[x + 1];
+        }
+    } else if (L.cyl) {
         const double PI_ = 4.0 * atan(1.0);
         double off = d->offset_first_layer;
         double D = (d->dimensions > 0 ? d->dimensions : 3.0) - 1;
@@ -176,7 +217,7 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
             }
         }
         if (L.cyl) w *= H->Lx[c[0]];
-        if (L.grad == 1) {
+        if (L.grad == 1 && !L.cyl) {   // flat MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269
             if (z == 1) w *= ladj;
             if (z == L.M - 2 && L.M > 3) w *= (2 - ladj);
         }
@@ -351,6 +392,13 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     SFGPU_CUDA_TRY(cudaMemcpy(d_lam_m, H.lam_m.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
     SFGPU_CUDA_TRY(cudaMemcpy(d_lam_p, H.lam_p.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
     L.lam_m = d_lam_m; L.lam_p = d_lam_p;
+    // contact tables: their own on 1D curved lattices (lambda_chi), else the step tables
+    const std::vector<double> &tcm = H.lamc_m.empty() ? H.lam_m : H.lamc_m;
+    const std::vector<double> &tcp = H.lamc_p.empty() ? H.lam_p : H.lamc_p;
+    if ((rc = alloc_d(&d_lamc_m, L.Md[0])) || (rc = alloc_d(&d_lamc_p, L.Md[0]))) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpy(d_lamc_m, tcm.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
+    SFGPU_CUDA_TRY(cudaMemcpy(d_lamc_p, tcp.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
+    L.lamc_m = d_lamc_m; L.lamc_p = d_lamc_p;
     if ((rc = alloc_d(&d_wgn, M)) || (rc = alloc_d(&d_wf, M))) return rc;
     SFGPU_CUDA_TRY(cudaMemcpy(d_wgn, H.w_gn.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
     SFGPU_CUDA_TRY(cudaMemcpy(d_wf, H.w_f.data(), sizeof(double) * M, cudaMemcpyHostToDevice));

@@ -5,7 +5,7 @@
 
 struct HostLat {
     DLat L;
-    std::vector<double> lam_m, lam_p, Lx, w_gn, w_f;
+    std::vector<double> lam_m, lam_p, lamc_m, lamc_p, Lx, w_gn, w_f;
 };
 int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H);
 
@@ -30,7 +30,8 @@ struct sfgpu_system {
     sfk::BulkParam bp;
     ChiTable ct;
     // device buffers
-    double *d_lam_m = nullptr, *d_lam_p = nullptr, *d_wgn = nullptr, *d_wf = nullptr;
+    double *d_lam_m = nullptr, *d_lam_p = nullptr, *d_lamc_m = nullptr, *d_lamc_p = nullptr;
+    double *d_wgn = nullptr, *d_wf = nullptr;
     int *d_jmap = nullptr, *d_sites = nullptr;
     std::vector<double *> d_range, d_gfull, d_gseg, d_phi;
     double *d_gi = nullptr, *d_ginv[2] = {nullptr, nullptr};

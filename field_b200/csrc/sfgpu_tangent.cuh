@@ -46,7 +46,10 @@ __device__ __forceinline__ double raw1_row(const DLat &L, const RowInfo &R, cons
     const int km = (k == 1) ? L.map_lo[d] : k - 1;
     const int kp = (k == nlast) ? L.map_hi[d] : k + 1;
     const double a = p[R.base + km], b = p[t], c = p[R.base + kp];
-    if (L.grad == 1) return b + L.l1 * (a - b - b + c);
+    if (L.grad == 1) {
+        if (L.cyl) return b + L.lam_m[t] * (a - b) + L.lam_p[t] * (c - b);
+        return b + L.l1 * (a - b - b + c);
+    }
     if (L.grad == 2) {
         const double u = p[t + R.up], dd = p[t + R.dn];
         if (L.cyl) return b + L.lam_m[R.x] * (u - b) + L.lam_p[R.x] * (dd - b) + L.l1 * (a + c - b - b);

@@ -14,7 +14,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 BOUND_SURFACE, BOUND_MIRROR1, BOUND_MIRROR2, BOUND_PERIODIC = 1, 2, 3, 4
-GEOM_FLAT, GEOM_CYLINDRICAL = 0, 1
+GEOM_FLAT, GEOM_CYLINDRICAL, GEOM_SPHERICAL = 0, 1, 2
 SEG_FREE, SEG_FROZEN, SEG_PINNED = 0, 1, 2
 MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT = 0, 1, 2
 

@@ -17,7 +17,7 @@ from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
-from .desc import (BOUND_NAMES, BOUND_MIRROR1, BOUND_PERIODIC, GEOM_CYLINDRICAL, GEOM_FLAT,
+from .desc import (BOUND_NAMES, BOUND_MIRROR1, BOUND_PERIODIC, GEOM_CYLINDRICAL, GEOM_FLAT, GEOM_SPHERICAL,
                    Lattice, Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, Segment,
                    SEG_FREE, SEG_FROZEN, SEG_PINNED, SystemSpec)
 
@@ -135,7 +135,7 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
     ln = lats[0]
     g = int(_get(calc, "lat", ln, "gradients", "1"))
     geom = _get(calc, "lat", ln, "geometry", "flat")
-    if geom not in ("flat", "cylindrical"):
+    if geom not in ("flat", "cylindrical", "spherical"):
         raise ValueError(f"lat : {ln} : geometry : {geom} is not on this path")
     order = 1
     for sysname in _names(calc, "sys"):
@@ -163,14 +163,26 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
             lo.append(l)
             hi.append(h)
     lam = float(_get(calc, "lat", ln, "lambda", repr(1.0 / 6.0)))
+    ladj = float(_get(calc, "lat", ln, "layer_adjustment", "1"))
+    if g == 1 and geom != "flat":
+        # one-gradient curved lattices read offset_first_layer and may give the
+        # first layer's size instead of layer_adjustment
+        # (Lat1DCylinder.cpp:43-52, Lat1DSphere.cpp:6-12)
+        off = float(_get(calc, "lat", ln, "offset_first_layer", "0"))
+        nsites = _get(calc, "lat", ln, "n_sites_first_layer", None)
+        if nsites is not None:
+            v = float(nsites)
+            ladj = np.sqrt(v / np.pi) if geom == "cylindrical" else (3 * v / (4 * np.pi)) ** (1.0 / 3.0)
+    else:
+        off = float(_get(calc, "lat", ln, "offset_first_layer_x", "0"))
+    geometry = {"flat": GEOM_FLAT, "cylindrical": GEOM_CYLINDRICAL, "spherical": GEOM_SPHERICAL}[geom]
     lat = Lattice(gradients=g, n_layers=n + [0] * (3 - g), bound_lo=lo + [0] * (3 - g),
-                  bound_hi=hi + [0] * (3 - g),
-                  geometry=GEOM_CYLINDRICAL if geom == "cylindrical" else GEOM_FLAT,
+                  bound_hi=hi + [0] * (3 - g), geometry=geometry,
                   order=order, lam=lam,
                   lambda_chi=float(_get(calc, "lat", ln, "lambda_chi", "-1")),
-                  layer_adjustment=float(_get(calc, "lat", ln, "layer_adjustment", "1")),
+                  layer_adjustment=ladj,
                   dimensions=float(_get(calc, "lat", ln, "dimensions", "3")),
-                  offset_first_layer=float(_get(calc, "lat", ln, "offset_first_layer_x", "0")))
+                  offset_first_layer=off)
     # segments
     seg_names = _names(calc, "mon")
     segs: List[Segment] = []

@@ -54,8 +54,13 @@ extern "C" {
 #define SFGPU_BOUND_MIRROR2   3
 #define SFGPU_BOUND_PERIODIC  4
 
+/* geometry: SFbox's choices flat / cylindrical / spherical
+ * (SF_System.cpp:437-441) minus one.  Cylindrical takes 1 gradient
+ * (Lat1DCyl1stO) or 2 (Lat2DCyl1stO), spherical 1 (Lat1DSphere1stO); the
+ * radial coordinate is the first gradient. */
 #define SFGPU_GEOM_FLAT        0
 #define SFGPU_GEOM_CYLINDRICAL 1
+#define SFGPU_GEOM_SPHERICAL   2
 
 /* segment freedom, SF_Segment.cpp:61-65 ('grafted' is not on this path) */
 #define SFGPU_SEG_FREE    0
@@ -75,7 +80,7 @@ extern "C" {
 /* ---- system description ------------------------------------------------ */
 typedef struct {
     int    gradients;          /* 1, 2 or 3 */
-    int    geometry;           /* SFGPU_GEOM_*; cylindrical only with 2 gradients */
+    int    geometry;           /* SFGPU_GEOM_* */
     int    order;              /* 1 = first-order chains, 2 = semiflexible (3D,
                                   and flat 1D/2D with lumped directions) */
     int    n_layers[3];        /* interior layers per gradient (unused entries 0) */
@@ -83,9 +88,9 @@ typedef struct {
     int    bound_hi[3];
     double lambda;             /* a-priori step probability l1 (1D/2D); 3D uses 1/6 */
     double lambda_chi;         /* l1 used in contact averages; < 0 means lambda */
-    double layer_adjustment;   /* 1D only (Lat1DFlat.cpp:139); 1 = none */
-    double dimensions;         /* cylinder: spatial dimensions D (default 3) */
-    double offset_first_layer; /* cylinder: offset_first_layer_x (default 0) */
+    double layer_adjustment;   /* 1D only (Lat1DFlat.cpp:139, Lat1DCylinder.cpp:43); 1 = none */
+    double dimensions;         /* curved: spatial dimensions D (default 3) */
+    double offset_first_layer; /* curved: offset_first_layer(_x) (default 0) */
 } sfgpu_lattice_desc;
 
 typedef struct {

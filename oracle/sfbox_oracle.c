@@ -37,7 +37,8 @@ typedef struct {
     int bc_lo[3], bc_hi[3];     /* SFGPU_BOUND_* */
     int map_lo[3], map_hi[3];   /* coordinate copied into 0 / Md-1 */
     double l1, l1chi, ladj;
-    double *lam_m, *lam_p, *Lx; /* cylinder tables by 0-based x (0..MX-1) */
+    double *lam_m, *lam_p, *Lx; /* curved-lattice tables by 0-based x (0..MX-1) */
+    double *lamc_m, *lamc_p;    /* 1D curved: contact tables with lambda_chi */
     double *w_gn;      /* weights of interior sites in lnGN sums */
     double *w_f;       /* weights in the free-energy sum (surfaces included) */
     int K;             /* 2nd-order direction components: 3 (1D), 5 (2D), 6 (3D); 1 first order */
@@ -127,9 +128,12 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
     memset(L, 0, sizeof(*L));
     L->grad = d->gradients;
     L->order = d->order;
-    L->cyl = (d->gradients == 2 && d->geometry == SFGPU_GEOM_CYLINDRICAL);
+    /* curved: Lat2DCylinder, Lat1DCylinder, Lat1DSphere (SF_System.cpp:434-519) */
+    L->cyl = (d->geometry == SFGPU_GEOM_CYLINDRICAL && (d->gradients == 1 || d->gradients == 2)) ||
+             (d->geometry == SFGPU_GEOM_SPHERICAL && d->gradients == 1);
     if (L->grad < 1 || L->grad > 3) return SFGPU_ERR_INVALID;
-    if (d->geometry == SFGPU_GEOM_CYLINDRICAL && d->gradients != 2) return SFGPU_ERR_UNSUPPORTED;
+    if (d->geometry < SFGPU_GEOM_FLAT || d->geometry > SFGPU_GEOM_SPHERICAL) return SFGPU_ERR_INVALID;
+    if (d->geometry != SFGPU_GEOM_FLAT && !L->cyl) return SFGPU_ERR_UNSUPPORTED;
     if (L->order == 2 && L->cyl) return SFGPU_ERR_UNSUPPORTED;
     for (int k = 0; k < 3; k++) { L->Md[k] = 1; }
     for (int k = 0; k < L->grad; k++) {
@@ -169,7 +173,47 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
     L->ladj = (L->grad == 1 && d->layer_adjustment > 0) ? d->layer_adjustment : 1.0;
 
     int MX = L->Md[0];
-    if (L->cyl) {
+    if (L->cyl && L->grad == 1) {
+        /* Lat1DCylinder::calculateLambdas (Lat1DCylinder.cpp:375-415) and
+           Lat1DSphere::calculateLambdas (Lat1DSphere.cpp:240-286), tables
+           indexed 1..M there, 0..M-1 here; adjustOuterLayer holds whenever
+           layer_adjustment differs from 1 (Lat1DFlat.cpp:139-148) */
+        const double PI_ = 4.0 * atan(1.0);
+        int sph = d->geometry == SFGPU_GEOM_SPHERICAL;
+        double off = d->offset_first_layer;
+        if (off <= 0 && d->bound_lo[0] == SFGPU_BOUND_SURFACE) return SFGPU_ERR_INVALID;   /* Lat1DCylinder.cpp:50-53 */
+        double dim = d->dimensions > 0 ? d->dimensions : 3.0;
+        double D = sph ? dim : dim - 1;
+        double *V = calloc(MX + 1, sizeof(double)), *S = calloc(MX + 1, sizeof(double));
+        double *LL = calloc(MX + 1, sizeof(double));
+        double *lm = calloc(MX + 1, sizeof(double)), *lp = calloc(MX + 1, sizeof(double));
+        double *lcm = calloc(MX + 1, sizeof(double)), *lcp = calloc(MX + 1, sizeof(double));
+        if (sph) { S[1] = off * off * PI_ * 4; V[1] = (4.0 / 3.0) * pow(off, 3) * PI_; }
+        else { S[1] = off * PI_ * 2; V[1] = off * off * PI_; }
+        LL[1] = V[1];
+        for (int z = 2; z <= MX; z++) {
+            double x = z + off - 2 + L->ladj;
+            if (z == MX - 1 && L->ladj != 1.0) x += -L->ladj + 1;
+            V[z] = (PI_ * pow(2, (D - 1)) / D) * pow(x, D);
+            LL[z] = V[z] - V[z - 1];
+            S[z] = pow(2, (D - 1)) * PI_ * pow(x, (D - 1));
+            lm[z] = L->l1 * S[z - 1] / LL[z];
+            lp[z] = L->l1 * S[z] / LL[z];
+            lcm[z] = L->l1chi * S[z - 1] / LL[z];
+            lcp[z] = L->l1chi * S[z] / LL[z];
+        }
+        if (sph) { if (LL[1] > 4.0 * PI_ / 3.0) LL[1] = V[1] - pow((off - 1), 3) * PI_ * 4.0 / 3.0; }
+        else if (LL[1] > PI_) LL[1] = V[1] - (off - 1) * (off - 1) * PI_;
+        if (LL[1] > 0) { lp[1] = LL[2] * lm[2] / LL[1]; lcp[1] = LL[2] * lcm[2] / LL[1]; }
+        L->lam_m = calloc(MX, sizeof(double)); L->lam_p = calloc(MX, sizeof(double));
+        L->lamc_m = calloc(MX, sizeof(double)); L->lamc_p = calloc(MX, sizeof(double));
+        L->Lx = calloc(MX, sizeof(double));
+        for (int x = 0; x < MX; x++) {
+            L->lam_m[x] = lm[x + 1]; L->lam_p[x] = lp[x + 1]; L->Lx[x] = LL[x + 1];
+            L->lamc_m[x] = lcm[x + 1]; L->lamc_p[x] = lcp[x + 1];
+        }
+        free(V); free(S); free(LL); free(lm); free(lp); free(lcm); free(lcp);
+    } else if (L->cyl) {
         /* Lat2DCylinder.cpp:7-55 (tables indexed 1..MX there, 0..MX-1 here) */
         const double PI_ = 4.0 * atan(1.0);
         double off = d->offset_first_layer;
@@ -214,7 +258,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
             }
         }
         if (L->cyl) w *= L->Lx[c[0]];
-        if (L->grad == 1) {
+        if (L->grad == 1 && !L->cyl) {   /* flat: Lat1DFlat.cpp:266-269 */
             if (z == 1) w *= L->ladj;
             if (z == L->M - 2 && L->M > 3) w *= (2 - L->ladj);
         }
@@ -228,7 +272,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
 }
 
 static void olat_free(olat *L) {
-    free(L->lam_m); free(L->lam_p); free(L->Lx); free(L->w_gn); free(L->w_f);
+    free(L->lam_m); free(L->lam_p); free(L->lamc_m); free(L->lamc_p); free(L->Lx); free(L->w_gn); free(L->w_f);
 }
 
 /* one first-order step gout = G * stencil(gin); gin must carry valid
@@ -241,7 +285,8 @@ static void olat_prop1(const olat *L, const double *gin, const double *G, double
         double g = G[z], r;
         if (L->grad == 1) {
             double a = gin[z - 1], b = gin[z], c = gin[z + 1];
-            r = g * (b + L->l1 * (a - b - b + c));
+            if (L->cyl) r = g * (b + L->lam_m[z] * (a - b) + L->lam_p[z] * (c - b));   /* Lat1DCyl1stO.cpp:14-27 */
+            else r = g * (b + L->l1 * (a - b - b + c));
         } else if (L->grad == 2) {
             int MY = L->Md[1];
             double a = gin[z - 1], b = gin[z], c = gin[z + 1];
@@ -433,6 +478,19 @@ static void olat_side(const olat *L, const double *phi_in, double *rho) {
             acc += l1 * p[z + jy]; acc += l1 * p[z - jy];
             acc += l1 * p[z + 1]; acc += l1 * p[z - 1];
             rho[z] = acc;
+            continue;
+        }
+        if (L->grad == 1 && L->cyl) {
+            /* Lat1DCylinder::SideFraction (Lat1DCylinder.cpp:159-171) */
+            int zz = z;
+            if (z == 0) {
+                if (L->bc_lo[0] == SFGPU_BOUND_SURFACE) { rho[z] = p[0] + L->lamc_p[0] * (-p[0] - p[0] + p[1]); continue; }
+                zz = L->map_lo[0];
+            } else if (z == M - 1) {
+                if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) { rho[z] = p[z] + L->lamc_m[z] * (-p[z] - p[z] + p[z - 1]); continue; }
+                zz = L->map_hi[0];
+            }
+            rho[z] = p[zz] + L->lamc_p[zz] * (p[zz + 1] - p[zz]) + L->lamc_m[zz] * (p[zz - 1] - p[zz]);
             continue;
         }
         if (L->grad == 1) {

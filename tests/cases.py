@@ -3,8 +3,9 @@ the hot path; shared by the parity tests."""
 import numpy as np
 
 from field_b200 import configs
-from field_b200.desc import (BOUND_MIRROR1, BOUND_MIRROR2, BOUND_PERIODIC, BOUND_SURFACE, GEOM_FLAT, Lattice,
-                             Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, Segment, SEG_FROZEN, SystemSpec)
+from field_b200.desc import (BOUND_MIRROR1, BOUND_MIRROR2, BOUND_PERIODIC, BOUND_SURFACE, GEOM_CYLINDRICAL,
+                             GEOM_FLAT, GEOM_SPHERICAL, Lattice, Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT,
+                             Segment, SEG_FROZEN, SystemSpec)
 
 
 def _flat2d_surface():
@@ -47,6 +48,35 @@ def _flat1d_mirror2_layeradj():
     spec, _ = configs.flat_adsorption(n=25, N=9, phib=0.03, chi_aw=0.7, chi_as=-1.5)
     spec.lattice.lambda_chi = 0.2
     return spec
+
+
+def _cyl1d_micelle():
+    """Lat1DCyl1stO around the axis (no offset), mirror1 both sides with a
+    layer adjustment of the first and last layer, lambda_chi != lambda, an
+    AB diblock, a restricted homopolymer and solvent."""
+    lat = Lattice(1, [22, 0, 0], [BOUND_MIRROR1, 0, 0], [BOUND_MIRROR1, 0, 0], geometry=GEOM_CYLINDRICAL,
+                  lam=1 / 6, lambda_chi=0.2, layer_adjustment=0.8)
+    segs = [Segment("A"), Segment("B"), Segment("W")]
+    chi = np.array([[0, 0.3, 1.4], [0.3, 0, -0.1], [1.4, -0.1, 0]])
+    mols = [Molecule("AB", [(0, 7), (1, 6)], MOL_FREE, phibulk=0.02),
+            Molecule("h", [(0, 9)], MOL_RESTRICTED, theta=5.0),
+            Molecule("W", [(2, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols)
+
+
+def _sphere1d_colloid():
+    """Lat1DSphere1stO: a colloid of radius 3 (offset_first_layer) whose
+    surface layer adsorbs a homopolymer, mirror2 at the outer edge."""
+    lat = Lattice(1, [18, 0, 0], [BOUND_SURFACE, 0, 0], [BOUND_MIRROR2, 0, 0], geometry=GEOM_SPHERICAL,
+                  lam=1 / 6, offset_first_layer=3.0)
+    surf = np.zeros(lat.M)
+    surf[0] = 1.0
+    segs = [Segment("S", SEG_FROZEN, surf), Segment("A"), Segment("W")]
+    chi = np.zeros((3, 3))
+    chi[0, 1] = chi[1, 0] = -1.4
+    chi[1, 2] = chi[2, 1] = 0.6
+    mols = [Molecule("A", [(1, 16)], MOL_FREE, phibulk=0.01), Molecule("W", [(2, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols)
 
 
 def _flat1d_2nd():
@@ -104,6 +134,8 @@ CASES = {
     "3d_periodic_melt": lambda: configs.melt3d(n=9, nA=7, nB=6)[0],
     "3d_mirror_mix": _melt_mirror,
     "3d_2nd_brush": lambda: configs.brush3d(n=6, N=15, sigma=0.2, S=0.5)[0],
+    "1d_cylinder": _cyl1d_micelle,
+    "1d_sphere_colloid": _sphere1d_colloid,
     "1d_2nd_lumped": _flat1d_2nd,
     "2d_2nd_lumped": _flat2d_2nd,
     "2d_2nd_lumped_periodic": _flat2d_2nd_periodic,

@@ -80,3 +80,32 @@ def test_synthetic_configs_shapes():
     assert len(inst) == 8 and all(50 <= s.lattice.n_layers[0] <= 400 for s, _ in inst)
     spec, x = configs.brush3d(n=12, N=20, sigma=0.05)
     assert spec.segments[0].range.sum() == round(0.05 * 144)
+
+
+@pytest.mark.parametrize("geom,expect", [("spherical", (3 * 20.0 / (4 * np.pi)) ** (1 / 3)),
+                                         ("cylindrical", np.sqrt(20.0 / np.pi))])
+def test_curved_one_gradient_lattice(geom, expect):
+    """One-gradient curved lattices read offset_first_layer (no _x) and
+    n_sites_first_layer, which sets the layer adjustment of the first layer
+    (Lat1DCylinder.cpp:43-52, Lat1DSphere.cpp:6-12)."""
+    from field_b200.desc import GEOM_CYLINDRICAL, GEOM_SPHERICAL
+    text = f"""lat : l : gradients : 1
+lat : l : geometry : {geom}
+lat : l : n_layers : 30
+lat : l : lowerbound : mirror1
+lat : l : n_sites_first_layer : 20
+mon : A : freedom : free
+mon : W : freedom : free
+mol : p : composition : (A)5
+mol : p : freedom : free
+mol : p : phibulk : 0.1
+mol : w : composition : (W)1
+mol : w : freedom : solvent
+"""
+    spec, _ = build_system(parse_input(text)[0])
+    lat = spec.lattice
+    assert lat.geometry == (GEOM_SPHERICAL if geom == "spherical" else GEOM_CYLINDRICAL)
+    assert lat.layer_adjustment == pytest.approx(expect)
+    text2 = text.replace("lat : l : n_sites_first_layer : 20\n", "lat : l : offset_first_layer : 2.5\n")
+    spec2, _ = build_system(parse_input(text2)[0])
+    assert spec2.lattice.offset_first_layer == 2.5 and spec2.lattice.layer_adjustment == 1.0

@@ -288,3 +288,58 @@ def test_bond_orientation_isotropic_melt():
     inner = inner.ravel()
     for a in range(3):
         np.testing.assert_allclose(o.bond_orientation(0, a)[inner], 0.1, rtol=1e-13)
+
+
+@pytest.mark.parametrize("geom", ["cylindrical", "spherical"])
+def test_curved_1d_step_by_hand(geom):
+    """Lat1DCyl1stO / Lat1DSphere1stO around the centre (no offset, no layer
+    adjustment): layer z (1-based radius x = z - 1 at its outer edge) holds
+    L = V(x) - V(x - 1) sites with V = pi x^2 (cylinder) or 4/3 pi x^3
+    (sphere), and a step goes inward with lambda S(x - 1) / L and outward
+    with lambda S(x) / L, S the circumference / surface."""
+    from field_b200.desc import GEOM_SPHERICAL
+    n, lam = 9, 0.2
+    g_ = GEOM_CYLINDRICAL if geom == "cylindrical" else GEOM_SPHERICAL
+    lat = Lattice(1, [n, 0, 0], [BOUND_MIRROR1, 0, 0], [BOUND_MIRROR1, 0, 0], geometry=g_, lam=lam)
+    spec = SystemSpec(lat, [Segment("A"), Segment("W")], np.zeros((2, 2)),
+                      [Molecule("p", [(0, 3)], MOL_FREE, phibulk=0.1), Molecule("w", [(1, 1)], MOL_SOLVENT)])
+    o = Oracle(spec)
+    rng = np.random.default_rng(8)
+    gin = o.set_boundaries(rng.uniform(0.2, 1.5, o.M))
+    g = rng.uniform(0.5, 1.5, o.M)
+    out = o.propagate(gin, g)
+    x = np.arange(o.M, dtype=float)
+    if geom == "cylindrical":
+        V, S = np.pi * x ** 2, 2 * np.pi * x
+    else:
+        V, S = 4 / 3 * np.pi * x ** 3, 4 * np.pi * x ** 2
+    for z in range(1, n + 1):
+        L = V[z] - V[z - 1]
+        lm, lp = lam * S[z - 1] / L, lam * S[z] / L
+        want = g[z] * (gin[z] + lm * (gin[z - 1] - gin[z]) + lp * (gin[z + 1] - gin[z]))
+        assert out[z] == pytest.approx(want, rel=1e-13)
+        assert o.site_weights()[z] == pytest.approx(L, rel=1e-14)
+
+
+@pytest.mark.parametrize("geom", ["cylindrical", "spherical"])
+@pytest.mark.parametrize("off,ladj", [(0.0, 1.0), (2.5, 1.0), (0.0, 0.8), (1.5, 1.3)])
+def test_curved_1d_detailed_balance(geom, off, ladj):
+    """L(z) lam_+(z) = L(z+1) lam_-(z+1), with any core offset and layer
+    adjustment: between mirror1 walls a step with G = 1 keeps the L-weighted
+    sum, and u = 0 is the bulk with lnGN = ln(sum of L)."""
+    from field_b200.desc import GEOM_SPHERICAL
+    g_ = GEOM_CYLINDRICAL if geom == "cylindrical" else GEOM_SPHERICAL
+    lat = Lattice(1, [14, 0, 0], [BOUND_MIRROR1, 0, 0], [BOUND_MIRROR1, 0, 0], geometry=g_, lam=1 / 6,
+                  offset_first_layer=off, layer_adjustment=ladj)
+    spec = SystemSpec(lat, [Segment("A"), Segment("W")], np.zeros((2, 2)),
+                      [Molecule("p", [(0, 6)], MOL_FREE, phibulk=0.1), Molecule("w", [(1, 1)], MOL_SOLVENT)])
+    o = Oracle(spec)
+    rng = np.random.default_rng(2)
+    gin = o.set_boundaries(rng.uniform(0.5, 1.5, o.M))
+    out = o.propagate(gin, np.ones(o.M))
+    w = o.site_weights()
+    assert abs((w * out).sum() - (w * gin).sum()) < 1e-12 * (w * gin).sum()
+    f = o.residual(np.zeros(o.nvar))
+    np.testing.assert_allclose(f, 0.0, atol=1e-13)
+    np.testing.assert_allclose(o.phi(0)[1:-1], 0.1, rtol=1e-13)
+    assert o.lngn(0) == pytest.approx(np.log(w.sum()), rel=1e-13)
