@@ -348,6 +348,21 @@ __host__ __device__ inline int lump2_read(const Lump2 &q, int kp, int a, int sm)
     return kp;
 }
 
+// Curved lumped lattices (Lat1DCyl2ndO.cpp:52-95, :149-186; Lat1DSphere2ndO
+// alike; Lat2DCyl2ndO.cpp:45-115, :180-249): a radial read of component kp
+// one layer away becomes f * g_kp(neighbour) + (1 - f) * g_refl(kp)(t)
+// (LReflect / UReflect), refl swapping +x and -x, with f = 6 lambda_-(x) for
+// a read from the inner layer and 6 lambda_+(x) from the outer one.  Forward
+// steps mix every radial read.  The 2D cylinder's backward step mixes only
+// the reads of -x (SFbox computes the +x mixture there and does not use it,
+// Lat2DCyl2ndO.cpp:203-207); the 1D backward step mixes both.
+__device__ __forceinline__ double lump2_mix(const DLat &L, const double *__restrict__ gin, int M, double v, int refl,
+                                            int t, int x, int dir) {
+    const double f = 6 * ((dir > 0) ? L.lam_p[x] : L.lam_m[x]);
+    const double fc = 1.0 - f;
+    return f * v + fc * gin[(size_t)refl * M + t];
+}
+
 static __global__ void step2l_rows(DLat L, const double *__restrict__ gin, const double *__restrict__ G, double S,
                                    double *__restrict__ gout, const double *__restrict__ other,
                                    double *__restrict__ phi, int mode, int backward) {
@@ -365,13 +380,16 @@ static __global__ void step2l_rows(DLat L, const double *__restrict__ gin, const
                 int src = t;
                 int sm = 0;
                 if (q.axis[kk] >= 0) src = lump2_nb(L, x, y, q.axis[kk], -q.sgn[kk], sm);
+                const bool mix = L.cyl && q.axis[kk] == 0;
                 double acc = 0;
                 bool first = true;
                 for (int kp = 0; kp < q.K; kp++) {
                     const double w = lump2_w(q, kk, kp, S, Lw);
                     if (w == 0.0) continue;
                     const int c = lump2_read(q, kp, q.axis[kk], sm);
-                    const double v = w * gin[(size_t)c * M + src];
+                    double r = gin[(size_t)c * M + src];
+                    if (mix) r = lump2_mix(L, gin, M, r, lump2_read(q, kp, 0, 1), t, x, -q.sgn[kk]);
+                    const double v = w * r;
                     if (first) { acc = v; first = false; } else acc += v;
                 }
                 out[kk] = acc * g;
@@ -384,6 +402,8 @@ static __global__ void step2l_rows(DLat L, const double *__restrict__ gin, const
                 if (q.axis[kp] >= 0) src = lump2_nb(L, x, y, q.axis[kp], q.sgn[kp], sm);
                 const int c = lump2_read(q, kp, q.axis[kp], sm);
                 v[kp] = gin[(size_t)c * M + src];
+                if (L.cyl && q.axis[kp] == 0 && (L.grad == 1 || q.sgn[kp] < 0))
+                    v[kp] = lump2_mix(L, gin, M, v[kp], lump2_swap(q, kp), t, x, q.sgn[kp]);
             }
             for (int kq = 0; kq < q.K; kq++) {
                 double acc = 0;

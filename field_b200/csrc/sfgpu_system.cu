@@ -94,7 +94,6 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
     if (d->geometry != SFGPU_GEOM_FLAT && !L.cyl)
         return fail(SFGPU_ERR_UNSUPPORTED, "cylindrical geometry needs 1 or 2 gradients, spherical 1");
     if (L.order != 1 && L.order != 2) return fail(SFGPU_ERR_INVALID, "order must be 1 or 2");
-    if (L.order == 2 && L.cyl) return fail(SFGPU_ERR_UNSUPPORTED, "second order is implemented for flat lattices");
     for (int k = 0; k < 3; k++) L.Md[k] = 1;
     for (int k = 0; k < L.grad; k++) {
         int n = d->n_layers[k];
@@ -224,8 +223,10 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
         H->w_f[z] = keep ? w : 0.0;
         H->w_gn[z] = interior ? w : 0.0;
         // Lat1D2ndO::ComputeLnGN sums the interior without mirror2 halves or
-        // layer adjustment (Lat1D2ndO.cpp:275-285)
-        if (L.order == 2 && L.grad == 1) H->w_gn[z] = interior ? 1.0 : 0.0;
+        // layer adjustment (Lat1D2ndO.cpp:291-300); the curved second-order
+        // lattices keep L(z) and the mirror2 halves (Lat1DCyl2ndO.cpp:318-330,
+        // Lat2DCyl2ndO.cpp:420-469)
+        if (L.order == 2 && L.grad == 1 && !L.cyl) H->w_gn[z] = interior ? 1.0 : 0.0;
     }
     return SFGPU_OK;
 }

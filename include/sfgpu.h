@@ -55,9 +55,10 @@ extern "C" {
 #define SFGPU_BOUND_PERIODIC  4
 
 /* geometry: SFbox's choices flat / cylindrical / spherical
- * (SF_System.cpp:437-441) minus one.  Cylindrical takes 1 gradient
- * (Lat1DCyl1stO) or 2 (Lat2DCyl1stO), spherical 1 (Lat1DSphere1stO); the
- * radial coordinate is the first gradient. */
+ * (SF_System.cpp:378-441) minus one.  Cylindrical takes 1 gradient
+ * (Lat1DCyl1stO / Lat1DCyl2ndO) or 2 (Lat2DCyl1stO / Lat2DCyl2ndO), spherical
+ * 1 (Lat1DSphere1stO / Lat1DSphere2ndO); the radial coordinate is the first
+ * gradient. */
 #define SFGPU_GEOM_FLAT        0
 #define SFGPU_GEOM_CYLINDRICAL 1
 #define SFGPU_GEOM_SPHERICAL   2
@@ -81,8 +82,8 @@ extern "C" {
 typedef struct {
     int    gradients;          /* 1, 2 or 3 */
     int    geometry;           /* SFGPU_GEOM_* */
-    int    order;              /* 1 = first-order chains, 2 = semiflexible (3D,
-                                  and flat 1D/2D with lumped directions) */
+    int    order;              /* 1 = first-order chains, 2 = semiflexible (every
+                                  geometry; 1D/2D lump the homogeneous directions) */
     int    n_layers[3];        /* interior layers per gradient (unused entries 0) */
     int    bound_lo[3];        /* SFGPU_BOUND_* per gradient */
     int    bound_hi[3];

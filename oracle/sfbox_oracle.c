@@ -134,7 +134,6 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
     if (L->grad < 1 || L->grad > 3) return SFGPU_ERR_INVALID;
     if (d->geometry < SFGPU_GEOM_FLAT || d->geometry > SFGPU_GEOM_SPHERICAL) return SFGPU_ERR_INVALID;
     if (d->geometry != SFGPU_GEOM_FLAT && !L->cyl) return SFGPU_ERR_UNSUPPORTED;
-    if (L->order == 2 && L->cyl) return SFGPU_ERR_UNSUPPORTED;
     for (int k = 0; k < 3; k++) { L->Md[k] = 1; }
     for (int k = 0; k < L->grad; k++) {
         L->n[k] = d->n_layers[k];
@@ -266,7 +265,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
         L->w_gn[z] = interior ? w : 0.0;
         /* Lat1D2ndO::ComputeLnGN: interior sum without mirror2 halves or layer
            adjustment (Lat1D2ndO.cpp:275-285) */
-        if (L->order == 2 && L->grad == 1) L->w_gn[z] = interior ? 1.0 : 0.0;
+        if (L->order == 2 && L->grad == 1 && !L->cyl) L->w_gn[z] = interior ? 1.0 : 0.0;
     }
     return SFGPU_OK;
 }
@@ -407,6 +406,19 @@ static void olat_set_boundaries_lumped(const olat *L, double *P) {
         }
     }
 }
+/* the opposite radial direction of component kp (kp itself off the radial axis) */
+static int lump_refl(int g, int kp) {
+    if (LUMP_AXIS[g][kp] != 0) return kp;
+    return (LUMP_SGN[g][kp] > 0) ? (g == 0 ? 2 : 4) : 0;
+}
+/* Curved lattices (Lat1DCyl2ndO.cpp:52-95 and :149-186, Lat1DSphere2ndO the
+   same with spherical tables, Lat2DCyl2ndO.cpp:45-115 and :180-249): a
+   radial read of component kp one layer away is the mixture
+   f * g_kp(neighbour) + (1 - f) * g_refl(kp)(z) (LReflect / UReflect), with
+   f = 6 lambda_-(x) for a read from the inner layer and 6 lambda_+(x) for
+   one from the outer layer.  Forward steps mix every radial read; the 2D
+   cylinder's backward step mixes only the reads of -x (its UReflect of +x is
+   computed and not used, Lat2DCyl2ndO.cpp:203-207), the 1D backward both. */
 static void olat_prop2l(const olat *L, const double *gin_, const double *G, double S, double *gout, int backward) {
     int g = L->grad - 1, K = L->K, M = L->M;
     int e[2] = {L->st[0], L->grad == 2 ? L->st[1] : 0};
@@ -416,15 +428,27 @@ static void olat_prop2l(const olat *L, const double *gin_, const double *G, doub
     olat_set_boundaries_lumped(L, gin);
     for (int z = 0; z < M; z++) {
         if (!is_interior(L, z)) continue;
+        int x = z / L->st[0];   /* radial coordinate */
         for (int kk = 0; kk < K; kk++) {
             double acc = 0; int first = 1;
             for (int kp = 0; kp < K; kp++) {
                 double w = lump_w(g, kk, kp, S, Lw);
                 if (w == 0.0) continue;
-                int src;
-                if (!backward) src = (LUMP_AXIS[g][kk] >= 0) ? z - LUMP_SGN[g][kk] * e[LUMP_AXIS[g][kk]] : z;
-                else src = (LUMP_AXIS[g][kp] >= 0) ? z + LUMP_SGN[g][kp] * e[LUMP_AXIS[g][kp]] : z;
-                double t = w * gin[(size_t)kp * M + src];
+                int src, dir;   /* dir: +1 read from the outer layer, -1 from the inner, 0 no radial mixing */
+                if (!backward) {
+                    src = (LUMP_AXIS[g][kk] >= 0) ? z - LUMP_SGN[g][kk] * e[LUMP_AXIS[g][kk]] : z;
+                    dir = (LUMP_AXIS[g][kk] == 0) ? -LUMP_SGN[g][kk] : 0;
+                } else {
+                    src = (LUMP_AXIS[g][kp] >= 0) ? z + LUMP_SGN[g][kp] * e[LUMP_AXIS[g][kp]] : z;
+                    dir = (LUMP_AXIS[g][kp] == 0 && (g == 0 || LUMP_SGN[g][kp] < 0)) ? LUMP_SGN[g][kp] : 0;
+                }
+                double v = gin[(size_t)kp * M + src];
+                if (L->cyl && dir != 0) {
+                    double f = 6 * ((dir > 0) ? L->lam_p[x] : L->lam_m[x]);
+                    double fc = 1.0 - f;
+                    v = f * v + fc * gin[(size_t)lump_refl(g, kp) * M + z];
+                }
+                double t = w * v;
                 if (first) { acc = t; first = 0; } else acc += t;
             }
             gout[(size_t)kk * M + z] = acc * G[z];

@@ -124,6 +124,50 @@ def _flat2d_2nd_periodic():
     return SystemSpec(lat, segs, chi, mols, pf=pf)
 
 
+def _cyl1d_2nd():
+    """Lat1DCyl2ndO around the axis, mirror1 both sides: a stiff AB diblock
+    (S = 0.5 inside A, 0.3 across the junction) and solvent."""
+    lat = Lattice(1, [20, 0, 0], [BOUND_MIRROR1, 0, 0], [BOUND_MIRROR1, 0, 0], geometry=GEOM_CYLINDRICAL,
+                  order=2, lam=1 / 6)
+    segs = [Segment("A"), Segment("B"), Segment("W")]
+    chi = np.array([[0, 0.3, 1.3], [0.3, 0, -0.1], [1.3, -0.1, 0]])
+    pf = np.full((3, 3), 0.2)
+    pf[0, 0], pf[0, 1], pf[1, 0] = 0.5, 0.3, 0.3
+    mols = [Molecule("AB", [(0, 8), (1, 6)], MOL_FREE, phibulk=0.03), Molecule("W", [(2, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols, pf=pf)
+
+
+def _sphere1d_2nd():
+    """Lat1DSphere2ndO: a colloid of radius 4 with an adsorbing surface
+    layer, mirror2 outside; stiff free chains and a restricted one."""
+    lat = Lattice(1, [16, 0, 0], [BOUND_SURFACE, 0, 0], [BOUND_MIRROR2, 0, 0], geometry=GEOM_SPHERICAL,
+                  order=2, lam=1 / 6, offset_first_layer=4.0)
+    surf = np.zeros(lat.M)
+    surf[0] = 1.0
+    segs = [Segment("S", SEG_FROZEN, surf), Segment("A"), Segment("W")]
+    chi = np.zeros((3, 3))
+    chi[0, 1] = chi[1, 0] = -1.2
+    chi[1, 2] = chi[2, 1] = 0.5
+    pf = np.full((3, 3), 0.2)
+    pf[1, 1] = 0.45
+    mols = [Molecule("A", [(1, 12)], MOL_FREE, phibulk=0.01), Molecule("r", [(1, 7)], MOL_RESTRICTED, theta=20.0),
+            Molecule("W", [(2, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols, pf=pf)
+
+
+def _cyl2d_2nd():
+    """Lat2DCyl2ndO: radius x with a core of radius 2 behind a surface,
+    mirror1 outside; y from a surface to mirror2; an AB diblock and solvent."""
+    lat = Lattice(2, [10, 8, 0], [BOUND_SURFACE, BOUND_SURFACE, 0], [BOUND_MIRROR1, BOUND_MIRROR2, 0],
+                  geometry=GEOM_CYLINDRICAL, order=2, lam=1 / 6, offset_first_layer=2.0)
+    segs = [Segment("A"), Segment("B"), Segment("W")]
+    chi = np.array([[0, 0.5, 1.1], [0.5, 0, 0.2], [1.1, 0.2, 0]])
+    pf = np.full((3, 3), 0.2)
+    pf[0, 0] = 0.4
+    mols = [Molecule("AB", [(0, 5), (1, 6)], MOL_FREE, phibulk=0.04), Molecule("W", [(2, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols, pf=pf)
+
+
 CASES = {
     "1d_surface": lambda: configs.flat_adsorption(n=40, N=21)[0],
     "1d_surface_even": lambda: configs.flat_adsorption(n=17, N=30, phib=0.002, chi_aw=0.2, chi_as=-2.0)[0],
@@ -139,6 +183,9 @@ CASES = {
     "1d_2nd_lumped": _flat1d_2nd,
     "2d_2nd_lumped": _flat2d_2nd,
     "2d_2nd_lumped_periodic": _flat2d_2nd_periodic,
+    "1d_cyl_2nd_lumped": _cyl1d_2nd,
+    "1d_sphere_2nd_lumped": _sphere1d_2nd,
+    "2d_cyl_2nd_lumped": _cyl2d_2nd,
 }
 
 # cases whose derivatives (forward and reverse mode) are implemented

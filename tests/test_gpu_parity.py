@@ -177,7 +177,7 @@ def test_autotuned_tile_keeps_results(gpu_lib):
     assert np.array_equal(s.residual(x0), f_ref)
 
 
-@pytest.mark.parametrize("case", ["1d_2nd_lumped", "2d_2nd_lumped"])
+@pytest.mark.parametrize("case", ["1d_2nd_lumped", "2d_2nd_lumped", "1d_sphere_2nd_lumped", "2d_cyl_2nd_lumped"])
 def test_lumped_second_order_converged_parity(gpu_lib, case):
     """Lat1D2ndO / Lat2D2ndO converged by the device Pure_DIIS and by the
     oracle's: profiles to 1e-10, free energy to 1e-9."""
@@ -210,7 +210,8 @@ def test_lumped_derivatives_report_unsupported(gpu_lib):
     assert np.all(np.isfinite(sys_.residual(x)))
 
 
-@pytest.mark.parametrize("case", ["3d_2nd_brush", "1d_2nd_lumped", "2d_2nd_lumped", "2d_2nd_lumped_periodic"])
+@pytest.mark.parametrize("case", ["3d_2nd_brush", "1d_2nd_lumped", "2d_2nd_lumped", "2d_2nd_lumped_periodic",
+                                  "1d_cyl_2nd_lumped", "2d_cyl_2nd_lumped"])
 def test_bond_orientation(gpu_lib, case):
     """Bond-orientation profiles of the second-order lattices against the
     oracle, per molecule and axis."""

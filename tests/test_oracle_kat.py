@@ -343,3 +343,152 @@ def test_curved_1d_detailed_balance(geom, off, ladj):
     np.testing.assert_allclose(f, 0.0, atol=1e-13)
     np.testing.assert_allclose(o.phi(0)[1:-1], 0.1, rtol=1e-13)
     assert o.lngn(0) == pytest.approx(np.log(w.sum()), rel=1e-13)
+
+
+def _curved_tables(n, geom):
+    """lambda_-/lambda_+ of a curved lattice around the centre (no offset, no
+    layer adjustment), lambda = 1/6, by 0-based radial index 0..n+1."""
+    x = np.arange(n + 2, dtype=float)
+    if geom == "sphere":
+        V, S = 4 / 3 * np.pi * x ** 3, 4 * np.pi * x ** 2
+    else:
+        V, S = np.pi * x ** 2, 2 * np.pi * x
+    lm, lp = np.zeros(n + 2), np.zeros(n + 2)
+    for z in range(1, n + 2):
+        Lz = V[z] - V[z - 1]
+        lm[z], lp[z] = S[z - 1] / Lz / 6, S[z] / Lz / 6
+    return lm, lp
+
+
+@pytest.mark.parametrize("geom", ["cylinder", "sphere"])
+@pytest.mark.parametrize("backward", [0, 1])
+def test_curved_1d_second_order_step_restated(geom, backward):
+    """One Lat1DCyl2ndO / Lat1DSphere2ndO step written out component by
+    component (three components +x, lateral x4, -x): a radial read mixes
+    f * g(neighbour) + (1 - f) * g_reflected(here), f = 6 lambda_-(z) from
+    inside, 6 lambda_+(z) from outside; mirror1 walls swap +x and -x."""
+    from field_b200.desc import GEOM_SPHERICAL
+    n, S = 9, 0.35
+    g_ = GEOM_SPHERICAL if geom == "sphere" else GEOM_CYLINDRICAL
+    lat = Lattice(1, [n, 0, 0], [BOUND_MIRROR1, 0, 0], [BOUND_MIRROR1, 0, 0], geometry=g_, order=2, lam=1 / 6)
+    spec = SystemSpec(lat, [Segment("A"), Segment("W")], np.zeros((2, 2)),
+                      [Molecule("p", [(0, 3)], MOL_FREE, phibulk=0.1), Molecule("w", [(1, 1)], MOL_SOLVENT)])
+    o = Oracle(spec)
+    M = n + 2
+    rng = np.random.default_rng(5 + backward)
+    gin = rng.uniform(0.2, 1.5, 3 * M)
+    G = rng.uniform(0.5, 1.5, M)
+    got = o.propagate(gin, G, S=S, backward=backward).reshape(3, M)
+    g0, g1, g2 = gin.reshape(3, M).copy()
+    g0[0], g2[0], g1[0] = g2[1], g0[1], g1[1]                     # SetBx1(g0,g2), SetBx1(g1)
+    g0[-1], g2[-1], g1[-1] = g2[-2], g0[-2], g1[-2]               # SetBxm(g0,g2), SetBxm(g1)
+    lm, lp = _curved_tables(n, geom)
+    fm, fp = 6 * lm, 6 * lp
+    L = (1 - S) / 4
+    t = np.arange(1, M - 1)
+    if not backward:
+        HL0 = fm[t] * g0[t - 1] + (1 - fm[t]) * g2[t]
+        HL1 = fm[t] * g1[t - 1] + (1 - fm[t]) * g1[t]
+        HU1 = fp[t] * g1[t + 1] + (1 - fp[t]) * g1[t]
+        HU2 = fp[t] * g2[t + 1] + (1 - fp[t]) * g0[t]
+        want = [S * HL0 + 4 * L * HL1, L * g0[t] + (2 * L + S) * g1[t] + L * g2[t], 4 * L * HU1 + S * HU2]
+    else:
+        H0 = fp[t] * g0[t + 1] + (1 - fp[t]) * g2[t]
+        H2 = fm[t] * g2[t - 1] + (1 - fm[t]) * g0[t]
+        want = [S * H0 + 4 * L * g1[t], L * H0 + (2 * L + S) * g1[t] + L * H2, S * H2 + 4 * L * g1[t]]
+    for k in range(3):
+        np.testing.assert_allclose(got[k, 1:-1], want[k] * G[t], rtol=1e-13)
+
+
+@pytest.mark.parametrize("backward", [0, 1])
+def test_curved_2d_second_order_step_restated(backward):
+    """One Lat2DCyl2ndO step written out (components +x, +y, z x2, -y, -x;
+    x radial).  Forward: every radial read is mixed with the reflected
+    component at the site.  Backward: only the reads of -x are (SFbox builds
+    the +x mixture and leaves it unused)."""
+    nx, ny, S = 7, 5, 0.3
+    lat = Lattice(2, [nx, ny, 0], [BOUND_MIRROR1, BOUND_MIRROR1, 0], [BOUND_MIRROR1, BOUND_MIRROR1, 0],
+                  geometry=GEOM_CYLINDRICAL, order=2, lam=1 / 6)
+    spec = SystemSpec(lat, [Segment("A"), Segment("W")], np.zeros((2, 2)),
+                      [Molecule("p", [(0, 3)], MOL_FREE, phibulk=0.1), Molecule("w", [(1, 1)], MOL_SOLVENT)])
+    o = Oracle(spec)
+    MX, MY = nx + 2, ny + 2
+    rng = np.random.default_rng(9 + backward)
+    gin = rng.uniform(0.2, 1.5, 5 * MX * MY)
+    G = rng.uniform(0.5, 1.5, (MX, MY))
+    got = o.propagate(gin, G.ravel(), S=S, backward=backward).reshape(5, MX, MY)
+    g = gin.reshape(5, MX, MY).copy()
+    for a, b in ((0, 1), (-1, -2)):          # x walls: swap +x/-x, copy the rest
+        g[0, a], g[4, a] = g[4, b].copy(), g[0, b].copy()
+        for k in (1, 2, 3):
+            g[k, a] = g[k, b]
+    for a, b in ((0, 1), (-1, -2)):          # y walls: swap +y/-y, copy the rest
+        g[1, :, a], g[3, :, a] = g[3, :, b].copy(), g[1, :, b].copy()
+        for k in (0, 2, 4):
+            g[k, :, a] = g[k, :, b]
+    lm, lp = _curved_tables(nx, "cylinder")
+    fm, fp = (6 * lm)[:, None], (6 * lp)[:, None]
+    L = (1 - S) / 4
+    X, Y = slice(1, -1), slice(1, -1)
+    c = lambda k, dx=0, dy=0: g[k, 1 + dx:MX - 1 + dx, 1 + dy:MY - 1 + dy]
+    fmi, fpi = fm[X], fp[X]
+    if not backward:
+        HL = [fmi * c(k, -1) + (1 - fmi) * c(4 if k == 0 else k) for k in range(4)]
+        HU = {k: fpi * c(k, 1) + (1 - fpi) * c(0 if k == 4 else k) for k in range(1, 5)}
+        want = [S * HL[0] + L * HL[1] + 2 * L * HL[2] + L * HL[3],
+                L * c(0, 0, -1) + S * c(1, 0, -1) + 2 * L * c(2, 0, -1) + L * c(4, 0, -1),
+                L * c(0) + L * c(1) + S * c(2) + L * c(3) + L * c(4),
+                L * c(0, 0, 1) + 2 * L * c(2, 0, 1) + S * c(3, 0, 1) + L * c(4, 0, 1),
+                L * HU[1] + 2 * L * HU[2] + L * HU[3] + S * HU[4]]
+    else:
+        H4 = fmi * c(4, -1) + (1 - fmi) * c(0)
+        want = [S * c(0, 1) + L * c(1, 0, 1) + 2 * L * c(2) + L * c(3, 0, -1),
+                L * c(0, 1) + S * c(1, 0, 1) + 2 * L * c(2) + L * H4,
+                L * c(0, 1) + L * c(1, 0, 1) + S * c(2) + L * c(3, 0, -1) + L * H4,
+                L * c(0, 1) + 2 * L * c(2) + S * c(3, 0, -1) + L * H4,
+                L * c(1, 0, 1) + 2 * L * c(2) + L * c(3, 0, -1) + S * H4]
+    for k in range(5):
+        np.testing.assert_allclose(got[k, X, Y], want[k] * G[X, Y], rtol=1e-13)
+
+
+@pytest.mark.parametrize("case", ["1d_cyl", "1d_sphere", "2d_cyl"])
+def test_curved_second_order_u_zero_is_bulk(case):
+    """Every mixture f + (1 - f) = 1, so with G = 1 between mirror walls the
+    all-ones distribution stays all ones: u = 0 is the bulk, and lnGN is
+    ln(sum of L)."""
+    from field_b200.desc import GEOM_SPHERICAL
+    g_ = GEOM_SPHERICAL if case == "1d_sphere" else GEOM_CYLINDRICAL
+    if case == "2d_cyl":
+        lat = Lattice(2, [9, 6, 0], [BOUND_MIRROR1, BOUND_MIRROR2, 0], [BOUND_MIRROR1, BOUND_MIRROR1, 0],
+                      geometry=g_, order=2, lam=1 / 6, offset_first_layer=1.5)
+    else:
+        lat = Lattice(1, [12, 0, 0], [BOUND_MIRROR1, 0, 0], [BOUND_MIRROR2, 0, 0], geometry=g_, order=2,
+                      lam=1 / 6, offset_first_layer=2.0)
+    spec = SystemSpec(lat, [Segment("A"), Segment("W")], np.zeros((2, 2)),
+                      [Molecule("p", [(0, 7)], MOL_FREE, phibulk=0.2), Molecule("w", [(1, 1)], MOL_SOLVENT)],
+                      pf=np.full((2, 2), 0.4))
+    o = Oracle(spec)
+    f = o.residual(np.zeros(o.nvar))
+    np.testing.assert_allclose(f, 0.0, atol=1e-13)
+    np.testing.assert_allclose(o.phi(0)[spec.itvar_sites()], 0.2, rtol=1e-13)
+    assert o.lngn(0) == pytest.approx(np.log(o.site_weights().sum()), rel=1e-13)
+
+
+def test_curved_second_order_large_radius_is_flat():
+    """Far from the axis the mixing fractions tend to 1 and Lat1DCyl2ndO
+    becomes Lat1D2ndO: profiles agree to the order of 1/R."""
+    from field_b200.desc import GEOM_FLAT
+    segs = [Segment("A"), Segment("W")]
+    chi = np.array([[0, 0.8], [0.8, 0]])
+    mols = [Molecule("p", [(0, 10)], MOL_FREE, phibulk=0.05), Molecule("w", [(1, 1)], MOL_SOLVENT)]
+    pf = np.full((2, 2), 0.5)
+    curved = Lattice(1, [15, 0, 0], [BOUND_MIRROR1, 0, 0], [BOUND_MIRROR1, 0, 0], geometry=GEOM_CYLINDRICAL,
+                     order=2, lam=1 / 6, offset_first_layer=1e6)
+    flat = Lattice(1, [15, 0, 0], [BOUND_MIRROR1, 0, 0], [BOUND_MIRROR1, 0, 0], geometry=GEOM_FLAT, order=2,
+                   lam=1 / 6)
+    oc = Oracle(SystemSpec(curved, segs, chi, mols, pf=pf))
+    of = Oracle(SystemSpec(flat, segs, chi, mols, pf=pf))
+    x = np.random.default_rng(4).normal(0.0, 0.3, of.nvar)
+    oc.residual(x)
+    of.residual(x)
+    np.testing.assert_allclose(oc.phi(0)[1:-1], of.phi(0)[1:-1], rtol=1e-4)
