@@ -215,12 +215,12 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         for (int sp = (N + 3) / 2; sp <= N; sp++) {
             const double *other = gi + (size_t)(N - sp) * M;
             double *dst = bufA;
-            for_interior4(L, threadIdx.x, blockDim.x,
+            for_interior4_acc(L, threadIdx.x, blockDim.x, phi, other,
                 [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, cur, G, k, nlast); },
-                [&](const RowInfo &R, int k, double out) {
+                [&](const RowInfo &R, int k, double out, double ph, double ot) {
                     const int z = R.base + k;
                     dst[z] = out;
-                    phi[z] += out * other[z];
+                    phi[z] = ph + out * ot;
                 });
             __syncthreads();
             cur = bufA; double *t = bufA; bufA = bufB; bufB = t;
@@ -263,12 +263,12 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         const double *gf = gi + (size_t)t * M;
         double *phi = o.phi[sg];
         double *dst = bufA;
-        for_interior4(L, threadIdx.x, blockDim.x,
+        for_interior4_acc(L, threadIdx.x, blockDim.x, phi, gf,
             [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, cur, G, k, nlast); },
-            [&](const RowInfo &R, int k, double out) {
+            [&](const RowInfo &R, int k, double out, double ph, double ot) {
                 const int z = R.base + k;
                 dst[z] = out;
-                phi[z] += out * gf[z];
+                phi[z] = ph + out * ot;
             });
         __syncthreads();
         cur = bufA; double *tt = bufA; bufA = bufB; bufB = tt;

@@ -232,6 +232,66 @@ __device__ __forceinline__ void for_interior(const DLat &L, int worker, int nwor
     }
 }
 
+// The walk of for_interior4 for a step fused with a composition
+// phi += out * other: the two operands of the four positions are loaded first,
+// with the stencils' loads, so that no load waits behind a store of an earlier
+// position (phi and other may alias nothing the compiler can see past).
+// compute(R, k, nlast) -> double, store(R, k, value, phi_value, other_value).
+template <class C, class S>
+__device__ __forceinline__ void for_interior4_acc(const DLat &L, int worker, int nworkers,
+                                                  const double *__restrict__ pphi, const double *__restrict__ pother,
+                                                  C &&compute, S &&store) {
+    const int d = L.grad - 1;
+    const int nlast = L.Md[d] - 2;
+    if (L.grad == 1) {
+        RowInfo R = lat_row(L, 0);
+        for (int k0 = worker + 1; k0 <= nlast; k0 += 4 * nworkers) {
+            double v[4], a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = k0 + u * nworkers;
+                a[u] = (k <= nlast) ? pphi[R.base + k] : 0.0;
+                b[u] = (k <= nlast) ? pother[R.base + k] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = k0 + u * nworkers;
+                v[u] = (k <= nlast) ? compute(R, k, nlast) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = k0 + u * nworkers;
+                if (k <= nlast) store(R, k, v[u], a[u], b[u]);
+            }
+        }
+        return;
+    }
+    const int lane = worker & 31, warp = worker >> 5, nw = nworkers >> 5;
+    const int nrows = lat_nrows(L);
+    for (int row = warp; row < nrows; row += nw) {
+        RowInfo R = lat_row(L, row);
+        for (int k0 = lane + 1; k0 <= nlast; k0 += 128) {
+            double v[4], a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = k0 + 32 * u;
+                a[u] = (k <= nlast) ? pphi[R.base + k] : 0.0;
+                b[u] = (k <= nlast) ? pother[R.base + k] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = k0 + 32 * u;
+                v[u] = (k <= nlast) ? compute(R, k, nlast) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = k0 + 32 * u;
+                if (k <= nlast) store(R, k, v[u], a[u], b[u]);
+            }
+        }
+    }
+}
+
 // Same walk, four positions per lane at a time: all four stencils are
 // computed (every load issued) before any result is stored, so one thread
 // keeps four rows' worth of loads in flight instead of waiting on each.

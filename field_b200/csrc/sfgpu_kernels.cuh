@@ -56,13 +56,22 @@ static __global__ void step1_rows(DLat L, const double *__restrict__ gin, const 
                                   double *__restrict__ gout, const double *__restrict__ other,
                                   double *__restrict__ phi, int mode) {
     const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mode == COMP_ACC) {
+        for_interior4_acc(L, worker, gridDim.x * blockDim.x, phi, other,
+            [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, gin, G, k, nlast); },
+            [&](const RowInfo &R, int k, double out, double ph, double ot) {
+                const int t = R.base + k;
+                gout[t] = out;
+                phi[t] = ph + out * ot;
+            });
+        return;
+    }
     for_interior4(L, worker, gridDim.x * blockDim.x,
         [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, gin, G, k, nlast); },
         [&](const RowInfo &R, int k, double out) {
             const int t = R.base + k;
             gout[t] = out;
-            if (mode == COMP_ACC) phi[t] += out * other[t];
-            else if (mode == COMP_CENTRE) phi[t] = (phi[t] + out * out) * 0.5;
+            if (mode == COMP_CENTRE) phi[t] = (phi[t] + out * out) * 0.5;
         });
 }
 
