@@ -1,0 +1,36 @@
+"""var : sweeps solved as batched instances (field_b200.sweep) on the GPU."""
+import numpy as np
+import pytest
+
+from field_b200 import configs
+from field_b200.sfinput import parse_input
+from field_b200.sweep import solve_sweep
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+SWEEP = (configs.C1_INPUT.format(n=40, N=20, phib=0.01, chi_aw=0.0, chi_as=-1.0)
+         + "var : mon : A : chi - W\nvar : mon : step : 0.1\nvar : mon : end_value : 1.0\nvar : mon : type : real\n"
+         + "newton : isaac : tolerance : 1e-9\n")
+
+
+def test_sweep_waves_agree_and_warm_starts_help(gpu_lib):
+    """The 11 points of a chi sweep solved in one batch from zero, in three
+    waves, and as SFbox's chain (each point from its predecessor): every point
+    converges, satisfies the oracle's equations, and the three schedules reach
+    the same solutions; warm-started points need fewer iterations."""
+    calc = parse_input(SWEEP)[-1]
+    cold = solve_sweep(calc, waves=1, m=5)
+    three = solve_sweep(calc, waves=3, m=5)
+    chain = solve_sweep(calc, waves=100, m=5)
+    assert len(cold.x) == 11 and (chain.wave == np.arange(11)).all()
+    for res in (cold, three, chain):
+        assert res.converged.all(), res.status
+    for i, spec in enumerate(cold.specs):
+        assert spec.chi[1, 2] == pytest.approx(0.1 * i)
+        o = Oracle(spec)
+        for res in (cold, three, chain):
+            assert np.linalg.norm(o.residual(res.x[i])) < 1e-8
+        np.testing.assert_allclose(three.x[i], cold.x[i], rtol=0, atol=1e-6)
+        np.testing.assert_allclose(chain.x[i], cold.x[i], rtol=0, atol=1e-6)
+    assert chain.iterations[1:].mean() < cold.iterations[1:].mean()
