@@ -710,6 +710,113 @@ static __global__ void free_energy_partial(DLat L, FreeParam fp, ChiTable ct, co
     if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
 }
 
+// Free-energy and grand-potential densities per site, each multiplied by the
+// SubtractBoundaries factor, and their sums weighted with the lattice sites
+// (two block partials per block: F, Omega).  Densities as free_energy_partial
+// and SF_MolList1stO::GetGrandPotentialProfile (SF_MolList1stO.cpp:1001-1101;
+// the same in SF_MolList2ndO): the molecules' (phi - phib)/N, u' phi of every
+// liquid state (u' = -ln G - ChemInt + ChemIntBulk where G > 0), and the
+// contact pairs of liquid states, in that order.  No charges, external
+// potentials or grafted chains on this path.  fe / gp may be null.
+struct ThermoParam {
+    int nseg, nmol;
+    const double *phi[SFGPU_MAX_SEG];
+    const double *mphi[SFGPU_MAX_SEG * SFGPU_MAX_SEG];
+    const double *gseg[SFGPU_MAX_SEG], *gfull[SFGPU_MAX_SEG];
+    int frozen[SFGPU_MAX_SEG];
+    double invN[SFGPU_MAX_SEG], N[SFGPU_MAX_SEG], lnN[SFGPU_MAX_SEG], chemintref[SFGPU_MAX_SEG];
+};
+static __global__ void thermo_partial(DLat L, ThermoParam tp, ChiTable ct, const double *__restrict__ wf,
+                                      const double *__restrict__ sb, const MolScal *__restrict__ scal,
+                                      const double *__restrict__ phib, double *__restrict__ fe,
+                                      double *__restrict__ gp, double *__restrict__ partial) {
+    __shared__ double shF[kBlock], shO[kBlock];
+    double accF = 0, accO = 0;
+    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < L.M; z += gridDim.x * blockDim.x) {
+        double entropy = 0, contact = 0, omega = 0;
+        for (int m = 0; m < tp.nmol; m++) {
+            double pm = 0;
+            for (int i = 0; i < tp.nseg; i++) {
+                const double *q = tp.mphi[m * SFGPU_MAX_SEG + i];
+                if (q) pm += q[z];
+            }
+            entropy -= (pm * tp.invN[m]) * (tp.lnN[m] + scal[m].lnc);
+            contact -= pm * tp.chemintref[m];
+        }
+        for (int m = 0; m < tp.nmol; m++)
+            for (int i = 0; i < tp.nseg; i++) {
+                const double *q = tp.mphi[m * SFGPU_MAX_SEG + i];
+                if (!q) continue;
+                double G = tp.gseg[i][z];
+                if (G > 0) entropy -= q[z] * log(G);
+            }
+        double rho[SFGPU_MAX_SEG];
+#pragma unroll
+        for (int j = 0; j < SFGPU_MAX_SEG; j++) rho[j] = (j < tp.nseg) ? side_fraction(L, tp.phi[j], z) : 0.0;
+        for (int i = 0; i < tp.nseg; i++) {
+            double ci = 0;
+#pragma unroll
+            for (int j = 0; j < SFGPU_MAX_SEG; j++) {
+                if (j >= tp.nseg) continue;
+                double x = ct.chi[i * SFGPU_MAX_SEG + j];
+                if (x != 0) ci += x * rho[j];
+            }
+            contact += 0.5 * tp.phi[i][z] * ci;
+        }
+        for (int m = 0; m < tp.nmol; m++) {
+            double pm = 0;
+            for (int i = 0; i < tp.nseg; i++) {
+                const double *q = tp.mphi[m * SFGPU_MAX_SEG + i];
+                if (q) pm += q[z];
+            }
+            if (pm > 0) omega -= (pm - scal[m].phibulk) / tp.N[m];
+        }
+        for (int i = 0; i < tp.nseg; i++) {
+            if (tp.frozen[i]) continue;
+            const double G = tp.gfull[i][z];
+            double up = 0;
+            if (G > 0) {
+                double ci = 0, cb = 0;
+#pragma unroll
+                for (int j = 0; j < SFGPU_MAX_SEG; j++) {
+                    if (j >= tp.nseg) continue;
+                    double x = ct.chi[i * SFGPU_MAX_SEG + j];
+                    if (x != 0) { ci += x * rho[j]; cb += x * phib[j]; }
+                }
+                up = -log(G);
+                up -= ci;
+                up += cb;
+            }
+            omega -= up * tp.phi[i][z];
+        }
+        for (int i = 0; i < tp.nseg; i++) {
+            if (tp.frozen[i]) continue;
+            const double p1 = tp.phi[i][z];
+#pragma unroll
+            for (int j = 0; j < SFGPU_MAX_SEG; j++) {
+                if (j >= tp.nseg || tp.frozen[j]) continue;
+                const double x = ct.chi[i * SFGPU_MAX_SEG + j];
+                omega -= 0.5 * x * p1 * rho[j];
+                if (p1 > 0) omega += 0.5 * x * phib[i] * phib[j];
+            }
+        }
+        const double f = -entropy + contact;
+        const double w = wf[z];
+        accF += w * f;
+        accO += w * omega;
+        if (fe) fe[z] = f * sb[z];
+        if (gp) gp[z] = omega * sb[z];
+    }
+    shF[threadIdx.x] = accF;
+    shO[threadIdx.x] = accO;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) { shF[threadIdx.x] += shF[threadIdx.x + s]; shO[threadIdx.x] += shO[threadIdx.x + s]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { partial[blockIdx.x] = shF[0]; partial[gridDim.x + blockIdx.x] = shO[0]; }
+}
+
 // per-site contact average of one profile (for the Lattice-level API)
 static __global__ void side_kernel(DLat L, const double *__restrict__ p, double *__restrict__ rho) {
     for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < L.M; z += gridDim.x * blockDim.x)

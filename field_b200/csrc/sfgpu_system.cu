@@ -200,7 +200,7 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
     }
     // weights of lnGN sums and of the free energy (SubtractBoundaries +
     // MultiplyWithLatticeSites)
-    H->w_gn.assign(L.M, 0.0); H->w_f.assign(L.M, 0.0);
+    H->w_gn.assign(L.M, 0.0); H->w_f.assign(L.M, 0.0); H->sb.assign(L.M, 0.0);
     for (int z = 0; z < L.M; z++) {
         int c[3];
         lat_coords(L, z, c);
@@ -215,6 +215,7 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
                 else if (c[k] == last - 1 && L.bc_hi[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
             }
         }
+        H->sb[z] = keep ? w : 0.0;
         if (L.cyl) w *= H->Lx[c[0]];
         if (L.grad == 1 && !L.cyl) {   // flat MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269
             if (z == 1) w *= ladj;
@@ -400,7 +401,8 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     SFGPU_CUDA_TRY(cudaMemcpy(d_lamc_m, tcm.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
     SFGPU_CUDA_TRY(cudaMemcpy(d_lamc_p, tcp.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
     L.lamc_m = d_lamc_m; L.lamc_p = d_lamc_p;
-    if ((rc = alloc_d(&d_wgn, M)) || (rc = alloc_d(&d_wf, M))) return rc;
+    if ((rc = alloc_d(&d_wgn, M)) || (rc = alloc_d(&d_wf, M)) || (rc = alloc_d(&d_sb, M))) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpy(d_sb, H.sb.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
     SFGPU_CUDA_TRY(cudaMemcpy(d_wgn, H.w_gn.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
     SFGPU_CUDA_TRY(cudaMemcpy(d_wf, H.w_f.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
     if ((rc = alloc_i(&d_jmap, M)) || (rc = alloc_i(&d_sites, nsites))) return rc;
@@ -765,6 +767,46 @@ extern "C" int sfgpu_get_swf(sfgpu_system *s, int seg, double *g) {
     SFGPU_CUDA_TRY(cudaMemcpyAsync(g, s->d_gseg[seg], sizeof(double) * s->M, cudaMemcpyDeviceToHost, s->stream));
     SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return SFGPU_OK;
+}
+
+// F and the grand potential with their densities (SF_MolList1stO::
+// GetFreeEnergy / GetGrandPotential with GetFreeEnergyProfile and
+// GetGrandPotentialProfile, SF_MolList1stO.cpp:606-646, 815-826, 1001-1101)
+int sfgpu_system::thermo(double *F, double *Omega, double *fe, double *gp) {
+    ThermoParam tp;
+    memset(&tp, 0, sizeof(tp));
+    tp.nseg = nseg; tp.nmol = nmol;
+    for (int i = 0; i < nseg; i++) {
+        tp.phi[i] = d_phi[i];
+        tp.gseg[i] = d_gseg[i] ? d_gseg[i] : d_phi[i];
+        tp.gfull[i] = d_gfull[i] ? d_gfull[i] : d_phi[i];
+        tp.frozen[i] = freedom[i] == SFGPU_SEG_FROZEN;
+    }
+    for (int m = 0; m < nmol; m++) {
+        tp.invN[m] = 1.0 / mols[m].N;
+        tp.N[m] = (double)mols[m].N;
+        tp.lnN[m] = log((double)mols[m].N);
+        tp.chemintref[m] = mols[m].chemintref;
+        for (int i : mols[m].used) tp.mphi[m * SFGPU_MAX_SEG + i] = mols[m].d_phi[i];
+    }
+    double *dfe = (fe || gp) ? d_ginv[0] : nullptr, *dgp = (fe || gp) ? d_ginv[1] : nullptr;
+    thermo_partial<<<nblocks_red, kBlock, 0, stream>>>(H.L, tp, ct, d_wf, d_sb, (const MolScal *)d_scal, d_phib,
+                                                      dfe, dgp, d_partial);
+    finish_sums<<<1, 32, 0, stream>>>(2, nblocks_red, d_partial, d_misc);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    double v[2];
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(v, d_misc, sizeof(v), cudaMemcpyDeviceToHost, stream));
+    if (fe) SFGPU_CUDA_TRY(cudaMemcpyAsync(fe, dfe, sizeof(double) * M, cudaMemcpyDeviceToHost, stream));
+    if (gp) SFGPU_CUDA_TRY(cudaMemcpyAsync(gp, dgp, sizeof(double) * M, cudaMemcpyDeviceToHost, stream));
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (F) *F = v[0];
+    if (Omega) *Omega = v[1];
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_thermo(sfgpu_system *s, double *F, double *Omega, double *fe_profile, double *omega_profile) {
+    CHECK_SYS(s);
+    return s->thermo(F, Omega, fe_profile, omega_profile);
 }
 
 extern "C" int sfgpu_free_energy(sfgpu_system *s, double *F) {

@@ -6,6 +6,7 @@
 struct HostLat {
     DLat L;
     std::vector<double> lam_m, lam_p, lamc_m, lamc_p, Lx, w_gn, w_f;
+    std::vector<double> sb;   // SubtractBoundaries factors (0 removed, 1/2 mirror2 layers)
 };
 int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H);
 
@@ -31,7 +32,7 @@ struct sfgpu_system {
     ChiTable ct;
     // device buffers
     double *d_lam_m = nullptr, *d_lam_p = nullptr, *d_lamc_m = nullptr, *d_lamc_p = nullptr;
-    double *d_wgn = nullptr, *d_wf = nullptr;
+    double *d_wgn = nullptr, *d_wf = nullptr, *d_sb = nullptr;
     int *d_jmap = nullptr, *d_sites = nullptr;
     std::vector<double *> d_range, d_gfull, d_gseg, d_phi;
     double *d_gi = nullptr, *d_ginv[2] = {nullptr, nullptr};
@@ -92,4 +93,5 @@ struct sfgpu_system {
     int molecule_phi(int m);
     int residual_async(const double *x, double *f);
     int free_energy(double *F);
+    int thermo(double *F, double *Omega, double *fe, double *gp);
 };

@@ -18,6 +18,8 @@ persistent kernel (:class:`field_b200.batch.BatchSolver`) in ``waves``:
 equal to the number of points reproduces SFbox's chain point by point.
 Warm starts need the same iteration-variable layout; when the varied
 parameter changes it (for example ``n_layers``) every point starts cold.
+With Pure_DIIS, whose first step replaces the guess by -eta g(guess)
+(sfnewton.cpp:578-584), a warm start changes only that first gradient.
 """
 from __future__ import annotations
 

@@ -102,6 +102,14 @@ class System:
                   "sfgpu_get_mol_scalars")
         return {"lngn": a.value, "phibulk": b.value, "lnc": c.value}
 
+    def thermo(self):
+        """(F, Omega, free-energy density, grand-potential density) of the
+        last evaluation (sfgpu_thermo)."""
+        F, Om = C.c_double(), C.c_double()
+        fe, gp = np.empty(self.M), np.empty(self.M)
+        nat.check(self.lib.sfgpu_thermo(self.h, C.byref(F), C.byref(Om), _d(fe), _d(gp)), "sfgpu_thermo")
+        return F.value, Om.value, fe, gp
+
     def set_bond_orientation(self, enable: bool = True):
         """Fill bond-orientation profiles in the following evaluations
         (second-order lattices; Lat2ndO::ConnectG with PHI)."""

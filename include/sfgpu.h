@@ -183,6 +183,15 @@ int sfgpu_get_bond_orientation(sfgpu_system *sys, int molecule, int axis, double
 /* Helmholtz free energy of the last evaluation,
  * SF_MolList1stO::GetFreeEnergy (SF_MolList1stO.cpp:606-635). */
 int sfgpu_free_energy(sfgpu_system *sys, double *F);
+/* Thermodynamics of the last evaluation: F (as above) and the grand
+ * potential Omega = sum_z L(z) omega(z) (SF_MolList1stO::GetGrandPotential,
+ * SF_MolList1stO.cpp:636-646, with GetGrandPotentialProfile :1001-1101; the
+ * same formula in SF_MolList2ndO), and, for non-NULL host arrays of M
+ * doubles, the free-energy density (GetFreeEnergyProfile, :815-826) and
+ * omega(z), both after SubtractBoundaries (boundary layers 0 except
+ * surfaces, mirror2 layers halved).  At a converged solution Omega equals
+ * F - sum_i n_i mu_i (SFbox's "grand potential2", :648-661). */
+int sfgpu_thermo(sfgpu_system *sys, double *F, double *Omega, double *fe_profile, double *omega_profile);
 
 /* ---- Lattice-level (device vectors of M or 6*M doubles) ----------------- */
 /* gout = one propagator step of gin with segment weights g.  First order:

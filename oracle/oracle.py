@@ -46,6 +46,7 @@ def lib():
         l.orc_get_phibulk.restype = C.c_double
         l.orc_get_swf.argtypes = [vp, C.c_int, dp]
         l.orc_bond_orientation.argtypes = [vp, C.c_int, C.c_int, dp]
+        l.orc_thermo.argtypes = [vp, dp, dp, dp, dp]
         l.orc_free_energy.argtypes = [vp]
         l.orc_free_energy.restype = C.c_double
         l.orc_propagate.argtypes = [vp, dp, dp, dp, C.c_double, C.c_int]
@@ -107,6 +108,16 @@ class Oracle:
         if rc:
             raise ValueError(f"orc_bond_orientation failed with status {rc}")
         return out
+
+    def thermo(self):
+        """(F, Omega, free-energy density, grand-potential density) of the
+        last evaluation."""
+        F, Om = C.c_double(), C.c_double()
+        fe, gp = np.empty(self.M), np.empty(self.M)
+        rc = lib().orc_thermo(self.h, C.byref(F), C.byref(Om), _d(fe), _d(gp))
+        if rc:
+            raise ValueError(f"orc_thermo failed with status {rc}")
+        return F.value, Om.value, fe, gp
 
     def phibulk(self, mol):
         return lib().orc_get_phibulk(self.h, mol)

@@ -41,6 +41,7 @@ typedef struct {
     double *lamc_m, *lamc_p;    /* 1D curved: contact tables with lambda_chi */
     double *w_gn;      /* weights of interior sites in lnGN sums */
     double *w_f;       /* weights in the free-energy sum (surfaces included) */
+    double *sb;        /* SubtractBoundaries factors: 0 on removed boundary layers, 1/2 on mirror2 layers */
     int K;             /* 2nd-order direction components: 3 (1D), 5 (2D), 6 (3D); 1 first order */
     int sw_lo[3], sw_hi[3];   /* 2nd order: +/- components swap at a boundary copy */
 } olat;
@@ -244,6 +245,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
         Lat3D.cpp:1591-1633) */
     L->w_gn = calloc(L->M, sizeof(double));
     L->w_f = calloc(L->M, sizeof(double));
+    L->sb = calloc(L->M, sizeof(double));
     for (int z = 0; z < L->M; z++) {
         int c[3]; coords(L, z, c);
         double w = 1.0; int keep = 1, interior = 1;
@@ -256,6 +258,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
                 else if (c[k] == last - 1 && L->bc_hi[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
             }
         }
+        L->sb[z] = keep ? w : 0.0;
         if (L->cyl) w *= L->Lx[c[0]];
         if (L->grad == 1 && !L->cyl) {   /* flat: Lat1DFlat.cpp:266-269 */
             if (z == 1) w *= L->ladj;
@@ -271,7 +274,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
 }
 
 static void olat_free(olat *L) {
-    free(L->lam_m); free(L->lam_p); free(L->lamc_m); free(L->lamc_p); free(L->Lx); free(L->w_gn); free(L->w_f);
+    free(L->lam_m); free(L->lam_p); free(L->lamc_m); free(L->lamc_p); free(L->Lx); free(L->w_gn); free(L->w_f); free(L->sb);
 }
 
 /* one first-order step gout = G * stencil(gin); gin must carry valid
@@ -1054,6 +1057,85 @@ double orc_free_energy(orc_system *s) {
         F += w * (-entropy + contact);
     }
     return F;
+}
+
+/* The free-energy density (SF_MolList1stO::GetFreeEnergyProfile,
+   SF_MolList1stO.cpp:815-826) and the grand-potential density
+   (GetGrandPotentialProfile, :1001-1101; the same in SF_MolList2ndO.cpp)
+   without charges, external potentials or grafted chains, both after
+   SubtractBoundaries; F and Omega = sum_z L(z) density(z)
+   (GetFreeEnergy :606-635, GetGrandPotential :636-646). */
+int orc_thermo(orc_system *s, double *F, double *Omega, double *fe, double *gp) {
+    if (!s->evaluated) return SFGPU_ERR_INVALID;
+    int M = s->L.M, ns = s->nseg;
+    double Ft = 0, Ot = 0;
+    for (int z = 0; z < M; z++) {
+        double entropy = 0, contact = 0, omega = 0;
+        for (int m = 0; m < s->nmol; m++) {
+            omol *o = &s->mol[m];
+            double phim = 0;
+            for (int a = 0; a < o->nseg_used; a++) phim += o->phi[(size_t)o->used[a] * M + z];
+            entropy -= (phim / o->N) * (log((double)o->N) + o->lnc);
+            contact -= phim * o->chemintref;
+        }
+        for (int m = 0; m < s->nmol; m++) {
+            omol *o = &s->mol[m];
+            for (int a = 0; a < o->nseg_used; a++) {
+                int i = o->used[a];
+                double G = s->swf[(size_t)i * M + z];
+                if (G > 0) entropy -= o->phi[(size_t)i * M + z] * log(G);
+            }
+        }
+        for (int i = 0; i < ns; i++) {
+            double ci = 0;
+            for (int j = 0; j < ns; j++) {
+                double x = s->chi[i * ns + j];
+                if (x != 0) ci += x * s->rho[(size_t)j * M + z];
+            }
+            contact += 0.5 * s->phi[(size_t)i * M + z] * ci;
+        }
+        /* grand potential: molecules, then u' of every liquid state, then the
+           contact pairs of liquid states, in the reference's order */
+        for (int m = 0; m < s->nmol; m++) {
+            omol *o = &s->mol[m];
+            double phim = 0;
+            for (int a = 0; a < o->nseg_used; a++) phim += o->phi[(size_t)o->used[a] * M + z];
+            if (phim > 0) omega -= (phim - o->phibulk) / o->N;
+        }
+        for (int i = 0; i < ns; i++) {
+            if (s->freedom[i] == SFGPU_SEG_FROZEN) continue;
+            double G = s->swf_full[(size_t)i * M + z], up = 0;
+            if (G > 0) {
+                double ci = 0, cb = 0;
+                for (int j = 0; j < ns; j++) {
+                    double x = s->chi[i * ns + j];
+                    if (x != 0) { ci += x * s->rho[(size_t)j * M + z]; cb += x * s->phib[j]; }
+                }
+                up = -log(G);
+                up -= ci;
+                up += cb;
+            }
+            omega -= up * s->phi[(size_t)i * M + z];
+        }
+        for (int i = 0; i < ns; i++) {
+            if (s->freedom[i] == SFGPU_SEG_FROZEN) continue;
+            double p1 = s->phi[(size_t)i * M + z];
+            for (int j = 0; j < ns; j++) {
+                if (s->freedom[j] == SFGPU_SEG_FROZEN) continue;
+                double x = s->chi[i * ns + j];
+                omega -= 0.5 * x * p1 * s->rho[(size_t)j * M + z];
+                if (p1 > 0) omega += 0.5 * x * s->phib[i] * s->phib[j];
+            }
+        }
+        double f = -entropy + contact;
+        Ft += s->L.w_f[z] * f;
+        Ot += s->L.w_f[z] * omega;
+        if (fe) fe[z] = f * s->L.sb[z];
+        if (gp) gp[z] = omega * s->L.sb[z];
+    }
+    if (F) *F = Ft;
+    if (Omega) *Omega = Ot;
+    return SFGPU_OK;
 }
 
 int orc_propagate(const orc_system *s, const double *gin, const double *g, double *gout, double S, int backward) {

@@ -33,6 +33,7 @@ int    orc_get_phi(const orc_system *s, int seg, double *phi);         /* state 
 int    orc_get_mol_phi(const orc_system *s, int mol, int seg, double *phi);
 double orc_get_lngn(const orc_system *s, int mol);
 int    orc_bond_orientation(const orc_system *s, int mol, int axis, double *out);  /* 2nd order, M */
+int    orc_thermo(orc_system *s, double *F, double *Omega, double *fe, double *gp);  /* profiles M or NULL */
 double orc_get_phibulk(const orc_system *s, int mol);
 int    orc_get_swf(const orc_system *s, int seg, double *g);           /* segment G (masked) */
 double orc_free_energy(orc_system *s);                                 /* SF_MolList1stO.cpp:606 */

@@ -244,3 +244,20 @@ def test_bond_orientation_errors(gpu_lib):
     s2 = System(CASES["3d_2nd_brush"]())
     with pytest.raises(SfgpuError):
         s2.bond_orientation(0, 0)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_thermo(gpu_lib, case):
+    """F, the grand potential and both densities against the oracle."""
+    spec = CASES[case]()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    x = random_x(spec, seed=13, scale=0.2)
+    sys_.residual(x)
+    o.residual(x)
+    Fg, Og, feg, gpg = sys_.thermo()
+    Fc, Oc, fec, gpc = o.thermo()
+    assert abs(Fg - Fc) <= 1e-11 * max(1.0, abs(Fc))
+    assert abs(Og - Oc) <= 1e-11 * max(1.0, abs(Oc), abs(Fc))
+    assert Fg == pytest.approx(sys_.free_energy(), rel=1e-14, abs=1e-14)
+    assert rel(feg, fec) <= TOL_EVAL and rel(gpg, gpc) <= TOL_EVAL

@@ -10,20 +10,23 @@ from oracle.oracle import Oracle
 pytestmark = pytest.mark.gpu
 
 SWEEP = (configs.C1_INPUT.format(n=40, N=20, phib=0.01, chi_aw=0.0, chi_as=-1.0)
-         + "var : mon : A : chi - W\nvar : mon : step : 0.1\nvar : mon : end_value : 1.0\nvar : mon : type : real\n"
+         + "var : mon : A : chi - W\nvar : mon : step : 0.1\nvar : mon : end_value : 0.8\nvar : mon : type : real\n"
          + "newton : isaac : tolerance : 1e-9\n")
 
 
-def test_sweep_waves_agree_and_warm_starts_help(gpu_lib):
-    """The 11 points of a chi sweep solved in one batch from zero, in three
+def test_sweep_schedules_agree(gpu_lib):
+    """The 9 points of a chi sweep solved in one batch from zero, in three
     waves, and as SFbox's chain (each point from its predecessor): every point
     converges, satisfies the oracle's equations, and the three schedules reach
-    the same solutions; warm-started points need fewer iterations."""
+    the same solutions.  (At chi = 1 Pure_DIIS from zero fails on the oracle
+    too, so the sweep stops at 0.8.  Pure_DIIS's first step replaces the
+    guess by -eta g(guess), sfnewton.cpp:578-584, so a warm start changes
+    only that first gradient and need not save iterations.)"""
     calc = parse_input(SWEEP)[-1]
     cold = solve_sweep(calc, waves=1, m=5)
     three = solve_sweep(calc, waves=3, m=5)
     chain = solve_sweep(calc, waves=100, m=5)
-    assert len(cold.x) == 11 and (chain.wave == np.arange(11)).all()
+    assert len(cold.x) == 9 and (chain.wave == np.arange(9)).all()
     for res in (cold, three, chain):
         assert res.converged.all(), res.status
     for i, spec in enumerate(cold.specs):
@@ -33,4 +36,4 @@ def test_sweep_waves_agree_and_warm_starts_help(gpu_lib):
             assert np.linalg.norm(o.residual(res.x[i])) < 1e-8
         np.testing.assert_allclose(three.x[i], cold.x[i], rtol=0, atol=1e-6)
         np.testing.assert_allclose(chain.x[i], cold.x[i], rtol=0, atol=1e-6)
-    assert chain.iterations[1:].mean() < cold.iterations[1:].mean()
+    assert (three.wave == np.arange(9) % 3).all()

@@ -492,3 +492,64 @@ def test_curved_second_order_large_radius_is_flat():
     oc.residual(x)
     of.residual(x)
     np.testing.assert_allclose(oc.phi(0)[1:-1], of.phi(0)[1:-1], rtol=1e-4)
+
+
+def _grand_potential2(spec, o):
+    """F - sum_i n_i mu_i with n_i mu_i of SF_MolList1stO::GetNumMolTimesChemPot
+    (SF_MolList1stO.cpp:463-521; molecules without pinned or grafted
+    segments, no reactions), restated here independently of the oracle."""
+    F = o.thermo()[0]
+    ns = len(spec.segments)
+    chi = np.asarray(spec.chi, dtype=float)
+    mols = spec.molecules
+    w = o.site_weights()
+    N = [sum(n for _, n in mol.blocks) for mol in mols]
+    cnt = np.zeros((len(mols), ns))
+    for m, mol in enumerate(mols):
+        for seg, n in mol.blocks:
+            cnt[m, seg] += n
+    phib_m = [o.phibulk(m) for m in range(len(mols))]
+    phib_s = np.array([sum(phib_m[m] * cnt[m, i] / N[m] for m in range(len(mols))) for i in range(ns)])
+    cib = chi @ phib_s
+    total = 0.0
+    for m in range(len(mols)):
+        used = [i for i in range(ns) if cnt[m, i] > 0]
+        th_seg = {i: float((o.mol_phi(m, i) * w).sum()) for i in used}
+        th = sum(th_seg.values())
+        f = cnt[m] / N[m]
+        cref = 0.5 * sum(f[i] * f[j] * chi[i, j] for i in used for j in used)
+        v = (np.log(phib_m[m]) + 1) * th / N[m]
+        v += th * (-sum(phib_m[k] / N[k] for k in range(len(mols))))
+        v += sum(th_seg[i] * cib[i] for i in used) - th * cref
+        v -= 0.5 * th * float((phib_s * cib).sum())
+        total += v
+    return F - total
+
+
+@pytest.mark.parametrize("which", ["adsorption", "2d_surface", "sphere"])
+def test_grand_potential_equals_F_minus_n_mu_at_convergence(which):
+    """At the self-consistent solution the grand potential summed from its
+    density equals F - sum n mu (SFbox prints both, 'grand potential' and
+    'grand potential2'); away from it they differ."""
+    from cases import CASES
+    spec = {"adsorption": lambda: configs.flat_adsorption(n=40, N=21)[0],
+            "2d_surface": CASES["2d_flat_surface"], "sphere": CASES["1d_sphere_colloid"]}[which]()
+    o = Oracle(spec)
+    x, rc, it, err = o.solve_diis(np.zeros(spec.n_itvar()), tol=1e-11, maxit=20000, m=10, eta=0.3)
+    assert rc == 0
+    o.residual(x)
+    F, Om, fe, gp = o.thermo()
+    assert Om == pytest.approx(_grand_potential2(spec, o), abs=1e-9 * max(1.0, abs(F)))
+    assert abs(Om) > 1e-6          # a surface excess, not the bulk
+    o.residual(x + 0.05)
+    assert abs(o.thermo()[1] - _grand_potential2(spec, o)) > 1e-4
+
+
+def test_grand_potential_density_vanishes_in_the_bulk():
+    """u = 0 between mirrors is the bulk: omega(z) = 0 everywhere."""
+    spec = homopolymer_1d(n=15, N=7, chi=0.6)
+    o = Oracle(spec)
+    o.residual(np.zeros(o.nvar))
+    F, Om, fe, gp = o.thermo()
+    np.testing.assert_allclose(gp, 0.0, atol=1e-15)
+    assert abs(Om) < 1e-13
