@@ -27,9 +27,9 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "cyl_micelle Lat2DCyl1stO 128x128 (r,z), (A)20(B)20 + W solvent, phibulk 0.005, chi_AW 1.6"
 METRIC = "converged SCF solves/s (resid<1e-7)"
-# ncu: 106.16 GB read + 77.81 GB written by one batch_diis_kernel launch of
+# ncu: 93.36 GB read + 76.00 GB written by one batch_diis_kernel launch of
 # 148 instances that made 148 * (33.63 + 1) residual evaluations
-DRAM_BYTES_PER_INSTANCE_ITERATION = (106.159e9 + 77.811e9) / (148 * 34.63)
+DRAM_BYTES_PER_INSTANCE_ITERATION = (93.365e9 + 76.002e9) / (148 * 34.63)
 TOL = 1e-7
 DIIS_M, DIIS_ETA, MAXIT = 10, 0.1, 2000
 
