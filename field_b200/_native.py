@@ -31,6 +31,7 @@ PROTOTYPES = {
     "sfgpu_get_mol_scalars": (i32, [vp, i32, dp, dp, dp]),
     "sfgpu_system_set_bond_orientation": (i32, [vp, i32]),
     "sfgpu_thermo": (i32, [vp, dp, dp, dp, dp]),
+    "sfgpu_lattice_weights": (i32, [vp, dp, dp]),
     "sfgpu_get_bond_orientation": (i32, [vp, i32, i32, dp]),
     "sfgpu_get_swf": (i32, [vp, i32, dp]),
     "sfgpu_free_energy": (i32, [vp, dp]),

@@ -804,6 +804,13 @@ int sfgpu_system::thermo(double *F, double *Omega, double *fe, double *gp) {
     return SFGPU_OK;
 }
 
+extern "C" int sfgpu_lattice_weights(sfgpu_system *s, double *w_lngn, double *w_sum) {
+    CHECK_SYS(s);
+    if (w_lngn) memcpy(w_lngn, s->H.w_gn.data(), sizeof(double) * s->M);
+    if (w_sum) memcpy(w_sum, s->H.w_f.data(), sizeof(double) * s->M);
+    return SFGPU_OK;
+}
+
 extern "C" int sfgpu_thermo(sfgpu_system *s, double *F, double *Omega, double *fe_profile, double *omega_profile) {
     CHECK_SYS(s);
     return s->thermo(F, Omega, fe_profile, omega_profile);

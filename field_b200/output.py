@@ -1,0 +1,191 @@
+"""Output files of a calculation in SFbox's formats (Output.cpp).
+
+A solved calculation is turned into SFbox's output lines -- ``class : name :
+key : value`` with profiles attached -- restricted to what the SCF path
+computes: the system's free energy and grand potential (with their
+densities), the lattice description, the chi list, per segment phibulk / theta /
+theta excess with the phi and G profiles, per molecule the quantities of
+SF_Molecule::GetOutput (SF_Molecule.cpp:355-465) that need no analysis
+beyond the path, and the solver's iteration record (SF_Solve.cpp:191-211).
+The keys are SFbox's.  Two writers:
+
+* ``ana`` (Output::OutputAna, Output.cpp:322-416): a ``system delimiter``
+  header on a new file, then every line ``c : n : k : v``; a profile line is
+  followed by its values one per line (boundary layers included unless
+  ``write_bounds`` is false), and each calculation ends with ``system
+  delimiter`` and a blank line.
+* ``kal`` (Output::OutputKal, Output.cpp:640-726): one header row of
+  ``c : n : k`` names of the scalar lines, tab separated, on a new file, then
+  one row of values per calculation.
+
+Scalars are printed with ``accuracy`` significant digits (default
+int(-log10(tolerance) + 0.5), SF_Box.cpp:93); profile values with six, as a
+default C++ stream prints them.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from .desc import (BOUND_NAMES, GEOM_CYLINDRICAL, GEOM_SPHERICAL, MOL_FREE, MOL_RESTRICTED, SEG_FROZEN,
+                   SEG_PINNED)
+from .sfinput import Key
+
+_BOUND_TEXT = {v: k for k, v in BOUND_NAMES.items()}
+
+
+@dataclass
+class OutputLine:
+    cls: str
+    name: str
+    key: str
+    value: str
+    profile: Optional[np.ndarray] = None
+
+
+def _names(calc: Dict[Key, str], cls: str, default: str) -> str:
+    for (c, n, _p) in calc:
+        if c == cls:
+            return n
+    return default
+
+
+def _real(v: float, acc: int) -> str:
+    return f"{v:.{acc}g}"
+
+
+def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: int, error: float,
+                 tolerance: float, iterationlimit: int, calc_number: int,
+                 accuracy: Optional[int] = None) -> List[OutputLine]:
+    """The output lines of one solved calculation.  sys_ is a
+    field_b200.system.System; x its converged iteration variables."""
+    acc = accuracy if accuracy is not None else int(-math.log10(tolerance) + 0.5)
+    sys_.residual(x)
+    F, Om, fe, gp = sys_.thermo()
+    w_lngn, w_sum = sys_.lattice_weights()
+    out: List[OutputLine] = []
+    R = lambda c, n, k, v: out.append(OutputLine(c, n, k, _real(float(v), acc)))
+    T = lambda c, n, k, v: out.append(OutputLine(c, n, k, str(v)))
+    P = lambda c, n, k, p: out.append(OutputLine(c, n, k, "profile", np.asarray(p, dtype=float)))
+    sname = _names(calc, "sys", "noname")
+    T("sys", sname, "calculation number", calc_number)
+    T("sys", sname, "matrix_approach", "second_order" if spec.lattice.order == 2 else "first_order")
+    R("sys", sname, "grand potential", Om)
+    R("sys", sname, "free energy", F)
+    P("sys", sname, "free energy density", fe)
+    P("sys", sname, "grand potential density", gp)
+    lat = spec.lattice
+    lname = _names(calc, "lat", "lat")
+    T("lat", lname, "gradients", lat.gradients)
+    geom = {GEOM_CYLINDRICAL: "cylindrical", GEOM_SPHERICAL: "spherical"}.get(lat.geometry, "flat")
+    T("lat", lname, "geometry", geom)
+    axes = [""] if lat.gradients == 1 else ["_x", "_y", "_z"][:lat.gradients]
+    for d, a in enumerate(axes):
+        T("lat", lname, "n_layers" + a, lat.n_layers[d])
+        T("lat", lname, "lowerbound" + a, _BOUND_TEXT.get(lat.bound_lo[d], "?"))
+        T("lat", lname, "upperbound" + a, _BOUND_TEXT.get(lat.bound_hi[d], "?"))
+    R("lat", lname, "lambda", lat.lam)
+    # chi list, then the segments (SF_SegmentList::GetOutput, SF_SegmentList.cpp:387-405;
+    # SF_Segment::GetOutput, SF_Segment.cpp:345-402)
+    ns = len(spec.segments)
+    chi = np.asarray(spec.chi, dtype=float).reshape(ns, ns)
+    for i in range(ns):
+        for j in range(ns):
+            if i != j:
+                R("chi list", spec.segments[i].name, "chi - " + spec.segments[j].name, chi[i, j])
+    sites = float(w_sum.sum())
+    mols = spec.molecules
+    N = [sum(n for _, n in m.blocks) for m in mols]
+    phib_m = [sys_.mol_scalars(m)["phibulk"] for m in range(len(mols))]
+    for i, seg in enumerate(spec.segments):
+        fr = {SEG_FROZEN: "frozen", SEG_PINNED: "pinned"}.get(seg.freedom, "free")
+        T("mon", seg.name, "freedom", fr)
+        phi = sys_.phi(i)
+        pb = 0.0
+        if seg.freedom != SEG_FROZEN:
+            for m, mol in enumerate(mols):
+                cnt = sum(n for s, n in mol.blocks if s == i)
+                pb += phib_m[m] * cnt / N[m]
+        R("mon", seg.name, "phibulk", pb)
+        theta = float((w_sum * phi).sum())
+        R("mon", seg.name, "theta", theta)
+        R("mon", seg.name, "theta excess", theta - sites * pb)
+        P("mon", seg.name, "phi", phi)
+        if seg.freedom != SEG_FROZEN:
+            P("mon", seg.name, "G", sys_.swf(i))
+    # molecules (SF_Molecule::GetOutput, SF_Molecule.cpp:355-465)
+    for m, mol in enumerate(mols):
+        sc = sys_.mol_scalars(m)
+        fr = {MOL_FREE: "free", MOL_RESTRICTED: "restricted"}.get(mol.freedom, "solvent")
+        T("mol", mol.name, "freedom", fr)
+        R("mol", mol.name, "phibulk", sc["phibulk"])
+        R("mol", mol.name, "log(phibulk)", math.log10(sc["phibulk"]) if sc["phibulk"] > 0 else 0.0)
+        used = sorted({s for s, _ in mol.blocks})
+        phi = sum(sys_.mol_phi(m, s) for s in used)
+        theta = float((w_sum * phi).sum())
+        exc = float((w_sum * np.where(phi > 0, phi - sc["phibulk"], phi)).sum())
+        R("mol", mol.name, "phi-av", theta / sites)
+        R("mol", mol.name, "theta", theta)
+        R("mol", mol.name, "theta excess", exc)
+        R("mol", mol.name, "n", theta / N[m])
+        R("mol", mol.name, "n exc", exc / N[m])
+        T("mol", mol.name, "composition", "".join(f"({spec.segments[s].name}){n}" for s, n in mol.blocks))
+        T("mol", mol.name, "chainlength", N[m])
+        R("mol", mol.name, "ln(G(N|1))", sc["lngn"])
+        R("mol", mol.name, "ln(norm_restricted)" if mol.freedom == MOL_RESTRICTED else "ln(norm_free)", sc["lnc"])
+        P("mol", mol.name, "phi", phi)
+    nname = _names(calc, "newton", "noname")
+    T("newton", nname, "iterations", int(iterations))
+    T("newton", nname, "iterationlimit", int(iterationlimit))
+    R("newton", nname, "accuracy", error)
+    R("newton", nname, "tolerance", tolerance)
+    T("newton", nname, "number iter var", spec.n_itvar())
+    return out
+
+
+def write_ana(path: str, lines: List[OutputLine], first: bool, write_bounds: bool = True,
+              lattice_shape: Tuple[int, ...] = ()) -> None:
+    """Append one calculation in the ana format (see the module docstring)."""
+    interior = None
+    if not write_bounds and lattice_shape:
+        mask = np.zeros(lattice_shape, bool)
+        mask[(slice(1, -1),) * len(lattice_shape)] = True
+        interior = mask.ravel()
+    with open(path, "w" if first else "a") as f:
+        if first:
+            f.write("system delimiter\n\n")
+        for ln in lines:
+            f.write(f"{ln.cls} : {ln.name} : {ln.key} : {ln.value}\n")
+            if ln.profile is not None:
+                vals = ln.profile if interior is None else ln.profile[interior]
+                f.write("".join(f"{v:g}\n" for v in vals))
+        f.write("system delimiter\n\n")
+
+
+def write_kal(path: str, lines: List[OutputLine], first: bool) -> None:
+    """Append one calculation in the kal format (see the module docstring)."""
+    scal = [ln for ln in lines if ln.profile is None]
+    with open(path, "w" if first else "a") as f:
+        if first:
+            f.write("\t".join(f"{ln.cls} : {ln.name} : {ln.key}" for ln in scal) + "\n")
+        f.write("\t".join(ln.value for ln in scal) + "\n")
+
+
+def output_requests(calc: Dict[Key, str]) -> List[Tuple[str, str, Dict[str, str]]]:
+    """The ``output : <file> : ...`` statements: (file name, type, parameters)."""
+    names: List[str] = []
+    for (c, n, _p) in calc:
+        if c == "output" and n not in names:
+            names.append(n)
+    out = []
+    for n in names:
+        params = {p: v for (c, nn, p), v in calc.items() if c == "output" and nn == n}
+        t = params.get("type")
+        if t not in ("ana", "kal"):
+            raise ValueError(f"output : {n} : type : {t} is not written here (ana and kal are)")
+        out.append((n, t, params))
+    return out

@@ -102,6 +102,12 @@ class System:
                   "sfgpu_get_mol_scalars")
         return {"lngn": a.value, "phibulk": b.value, "lnc": c.value}
 
+    def lattice_weights(self):
+        """(weights of lnGN sums, weights of lattice sums such as F and theta)."""
+        a, b = np.empty(self.M), np.empty(self.M)
+        nat.check(self.lib.sfgpu_lattice_weights(self.h, _d(a), _d(b)), "sfgpu_lattice_weights")
+        return a, b
+
     def thermo(self):
         """(F, Omega, free-energy density, grand-potential density) of the
         last evaluation (sfgpu_thermo)."""

@@ -192,6 +192,12 @@ int sfgpu_free_energy(sfgpu_system *sys, double *F);
  * surfaces, mirror2 layers halved).  At a converged solution Omega equals
  * F - sum_i n_i mu_i (SFbox's "grand potential2", :648-661). */
 int sfgpu_thermo(sfgpu_system *sys, double *F, double *Omega, double *fe_profile, double *omega_profile);
+/* Host copies (M doubles each, either may be NULL) of the site weights of
+ * lnGN sums (interior sites, mirror2 halves, lattice sites L(z) on curved
+ * lattices) and of sums over the lattice such as F or theta
+ * (SubtractBoundaries then MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269,
+ * 410-415; Lat1DCylinder.cpp:126-141). */
+int sfgpu_lattice_weights(sfgpu_system *sys, double *w_lngn, double *w_sum);
 
 /* ---- Lattice-level (device vectors of M or 6*M doubles) ----------------- */
 /* gout = one propagator step of gin with segment weights g.  First order:

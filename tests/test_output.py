@@ -1,0 +1,111 @@
+"""ana / kal writers and output statements (host logic, no GPU)."""
+import numpy as np
+import pytest
+
+from field_b200.output import OutputLine, output_requests, write_ana, write_kal
+from field_b200.sfinput import parse_input
+
+
+def _lines(F):
+    return [OutputLine("sys", "noname", "free energy", f"{F:.7g}"),
+            OutputLine("sys", "noname", "free energy density", "profile", np.array([0.0, 1.5, 2.25, 0.0])),
+            OutputLine("mol", "pol", "theta", "3.5")]
+
+
+def test_ana_blocks_and_profiles(tmp_path):
+    p = str(tmp_path / "out.ana")
+    write_ana(p, _lines(-1.25), first=True)
+    write_ana(p, _lines(-2.5), first=False)
+    text = open(p).read().splitlines()
+    assert text[0] == "system delimiter" and text[1] == ""
+    assert text[2] == "sys : noname : free energy : -1.25"
+    assert text[3] == "sys : noname : free energy density : profile"
+    assert text[4:8] == ["0", "1.5", "2.25", "0"]
+    assert text.count("system delimiter") == 3
+    assert "sys : noname : free energy : -2.5" in text
+    write_ana(p, _lines(-1.0), first=True, write_bounds=False, lattice_shape=(4,))
+    text = open(p).read().splitlines()
+    assert text[4:6] == ["1.5", "2.25"] and text[6] == "mol : pol : theta : 3.5"
+
+
+def test_kal_header_once_then_rows(tmp_path):
+    p = str(tmp_path / "out.kal")
+    for i, F in enumerate([-1.0, -2.0, -3.0]):
+        write_kal(p, _lines(F), first=(i == 0))
+    rows = [r.split("\t") for r in open(p).read().splitlines()]
+    assert rows[0] == ["sys : noname : free energy", "mol : pol : theta"]
+    assert [r[0] for r in rows[1:]] == ["-1", "-2", "-3"] and all(len(r) == 2 for r in rows)
+
+
+def test_output_requests():
+    calc = parse_input("output : run.ana : type : ana\noutput : run.kal : type : kal\n"
+                       "output : run.kal : append : true\n")[0]
+    req = output_requests(calc)
+    assert [(n, t) for n, t, _ in req] == [("run.ana", "ana"), ("run.kal", "kal")]
+    with pytest.raises(ValueError):
+        output_requests(parse_input("output : x.vtk : type : vtk\n")[0])
+
+
+class _OracleSystem:
+    """The parts of field_b200.system.System that output_lines reads, served
+    by the oracle on a flat 1D lattice (interior weights 1, boundaries 0)."""
+
+    def __init__(self, spec):
+        from oracle.oracle import Oracle
+        self.o, self.spec = Oracle(spec), spec
+
+    def residual(self, x):
+        return self.o.residual(x)
+
+    def thermo(self):
+        return self.o.thermo()
+
+    def lattice_weights(self):
+        w = np.ones(self.o.M)
+        w[0] = w[-1] = 0.0
+        return w, w
+
+    def mol_scalars(self, m):
+        return {"lngn": self.o.lngn(m), "phibulk": self.o.phibulk(m), "lnc": 0.0}
+
+    def phi(self, s):
+        return self.o.phi(s)
+
+    def swf(self, s):
+        return self.o.swf(s)
+
+    def mol_phi(self, m, s):
+        return self.o.mol_phi(m, s)
+
+
+def test_output_lines_keys_and_sums():
+    """SFbox's keys in SFbox's order; theta sums over interior sites,
+    segment theta excess = theta - sites * phibulk (SF_Segment.cpp:370-392),
+    molecule theta excess over phi > 0 only (SF_Molecule.cpp:727-749)."""
+    from field_b200 import configs
+    from field_b200.output import output_lines
+    from field_b200.sfinput import build_system
+    n = 20
+    calc = parse_input(configs.C1_INPUT.format(n=n, N=10, phib=0.01, chi_aw=0.5, chi_as=-1.0))[0]
+    spec, st = build_system(calc)
+    sys_ = _OracleSystem(spec)
+    x, rc, it, err = sys_.o.solve_diis(np.zeros(spec.n_itvar()), tol=1e-9, maxit=3000, m=5, eta=0.1)
+    assert rc == 0
+    lines = output_lines(calc, spec, sys_, x, it, err, st.tolerance, st.iterationlimit, 1)
+    d = {(l.cls, l.name, l.key): l for l in lines}
+    assert [l.cls for l in lines][:2] == ["sys", "sys"]
+    assert d[("sys", "noname", "free energy")].value == f"{sys_.o.thermo()[0]:.7g}"
+    assert float(d[("chi list", "A", "chi - W")].value) == 0.5
+    assert float(d[("chi list", "A", "chi - S")].value) == -1.0
+    phiA = sys_.o.phi(1)
+    theta = phiA[1:-1].sum()
+    assert float(d[("mon", "A", "theta")].value) == pytest.approx(theta, rel=1e-6)
+    assert float(d[("mon", "A", "theta excess")].value) == pytest.approx(theta - n * 0.01, rel=1e-6)
+    assert float(d[("mol", "pol", "theta")].value) == pytest.approx(theta, rel=1e-6)
+    assert float(d[("mol", "pol", "n")].value) == pytest.approx(theta / 10, rel=1e-6)
+    assert float(d[("mol", "pol", "phi-av")].value) == pytest.approx(theta / n, rel=1e-6)
+    assert d[("mol", "pol", "composition")].value == "(A)10"
+    assert d[("newton", "isaac", "iterations")].value == str(it)
+    assert d[("mon", "S", "freedom")].value == "frozen" and ("mon", "S", "G") not in d
+    mol_keys = [l.key for l in lines if l.cls == "mol" and l.name == "pol"]
+    assert mol_keys[:8] == ["freedom", "phibulk", "log(phibulk)", "phi-av", "theta", "theta excess", "n", "n exc"]
