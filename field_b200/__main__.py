@@ -28,7 +28,7 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     from .output import output_lines, output_requests, write_ana, write_kal
     from .sfinput import build_system, parse_input
-    from .sweep import solve_sweep, sweep_calculations
+    from .sweep import batchable, solve_sweep, sweep_calculations
     from .system import System
 
     with open(a.input) as f:
@@ -43,7 +43,7 @@ def main(argv=None) -> int:
         var, points = sweep_calculations(calc)
         built = [build_system(p) for p in points]
         st = built[0][1]
-        if len(points) > 1 and all(s.lattice.order == 1 for s, _ in built):
+        if len(points) > 1 and all(batchable(s) for s, _ in built):
             waves = a.waves if a.waves > 0 else len(points)
             same = x_prev is not None and len(x_prev) == built[0][0].n_itvar()
             res = solve_sweep(calc, waves=waves, x0=x_prev if same else None, tol=st.tolerance,

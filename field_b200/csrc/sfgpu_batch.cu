@@ -172,7 +172,11 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
     int maxM = 1;
     b->offset.resize(n);
     for (int i = 0; i < n && !rc; i++) {
-        if (descs[i].lattice.order != 1) { rc = SFGPU_ERR_UNSUPPORTED; break; }
+        if (descs[i].lattice.order != 1) { rc = fail_unsupported("batched second-order lattices"); break; }
+        if (descs[i].lattice.gradients == 3 && descs[i].lattice.lattice_type != SFGPU_LATTICE_STANDARD) {
+            rc = fail_unsupported("batched FCC, HEX and stencils 3D lattices");
+            break;
+        }
         sfgpu_system *s = new sfgpu_system();
         s->stream = b->stream;
         rc = s->setup(&descs[i]);

@@ -195,7 +195,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
             const double *src = gi + (size_t)(t - 1) * M;
             double *dst = gi + (size_t)t * M;
             for_interior4(L, threadIdx.x, blockDim.x,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, src, G, k, nlast); },
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, src, G, k, nlast); },
                 [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
             __syncthreads();
         }
@@ -203,7 +203,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         if (N % 2 == 1) {
             double *dst = bufA;
             for_interior4(L, threadIdx.x, blockDim.x,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, cur, G, k, nlast); },
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
                 [&](const RowInfo &R, int k, double out) {
                     const int z = R.base + k;
                     dst[z] = out;
@@ -216,7 +216,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
             const double *other = gi + (size_t)(N - sp) * M;
             double *dst = bufA;
             for_interior4_acc(L, threadIdx.x, blockDim.x, phi, other,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, cur, G, k, nlast); },
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
                 [&](const RowInfo &R, int k, double out, double ph, double ot) {
                     const int z = R.base + k;
                     dst[z] = out;
@@ -239,7 +239,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         double *dst = gi + (size_t)t * M;
         const double *G = gof(o.seg[t]);
         for_interior4(L, threadIdx.x, blockDim.x,
-            [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, src, G, k, nlast); },
+            [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, src, G, k, nlast); },
             [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
         __syncthreads();
     }
@@ -264,7 +264,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         double *phi = o.phi[sg];
         double *dst = bufA;
         for_interior4_acc(L, threadIdx.x, blockDim.x, phi, gf,
-            [&](const RowInfo &R, int k, int nlast) { return prop1_row(L, R, cur, G, k, nlast); },
+            [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
             [&](const RowInfo &R, int k, double out, double ph, double ot) {
                 const int z = R.base + k;
                 dst[z] = out;
@@ -298,7 +298,7 @@ __device__ __forceinline__ void site_residual(const InstDesc &I, const BlockShar
         if (i >= nseg) continue;
         bool need = false;
         for (int c = 0; c < ncl; c++) need |= I.ct.chi[I.rep[c] * SFGPU_MAX_SEG + i] != 0;
-        if (need) rho[i] = side_fraction(L, I.phi[i], z);
+        if (need) rho[i] = side_fraction<false>(L, I.phi[i], z);
     }
     double u[kResMax];
     double av = 0;

@@ -35,6 +35,10 @@ struct DLat {
     // the +d and -d components
     int K;
     int sw_lo[3], sw_hi[3];
+    // 3D lattice type (SFGPU_LATTICE_*) and the contact weights of the
+    // 27-site cube (centre, face, edge, corner) for STANDARD, STENCILS, FCC
+    int ltype;
+    double sl[4];
 };
 
 struct ChiTable {              // passed by value: small interaction tables
@@ -85,6 +89,50 @@ __device__ inline int swap_dir(int k, int sw) {
     return k;
 }
 
+// First-order step of the twelve-neighbour 3D lattices, g * sum / 12 with
+// the neighbours (dx, dy, dz) in the reference's summation order; v(dx, dy,
+// dz) returns the input value at that offset.
+//   FCC (Lat3DFCC1stO.cpp:79-91): -x-y, +x+y, -x+y, +x-y, -y-z, +y+z, -y+z,
+//       +y-z, -x-z, +x+z, -x+z, +x-z
+//   HEX (Lat3DHEX1stO.cpp:79-91): -x, +x, -x+y, +y, -y, +x-y, +y-z, -z, +x-z,
+//       -x+z, +z, -y+z
+template <class V>
+__device__ __forceinline__ double step12(int ltype, double g, V &&v) {
+    double acc;
+    if (ltype == SFGPU_LATTICE_FCC) {
+        acc = v(-1, -1, 0) * g;
+        acc += v(1, 1, 0) * g;
+        acc += v(-1, 1, 0) * g;
+        acc += v(1, -1, 0) * g;
+        acc += v(0, -1, -1) * g;
+        acc += v(0, 1, 1) * g;
+        acc += v(0, -1, 1) * g;
+        acc += v(0, 1, -1) * g;
+        acc += v(-1, 0, -1) * g;
+        acc += v(1, 0, 1) * g;
+        acc += v(-1, 0, 1) * g;
+        acc += v(1, 0, -1) * g;
+    } else {
+        acc = v(-1, 0, 0) * g;
+        acc += v(1, 0, 0) * g;
+        acc += v(-1, 1, 0) * g;
+        acc += v(0, 1, 0) * g;
+        acc += v(0, -1, 0) * g;
+        acc += v(1, -1, 0) * g;
+        acc += v(0, 1, -1) * g;
+        acc += v(0, 0, -1) * g;
+        acc += v(1, 0, -1) * g;
+        acc += v(-1, 0, 1) * g;
+        acc += v(0, 0, 1) * g;
+        acc += v(0, -1, 1) * g;
+    }
+    return acc * (1.0 / 12.0);
+}
+
+__host__ __device__ inline bool lat_twelve(const DLat &L) {
+    return L.grad == 3 && (L.ltype == SFGPU_LATTICE_FCC || L.ltype == SFGPU_LATTICE_HEX);
+}
+
 // First-order step at interior site t: G(t) * stencil(gin) in SFbox's
 // operation order (Lat1DFlat1stO.cpp:44-47, Lat2DFlat1stO.cpp:40-46,
 // Lat2DCyl1stO.cpp:24-33, Lat3D1stO.cpp:151-157).  The library is compiled
@@ -106,6 +154,8 @@ __device__ __forceinline__ double stencil1(const DLat &L, const double *__restri
         return g * (l0 * b + L.l1 * (a + c) + L.l1 * (u + d));
     } else {
         int jx = L.st[0], jy = L.st[1];
+        if (lat_twelve(L))
+            return step12(L.ltype, g, [&](int dx, int dy, int dz) { return gin[t + dx * jx + dy * jy + dz]; });
         double acc = gin[t - jx] * g;
         acc += gin[t + jx] * g;
         acc += gin[t - jy] * g;
@@ -184,7 +234,10 @@ __device__ __forceinline__ RowInfo lat_row(const DLat &L, int row) {
 }
 
 // new value at interior position k (1..n_last) of row R, same operation
-// order as stencil1
+// order as stencil1.  kTypes = false compiles the six-neighbour 3D step only
+// (callers that accept the standard 3D lattice type alone and must not carry
+// the registers of the twelve-neighbour steps).
+template <bool kTypes = true>
 __device__ __forceinline__ double prop1_row(const DLat &L, const RowInfo &R, const double *__restrict__ gin,
                                             const double *__restrict__ G, int k, int nlast) {
     const int d = L.grad - 1;
@@ -202,6 +255,16 @@ __device__ __forceinline__ double prop1_row(const DLat &L, const RowInfo &R, con
         if (L.cyl) return g * (b + L.lam_m[R.x] * (u - b) + L.lam_p[R.x] * (dd - b) + L.l1 * (a + c - b - b));
         double l0 = 1 - 4 * L.l1;
         return g * (l0 * b + L.l1 * (a + c) + L.l1 * (u + dd));
+    }
+    if (kTypes && lat_twelve(L)) {
+        // diagonal neighbours: the x and y row offsets add (each coordinate
+        // maps across its own boundary, as SetBoundaries' plane copies do)
+        return step12(L.ltype, g, [&](int dx, int dy, int dz) {
+            const int xo = dx < 0 ? R.up : (dx > 0 ? R.dn : 0);
+            const int yo = dy < 0 ? R.up2 : (dy > 0 ? R.dn2 : 0);
+            const int kk = dz < 0 ? km : (dz > 0 ? kp : k);
+            return gin[R.base + kk + xo + yo];
+        });
     }
     double acc = gin[t + R.up] * g;
     acc += gin[t + R.dn] * g;
@@ -340,17 +403,49 @@ __device__ __forceinline__ void for_interior4(const DLat &L, int worker, int nwo
 // Contact average <phi>(z) at any site (SideFraction, Lat1DFlat.cpp:511-524,
 // Lat2DFlat.cpp:996-1109, Lat2DCylinder.cpp:205-320; Sides with removed
 // boundaries in 3D, Lat3D.cpp:1729-1785).  p must carry boundary copies.
+// kTypes = false: the standard 3D lattice type only (see prop1_row).
+template <bool kTypes = true>
 __device__ inline double side_fraction(const DLat &L, const double *__restrict__ p, int z) {
     int c[3];
     lat_coords(L, z, c);
     if (L.grad == 3) {
         if (!lat_interior(L, c)) return 0.0;
         int jx = L.st[0], jy = L.st[1];
-        const double l1 = 1.0 / 6.0;
-        double acc = 0 * p[z];
-        acc += l1 * p[z + jx]; acc += l1 * p[z - jx];
-        acc += l1 * p[z + jy]; acc += l1 * p[z - jy];
-        acc += l1 * p[z + 1];  acc += l1 * p[z - 1];
+        if (!kTypes || L.ltype == SFGPU_LATTICE_STANDARD) {
+            const double l1 = 1.0 / 6.0;
+            double acc = 0 * p[z];
+            acc += l1 * p[z + jx]; acc += l1 * p[z - jx];
+            acc += l1 * p[z + jy]; acc += l1 * p[z - jy];
+            acc += l1 * p[z + 1];  acc += l1 * p[z - 1];
+            return acc;
+        }
+        auto q = [&](int dx, int dy, int dz) { return p[z + dx * jx + dy * jy + dz]; };
+        if (L.ltype == SFGPU_LATTICE_HEX) {
+            // the twelve HEX neighbours, 1/12 each (Lat3D.cpp:1733-1752)
+            const double l = 1.0 / 12.0;
+            double acc = q(1, 0, 0) * l;
+            acc += q(-1, 0, 0) * l; acc += q(1, -1, 0) * l; acc += q(0, -1, 0) * l;
+            acc += q(0, 1, 0) * l;  acc += q(-1, 1, 0) * l; acc += q(0, -1, 1) * l;
+            acc += q(0, 0, 1) * l;  acc += q(-1, 0, 1) * l; acc += q(1, 0, -1) * l;
+            acc += q(0, 0, -1) * l; acc += q(0, 1, -1) * l;
+            return acc;
+        }
+        // the 27-site cube: centre, faces, edges, corners (Lat3D.cpp:1765-1778)
+        const double l0 = L.sl[0], l1 = L.sl[1], l2 = L.sl[2], l3 = L.sl[3];
+        double acc = q(0, 0, 0) * l0;
+        acc += q(1, 0, 0) * l1;   acc += q(-1, 0, 0) * l1;
+        acc += q(0, 1, 0) * l1;   acc += q(0, -1, 0) * l1;
+        acc += q(0, 0, 1) * l1;   acc += q(0, 0, -1) * l1;
+        acc += q(1, 1, 0) * l2;   acc += q(1, -1, 0) * l2;
+        acc += q(-1, 1, 0) * l2;  acc += q(-1, -1, 0) * l2;
+        acc += q(1, 0, 1) * l2;   acc += q(1, 0, -1) * l2;
+        acc += q(-1, 0, 1) * l2;  acc += q(-1, 0, -1) * l2;
+        acc += q(0, 1, 1) * l2;   acc += q(0, 1, -1) * l2;
+        acc += q(0, -1, 1) * l2;  acc += q(0, -1, -1) * l2;
+        acc += q(1, 1, 1) * l3;   acc += q(1, 1, -1) * l3;
+        acc += q(1, -1, 1) * l3;  acc += q(1, -1, -1) * l3;
+        acc += q(-1, 1, 1) * l3;  acc += q(-1, 1, -1) * l3;
+        acc += q(-1, -1, 1) * l3; acc += q(-1, -1, -1) * l3;
         return acc;
     }
     double l = L.l1chi;

@@ -3,6 +3,7 @@
 // SF_Solve.cpp:647-651), free energy, the Lattice-level entry points and the
 // host-driven Pure_DIIS iteration (the plain GPU form).
 #include <cmath>
+#include <cfloat>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -43,12 +44,12 @@ static int grid_rows(const DLat &L) {
     return (int)std::max(1L, std::min(b, 148L * 32));
 }
 
-// first-order step inside a residual evaluation: x-marching tiles in 3D,
-// row-wise otherwise
+// first-order step inside a residual evaluation: x-marching tiles on the
+// six-neighbour 3D lattices, row-wise otherwise
 int sfgpu_system::launch_step1(const double *gin, const double *G, double *gout, const double *other, double *phi,
                                int mode) {
     const DLat &L = H.L;
-    if (L.grad == 3) {
+    if (L.grad == 3 && !lat_twelve(L)) {
         dim3 grid((L.Md[2] - 2 + kTZ - 1) / kTZ, (L.Md[1] - 2 + kTY - 1) / kTY, (L.Md[0] - 2 + tile_xc - 1) / tile_xc);
         step3d_march<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, tile_xc);
     } else {
@@ -136,6 +137,23 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
     else if (L.grad == 2) { L.st[0] = L.Md[1]; L.st[1] = 1; L.st[2] = 0; }
     else { L.st[0] = L.Md[1] * L.Md[2]; L.st[1] = L.Md[2]; L.st[2] = 1; }
     L.l1 = (L.grad == 3) ? 1.0 / 6.0 : d->lambda;
+    // 3D lattice type and its contact weights (Lat3D.cpp:212-259)
+    L.ltype = d->lattice_type;
+    if (L.ltype < SFGPU_LATTICE_STANDARD || L.ltype > SFGPU_LATTICE_HEX)
+        return fail(SFGPU_ERR_INVALID, "unknown lattice_type");
+    if (L.ltype != SFGPU_LATTICE_STANDARD && L.grad != 3)
+        return fail(SFGPU_ERR_UNSUPPORTED, "lattice types other than standard are built for 3 gradients");
+    L.sl[0] = 0; L.sl[1] = 1.0 / 6.0; L.sl[2] = 0; L.sl[3] = 0;
+    if (L.ltype == SFGPU_LATTICE_FCC) L.sl[0] = L.sl[1] = L.sl[2] = L.sl[3] = 1.0 / 27.0;
+    if (L.ltype == SFGPU_LATTICE_STENCILS) {
+        for (int k = 0; k < 4; k++) {
+            L.sl[k] = d->lambda_3d[k];
+            if (!(L.sl[k] >= 0 && L.sl[k] <= 0.5)) return fail(SFGPU_ERR_INVALID, "lambda0..lambda3 must be in [0, 0.5]");
+        }
+        double dev = L.sl[0] + 6.0 * L.sl[1] + 12.0 * L.sl[2] + 8.0 * L.sl[3] - 1.0;
+        if ((dev < 0 ? -dev : dev) > DBL_EPSILON) return fail(SFGPU_ERR_INVALID, "sum of the lambdas is not 1");
+        L.sl[3] = (1.0 - L.sl[0] - 6.0 * L.sl[1] - 12.0 * L.sl[2]) / 8.0;
+    }
     if (L.grad != 3 && !(d->lambda > 0 && d->lambda <= 0.5)) return fail(SFGPU_ERR_INVALID, "lambda must be in (0, 0.5]");
     L.l1chi = (L.grad == 1 && d->lambda_chi >= 0) ? d->lambda_chi : L.l1;
     double ladj = (L.grad == 1 && d->layer_adjustment > 0) ? d->layer_adjustment : 1.0;

@@ -15,6 +15,7 @@ import numpy as np
 
 BOUND_SURFACE, BOUND_MIRROR1, BOUND_MIRROR2, BOUND_PERIODIC = 1, 2, 3, 4
 GEOM_FLAT, GEOM_CYLINDRICAL, GEOM_SPHERICAL = 0, 1, 2
+LATTICE_STANDARD, LATTICE_STENCILS, LATTICE_FCC, LATTICE_HEX = 0, 1, 2, 3
 SEG_FREE, SEG_FROZEN, SEG_PINNED = 0, 1, 2
 MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT = 0, 1, 2
 
@@ -27,7 +28,8 @@ class LatticeDesc(C.Structure):
                 ("n_layers", C.c_int * 3), ("bound_lo", C.c_int * 3), ("bound_hi", C.c_int * 3),
                 ("lam", C.c_double), ("lambda_chi", C.c_double),
                 ("layer_adjustment", C.c_double), ("dimensions", C.c_double),
-                ("offset_first_layer", C.c_double)]
+                ("offset_first_layer", C.c_double), ("lattice_type", C.c_int),
+                ("lambda_3d", C.c_double * 4)]
 
 
 class SegmentDesc(C.Structure):
@@ -68,6 +70,8 @@ class Lattice:
     layer_adjustment: float = 1.0
     dimensions: float = 3.0
     offset_first_layer: float = 0.0
+    lattice_type: int = LATTICE_STANDARD
+    lambda_3d: Sequence[float] = (0.0, 0.0, 0.0, 0.0)
 
     @property
     def shape(self):
@@ -96,6 +100,9 @@ class Lattice:
         d.lam, d.lambda_chi = self.lam, self.lambda_chi
         d.layer_adjustment, d.dimensions = self.layer_adjustment, self.dimensions
         d.offset_first_layer = self.offset_first_layer
+        d.lattice_type = int(self.lattice_type)
+        for k in range(4):
+            d.lambda_3d[k] = float(self.lambda_3d[k])
         return d
 
 

@@ -18,7 +18,7 @@ from typing import Dict, List, Optional, Tuple
 import numpy as np
 
 from .desc import (BOUND_NAMES, BOUND_MIRROR1, BOUND_PERIODIC, GEOM_CYLINDRICAL, GEOM_FLAT, GEOM_SPHERICAL,
-                   Lattice, Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, Segment,
+                   LATTICE_FCC, LATTICE_HEX, LATTICE_STANDARD, LATTICE_STENCILS, Lattice, Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, Segment,
                    SEG_FREE, SEG_FROZEN, SEG_PINNED, SystemSpec)
 
 Key = Tuple[str, str, str]
@@ -142,8 +142,21 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
         if _get(calc, "sys", sysname, "matrix_approach", "first_order") == "second_order":
             order = 2
     ltype = _get(calc, "lat", ln, "latticetype", "standard")
-    if ltype != "standard":
+    ltypes = {"standard": LATTICE_STANDARD, "stencils": LATTICE_STENCILS, "FCC": LATTICE_FCC, "HEX": LATTICE_HEX}
+    if ltype not in ltypes or (ltype != "standard" and g != 3):
         raise ValueError(f"lat : {ln} : latticetype : {ltype} is not on this path")
+    # 3D contact weights of the stencils type (Lat3D.cpp:221-259): lambda0..3
+    # default to 1/27 and cannot be combined with lambda
+    lam3 = (0.0, 0.0, 0.0, 0.0)
+    lam_keys = [k for k in ("lambda0", "lambda1", "lambda2", "lambda3") if ("lat", ln, k) in calc]
+    if lam_keys:
+        if ("lat", ln, "lambda") in calc:
+            raise ValueError(f"lat : {ln} : lambda cannot be combined with {lam_keys[0]}")
+        if len(lam_keys) != 4:
+            raise ValueError(f"lat : {ln} : lambda0, lambda1, lambda2 and lambda3 go together")
+    if ltype == "stencils":
+        lam3 = tuple(float(_get(calc, "lat", ln, k, repr(1.0 / 27.0))) for k in ("lambda0", "lambda1", "lambda2",
+                                                                             "lambda3"))
     if g == 1:
         n = [int(_get(calc, "lat", ln, "n_layers"))]
         lo = [BOUND_NAMES[_get(calc, "lat", ln, "lowerbound", "mirror1")]]
@@ -182,7 +195,7 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
                   lambda_chi=float(_get(calc, "lat", ln, "lambda_chi", "-1")),
                   layer_adjustment=ladj,
                   dimensions=float(_get(calc, "lat", ln, "dimensions", "3")),
-                  offset_first_layer=off)
+                  offset_first_layer=off, lattice_type=ltypes[ltype], lambda_3d=lam3)
     # segments
     seg_names = _names(calc, "mon")
     segs: List[Segment] = []

@@ -172,6 +172,13 @@ def sweep_calculations(calc: Dict[Key, str]) -> Tuple[Optional[Variation], List[
     return var, out
 
 
+def batchable(spec) -> bool:
+    """Whether the batched persistent kernel takes this system: first order,
+    and the standard lattice type in 3D."""
+    from .desc import LATTICE_STANDARD
+    return spec.lattice.order == 1 and spec.lattice.lattice_type == LATTICE_STANDARD
+
+
 @dataclass
 class SweepResult:
     variation: Optional[Variation]
@@ -221,7 +228,7 @@ def solve_sweep(calc: Dict[Key, str], waves: int = 1, x0: Optional[np.ndarray] =
                 guesses.append(np.asarray(x0, dtype=np.float64))
             else:
                 guesses.append(np.zeros(nv[i]))
-        if all(specs[i].lattice.order == 1 for i in idx):
+        if all(batchable(specs[i]) for i in idx):
             bs = BatchSolver([specs[i] for i in idx], m=m, eta=eta)
             res = bs.solve(np.concatenate(guesses), tol=tol, maxit=maxit)
             parts = bs.split(res.x)
@@ -231,7 +238,8 @@ def solve_sweep(calc: Dict[Key, str], waves: int = 1, x0: Optional[np.ndarray] =
                 iters[i] = res.iterations[j]
             bs.close()
         else:
-            # second-order lattices: the host-driven device iteration, one point at a time
+            # second-order and twelve-neighbour lattices: the host-driven device
+            # iteration, one point at a time
             for j, i in enumerate(idx):
                 r = System(specs[i]).solve(guesses[j], tol=tol, maxit=maxit, m=m, eta=eta)
                 xs[i] = r.x

@@ -63,6 +63,24 @@ extern "C" {
 #define SFGPU_GEOM_CYLINDRICAL 1
 #define SFGPU_GEOM_SPHERICAL   2
 
+/* 3D lattice types, lat : latticetype (Lat3D.cpp:212-259; SF_System.cpp:478-486).
+ * STANDARD: six neighbours, propagation and contact weights 1/6 (Lat3D1stO).
+ * STENCILS: standard propagation; contacts over the 27-site cube with
+ *   lambda_3d[0..3] for the centre, the 6 faces, 12 edges and 8 corners
+ *   (Lat3D::Sides, Lat3D.cpp:1725-1785).
+ * FCC: first order, 12 neighbours (+-x+-y, +-y+-z, +-x+-z) with weight 1/12
+ *   (Lat3DFCC1stO.cpp:56-100); contacts over the 27-site cube, 1/27 each.
+ * HEX: first order, 12 neighbours (+-x, +-y, +-z, +-(x-y), +-(x-z), +-(y-z))
+ *   with weight 1/12 (Lat3DHEX1stO.cpp:56-100); contacts over the same 12
+ *   neighbours, 1/12 each (Lat3D.cpp:1733-1752).
+ * Second-order 3D lattices propagate as STANDARD whatever the type
+ * (SF_System::NewLat2ndO, SF_System.cpp:378-431) and take the type's
+ * contacts. */
+#define SFGPU_LATTICE_STANDARD 0
+#define SFGPU_LATTICE_STENCILS 1
+#define SFGPU_LATTICE_FCC      2
+#define SFGPU_LATTICE_HEX      3
+
 /* segment freedom, SF_Segment.cpp:61-65 ('grafted' is not on this path) */
 #define SFGPU_SEG_FREE    0
 #define SFGPU_SEG_FROZEN  1
@@ -92,6 +110,11 @@ typedef struct {
     double layer_adjustment;   /* 1D only (Lat1DFlat.cpp:139, Lat1DCylinder.cpp:43); 1 = none */
     double dimensions;         /* curved: spatial dimensions D (default 3) */
     double offset_first_layer; /* curved: offset_first_layer(_x) (default 0) */
+    int    lattice_type;       /* SFGPU_LATTICE_* (3 gradients; 0 otherwise) */
+    double lambda_3d[4];       /* SFGPU_LATTICE_STENCILS: lambda0..lambda3, each in
+                                  [0, 0.5], l0 + 6 l1 + 12 l2 + 8 l3 = 1 within
+                                  DBL_EPSILON; lambda3 is then recomputed from
+                                  the other three (Lat3D.cpp:246-259) */
 } sfgpu_lattice_desc;
 
 typedef struct {
@@ -320,7 +343,8 @@ int sfgpu_solve_diis(sfgpu_system *sys, double *x, double tol, int maxit, int m,
 /* Many independent first-order systems -- the calculations of a 'var :'
  * sweep, which SFbox runs one after another (Vary::NextCalculation,
  * Vary.cpp:127; SF_Box.cpp:145-177) -- solved together.  m is the DIIS
- * memory (1..16). */
+ * memory (1..16).  3D instances must have the standard lattice type
+ * (SFGPU_ERR_UNSUPPORTED otherwise: solve those one by one). */
 typedef struct sfgpu_batch sfgpu_batch;
 int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, sfgpu_batch **out);
 int sfgpu_batch_destroy(sfgpu_batch *batch);

@@ -21,6 +21,7 @@
  */
 #include "sfbox_oracle.h"
 #include <math.h>
+#include <float.h>
 #include <stdlib.h>
 #include <string.h>
 #include <stdio.h>
@@ -44,6 +45,8 @@ typedef struct {
     double *sb;        /* SubtractBoundaries factors: 0 on removed boundary layers, 1/2 on mirror2 layers */
     int K;             /* 2nd-order direction components: 3 (1D), 5 (2D), 6 (3D); 1 first order */
     int sw_lo[3], sw_hi[3];   /* 2nd order: +/- components swap at a boundary copy */
+    int ltype;         /* 3D lattice type, SFGPU_LATTICE_* */
+    double sl[4];      /* contact weights of the 27-site cube: centre, face, edge, corner */
 } olat;
 
 static int map_lo_of(int bc, int n) {
@@ -169,6 +172,24 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
     if (L->grad == 1) { L->st[0] = 1; L->st[1] = L->st[2] = 0; }
     if (L->grad == 2) { L->st[0] = L->Md[1]; L->st[1] = 1; L->st[2] = 0; }
     L->l1 = (L->grad == 3) ? 1.0 / 6.0 : d->lambda;   /* Lat3D.cpp:231-236 */
+    /* lattice type and contact weights, Lat3D.cpp:212-259: standard ("BCC")
+       l1 = 1/6 and the rest 0, FCC 1/27 everywhere, stencils from the input
+       with lambda3 recomputed from the other three */
+    L->ltype = d->lattice_type;
+    if (L->ltype < SFGPU_LATTICE_STANDARD || L->ltype > SFGPU_LATTICE_HEX) return SFGPU_ERR_INVALID;
+    if (L->ltype != SFGPU_LATTICE_STANDARD && L->grad != 3) return SFGPU_ERR_UNSUPPORTED;
+    L->sl[0] = 0; L->sl[1] = 1.0 / 6.0; L->sl[2] = 0; L->sl[3] = 0;
+    if (L->ltype == SFGPU_LATTICE_FCC) L->sl[0] = L->sl[1] = L->sl[2] = L->sl[3] = 1.0 / 27.0;
+    if (L->ltype == SFGPU_LATTICE_STENCILS) {
+        double dev;
+        for (int k = 0; k < 4; k++) {
+            L->sl[k] = d->lambda_3d[k];
+            if (!(L->sl[k] >= 0 && L->sl[k] <= 0.5)) return SFGPU_ERR_INVALID;
+        }
+        dev = fabs(L->sl[0] + 6.0 * L->sl[1] + 12.0 * L->sl[2] + 8.0 * L->sl[3] - 1.0);
+        if (dev > DBL_EPSILON) return SFGPU_ERR_INVALID;
+        L->sl[3] = (1.0 - L->sl[0] - 6.0 * L->sl[1] - 12.0 * L->sl[2]) / 8.0;
+    }
     L->l1chi = (d->lambda_chi >= 0 && L->grad == 1) ? d->lambda_chi : L->l1;
     L->ladj = (L->grad == 1 && d->layer_adjustment > 0) ? d->layer_adjustment : 1.0;
 
@@ -300,6 +321,20 @@ static void olat_prop1(const olat *L, const double *gin, const double *G, double
                 double l0 = 1 - 4 * L->l1;
                 r = g * (l0 * b + L->l1 * (a + c) + L->l1 * (u + dn));
             }
+        } else if (L->ltype == SFGPU_LATTICE_FCC || L->ltype == SFGPU_LATTICE_HEX) {
+            /* Lat3DFCC1stO.cpp:79-92 / Lat3DHEX1stO.cpp:79-92: twelve
+               neighbours (dx, dy, dz) summed in this order, then times 1/12 */
+            static const int fcc[12][3] = {{-1, -1, 0}, {1, 1, 0}, {-1, 1, 0}, {1, -1, 0},
+                                           {0, -1, -1}, {0, 1, 1}, {0, -1, 1}, {0, 1, -1},
+                                           {-1, 0, -1}, {1, 0, 1}, {-1, 0, 1}, {1, 0, -1}};
+            static const int hex[12][3] = {{-1, 0, 0}, {1, 0, 0}, {-1, 1, 0}, {0, 1, 0},
+                                           {0, -1, 0}, {1, -1, 0}, {0, 1, -1}, {0, 0, -1},
+                                           {1, 0, -1}, {-1, 0, 1}, {0, 0, 1}, {0, -1, 1}};
+            const int (*nb)[3] = (L->ltype == SFGPU_LATTICE_FCC) ? fcc : hex;
+            int jx = L->st[0], jy = L->st[1];
+            double acc = gin[z + nb[0][0] * jx + nb[0][1] * jy + nb[0][2]] * g;
+            for (int k = 1; k < 12; k++) acc += gin[z + nb[k][0] * jx + nb[k][1] * jy + nb[k][2]] * g;
+            r = acc * (1.0 / 12.0);
         } else {
             int jx = L->st[0], jy = L->st[1];
             double acc = gin[z - jx] * g;
@@ -500,10 +535,33 @@ static void olat_side(const olat *L, const double *phi_in, double *rho) {
         if (L->grad == 3) {
             if (!is_interior(L, z)) { rho[z] = 0; continue; }
             int jx = L->st[0], jy = L->st[1];
-            double l1 = 1.0 / 6.0, acc = 0 * p[z];
-            acc += l1 * p[z + jx]; acc += l1 * p[z - jx];
-            acc += l1 * p[z + jy]; acc += l1 * p[z - jy];
-            acc += l1 * p[z + 1]; acc += l1 * p[z - 1];
+            if (L->ltype == SFGPU_LATTICE_HEX) {
+                /* Lat3D.cpp:1733-1752: the twelve HEX neighbours, 1/12 each
+                   (boundary values, which no sum reads, set to 0 here) */
+                static const int hx[12][3] = {{1, 0, 0}, {-1, 0, 0}, {1, -1, 0}, {0, -1, 0},
+                                              {0, 1, 0}, {-1, 1, 0}, {0, -1, 1}, {0, 0, 1},
+                                              {-1, 0, 1}, {1, 0, -1}, {0, 0, -1}, {0, 1, -1}};
+                double l = 1.0 / 12.0, acc = p[z + hx[0][0] * jx + hx[0][1] * jy + hx[0][2]] * l;
+                for (int k = 1; k < 12; k++) acc += p[z + hx[k][0] * jx + hx[k][1] * jy + hx[k][2]] * l;
+                rho[z] = acc;
+                continue;
+            }
+            /* Lat3D.cpp:1765-1778: the 27-site cube in the order centre,
+               faces, edges, corners (standard: only the faces weigh) */
+            static const int cube[27][4] = {
+                {0, 0, 0, 0},
+                {1, 0, 0, 1}, {-1, 0, 0, 1}, {0, 1, 0, 1}, {0, -1, 0, 1}, {0, 0, 1, 1}, {0, 0, -1, 1},
+                {1, 1, 0, 2}, {1, -1, 0, 2}, {-1, 1, 0, 2}, {-1, -1, 0, 2},
+                {1, 0, 1, 2}, {1, 0, -1, 2}, {-1, 0, 1, 2}, {-1, 0, -1, 2},
+                {0, 1, 1, 2}, {0, 1, -1, 2}, {0, -1, 1, 2}, {0, -1, -1, 2},
+                {1, 1, 1, 3}, {1, 1, -1, 3}, {1, -1, 1, 3}, {1, -1, -1, 3},
+                {-1, 1, 1, 3}, {-1, 1, -1, 3}, {-1, -1, 1, 3}, {-1, -1, -1, 3}};
+            double acc = p[z] * L->sl[0];
+            for (int k = 1; k < 27; k++) {
+                double w = L->sl[cube[k][3]];
+                if (w == 0) continue;   /* adding +0 products changes no sum */
+                acc += p[z + cube[k][0] * jx + cube[k][1] * jy + cube[k][2]] * w;
+            }
             rho[z] = acc;
             continue;
         }

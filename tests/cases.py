@@ -4,8 +4,8 @@ import numpy as np
 
 from field_b200 import configs
 from field_b200.desc import (BOUND_MIRROR1, BOUND_MIRROR2, BOUND_PERIODIC, BOUND_SURFACE, GEOM_CYLINDRICAL,
-                             GEOM_FLAT, GEOM_SPHERICAL, Lattice, Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT,
-                             Segment, SEG_FROZEN, SystemSpec)
+                             GEOM_FLAT, GEOM_SPHERICAL, LATTICE_FCC, LATTICE_HEX, LATTICE_STENCILS, Lattice,
+                             Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, Segment, SEG_FROZEN, SystemSpec)
 
 
 def _flat2d_surface():
@@ -33,6 +33,37 @@ def _melt_mirror():
     mols = [Molecule("AB", [(0, 6), (1, 5)], MOL_FREE, phibulk=0.1), Molecule("A8", [(0, 8)], MOL_FREE, phibulk=0.05),
             Molecule("W", [(2, 1)], MOL_SOLVENT)]
     return SystemSpec(lat, segs, chi, mols)
+
+
+def _typed(spec, ltype, lambda_3d=(0.0, 0.0, 0.0, 0.0)):
+    """The same system on another 3D lattice type (lat : latticetype)."""
+    spec.lattice.lattice_type = ltype
+    spec.lattice.lambda_3d = tuple(lambda_3d)
+    return spec
+
+
+def _colloid3d(periodic=False):
+    """Frozen block of sites (a particle) in a mirror/periodic (or fully
+    periodic) 3D box with an adsorbing diblock and a solvent: converges to a
+    non-uniform solution."""
+    if periodic:
+        lat = Lattice(3, [8, 7, 6], [BOUND_PERIODIC] * 3, [BOUND_PERIODIC] * 3)
+    else:
+        lat = Lattice(3, [8, 7, 6], [BOUND_MIRROR1, BOUND_MIRROR2, BOUND_PERIODIC],
+                      [BOUND_MIRROR2, BOUND_MIRROR1, BOUND_PERIODIC])
+    mask = np.zeros(lat.shape)
+    mask[1:3, 1:3, 2:5] = 1.0
+    segs = [Segment("S", SEG_FROZEN, mask.reshape(-1)), Segment("A"), Segment("B"), Segment("W")]
+    chi = np.zeros((4, 4))
+    chi[0, 1] = chi[1, 0] = -1.5
+    chi[1, 3] = chi[3, 1] = 0.7
+    chi[2, 3] = chi[3, 2] = 0.2
+    mols = [Molecule("AB", [(1, 5), (2, 4)], MOL_FREE, phibulk=0.02), Molecule("W", [(3, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols)
+
+
+# stencils contact weights: centre, face, edge, corner (0.1 + 6*0.08 + 12*0.02 + 8*0.0225 = 1)
+STENCILS = (0.1, 0.08, 0.02, 0.0225)
 
 
 def _flat1d_periodic():
@@ -178,6 +209,14 @@ CASES = {
     "3d_periodic_melt": lambda: configs.melt3d(n=9, nA=7, nB=6)[0],
     "3d_mirror_mix": _melt_mirror,
     "3d_2nd_brush": lambda: configs.brush3d(n=6, N=15, sigma=0.2, S=0.5)[0],
+    "3d_fcc_colloid": lambda: _typed(_colloid3d(), LATTICE_FCC),
+    # HEX neighbours are not mirror symmetric: on mirror boundaries its step
+    # is not detailed-balanced, so the periodic box is the physical case
+    "3d_hex_colloid": lambda: _typed(_colloid3d(periodic=True), LATTICE_HEX),
+    "3d_hex_mirror": lambda: _typed(_colloid3d(), LATTICE_HEX),
+    "3d_stencils_colloid": lambda: _typed(_colloid3d(), LATTICE_STENCILS, STENCILS),
+    "3d_stencils_melt": lambda: _typed(configs.melt3d(n=7, nA=5, nB=6)[0], LATTICE_STENCILS, STENCILS),
+    "3d_2nd_fcc_brush": lambda: _typed(configs.brush3d(n=6, N=15, sigma=0.2, S=0.5)[0], LATTICE_FCC),
     "1d_cylinder": _cyl1d_micelle,
     "1d_sphere_colloid": _sphere1d_colloid,
     "1d_2nd_lumped": _flat1d_2nd,
@@ -188,8 +227,10 @@ CASES = {
     "2d_cyl_2nd_lumped": _cyl2d_2nd,
 }
 
-# cases whose derivatives (forward and reverse mode) are implemented
-DIFFERENTIABLE = sorted(k for k in CASES if "lumped" not in k)
+# cases whose derivatives (forward and reverse mode) are implemented: not the
+# lumped second-order lattices nor the 3D lattice types other than standard
+NOT_DIFFERENTIABLE = ("lumped", "fcc", "hex", "stencils")
+DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFERENTIABLE))
 
 
 def random_x(spec, seed=7, scale=0.3):

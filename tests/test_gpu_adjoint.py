@@ -13,14 +13,14 @@ import numpy as np
 import torch
 import pytest
 
-from cases import CASES, random_x
+from cases import CASES, DIFFERENTIABLE, random_x
 from field_b200 import configs
 from field_b200.system import System
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
-FIRST_ORDER = sorted(k for k in CASES if "2nd" not in k)
+FIRST_ORDER = sorted(k for k in DIFFERENTIABLE if "2nd" not in k)
 
 
 @pytest.mark.parametrize("case", FIRST_ORDER)

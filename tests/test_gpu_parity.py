@@ -261,3 +261,42 @@ def test_thermo(gpu_lib, case):
     assert abs(Og - Oc) <= 1e-11 * max(1.0, abs(Oc), abs(Fc))
     assert Fg == pytest.approx(sys_.free_energy(), rel=1e-14, abs=1e-14)
     assert rel(feg, fec) <= TOL_EVAL and rel(gpg, gpc) <= TOL_EVAL
+
+
+@pytest.mark.parametrize("case", ["3d_fcc_colloid", "3d_hex_colloid", "3d_hex_mirror", "3d_stencils_colloid",
+                                  "3d_2nd_fcc_brush"])
+def test_lattice_types_converged_parity(gpu_lib, case):
+    """FCC, HEX and stencils 3D lattices (and a second-order lattice with FCC
+    contacts) converged by the device Pure_DIIS and by the oracle's."""
+    spec = CASES[case]()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    x0 = np.zeros(spec.n_itvar())
+    rg = sys_.solve(x0, tol=1e-10, maxit=3000, m=8, eta=0.3)
+    xc, rc, it, err = o.solve_diis(x0, tol=1e-10, maxit=3000, m=8, eta=0.3)
+    assert rg.converged and rc == 0, (rg.converged, rc, err)
+    assert rg.iterations > 5
+    sys_.residual(rg.x)
+    o.residual(xc)
+    for i in range(len(spec.segments)):
+        np.testing.assert_allclose(sys_.phi(i), o.phi(i), rtol=1e-9, atol=1e-12)
+    assert abs(sys_.free_energy() - o.free_energy()) <= 1e-9 * max(1.0, abs(o.free_energy()))
+
+
+def test_lattice_types_outside_derivatives_and_batch(gpu_lib):
+    """Derivatives and the batched kernel take the standard 3D lattice only:
+    both report SFGPU_ERR_UNSUPPORTED for FCC; a sweep of FCC points is solved
+    point by point and agrees with the single-system solve."""
+    from field_b200._native import SfgpuError
+    from field_b200.batch import BatchSolver
+    spec = CASES["3d_fcc_colloid"]()
+    sys_ = System(spec)
+    x = random_x(spec)
+    for call in (lambda: sys_.jvp(x, x), lambda: sys_.vjp(x, x)):
+        with pytest.raises(SfgpuError) as e:
+            call()
+        assert e.value.code == 7
+    with pytest.raises(SfgpuError) as e:
+        BatchSolver([spec], m=5, eta=0.1)
+    assert e.value.code == 7
+    assert np.all(np.isfinite(sys_.residual(x)))

@@ -526,14 +526,16 @@ def _grand_potential2(spec, o):
     return F - total
 
 
-@pytest.mark.parametrize("which", ["adsorption", "2d_surface", "sphere"])
+@pytest.mark.parametrize("which", ["adsorption", "2d_surface", "sphere", "3d_fcc_colloid", "3d_hex_colloid",
+                                   "3d_stencils_colloid"])
 def test_grand_potential_equals_F_minus_n_mu_at_convergence(which):
     """At the self-consistent solution the grand potential summed from its
     density equals F - sum n mu (SFbox prints both, 'grand potential' and
     'grand potential2'); away from it they differ."""
     from cases import CASES
     spec = {"adsorption": lambda: configs.flat_adsorption(n=40, N=21)[0],
-            "2d_surface": CASES["2d_flat_surface"], "sphere": CASES["1d_sphere_colloid"]}[which]()
+            "2d_surface": CASES["2d_flat_surface"], "sphere": CASES["1d_sphere_colloid"],
+            **{k: CASES[k] for k in ("3d_fcc_colloid", "3d_hex_colloid", "3d_stencils_colloid")}}[which]()
     o = Oracle(spec)
     x, rc, it, err = o.solve_diis(np.zeros(spec.n_itvar()), tol=1e-11, maxit=20000, m=10, eta=0.3)
     assert rc == 0
