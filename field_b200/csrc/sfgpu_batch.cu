@@ -173,6 +173,7 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
     b->offset.resize(n);
     for (int i = 0; i < n && !rc; i++) {
         if (descs[i].lattice.order != 1) { rc = fail_unsupported("batched second-order lattices"); break; }
+        if (descs[i].overflow_protection) { rc = fail_unsupported("batched systems with overflow protection"); break; }
         if (descs[i].lattice.gradients == 3 && descs[i].lattice.lattice_type != SFGPU_LATTICE_STANDARD) {
             rc = fail_unsupported("batched FCC, HEX and stencils 3D lattices");
             break;

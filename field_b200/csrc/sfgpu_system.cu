@@ -471,12 +471,179 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     for (int c = 0; c < nclass; c++) bp.rep[c] = rep_of_class[c];
     for (int i = 0; i < nseg; i++)
         for (int m = 0; m < nmol; m++) bp.frac[i * SFGPU_MAX_SEG + m] = (double)mols[m].count[i] / mols[m].N;
+    if (d->overflow_protection) return setup_logspace();
+    return SFGPU_OK;
+}
+
+// Overflow protection (sys : overflow_protection, SF_System.cpp:67, :445-519):
+// the *1stOS lattice constants (Lat1DFlat1stOS.cpp:3-9, Lat2DFlat1stOS.cpp:8-13,
+// Lat2DCyl1stOS.cpp:3-25), the weights of their ComputeLnGN and the log-space
+// buffers.
+int sfgpu_system::setup_logspace() {
+    const DLat &L = H.L;
+    if (L.order != 1 || L.grad > 2)
+        return fail(SFGPU_ERR_UNSUPPORTED, "overflow protection needs a first-order 1D or 2D lattice");
+    logmode = true;
+    logc.lmax = log(DBL_MAX);
+    logc.logcutoff = 100.0;
+    logc.cutoff = exp(logc.logcutoff);
+    logc.prefactor = logc.lmax - logc.logcutoff - 50.0;
+    memset(&logq, 0, sizeof(logq));
+    const double l1 = L.l1;
+    logq.kind = (L.grad == 1) ? (L.cyl ? LOG_CURVED1 : LOG_FLAT1) : (L.cyl ? LOG_CYL2 : LOG_FLAT2);
+    if (logq.kind == LOG_FLAT1 || logq.kind == LOG_FLAT2) {
+        const double l0 = (logq.kind == LOG_FLAT1) ? 1 - 2 * l1 : 1 - 4 * l1;
+        logq.logl1l0 = log(l1 / l0);
+        logq.logl0 = log(l0);
+        logq.logl1 = log(l1);
+    }
+    int rc;
+    const int MX = L.Md[0];
+    if (logq.kind == LOG_CYL2) {
+        std::vector<double> a(MX, 0.0), b(MX, 0.0), c(MX, 0.0);
+        for (int x = 1; x < MX - 1; x++) {
+            const double lm = H.lam_m[x], lp = H.lam_p[x];
+            b[x] = lm > 0 ? log(lm) : 0;
+            c[x] = lp > 0 ? log(lp) : 0;
+            const double l0 = 1.0 - lm - lp - 2 * l1;
+            a[x] = l0 > 0 ? log(l0) : 0;
+        }
+        logq.logl1 = l1 > 0 ? log(l1) : 0;
+        logq.nl_centre = 1.0 - l1 - l1 - l1 - l1;
+        if ((rc = alloc_d(&d_logl0x, MX)) || (rc = alloc_d(&d_loglmx, MX)) || (rc = alloc_d(&d_loglpx, MX))) return rc;
+        SFGPU_CUDA_TRY(cudaMemcpy(d_logl0x, a.data(), sizeof(double) * MX, cudaMemcpyHostToDevice));
+        SFGPU_CUDA_TRY(cudaMemcpy(d_loglmx, b.data(), sizeof(double) * MX, cudaMemcpyHostToDevice));
+        SFGPU_CUDA_TRY(cudaMemcpy(d_loglpx, c.data(), sizeof(double) * MX, cudaMemcpyHostToDevice));
+        logq.logl0x = d_logl0x; logq.loglmx = d_loglmx; logq.loglpx = d_loglpx;
+    }
+    // ComputeLnGN of the log-space lattices as weights: 1D
+    // (Lat1DFlat1stOS.cpp:441-478, Lat1DCyl1stOS.cpp:242-281) weighs the
+    // first interior layer 1/2 when the lower copy layer is 3, the last one
+    // 1/2 when the upper copy layer is M-2 (1-based; mirror2), and takes no
+    // layer adjustment; curved layers also weigh L(z).  2D
+    // (Lat2DFlat1stOS.cpp:449-505, Lat2DCyl1stOS.cpp:471-540) adds every
+    // interior site (times L(x) on the cylinder), takes half of the x rows
+    // and y columns next to a mirror2, the upper one in y being the column
+    // y = MY-2 (1-based), and adds the four corners back with 1/4 (flat) or
+    // 4 L(x) (cylinder).
+    w_os.assign(M, 0.0);
+    auto copy_lo = [&](int k) { return L.bc_lo[k] == SFGPU_BOUND_PERIODIC ? L.Md[k] - 1 : L.bc_lo[k]; };
+    auto copy_hi = [&](int k) { return L.bc_hi[k] == SFGPU_BOUND_PERIODIC ? 2 : L.Md[k] - L.bc_hi[k] + 1; };
+    auto Lx = [&](int x) { return L.cyl ? H.Lx[x] : 1.0; };
+    if (L.grad == 1) {
+        const int Mz = L.Md[0];
+        w_os[1] = Lx(1) * (copy_lo(0) == 3 ? 0.5 : 1.0);
+        for (int z = 2; z <= Mz - 3; z++) w_os[z] = Lx(z);
+        // the last term is added on top of the first one when both are the
+        // same layer (one interior layer)
+        if (copy_hi(0) == Mz - 2) w_os[Mz - 2] += 0.5 * Lx(Mz - 2);
+        else if (Mz > 3) w_os[Mz - 2] = Lx(Mz - 2);
+    } else {
+        const int MY = L.Md[1], nx = MX - 2, ny = MY - 2;
+        auto at = [&](int x, int y) -> double & { return w_os[(size_t)x * MY + y]; };
+        for (int x = 1; x <= nx; x++)
+            for (int y = 1; y <= ny; y++) at(x, y) = Lx(x);
+        const bool X1 = copy_lo(0) == 3, X2 = copy_hi(0) == MX - 2;
+        const bool Y1 = copy_lo(1) == 3, Y2 = copy_hi(1) == MY - 2;
+        if (X1) for (int y = 1; y <= ny; y++) at(1, y) -= 0.5 * Lx(1);
+        if (X2) for (int y = 1; y <= ny; y++) at(nx, y) -= 0.5 * Lx(nx);
+        if (Y1) for (int x = 1; x <= nx; x++) at(x, 1) -= 0.5 * Lx(x);
+        if (Y2) for (int x = 1; x <= nx; x++) at(x, ny - 1) -= 0.5 * Lx(x);
+        const double f1 = L.cyl ? 4.0 * Lx(1) : 0.25, f2 = L.cyl ? 4.0 * Lx(nx) : 0.25;
+        if (X1 && Y1) at(1, 1) += f1;
+        if (X1 && Y2) at(1, ny - 1) += f1;
+        if (X2 && Y1) at(nx, 1) += f2;
+        if (X2 && Y2) at(nx, ny - 1) += f2;
+    }
+    if ((rc = alloc_d(&d_wos, M)) || (rc = alloc_d(&d_lse, nmol))) return rc;
+    SFGPU_CUDA_TRY(cudaMemcpy(d_wos, w_os.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+    d_lgseg.assign(nseg, nullptr);
+    for (int i = 0; i < nseg; i++)
+        if (freedom[i] != SFGPU_SEG_FROZEN && (rc = alloc_d(&d_lgseg[i], M))) return rc;
     return SFGPU_OK;
 }
 
 // propagation of one molecule (SF_Monomer1stO::Matrix1, SF_Homopol1stO::Matrix1,
 // SF_Copol1stO::Matrix1, SF_Homopol2ndO::Matrix1, SF_Copol2ndO::Matrix1)
+// molecule_phi in logarithms, for overflow protection: the same chain walks
+// with the *1stOS steps, ConnectG, CorrectDoubleCountG, ComputeLnGN and
+// NormPhi* of Lat1DFlat1stOS.cpp:289-358 (and the 1D curved and 2D ones),
+// between MakeSafe(G) and RestoreFromSafe(phi) as in SF_Monomer1stO.cpp:105-132,
+// SF_Homopol1stO.cpp:562-621 and SF_Copol1stO.cpp:1196-1281.
+int sfgpu_system::molecule_phi_log(int m) {
+    HMol &o = mols[m];
+    const DLat &L = H.L;
+    const int g = grid_for(M), gr = grid_rows(L);
+    cudaStream_t s = stream;
+    MolParam p;
+    p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = o.sym; p.K = 1;
+    p.pinned = o.pinned; p.solvent = (m == solvent); p.nmol = nmol;
+    p.phibulk_in = o.phibulk; p.theta = o.theta;
+    MolScal *scal = (MolScal *)d_scal;
+    const int restr = (o.freedom == SFGPU_MOL_RESTRICTED);
+    const double N = (double)o.N;
+    const double LZ = SFGPU_LOGZERO;
+    if (o.type == 0) {
+        const int i = o.seg[0];
+        lse_weighted<<<1, 1024, 0, s>>>(M, d_lgseg[i], d_wos, d_lse + m);
+        mol_scalars_log<<<1, 1, 0, s>>>(p, d_lse + m, scal, m);
+        finalize_phi_log<<<g, kBlock, 0, s>>>(M, logc, d_lgseg[i], o.d_phi[i], scal, m, 1, restr,
+                                              restr ? log(o.theta) : 0.0);
+        return SFGPU_OK;
+    }
+    for (int i : o.used) fill_value<<<g, kBlock, 0, s>>>(M, LZ, o.d_phi[i]);
+    double *ginv = d_ginv[0], *tmp = d_ginv[1];
+    const double *cur;
+    if (o.sym) {
+        const int i = o.seg[0], half = o.N / 2;
+        const double *lG = d_lgseg[i];
+        double *phi = o.d_phi[i];
+        SFGPU_CUDA_TRY(cudaMemcpyAsync(d_gi, lG, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+        for (int t = 1; t < half; t++)
+            step1_log_rows<<<gr, kBlock, 0, s>>>(L, logq, logc, d_gi + (size_t)(t - 1) * M, lG, d_gi + (size_t)t * M,
+                                                 nullptr, nullptr, COMP_NONE);
+        cur = d_gi + (size_t)(half - 1) * M;
+        if (o.N % 2 == 1) {
+            step1_log_rows<<<gr, kBlock, 0, s>>>(L, logq, logc, cur, lG, ginv, nullptr, phi, COMP_CENTRE);
+            cur = ginv; std::swap(ginv, tmp);
+        }
+        for (int sp = (o.N + 3) / 2; sp <= o.N; sp++) {
+            const int sinv = o.N - sp + 1;
+            step1_log_rows<<<gr, kBlock, 0, s>>>(L, logq, logc, cur, lG, ginv, d_gi + (size_t)(sinv - 1) * M, phi,
+                                                 COMP_ACC);
+            cur = ginv; std::swap(ginv, tmp);
+        }
+        lse_weighted<<<1, 1024, 0, s>>>(M, cur, d_wos, d_lse + m);
+        mol_scalars_log<<<1, 1, 0, s>>>(p, d_lse + m, scal, m);
+        finalize_phi_log<<<g, kBlock, 0, s>>>(M, logc, lG, phi, scal, m, 0, restr, restr ? log(2 * o.theta / N) : 0.0);
+        set_boundaries<<<g, kBlock, 0, s>>>(L, 1, phi);
+        return SFGPU_OK;
+    }
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(d_gi, d_lgseg[o.seg[0]], sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+    for (int t = 1; t < o.N; t++)
+        step1_log_rows<<<gr, kBlock, 0, s>>>(L, logq, logc, d_gi + (size_t)(t - 1) * M, d_lgseg[o.seg[t]],
+                                             d_gi + (size_t)t * M, nullptr, nullptr, COMP_NONE);
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(ginv, d_lgseg[o.seg[o.N - 1]], sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+    connect_log<<<g, kBlock, 0, s>>>(M, logc, ginv, d_gi + (size_t)(o.N - 1) * M, o.d_phi[o.seg[o.N - 1]]);
+    cur = ginv; std::swap(ginv, tmp);
+    for (int t = o.N - 2; t >= 0; t--) {
+        const int sg = o.seg[t];
+        step1_log_rows<<<gr, kBlock, 0, s>>>(L, logq, logc, cur, d_lgseg[sg], ginv, d_gi + (size_t)t * M, o.d_phi[sg],
+                                             COMP_ACC);
+        cur = ginv; std::swap(ginv, tmp);
+    }
+    lse_weighted<<<1, 1024, 0, s>>>(M, cur, d_wos, d_lse + m);
+    mol_scalars_log<<<1, 1, 0, s>>>(p, d_lse + m, scal, m);
+    for (int i : o.used) {
+        finalize_phi_log<<<g, kBlock, 0, s>>>(M, logc, d_lgseg[i], o.d_phi[i], scal, m, 0, restr,
+                                              restr ? log(o.theta / N) : 0.0);
+        set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_phi[i]);
+    }
+    return SFGPU_OK;
+}
+
 int sfgpu_system::molecule_phi(int m) {
+    if (logmode) return molecule_phi_log(m);
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_for(M);
@@ -603,6 +770,7 @@ int sfgpu_system::residual_async(const double *x, double *f) {
         if (freedom[i] == SFGPU_SEG_FROZEN) continue;
         swf_update<<<g, kBlock, 0, s>>>(L, x, d_jmap, nclass, class_of[i], d_range[i],
                                         freedom[i] == SFGPU_SEG_PINNED, d_gfull[i], d_gseg[i]);
+        if (logmode) make_safe<<<g, kBlock, 0, s>>>(M, logc, d_gseg[i], d_lgseg[i]);
     }
     // molecules, solvent last (SF_MolList1stO.cpp:274-291)
     for (int m = 0; m < nmol; m++) {
@@ -846,7 +1014,14 @@ extern "C" int sfgpu_lat_propagate(sfgpu_system *s, const double *gin, const dou
     CHECK_SYS(s);
     if (gin == gout) return fail(SFGPU_ERR_INVALID, "gin and gout must differ");
     int gr = grid_for(s->M);
-    if (s->K == 1)
+    if (s->logmode) {
+        // Lat1DFlat1stOS::PropagateG and the other *1stOS steps on logarithms:
+        // interior by the step, surfaces LOGZERO, other boundaries copies
+        fill_value<<<gr, kBlock, 0, s->stream>>>(s->M, SFGPU_LOGZERO, gout);
+        step1_log_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, s->logq, s->logc, gin, g, gout, nullptr,
+                                                                    nullptr, COMP_NONE);
+        set_boundaries<<<gr, kBlock, 0, s->stream>>>(s->H.L, 1, gout);
+    } else if (s->K == 1)
         step1<<<gr, kBlock, 0, s->stream>>>(s->H.L, gin, g, gout, nullptr, nullptr, COMP_NONE);
     else if (s->K == 6)
         step2<<<gr, kBlock, 0, s->stream>>>(s->H.L, gin, g, S, gout, nullptr, nullptr, COMP_NONE, backward);
@@ -875,6 +1050,12 @@ extern "C" int sfgpu_lat_side_fraction(sfgpu_system *s, const double *phi, doubl
 extern "C" int sfgpu_lat_lngn(sfgpu_system *s, const double *g, int components, double *lngn) {
     CHECK_SYS(s);
     if (components != 1 && components != s->K) return fail(SFGPU_ERR_INVALID, "components must be 1 or the lattice's K");
+    if (s->logmode) {   // ComputeLnGN of the *1stOS lattices: g holds logarithms
+        lse_weighted<<<1, 1024, 0, s->stream>>>(s->M, g, s->d_wos, s->d_misc);
+        SFGPU_CUDA_TRY(cudaMemcpyAsync(lngn, s->d_misc, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        SFGPU_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        return SFGPU_OK;
+    }
     wsum_partial<<<s->nblocks_red, kBlock, 0, s->stream>>>(s->M, components, g, s->d_wgn, s->d_partial);
     finish_sums<<<1, 32, 0, s->stream>>>(1, s->nblocks_red, s->d_partial, s->d_misc);
     double v = 0;

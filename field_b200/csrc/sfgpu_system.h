@@ -1,7 +1,7 @@
 // sfgpu_system.h -- host object behind the opaque sfgpu_system handle.
 #pragma once
 #include <vector>
-#include "sfgpu_kernels.cuh"
+#include "sfgpu_logspace.cuh"
 
 struct HostLat {
     DLat L;
@@ -84,6 +84,16 @@ struct sfgpu_system {
     std::vector<double *> a_phibar_m;
     int vjp_async(const double *x, const double *w, double *f, double *xbar);
     int launch_step1(const double *gin, const double *G, double *gout, const double *other, double *phi, int mode);
+    // overflow protection: chain statistics in logarithms (first-order 1D/2D)
+    bool logmode = false;
+    sfk::LogLat logq;
+    sfk::LogConst logc;
+    std::vector<double> w_os;                 // lnGN weights of the log-space lattices
+    double *d_wos = nullptr, *d_lse = nullptr;
+    double *d_logl0x = nullptr, *d_loglmx = nullptr, *d_loglpx = nullptr;
+    std::vector<double *> d_lgseg;            // log G per segment (MakeSafe)
+    int setup_logspace();
+    int molecule_phi_log(int m);
     std::vector<void *> allocs;
 
     ~sfgpu_system();

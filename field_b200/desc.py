@@ -46,7 +46,7 @@ class SystemDesc(C.Structure):
     _fields_ = [("lattice", LatticeDesc), ("n_segments", C.c_int),
                 ("segments", C.POINTER(SegmentDesc)), ("chi", C.POINTER(C.c_double)),
                 ("pf", C.POINTER(C.c_double)), ("n_molecules", C.c_int),
-                ("molecules", C.POINTER(MoleculeDesc))]
+                ("molecules", C.POINTER(MoleculeDesc)), ("overflow_protection", C.c_int)]
 
 
 def dptr(a: np.ndarray):
@@ -133,6 +133,7 @@ class SystemSpec:
     chi: np.ndarray
     molecules: List[Molecule]
     pf: Optional[np.ndarray] = None
+    overflow_protection: bool = False
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -182,6 +183,7 @@ class SystemSpec:
             d.pf = C.POINTER(C.c_double)()
         d.n_molecules = len(self.molecules)
         d.molecules = C.cast(mols, C.POINTER(MoleculeDesc))
+        d.overflow_protection = int(bool(self.overflow_protection))
         keep += [segs, mols]
         self._keep = keep
         return d

@@ -74,6 +74,7 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
     sname = _names(calc, "sys", "noname")
     T("sys", sname, "calculation number", calc_number)
     T("sys", sname, "matrix_approach", "second_order" if spec.lattice.order == 2 else "first_order")
+    T("sys", sname, "overflow_protection", "true" if getattr(spec, "overflow_protection", False) else "false")
     R("sys", sname, "grand potential", Om)
     R("sys", sname, "free energy", F)
     P("sys", sname, "free energy density", fe)

@@ -239,7 +239,16 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
             mols.append(Molecule(mn, blocks, MOL_SOLVENT))
         else:
             raise ValueError(f"mol : {mn} : freedom : {fr} is not on this path")
-    spec = SystemSpec(lat, segs, chi, mols, pf=pf if order == 2 else None)
+    # sys : overflow_protection (SF_System.cpp:67): log-space chain statistics
+    overflow = False
+    for sysname in _names(calc, "sys"):
+        v = _get(calc, "sys", sysname, "overflow_protection", "false").lower()
+        if v not in ("true", "false"):
+            raise ValueError(f"sys : {sysname} : overflow_protection : {v} is not a boolean")
+        overflow |= v == "true"
+    if overflow and (order != 1 or g == 3):
+        raise ValueError("overflow_protection needs a first-order 1D or 2D lattice (SF_System.cpp:395, :478-481)")
+    spec = SystemSpec(lat, segs, chi, mols, pf=pf if order == 2 else None, overflow_protection=overflow)
     st = SolverSettings()
     for nn in _names(calc, "newton"):
         st.method = _get(calc, "newton", nn, "method", st.method)

@@ -142,6 +142,17 @@ typedef struct {
                                          SF_Copol2ndO.cpp:234-247) */
     int                        n_molecules;
     const sfgpu_molecule_desc *molecules;
+    int                        overflow_protection;
+                               /* sys : overflow_protection (SF_System.cpp:67):
+                                  chain statistics in natural logarithms on the
+                                  first-order 1D and 2D lattices (Lat1DFlat1stOS,
+                                  Lat1DCyl1stOS, Lat1DSphere1stOS, Lat2DFlat1stOS,
+                                  Lat2DCyl1stOS); SFGPU_ERR_UNSUPPORTED on 3D and
+                                  second-order lattices, where SFbox stops with an
+                                  error (SF_System.cpp:395, :478-481).  The lattice-
+                                  level propagate and lnGN calls then take and
+                                  return logarithms; batches and derivatives
+                                  return SFGPU_ERR_UNSUPPORTED. */
 } sfgpu_system_desc;
 
 typedef struct sfgpu_system sfgpu_system;   /* opaque handle, owns device buffers */

@@ -51,6 +51,7 @@ def lib():
         l.orc_free_energy.restype = C.c_double
         l.orc_propagate.argtypes = [vp, dp, dp, dp, C.c_double, C.c_int]
         l.orc_side.argtypes = [vp, dp, dp]
+        l.orc_lat_lngn.argtypes = [vp, dp, dp]
         l.orc_site_weights.argtypes = [vp, dp]
         l.orc_set_boundaries.argtypes = [vp, dp]
         l.orc_solve_diis.argtypes = [vp, dp, C.c_double, C.c_int, C.c_int, C.c_double, ip, dp]
@@ -136,6 +137,13 @@ class Oracle:
         out = np.zeros(self.K * self.M)
         lib().orc_propagate(self.h, _d(gin), _d(g), _d(out), S, int(backward))
         return out
+
+    def lat_lngn(self, g):
+        """ComputeLnGN of one propagator (logarithms with overflow protection)."""
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        out = C.c_double()
+        lib().orc_lat_lngn(self.h, _d(g), C.byref(out))
+        return out.value
 
     def side(self, phi):
         phi = np.ascontiguousarray(phi, dtype=np.float64)

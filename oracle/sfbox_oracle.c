@@ -47,6 +47,11 @@ typedef struct {
     int sw_lo[3], sw_hi[3];   /* 2nd order: +/- components swap at a boundary copy */
     int ltype;         /* 3D lattice type, SFGPU_LATTICE_* */
     double sl[4];      /* contact weights of the 27-site cube: centre, face, edge, corner */
+    /* overflow protection (*1stOS lattices): constants of the log-space steps */
+    int logmode;
+    double LogL0, LogL1, LogL1L0;          /* flat 1D / 2D */
+    double *logl0x, *loglmx, *loglpx;      /* 2D cylinder, by x (0 where lambda <= 0) */
+    double logl1, nl_centre;               /* 2D cylinder */
 } olat;
 
 static int map_lo_of(int bc, int n) {
@@ -296,6 +301,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
 
 static void olat_free(olat *L) {
     free(L->lam_m); free(L->lam_p); free(L->lamc_m); free(L->lamc_p); free(L->Lx); free(L->w_gn); free(L->w_f); free(L->sb);
+    free(L->logl0x); free(L->loglmx); free(L->loglpx);
 }
 
 /* one first-order step gout = G * stencil(gin); gin must carry valid
@@ -664,11 +670,14 @@ static int chi_rows_equal(const orc_system *s, int a, int b) {
     return 1;
 }
 
+static int olat_init_log(olat *L);
+
 int orc_create(const sfgpu_system_desc *d, orc_system **out) {
     *out = NULL;
     orc_system *s = calloc(1, sizeof(orc_system));
     int rc = olat_init(&s->L, &d->lattice);
     if (rc) { free(s); return rc; }
+    if (d->overflow_protection && (rc = olat_init_log(&s->L))) { olat_free(&s->L); free(s); return rc; }
     int M = s->L.M, ns = d->n_segments;
     s->nseg = ns;
     s->freedom = calloc(ns, sizeof(int));
@@ -845,12 +854,360 @@ static void orient_acc(const olat *L, const double *a, const double *b, double *
             if (is_interior(L, z)) out[2 * (size_t)M + z] += a[2 * (size_t)M + z] * b[2 * (size_t)M + z];
 }
 
+/* ------------------------------------------------------------------------ */
+/* Overflow protection: the *1stOS lattices in natural logarithms            */
+/* ------------------------------------------------------------------------ */
+#define LOGZERO (-DBL_MAX / 2)          /* SF_Box.h:51 */
+#define LOGCUTOFF 100.0                 /* SF_Box.h:45 */
+#define LOGTOLERANCE 50.0               /* SF_Box.h:47 */
+static double logmaxdouble(void) { return log(DBL_MAX); }                         /* SF_Box.h:31 */
+static double logmaxprefactor(void) { return logmaxdouble() - LOGCUTOFF - LOGTOLERANCE; }   /* SF_Box.h:49 */
+
+/* Lat1DFlat1stOS.cpp:3-9, Lat2DFlat1stOS.cpp:8-13, Lat2DCyl1stOS.cpp:3-25 */
+static int olat_init_log(olat *L) {
+    if (L->order != 1 || L->grad > 2) return SFGPU_ERR_UNSUPPORTED;   /* SF_System.cpp:395, :478-481 */
+    L->logmode = 1;
+    double l1 = L->l1;
+    if (!L->cyl) {
+        double l0 = (L->grad == 1) ? 1 - 2 * l1 : 1 - 4 * l1;
+        L->LogL1L0 = log(l1 / l0);
+        L->LogL0 = log(l0);
+        L->LogL1 = log(l1);
+    }
+    if (L->cyl && L->grad == 2) {
+        int MX = L->Md[0];
+        L->logl0x = calloc(MX, sizeof(double));
+        L->loglmx = calloc(MX, sizeof(double));
+        L->loglpx = calloc(MX, sizeof(double));
+        for (int x = 1; x < MX - 1; x++) {
+            double lm = L->lam_m[x], lp = L->lam_p[x];
+            L->loglpx[x] = (lp > 0) ? log(lp) : 0;
+            L->loglmx[x] = (lm > 0) ? log(lm) : 0;
+            double l0 = 1.0 - lm - lp - 2 * l1;
+            L->logl0x[x] = (l0 > 0) ? log(l0) : 0;
+        }
+        L->logl1 = (l1 > 0) ? log(l1) : 0;
+        L->nl_centre = 1.0 - l1 - l1 - l1 - l1;   /* nl[1], Lat2DCyl1stOS.cpp:191 */
+    }
+    return SFGPU_OK;
+}
+
+/* MakeSafe / RestoreFromSafe, Lat1DFlat1stOS.cpp:21-56 */
+static void make_safe(int M, double *A) {
+    for (int z = 0; z < M; z++) {
+        if (A[z] > 0) {
+            if (A[z] > exp(LOGCUTOFF)) {
+                double y = (log(A[z]) - LOGCUTOFF) / logmaxprefactor();
+                A[z] = LOGCUTOFF + 0.5 * logmaxprefactor() * log((1 + y) / (1 - y));
+            } else {
+                A[z] = log(A[z]);
+            }
+        } else {
+            A[z] = LOGZERO;
+        }
+    }
+}
+static void restore_from_safe(int M, double *A) {
+    for (int z = 0; z < M; z++) {
+        if (A[z] > LOGZERO) {
+            if (A[z] > LOGCUTOFF) A[z] = exp(LOGCUTOFF + logmaxprefactor() * tanh((A[z] - LOGCUTOFF) / logmaxprefactor()));
+            else A[z] = exp(A[z]);
+        } else {
+            A[z] = 0;
+        }
+    }
+}
+
+/* boundary values of a log-space vector: LOGZERO on surfaces, copies
+   elsewhere (Gout[1] = LOGZERO; Gout[1] = Gout[bound1], Lat1DFlat1stOS.cpp:140-143;
+   UpdateBoundaries, Lat2DFlat1stOS.cpp:538-573) */
+static void olat_log_boundaries(const olat *L, double *p) {
+    for (int z = 0; z < L->M; z++) {
+        if (is_interior(L, z)) continue;
+        int c[3]; coords(L, z, c);
+        for (int k = 0; k < L->grad; k++)
+            if ((c[k] == 0 && L->bc_lo[k] == SFGPU_BOUND_SURFACE) || (c[k] == L->Md[k] - 1 && L->bc_hi[k] == SFGPU_BOUND_SURFACE))
+                p[z] = LOGZERO;
+    }
+    for (int z = 0; z < L->M; z++) {
+        if (is_interior(L, z)) continue;
+        int m = mapped_site(L, z, NULL);
+        if (m != z && is_interior(L, m)) p[z] = p[m];
+    }
+}
+
+/* one log-space step; gin carries its boundary values.  Lat1DFlat1stOS.cpp:120-145,
+   Lat1DCyl1stOS.cpp:45-74 (also the sphere), Lat2DFlat1stOS.cpp:140-169 with
+   getNewGi (:335-362), Lat2DCyl1stOS.cpp:173-228 */
+static void olat_prop1_log(const olat *L, const double *gin, const double *G, double *gout) {
+    int M = L->M;
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(L, z)) continue;
+        if (G[z] == LOGZERO) { gout[z] = LOGZERO; continue; }
+        double r;
+        if (L->grad == 1) {
+            double a = gin[z - 1], b = gin[z], c = gin[z + 1];
+            if (!L->cyl) {
+                if (b > LOGZERO && L->l1 < 0.5) r = G[z] + L->LogL0 + b + log1p(exp(L->LogL1L0 + a - b) + exp(L->LogL1L0 + c - b));
+                else if (a > LOGZERO) r = G[z] + L->LogL1 + a + log1p(exp(c - a));
+                else if (c > LOGZERO) r = G[z] + L->LogL1 + c;
+                else r = LOGZERO;
+            } else {
+                double lp = L->lam_p[z], lm = L->lam_m[z];
+                double lambda0 = 1 - lp - lm;
+                if (b > LOGZERO && lambda0 > 0) r = G[z] + log(lambda0) + b + log1p((lm / lambda0) * exp(a - b) + (lp / lambda0) * exp(c - b));
+                else if (a > LOGZERO) r = G[z] + log(lm) + a + log1p((lp / lm) * exp(c - a));
+                else if (c > LOGZERO) r = G[z] + log(lp) + c;
+                else r = LOGZERO;
+            }
+        } else {
+            int MY = L->Md[1], x = z / MY;
+            double b = gin[z];
+            if (!L->cyl) {
+                double n[4] = {gin[z - 1], gin[z + 1], gin[z - MY], gin[z + MY]};
+                double lnterm = 0;
+                if (b != LOGZERO && L->l1 < 0.25) {
+                    for (int i = 0; i < 4; i++) if (n[i] != LOGZERO) lnterm += exp(L->LogL1L0 + n[i] - b);
+                    r = G[z] + L->LogL0 + b + log1p(lnterm);
+                } else {
+                    int i = 0;
+                    while (i < 4 && n[i] == LOGZERO) i++;
+                    if (i == 4) r = LOGZERO;
+                    else {
+                        for (int j = i + 1; j < 4; j++) if (n[j] != LOGZERO) lnterm += exp(n[j] - n[i]);
+                        r = G[z] + L->LogL1 + n[i] + log1p(lnterm);
+                    }
+                }
+            } else {
+                double ng[5] = {gin[z - 1], b, gin[z + 1], gin[z - MY], gin[z + MY]};
+                double nl[5] = {L->l1, L->nl_centre, L->l1, L->lam_m[x], L->lam_p[x]};
+                double lognl[5] = {L->logl1, L->logl0x[x], L->logl1, L->loglmx[x], L->loglpx[x]};
+                int i = 0;
+                while (i < 5 && (ng[i] == LOGZERO || nl[i] <= 0)) i++;
+                if (i == 5) r = LOGZERO;
+                else {
+                    double lnterm = 0;
+                    for (int j = 0; j < 5; j++) if (j != i && ng[j] != LOGZERO) lnterm += nl[j] * exp(ng[j] - ng[i]);
+                    r = G[z] + lognl[i] + ng[i] + log1p(lnterm / nl[i]);
+                }
+            }
+        }
+        gout[z] = r;
+    }
+    olat_log_boundaries(L, gout);
+}
+
+/* copy layer indices of the reference (1-based): lower surface 1, mirror1 2,
+   mirror2 3, periodic M-1; upper M, M-1, M-2, periodic 2 */
+static int copy_lo1(const olat *L, int k) { return L->bc_lo[k] == SFGPU_BOUND_PERIODIC ? L->Md[k] - 1 : L->bc_lo[k]; }
+static int copy_hi1(const olat *L, int k) { return L->bc_hi[k] == SFGPU_BOUND_PERIODIC ? 2 : L->Md[k] - L->bc_hi[k] + 1; }
+
+/* addLntoLn, Lat2DFlat1stOS.cpp:430-447 */
+static void add_ln_to_ln(double v1, double v2, double *v, int add) {
+    if (v1 != LOGZERO && v2 != LOGZERO) {
+        if (*v == LOGZERO) *v = v1 + v2;
+        else {
+            double sum = v1 + v2 - *v;
+            if (sum > logmaxdouble() - 1) *v = v1 + v2;
+            else { sum = add ? exp(sum) : -exp(sum); *v += log1p(sum); }
+        }
+    }
+}
+
+/* ComputeLnGN of the log-space lattices, in the reference's own sequence:
+   Lat1DFlat1stOS.cpp:441-478, Lat1DCyl1stOS.cpp:242-281,
+   Lat2DFlat1stOS.cpp:449-505, Lat2DCyl1stOS.cpp:471-540 */
+static double olat_lngn_log(const olat *L, const double *Gi) {
+    double value = LOGZERO, lmax = logmaxdouble();
+    if (L->grad == 1) {
+        int M = L->M;   /* the reference's 1-based layer z is z - 1 here */
+        #define LNL(z) (L->cyl ? log(L->Lx[z]) : 0.0)
+        if (Gi[1] > LOGZERO) {
+            value = L->cyl ? LNL(1) + Gi[1] : Gi[1];
+            if (copy_lo1(L, 0) == 3) value -= log(2.0);
+        }
+        for (int z = 2; z <= M - 3; z++) {
+            if (Gi[z] > LOGZERO) {
+                double t = L->cyl ? LNL(z) + Gi[z] : Gi[z];
+                double x = t - value;
+                if (x > lmax - 1 || value == LOGZERO) value = t;
+                else value += log1p(exp(x));
+            }
+        }
+        if (copy_hi1(L, 0) == M - 2 && Gi[M - 2] > LOGZERO) {
+            double x = L->cyl ? LNL(M - 2) + Gi[M - 2] - value - log(2.0) : Gi[M - 2] - log(2.0) - value;
+            if (x > lmax - 1 || value == LOGZERO) value = L->cyl ? LNL(M - 2) + Gi[M - 2] - log(2.0) : Gi[M - 2] - log(2.0);
+            else value += log1p(exp(x));
+        } else if (M > 3) {
+            if (Gi[M - 2] > LOGZERO) {
+                double t = L->cyl ? LNL(M - 2) + Gi[M - 2] : Gi[M - 2];
+                double x = t - value;
+                if (x > lmax - 1 || value == LOGZERO) value = t;
+                else value += log1p(exp(x));
+            }
+        }
+        #undef LNL
+        return value;
+    }
+    int MX = L->Md[0], MY = L->Md[1];
+    double log2 = log(2.0), log4 = log(4.0);
+    #define AT(x, y) Gi[(x) * MY + (y)]
+    #define LX(x) (L->cyl ? log(L->Lx[x]) : 0.0)
+    for (int x = 1; x < MX - 1; x++)
+        for (int y = 1; y < MY - 1; y++) add_ln_to_ln(AT(x, y), LX(x), &value, 1);
+    if (copy_lo1(L, 0) == 3)
+        for (int y = 1; y < MY - 1; y++) add_ln_to_ln(AT(1, y), LX(1) - log2, &value, 0);
+    if (copy_hi1(L, 0) == MX - 2)
+        for (int y = 1; y < MY - 1; y++) add_ln_to_ln(AT(MX - 2, y), LX(MX - 2) - log2, &value, 0);
+    if (copy_lo1(L, 1) == 3)
+        for (int x = 1; x < MX - 1; x++) add_ln_to_ln(AT(x, 1), LX(x) - log2, &value, 0);
+    /* the upper y column is taken at 1-based y = MY-2, 0-based MY-3 */
+    if (copy_hi1(L, 1) == MY - 2)
+        for (int x = 1; x < MX - 1; x++) add_ln_to_ln(AT(x, MY - 3), LX(x) - log2, &value, 0);
+    {
+        /* corners back: flat -log 4, cylinder log L + log 4 */
+        double c1 = L->cyl ? LX(1) + log4 : -log4, c2 = L->cyl ? LX(MX - 2) + log4 : -log4;
+        int X1 = copy_lo1(L, 0) == 3, X2 = copy_hi1(L, 0) == MX - 2;
+        int Y1 = copy_lo1(L, 1) == 3, Y2 = copy_hi1(L, 1) == MY - 2;
+        if (X1 && Y1) add_ln_to_ln(AT(1, 1), c1, &value, 1);
+        if (X1 && Y2) add_ln_to_ln(AT(1, MY - 3), c1, &value, 1);
+        if (X2 && Y1) add_ln_to_ln(AT(MX - 2, 1), c2, &value, 1);
+        if (X2 && Y2) add_ln_to_ln(AT(MX - 2, MY - 3), c2, &value, 1);
+    }
+    #undef AT
+    #undef LX
+    return value;
+}
+
+/* ConnectG of the log-space lattices, Lat1DFlat1stOS.cpp:344-375, on every site */
+static void connect_log(int M, const double *a, const double *b, double *out) {
+    for (int z = 0; z < M; z++) {
+        if (a[z] > LOGZERO && b[z] > LOGZERO) {
+            double x = a[z] + b[z] - out[z];
+            if (x > logmaxdouble() - 1 || out[z] == LOGZERO) out[z] = a[z] + b[z];
+            else out[z] += log1p(exp(x));
+        }
+    }
+}
+/* CorrectDoubleCountG, Lat1DFlat1stOS.cpp:289-298 */
+static void correct_double_count_log(int M, double *phi, const double *G) {
+    for (int z = 0; z < M; z++) {
+        if (G[z] > LOGZERO && phi[z] > LOGZERO) phi[z] -= G[z];
+        else phi[z] = LOGZERO;
+    }
+}
+/* NormPhiFree, Lat1DFlat1stOS.cpp:340-347 and Lat2DFlat1stOS.cpp:507-522 */
+static void norm_phi_log(const olat *L, int M, double *phi, double lognorm, int norm_is_zero) {
+    if (norm_is_zero && L->grad == 2) { for (int z = 0; z < M; z++) phi[z] = LOGZERO; return; }
+    for (int z = 0; z < M; z++) if (phi[z] > LOGZERO) phi[z] += lognorm;
+}
+
+/* molecule_phi with overflow protection: SF_Monomer1stO.cpp:101-133,
+   SF_Homopol1stO.cpp:553-622, SF_Copol1stO.cpp:1187-1281 on the log-space
+   lattice functions above; the segment weights enter through MakeSafe and
+   the volume fractions leave through RestoreFromSafe */
+static void molecule_phi_log(orc_system *s, omol *o) {
+    olat *L = &s->L;
+    int M = L->M, N = o->N;
+    double *lG = malloc(sizeof(double) * M * (size_t)s->nseg);
+    for (int a = 0; a < o->nseg_used; a++) {
+        int i = o->used[a];
+        memcpy(lG + (size_t)i * M, s->swf + (size_t)i * M, sizeof(double) * M);
+        make_safe(M, lG + (size_t)i * M);
+        for (int z = 0; z < M; z++) o->phi[(size_t)i * M + z] = LOGZERO;
+    }
+    if (o->type == 0) {
+        int i = o->seg[0];
+        double *phi = o->phi + (size_t)i * M;
+        const double *G = lG + (size_t)i * M;
+        memcpy(phi, G, sizeof(double) * M);
+        o->lngn = olat_lngn_log(L, G);
+        if (o->freedom == SFGPU_MOL_RESTRICTED) {
+            o->lnc = log(o->theta) - o->lngn;
+            norm_phi_log(L, M, phi, log(o->theta) - olat_lngn_log(L, G), 0);
+            o->phibulk = o->theta / exp(o->lngn);
+        } else {
+            o->lnc = log(o->phibulk);
+            norm_phi_log(L, M, phi, log(o->phibulk), o->phibulk == 0);
+        }
+        restore_from_safe(M, phi);
+        free(lG);
+        return;
+    }
+    double *Ginv = malloc(sizeof(double) * M), *tmp = malloc(sizeof(double) * M);
+    if (o->type == 1) {
+        int i = o->seg[0], half = N / 2;
+        const double *G = lG + (size_t)i * M;
+        double *phi = o->phi + (size_t)i * M;
+        double *Gi = malloc(sizeof(double) * M * (size_t)half);
+        memcpy(Gi, G, sizeof(double) * M);
+        for (int t = 1; t < half; t++) olat_prop1_log(L, Gi + (size_t)(t - 1) * M, G, Gi + (size_t)t * M);
+        memcpy(Ginv, Gi + (size_t)(half - 1) * M, sizeof(double) * M);
+        if (N % 2 == 1) {
+            olat_prop1_log(L, Ginv, G, tmp); memcpy(Ginv, tmp, sizeof(double) * M);
+            connect_log(M, Ginv, Ginv, phi);
+            norm_phi_log(L, M, phi, log(0.5), 0);
+        }
+        for (int sp = (N + 3) / 2; sp <= N; sp++) {
+            int sinv = N - sp + 1;
+            olat_prop1_log(L, Ginv, G, tmp); memcpy(Ginv, tmp, sizeof(double) * M);
+            connect_log(M, Ginv, Gi + (size_t)(sinv - 1) * M, phi);
+        }
+        correct_double_count_log(M, phi, G);
+        o->lngn = olat_lngn_log(L, Ginv);
+        if (o->freedom == SFGPU_MOL_RESTRICTED) {
+            o->lnc = log(o->theta) - o->lngn - log(1.0 * N);
+            norm_phi_log(L, M, phi, log(2 * o->theta / N) - olat_lngn_log(L, Ginv), 0);
+            o->phibulk = o->theta / exp(o->lngn);
+        } else {
+            norm_phi_log(L, M, phi, log(2 * o->phibulk / N), o->phibulk == 0);
+            o->lnc = log(o->phibulk / N);
+        }
+        restore_from_safe(M, phi);
+        free(Gi);
+    } else {
+        double *Gi = malloc(sizeof(double) * M * (size_t)N);
+        memcpy(Gi, lG + (size_t)o->seg[0] * M, sizeof(double) * M);
+        for (int t = 1; t < N; t++)
+            olat_prop1_log(L, Gi + (size_t)(t - 1) * M, lG + (size_t)o->seg[t] * M, Gi + (size_t)t * M);
+        memcpy(Ginv, lG + (size_t)o->seg[N - 1] * M, sizeof(double) * M);
+        connect_log(M, Ginv, Gi + (size_t)(N - 1) * M, o->phi + (size_t)o->seg[N - 1] * M);
+        for (int t = N - 2; t >= 0; t--) {
+            int sg = o->seg[t];
+            olat_prop1_log(L, Ginv, lG + (size_t)sg * M, tmp); memcpy(Ginv, tmp, sizeof(double) * M);
+            connect_log(M, Ginv, Gi + (size_t)t * M, o->phi + (size_t)sg * M);
+        }
+        o->lngn = olat_lngn_log(L, Ginv);
+        for (int a = 0; a < o->nseg_used; a++)
+            correct_double_count_log(M, o->phi + (size_t)o->used[a] * M, lG + (size_t)o->used[a] * M);
+        double lognorm;
+        int zero = 0;
+        if (o->freedom == SFGPU_MOL_RESTRICTED) {
+            o->lnc = log(o->theta) - o->lngn - log(1.0 * N);
+            o->phibulk = o->theta / exp(o->lngn);
+            lognorm = log(o->theta / N) - olat_lngn_log(L, Ginv);
+        } else {
+            o->lnc = log(o->phibulk / N);
+            lognorm = log(o->phibulk / N);
+            zero = (o->phibulk == 0);
+        }
+        for (int a = 0; a < o->nseg_used; a++) {
+            double *phi = o->phi + (size_t)o->used[a] * M;
+            norm_phi_log(L, M, phi, lognorm, zero);
+            restore_from_safe(M, phi);
+        }
+        free(Gi);
+    }
+    free(Ginv); free(tmp); free(lG);
+}
+
 /* one molecule: SF_Monomer1stO::Matrix1 (SF_Monomer1stO.cpp:99-130),
    SF_Homopol1stO::Matrix1 (SF_Homopol1stO.cpp:553-622),
    SF_Copol1stO::Matrix1 (SF_Copol1stO.cpp:1187-1281),
    SF_Homopol2ndO::Matrix1 (SF_Homopol2ndO.cpp:153-207),
    SF_Copol2ndO::Matrix1 (SF_Copol2ndO.cpp:250-356) */
 static void molecule_phi(orc_system *s, omol *o) {
+    if (s->L.logmode) { molecule_phi_log(s, o); return; }
     olat *L = &s->L;
     int M = L->M, N = o->N, K = L->K;
     size_t KM = (size_t)K * M;
@@ -1200,11 +1557,23 @@ int orc_propagate(const orc_system *s, const double *gin, const double *g, doubl
     int M = s->L.M, K = s->L.K;
     double *tmp = malloc(sizeof(double) * K * M);
     memcpy(tmp, gin, sizeof(double) * K * M);
+    if (s->L.logmode) {   /* the *1stOS step on logarithms */
+        olat_log_boundaries(&s->L, tmp);
+        olat_prop1_log(&s->L, tmp, g, gout);
+        free(tmp);
+        return SFGPU_OK;
+    }
     if (K == 6) olat_set_boundaries6(&s->L, tmp);
     else if (K > 1) olat_set_boundaries_lumped(&s->L, tmp);
     else olat_set_boundaries(&s->L, tmp);
     propagate_any(s, tmp, g, S, gout, backward);
     free(tmp);
+    return SFGPU_OK;
+}
+/* lnGN of a propagator at the lattice level: ComputeLnGN (on logarithms
+   with overflow protection) */
+int orc_lat_lngn(const orc_system *s, const double *g, double *lngn) {
+    *lngn = s->L.logmode ? olat_lngn_log(&s->L, g) : olat_lngn(&s->L, g);
     return SFGPU_OK;
 }
 int orc_side(const orc_system *s, const double *phi, double *rho) { olat_side(&s->L, phi, rho); return SFGPU_OK; }

@@ -109,3 +109,19 @@ mol : w : freedom : solvent
     text2 = text.replace("lat : l : n_sites_first_layer : 20\n", "lat : l : offset_first_layer : 2.5\n")
     spec2, _ = build_system(parse_input(text2)[0])
     assert spec2.lattice.offset_first_layer == 2.5 and spec2.lattice.layer_adjustment == 1.0
+
+
+def test_overflow_protection_statement():
+    """sys : overflow_protection : true selects the log-space lattices; 3D and
+    second-order systems reject it as SFbox does (SF_System.cpp:395, :478-481)."""
+    from field_b200 import configs
+    base = configs.C1_INPUT.format(n=20, N=10, phib=0.01, chi_aw=0.5, chi_as=-1.0).replace("start\n", "")
+    spec, _ = build_system(parse_input(base + "sys : noname : overflow_protection : true\nstart\n")[0])
+    assert spec.overflow_protection
+    spec, _ = build_system(parse_input(base + "start\n")[0])
+    assert not spec.overflow_protection
+    with pytest.raises(ValueError):
+        build_system(parse_input(base + "sys : noname : overflow_protection : maybe\nstart\n")[0])
+    with pytest.raises(ValueError):
+        build_system(parse_input(base + "sys : noname : overflow_protection : true\n"
+                                 "sys : noname : matrix_approach : second_order\nstart\n")[0])
