@@ -5,7 +5,8 @@ Runs an SFbox input file the way ``sfbox input.in`` does for the SCF path
 ``var :`` sweep in order, each point started from the previous point's
 result (``newton : initial_guess : previous_result``, the default), and
 ``ana`` / ``kal`` output files written after every point
-(field_b200.output).  Sweeps of first-order systems are solved as batched
+(field_b200.output).  ``vtk`` files are written one per
+calculation under numbered names.  Sweeps of first-order systems are solved as batched
 instances (field_b200.sweep): ``--waves`` sets how many batched launches the
 sweep is split into (default: one per point, SFbox's chain).  Solver:
 Pure_DIIS on the device with the file's tolerance, iterationlimit, m and
@@ -26,7 +27,9 @@ def main(argv=None) -> int:
     ap.add_argument("--outdir", default=None, help="directory for the output files (default: the input's)")
     ap.add_argument("--waves", type=int, default=0, help="batched launches per sweep (0: one per point)")
     a = ap.parse_args(argv)
-    from .output import output_lines, output_requests, write_ana, write_kal
+    from .output import (numbered_filename, output_lines, output_requests, read_template, write_ana, write_kal,
+                         write_vtk)
+    from .desc import LATTICE_HEX
     from .sfinput import build_system, parse_input
     from .sweep import batchable, solve_sweep, sweep_calculations
     from .system import System
@@ -39,7 +42,9 @@ def main(argv=None) -> int:
     calc_number = 0
     x_prev = None
     all_ok = True
-    for calc in parse_input(text):
+    calcs = parse_input(text)
+    indir = os.path.dirname(os.path.abspath(a.input))
+    for ci, calc in enumerate(calcs, start=1):
         var, points = sweep_calculations(calc)
         built = [build_system(p) for p in points]
         st = built[0][1]
@@ -58,7 +63,7 @@ def main(argv=None) -> int:
                 r = System(spec).solve(x, tol=st.tolerance, maxit=st.iterationlimit, m=st.m, eta=st.deltamax)
                 results.append((r.x, r.iterations, r.status))
                 x = r.x
-        for (spec, stp), (x, its, status), p in zip(built, results, points):
+        for pi, ((spec, stp), (x, its, status), p) in enumerate(zip(built, results, points)):
             calc_number += 1
             all_ok &= status == 0
             sys_ = System(spec)
@@ -67,11 +72,20 @@ def main(argv=None) -> int:
             for name, kind, params in output_requests(p):
                 path = os.path.join(outdir, name)
                 first = path not in written
+                if params.get("write", "true") == "false":
+                    continue
                 if kind == "ana":
                     write_ana(path, lines, first, params.get("write_bounds", "true") != "false",
                               spec.lattice.shape)
-                else:
+                elif kind == "kal":
                     write_kal(path, lines, first)
+                else:
+                    tmpl = params.get("template")
+                    tmpl = read_template(os.path.join(indir, tmpl)) if tmpl else None
+                    vpath = os.path.join(outdir, numbered_filename(name, ci, len(calcs), var,
+                                                                   var.values[pi] if var else None))
+                    write_vtk(vpath, lines, spec.lattice.shape, tmpl,
+                              spec.lattice.gradients == 3 and spec.lattice.lattice_type == LATTICE_HEX)
                 written.add(path)
             print(f"calculation {calc_number}: {'converged' if status == 0 else 'NOT converged'} "
                   f"in {its} iterations, |f| = {err:.3g}", flush=True)

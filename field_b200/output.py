@@ -17,6 +17,8 @@ The keys are SFbox's.  Two writers:
 * ``kal`` (Output::OutputKal, Output.cpp:640-726): one header row of
   ``c : n : k`` names of the scalar lines, tab separated, on a new file, then
   one row of values per calculation.
+* ``vtk`` (Output::OutputVtkProfiles, Output.cpp:727-905): one file per
+  calculation (numbered names) with the profiles a template selects.
 
 Scalars are printed with ``accuracy`` significant digits (default
 int(-log10(tolerance) + 0.5), SF_Box.cpp:93); profile values with six, as a
@@ -176,6 +178,120 @@ def write_kal(path: str, lines: List[OutputLine], first: bool) -> None:
         f.write("\t".join(ln.value for ln in scal) + "\n")
 
 
+def _wild(pattern: str, text: str) -> bool:
+    """WildCompare (Input.cpp:977-1030): '*' stands for any run of characters."""
+    import re
+    return re.fullmatch(".*".join(re.escape(p) for p in pattern.split("*")), text) is not None
+
+
+def read_template(path: str) -> List[Tuple[str, str, str]]:
+    """The ``class : name : key`` triples of an output template file (an
+    input file whose lines name the output lines to write)."""
+    out = []
+    with open(path) as f:
+        for raw in f:
+            parts = [p.strip() for p in raw.split(":")]
+            if len(parts) >= 3 and parts[0] and not parts[0].startswith("//"):
+                out.append((parts[0], parts[1], parts[2]))
+    return out
+
+
+def in_template(template, line: OutputLine) -> bool:
+    """Output::ValueInTemplate (Output.cpp:1264-1268)."""
+    return any(_wild(a, line.cls) and _wild(b, line.name) and _wild(c, line.key) for a, b, c in template)
+
+
+def vary_value_text(variation, value: float) -> str:
+    """Vary::GetCurrValue (Vary.cpp:227-290), the value put into numbered
+    file names: integers zero-padded to the digits of the larger end point;
+    linear reals as %.5f of the value over 10^e followed by 'e' and e printed
+    unsigned, e = int(log10 of the larger end point); exponential sweeps
+    (Text::Putreal there) as %g with that many significant digits."""
+    big = max(abs(variation.start), abs(variation.end))
+    if variation.scale == "linear":
+        if variation.vtype == "integer":
+            width = min(int(math.log10(big)) + 1, 100) if big > 0 else 1
+            return f"{int(value):0{width}d}"
+        expo = int(math.log10(big)) if big > 0 else 0
+        return f"{value / 10.0 ** expo:.5f}e{expo & 0xFFFFFFFF}"
+    f = math.exp(math.log(10.0) / variation.step)
+    width = int(math.log10(abs(value / (value * f - value)))) + 1
+    if width == 1:
+        width = 2
+    return f"{value:.{width}g}"
+
+
+def numbered_filename(name: str, calc_number: int, total_calcs: int, variation=None, value=None) -> str:
+    """Output::getNumberedFilename (Output.cpp:1291-1350): the calculation
+    number, zero-padded, when the input has more than one calculation, and
+    ``_<variable>=<value>`` during a sweep, inserted before the extension."""
+    insert = ""
+    if total_calcs > 1:
+        digits = int(math.log10(total_calcs)) + 1
+        insert = "_" + str(calc_number).zfill(digits)
+    if variation is not None:
+        insert += "_" + variation.name + "=" + vary_value_text(variation, value)
+    base, dot, ext = name.rpartition(".")
+    return (base + insert + dot + ext) if dot else (name + insert)
+
+
+def write_vtk(path: str, lines: List[OutputLine], lattice_shape: Tuple[int, ...], template=None,
+              hex_lattice: bool = False) -> None:
+    """Output::OutputVtkProfiles (Output.cpp:727-905), as it writes the file:
+    a structured-points header ('DIMENSIONS' and the layer count run together
+    in 1D; the HEX lattice as a structured grid with its sheared points),
+    one 'SFBox_profile double' per profile written, and the data of the
+    interior sites -- in 1D the selected profiles side by side for the layers
+    1..n-1 (0-based), in 2D the template's first profile at (x, y-1) for
+    y = 1..n_y, x = 1..n_x, in 3D at (x, y, z) with x fastest."""
+    prof = [ln for ln in lines if ln.profile is not None and (template is None or in_template(template, ln))]
+    n = [int(s) - 2 for s in lattice_shape]
+    g = len(n)
+    out = ["# vtk DataFile Version 3.0", "vtk output", "ASCII",
+           "DATASET STRUCTURED_GRID" if hex_lattice else "DATASET STRUCTURED_POINTS"]
+    if g == 1:
+        out += [f"DIMENSIONS{n[0]}", "SPACING 1", "ORIGIN 0", f"POINT_DATA {n[0]}"]
+    elif g == 2:
+        out += [f"DIMENSIONS {n[0]} {n[1]} 1", "SPACING 1 1 1", "ORIGIN 0 0 0", f"POINT_DATA {n[0] * n[1]}"]
+    else:
+        out.append(f"DIMENSIONS {n[0]} {n[1]} {n[2]}")
+        if hex_lattice:
+            out.append(f"POINTS {n[0] * n[1] * n[2]} double")
+            yc1, yc2 = 0.75 ** 0.5, 0.1875 ** 0.5
+            for i in range(n[2]):
+                for j in range(n[1]):
+                    for k in range(n[0]):
+                        out.append(f"{k + 0.5 * j + 0.5 * i:g} {yc1 * j + yc2 * i:g} {0.75 * i:g}")
+        else:
+            out += ["SPACING 1 1 1", "ORIGIN 0 0 0"]
+        out.append(f"POINT_DATA {n[0] * n[1] * n[2]}")
+    out.append("SCALARS " + "\n".join("SFBox_profile double" for _ in prof))
+    out.append("LOOKUP_TABLE default ")
+    if g == 1:
+        for z in range(1, n[0]):
+            out.append("".join(f"{ln.profile[z]:g}" for ln in prof))
+    else:
+        sel = None
+        for ln in lines:
+            if template is not None and in_template(template, ln):
+                sel = ln
+                break
+        if sel is None or sel.profile is None:
+            raise ValueError("vtk output of a 2D or 3D lattice needs a template naming a profile")
+        p = np.asarray(sel.profile).reshape(lattice_shape)
+        if g == 2:
+            for y in range(1, n[1] + 1):
+                for x in range(1, n[0] + 1):
+                    out.append(f"{p[x, y - 1]:g}")
+        else:
+            for z in range(1, n[2] + 1):
+                for y in range(1, n[1] + 1):
+                    for x in range(1, n[0] + 1):
+                        out.append(f"{p[x, y, z]:g}")
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+
+
 def output_requests(calc: Dict[Key, str]) -> List[Tuple[str, str, Dict[str, str]]]:
     """The ``output : <file> : ...`` statements: (file name, type, parameters)."""
     names: List[str] = []
@@ -186,7 +302,7 @@ def output_requests(calc: Dict[Key, str]) -> List[Tuple[str, str, Dict[str, str]
     for n in names:
         params = {p: v for (c, nn, p), v in calc.items() if c == "output" and nn == n}
         t = params.get("type")
-        if t not in ("ana", "kal"):
-            raise ValueError(f"output : {n} : type : {t} is not written here (ana and kal are)")
+        if t not in ("ana", "kal", "vtk"):
+            raise ValueError(f"output : {n} : type : {t} is not written here (ana, kal and vtk are)")
         out.append((n, t, params))
     return out

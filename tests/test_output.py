@@ -43,7 +43,7 @@ def test_output_requests():
     req = output_requests(calc)
     assert [(n, t) for n, t, _ in req] == [("run.ana", "ana"), ("run.kal", "kal")]
     with pytest.raises(ValueError):
-        output_requests(parse_input("output : x.vtk : type : vtk\n")[0])
+        output_requests(parse_input("output : x.ave : type : ave\n")[0])
 
 
 class _OracleSystem:
@@ -109,3 +109,54 @@ def test_output_lines_keys_and_sums():
     assert d[("mon", "S", "freedom")].value == "frozen" and ("mon", "S", "G") not in d
     mol_keys = [l.key for l in lines if l.cls == "mol" and l.name == "pol"]
     assert mol_keys[:8] == ["freedom", "phibulk", "log(phibulk)", "phi-av", "theta", "theta excess", "n", "n exc"]
+
+
+def test_vtk_1d_and_2d_layout(tmp_path):
+    """OutputVtkProfiles as SFbox writes it: 1D puts the selected profiles side
+    by side for the layers 1..n-1 (0-based) under 'DIMENSIONS<n>'; 2D writes
+    the template's first profile at (x, y-1), y outer, x inner."""
+    from field_b200.output import write_vtk
+    prof = np.arange(7, dtype=float)          # 1D, n = 5 interior layers
+    lines = [OutputLine("mon", "A", "theta", "1"), OutputLine("mon", "A", "phi", "profile", prof)]
+    p = str(tmp_path / "a.vtk")
+    write_vtk(p, lines, (7,))
+    text = open(p).read().splitlines()
+    assert text[:4] == ["# vtk DataFile Version 3.0", "vtk output", "ASCII", "DATASET STRUCTURED_POINTS"]
+    assert text[4] == "DIMENSIONS5" and text[7] == "POINT_DATA 5"
+    assert text[8] == "SCALARS SFBox_profile double" and text[9] == "LOOKUP_TABLE default "
+    assert text[10:] == ["1", "2", "3", "4"]
+    grid = np.arange(5 * 4, dtype=float).reshape(5, 4)   # nx = 3, ny = 2
+    lines2 = [OutputLine("mon", "A", "phi", "profile", grid.ravel()),
+              OutputLine("mon", "B", "phi", "profile", -grid.ravel())]
+    p2 = str(tmp_path / "b.vtk")
+    write_vtk(p2, lines2, (5, 4), template=[("mon", "B", "*")])
+    t2 = open(p2).read().splitlines()
+    assert t2[4] == "DIMENSIONS 3 2 1" and t2[7] == "POINT_DATA 6"
+    vals = [float(v) for v in t2[10:]]
+    want = [-grid[x, y - 1] for y in (1, 2) for x in (1, 2, 3)]
+    assert vals == want
+    with pytest.raises(ValueError):
+        write_vtk(p2, lines2, (5, 4))
+
+
+def test_numbered_filenames_and_sweep_values():
+    from field_b200.output import numbered_filename
+    from field_b200.sweep import expand_variation
+    assert numbered_filename("run.vtk", 3, 12) == "run_03.vtk"
+    assert numbered_filename("run.vtk", 1, 1) == "run.vtk"
+    calc = parse_input("mon : A : chi - W : 0.2\nvar : mon : A : chi - W\nvar : mon : step : 0.2\n"
+                       "var : mon : end_value : 0.8\nvar : mon : type : real\n")[0]
+    var = expand_variation(calc)
+    assert numbered_filename("run.vtk", 1, 1, var, 0.4) == "run_chi - W=0.40000e0.vtk"
+    calc = parse_input("lat : l : n_layers : 20\nvar : lat : l : n_layers\nvar : lat : step : 5\n"
+                       "var : lat : end_value : 40\nvar : lat : type : integer\n")[0]
+    var = expand_variation(calc)
+    assert numbered_filename("p.vtk", 2, 3, var, 25) == "p_2_n_layers=25.vtk"
+
+
+def test_template_wildcards():
+    from field_b200.output import in_template
+    ln = OutputLine("mon", "A", "phi", "profile", np.zeros(3))
+    assert in_template([("mon", "*", "phi")], ln)
+    assert in_template([("m*", "A", "p*")], ln)
+    assert not in_template([("mol", "*", "phi")], ln)
