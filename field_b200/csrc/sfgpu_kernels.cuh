@@ -579,6 +579,27 @@ static __global__ void finalize_phi(int M, const double *__restrict__ G, double 
     }
 }
 
+// Dendrimer branch points (SF_Dend1stO.cpp:199-214, :245-253): out = a b / G
+// where G > 0, else 0 -- ConnectG into a zero vector, then CorrectDoubleCountG
+static __global__ void dend_combine(int M, const double *__restrict__ a, const double *__restrict__ b,
+                                    const double *__restrict__ G, double *__restrict__ out) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+        const double g = G[r];
+        out[r] = (g > 0) ? (a[r] * b[r]) / g : 0.0;
+    }
+}
+
+// NormPhiFree(Gi_inv, nr); ConnectG(Gi_inv, Gi, s, phi); NormPhiFree(Gi_inv,
+// 1/nr) of SF_Dend1stO.cpp:254-262 in one pass, with the same roundings
+static __global__ void dend_connect(int M, double *__restrict__ ginv, const double *__restrict__ gf,
+                                    double *__restrict__ phi, double nr, double inv_nr) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+        const double t = ginv[r] * nr;
+        phi[r] += t * gf[r];
+        ginv[r] = t * inv_nr;
+    }
+}
+
 // state phi = sum of the molecule contributions (SF_State::GetPhi, SF_State.cpp:302-320)
 struct PtrList { const double *p[SFGPU_MAX_SEG]; int n; };
 static __global__ void sum_profiles(int M, PtrList src, double *__restrict__ out) {

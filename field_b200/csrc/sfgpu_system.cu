@@ -337,11 +337,49 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
             if (freedom[sg] == SFGPU_SEG_FROZEN) return fail(SFGPU_ERR_INVALID, "frozen segment inside a molecule");
             o.count[sg]++;
         }
+        o.dend = 0;
+        if (md.n_generations > 0) {
+            // symmetric dendrimer: generations of consecutive blocks, the
+            // chain length and segment numbers of SF_MolStructure::SetMolLength
+            // and GetAvNumSegments (SF_MolStructure.cpp:552-595, :847-877)
+            if (!md.generation_blocks || !md.generation_repeat) return fail(SFGPU_ERR_INVALID, "dendrimer without generations");
+            if (K != 1) return fail(SFGPU_ERR_UNSUPPORTED, "dendrimers on second-order lattices");
+            const int G = md.n_generations;
+            o.gen_seg.assign(G, {});
+            o.gen_rep.assign(G, 0);
+            int b = 0;
+            for (int i = 0; i < G; i++) {
+                const int nb = md.generation_blocks[i];
+                if (nb < 1 || b + nb > md.n_blocks) return fail(SFGPU_ERR_INVALID, "dendrimer generation blocks");
+                for (int q = b; q < b + nb; q++)
+                    for (int r = 0; r < md.block_length[q]; r++) o.gen_seg[i].push_back(md.block_segment[q]);
+                b += nb;
+                o.gen_rep[i] = md.generation_repeat[i];
+                if (o.gen_rep[i] < 1) return fail(SFGPU_ERR_INVALID, "dendrimer functionality must be positive");
+            }
+            if (b != md.n_blocks) return fail(SFGPU_ERR_INVALID, "dendrimer generations must cover the blocks");
+            long long L = 0;
+            o.nshort = 0;
+            for (int i = G - 1; i >= 0; i--) L = (L + (long long)o.gen_seg[i].size() - 1) * o.gen_rep[i] + 1;
+            for (int i = 0; i < G; i++) o.nshort += (int)o.gen_seg[i].size();
+            if (L > (1LL << 30)) return fail(SFGPU_ERR_INVALID, "dendrimer too large");
+            for (int sg = 0; sg < nseg; sg++) {
+                long long num = 0;
+                for (int i = G - 1; i >= 0; i--) {
+                    long long n = 0;
+                    for (int q : o.gen_seg[i]) n += (q == sg);
+                    num = (o.gen_seg[i][0] == sg) ? (num + n - 1) * o.gen_rep[i] + 1 : (num + n) * o.gen_rep[i];
+                }
+                o.count[sg] = (int)num;
+            }
+            o.N = (int)L;
+            o.dend = (L > 1);
+        }
         o.used.clear();
         o.pinned = 0;
         for (int i = 0; i < nseg; i++)
             if (o.count[i]) { o.used.push_back(i); if (freedom[i] == SFGPU_SEG_PINNED) o.pinned = 1; }
-        o.type = (o.N == 1) ? 0 : (o.used.size() == 1 ? 1 : 2);
+        o.type = (o.N == 1) ? 0 : (o.used.size() == 1 && !o.dend ? 1 : 2);
         o.sym = (o.type == 1 && K == 1);
         o.freedom = md.freedom;
         o.phibulk = md.phibulk;
@@ -448,7 +486,7 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     for (auto &o : mols) {
         o.d_phi.assign(nseg, nullptr);
         for (int i : o.used) if ((rc = alloc_d(&o.d_phi[i], M))) return rc;
-        size_t need = (o.type == 0) ? 0 : (size_t)(o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
+        size_t need = (o.type == 0) ? 0 : (size_t)(o.dend ? o.nshort : o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
         store = std::max(store, need);
     }
     if ((rc = alloc_d(&d_gi, store))) return rc;
@@ -483,6 +521,8 @@ int sfgpu_system::setup_logspace() {
     const DLat &L = H.L;
     if (L.order != 1 || L.grad > 2)
         return fail(SFGPU_ERR_UNSUPPORTED, "overflow protection needs a first-order 1D or 2D lattice");
+    for (auto &o : mols)
+        if (o.dend) return fail(SFGPU_ERR_UNSUPPORTED, "dendrimers with overflow protection");
     logmode = true;
     logc.lmax = log(DBL_MAX);
     logc.logcutoff = 100.0;
@@ -642,8 +682,84 @@ int sfgpu_system::molecule_phi_log(int m) {
     return SFGPU_OK;
 }
 
+// SF_Dend1stO::Matrix1 (SF_Dend1stO.cpp:163-312): the propagator from the
+// ends inwards along one path from an end to the centre (nshort positions,
+// stored), the branch points combining f copies of the arriving propagator
+// (product divided by the branch point's G f-1 times), then from the centre
+// outwards with the composition weighted by the number of equivalent copies.
+int sfgpu_system::molecule_phi_dend(int m) {
+    HMol &o = mols[m];
+    const DLat &L = H.L;
+    const int g = grid_for(M);
+    cudaStream_t s = stream;
+    const int G = (int)o.gen_seg.size(), NS = o.nshort;
+    auto slice = [&](int sp) { return d_gi + (size_t)(sp - 1) * M; };   // position sp = 1..NS
+    for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_phi[i], 0, sizeof(double) * M, s));
+    double *ginv = d_ginv[0], *tmp = d_ginv[1];
+    // ends inwards
+    int sp = 0;
+    const double *Gold = nullptr;
+    for (int i = G - 1; i >= 0; i--) {
+        const int len = (int)o.gen_seg[i].size();
+        for (int j = len; j >= 1; j--) {
+            const double *Gc = d_gseg[o.gen_seg[i][j - 1]];
+            sp++;
+            if (sp == 1) {
+                SFGPU_CUDA_TRY(cudaMemcpyAsync(slice(1), Gc, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+            } else if (j == len && i + 1 < G && o.gen_rep[i + 1] > 1) {
+                // the node: f copies of the branch arriving at the outer
+                // generation's first segment (Gold)
+                const double *arr = slice(sp - 1);
+                const double *acc = arr;
+                for (int k = 1; k <= o.gen_rep[i + 1] - 1; k++) {
+                    dend_combine<<<g, kBlock, 0, s>>>(M, arr, acc, Gold, ginv);
+                    acc = ginv; std::swap(ginv, tmp);
+                }
+                launch_step1(acc, Gc, slice(sp), nullptr, nullptr, COMP_NONE);
+            } else {
+                launch_step1(slice(sp - 1), Gc, slice(sp), nullptr, nullptr, COMP_NONE);
+            }
+            Gold = Gc;
+        }
+    }
+    // centre outwards
+    sp = NS;
+    double nr = 1.0;
+    const double *cur = nullptr;
+    for (int i = 0; i < G; i++) {
+        const int len = (int)o.gen_seg[i].size(), rep = o.gen_rep[i];
+        for (int j = 1; j <= len; j++) {
+            const int sg = o.gen_seg[i][j - 1];
+            const double *Gc = d_gseg[sg];
+            if (sp == NS) SFGPU_CUDA_TRY(cudaMemcpyAsync(ginv, Gc, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+            else launch_step1(cur, Gc, ginv, nullptr, nullptr, COMP_NONE);
+            cur = ginv; std::swap(ginv, tmp);
+            if (j == 1)
+                for (int k = 1; k <= rep - 1; k++) {
+                    dend_combine<<<g, kBlock, 0, s>>>(M, cur, slice(sp), Gc, ginv);
+                    cur = ginv; std::swap(ginv, tmp);
+                }
+            dend_connect<<<g, kBlock, 0, s>>>(M, const_cast<double *>(cur), slice(sp), o.d_phi[sg], nr, 1.0 / nr);
+            if (j == 1) nr *= rep;
+            sp--;
+        }
+    }
+    MolParam p;
+    p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = 0; p.K = 1;
+    p.pinned = o.pinned; p.solvent = (m == solvent); p.nmol = nmol;
+    p.phibulk_in = o.phibulk; p.theta = o.theta;
+    wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, cur, d_wgn, d_partial);
+    mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, (MolScal *)d_scal, m);
+    for (int i : o.used) {
+        finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], (const MolScal *)d_scal, m, 0);
+        set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_phi[i]);
+    }
+    return SFGPU_OK;
+}
+
 int sfgpu_system::molecule_phi(int m) {
     if (logmode) return molecule_phi_log(m);
+    if (mols[m].dend) return molecule_phi_dend(m);
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_for(M);

@@ -14,6 +14,12 @@ struct HMol {
     int N = 0, type = 0, sym = 0, freedom = 0, pinned = 0;
     double phibulk = 0, theta = 0, chemintref = 0;
     std::vector<int> seg, used, count;
+    // symmetric dendrimer (SF_Dend1stO): per generation its positions'
+    // segments (first = branch point) and functionality; nshort = positions
+    // from the centre to an end
+    int dend = 0, nshort = 0;
+    std::vector<std::vector<int>> gen_seg;
+    std::vector<int> gen_rep;
     std::vector<double *> d_phi;      // per segment (used ones)
     std::vector<double *> d_dphi;     // tangents (allocated on first J*v)
     std::vector<double *> d_ori;      // bond orientation per segment, mphi*M (when enabled)
@@ -94,6 +100,7 @@ struct sfgpu_system {
     std::vector<double *> d_lgseg;            // log G per segment (MakeSafe)
     int setup_logspace();
     int molecule_phi_log(int m);
+    int molecule_phi_dend(int m);
     std::vector<void *> allocs;
 
     ~sfgpu_system();

@@ -39,7 +39,8 @@ class SegmentDesc(C.Structure):
 class MoleculeDesc(C.Structure):
     _fields_ = [("n_blocks", C.c_int), ("block_segment", C.POINTER(C.c_int)),
                 ("block_length", C.POINTER(C.c_int)), ("freedom", C.c_int),
-                ("phibulk", C.c_double), ("theta", C.c_double)]
+                ("phibulk", C.c_double), ("theta", C.c_double), ("n_generations", C.c_int),
+                ("generation_blocks", C.POINTER(C.c_int)), ("generation_repeat", C.POINTER(C.c_int))]
 
 
 class SystemDesc(C.Structure):
@@ -120,10 +121,42 @@ class Molecule:
     freedom: int = MOL_FREE
     phibulk: float = 0.0
     theta: float = 0.0
+    # symmetric dendrimer: per generation (number of its blocks in `blocks`,
+    # functionality f); None for a linear chain
+    generations: Optional[List[tuple]] = None
+
+    def generation_blocks(self) -> List[List[tuple]]:
+        out, b = [], 0
+        for nb, _f in self.generations or []:
+            out.append(self.blocks[b:b + nb])
+            b += nb
+        return out
 
     @property
     def N(self) -> int:
-        return int(sum(n for _, n in self.blocks))
+        """Chain length; a dendrimer's generation blocks share their first
+        segment among f copies (SF_MolStructure::SetMolLength,
+        SF_MolStructure.cpp:847-877)."""
+        if not self.generations:
+            return int(sum(n for _, n in self.blocks))
+        L = 0
+        for blocks, (_nb, f) in reversed(list(zip(self.generation_blocks(), self.generations))):
+            L = (L + sum(n for _, n in blocks) - 1) * f + 1
+        return int(L)
+
+    def count(self, seg: int) -> int:
+        """Segments of type seg in one molecule (GetAvNumSegments,
+        SF_MolStructure.cpp:552-595)."""
+        if not self.generations:
+            return int(sum(n for s, n in self.blocks if s == seg))
+        num = 0
+        for blocks, (_nb, f) in reversed(list(zip(self.generation_blocks(), self.generations))):
+            n = sum(k for s, k in blocks if s == seg)
+            num = (num + n - 1) * f + 1 if blocks[0][0] == seg else (num + n) * f
+        return int(num)
+
+    def segment_types(self) -> List[int]:
+        return sorted({s for s, _ in self.blocks})
 
 
 @dataclass
@@ -170,6 +203,16 @@ class SystemSpec:
             mols[m].n_blocks = len(mol.blocks)
             mols[m].block_segment, mols[m].block_length = iptr(bs), iptr(bl)
             mols[m].freedom, mols[m].phibulk, mols[m].theta = mol.freedom, mol.phibulk, mol.theta
+            if mol.generations:
+                gb = np.array([g[0] for g in mol.generations], dtype=np.int32)
+                gr = np.array([g[1] for g in mol.generations], dtype=np.int32)
+                keep += [gb, gr]
+                mols[m].n_generations = len(mol.generations)
+                mols[m].generation_blocks, mols[m].generation_repeat = iptr(gb), iptr(gr)
+            else:
+                mols[m].n_generations = 0
+                mols[m].generation_blocks = C.POINTER(C.c_int)()
+                mols[m].generation_repeat = C.POINTER(C.c_int)()
         d = SystemDesc()
         d.lattice = self.lattice.to_c()
         d.n_segments = ns

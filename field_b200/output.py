@@ -102,7 +102,7 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
                 R("chi list", spec.segments[i].name, "chi - " + spec.segments[j].name, chi[i, j])
     sites = float(w_sum.sum())
     mols = spec.molecules
-    N = [sum(n for _, n in m.blocks) for m in mols]
+    N = [m.N for m in mols]
     phib_m = [sys_.mol_scalars(m)["phibulk"] for m in range(len(mols))]
     for i, seg in enumerate(spec.segments):
         fr = {SEG_FROZEN: "frozen", SEG_PINNED: "pinned"}.get(seg.freedom, "free")
@@ -111,7 +111,7 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
         pb = 0.0
         if seg.freedom != SEG_FROZEN:
             for m, mol in enumerate(mols):
-                cnt = sum(n for s, n in mol.blocks if s == i)
+                cnt = mol.count(i)
                 pb += phib_m[m] * cnt / N[m]
         R("mon", seg.name, "phibulk", pb)
         theta = float((w_sum * phi).sum())
@@ -136,7 +136,14 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
         R("mol", mol.name, "theta excess", exc)
         R("mol", mol.name, "n", theta / N[m])
         R("mol", mol.name, "n exc", exc / N[m])
-        T("mol", mol.name, "composition", "".join(f"({spec.segments[s].name}){n}" for s, n in mol.blocks))
+        if mol.generations:
+            parts = [f"{len(mol.generations)}"]
+            for blocks, (_nb, f) in zip(mol.generation_blocks(), mol.generations):
+                parts += ["".join(f"({spec.segments[s].name}){n}" for s, n in blocks), str(f)]
+            comp = "@dend(" + ",".join(parts) + ")"
+        else:
+            comp = "".join(f"({spec.segments[s].name}){n}" for s, n in mol.blocks)
+        T("mol", mol.name, "composition", comp)
         T("mol", mol.name, "chainlength", N[m])
         R("mol", mol.name, "ln(G(N|1))", sc["lngn"])
         R("mol", mol.name, "ln(norm_restricted)" if mol.freedom == MOL_RESTRICTED else "ln(norm_free)", sc["lnc"])

@@ -77,6 +77,31 @@ def parse_composition(text: str) -> List[Tuple[str, int]]:
     return [(a, int(b)) for a, b in blocks]
 
 
+def parse_dendrimer(text: str) -> Optional[List[Tuple[List[Tuple[str, int]], int]]]:
+    """Symmetric dendrimer compositions '@dend(G, T1, f1, ..., TG, fG)'
+    (SF_MolStructure.cpp:116-140, :348-359): per generation its linear block
+    sequence Ti and its functionality fi.  None for other compositions."""
+    t = text.replace(" ", "")
+    if not t.startswith("@"):
+        return None
+    m = re.fullmatch(r"@dend\((.*)\)", t)
+    if not m:
+        raise ValueError(f"composition '{text}': only symmetric dendrimers @dend(G, T1, f1, ...) are on this path")
+    args = m.group(1).split(",")
+    if not args[0].isdigit():
+        raise ValueError(f"composition '{text}': asymmetric dendrimers and combs are not on this path")
+    G = int(args[0])
+    if len(args) - 1 != 2 * G or G < 1:
+        raise ValueError(f"composition '{text}': @dend(G, ...) needs G generations of (block, functionality)")
+    gens = []
+    for i in range(G):
+        f = args[2 + 2 * i]
+        if not f.isdigit() or int(f) < 1:
+            raise ValueError(f"composition '{text}': functionality '{f}' is not a positive integer")
+        gens.append((parse_composition(args[1 + 2 * i]), int(f)))
+    return gens
+
+
 @dataclass
 class SolverSettings:
     method: str = "Pure_DIIS"
@@ -222,20 +247,31 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
                 pf[i, j] = pf[j, i] = float(v)
     mols: List[Molecule] = []
     for mn in _names(calc, "mol"):
-        comp = parse_composition(_get(calc, "mol", mn, "composition"))
+        ctext = _get(calc, "mol", mn, "composition")
+        dend = parse_dendrimer(ctext)
+        gens = None
+        if dend is not None:
+            comp = [b for blocks_i, _f in dend for b in blocks_i]
+            gens = [(len(blocks_i), f) for blocks_i, f in dend]
+        else:
+            comp = parse_composition(ctext)
         blocks = [(seg_names.index(a), n_) for a, n_ in comp]
+        length = Molecule(mn, blocks, generations=gens).N
         fr = _get(calc, "mol", mn, "freedom", "free")
         if fr == "free":
-            mols.append(Molecule(mn, blocks, MOL_FREE, phibulk=float(_get(calc, "mol", mn, "phibulk"))))
+            mols.append(Molecule(mn, blocks, MOL_FREE, phibulk=float(_get(calc, "mol", mn, "phibulk")),
+                                 generations=gens))
         elif fr == "restricted":
             th = _get(calc, "mol", mn, "theta")
             if th is None:
                 nn = _get(calc, "mol", mn, "n")
                 if nn is None:
                     raise ValueError(f"mol : {mn} needs theta or n")
-                th = float(nn) * sum(b for _, b in blocks)
-            mols.append(Molecule(mn, blocks, MOL_RESTRICTED, theta=float(th)))
+                th = float(nn) * length
+            mols.append(Molecule(mn, blocks, MOL_RESTRICTED, theta=float(th), generations=gens))
         elif fr == "solvent":
+            if gens:
+                raise ValueError(f"mol : {mn} : a dendrimer cannot be the solvent here")
             mols.append(Molecule(mn, blocks, MOL_SOLVENT))
         else:
             raise ValueError(f"mol : {mn} : freedom : {fr} is not on this path")

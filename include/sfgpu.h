@@ -130,6 +130,14 @@ typedef struct {
     int        freedom;        /* SFGPU_MOL_* */
     double     phibulk;        /* free molecules */
     double     theta;          /* restricted molecules */
+    /* symmetric dendrimer, @dend(G, T1, f1, ..., TG, fG) (SF_MolStructure.cpp:116-140,
+     * :348-359; SF_Dend1stO): n_generations = G > 0 splits the blocks above into
+     * generations of generation_blocks[i] consecutive blocks (Ti, first order
+     * lattices), each repeated generation_repeat[i] = fi times around its first
+     * segment; 0 for a linear chain */
+    int        n_generations;
+    const int *generation_blocks;
+    const int *generation_repeat;
 } sfgpu_molecule_desc;
 
 typedef struct {

@@ -638,6 +638,10 @@ typedef struct {
     double lngn, lnc, chemintref;
     double *phi;          /* n_segments * M (only used ones nonzero) */
     double *ori;          /* 2nd order: n_segments * 3 * M bond-orientation slots */
+    /* symmetric dendrimer: generations (segments of each position, first =
+       branch point) and functionalities; nshort positions centre to end */
+    int ngen, nshort;
+    int *gen_len, *gen_rep, *gen_seg;   /* gen_seg: positions of all generations in order */
 } omol;
 
 struct orc_system {
@@ -718,7 +722,43 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
             o->used[o->nseg_used++] = i;
             if (s->freedom[i] == SFGPU_SEG_PINNED) o->pinned = 1;
         }
-        o->type = (N == 1) ? 0 : (o->nseg_used == 1 ? 1 : 2);
+        if (md->n_generations > 0) {
+            /* symmetric dendrimer, SF_MolStructure.cpp:348-359, :552-595, :847-877 */
+            int G = md->n_generations, b = 0, pos = 0;
+            if (s->L.order != 1) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
+            o->ngen = G;
+            o->gen_len = calloc(G, sizeof(int)); o->gen_rep = calloc(G, sizeof(int));
+            o->gen_seg = calloc(N, sizeof(int));
+            for (int i = 0; i < G; i++) {
+                int nb = md->generation_blocks[i];
+                if (nb < 1 || b + nb > md->n_blocks || md->generation_repeat[i] < 1) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+                for (int q = b; q < b + nb; q++)
+                    for (int r = 0; r < md->block_length[q]; r++) { o->gen_seg[pos++] = md->block_segment[q]; o->gen_len[i]++; }
+                b += nb;
+                o->gen_rep[i] = md->generation_repeat[i];
+            }
+            if (b != md->n_blocks) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+            o->nshort = pos;
+            long long Lm = 0;
+            for (int i = G - 1; i >= 0; i--) Lm = (Lm + o->gen_len[i] - 1) * o->gen_rep[i] + 1;
+            int off[64];
+            if (G > 64) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+            off[0] = 0;
+            for (int i = 1; i < G; i++) off[i] = off[i - 1] + o->gen_len[i - 1];
+            for (int sg = 0; sg < ns; sg++) {
+                long long num = 0;
+                for (int i = G - 1; i >= 0; i--) {
+                    long long n = 0;
+                    for (int q = 0; q < o->gen_len[i]; q++) n += (o->gen_seg[off[i] + q] == sg);
+                    num = (o->gen_seg[off[i]] == sg) ? (num + n - 1) * o->gen_rep[i] + 1 : (num + n) * o->gen_rep[i];
+                }
+                o->count[sg] = (int)num;
+            }
+            N = (int)Lm;
+            o->N = N;
+            if (N == 1) o->ngen = 0;
+        }
+        o->type = (N == 1) ? 0 : (o->nseg_used == 1 && !o->ngen ? 1 : 2);
         o->freedom = md->freedom; o->phibulk = md->phibulk; o->theta = md->theta;
         if (o->freedom == SFGPU_MOL_SOLVENT) {
             if (s->solvent >= 0) { orc_destroy(s); return SFGPU_ERR_INVALID; }
@@ -791,6 +831,7 @@ void orc_destroy(orc_system *s) {
     olat_free(&s->L);
     for (int m = 0; m < s->nmol; m++) {
         free(s->mol[m].seg); free(s->mol[m].count); free(s->mol[m].used); free(s->mol[m].phi); free(s->mol[m].ori);
+        free(s->mol[m].gen_len); free(s->mol[m].gen_rep); free(s->mol[m].gen_seg);
     }
     free(s->mol); free(s->freedom); free(s->range); free(s->chi); free(s->pf);
     free(s->stateQ); free(s->class_of); free(s->rep_of_class); free(s->sites);
@@ -1206,8 +1247,93 @@ static void molecule_phi_log(orc_system *s, omol *o) {
    SF_Copol1stO::Matrix1 (SF_Copol1stO.cpp:1187-1281),
    SF_Homopol2ndO::Matrix1 (SF_Homopol2ndO.cpp:153-207),
    SF_Copol2ndO::Matrix1 (SF_Copol2ndO.cpp:250-356) */
+/* SF_Dend1stO::Matrix1 (SF_Dend1stO.cpp:163-312) with the plain first-order
+   lattice functions: ends inwards along one end-to-centre path, f copies
+   combined at each branch point (ConnectG into zero, CorrectDoubleCountG),
+   then centre outwards with NormPhiFree(Gi_inv, NormRepeat) around ConnectG */
+static void molecule_phi_dend(orc_system *s, omol *o) {
+    olat *L = &s->L;
+    int M = L->M, G = o->ngen, NS = o->nshort, N = o->N;
+    double *Gi = calloc((size_t)M * NS, sizeof(double));
+    double *Ginv = malloc(sizeof(double) * M), *tmp = malloc(sizeof(double) * M);
+    double *add = malloc(sizeof(double) * M), *gt = malloc(sizeof(double) * M);
+    int off[64];
+    off[0] = 0;
+    for (int i = 1; i < G; i++) off[i] = off[i - 1] + o->gen_len[i - 1];
+    #define SEGAT(i, j) (o->gen_seg[off[i] + (j) - 1])
+    #define SLICE(sp) (Gi + (size_t)((sp) - 1) * M)
+    int sp = 0;
+    const double *Gold = NULL;
+    for (int i = G - 1; i >= 0; i--) {
+        for (int j = o->gen_len[i]; j >= 1; j--) {
+            const double *Gc = s->swf + (size_t)SEGAT(i, j) * M;
+            sp++;
+            if (sp == 1) memcpy(SLICE(1), Gc, sizeof(double) * M);
+            else if (j == o->gen_len[i] && i + 1 < G && o->gen_rep[i + 1] > 1) {
+                memcpy(gt, SLICE(sp - 1), sizeof(double) * M);
+                for (int k = 1; k <= o->gen_rep[i + 1] - 1; k++) {
+                    for (int z = 0; z < M; z++) add[z] = 0 + SLICE(sp - 1)[z] * gt[z];
+                    for (int z = 0; z < M; z++) add[z] = (Gold[z] > 0) ? add[z] / Gold[z] : 0;
+                    memcpy(gt, add, sizeof(double) * M);
+                }
+                olat_prop1(L, add, Gc, SLICE(sp));
+            } else {
+                olat_prop1(L, SLICE(sp - 1), Gc, SLICE(sp));
+            }
+            Gold = Gc;
+        }
+    }
+    sp = NS;
+    double nr = 1;
+    for (int i = 0; i < G; i++) {
+        int rep = o->gen_rep[i];
+        for (int j = 1; j <= o->gen_len[i]; j++) {
+            int sg = SEGAT(i, j);
+            const double *Gc = s->swf + (size_t)sg * M;
+            if (sp == NS) memcpy(Ginv, Gc, sizeof(double) * M);
+            else { olat_prop1(L, Ginv, Gc, tmp); memcpy(Ginv, tmp, sizeof(double) * M); }
+            double *phi = o->phi + (size_t)sg * M;
+            if (j == 1)
+                for (int k = 1; k <= rep - 1; k++) {
+                    for (int z = 0; z < M; z++) add[z] = 0 + Ginv[z] * SLICE(sp)[z];
+                    for (int z = 0; z < M; z++) Ginv[z] = (Gc[z] > 0) ? add[z] / Gc[z] : 0;
+                }
+            for (int z = 0; z < M; z++) Ginv[z] *= nr;
+            for (int z = 0; z < M; z++) phi[z] += Ginv[z] * SLICE(sp)[z];
+            double inv = 1.0 / nr;
+            for (int z = 0; z < M; z++) Ginv[z] *= inv;
+            if (j == 1) nr *= rep;
+            sp--;
+        }
+    }
+    #undef SEGAT
+    #undef SLICE
+    o->lngn = olat_lngn(L, Ginv);
+    for (int a = 0; a < o->nseg_used; a++) {
+        double *phi = o->phi + (size_t)o->used[a] * M;
+        const double *G1 = s->swf + (size_t)o->used[a] * M;
+        for (int z = 0; z < M; z++) { if (G1[z] > 0) phi[z] /= G1[z]; else phi[z] = 0; }
+    }
+    double norm;
+    if (o->freedom == SFGPU_MOL_RESTRICTED) {
+        o->lnc = log(o->theta) - o->lngn - log(1.0 * N);
+        o->phibulk = o->theta / exp(o->lngn);
+        norm = (o->theta / N) / exp(o->lngn);
+    } else {
+        o->lnc = log(o->phibulk / N);
+        norm = o->phibulk / N;
+    }
+    for (int a = 0; a < o->nseg_used; a++) {
+        double *phi = o->phi + (size_t)o->used[a] * M;
+        for (int z = 0; z < M; z++) phi[z] *= norm;
+    }
+    free(Gi); free(Ginv); free(tmp); free(add); free(gt);
+}
+
 static void molecule_phi(orc_system *s, omol *o) {
     if (s->L.logmode) { molecule_phi_log(s, o); return; }
+    if (o->ngen) { for (int a = 0; a < o->nseg_used; a++) memset(o->phi + (size_t)o->used[a] * s->L.M, 0, sizeof(double) * s->L.M);
+                   molecule_phi_dend(s, o); return; }
     olat *L = &s->L;
     int M = L->M, N = o->N, K = L->K;
     size_t KM = (size_t)K * M;

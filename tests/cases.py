@@ -62,6 +62,33 @@ def _colloid3d(periodic=False):
     return SystemSpec(lat, segs, chi, mols)
 
 
+def _dendrimer(gradients):
+    """A two-generation dendrimer @dend(2, (A)3, 3, (B)2(A)1, 2) (N = 22)
+    adsorbing on a surface (1D, 2D) or free in a periodic/mirror box (3D),
+    with a free linear chain and a solvent."""
+    if gradients == 1:
+        lat = Lattice(1, [24, 0, 0], [BOUND_SURFACE, 0, 0], [BOUND_MIRROR1, 0, 0], lam=1 / 6)
+    elif gradients == 2:
+        lat = Lattice(2, [12, 9, 0], [BOUND_SURFACE, BOUND_MIRROR1, 0], [BOUND_MIRROR2, BOUND_MIRROR1, 0], lam=0.2)
+    else:
+        lat = Lattice(3, [6, 5, 7], [BOUND_MIRROR1, BOUND_PERIODIC, BOUND_MIRROR2],
+                      [BOUND_MIRROR2, BOUND_PERIODIC, BOUND_MIRROR1])
+    mask = np.zeros(lat.shape)
+    if gradients < 3:
+        mask[0] = 1.0
+    else:
+        mask[2:4, 2:4, 3:5] = 1.0
+    segs = [Segment("S", SEG_FROZEN, mask.reshape(-1)), Segment("A"), Segment("B"), Segment("W")]
+    chi = np.zeros((4, 4))
+    chi[0, 1] = chi[1, 0] = -1.2
+    chi[1, 3] = chi[3, 1] = 0.5
+    chi[2, 3] = chi[3, 2] = -0.3
+    d = Molecule("dend", [(1, 3), (2, 2), (1, 1)], MOL_RESTRICTED if gradients != 3 else MOL_FREE,
+                 theta=1.5, phibulk=0.01, generations=[(1, 3), (2, 2)])
+    return SystemSpec(lat, segs, chi, [d, Molecule("B6", [(2, 6)], MOL_FREE, phibulk=0.02),
+                                       Molecule("W", [(3, 1)], MOL_SOLVENT)])
+
+
 # stencils contact weights: centre, face, edge, corner (0.1 + 6*0.08 + 12*0.02 + 8*0.0225 = 1)
 STENCILS = (0.1, 0.08, 0.02, 0.0225)
 
@@ -216,6 +243,9 @@ CASES = {
     "3d_hex_mirror": lambda: _typed(_colloid3d(), LATTICE_HEX),
     "3d_stencils_colloid": lambda: _typed(_colloid3d(), LATTICE_STENCILS, STENCILS),
     "3d_stencils_melt": lambda: _typed(configs.melt3d(n=7, nA=5, nB=6)[0], LATTICE_STENCILS, STENCILS),
+    "1d_dendrimer": lambda: _dendrimer(1),
+    "2d_dendrimer": lambda: _dendrimer(2),
+    "3d_dendrimer": lambda: _dendrimer(3),
     "3d_2nd_fcc_brush": lambda: _typed(configs.brush3d(n=6, N=15, sigma=0.2, S=0.5)[0], LATTICE_FCC),
     "1d_cylinder": _cyl1d_micelle,
     "1d_sphere_colloid": _sphere1d_colloid,
@@ -228,8 +258,9 @@ CASES = {
 }
 
 # cases whose derivatives (forward and reverse mode) are implemented: not the
-# lumped second-order lattices nor the 3D lattice types other than standard
-NOT_DIFFERENTIABLE = ("lumped", "fcc", "hex", "stencils")
+# lumped second-order lattices, the 3D lattice types other than standard,
+# nor dendrimers
+NOT_DIFFERENTIABLE = ("lumped", "fcc", "hex", "stencils", "dendrimer")
 DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFERENTIABLE))
 
 

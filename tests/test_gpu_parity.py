@@ -300,3 +300,30 @@ def test_lattice_types_outside_derivatives_and_batch(gpu_lib):
         BatchSolver([spec], m=5, eta=0.1)
     assert e.value.code == 7
     assert np.all(np.isfinite(sys_.residual(x)))
+
+
+@pytest.mark.parametrize("case", ["1d_dendrimer", "2d_dendrimer", "3d_dendrimer"])
+def test_dendrimer_converged_parity(gpu_lib, case):
+    """Symmetric dendrimers (SF_Dend1stO) converged by the device Pure_DIIS and
+    by the oracle's; the batched kernel and the derivatives report
+    SFGPU_ERR_UNSUPPORTED for them."""
+    from field_b200._native import SfgpuError
+    from field_b200.batch import BatchSolver
+    spec = CASES[case]()
+    sys_ = System(spec)
+    o = Oracle(spec)
+    x0 = np.zeros(spec.n_itvar())
+    rg = sys_.solve(x0, tol=1e-10, maxit=4000, m=8, eta=0.3)
+    xc, rc, it, err = o.solve_diis(x0, tol=1e-10, maxit=4000, m=8, eta=0.3)
+    assert rg.converged and rc == 0, (rg.converged, rc, err)
+    sys_.residual(rg.x)
+    o.residual(xc)
+    for i in range(len(spec.segments)):
+        np.testing.assert_allclose(sys_.phi(i), o.phi(i), rtol=1e-9, atol=1e-12)
+    assert abs(sys_.free_energy() - o.free_energy()) <= 1e-9 * max(1.0, abs(o.free_energy()))
+    with pytest.raises(SfgpuError) as e:
+        sys_.vjp(rg.x, rg.x)
+    assert e.value.code == 7
+    with pytest.raises(SfgpuError) as e:
+        BatchSolver([spec], m=5, eta=0.1)
+    assert e.value.code == 7
