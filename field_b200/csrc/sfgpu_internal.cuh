@@ -39,6 +39,8 @@ struct DLat {
     // 27-site cube (centre, face, edge, corner) for STANDARD, STENCILS, FCC
     int ltype;
     double sl[4];
+    // 3D second order: nonzero inside 'lat : stiff_range' (M values), or null
+    const double *stiff;
 };
 
 struct ChiTable {              // passed by value: small interaction tables

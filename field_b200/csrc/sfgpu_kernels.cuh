@@ -213,9 +213,19 @@ static __global__ void step2(DLat L, const double *__restrict__ gin, const doubl
 __device__ __forceinline__ bool is_mirror(int bc) {
     return bc == SFGPU_BOUND_MIRROR1 || bc == SFGPU_BOUND_MIRROR2;
 }
+// wmode: STEP2_PLAIN weights S and (1-S)/4 (PropagateF/B(..., S),
+// Lat3D2ndO.cpp:65-152, :597-678); STEP2_STIFF the stiff_range steps
+// (:155-247, :680-764): per site S inside the range and 0.2 outside, the
+// weight taken at the unshifted index of the reference's array operation --
+// the source site for the +x/+y/+z components forward and for reads from the
+// lower neighbour backward, the target site otherwise -- and multiplied
+// after G; STEP2_ISO the isotropic steps with G/6 for all six components
+// (:250-344, :765-850), whose forward -y component reads +z twice and -y
+// never (Lat3D2ndO.cpp:308-313).
+enum { STEP2_PLAIN = 0, STEP2_STIFF = 1, STEP2_ISO = 2 };
 static __global__ void step2_rows(DLat L, const double *__restrict__ gin, const double *__restrict__ G, double S,
                                   double *__restrict__ gout, const double *__restrict__ other,
-                                  double *__restrict__ phi, int mode, int backward) {
+                                  double *__restrict__ phi, int mode, int backward, int wmode = STEP2_PLAIN) {
     const int M = L.M;
     const double Lw = (1.0 - S) / 4.0;
     const int nx = L.Md[0] - 2, ny = L.Md[1] - 2;
@@ -232,7 +242,74 @@ static __global__ void step2_rows(DLat L, const double *__restrict__ gin, const 
         const double g = G[t];
         const double gS = g * S, gL = g * Lw;
         double out[6];
-        if (!backward) {
+        if (wmode != STEP2_PLAIN) {
+            const int raw[6] = {L.st[0], L.st[1], 1, 1, L.st[1], L.st[0]};   // axis stride by component
+            const double gI = g * (1.0 / 6.0);
+            auto ps_at = [&](int i) { return (L.stiff[i] != 0) ? S : 0.2; };
+            if (!backward) {
+                const int dir_of[6] = {0, 2, 4, 5, 3, 1};
+#pragma unroll
+                for (int kk = 0; kk < 6; kk++) {
+                    const int dd = dir_of[kk];
+                    const int src = t + off[dd];
+                    const int axis = dd >> 1;
+                    const bool sflag = sw[dd];
+                    auto comp = [&](int kp) {
+                        int c = kp;
+                        if (sflag) {
+                            if (axis == 0 && (kp == 0 || kp == 5)) c = 5 - kp;
+                            if (axis == 1 && (kp == 1 || kp == 4)) c = 5 - kp;
+                            if (axis == 2 && (kp == 2 || kp == 3)) c = 5 - kp;
+                        }
+                        return gin[(size_t)c * M + src];
+                    };
+                    double acc;
+                    if (wmode == STEP2_ISO) {
+                        const int seq4[6] = {0, 2, 2, 3, 4, 5};
+                        acc = comp(kk == 4 ? seq4[0] : 0) * gI;
+                        for (int q = 1; q < 6; q++) acc += comp(kk == 4 ? seq4[q] : q) * gI;
+                    } else {
+                        const int pi = (kk < 3) ? t - raw[kk] : t;
+                        const double ps = ps_at(pi), pl = (1.0 - ps) / 4.0;
+                        bool first = true;
+                        acc = 0;
+                        for (int kp = 0; kp < 6; kp++) {
+                            if (kp == 5 - kk) continue;
+                            const double v = comp(kp) * g * (kp == kk ? ps : pl);
+                            if (first) { acc = v; first = false; } else acc += v;
+                        }
+                    }
+                    out[kk] = acc;
+                }
+            } else {
+                const int dir_of[6] = {1, 3, 5, 4, 2, 0};
+                double v[6];
+#pragma unroll
+                for (int kk = 0; kk < 6; kk++) {
+                    const int dd = dir_of[kk];
+                    const int c = sw[dd] ? 5 - kk : kk;
+                    v[kk] = gin[(size_t)c * M + t + off[dd]];
+                }
+#pragma unroll
+                for (int kq = 0; kq < 6; kq++) {
+                    double acc = 0;
+                    bool first = true;
+                    for (int kp = 5; kp >= 0; kp--) {
+                        double w;
+                        if (wmode == STEP2_ISO) {
+                            w = v[kp] * gI;
+                        } else {
+                            if (kp == 5 - kq) continue;
+                            const int pi = (kp >= 3) ? t - raw[kp] : t;
+                            const double ps = ps_at(pi), pl = (1.0 - ps) / 4.0;
+                            w = v[kp] * g * (kp == kq ? ps : pl);
+                        }
+                        if (first) { acc = w; first = false; } else acc += w;
+                    }
+                    out[kq] = acc;
+                }
+            }
+        } else if (!backward) {
             // source of component kk is t - e_kk: kk=0 -> -x, 5 -> +x, 1 -> -y, 4 -> +y, 2 -> -z, 3 -> +z
             const int dir_of[6] = {0, 2, 4, 5, 3, 1};
 #pragma unroll

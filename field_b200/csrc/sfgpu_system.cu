@@ -133,6 +133,14 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
     }
     L.K = (L.order == 2) ? (L.grad == 1 ? 3 : (L.grad == 2 ? 5 : 6)) : 1;
     L.M = L.Md[0] * L.Md[1] * L.Md[2];
+    // lat : stiff_range (Lat3D.cpp:265-268): read by the 3D lattices, used by
+    // the second-order copolymers (SF_MolList2ndO.cpp:22-47)
+    H->stiff.clear();
+    L.stiff = nullptr;
+    if (d->stiff_range) {
+        if (L.grad != 3) return fail(SFGPU_ERR_INVALID, "stiff_range is a 3D lattice parameter");
+        if (L.order == 2) H->stiff.assign(d->stiff_range, d->stiff_range + L.M);
+    }
     if (L.grad == 1) { L.st[0] = 1; L.st[1] = 0; L.st[2] = 0; }
     else if (L.grad == 2) { L.st[0] = L.Md[1]; L.st[1] = 1; L.st[2] = 0; }
     else { L.st[0] = L.Md[1] * L.Md[2]; L.st[1] = L.Md[2]; L.st[2] = 1; }
@@ -458,6 +466,13 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     SFGPU_CUDA_TRY(cudaMemcpy(d_lamc_p, tcp.data(), sizeof(double) * L.Md[0], cudaMemcpyHostToDevice));
     L.lamc_m = d_lamc_m; L.lamc_p = d_lamc_p;
     if ((rc = alloc_d(&d_wgn, M)) || (rc = alloc_d(&d_wf, M)) || (rc = alloc_d(&d_sb, M))) return rc;
+    if (!H.stiff.empty()) {
+        for (auto &o : mols)
+            if (o.type == 1) return fail(SFGPU_ERR_UNSUPPORTED, "a stiff range with homopolymers (SFbox: only copolymers)");
+        if ((rc = alloc_d(&d_stiff, M))) return rc;
+        SFGPU_CUDA_TRY(cudaMemcpy(d_stiff, H.stiff.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+        L.stiff = d_stiff;
+    }
     SFGPU_CUDA_TRY(cudaMemcpy(d_sb, H.sb.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
     SFGPU_CUDA_TRY(cudaMemcpy(d_wgn, H.w_gn.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
     SFGPU_CUDA_TRY(cudaMemcpy(d_wf, H.w_f.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
@@ -813,7 +828,15 @@ int sfgpu_system::molecule_phi(int m) {
         int sg = o.seg[t];
         if (K == 1)
             launch_step1(d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
-        else if (K == 6)
+        else if (K == 6 && L.stiff) {
+            // SF_Copol2ndO_stiff_range::Matrix1 (SF_Copol2ndO_stiff_range.cpp:211-217):
+            // step s (1-based) takes Pf(s-1, s+1); the last one is isotropic
+            const bool last = (t == N - 1);
+            const double Sv = last ? 0.2 : pf[o.seg[t - 1] * nseg + o.seg[t + 1]];
+            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], Sv,
+                                       d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0,
+                                       last ? STEP2_ISO : STEP2_STIFF);
+        } else if (K == 6)
             step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
                                        d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0);
         else
@@ -834,7 +857,14 @@ int sfgpu_system::molecule_phi(int m) {
         int sg = o.seg[t];
         if (K == 1)
             launch_step1(cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
-        else if (K == 6)
+        else if (K == 6 && L.stiff) {
+            // backward step s (1-based) takes Pf(s, s+2); the first one
+            // (s = N-1) is isotropic (SF_Copol2ndO_stiff_range.cpp:229-234)
+            const bool first = (t == N - 2);
+            const double Sv = first ? 0.2 : pf[sg * nseg + o.seg[t + 2]];
+            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], Sv, ginv, d_gi + (size_t)t * KM, o.d_phi[sg],
+                                       COMP_ACC, 1, first ? STEP2_ISO : STEP2_STIFF);
+        } else if (K == 6)
             step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv,
                                        d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC, 1);
         else
@@ -862,6 +892,7 @@ int sfgpu_system::molecule_phi(int m) {
 // segment type mphi profiles, filled by the residual evaluations that follow.
 int sfgpu_system::set_orientation(int enable) {
     if (K == 1) return fail(SFGPU_ERR_UNSUPPORTED, "bond orientation needs a second-order lattice");
+    if (H.L.stiff) return fail(SFGPU_ERR_UNSUPPORTED, "bond orientation with a stiff range");
     if (enable && !d_ori_sum) {
         int rc = alloc_d(&d_ori_sum, M);
         if (rc) return rc;

@@ -7,6 +7,7 @@ struct HostLat {
     DLat L;
     std::vector<double> lam_m, lam_p, lamc_m, lamc_p, Lx, w_gn, w_f;
     std::vector<double> sb;   // SubtractBoundaries factors (0 removed, 1/2 mirror2 layers)
+    std::vector<double> stiff; // 'lat : stiff_range' mask (3D second order), empty if none
 };
 int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H);
 
@@ -38,7 +39,7 @@ struct sfgpu_system {
     ChiTable ct;
     // device buffers
     double *d_lam_m = nullptr, *d_lam_p = nullptr, *d_lamc_m = nullptr, *d_lamc_p = nullptr;
-    double *d_wgn = nullptr, *d_wf = nullptr, *d_sb = nullptr;
+    double *d_wgn = nullptr, *d_wf = nullptr, *d_sb = nullptr, *d_stiff = nullptr;
     int *d_jmap = nullptr, *d_sites = nullptr;
     std::vector<double *> d_range, d_gfull, d_gseg, d_phi;
     double *d_gi = nullptr, *d_ginv[2] = {nullptr, nullptr};

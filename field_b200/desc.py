@@ -28,7 +28,8 @@ class LatticeDesc(C.Structure):
                 ("n_layers", C.c_int * 3), ("bound_lo", C.c_int * 3), ("bound_hi", C.c_int * 3),
                 ("lam", C.c_double), ("lambda_chi", C.c_double),
                 ("layer_adjustment", C.c_double), ("dimensions", C.c_double),
-                ("offset_first_layer", C.c_double), ("lattice_type", C.c_int),
+                ("offset_first_layer", C.c_double), ("stiff_range", C.POINTER(C.c_double)),
+                ("lattice_type", C.c_int),
                 ("lambda_3d", C.c_double * 4)]
 
 
@@ -73,6 +74,7 @@ class Lattice:
     offset_first_layer: float = 0.0
     lattice_type: int = LATTICE_STANDARD
     lambda_3d: Sequence[float] = (0.0, 0.0, 0.0, 0.0)
+    stiff_range: Optional[np.ndarray] = None     # M values, 1 inside 'lat : stiff_range'
 
     @property
     def shape(self):
@@ -104,6 +106,13 @@ class Lattice:
         d.lattice_type = int(self.lattice_type)
         for k in range(4):
             d.lambda_3d[k] = float(self.lambda_3d[k])
+        if self.stiff_range is not None:
+            self._stiff = np.ascontiguousarray(self.stiff_range, dtype=np.float64).reshape(-1)
+            if self._stiff.size != self.M:
+                raise ValueError(f"stiff_range has {self._stiff.size} values, lattice has {self.M}")
+            d.stiff_range = dptr(self._stiff)
+        else:
+            d.stiff_range = C.POINTER(C.c_double)()
         return d
 
 

@@ -221,6 +221,12 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
                   layer_adjustment=ladj,
                   dimensions=float(_get(calc, "lat", ln, "dimensions", "3")),
                   offset_first_layer=off, lattice_type=ltypes[ltype], lambda_3d=lam3)
+    # lat : stiff_range (Lat3D.cpp:265-268): second-order copolymers stiffen there
+    sr = _get(calc, "lat", ln, "stiff_range", None)
+    if sr is not None:
+        if g != 3:
+            raise ValueError(f"lat : {ln} : stiff_range is a 3D lattice parameter")
+        lat.stiff_range = _range_mask(lat, sr)
     # segments
     seg_names = _names(calc, "mon")
     segs: List[Segment] = []

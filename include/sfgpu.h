@@ -110,6 +110,13 @@ typedef struct {
     double layer_adjustment;   /* 1D only (Lat1DFlat.cpp:139, Lat1DCylinder.cpp:43); 1 = none */
     double dimensions;         /* curved: spatial dimensions D (default 3) */
     double offset_first_layer; /* curved: offset_first_layer(_x) (default 0) */
+    const double *stiff_range; /* 3D second order: M values, nonzero inside 'lat : stiff_range'
+                                  (Lat3D.cpp:265-268), or NULL.  Copolymers then
+                                  take SF_Copol2ndO_stiff_range's steps: persistence
+                                  S inside the range and 0.2 outside (Lat3D2ndO.cpp:
+                                  155-247, 680-764), isotropic 1/6 steps at the
+                                  chain's last forward and first backward step
+                                  (:250-344, :765-850); homopolymers are refused */
     int    lattice_type;       /* SFGPU_LATTICE_* (3 gradients; 0 otherwise) */
     double lambda_3d[4];       /* SFGPU_LATTICE_STENCILS: lambda0..lambda3, each in
                                   [0, 0.5], l0 + 6 l1 + 12 l2 + 8 l3 = 1 within

@@ -52,6 +52,7 @@ def lib():
         l.orc_propagate.argtypes = [vp, dp, dp, dp, C.c_double, C.c_int]
         l.orc_side.argtypes = [vp, dp, dp]
         l.orc_lat_lngn.argtypes = [vp, dp, dp]
+        l.orc_propagate_stiff.argtypes = [vp, dp, dp, dp, C.c_double, C.c_int, C.c_int]
         l.orc_site_weights.argtypes = [vp, dp]
         l.orc_set_boundaries.argtypes = [vp, dp]
         l.orc_solve_diis.argtypes = [vp, dp, C.c_double, C.c_int, C.c_int, C.c_double, ip, dp]
@@ -136,6 +137,16 @@ class Oracle:
         g = np.ascontiguousarray(g, dtype=np.float64)
         out = np.zeros(self.K * self.M)
         lib().orc_propagate(self.h, _d(gin), _d(g), _d(out), S, int(backward))
+        return out
+
+    def propagate_stiff(self, gin, g, S, backward=False, iso=False):
+        """One stiff_range (or isotropic) 3D second-order step."""
+        gin = np.ascontiguousarray(gin, dtype=np.float64)
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        out = np.zeros(6 * self.M)
+        rc = lib().orc_propagate_stiff(self.h, _d(gin), _d(g), _d(out), S, int(backward), int(iso))
+        if rc:
+            raise ValueError(f"orc_propagate_stiff failed with status {rc}")
         return out
 
     def lat_lngn(self, g):

@@ -48,6 +48,7 @@ typedef struct {
     int ltype;         /* 3D lattice type, SFGPU_LATTICE_* */
     double sl[4];      /* contact weights of the 27-site cube: centre, face, edge, corner */
     /* overflow protection (*1stOS lattices): constants of the log-space steps */
+    double *stiff;     /* 'lat : stiff_range' mask (3D second order), NULL if none */
     int logmode;
     double LogL0, LogL1, LogL1L0;          /* flat 1D / 2D */
     double *logl0x, *loglmx, *loglpx;      /* 2D cylinder, by x (0 where lambda <= 0) */
@@ -173,6 +174,14 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
     }
     L->K = (L->order == 2) ? (L->grad == 1 ? 3 : (L->grad == 2 ? 5 : 6)) : 1;
     L->M = L->Md[0] * L->Md[1] * L->Md[2];
+    /* lat : stiff_range, Lat3D.cpp:265-268 (used by second-order copolymers) */
+    if (d->stiff_range) {
+        if (L->grad != 3) return SFGPU_ERR_INVALID;
+        if (L->order == 2) {
+            L->stiff = malloc(sizeof(double) * L->M);
+            memcpy(L->stiff, d->stiff_range, sizeof(double) * L->M);
+        }
+    }
     L->st[2] = 1; L->st[1] = L->Md[2]; L->st[0] = L->Md[1] * L->Md[2];
     if (L->grad == 1) { L->st[0] = 1; L->st[1] = L->st[2] = 0; }
     if (L->grad == 2) { L->st[0] = L->Md[1]; L->st[1] = 1; L->st[2] = 0; }
@@ -301,7 +310,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
 
 static void olat_free(olat *L) {
     free(L->lam_m); free(L->lam_p); free(L->lamc_m); free(L->lamc_p); free(L->Lx); free(L->w_gn); free(L->w_f); free(L->sb);
-    free(L->logl0x); free(L->loglmx); free(L->loglpx);
+    free(L->logl0x); free(L->loglmx); free(L->loglpx); free(L->stiff);
 }
 
 /* one first-order step gout = G * stencil(gin); gin must carry valid
@@ -384,6 +393,60 @@ static void olat_prop2(const olat *L, const double *gin, const double *G, double
                 for (int kp = 5; kp >= 0; kp--) {
                     if (kp == OPP[k]) continue;
                     double t = gin[kp * M + z + e[kp]] * (kp == k ? gS : gL);
+                    if (first) { acc = t; first = 0; } else acc += t;
+                }
+            }
+            gout[k * M + z] = acc;
+        }
+    }
+    olat_set_boundaries6(L, gout);
+}
+
+/* the stiff_range and isotropic 3D second-order steps of
+   SF_Copol2ndO_stiff_range: PropagateF/B(..., S, stiff) (Lat3D2ndO.cpp:155-247,
+   :680-764) weigh with ps = S inside the range and 0.2 outside, pl = (1-ps)/4,
+   taken at the unshifted index of each array operation (the source site for
+   the + components forward and for reads of the - components backward, the
+   target site otherwise), as (Gi * G) * p; PropagateF/B(Gi, G) (:250-344,
+   :765-850) weigh all six components with G/6, the forward -y component
+   reading +z twice and -y not at all (:308-313). */
+static void olat_prop2_var(const olat *L, const double *gin, const double *G, double S,
+                           double *gout, int backward, int iso) {
+    int M = L->M, jx = L->st[0], jy = L->st[1];
+    int e[6] = {jx, jy, 1, -1, -jy, -jx};
+    static const int seq[6] = {0, 1, 2, 3, 4, 5}, seq4[6] = {0, 2, 2, 3, 4, 5};
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(L, z)) continue;
+        double gI = G[z] * (1.0 / 6.0);
+        for (int k = 0; k < 6; k++) {
+            double acc = 0; int first = 1;
+            if (!backward) {
+                int src = z - e[k];
+                if (iso) {
+                    const int *q = (k == 4) ? seq4 : seq;
+                    for (int i = 0; i < 6; i++) {
+                        double t = gin[q[i] * M + src] * gI;
+                        if (first) { acc = t; first = 0; } else acc += t;
+                    }
+                } else {
+                    int pi = (k < 3) ? src : z;
+                    double ps = (L->stiff[pi] != 0) ? S : 0.2, pl = (1.0 - ps) / 4.0;
+                    for (int kp = 0; kp < 6; kp++) {
+                        if (kp == OPP[k]) continue;
+                        double t = gin[kp * M + src] * G[z] * (kp == k ? ps : pl);
+                        if (first) { acc = t; first = 0; } else acc += t;
+                    }
+                }
+            } else {
+                for (int kp = 5; kp >= 0; kp--) {
+                    double t;
+                    if (iso) t = gin[kp * M + z + e[kp]] * gI;
+                    else {
+                        if (kp == OPP[k]) continue;
+                        int pi = (kp >= 3) ? z + e[kp] : z;
+                        double ps = (L->stiff[pi] != 0) ? S : 0.2, pl = (1.0 - ps) / 4.0;
+                        t = gin[kp * M + z + e[kp]] * G[z] * (kp == k ? ps : pl);
+                    }
                     if (first) { acc = t; first = 0; } else acc += t;
                 }
             }
@@ -780,6 +843,9 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
         o->ori = calloc((size_t)ns * 3 * M, sizeof(double));
     }
     if (s->solvent < 0) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+    if (s->L.stiff)   /* SF_MolList2ndO.cpp:39: only copolymers take a stiff range */
+        for (int m = 0; m < s->nmol; m++)
+            if (s->mol[m].type == 1) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
 
     /* liquid states and their classes, SF_Solve.cpp:37-86 */
     s->stateQ = calloc(ns, sizeof(int));
@@ -1404,7 +1470,14 @@ static void molecule_phi(orc_system *s, omol *o) {
     for (int t = 1; t < N; t++) {
         int sg = o->seg[t];
         double S = s->pf[o->seg[t - 1] * s->nseg + sg];
-        propagate_any(s, Gi + (size_t)(t - 1) * KM, s->swf + (size_t)sg * M, S, Gi + (size_t)t * KM, 0);
+        if (L->stiff && K == 6) {
+            /* SF_Copol2ndO_stiff_range::Matrix1, SF_Copol2ndO_stiff_range.cpp:211-217:
+               Pf(s-1, s+1) (1-based s), the last step isotropic */
+            int last = (t == N - 1);
+            S = last ? 0.2 : s->pf[o->seg[t - 1] * s->nseg + o->seg[t + 1]];
+            olat_prop2_var(L, Gi + (size_t)(t - 1) * KM, s->swf + (size_t)sg * M, S, Gi + (size_t)t * KM, 0, last);
+        } else
+            propagate_any(s, Gi + (size_t)(t - 1) * KM, s->swf + (size_t)sg * M, S, Gi + (size_t)t * KM, 0);
     }
     const double *GN = s->swf + (size_t)o->seg[N - 1] * M;
     for (int k = 0; k < K; k++) memcpy(Ginv + (size_t)k * M, GN, sizeof(double) * M);
@@ -1427,7 +1500,14 @@ static void molecule_phi(orc_system *s, omol *o) {
     for (int t = N - 2; t >= 0; t--) {
         int sg = o->seg[t];
         double S = s->pf[sg * s->nseg + o->seg[t + 1]];
-        propagate_any(s, Ginv, s->swf + (size_t)sg * M, S, tmp, 1);
+        if (L->stiff && K == 6) {
+            /* backward: Pf(s, s+2), the first step (s = N-1) isotropic,
+               SF_Copol2ndO_stiff_range.cpp:229-234 */
+            int firstb = (t == N - 2);
+            S = firstb ? 0.2 : s->pf[sg * s->nseg + o->seg[t + 2]];
+            olat_prop2_var(L, Ginv, s->swf + (size_t)sg * M, S, tmp, 1, firstb);
+        } else
+            propagate_any(s, Ginv, s->swf + (size_t)sg * M, S, tmp, 1);
         memcpy(Ginv, tmp, sizeof(double) * KM);
         if (K > 1) orient_acc(L, Ginv, Gi + (size_t)t * KM, o->ori + (size_t)sg * 3 * M);
         double *phi = o->phi + (size_t)sg * M;
@@ -1696,6 +1776,20 @@ int orc_propagate(const orc_system *s, const double *gin, const double *g, doubl
     free(tmp);
     return SFGPU_OK;
 }
+/* one stiff_range (iso = 0) or isotropic (iso = 1) 3D second-order step,
+   6*M values, with the lattice's stiff_range mask */
+int orc_propagate_stiff(const orc_system *s, const double *gin, const double *g, double *gout, double S,
+                        int backward, int iso) {
+    int M = s->L.M;
+    if (s->L.K != 6 || (!iso && !s->L.stiff)) return SFGPU_ERR_INVALID;
+    double *tmp = malloc(sizeof(double) * 6 * M);
+    memcpy(tmp, gin, sizeof(double) * 6 * M);
+    olat_set_boundaries6(&s->L, tmp);
+    olat_prop2_var(&s->L, tmp, g, S, gout, backward, iso);
+    free(tmp);
+    return SFGPU_OK;
+}
+
 /* lnGN of a propagator at the lattice level: ComputeLnGN (on logarithms
    with overflow protection) */
 int orc_lat_lngn(const orc_system *s, const double *g, double *lngn) {

@@ -40,6 +40,9 @@ double orc_free_energy(orc_system *s);                                 /* SF_Mol
 
 /* one propagator step, Gout = G * stencil(Gin) with SFbox boundaries
    (1st order: M values; 2nd order: 6*M values, forward or backward) */
+/* stiff_range (iso 0) or isotropic (iso 1) 3D second-order step, 6*M values */
+int    orc_propagate_stiff(const orc_system *s, const double *gin, const double *g, double *gout, double S,
+                           int backward, int iso);
 /* ComputeLnGN of a propagator (on logarithms with overflow protection) */
 int    orc_lat_lngn(const orc_system *s, const double *g, double *lngn);
 int    orc_propagate(const orc_system *s, const double *gin, const double *g,

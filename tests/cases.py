@@ -89,6 +89,28 @@ def _dendrimer(gradients):
                                        Molecule("W", [(3, 1)], MOL_SOLVENT)])
 
 
+def _stiff_copolymer():
+    """A 3D second-order lattice with 'lat : stiff_range' over the lower half
+    in z (SF_Copol2ndO_stiff_range), a triblock with its own persistence
+    factors, a frozen particle and a solvent."""
+    lat = Lattice(3, [6, 5, 7], [BOUND_MIRROR1, BOUND_PERIODIC, BOUND_MIRROR2],
+                  [BOUND_MIRROR2, BOUND_PERIODIC, BOUND_MIRROR1], order=2)
+    mask = np.zeros(lat.shape)
+    mask[:, :, :4] = 1.0
+    lat.stiff_range = mask.reshape(-1)
+    part = np.zeros(lat.shape)
+    part[3:5, 2:4, 5:7] = 1.0
+    segs = [Segment("S", SEG_FROZEN, part.reshape(-1)), Segment("A"), Segment("B"), Segment("W")]
+    chi = np.zeros((4, 4))
+    chi[0, 1] = chi[1, 0] = -1.0
+    chi[1, 3] = chi[3, 1] = 0.6
+    pf = np.full((4, 4), 0.2)
+    pf[1, 2] = pf[2, 1] = 0.5
+    pf[1, 1] = 0.4
+    mols = [Molecule("ABA", [(1, 4), (2, 3), (1, 3)], MOL_FREE, phibulk=0.03), Molecule("W", [(3, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols, pf=pf)
+
+
 # stencils contact weights: centre, face, edge, corner (0.1 + 6*0.08 + 12*0.02 + 8*0.0225 = 1)
 STENCILS = (0.1, 0.08, 0.02, 0.0225)
 
@@ -246,6 +268,7 @@ CASES = {
     "1d_dendrimer": lambda: _dendrimer(1),
     "2d_dendrimer": lambda: _dendrimer(2),
     "3d_dendrimer": lambda: _dendrimer(3),
+    "3d_2nd_stiff_copol": _stiff_copolymer,
     "3d_2nd_fcc_brush": lambda: _typed(configs.brush3d(n=6, N=15, sigma=0.2, S=0.5)[0], LATTICE_FCC),
     "1d_cylinder": _cyl1d_micelle,
     "1d_sphere_colloid": _sphere1d_colloid,
@@ -260,7 +283,7 @@ CASES = {
 # cases whose derivatives (forward and reverse mode) are implemented: not the
 # lumped second-order lattices, the 3D lattice types other than standard,
 # nor dendrimers
-NOT_DIFFERENTIABLE = ("lumped", "fcc", "hex", "stencils", "dendrimer")
+NOT_DIFFERENTIABLE = ("lumped", "fcc", "hex", "stencils", "dendrimer", "stiff")
 DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFERENTIABLE))
 
 

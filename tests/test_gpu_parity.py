@@ -264,7 +264,7 @@ def test_thermo(gpu_lib, case):
 
 
 @pytest.mark.parametrize("case", ["3d_fcc_colloid", "3d_hex_colloid", "3d_hex_mirror", "3d_stencils_colloid",
-                                  "3d_2nd_fcc_brush"])
+                                  "3d_2nd_fcc_brush", "3d_2nd_stiff_copol"])
 def test_lattice_types_converged_parity(gpu_lib, case):
     """FCC, HEX and stencils 3D lattices (and a second-order lattice with FCC
     contacts) converged by the device Pure_DIIS and by the oracle's."""
@@ -326,4 +326,24 @@ def test_dendrimer_converged_parity(gpu_lib, case):
     assert e.value.code == 7
     with pytest.raises(SfgpuError) as e:
         BatchSolver([spec], m=5, eta=0.1)
+    assert e.value.code == 7
+
+
+def test_stiff_range_refusals(gpu_lib):
+    """A stiff range takes copolymers only (SF_MolList2ndO.cpp:39-47); bond
+    orientation and derivatives are not built for it."""
+    from field_b200._native import SfgpuError
+    from field_b200.desc import Molecule, MOL_FREE
+    spec = CASES["3d_2nd_stiff_copol"]()
+    s = System(spec)
+    with pytest.raises(SfgpuError) as e:
+        s.set_bond_orientation(True)
+    assert e.value.code == 7
+    x = random_x(spec)
+    with pytest.raises(SfgpuError) as e:
+        s.jvp(x, x)
+    assert e.value.code == 7
+    spec.molecules[0] = Molecule("A9", [(1, 9)], MOL_FREE, phibulk=0.03)
+    with pytest.raises(SfgpuError) as e:
+        System(spec)
     assert e.value.code == 7
