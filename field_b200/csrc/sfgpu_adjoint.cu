@@ -180,7 +180,7 @@ int sfgpu_system::ensure_adjoint() {
     if (logmode) return fail_unsupported("derivatives with overflow protection");
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
-        if (o.dend) return fail_unsupported("derivatives of dendrimers");
+        if (o.dend || o.force != 0) return fail_unsupported("derivatives of dendrimers and of the force ensemble");
     int rc = ensure_adjoint_misc();
     if (rc) return rc;
     if (!a_store) {

@@ -656,6 +656,56 @@ static __global__ void finalize_phi(int M, const double *__restrict__ G, double 
     }
 }
 
+// Constant-force steps (mol : force) of the first-order lattices, with the
+// weights the host computes as the reference does:
+//  1D flat   (Lat1DFlat1stO.cpp:116-130): g (b + a1 (a - b) + a2 (c - b)),
+//            a1 = l1 e^f / n, a2 = l1 e^-f / n, n = l1 (e^-f + e^f - 2) + 1
+//  1D curved (Lat1DCyl1stO.cpp:112-133): g (l-(z) a2 a + (1 - l+ - l-)/a3 b
+//            + l+(z) a1 c), a1 = e^-f / a3, a2 = e^f / a3, a3 = (4 + e^-f + e^f)/6
+//  2D cyl    (Lat2DCyl1stO.cpp:100-126): g (b + l-(x)(u - b) + l+(x)(d - b)
+//            + l1 (a a1 + c a2 - b - b)) / a3, a1 = e^f, a2 = e^-f,
+//            a3 = l1 (e^-f + e^f - 2) + 1, along y
+//  3D        (Lat3D1stO.cpp:94-130): (x-, x+, y-, y+ times g, z- g a1, z+ g a2) a3,
+//            a1 = e^f, a2 = e^-f, a3 = 1 / (4 + e^f + e^-f)
+struct ForceW { double a1, a2, a3; };
+__device__ __forceinline__ double force_row(const DLat &L, const RowInfo &R, const double *__restrict__ gin,
+                                            const double *__restrict__ G, int k, int nlast, const ForceW &w) {
+    const int d = L.grad - 1;
+    const int t = R.base + k;
+    const int km = (k == 1) ? L.map_lo[d] : k - 1;
+    const int kp = (k == nlast) ? L.map_hi[d] : k + 1;
+    const double g = G[t];
+    const double a = gin[R.base + km], b = gin[t], c = gin[R.base + kp];
+    if (L.grad == 1 && !L.cyl) return g * (b + w.a1 * (a - b) + w.a2 * (c - b));
+    if (L.grad == 1) {
+        const double f1z = L.lam_p[t] * w.a1, f_1z = L.lam_m[t] * w.a2;
+        const double f0z = (1 - L.lam_p[t] - L.lam_m[t]) / w.a3;
+        return g * (f_1z * a + f0z * b + f1z * c);
+    }
+    if (L.grad == 2)
+        return g * (b + L.lam_m[R.x] * (gin[t + R.up] - b) + L.lam_p[R.x] * (gin[t + R.dn] - b) +
+                    L.l1 * (a * w.a1 + c * w.a2 - b - b)) / w.a3;
+    double acc = gin[t + R.up] * g;
+    acc += gin[t + R.dn] * g;
+    acc += gin[t + R.up2] * g;
+    acc += gin[t + R.dn2] * g;
+    acc += a * g * w.a1;
+    acc += c * g * w.a2;
+    return acc * w.a3;
+}
+
+static __global__ void step1_force_rows(DLat L, ForceW w, const double *__restrict__ gin, const double *__restrict__ G,
+                                        double *__restrict__ gout, const double *__restrict__ other,
+                                        double *__restrict__ phi, int mode) {
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const int t = R.base + k;
+        const double out = force_row(L, R, gin, G, k, nlast, w);
+        gout[t] = out;
+        if (mode == COMP_ACC) phi[t] += out * other[t];
+    });
+}
+
 // Dendrimer branch points (SF_Dend1stO.cpp:199-214, :245-253): out = a b / G
 // where G > 0, else 0 -- ConnectG into a zero vector, then CorrectDoubleCountG
 static __global__ void dend_combine(int M, const double *__restrict__ a, const double *__restrict__ b,

@@ -392,6 +392,17 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
         o.freedom = md.freedom;
         o.phibulk = md.phibulk;
         o.theta = md.theta;
+        // mol : force: first-order copolymers on the lattices with a force
+        // step (Lat2DFlat1stO.cpp:115-117 and the homopolymer and dendrimer
+        // drivers stop with an error; the monomer has no step)
+        o.force = (o.type == 0) ? 0.0 : md.force;
+        if (o.force != 0) {
+            if (!(o.force >= -1000.0 && o.force <= 1000.0)) return fail(SFGPU_ERR_INVALID, "force must lie in [-1000, 1000]");
+            if (K != 1 || o.type != 2 || o.dend)
+                return fail(SFGPU_ERR_UNSUPPORTED, "the force ensemble takes first-order linear copolymers");
+            if (L.grad == 2 && !L.cyl) return fail(SFGPU_ERR_UNSUPPORTED, "no force ensemble on the 2D flat lattice");
+            if (L.ltype != SFGPU_LATTICE_STANDARD) return fail(SFGPU_ERR_UNSUPPORTED, "force ensemble on FCC, HEX or stencils lattices");
+        }
         if (o.freedom == SFGPU_MOL_SOLVENT) {
             if (solvent >= 0) return fail(SFGPU_ERR_INVALID, "more than one solvent molecule");
             solvent = m;
@@ -536,8 +547,10 @@ int sfgpu_system::setup_logspace() {
     const DLat &L = H.L;
     if (L.order != 1 || L.grad > 2)
         return fail(SFGPU_ERR_UNSUPPORTED, "overflow protection needs a first-order 1D or 2D lattice");
-    for (auto &o : mols)
+    for (auto &o : mols) {
         if (o.dend) return fail(SFGPU_ERR_UNSUPPORTED, "dendrimers with overflow protection");
+        if (o.force != 0) return fail(SFGPU_ERR_UNSUPPORTED, "the force ensemble with overflow protection");
+    }
     logmode = true;
     logc.lmax = log(DBL_MAX);
     logc.logcutoff = 100.0;
@@ -697,6 +710,32 @@ int sfgpu_system::molecule_phi_log(int m) {
     return SFGPU_OK;
 }
 
+// weights of a constant-force step with force f (see force_row)
+static ForceW force_weights(const DLat &L, double f) {
+    ForceW w;
+    const double l1 = L.l1;
+    if (L.grad == 1 && !L.cyl) {
+        const double norm = l1 * (exp(-f) + exp(f) - 2) + 1;
+        w.a2 = l1 * exp(-f) / norm;
+        w.a1 = l1 * exp(f) / norm;
+        w.a3 = norm;
+    } else if (L.grad == 1) {
+        double f_1 = exp(f), f1 = exp(-f);
+        const double fnorm = (4.0 + f1 + f_1) / 6.0;
+        w.a1 = f1 / fnorm;
+        w.a2 = f_1 / fnorm;
+        w.a3 = fnorm;
+    } else if (L.grad == 2) {
+        const double f_1 = exp(-f), f1 = exp(f);
+        w.a1 = f1; w.a2 = f_1;
+        w.a3 = l1 * (f_1 + f1 - 2) + 1;
+    } else {
+        w.a1 = exp(f); w.a2 = exp(-f);
+        w.a3 = 1.0 / (4.0 + exp(f) + exp(-f));
+    }
+    return w;
+}
+
 // SF_Dend1stO::Matrix1 (SF_Dend1stO.cpp:163-312): the propagator from the
 // ends inwards along one path from an end to the centre (nshort positions,
 // stored), the branch points combining f copies of the arriving propagator
@@ -826,7 +865,10 @@ int sfgpu_system::molecule_phi(int m) {
     if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, d_gi);
     for (int t = 1; t < N; t++) {
         int sg = o.seg[t];
-        if (K == 1)
+        if (K == 1 && o.force != 0)   // SF_Copol1stO.cpp:1207-1211: PropagateG(Gi, G, s, force)
+            step1_force_rows<<<grid_rows(L), kBlock, 0, s>>>(L, force_weights(L, o.force), d_gi + (size_t)(t - 1) * KM,
+                                                             d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
+        else if (K == 1)
             launch_step1(d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
         else if (K == 6 && L.stiff) {
             // SF_Copol2ndO_stiff_range::Matrix1 (SF_Copol2ndO_stiff_range.cpp:211-217):
@@ -855,7 +897,10 @@ int sfgpu_system::molecule_phi(int m) {
     std::swap(ginv, tmp);
     for (int t = N - 2; t >= 0; t--) {
         int sg = o.seg[t];
-        if (K == 1)
+        if (K == 1 && o.force != 0)   // backward steps with -force (SF_Copol1stO.cpp:1226-1230)
+            step1_force_rows<<<grid_rows(L), kBlock, 0, s>>>(L, force_weights(L, -o.force), cur, d_gseg[sg], ginv,
+                                                             d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
+        else if (K == 1)
             launch_step1(cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
         else if (K == 6 && L.stiff) {
             // backward step s (1-based) takes Pf(s, s+2); the first one

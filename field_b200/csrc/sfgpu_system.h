@@ -19,6 +19,7 @@ struct HMol {
     // segments (first = branch point) and functionality; nshort = positions
     // from the centre to an end
     int dend = 0, nshort = 0;
+    double force = 0;                 // mol : force (constant-force ensemble)
     std::vector<std::vector<int>> gen_seg;
     std::vector<int> gen_rep;
     std::vector<double *> d_phi;      // per segment (used ones)

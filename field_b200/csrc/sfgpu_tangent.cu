@@ -29,7 +29,7 @@ int sfgpu_system::ensure_tangent() {
     if (logmode) return fail_unsupported("derivatives with overflow protection");
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
-        if (o.dend) return fail_unsupported("derivatives of dendrimers");
+        if (o.dend || o.force != 0) return fail_unsupported("derivatives of dendrimers and of the force ensemble");
     if (t_ready) return SFGPU_OK;
     int rc;
     dgfull.assign(nseg, nullptr); dgseg.assign(nseg, nullptr); dphi.assign(nseg, nullptr);

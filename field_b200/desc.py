@@ -41,7 +41,8 @@ class MoleculeDesc(C.Structure):
     _fields_ = [("n_blocks", C.c_int), ("block_segment", C.POINTER(C.c_int)),
                 ("block_length", C.POINTER(C.c_int)), ("freedom", C.c_int),
                 ("phibulk", C.c_double), ("theta", C.c_double), ("n_generations", C.c_int),
-                ("generation_blocks", C.POINTER(C.c_int)), ("generation_repeat", C.POINTER(C.c_int))]
+                ("generation_blocks", C.POINTER(C.c_int)), ("generation_repeat", C.POINTER(C.c_int)),
+                ("force", C.c_double)]
 
 
 class SystemDesc(C.Structure):
@@ -133,6 +134,7 @@ class Molecule:
     # symmetric dendrimer: per generation (number of its blocks in `blocks`,
     # functionality f); None for a linear chain
     generations: Optional[List[tuple]] = None
+    force: float = 0.0                      # mol : force (constant-force ensemble)
 
     def generation_blocks(self) -> List[List[tuple]]:
         out, b = [], 0
@@ -212,6 +214,7 @@ class SystemSpec:
             mols[m].n_blocks = len(mol.blocks)
             mols[m].block_segment, mols[m].block_length = iptr(bs), iptr(bl)
             mols[m].freedom, mols[m].phibulk, mols[m].theta = mol.freedom, mol.phibulk, mol.theta
+            mols[m].force = float(mol.force)
             if mol.generations:
                 gb = np.array([g[0] for g in mol.generations], dtype=np.int32)
                 gr = np.array([g[1] for g in mol.generations], dtype=np.int32)

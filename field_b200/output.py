@@ -146,6 +146,7 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
         T("mol", mol.name, "composition", comp)
         T("mol", mol.name, "chainlength", N[m])
         R("mol", mol.name, "ln(G(N|1))", sc["lngn"])
+        R("mol", mol.name, "force", getattr(mol, "force", 0.0))
         R("mol", mol.name, "ln(norm_restricted)" if mol.freedom == MOL_RESTRICTED else "ln(norm_free)", sc["lnc"])
         P("mol", mol.name, "phi", phi)
     nname = _names(calc, "newton", "noname")

@@ -263,10 +263,13 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
             comp = parse_composition(ctext)
         blocks = [(seg_names.index(a), n_) for a, n_ in comp]
         length = Molecule(mn, blocks, generations=gens).N
+        force = float(_get(calc, "mol", mn, "force", "0"))
+        if not -1000.0 <= force <= 1000.0:   # SF_Molecule.cpp:42
+            raise ValueError(f"mol : {mn} : force must lie in [-1000, 1000]")
         fr = _get(calc, "mol", mn, "freedom", "free")
         if fr == "free":
             mols.append(Molecule(mn, blocks, MOL_FREE, phibulk=float(_get(calc, "mol", mn, "phibulk")),
-                                 generations=gens))
+                                 generations=gens, force=force))
         elif fr == "restricted":
             th = _get(calc, "mol", mn, "theta")
             if th is None:
@@ -274,7 +277,7 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
                 if nn is None:
                     raise ValueError(f"mol : {mn} needs theta or n")
                 th = float(nn) * length
-            mols.append(Molecule(mn, blocks, MOL_RESTRICTED, theta=float(th), generations=gens))
+            mols.append(Molecule(mn, blocks, MOL_RESTRICTED, theta=float(th), generations=gens, force=force))
         elif fr == "solvent":
             if gens:
                 raise ValueError(f"mol : {mn} : a dendrimer cannot be the solvent here")

@@ -145,6 +145,13 @@ typedef struct {
     int        n_generations;
     const int *generation_blocks;
     const int *generation_repeat;
+    /* mol : force (SF_Molecule.cpp:41-43): the constant-force ensemble of
+     * first-order copolymers, forward steps biased by +force along x (1D),
+     * y (2D cylinder) or z (3D), backward steps by -force (Lat1DFlat1stO.cpp:
+     * 116-130, Lat1DCyl1stO.cpp:112-133, Lat2DCyl1stO.cpp:100-126,
+     * Lat3D1stO.cpp:94-130); 0 for none.  Homopolymers, dendrimers, the 2D
+     * flat lattice and overflow protection refuse it as SFbox does. */
+    double     force;
 } sfgpu_molecule_desc;
 
 typedef struct {

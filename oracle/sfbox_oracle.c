@@ -402,6 +402,51 @@ static void olat_prop2(const olat *L, const double *gin, const double *G, double
     olat_set_boundaries6(L, gout);
 }
 
+/* one constant-force step (mol : force), Lat1DFlat1stO.cpp:116-130,
+   Lat1DCyl1stO.cpp:112-133 (the sphere inherits it), Lat2DCyl1stO.cpp:100-126,
+   Lat3D1stO.cpp:94-130; gin carries boundary copies */
+static void olat_prop1_force(const olat *L, const double *gin, const double *G, double *gout, double f) {
+    int M = L->M;
+    double l1 = L->l1;
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(L, z)) continue;
+        double g = G[z], r;
+        if (L->grad == 1 && !L->cyl) {
+            double norm = l1 * (exp(-f) + exp(f) - 2) + 1;
+            double f_1 = l1 * exp(-f) / norm, f1 = l1 * exp(f) / norm;
+            double a = gin[z - 1], b = gin[z], c = gin[z + 1];
+            r = g * (b + f1 * (a - b) + f_1 * (c - b));
+        } else if (L->grad == 1) {
+            double f_1 = exp(f), f1 = exp(-f);
+            double fnorm = (4.0 + f1 + f_1) / 6.0;
+            f1 = f1 / fnorm; f_1 = f_1 / fnorm;
+            double f1z = L->lam_p[z] * f1, f_1z = L->lam_m[z] * f_1, f0z = (1 - L->lam_p[z] - L->lam_m[z]) / fnorm;
+            r = g * (f_1z * gin[z - 1] + f0z * gin[z] + f1z * gin[z + 1]);
+        } else if (L->grad == 2) {
+            int MY = L->Md[1], x = z / MY;
+            double f_1 = exp(-f), f1 = exp(f), norm = l1 * (f_1 + f1 - 2) + 1;
+            double a = gin[z - 1], b = gin[z], c = gin[z + 1];
+            r = g * (b + L->lam_m[x] * (gin[z - MY] - b) + L->lam_p[x] * (gin[z + MY] - b) + l1 * (a * f1 + c * f_1 - b - b)) / norm;
+        } else {
+            int jx = L->st[0], jy = L->st[1];
+            double f1 = exp(f), f_1 = exp(-f), fnorm = 1.0 / (4.0 + exp(f) + exp(-f));
+            double acc = gin[z - jx] * g;
+            acc += gin[z + jx] * g;
+            acc += gin[z - jy] * g;
+            acc += gin[z + jy] * g;
+            acc += gin[z - 1] * g * f1;
+            acc += gin[z + 1] * g * f_1;
+            r = acc * fnorm;
+        }
+        gout[z] = r;
+    }
+    for (int z = 0; z < M; z++) {
+        if (is_interior(L, z)) continue;
+        int m = mapped_site(L, z, NULL);
+        gout[z] = is_interior(L, m) ? gout[m] : gin[m];
+    }
+}
+
 /* the stiff_range and isotropic 3D second-order steps of
    SF_Copol2ndO_stiff_range: PropagateF/B(..., S, stiff) (Lat3D2ndO.cpp:155-247,
    :680-764) weigh with ps = S inside the range and 0.2 outside, pl = (1-ps)/4,
@@ -705,6 +750,7 @@ typedef struct {
        branch point) and functionalities; nshort positions centre to end */
     int ngen, nshort;
     int *gen_len, *gen_rep, *gen_seg;   /* gen_seg: positions of all generations in order */
+    double force;         /* mol : force, constant-force ensemble */
 } omol;
 
 struct orc_system {
@@ -823,6 +869,13 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
         }
         o->type = (N == 1) ? 0 : (o->nseg_used == 1 && !o->ngen ? 1 : 2);
         o->freedom = md->freedom; o->phibulk = md->phibulk; o->theta = md->theta;
+        o->force = (o->type == 0) ? 0.0 : md->force;
+        if (o->force != 0) {
+            /* copolymers only (SF_Homopol1stO.cpp:24-27, SF_Dend1stO.cpp:11-14);
+               no step on the 2D flat lattice (Lat2DFlat1stO.cpp:115-117) */
+            if (s->L.order != 1 || o->type != 2 || o->ngen || (s->L.grad == 2 && !s->L.cyl) ||
+                s->L.ltype != SFGPU_LATTICE_STANDARD || s->L.logmode) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
+        }
         if (o->freedom == SFGPU_MOL_SOLVENT) {
             if (s->solvent >= 0) { orc_destroy(s); return SFGPU_ERR_INVALID; }
             s->solvent = m;
@@ -1470,7 +1523,9 @@ static void molecule_phi(orc_system *s, omol *o) {
     for (int t = 1; t < N; t++) {
         int sg = o->seg[t];
         double S = s->pf[o->seg[t - 1] * s->nseg + sg];
-        if (L->stiff && K == 6) {
+        if (o->force != 0) {   /* SF_Copol1stO.cpp:1207-1211: PropagateG(Gi, G, s, force) */
+            olat_prop1_force(L, Gi + (size_t)(t - 1) * KM, s->swf + (size_t)sg * M, Gi + (size_t)t * KM, o->force);
+        } else if (L->stiff && K == 6) {
             /* SF_Copol2ndO_stiff_range::Matrix1, SF_Copol2ndO_stiff_range.cpp:211-217:
                Pf(s-1, s+1) (1-based s), the last step isotropic */
             int last = (t == N - 1);
@@ -1500,7 +1555,9 @@ static void molecule_phi(orc_system *s, omol *o) {
     for (int t = N - 2; t >= 0; t--) {
         int sg = o->seg[t];
         double S = s->pf[sg * s->nseg + o->seg[t + 1]];
-        if (L->stiff && K == 6) {
+        if (o->force != 0) {   /* backward with -force, SF_Copol1stO.cpp:1226-1230 */
+            olat_prop1_force(L, Ginv, s->swf + (size_t)sg * M, tmp, -o->force);
+        } else if (L->stiff && K == 6) {
             /* backward: Pf(s, s+2), the first step (s = N-1) isotropic,
                SF_Copol2ndO_stiff_range.cpp:229-234 */
             int firstb = (t == N - 2);

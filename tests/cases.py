@@ -111,6 +111,33 @@ def _stiff_copolymer():
     return SystemSpec(lat, segs, chi, mols, pf=pf)
 
 
+def _force_copolymer(gradients):
+    """A diblock pulled with mol : force (+0.8 forward, -0.8 backward) next to
+    a surface (1D), in a cylinder with a core (2D) or around a particle (3D)."""
+    if gradients == 1:
+        lat = Lattice(1, [20, 0, 0], [BOUND_SURFACE, 0, 0], [BOUND_MIRROR1, 0, 0], lam=1 / 6)
+    elif gradients == 2:
+        lat = Lattice(2, [10, 9, 0], [BOUND_MIRROR1, BOUND_MIRROR2, 0], [BOUND_MIRROR1, BOUND_MIRROR1, 0],
+                      geometry=GEOM_CYLINDRICAL, lam=0.2)
+    else:
+        lat = Lattice(3, [5, 6, 7], [BOUND_MIRROR1, BOUND_PERIODIC, BOUND_MIRROR2],
+                      [BOUND_MIRROR2, BOUND_PERIODIC, BOUND_MIRROR1])
+    mask = np.zeros(lat.shape)
+    if gradients == 1:
+        mask[0] = 1.0
+    elif gradients == 2:
+        mask[1:3, 1:4] = 1.0
+    else:
+        mask[2:4, 2:4, 3:5] = 1.0
+    segs = [Segment("S", SEG_FROZEN, mask.reshape(-1)), Segment("A"), Segment("B"), Segment("W")]
+    chi = np.zeros((4, 4))
+    chi[0, 1] = chi[1, 0] = -1.3
+    chi[2, 3] = chi[3, 2] = 0.5
+    mols = [Molecule("AB", [(1, 5), (2, 7)], MOL_FREE, phibulk=0.02, force=0.8),
+            Molecule("W", [(3, 1)], MOL_SOLVENT)]
+    return SystemSpec(lat, segs, chi, mols)
+
+
 # stencils contact weights: centre, face, edge, corner (0.1 + 6*0.08 + 12*0.02 + 8*0.0225 = 1)
 STENCILS = (0.1, 0.08, 0.02, 0.0225)
 
@@ -269,6 +296,9 @@ CASES = {
     "2d_dendrimer": lambda: _dendrimer(2),
     "3d_dendrimer": lambda: _dendrimer(3),
     "3d_2nd_stiff_copol": _stiff_copolymer,
+    "1d_force": lambda: _force_copolymer(1),
+    "2d_cyl_force": lambda: _force_copolymer(2),
+    "3d_force": lambda: _force_copolymer(3),
     "3d_2nd_fcc_brush": lambda: _typed(configs.brush3d(n=6, N=15, sigma=0.2, S=0.5)[0], LATTICE_FCC),
     "1d_cylinder": _cyl1d_micelle,
     "1d_sphere_colloid": _sphere1d_colloid,
@@ -283,7 +313,7 @@ CASES = {
 # cases whose derivatives (forward and reverse mode) are implemented: not the
 # lumped second-order lattices, the 3D lattice types other than standard,
 # nor dendrimers
-NOT_DIFFERENTIABLE = ("lumped", "fcc", "hex", "stencils", "dendrimer", "stiff")
+NOT_DIFFERENTIABLE = ("lumped", "fcc", "hex", "stencils", "dendrimer", "stiff", "force")
 DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFERENTIABLE))
 
 

@@ -302,11 +302,12 @@ def test_lattice_types_outside_derivatives_and_batch(gpu_lib):
     assert np.all(np.isfinite(sys_.residual(x)))
 
 
-@pytest.mark.parametrize("case", ["1d_dendrimer", "2d_dendrimer", "3d_dendrimer"])
+@pytest.mark.parametrize("case", ["1d_dendrimer", "2d_dendrimer", "3d_dendrimer", "1d_force", "2d_cyl_force",
+                                  "3d_force"])
 def test_dendrimer_converged_parity(gpu_lib, case):
-    """Symmetric dendrimers (SF_Dend1stO) converged by the device Pure_DIIS and
-    by the oracle's; the batched kernel and the derivatives report
-    SFGPU_ERR_UNSUPPORTED for them."""
+    """Symmetric dendrimers (SF_Dend1stO) and force-ensemble copolymers
+    converged by the device Pure_DIIS and by the oracle's; the batched kernel
+    and the derivatives report SFGPU_ERR_UNSUPPORTED for them."""
     from field_b200._native import SfgpuError
     from field_b200.batch import BatchSolver
     spec = CASES[case]()
