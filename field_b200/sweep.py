@@ -174,9 +174,13 @@ def sweep_calculations(calc: Dict[Key, str]) -> Tuple[Optional[Variation], List[
 
 def batchable(spec) -> bool:
     """Whether the batched persistent kernel takes this system: first order,
-    and the standard lattice type in 3D."""
+    the standard lattice type in 3D, no overflow protection, and linear
+    chains without a force (dendrimers and the force ensemble run on the
+    single-system path)."""
     from .desc import LATTICE_STANDARD
-    return spec.lattice.order == 1 and spec.lattice.lattice_type == LATTICE_STANDARD
+    return (spec.lattice.order == 1 and spec.lattice.lattice_type == LATTICE_STANDARD
+            and not getattr(spec, "overflow_protection", False)
+            and all(not m.generations and m.force == 0 for m in spec.molecules))
 
 
 @dataclass

@@ -70,3 +70,16 @@ def test_sweep_calculations_set_the_parameter():
 def test_invalid_variations_are_rejected(extra):
     with pytest.raises(ValueError):
         expand_variation(_calc(extra))
+
+
+def test_batchable_routes_special_systems_to_the_single_system_path():
+    import sys, os
+    sys.path.insert(0, os.path.dirname(__file__))
+    from cases import CASES
+    from field_b200.sweep import batchable
+    assert batchable(CASES["1d_surface"]())
+    for k in ("1d_dendrimer", "1d_force", "3d_fcc_colloid", "3d_2nd_brush"):
+        assert not batchable(CASES[k]())
+    spec = CASES["1d_surface"]()
+    spec.overflow_protection = True
+    assert not batchable(spec)
