@@ -153,7 +153,25 @@ def _range_mask(lat: Lattice, text: str) -> np.ndarray:
     return mask.reshape(-1)
 
 
+def _refuse_unbuilt(calc: Dict[Key, str]) -> None:
+    """Statements that change the physics of a calculation but are not built
+    here: refused by name instead of being ignored."""
+    for (c, n, p), v in calc.items():
+        lv = v.strip().lower()
+        if c == "mol" and p == "ring" and lv == "true":
+            raise ValueError(f"mol : {n} : ring : true -- ring chains (SF_HomoRing1stO) are not built")
+        if c in ("mon", "state") and p == "valence" and float(v) != 0.0:
+            raise ValueError(f"{c} : {n} : valence : {v} -- charges and electrostatics are not built")
+        if c == "mon" and p.startswith("state"):
+            raise ValueError(f"mon : {n} : {p} -- multistate segments are not built")
+        if c in ("reaction", "state"):
+            raise ValueError(f"{c} : {n} : {p} -- reactions and states are not built")
+        if c == "lat" and p == "n_layers_extended":
+            raise ValueError(f"lat : {n} : n_layers_extended is not built")
+
+
 def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
+    _refuse_unbuilt(calc)
     lats = _names(calc, "lat")
     if len(lats) != 1:
         raise ValueError("exactly one 'lat' is supported")

@@ -125,3 +125,17 @@ def test_overflow_protection_statement():
     with pytest.raises(ValueError):
         build_system(parse_input(base + "sys : noname : overflow_protection : true\n"
                                  "sys : noname : matrix_approach : second_order\nstart\n")[0])
+
+
+@pytest.mark.parametrize("extra", ["mol : pol : ring : true\n", "mon : A : valence : 1\n",
+                                   "mon : A : state1 : Ap\n", "reaction : r1 : equation : 2(A)=(B)\n",
+                                   "lat : flat : n_layers_extended : 40\n"])
+def test_unbuilt_physics_is_refused(extra):
+    """Statements that change the physics but are not built are refused by
+    name, not ignored."""
+    from field_b200 import configs
+    base = configs.C1_INPUT.format(n=20, N=10, phib=0.01, chi_aw=0.5, chi_as=-1.0).replace("start\n", "")
+    with pytest.raises(ValueError):
+        build_system(parse_input(base + extra + "start\n")[0])
+    # statements without effect on this path are accepted
+    build_system(parse_input(base + "mol : pol : save_memory : true\nmon : A : valence : 0\nstart\n")[0])
