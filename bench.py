@@ -291,8 +291,7 @@ def run_ours(a, rank, world, local_rank):
         kp_bytes = solver.algorithmic_bytes(last_iters)
         # DRAM traffic measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
         # on one launch of 148 instances of this workload, per instance and
-        # DIIS iteration (profiles/batch_diis_kernel_lat2dcyl_128x128.md),
-        # scaled to this launch's iterations
+        # DIIS iteration, scaled to this launch's iterations
         traffic = DRAM_BYTES_PER_INSTANCE_ITERATION * float(sum(int(i) + 1 for i in last_iters))
         solver.kernel_profile = {"kernel": "batch_diis_kernel (persistent, one launch per batch solve)",
                                  "bytes": kp_bytes, "ms": statistics.median(kms), "traffic": traffic,

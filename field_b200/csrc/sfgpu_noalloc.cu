@@ -18,6 +18,7 @@
 // caller's outputs.
 #include <cstring>
 #include <mutex>
+#include <set>
 #include <vector>
 #include "sfgpu_kernels.cuh"
 #include "sfgpu_system.h"
@@ -30,14 +31,28 @@ static __device__ __align__(256) double g_noalloc_scratch[SFGPU_NOALLOC_SCRATCH_
 // Host code cannot use the symbol g_noalloc_scratch as a device address: on
 // the host it names a stand-in object, not GPU memory.  The device address
 // is looked up once per device (with that device current) and cached here.
+// The cache assumes the device's primary context lives as long as the
+// process: after a cudaDeviceReset the cached address is stale, and calling
+// this entry point again on that device is not supported.
 static double *g_scratch_ptr[SFGPU_NOALLOC_MAX_DEVICES];
 static std::mutex g_scratch_mu;
+
+// Host copies of the lattice tables (lambda tables and lnGN weights), one per
+// distinct table content, kept until the process exits.  The table copy of
+// every call reads from here, so its host source outlives the call whatever
+// the stream does with the copy later.  Grows by 8*(2*MX + M) bytes per
+// distinct lattice a process uses.
+static std::set<std::vector<double>> g_table_store;
 
 static int scratch_for_current_device(double **out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { sfgpu_set_error(e, "cudaGetDevice", __FILE__, __LINE__); return SFGPU_ERR_CUDA; }
-    if (dev < 0 || dev >= SFGPU_NOALLOC_MAX_DEVICES) return SFGPU_ERR_UNSUPPORTED;
+    if (dev < 0 || dev >= SFGPU_NOALLOC_MAX_DEVICES) {
+        sfgpu_set_error(cudaSuccess, "sfgpu_chain_phi_noalloc: device index beyond the 64 devices it caches",
+                        __FILE__, __LINE__);
+        return SFGPU_ERR_UNSUPPORTED;
+    }
     std::lock_guard<std::mutex> lock(g_scratch_mu);
     if (!g_scratch_ptr[dev]) {
         void *p = nullptr;
@@ -101,10 +116,20 @@ extern "C" int sfgpu_chain_phi_noalloc(const sfgpu_lattice_desc *lat, int N, con
     double *lam_m = scr, *lam_p = lam_m + MX, *w_gn = lam_p + MX, *partial = w_gn + M;
     double *gb0 = partial + 1024, *gb1 = gb0 + M, *gf = gb1 + M;
     cudaStream_t st = (cudaStream_t)stream;
-    // lattice tables: plain copies into the scratch array (no allocation)
-    SFGPU_CUDA_TRY(cudaMemcpyAsync(lam_m, H.lam_m.data(), sizeof(double) * MX, cudaMemcpyHostToDevice, st));
-    SFGPU_CUDA_TRY(cudaMemcpyAsync(lam_p, H.lam_p.data(), sizeof(double) * MX, cudaMemcpyHostToDevice, st));
-    SFGPU_CUDA_TRY(cudaMemcpyAsync(w_gn, H.w_gn.data(), sizeof(double) * M, cudaMemcpyHostToDevice, st));
+    // lattice tables: one plain copy into the scratch array (no allocation),
+    // from the process-lifetime host store (lam_m, lam_p, w_gn are adjacent
+    // in the scratch layout)
+    const double *tables = nullptr;
+    {
+        std::vector<double> t;
+        t.reserve(2 * MX + M);
+        t.insert(t.end(), H.lam_m.begin(), H.lam_m.begin() + MX);
+        t.insert(t.end(), H.lam_p.begin(), H.lam_p.begin() + MX);
+        t.insert(t.end(), H.w_gn.begin(), H.w_gn.begin() + M);
+        std::lock_guard<std::mutex> lock(g_scratch_mu);
+        tables = g_table_store.insert(std::move(t)).first->data();
+    }
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(lam_m, tables, sizeof(double) * (2 * MX + M), cudaMemcpyHostToDevice, st));
     DLat L = H.L;
     L.lam_m = lam_m;
     L.lam_p = lam_p;

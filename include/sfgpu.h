@@ -429,6 +429,10 @@ int sfgpu_batch_get_phi(sfgpu_batch *batch, int instance, int segment, double *p
  * rejected with SFGPU_ERR_INVALID before any work is queued.  The first call
  * on a device looks up the array's device address (once per device, with
  * that device current); make that first call before any stream capture.
+ * That address is kept for the life of the process: after a cudaDeviceReset
+ * of the device, further calls on it are not supported.  The lattice tables
+ * (8*(2*MX + M) bytes) are copied from host memory that the library keeps
+ * until the process exits, one copy per distinct lattice.
  * All work is queued on `stream` (0 = legacy default stream).  Every call
  * uses the same array and overwrites it, and nothing in it has to start at
  * zero (phi is cleared by the call); two calls that overlap on the GPU, on

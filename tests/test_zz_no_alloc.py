@@ -18,6 +18,8 @@ from field_b200 import _native, configs
 from field_b200.desc import MOL_FREE
 from field_b200.system import System
 
+from cases import CASES
+
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-12
@@ -33,9 +35,28 @@ def _run_noalloc(lib, spec, mol, G_dev, phi_dev, lngn_dev, stream):
                                        g_ptrs, p_ptrs, C.c_void_p(lngn_dev.data_ptr()), C.c_void_p(stream))
 
 
-def test_noalloc_chain_matches_system_path(gpu_lib):
+def _flat1d_layer_adjustment():
+    spec, _ = configs.flat_adsorption(n=30, N=21, phib=0.02, chi_aw=0.6, chi_as=-1.2)
+    spec.lattice.layer_adjustment = 0.8
+    return spec
+
+
+# one case per family of lattice tables the call builds: the 2D cylinder
+# (radial lambda tables), the 1D flat lattice with a surface and a layer
+# adjustment in the lnGN weights, the 1D sphere around a colloid (curved
+# tables with an offset), a 3D FCC box (twelve-neighbour step)
+NOALLOC_CASES = {
+    "2d_cylinder": lambda: configs.cyl_micelle(nx=40, ny=36, nA=12, nB=9, radius=5)[0],
+    "1d_flat_layer_adjustment": _flat1d_layer_adjustment,
+    "1d_sphere_colloid": lambda: CASES["1d_sphere_colloid"](),
+    "3d_fcc_colloid": lambda: CASES["3d_fcc_colloid"](),
+}
+
+
+@pytest.mark.parametrize("name", sorted(NOALLOC_CASES))
+def test_noalloc_chain_matches_system_path(gpu_lib, name):
     lib = _native.load()
-    spec, _ = configs.cyl_micelle(nx=40, ny=36, nA=12, nB=9, radius=5)
+    spec = NOALLOC_CASES[name]()
     mol_index = 0
     mol = spec.molecules[mol_index]
     assert mol.freedom == MOL_FREE
