@@ -227,10 +227,16 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
     // weights of lnGN sums and of the free energy (SubtractBoundaries +
     // MultiplyWithLatticeSites)
     H->w_gn.assign(L.M, 0.0); H->w_f.assign(L.M, 0.0); H->sb.assign(L.M, 0.0);
+    // Lat2DFlat1stO::ComputeLnGN and Lat2DCyl1stO::ComputeLnGN halve the
+    // 1-based column y = MY-2 for an upper mirror2 in y, one layer inside the
+    // last interior one that SubtractBoundaries halves (Lat2DFlat1stO.cpp:
+    // 321-326, :333-341; Lat2DCyl1stO.cpp:415-437): the lnGN weights follow
+    // them, the free-energy weights do not
+    const int gn_y_shift = (L.grad == 2 && L.order == 1) ? 1 : 0;
     for (int z = 0; z < L.M; z++) {
         int c[3];
         lat_coords(L, z, c);
-        double w = 1.0;
+        double w = 1.0, wg = 1.0;
         bool keep = true, interior = true;
         for (int k = 0; k < L.grad; k++) {
             int last = L.Md[k] - 1;
@@ -239,16 +245,19 @@ int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H) {
             else {
                 if (c[k] == 1 && L.bc_lo[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
                 else if (c[k] == last - 1 && L.bc_hi[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
+                const int hi_gn = last - 1 - (k == 1 ? gn_y_shift : 0);
+                if (c[k] == 1 && L.bc_lo[k] == SFGPU_BOUND_MIRROR2) wg *= 0.5;
+                else if (c[k] == hi_gn && L.bc_hi[k] == SFGPU_BOUND_MIRROR2) wg *= 0.5;
             }
         }
         H->sb[z] = keep ? w : 0.0;
-        if (L.cyl) w *= H->Lx[c[0]];
+        if (L.cyl) { w *= H->Lx[c[0]]; wg *= H->Lx[c[0]]; }
         if (L.grad == 1 && !L.cyl) {   // flat MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269
-            if (z == 1) w *= ladj;
-            if (z == L.M - 2 && L.M > 3) w *= (2 - ladj);
+            if (z == 1) { w *= ladj; wg *= ladj; }
+            if (z == L.M - 2 && L.M > 3) { w *= (2 - ladj); wg *= (2 - ladj); }
         }
         H->w_f[z] = keep ? w : 0.0;
-        H->w_gn[z] = interior ? w : 0.0;
+        H->w_gn[z] = interior ? wg : 0.0;
         // Lat1D2ndO::ComputeLnGN sums the interior without mirror2 halves or
         // layer adjustment (Lat1D2ndO.cpp:291-300); the curved second-order
         // lattices keep L(z) and the mirror2 halves (Lat1DCyl2ndO.cpp:318-330,
@@ -478,8 +487,15 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     L.lamc_m = d_lamc_m; L.lamc_p = d_lamc_p;
     if ((rc = alloc_d(&d_wgn, M)) || (rc = alloc_d(&d_wf, M)) || (rc = alloc_d(&d_sb, M))) return rc;
     if (!H.stiff.empty()) {
-        for (auto &o : mols)
+        for (auto &o : mols) {
             if (o.type == 1) return fail(SFGPU_ERR_UNSUPPORTED, "a stiff range with homopolymers (SFbox: only copolymers)");
+            // a palindromic copolymer takes SF_Copol2ndO_stiff_range::SymMatrix1
+            // (SF_Copol2ndO_stiff_range.cpp:97-99, :407-452), whose half-chain
+            // route has no isotropic end steps and other Pf indices: not built
+            bool pal = o.type == 2 && !o.dend;
+            for (int s = 0; pal && s < o.N / 2; s++) pal = o.seg[s] == o.seg[o.N - 1 - s];
+            if (pal) return fail(SFGPU_ERR_UNSUPPORTED, "a palindromic copolymer on a stiff range (SFbox's SymMatrix1)");
+        }
         if ((rc = alloc_d(&d_stiff, M))) return rc;
         SFGPU_CUDA_TRY(cudaMemcpy(d_stiff, H.stiff.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
         L.stiff = d_stiff;

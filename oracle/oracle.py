@@ -1,9 +1,10 @@
 """ctypes wrapper of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
 
 Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
-the checker; the product (field_b200) never imports it.  Parity unpinned: the
-oracle restates SFbox's equations (see sfbox_oracle.c) and is validated by
-known-answer tests, since SFbox ships no golden data and cannot be built here.
+the checker; the product (field_b200) never imports it.  The oracle restates
+SFbox's equations (see sfbox_oracle.c) and is pinned against SFbox itself:
+build_reference() compiles the reference's own sources (oracle/refbuild) and
+tests/golden/reference_cases.npz holds that build's outputs.
 """
 from __future__ import annotations
 
@@ -23,6 +24,19 @@ def build(force: bool = False) -> str:
     if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(src):
         subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
     return _LIB
+
+
+REFBUILD = os.path.join(_HERE, "refbuild")
+REFERENCE_SRC = "/root/reference"
+
+
+def build_reference() -> bool:
+    """Build SFbox from the reference's own sources into oracle/_ref (sfbox and
+    the sfref driver) when the sources are present; False otherwise."""
+    if not os.path.isdir(REFERENCE_SRC):
+        return False
+    subprocess.check_call(["make", "-s", "-j8", "-C", REFBUILD, f"REF={REFERENCE_SRC}"])
+    return True
 
 
 def lib():

@@ -8,10 +8,13 @@
  * the reference lines it follows.  Arrays are 0-based; SFbox's 1-based site
  * z corresponds to index z-1 here.
  *
- * Parity unpinned: SFbox has no tests or golden files for this path and it
- * cannot be built in this environment (it needs the absent 'fenk' container
- * library and CLAPACK), so this file is validated by known-answer tests
- * derived from the equations.
+ * Pinned against SFbox itself: SFbox ships no tests or golden files for this
+ * path, so oracle/refbuild builds the reference's own C++ sources (with
+ * stand-ins for its absent 'fenk' container library and CLAPACK) and
+ * tests/golden/reference_cases.npz holds that build's outputs on one system
+ * per lattice family; this file meets them to 1e-13 per evaluation and to
+ * 1e-10 (phi) / 1e-9 (F) at convergence.  Known-answer tests derived from the
+ * equations check it further.
  *
  * Where SFbox leaves boundary-site values unspecified (3D propagator slices
  * keep stale scratch values on the boundary planes, Lat3D1stO.cpp:151-157;
@@ -281,9 +284,15 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
     L->w_gn = calloc(L->M, sizeof(double));
     L->w_f = calloc(L->M, sizeof(double));
     L->sb = calloc(L->M, sizeof(double));
+    /* Lat2DFlat1stO::ComputeLnGN and Lat2DCyl1stO::ComputeLnGN halve the
+       1-based column y = MY-2 for an upper mirror2 in y, one layer inside the
+       last interior one that SubtractBoundaries halves (Lat2DFlat1stO.cpp:
+       321-326, :333-341; Lat2DCyl1stO.cpp:415-437); the lnGN weights follow
+       them, the free-energy weights do not */
+    const int gn_y_shift = (L->grad == 2 && L->order == 1) ? 1 : 0;
     for (int z = 0; z < L->M; z++) {
         int c[3]; coords(L, z, c);
-        double w = 1.0; int keep = 1, interior = 1;
+        double w = 1.0, wg = 1.0; int keep = 1, interior = 1;
         for (int k = 0; k < L->grad; k++) {
             int last = L->Md[k] - 1;
             if (c[k] == 0) { interior = 0; if (L->bc_lo[k] != SFGPU_BOUND_SURFACE) keep = 0; }
@@ -291,16 +300,19 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
             else {
                 if (c[k] == 1 && L->bc_lo[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
                 else if (c[k] == last - 1 && L->bc_hi[k] == SFGPU_BOUND_MIRROR2) w *= 0.5;
+                int hi_gn = last - 1 - (k == 1 ? gn_y_shift : 0);
+                if (c[k] == 1 && L->bc_lo[k] == SFGPU_BOUND_MIRROR2) wg *= 0.5;
+                else if (c[k] == hi_gn && L->bc_hi[k] == SFGPU_BOUND_MIRROR2) wg *= 0.5;
             }
         }
         L->sb[z] = keep ? w : 0.0;
-        if (L->cyl) w *= L->Lx[c[0]];
+        if (L->cyl) { w *= L->Lx[c[0]]; wg *= L->Lx[c[0]]; }
         if (L->grad == 1 && !L->cyl) {   /* flat: Lat1DFlat.cpp:266-269 */
-            if (z == 1) w *= L->ladj;
-            if (z == L->M - 2 && L->M > 3) w *= (2 - L->ladj);
+            if (z == 1) { w *= L->ladj; wg *= L->ladj; }
+            if (z == L->M - 2 && L->M > 3) { w *= (2 - L->ladj); wg *= (2 - L->ladj); }
         }
         L->w_f[z] = keep ? w : 0.0;
-        L->w_gn[z] = interior ? w : 0.0;
+        L->w_gn[z] = interior ? wg : 0.0;
         /* Lat1D2ndO::ComputeLnGN: interior sum without mirror2 halves or layer
            adjustment (Lat1D2ndO.cpp:275-285) */
         if (L->order == 2 && L->grad == 1 && !L->cyl) L->w_gn[z] = interior ? 1.0 : 0.0;
@@ -897,8 +909,15 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
     }
     if (s->solvent < 0) { orc_destroy(s); return SFGPU_ERR_INVALID; }
     if (s->L.stiff)   /* SF_MolList2ndO.cpp:39: only copolymers take a stiff range */
-        for (int m = 0; m < s->nmol; m++)
+        for (int m = 0; m < s->nmol; m++) {
             if (s->mol[m].type == 1) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
+            /* palindromic copolymers take SF_Copol2ndO_stiff_range::SymMatrix1
+               (SF_Copol2ndO_stiff_range.cpp:97-99, :407-452): not restated */
+            const omol *o = &s->mol[m];
+            int pal = o->type == 2 && o->ngen == 0;
+            for (int q = 0; pal && q < o->N / 2; q++) pal = o->seg[q] == o->seg[o->N - 1 - q];
+            if (pal) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
+        }
 
     /* liquid states and their classes, SF_Solve.cpp:37-86 */
     s->stateQ = calloc(ns, sizeof(int));

@@ -3,10 +3,12 @@
  *
  * CPU restatement of the SFbox 2.1 SF-SCF hot path, used by tests/, the
  * smoke check and bench.py's CPU-baseline leg to check the CUDA library.
- * Parity unpinned: the reference ships no golden vectors and cannot be built
- * here (it needs the absent 'fenk' container library and CLAPACK), so this
- * restatement is checked against known-answer tests derived from the
- * equations (u = 0 limits, sum rules, symmetry) instead of reference output.
+ * Pinned against SFbox itself: oracle/refbuild builds the reference's own
+ * C++ sources (with stand-ins for its absent 'fenk' container library and
+ * CLAPACK), and tests/golden/reference_cases.npz holds that build's residuals,
+ * profiles, lnGN and free energies on one system per lattice family, which
+ * this restatement meets to 1e-13 (tests/test_reference_parity.py); it is
+ * further checked by known-answer tests derived from the equations.
  */
 #ifndef SFBOX_ORACLE_H
 #define SFBOX_ORACLE_H

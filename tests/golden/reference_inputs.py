@@ -1,0 +1,664 @@
+"""SFbox input files of the parity cases run through the reference's own
+sources (oracle/_ref/sfref) and through this library's input reader.
+
+One small system per lattice family of the hot path, with the boundary,
+molecule and segment kinds each family takes.  Shared by the fixture
+generator (make_reference_golden.py) and the parity tests.
+"""
+
+_SOLVENT_TAIL = """mol : water : composition : (W)1
+mol : water : freedom : solvent
+"""
+
+INPUTS = {
+    # Lat1DFlat1stO, the C1 system at reduced size: surface, frozen S
+    "1d_flat_surface": """lat : flat : gradients : 1
+lat : flat : n_layers : 30
+lat : flat : geometry : flat
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.5
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)21
+mol : pol : freedom : free
+mol : pol : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # the C1 system itself
+    "1d_flat_c1": """lat : flat : gradients : 1
+lat : flat : n_layers : 100
+lat : flat : geometry : flat
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.5
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)100
+mol : pol : freedom : free
+mol : pol : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # mirror2 above, lambda_chi != lambda, copolymer and restricted
+    # homopolymer
+    "1d_flat_mirror2": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 25
+lat : flat : lambda : 0.25
+lat : flat : lambda_chi : 0.2
+lat : flat : lowerbound : mirror1
+lat : flat : upperbound : mirror2
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 1.1
+mon : B : chi - W : -0.2
+mon : A : chi - B : 0.5
+mol : ab : composition : (A)6(B)5(A)3
+mol : ab : freedom : free
+mol : ab : phibulk : 0.02
+mol : h : composition : (B)9
+mol : h : freedom : restricted
+mol : h : theta : 2.5
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # a layer adjustment (SFbox allows it with mirror1 on both sides only)
+    "1d_flat_layer_adjustment": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 19
+lat : flat : lambda : 0.16666666666666667
+lat : flat : layer_adjustment : 0.7
+lat : flat : lowerbound : mirror1
+lat : flat : upperbound : mirror1
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.9
+mon : B : chi - W : 0.3
+mol : ab : composition : (A)5(B)5
+mol : ab : freedom : free
+mol : ab : phibulk : 0.03
+mol : h : composition : (A)8
+mol : h : freedom : restricted
+mol : h : theta : 1.5
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    "1d_flat_periodic": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 33
+lat : flat : lambda : 0.25
+lat : flat : lowerbound : periodic
+lat : flat : upperbound : periodic
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - B : 0.5
+mon : A : chi - W : 1.2
+mon : B : chi - W : -0.2
+mol : aba : composition : (A)4(B)9(A)4
+mol : aba : freedom : restricted
+mol : aba : theta : 6
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # Lat2DCyl1stO, the C2 system at reduced size
+    "2d_cylinder": """lat : cyl : gradients : 2
+lat : cyl : geometry : cylindrical
+lat : cyl : n_layers_x : 20
+lat : cyl : n_layers_y : 16
+lat : cyl : lambda : 0.16666666666666667
+lat : cyl : lowerbound_x : mirror1
+lat : cyl : upperbound_x : mirror1
+lat : cyl : lowerbound_y : mirror1
+lat : cyl : upperbound_y : mirror1
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 1.6
+mon : B : chi - W : 0.0
+mol : AB : composition : (A)6(B)5
+mol : AB : freedom : free
+mol : AB : phibulk : 0.005
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # Lat2DCyl1stO with a core (offset), a surface and mirror2
+    "2d_cylinder_core": """lat : cyl : gradients : 2
+lat : cyl : geometry : cylindrical
+lat : cyl : n_layers_x : 14
+lat : cyl : n_layers_y : 11
+lat : cyl : offset_first_layer_x : 2
+lat : cyl : lambda : 0.2
+lat : cyl : lowerbound_x : surface
+lat : cyl : upperbound_x : mirror1
+lat : cyl : lowerbound_y : mirror1
+lat : cyl : upperbound_y : mirror2
+mon : S : freedom : frozen
+mon : S : frozen_range : 0,0;0,12
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.9
+mon : A : chi - S : -0.8
+mol : a : composition : (A)12
+mol : a : freedom : free
+mol : a : phibulk : 0.02
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # Lat2DFlat1stO with a surface, mirror2 and a restricted molecule
+    "2d_flat_surface": """lat : sq : gradients : 2
+lat : sq : geometry : flat
+lat : sq : n_layers_x : 14
+lat : sq : n_layers_y : 11
+lat : sq : lambda : 0.16666666666666667
+lat : sq : lowerbound_x : surface
+lat : sq : upperbound_x : mirror1
+lat : sq : lowerbound_y : mirror2
+lat : sq : upperbound_y : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : 0,0;0,12
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -0.8
+mon : A : chi - W : 0.9
+mon : B : chi - W : 0.2
+mol : AB : composition : (A)5(B)4(A)2
+mol : AB : freedom : free
+mol : AB : phibulk : 0.02
+mol : h : composition : (B)7
+mol : h : freedom : restricted
+mol : h : theta : 3
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # Lat3D1stO periodic diblock melt, the C3 system at reduced size
+    "3d_periodic_melt": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : n_layers_x : 9
+lat : box : n_layers_y : 9
+lat : box : n_layers_z : 9
+mon : A : freedom : free
+mon : B : freedom : free
+mon : A : chi - B : 0.2
+mol : AB : composition : (A)7(B)6
+mol : AB : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # Lat3D1stO with mixed mirror1 / mirror2 / periodic bounds and a particle
+    "3d_mirror_colloid": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : n_layers_x : 8
+lat : box : n_layers_y : 7
+lat : box : n_layers_z : 6
+lat : box : lowerbound_x : mirror1
+lat : box : upperbound_x : mirror2
+lat : box : lowerbound_y : mirror2
+lat : box : upperbound_y : mirror1
+lat : box : lowerbound_z : periodic
+lat : box : upperbound_z : periodic
+mon : S : freedom : frozen
+mon : S : frozen_range : 1,1,2;2,2,4
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.5
+mon : A : chi - W : 0.7
+mon : B : chi - W : 0.2
+mol : AB : composition : (A)5(B)4
+mol : AB : freedom : free
+mol : AB : phibulk : 0.02
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # Lat3D2ndO grafted brush, the C5 system at reduced size
+    "3d_2nd_brush": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : n_layers_x : 6
+lat : box : n_layers_y : 6
+lat : box : n_layers_z : 8
+lat : box : lowerbound_x : mirror1
+lat : box : upperbound_x : mirror1
+lat : box : lowerbound_y : mirror1
+lat : box : upperbound_y : mirror1
+lat : box : lowerbound_z : mirror1
+lat : box : upperbound_z : mirror1
+sys : noname : matrix_approach : second_order
+mon : X : freedom : pinned
+mon : X : pinned_range : =(1,1,1)(3,4,1)(5,2,1)(6,6,1)
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.3
+mon : X : chi - W : 0.3
+mon : A : Pf - A : 0.5
+mol : brush : composition : (X)1(A)14
+mol : brush : freedom : restricted
+mol : brush : theta : 60
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # 3D FCC and HEX lattices around a particle, periodic box
+    "3d_fcc_colloid": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : latticetype : FCC
+lat : box : n_layers_x : 8
+lat : box : n_layers_y : 7
+lat : box : n_layers_z : 6
+mon : S : freedom : frozen
+mon : S : frozen_range : 1,1,2;2,2,4
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.5
+mon : A : chi - W : 0.7
+mon : B : chi - W : 0.2
+mol : AB : composition : (A)5(B)4
+mol : AB : freedom : free
+mol : AB : phibulk : 0.02
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # Lat1DCyl1stO and Lat1DSphere1stO
+    "1d_cylinder": """lat : l : gradients : 1
+lat : l : geometry : cylindrical
+lat : l : n_layers : 22
+lat : l : lambda : 0.16666666666666667
+lat : l : lambda_chi : 0.2
+lat : l : lowerbound : mirror1
+lat : l : upperbound : mirror1
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - B : 0.3
+mon : A : chi - W : 1.4
+mon : B : chi - W : -0.1
+mol : AB : composition : (A)7(B)6
+mol : AB : freedom : free
+mol : AB : phibulk : 0.02
+mol : h : composition : (A)9
+mol : h : freedom : restricted
+mol : h : theta : 5
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    "1d_sphere_colloid": """lat : l : gradients : 1
+lat : l : geometry : spherical
+lat : l : n_layers : 18
+lat : l : offset_first_layer : 3
+lat : l : lambda : 0.16666666666666667
+lat : l : lowerbound : surface
+lat : l : upperbound : mirror2
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.4
+mon : A : chi - W : 0.6
+mol : A : composition : (A)16
+mol : A : freedom : free
+mol : A : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # lumped second order, Lat1D2ndO
+    "1d_2nd_lumped": """lat : l : gradients : 1
+lat : l : geometry : flat
+lat : l : n_layers : 24
+lat : l : lambda : 0.16666666666666667
+lat : l : lowerbound : surface
+lat : l : upperbound : mirror2
+sys : noname : matrix_approach : second_order
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.2
+mon : A : chi - W : 0.6
+mon : A : Pf - A : 0.5
+mol : A : composition : (A)15
+mol : A : freedom : free
+mol : A : phibulk : 0.02
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # lumped second order, Lat2D2ndO: mirror2/mirror1 in x, surface/mirror2 in y
+    "2d_2nd_lumped": """lat : sq : gradients : 2
+lat : sq : geometry : flat
+lat : sq : n_layers_x : 11
+lat : sq : n_layers_y : 9
+lat : sq : lambda : 0.16666666666666667
+lat : sq : lowerbound_x : mirror2
+lat : sq : upperbound_x : mirror1
+lat : sq : lowerbound_y : surface
+lat : sq : upperbound_y : mirror2
+sys : noname : matrix_approach : second_order
+mon : S : freedom : frozen
+mon : S : frozen_range : 0,0;12,0
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -0.6
+mon : A : chi - B : 0.4
+mon : A : chi - W : 1.0
+mon : B : chi - W : 0.1
+mon : A : Pf - A : 0.45
+mon : A : Pf - B : 0.3
+mol : AB : composition : (A)6(B)5
+mol : AB : freedom : free
+mol : AB : phibulk : 0.05
+mol : h : composition : (B)7
+mol : h : freedom : restricted
+mol : h : theta : 4
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # curved second order: Lat1DCyl2ndO, Lat1DSphere2ndO, Lat2DCyl2ndO
+    "1d_cyl_2nd": """lat : l : gradients : 1
+lat : l : geometry : cylindrical
+lat : l : n_layers : 20
+lat : l : lambda : 0.16666666666666667
+lat : l : lowerbound : mirror1
+lat : l : upperbound : mirror1
+sys : noname : matrix_approach : second_order
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - B : 0.3
+mon : A : chi - W : 1.3
+mon : B : chi - W : -0.1
+mon : A : Pf - A : 0.5
+mon : A : Pf - B : 0.3
+mol : AB : composition : (A)8(B)6
+mol : AB : freedom : free
+mol : AB : phibulk : 0.03
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    "1d_sphere_2nd": """lat : l : gradients : 1
+lat : l : geometry : spherical
+lat : l : n_layers : 16
+lat : l : offset_first_layer : 4
+lat : l : lambda : 0.16666666666666667
+lat : l : lowerbound : surface
+lat : l : upperbound : mirror2
+sys : noname : matrix_approach : second_order
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.2
+mon : A : chi - W : 0.5
+mon : A : Pf - A : 0.45
+mol : A : composition : (A)12
+mol : A : freedom : free
+mol : A : phibulk : 0.01
+mol : r : composition : (A)7
+mol : r : freedom : restricted
+mol : r : theta : 20
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    "2d_cyl_2nd": """lat : cyl : gradients : 2
+lat : cyl : geometry : cylindrical
+lat : cyl : n_layers_x : 10
+lat : cyl : n_layers_y : 8
+lat : cyl : offset_first_layer_x : 2
+lat : cyl : lambda : 0.16666666666666667
+lat : cyl : lowerbound_x : surface
+lat : cyl : upperbound_x : mirror1
+lat : cyl : lowerbound_y : surface
+lat : cyl : upperbound_y : mirror2
+sys : noname : matrix_approach : second_order
+mon : S : freedom : frozen
+mon : S : frozen_range : 0,0;0,9
+mon : T : freedom : frozen
+mon : T : frozen_range : 1,0;11,0
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -0.7
+mon : A : chi - B : 0.5
+mon : A : chi - W : 1.1
+mon : B : chi - W : 0.2
+mon : A : Pf - A : 0.4
+mol : AB : composition : (A)5(B)6
+mol : AB : freedom : free
+mol : AB : phibulk : 0.04
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # 3D HEX (periodic) and stencils lattices
+    "3d_hex_colloid": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : latticetype : HEX
+lat : box : n_layers_x : 8
+lat : box : n_layers_y : 7
+lat : box : n_layers_z : 6
+mon : S : freedom : frozen
+mon : S : frozen_range : 1,1,2;2,2,4
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.5
+mon : A : chi - W : 0.7
+mon : B : chi - W : 0.2
+mol : AB : composition : (A)5(B)4
+mol : AB : freedom : free
+mol : AB : phibulk : 0.02
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    "3d_stencils_colloid": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : latticetype : stencils
+lat : box : lambda0 : 0.1
+lat : box : lambda1 : 0.08
+lat : box : lambda2 : 0.02
+lat : box : lambda3 : 0.0225
+lat : box : n_layers_x : 8
+lat : box : n_layers_y : 7
+lat : box : n_layers_z : 6
+lat : box : lowerbound_x : mirror1
+lat : box : upperbound_x : mirror2
+lat : box : lowerbound_y : mirror2
+lat : box : upperbound_y : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : 1,1,2;2,2,4
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.5
+mon : A : chi - W : 0.7
+mon : B : chi - W : 0.2
+mol : AB : composition : (A)5(B)4
+mol : AB : freedom : free
+mol : AB : phibulk : 0.02
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # overflow protection: the log-space Lat1DFlat1stOS and Lat2DCyl1stOS
+    "1d_flat_overflow": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 30
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror2
+sys : noname : overflow_protection : true
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.5
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)21
+mol : pol : freedom : free
+mol : pol : phibulk : 0.01
+mol : r : composition : (A)9
+mol : r : freedom : restricted
+mol : r : theta : 2
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    "2d_cyl_overflow": """lat : cyl : gradients : 2
+lat : cyl : geometry : cylindrical
+lat : cyl : n_layers_x : 12
+lat : cyl : n_layers_y : 10
+lat : cyl : lambda : 0.16666666666666667
+lat : cyl : lowerbound_x : mirror1
+lat : cyl : upperbound_x : mirror2
+lat : cyl : lowerbound_y : mirror1
+lat : cyl : upperbound_y : mirror2
+sys : noname : overflow_protection : true
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 1.6
+mon : B : chi - W : 0.0
+mol : AB : composition : (A)6(B)5
+mol : AB : freedom : free
+mol : AB : phibulk : 0.005
+mol : r : composition : (B)8
+mol : r : freedom : restricted
+mol : r : theta : 3
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # a symmetric dendrimer at a surface (SF_Dend1stO)
+    "1d_dendrimer": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 24
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.0
+mon : A : chi - W : 0.6
+mon : B : chi - W : 0.2
+mol : den : composition : @dend(2,(A)3,3,(B)2(A)1,2)
+mol : den : freedom : restricted
+mol : den : theta : 3
+mol : lin : composition : (A)4(B)4
+mol : lin : freedom : free
+mol : lin : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # constant-force ensemble (mol : force) of a diblock at a surface
+    "1d_force": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 26
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.2
+mon : B : chi - W : 0.4
+mol : AB : composition : (A)3(B)9
+mol : AB : freedom : restricted
+mol : AB : theta : 2
+mol : AB : force : 0.3
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # second-order copolymer with a stiff range (SF_Copol2ndO_stiff_range)
+    "3d_2nd_stiff_range": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : n_layers_x : 6
+lat : box : n_layers_y : 5
+lat : box : n_layers_z : 6
+lat : box : lowerbound_x : mirror1
+lat : box : upperbound_x : mirror1
+lat : box : lowerbound_y : mirror1
+lat : box : upperbound_y : mirror1
+lat : box : lowerbound_z : mirror1
+lat : box : upperbound_z : mirror1
+lat : box : stiff_range : 1,1,1;3,5,6
+sys : noname : matrix_approach : second_order
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.8
+mon : B : chi - W : 0.1
+mon : A : Pf - A : 0.6
+mon : A : Pf - B : 0.4
+mol : tri : composition : (A)4(B)5(A)3
+mol : tri : freedom : restricted
+mol : tri : theta : 20
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # a palindromic second-order copolymer (SF_Copol2ndO's symmetric route)
+    "3d_2nd_palindrome": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : n_layers_x : 6
+lat : box : n_layers_y : 5
+lat : box : n_layers_z : 6
+lat : box : lowerbound_x : mirror1
+lat : box : upperbound_x : mirror2
+lat : box : lowerbound_y : periodic
+lat : box : upperbound_y : periodic
+lat : box : lowerbound_z : mirror1
+lat : box : upperbound_z : mirror1
+sys : noname : matrix_approach : second_order
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.8
+mon : B : chi - W : 0.1
+mon : A : Pf - A : 0.6
+mon : A : Pf - B : 0.4
+mol : tri : composition : (A)4(B)5(A)4
+mol : tri : freedom : restricted
+mol : tri : theta : 20
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+}

@@ -1,0 +1,173 @@
+"""Parity against SFbox 2.1 itself.
+
+tests/golden/reference_cases.npz was written by the reference's own C++
+sources (built by oracle/refbuild, driven by oracle/_ref/sfref; generator
+tests/golden/make_reference_golden.py) on the input files of
+tests/golden/reference_inputs.py: one system per lattice family of the hot
+path.  The oracle (CPU) and the CUDA library (GPU) must meet those numbers:
+
+* one residual evaluation at seeded x: the residual, every state's volume
+  fraction on the interior sites, lnGN of every molecule and the free
+  energy, to 1e-13 (oracle) and 1e-12 (CUDA) relative;
+* SFbox's Pure_DIIS solve to 1e-12 from a seeded start: the same iteration
+  run here converges to phi within 1e-10 and F within 1e-9 relative.
+
+Boundary entries of the profiles are not compared: SFbox leaves stale
+values there on 3D and second-order lattices, and no interior quantity reads
+them.  If oracle/_ref/sfref is present (built from the reference's sources
+where they are available), a live test also runs SFbox on a fresh seed.
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+from reference_inputs import INPUTS  # noqa: E402
+from field_b200.sfinput import build_system, parse_input  # noqa: E402
+
+REFERENCE = os.path.join(HERE, "golden", "reference_cases.npz")
+SFREF = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "sfref")
+
+
+def _load():
+    with np.load(REFERENCE) as z:
+        return {k: z[k] for k in z.files}
+
+
+DATA = _load()
+CASES = sorted({k.split("/")[0] for k in DATA})
+SOLVED = sorted({k.split("/")[0] for k in DATA if k.endswith("/solve_x")})
+
+
+def _spec(case):
+    return build_system(parse_input(INPUTS[case])[0])
+
+
+def interior(spec):
+    """Sites with every coordinate inside 1..n (no boundary layer)."""
+    shape = spec.lattice.shape
+    mask = np.ones(shape, dtype=bool)
+    for k, n in enumerate(shape):
+        idx = [slice(None)] * len(shape)
+        idx[k] = 0
+        mask[tuple(idx)] = False
+        idx[k] = n - 1
+        mask[tuple(idx)] = False
+    return mask.reshape(-1)
+
+
+def _rel(a, b):
+    return np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300)
+
+
+def _check_eval(spec, f, phi_of, lngn_of, F, case, tol_f, tol_phi, tol_F):
+    g = DATA[f"{case}/g"]
+    assert np.max(np.abs(f - g)) <= tol_f * max(1.0, np.max(np.abs(g))), case
+    inner = interior(spec)
+    want = DATA[f"{case}/phi"]
+    for i in range(len(spec.segments)):
+        got = phi_of(i)
+        assert _rel(got[inner], want[i][inner]) <= tol_phi or np.max(np.abs(want[i][inner])) == 0, (case, i)
+    for m, v in enumerate(DATA[f"{case}/lngn"]):
+        assert abs(lngn_of(m) - v) <= tol_phi * max(1.0, abs(v)), (case, m)
+    Fw = DATA[f"{case}/F"][0]
+    assert abs(F - Fw) <= tol_F * max(1.0, abs(Fw)), case
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_meets_reference_evaluation(case):
+    from oracle.oracle import Oracle
+    spec, _ = _spec(case)
+    o = Oracle(spec)
+    f = o.residual(DATA[f"{case}/x"])
+    _check_eval(spec, f, o.phi, o.lngn, o.free_energy(), case, 1e-13, 1e-13, 1e-13)
+
+
+@pytest.mark.parametrize("case", SOLVED)
+def test_oracle_converges_to_reference(case):
+    from oracle.oracle import Oracle
+    spec, st = _spec(case)
+    o = Oracle(spec)
+    x, rc, it, err = o.solve_diis(DATA[f"{case}/solve_x0"], tol=1e-12, maxit=20000, m=st.m, eta=st.deltamax)
+    assert rc == 0, (case, rc, it, err)
+    o.residual(x)
+    inner = interior(spec)
+    want = DATA[f"{case}/solve_phi"]
+    for i in range(len(spec.segments)):
+        if np.max(np.abs(want[i][inner])) > 0:
+            assert _rel(o.phi(i)[inner], want[i][inner]) <= 1e-10, (case, i)
+    Fw = DATA[f"{case}/solve_F"][0]
+    assert abs(o.free_energy() - Fw) <= 1e-9 * max(1.0, abs(Fw))
+
+
+def test_reference_fixture_covers_every_lattice_family():
+    """Every lattice family of the hot path has a reference case."""
+    fam = set()
+    for case in CASES:
+        spec, _ = _spec(case)
+        L = spec.lattice
+        fam.add((L.gradients, L.geometry, L.order, L.lattice_type, bool(spec.overflow_protection)))
+    # 1D flat/cylinder/sphere, 2D flat/cylinder, 3D standard/FCC/HEX/stencils
+    # (first order); 1D flat/cylinder/sphere, 2D flat/cylinder, 3D (second
+    # order); overflow protection in 1D and 2D
+    assert len(fam) >= 16, sorted(fam)
+
+
+@pytest.mark.skipif(not os.path.exists(SFREF), reason="oracle/_ref/sfref is built where the reference sources are")
+@pytest.mark.parametrize("case", ["1d_flat_c1", "2d_cylinder_core", "3d_mirror_colloid", "3d_2nd_brush",
+                                  "2d_2nd_lumped", "1d_dendrimer"])
+def test_oracle_against_live_reference(case):
+    """SFbox run now on a seed the fixture does not hold."""
+    from oracle.oracle import Oracle
+    spec, _ = _spec(case)
+    o = Oracle(spec)
+    x = np.random.default_rng(99).normal(0.0, 0.25, o.nvar)
+    with tempfile.TemporaryDirectory() as wd:
+        inp, xf, out = (os.path.join(wd, n) for n in ("c.in", "c.x", "c.out"))
+        with open(inp, "w") as fh:
+            fh.write(INPUTS[case])
+        x.astype("<f8").tofile(xf)
+        subprocess.run([SFREF, "eval", inp, xf, out], check=True, capture_output=True, cwd=wd)
+        d = {}
+        for line in open(out):
+            p = line.split()
+            d[p[0]] = np.array([float(v) for v in p[2:]])
+    f = o.residual(x)
+    assert np.max(np.abs(f - d["g"])) <= 1e-13 * max(1.0, np.max(np.abs(d["g"])))
+    assert abs(o.free_energy() - d["F"][0]) <= 1e-13 * max(1.0, abs(d["F"][0]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES)
+def test_gpu_meets_reference_evaluation(gpu_lib, case):
+    from field_b200.system import System
+    spec, _ = _spec(case)
+    s = System(spec)
+    f = s.residual(DATA[f"{case}/x"])
+    _check_eval(spec, f, s.phi, lambda m: s.mol_scalars(m)["lngn"], s.free_energy(), case, 1e-12, 1e-12, 1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", SOLVED)
+def test_gpu_converges_to_reference(gpu_lib, case):
+    """The CUDA Pure_DIIS from SFbox's start reaches SFbox's solution: phi to
+    1e-10 and F to 1e-9 relative."""
+    from field_b200.system import System
+    spec, st = _spec(case)
+    s = System(spec)
+    res = s.solve(DATA[f"{case}/solve_x0"], tol=1e-12, maxit=20000, m=st.m, eta=st.deltamax)
+    assert res.converged, (case, res.status, res.iterations, res.error)
+    s.residual(res.x)
+    inner = interior(spec)
+    want = DATA[f"{case}/solve_phi"]
+    for i in range(len(spec.segments)):
+        if np.max(np.abs(want[i][inner])) > 0:
+            assert _rel(s.phi(i)[inner], want[i][inner]) <= 1e-10, (case, i)
+    Fw = DATA[f"{case}/solve_F"][0]
+    assert abs(s.free_energy() - Fw) <= 1e-9 * max(1.0, abs(Fw))
