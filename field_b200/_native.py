@@ -39,6 +39,10 @@ PROTOTYPES = {
     "sfgpu_lat_set_boundaries": (i32, [vp, vp, i32]),
     "sfgpu_lat_side_fraction": (i32, [vp, vp, vp]),
     "sfgpu_lat_lngn": (i32, [vp, vp, i32, dp]),
+    "sfgpu_lat_connect": (i32, [vp, vp, vp, vp, i32]),
+    "sfgpu_lat_correct_double_count": (i32, [vp, vp, vp]),
+    "sfgpu_lat_norm_phi_free": (i32, [vp, vp, f64]),
+    "sfgpu_lat_norm_phi_restr": (i32, [vp, vp, vp, i32, f64]),
     "sfgpu_solve_diis": (i32, [vp, dp, f64, i32, i32, f64, ip, dp]),
     "sfgpu_profile_propagator": (i32, [vp, i32, dp, dp, dp, dp]),
     "sfgpu_system_set_tile": (i32, [vp, i32]),

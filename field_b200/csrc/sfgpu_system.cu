@@ -1274,6 +1274,72 @@ extern "C" int sfgpu_lat_lngn(sfgpu_system *s, const double *g, int components, 
     return SFGPU_OK;
 }
 
+// ---- composition and normalisation on device vectors --------------------
+namespace {
+// CorrectDoubleCountG: phi /= G where G > 0, else 0 (tools.cpp:86-90)
+__global__ void lat_correct_kernel(int M, const double *__restrict__ G, double *__restrict__ phi) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+        const double g = G[r];
+        phi[r] = (g > 0) ? phi[r] / g : 0.0;
+    }
+}
+// NormPhiFree: phi *= C
+__global__ void lat_scale_kernel(int M, double C, double *__restrict__ phi) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) phi[r] *= C;
+}
+// NormPhiRestr: C /= exp(ComputeLnGN(Gi)) (first order) or
+// 6 exp(ComputeLnGN(Gi)) (second order, whose lnGN already holds the 1/6),
+// with the weighted end-point sum in *wsum
+__global__ void lat_scale_restr_kernel(int M, double C, int K, const double *__restrict__ wsum,
+                                       double *__restrict__ phi) {
+    double v = *wsum;
+    if (K > 1) v /= 6.0;
+    const double lngn = log(v);
+    const double c = (K > 1) ? C / (6.0 * exp(lngn)) : C / exp(lngn);
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) phi[r] *= c;
+}
+}  // namespace
+
+extern "C" int sfgpu_lat_connect(sfgpu_system *s, const double *gb, const double *gf, double *phi, int components) {
+    CHECK_SYS(s);
+    if (s->logmode) return fail(SFGPU_ERR_UNSUPPORTED, "lattice-level composition on the log-space lattices");
+    if (components != s->K) return fail(SFGPU_ERR_INVALID, "components must be the lattice's K");
+    if (!gb || !gf || !phi) return fail(SFGPU_ERR_INVALID, "null device vector");
+    connect<<<grid_for(s->M), kBlock, 0, s->stream>>>(s->M, components, gb, gf, phi);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_lat_correct_double_count(sfgpu_system *s, double *phi, const double *g) {
+    CHECK_SYS(s);
+    if (s->logmode) return fail(SFGPU_ERR_UNSUPPORTED, "lattice-level composition on the log-space lattices");
+    if (!g || !phi) return fail(SFGPU_ERR_INVALID, "null device vector");
+    lat_correct_kernel<<<grid_for(s->M), kBlock, 0, s->stream>>>(s->M, g, phi);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_lat_norm_phi_free(sfgpu_system *s, double *phi, double C) {
+    CHECK_SYS(s);
+    if (s->logmode) return fail(SFGPU_ERR_UNSUPPORTED, "lattice-level normalisation on the log-space lattices");
+    if (!phi) return fail(SFGPU_ERR_INVALID, "null device vector");
+    lat_scale_kernel<<<grid_for(s->M), kBlock, 0, s->stream>>>(s->M, C, phi);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_lat_norm_phi_restr(sfgpu_system *s, double *phi, const double *gb, int components, double C) {
+    CHECK_SYS(s);
+    if (s->logmode) return fail(SFGPU_ERR_UNSUPPORTED, "lattice-level normalisation on the log-space lattices");
+    if (components != s->K) return fail(SFGPU_ERR_INVALID, "components must be the lattice's K");
+    if (!gb || !phi) return fail(SFGPU_ERR_INVALID, "null device vector");
+    wsum_partial<<<s->nblocks_red, kBlock, 0, s->stream>>>(s->M, components, gb, s->d_wgn, s->d_partial);
+    finish_sums<<<1, 32, 0, s->stream>>>(1, s->nblocks_red, s->d_partial, s->d_misc);
+    lat_scale_restr_kernel<<<grid_for(s->M), kBlock, 0, s->stream>>>(s->M, C, components, s->d_misc, phi);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
 // Timing of the dominant kernels on this system's buffers: reps launches of
 // a forward step and of a backward step with fused composition, bracketed by
 // CUDA events on the system stream.  Algorithmic bytes per launch follow the

@@ -85,6 +85,17 @@ class Lattice:
     def M(self) -> int:
         return int(np.prod(self.shape))
 
+    def interior_mask(self) -> np.ndarray:
+        """M booleans, True on sites with no coordinate in a boundary layer."""
+        mask = np.ones(self.shape, dtype=bool)
+        for k, n in enumerate(self.shape):
+            idx = [slice(None)] * len(self.shape)
+            idx[k] = 0
+            mask[tuple(idx)] = False
+            idx[k] = n - 1
+            mask[tuple(idx)] = False
+        return mask.reshape(-1)
+
     @property
     def components(self) -> int:
         """Direction components of a propagator: 1 (first order); second order

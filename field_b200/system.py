@@ -242,7 +242,9 @@ class System:
 
     def propagate(self, gin, g, S: float = 0.2, backward: bool = False):
         import torch
-        out = torch.empty_like(gin)
+        # zeroed: the lumped second-order steps write interior entries only,
+        # and a surface layer, which later steps read, holds 0 in a propagator
+        out = torch.zeros_like(gin)
         self._sync_torch()
         nat.check(self.lib.sfgpu_lat_propagate(self.h, C.c_void_p(gin.data_ptr()), C.c_void_p(g.data_ptr()),
                                                C.c_void_p(out.data_ptr()), float(S), int(backward)),
@@ -265,6 +267,42 @@ class System:
         nat.check(self.lib.sfgpu_lat_set_boundaries(self.h, C.c_void_p(p.data_ptr()), comps), "set_boundaries")
         self.synchronize()
         return p
+
+    def connect(self, gb, gf, phi):
+        """phi += sum_k gb_k gf_k (ConnectG), in place on device tensors."""
+        self._sync_torch()
+        nat.check(self.lib.sfgpu_lat_connect(self.h, C.c_void_p(gb.data_ptr()), C.c_void_p(gf.data_ptr()),
+                                             C.c_void_p(phi.data_ptr()), gb.numel() // self.M),
+                  "sfgpu_lat_connect")
+        self.synchronize()
+        return phi
+
+    def correct_double_count(self, phi, g):
+        """phi /= g where g > 0, else 0 (CorrectDoubleCountG), in place."""
+        self._sync_torch()
+        nat.check(self.lib.sfgpu_lat_correct_double_count(self.h, C.c_void_p(phi.data_ptr()),
+                                                          C.c_void_p(g.data_ptr())),
+                  "sfgpu_lat_correct_double_count")
+        self.synchronize()
+        return phi
+
+    def norm_phi_free(self, phi, c: float):
+        """phi *= c (NormPhiFree), in place."""
+        self._sync_torch()
+        nat.check(self.lib.sfgpu_lat_norm_phi_free(self.h, C.c_void_p(phi.data_ptr()), float(c)),
+                  "sfgpu_lat_norm_phi_free")
+        self.synchronize()
+        return phi
+
+    def norm_phi_restr(self, phi, gb, c: float):
+        """phi *= c / exp(lnGN(gb)) (second order: c / (6 exp(lnGN))), in place
+        (NormPhiRestr)."""
+        self._sync_torch()
+        nat.check(self.lib.sfgpu_lat_norm_phi_restr(self.h, C.c_void_p(phi.data_ptr()), C.c_void_p(gb.data_ptr()),
+                                                    gb.numel() // self.M, float(c)),
+                  "sfgpu_lat_norm_phi_restr")
+        self.synchronize()
+        return phi
 
     def lngn(self, g) -> float:
         self._sync_torch()

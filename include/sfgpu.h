@@ -277,6 +277,28 @@ int sfgpu_lat_side_fraction(sfgpu_system *sys, const double *phi, double *rho);
  * Lat3D2ndO.cpp:995-1025) of an end-point distribution */
 int sfgpu_lat_lngn(sfgpu_system *sys, const double *g, int components, double *lngn);
 
+/* Composition and normalisation on device vectors, for callers that keep
+ * their own chain loop over sfgpu_lat_propagate (the Matrix1 drivers,
+ * SF_Homopol1stO.cpp:553-622) or port Cuda_tools.h's Composition /
+ * CorrectDoubleCounting / NormPhi (Cuda_tools.cu:208-236).  All are
+ * asynchronous on the system's stream; K = components is 1 for first order
+ * or the lattice's direction count (6 in 3D, 3 or 5 on the lumped 1D/2D
+ * lattices, whose lateral groups count with their multiplicity 4 or 2).
+ * The log-space lattices (overflow_protection) return SFGPU_ERR_UNSUPPORTED.
+ *
+ * phi(z) += sum_k gb_k(z) gf_k(z): Lat1stO::ConnectG(GiA, GiB, out)
+ * (Lat1stO.h:36; Lat1DFlat1stO.cpp:268-274, Lat3D2ndO.cpp:895-903) */
+int sfgpu_lat_connect(sfgpu_system *sys, const double *gb, const double *gf, double *phi, int components);
+/* phi(z) /= g(z) where g(z) > 0, else 0: CorrectDoubleCountG (Lat1stO.h:40;
+ * Lat1DFlat1stO.cpp:294-300, tools.cpp:86-90) */
+int sfgpu_lat_correct_double_count(sfgpu_system *sys, double *phi, const double *g);
+/* phi *= C: NormPhiFree (Lat1stO.h:46; Lat1DFlat1stO.cpp:317-322) */
+int sfgpu_lat_norm_phi_free(sfgpu_system *sys, double *phi, double C);
+/* phi *= C / exp(lnGN(gb)) on first-order lattices, C / (6 exp(lnGN(gb))) on
+ * second-order ones, lnGN as sfgpu_lat_lngn: NormPhiRestr (Lat1stO.h:48;
+ * Lat1DFlat1stO.cpp:323-331, Lat3D2ndO.cpp:1036-1039).  C is theta/N. */
+int sfgpu_lat_norm_phi_restr(sfgpu_system *sys, double *phi, const double *gb, int components, double C);
+
 /* ---- derivatives ------------------------------------------------------- */
 /* f = residuals(x) and jv = J(x) v with J the exact Jacobian df/dx, by a
  * forward-mode (tangent) sweep through UpdateSWF, both propagator sweeps, the
