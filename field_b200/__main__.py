@@ -8,9 +8,12 @@ result (``newton : initial_guess : previous_result``, the default), and
 (field_b200.output).  ``vtk`` files are written one per
 calculation under numbered names.  Sweeps of first-order systems are solved as batched
 instances (field_b200.sweep): ``--waves`` sets how many batched launches the
-sweep is split into (default: one per point, SFbox's chain).  Solver:
-Pure_DIIS on the device with the file's tolerance, iterationlimit, m and
-deltamax.  Exit status 0 when every point converged, 1 otherwise.
+sweep is split into (default: one per point, SFbox's chain).  Solver: the
+file's newton : method -- SFbox's Newton iteration (pseudohessian, the
+default, or hessian) over the device residual, or Pure_DIIS on the device --
+with its tolerance, iterationlimit, deltamax (and m for Pure_DIIS).  Newton
+sweeps are solved point after point.  Exit status 0 when every point
+converged, 1 otherwise.
 """
 from __future__ import annotations
 
@@ -48,7 +51,8 @@ def main(argv=None) -> int:
         var, points = sweep_calculations(calc)
         built = [build_system(p) for p in points]
         st = built[0][1]
-        if len(points) > 1 and all(batchable(s) for s, _ in built):
+        newton = st.method in ("pseudohessian", "hessian")
+        if len(points) > 1 and not newton and all(batchable(s) for s, _ in built):
             waves = a.waves if a.waves > 0 else len(points)
             same = x_prev is not None and len(x_prev) == built[0][0].n_itvar()
             res = solve_sweep(calc, waves=waves, x0=x_prev if same else None, tol=st.tolerance,
@@ -60,7 +64,11 @@ def main(argv=None) -> int:
             for spec, _ in built:
                 if x is None or len(x) != spec.n_itvar():
                     x = np.zeros(spec.n_itvar())
-                r = System(spec).solve(x, tol=st.tolerance, maxit=st.iterationlimit, m=st.m, eta=st.deltamax)
+                if newton:
+                    r = System(spec).solve_newton(x, tol=st.tolerance, maxit=st.iterationlimit,
+                                                  pseudohessian=st.method == "pseudohessian", deltamax=st.deltamax)
+                else:
+                    r = System(spec).solve(x, tol=st.tolerance, maxit=st.iterationlimit, m=st.m, eta=st.deltamax)
                 results.append((r.x, r.iterations, r.status))
                 x = r.x
         for pi, ((spec, stp), (x, its, status), p) in enumerate(zip(built, results, points)):

@@ -44,6 +44,8 @@ PROTOTYPES = {
     "sfgpu_lat_norm_phi_free": (i32, [vp, vp, f64]),
     "sfgpu_lat_norm_phi_restr": (i32, [vp, vp, vp, i32, f64]),
     "sfgpu_solve_diis": (i32, [vp, dp, f64, i32, i32, f64, ip, dp]),
+    "sfgpu_newton_default_settings": (i32, [vp]),
+    "sfgpu_solve_newton": (i32, [vp, dp, vp, ip, ip, dp]),
     "sfgpu_profile_propagator": (i32, [vp, i32, dp, dp, dp, dp]),
     "sfgpu_system_set_tile": (i32, [vp, i32]),
     "sfgpu_jvp": (i32, [vp, vp, vp, vp, vp]),

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsfgpu.so")
 SOURCES = ["sfgpu_system.cu", "sfgpu_solve.cu", "sfgpu_batch.cu", "sfgpu_tangent.cu", "sfgpu_adjoint.cu",
-           "sfgpu_noalloc.cu"]
+           "sfgpu_noalloc.cu", "sfgpu_newton.cu"]
 HEADERS = ["sfgpu_internal.cuh", "sfgpu_kernels.cuh", "sfgpu_system.h", "sfgpu_batch.cuh", "sfgpu_tangent.cuh",
            "sfgpu_adjoint.cuh",
            "../../include/sfgpu.h"]

@@ -52,6 +52,15 @@ class SystemDesc(C.Structure):
                 ("molecules", C.POINTER(MoleculeDesc)), ("overflow_protection", C.c_int)]
 
 
+class NewtonSettings(C.Structure):
+    """sfgpu_newton_settings: SFbox's Newton iteration parameters."""
+    _fields_ = [("tolerance", C.c_double), ("iterationlimit", C.c_int), ("pseudohessian", C.c_int),
+                ("deltamax", C.c_double), ("deltamin", C.c_double), ("linesearchlimit", C.c_int),
+                ("small_alpha", C.c_double), ("max_n_small_alpha", C.c_int),
+                ("reset_hessian_criterion", C.c_double), ("max_accuracy_for_hessian_scaling", C.c_double),
+                ("ignore_newton_direction", C.c_int)]
+
+
 def dptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 

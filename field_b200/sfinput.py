@@ -102,9 +102,15 @@ def parse_dendrimer(text: str) -> Optional[List[Tuple[List[Tuple[str, int]], int
     return gens
 
 
+# newton : method choices on this path: SFbox's Newton with its BFGS-updated
+# pseudo-Hessian (the default, SF_Solve.cpp:1867-1869) or a finite-difference
+# Hessian, and Pure_DIIS; LBFGS, CG, SD, TN, BRR and experimental are refused
+NEWTON_METHODS = ("pseudohessian", "hessian", "Pure_DIIS")
+
+
 @dataclass
 class SolverSettings:
-    method: str = "Pure_DIIS"
+    method: str = "pseudohessian"
     tolerance: float = 1e-7
     iterationlimit: int = 5000
     m: int = 5
@@ -320,4 +326,10 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
         st.m = int(_get(calc, "newton", nn, "m", st.m))
         st.deltamax = float(_get(calc, "newton", nn, "deltamax", st.deltamax))
         st.initial_guess_file = _get(calc, "newton", nn, "initial_guess_input_file")
+        # deltamax's default is SFbox's 0.5 for every method (SF_Solve.cpp:1885);
+        # Pure_DIIS uses it as its step eta
+        if ("newton", nn, "deltamax") not in calc and st.method != "Pure_DIIS":
+            st.deltamax = 0.5
+    if st.method not in NEWTON_METHODS:
+        raise ValueError(f"newton : method : {st.method} is not built (methods: {', '.join(NEWTON_METHODS)})")
     return spec, st

@@ -144,6 +144,26 @@ class System:
             nat.check(rc, "sfgpu_solve_diis")
         return SolveResult(x, rc, it.value, err.value)
 
+    def solve_newton(self, x0=None, tol=1e-7, maxit=5000, pseudohessian=True, deltamax=0.5, **extra) -> SolveResult:
+        """SFbox's Newton iteration (SFNewton::iterate, Scheutjens step search)
+        over the device residual (sfgpu_solve_newton); extra keys override the
+        other sfgpu_newton_settings fields."""
+        from .desc import NewtonSettings
+        st = NewtonSettings()
+        nat.check(self.lib.sfgpu_newton_default_settings(C.byref(st)), "sfgpu_newton_default_settings")
+        st.tolerance, st.iterationlimit = float(tol), int(maxit)
+        st.pseudohessian, st.deltamax = int(bool(pseudohessian)), float(deltamax)
+        for k, v in extra.items():
+            setattr(st, k, v)
+        x = np.zeros(self.nvar) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+        it, nf, acc = C.c_int(), C.c_int(), C.c_double()
+        rc = self.lib.sfgpu_solve_newton(self.h, _d(x), C.byref(st), C.byref(it), C.byref(nf), C.byref(acc))
+        if rc not in (0, 4, 5):
+            nat.check(rc, "sfgpu_solve_newton")
+        r = SolveResult(x, rc, it.value, acc.value)
+        r.evaluations = nf.value
+        return r
+
     def jvp(self, x, v):
         """(f(x), J(x) v) with the exact forward-mode tangent."""
         x = np.ascontiguousarray(x, dtype=np.float64)

@@ -387,6 +387,39 @@ int sfgpu_system_set_tile(sfgpu_system *sys, int xc);
 int sfgpu_system_autotune(sfgpu_system *sys, int reps, int *chosen_xc, double *best_ms);
 
 /* ---- iterations ------------------------------------------------------- */
+/* SFbox's Newton iteration (SFNewton::iterate, sfnewton.cpp:844-1143, with
+ * Scheutjens' trust-region step search, :1946-2022) over this library's
+ * residual: the "plain Newton form".  The Hessian is dense, single
+ * precision and held as an LDU factorisation (sfnewton.h:147,
+ * newttool.cpp); pseudohessian = 1 (SFbox's default method 'pseudohessian')
+ * starts from diag(1 + |g|) and updates it BFGS-style each iteration
+ * (:1433-1521), pseudohessian = 0 (method 'hessian') rebuilds it from nvar
+ * finite-difference residuals (numhessian, :1627-1652).  SF_Solve's reset
+ * heuristics are kept (walking backwards, too many small steps,
+ * SF_Solve.cpp:659-727).  Residuals run on the device, the iteration on the
+ * host; nvar^2 floats of host memory, refused beyond nvar = 8192.  Stops as
+ * SFbox does: accuracy = sqrt(|p| |g| / (1 + |x|)) <= tolerance and
+ * |g| <= 10 tolerance (sfnewton.cpp:925, :2040-2042).  x (host) is the start
+ * and receives the result; returns SFGPU_ERR_NOTCONVERGED at the iteration
+ * limit. */
+typedef struct {
+    double tolerance;                       /* newton : tolerance (1e-7) */
+    int    iterationlimit;                  /* newton : iterationlimit (5000) */
+    int    pseudohessian;                   /* 1 pseudohessian (default), 0 hessian */
+    double deltamax;                        /* newton : deltamax (0.5) */
+    double deltamin;                        /* newton : deltamin (0) */
+    int    linesearchlimit;                 /* newton : linesearchlimit (20) */
+    double small_alpha;                     /* newton : small_alpha (1e-5) */
+    int    max_n_small_alpha;               /* newton : max_n_small_alpha (50) */
+    double reset_hessian_criterion;         /* newton : reset_hessian_criterion (1e3) */
+    double max_accuracy_for_hessian_scaling;/* (0.1) */
+    int    ignore_newton_direction;         /* (0) */
+} sfgpu_newton_settings;
+/* SFbox's defaults for an input file with a 'newton' block (SF_Solve.cpp:1779-2182) */
+int sfgpu_newton_default_settings(sfgpu_newton_settings *settings);
+int sfgpu_solve_newton(sfgpu_system *sys, double *x, const sfgpu_newton_settings *settings,
+                       int *iterations, int *function_calls, double *accuracy);
+
 /* Pure_DIIS: SFNewton::PlainLBFGSDIIS (sfnewton.cpp:566-664) on the device,
  * coefficients as SFNewton::Ax (sfnewton.cpp:531-557).  x is a host array,
  * in: initial guess, out: last iterate.  Returns SFGPU_ERR_NOTCONVERGED when

@@ -13,6 +13,9 @@ For every case:
 and for the cases of SOLVE_CASES, SFbox's Pure_DIIS (SF_Solve::Iterate,
 tolerance 1e-12) from the seeded start x0 (normal, sd 0.1):
   <case>/solve_x0, solve_x, solve_phi, solve_F, solve_Omega, solve_g
+and for NEWTON_CASES, SFbox's Newton iteration (newton : method pseudohessian,
+its default, and hessian; tolerance 1e-12) from x = 0:
+  <case>/newton_<method>_x, _phi, _F, _iterations
 
     python tests/golden/make_reference_golden.py
 """
@@ -40,6 +43,16 @@ SOLVE_CASES = ["1d_flat_surface", "1d_flat_c1", "1d_flat_mirror2", "1d_flat_peri
                "3d_fcc_colloid", "3d_hex_colloid", "3d_stencils_colloid", "1d_cylinder", "1d_sphere_colloid",
                "1d_2nd_lumped", "2d_2nd_lumped", "1d_cyl_2nd", "1d_sphere_2nd", "2d_cyl_2nd", "1d_flat_overflow",
                "2d_cyl_overflow", "1d_dendrimer", "1d_force", "3d_2nd_stiff_range", "3d_2nd_palindrome"]
+
+
+NEWTON_CASES = ["1d_flat_c1", "1d_flat_surface", "1d_sphere_colloid", "2d_cylinder_core", "2d_flat_surface",
+                "1d_dendrimer", "1d_2nd_lumped", "1d_force"]
+NEWTON_METHODS = ["pseudohessian", "hessian"]
+
+
+def newton_input(text, method):
+    """The case's input file with its newton method replaced."""
+    return text.replace("newton : isaac : method : Pure_DIIS", f"newton : isaac : method : {method}")
 
 
 def case_seed(name):
@@ -98,6 +111,14 @@ def reference_arrays():
                 data[f"{name}/solve_phi"] = state_rows(spec, s)
                 data[f"{name}/solve_F"] = s["F"]
                 data[f"{name}/solve_Omega"] = s["Omega"]
+            if name in NEWTON_CASES:
+                for meth in NEWTON_METHODS:
+                    s = run_sfref("solve", newton_input(text, meth), np.zeros(spec.n_itvar()), wd,
+                                  f"{name}_{meth}")
+                    data[f"{name}/newton_{meth}_x"] = s["x"]
+                    data[f"{name}/newton_{meth}_phi"] = state_rows(spec, s)
+                    data[f"{name}/newton_{meth}_F"] = s["F"]
+                    data[f"{name}/newton_{meth}_iterations"] = s["iterations"]
     return data
 
 
