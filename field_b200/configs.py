@@ -100,9 +100,10 @@ def melt3d(n=128, nA=50, nB=50, chi_ab=0.2, amp=0.05, seed=BASE_SEED + 3):
     return spec, x
 
 
-def sweep1d(count=256, seed=BASE_SEED + 4, n_range=(50, 400), N_range=(20, 1000)):
-    """Uneven 1D instances: layers U{50..400}, N log-uniform, chi_AW on a
-    shuffled grid over [0,1], phibulk log-uniform in [1e-4,1e-1], chi_AS U[-2,0]."""
+def sweep1d_inputs(count=256, seed=BASE_SEED + 4, n_range=(50, 400), N_range=(20, 1000), tolerance=1e-7):
+    """SFbox input files of the uneven 1D instances: layers U{50..400}, N
+    log-uniform, chi_AW on a shuffled grid over [0,1], phibulk log-uniform in
+    [1e-4,1e-1], chi_AS U[-2,0] (Pure_DIIS at the given tolerance)."""
     rng = np.random.default_rng(seed)
     chis = rng.permutation(np.linspace(0.0, 1.0, count))
     out = []
@@ -111,8 +112,18 @@ def sweep1d(count=256, seed=BASE_SEED + 4, n_range=(50, 400), N_range=(20, 1000)
         N = int(round(np.exp(rng.uniform(np.log(N_range[0]), np.log(N_range[1])))))
         phib = float(np.exp(rng.uniform(np.log(1e-4), np.log(1e-1))))
         chi_as = float(rng.uniform(-2.0, 0.0))
-        spec, x = flat_adsorption(n=n, N=N, phib=phib, chi_aw=float(chis[i]), chi_as=chi_as)
-        out.append((spec, x))
+        text = C1_INPUT.format(n=n, N=N, phib=phib, chi_aw=float(chis[i]), chi_as=chi_as)
+        out.append(text.replace("newton : isaac : tolerance : 1e-7", f"newton : isaac : tolerance : {tolerance!r}"))
+    return out
+
+
+def sweep1d(count=256, seed=BASE_SEED + 4, n_range=(50, 400), N_range=(20, 1000)):
+    """The uneven 1D instances of sweep1d_inputs as (spec, x0 = 0)."""
+    from .sfinput import build_system, parse_input
+    out = []
+    for text in sweep1d_inputs(count, seed, n_range, N_range):
+        spec, _ = build_system(parse_input(text)[0])
+        out.append((spec, np.zeros(spec.n_itvar())))
     return out
 
 

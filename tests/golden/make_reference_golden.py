@@ -80,7 +80,12 @@ def run_sfref(mode, text, x, workdir, tag):
     r = subprocess.run([SFREF, mode, inp, xf, out], capture_output=True, text=True, cwd=workdir)
     if r.returncode != 0:
         raise RuntimeError(f"sfref {mode} {tag} failed ({r.returncode}):\n{r.stdout[-1500:]}\n{r.stderr[-1500:]}")
-    return read_dump(out)
+    d = read_dump(out)
+    # Pure_DIIS reports its iterations only on the console ("i = <k> |g| = ...")
+    its = [int(ln.split()[2]) for ln in r.stdout.splitlines() if ln.startswith("i = ")]
+    if its:
+        d["diis_iterations"] = np.array([float(its[-1])])
+    return d
 
 
 def state_rows(spec, dump, prefix=""):

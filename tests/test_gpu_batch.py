@@ -1,6 +1,9 @@
 """Batched persistent solver: every instance matches the single-system
 Pure_DIIS path and the oracle (same algorithm, same iterates up to the order
-of floating-point reductions)."""
+of floating-point reductions), and at the batching configuration's full size
+(256 uneven instances, N up to 1000) SFbox's own solutions."""
+import os
+
 import numpy as np
 import pytest
 
@@ -21,25 +24,67 @@ def test_batch_uneven_sweep_matches_oracle(gpu_lib):
     specs = [s for s, _ in insts]
     bs = BatchSolver(specs, m=5, eta=0.1)
     x0 = np.concatenate([x for _, x in insts])
-    res = bs.solve(x0, tol=1e-9, maxit=3000)
+    res = bs.solve(x0, tol=1e-12, maxit=3000)
     assert res.converged.sum() >= len(insts) // 2
     for i, (spec, x) in enumerate(insts):
         o = Oracle(spec)
-        xo, rc, it, err = o.solve_diis(x, tol=1e-9, maxit=3000, m=5, eta=0.1)
+        xo, rc, it, err = o.solve_diis(x, tol=1e-12, maxit=3000, m=5, eta=0.1)
         assert (rc == 0) == bool(res.converged[i]), (i, rc, res.status[i])
         if rc != 0:
             continue
         # the converged iterate satisfies the oracle's equations
         xi = bs.split(res.x)[i]
-        assert np.linalg.norm(o.residual(xi)) < 1e-8
-        o.solve_diis(x, tol=1e-9, maxit=3000, m=5, eta=0.1)
+        assert np.linalg.norm(o.residual(xi)) < 1e-11
+        o.solve_diis(x, tol=1e-12, maxit=3000, m=5, eta=0.1)
+        inner = spec.lattice.interior_mask()
         for seg in range(len(spec.segments)):
-            want = o.phi(seg)
-            got = bs.phi(i, seg)
-            assert np.max(np.abs(got - want)) <= 1e-7 * max(1e-300, np.max(np.abs(want)))
+            want = o.phi(seg)[inner]
+            got = bs.phi(i, seg)[inner]
+            assert np.max(np.abs(got - want)) <= 1e-10 * max(1e-300, np.max(np.abs(want)))
         # DIIS trajectories separate in the last bits over many iterations
         # (reduction order), so the iteration counts agree only roughly
         assert abs(int(res.iterations[i]) - it) <= max(3, it // 2)
+
+
+C4_REFERENCE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c4_reference.npz")
+
+
+def test_batch_c4_full_size_meets_sfbox(gpu_lib):
+    """The 256 uneven Lat1DFlat1stO instances of the batching configuration
+    (layers 50..400, N 20..1000) in one launch, Pure_DIIS (m = 5, eta = 0.1,
+    SFbox's defaults) to |g| <= 1e-12 within 8000 iterations.  SFbox's own
+    Pure_DIIS (tests/golden/c4_reference.npz, from the reference's sources,
+    20000 iterations allowed) decides the outcome: every instance it solves
+    within 6000 iterations converges here, none it fails on (|g| growing to
+    overflow, or stalling for 20000 iterations near the spinodal) does; on the
+    converged ones phi agrees within 1e-10 and F within 1e-9 relative, both
+    evaluated by the oracle (pinned to SFbox per evaluation) at the two
+    solutions."""
+    with np.load(C4_REFERENCE) as z:
+        xr, offs, gnorm, Fr, its = z["x"], z["offsets"], z["gnorm"], z["F"], z["iterations"]
+    insts = configs.sweep1d(count=256)
+    specs = [s for s, _ in insts]
+    bs = BatchSolver(specs, m=5, eta=0.1)
+    res = bs.solve(np.zeros(bs.total), tol=1e-12, maxit=8000)
+    ref_conv = gnorm <= 1e-12
+    must = ref_conv & (its <= 6000)
+    assert must.sum() >= 150
+    assert res.converged[must].all(), np.flatnonzero(must & ~res.converged)
+    assert not res.converged[~ref_conv].any(), np.flatnonzero(~ref_conv & res.converged)
+    xs = bs.split(res.x)
+    for i in np.flatnonzero(res.converged):
+        spec = specs[i]
+        o = Oracle(spec)
+        inner = spec.lattice.interior_mask()
+        o.residual(xr[offs[i]:offs[i + 1]])
+        want = [o.phi(k)[inner] for k in range(len(spec.segments))]
+        assert abs(o.free_energy() - Fr[i]) <= 1e-12 * max(1.0, abs(Fr[i]))
+        f = o.residual(xs[i])
+        assert np.linalg.norm(f) <= 1e-11, (i, np.linalg.norm(f))
+        for k in range(len(spec.segments)):
+            if np.max(np.abs(want[k])) > 0:
+                assert np.max(np.abs(o.phi(k)[inner] - want[k])) <= 1e-10 * np.max(np.abs(want[k])), (i, k)
+        assert abs(o.free_energy() - Fr[i]) <= 1e-9 * max(1.0, abs(Fr[i])), i
 
 
 def test_batch_equals_single_system(gpu_lib):
@@ -54,6 +99,17 @@ def test_batch_equals_single_system(gpu_lib):
         assert r.converged
         assert abs(r.iterations - res.iterations[i]) <= 2
         np.testing.assert_allclose(bs.split(res.x)[i], r.x, rtol=0, atol=1e-7)
+        # converged tighter, both forms reach the same profiles to 1e-10
+    res12 = bs.solve(np.concatenate([x for _, x in insts]), tol=1e-12, maxit=4000)
+    assert res12.converged.all()
+    for i, (spec, x0) in enumerate(insts):
+        s = System(spec)
+        r = s.solve(x0, tol=1e-12, maxit=4000, m=10, eta=0.1)
+        assert r.converged
+        inner = spec.lattice.interior_mask()
+        for seg in range(len(spec.segments)):
+            want = s.phi(seg)[inner]
+            assert np.max(np.abs(bs.phi(i, seg)[inner] - want)) <= 1e-10 * max(1e-300, np.max(np.abs(want)))
 
 
 def test_batch_reports_nonconvergence(gpu_lib):
