@@ -1,15 +1,25 @@
-"""Benchmark: converged SCF solves per second on the cylindrical diblock
-system (Lat2DCyl1stO 128x128, A20B20 in W, phibulk 0.005, chi_AW 1.6,
-seeded micelle + N(0, 0.1) noise, residual < 1e-7).
+"""Benchmark: converged SCF solves per second.
 
-One step = one batch of seeded instances of that system solved to
-convergence.  ``--form chosen`` runs the batched persistent solver
-(one launch per batch), ``--form plain`` the per-instance host-driven
-Pure_DIIS with one launch per propagator step.  ``--impl reference`` times
-the CPU restatement of SFbox's solver on the host cores (SFbox itself cannot
-be built here).  Under torchrun every rank solves its own instances (weak
-scaling, no data-path collective); the timed region is bracketed by a barrier
-and a synchronize and the max over ranks is reported.
+Default workload (the headline): the cylindrical diblock system
+(Lat2DCyl1stO 128x128, A20B20 in W, phibulk 0.005, chi_AW 1.6, seeded micelle
++ N(0, 0.1) noise, residual < 1e-7).  ``--config c4`` runs the batching
+configuration instead: 256 uneven Lat1DFlat1stO instances (layers 50..400,
+N 20..1000) from x = 0.
+
+One step = one batch of instances solved to convergence.  ``--form chosen``
+runs the batched persistent solver (one launch per batch), ``--form plain``
+the per-instance host-driven form.  The line also carries ``plain_gpu_form``:
+per-instance Pure_DIIS with one launch per propagator step on the cylinder,
+SFbox's own Newton iteration (pseudohessian) over the device residual on the
+1D instances, where its dense Hessian fits.
+
+``--impl reference`` times SFbox itself -- the reference's C++ sources built
+by oracle/refbuild (oracle/_ref/sfref) -- on all host cores, one process per
+instance, on the same systems and settings; without that build it times the
+CPU restatement (oracle) instead and says so.  Under torchrun every rank
+solves its own instances, split by estimated cost (weak scaling, no
+data-path collective); the timed region is bracketed by a barrier and a
+synchronize and the max over ranks is reported.
 """
 from __future__ import annotations
 
@@ -19,19 +29,28 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "cyl_micelle Lat2DCyl1stO 128x128 (r,z), (A)20(B)20 + W solvent, phibulk 0.005, chi_AW 1.6"
 METRIC = "converged SCF solves/s (resid<1e-7)"
-# ncu: 93.36 GB read + 76.00 GB written by one batch_diis_kernel launch of
-# 148 instances that made 148 * (33.63 + 1) residual evaluations
-DRAM_BYTES_PER_INSTANCE_ITERATION = (93.365e9 + 76.002e9) / (148 * 34.63)
+SFREF = os.path.join(ROOT, "oracle", "_ref", "sfref")
 TOL = 1e-7
-DIIS_M, DIIS_ETA, MAXIT = 10, 0.1, 2000
+
+# workload table: one entry per benchmarked configuration
+WORKLOADS = {
+    "c2": {"name": "cyl_micelle Lat2DCyl1stO 128x128 (r,z), (A)20(B)20 + W solvent, phibulk 0.005, chi_AW 1.6",
+           "m": 10, "eta": 0.1, "maxit": 2000},
+    "c4": {"name": "sweep1d: 256 uneven Lat1DFlat1stO instances (layers 50..400, N 20..1000 log-uniform, "
+                   "chi_AW grid over [0,1], phibulk 1e-4..1e-1, chi_AS -2..0), (A)N + W at a frozen surface, x0 = 0",
+           "m": 5, "eta": 0.1, "maxit": 5000},
+}
+# ncu: 93.36 GB read + 76.00 GB written by one batch_diis_kernel launch of
+# 148 cylinder instances that made 148 * (33.63 + 1) residual evaluations
+DRAM_BYTES_PER_INSTANCE_ITERATION_C2 = (93.365e9 + 76.002e9) / (148 * 34.63)
 
 
 def parse():
@@ -40,16 +59,41 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--form", default="chosen", choices=["chosen", "plain"])
     ap.add_argument("--batch", type=int, default=0, help="instances per rank per step (0: form default)")
     ap.add_argument("--cpu-sample", type=int, default=8, help="instances in the CPU-baseline sample")
+    ap.add_argument("--plain-sample", type=int, default=16, help="instances timed in the plain GPU form")
     return ap.parse_args()
 
 
-def instances(rank: int, count: int):
+# ---------------------------------------------------------------------------
+# instances: (spec, x0, SFbox input text) per instance
+def instances(config: str, rank: int, world: int, count: int):
     from field_b200 import configs
-    from field_b200.shard import instance_seeds
-    return [configs.cyl_micelle(seed=sd) for sd in instance_seeds(rank, count, configs.BASE_SEED + 2)]
+    if config == "c2":
+        from field_b200.shard import instance_seeds
+        w = WORKLOADS["c2"]
+        text = configs.cyl_micelle_input(m=w["m"], eta=w["eta"], tol=TOL, maxit=w["maxit"])
+        out = []
+        for sd in instance_seeds(rank, count, configs.BASE_SEED + 2):
+            spec, x0 = configs.cyl_micelle(seed=sd)
+            out.append((spec, x0, text))
+        return out
+    from field_b200.shard import estimate_cost, partition
+    texts = configs.sweep1d_inputs(count=256, tolerance=TOL)
+    allinst = [(s, x, t) for (s, x), t in zip(configs.sweep1d(count=256), texts)]
+    parts = partition([estimate_cost(s) for s, _, _ in allinst], world)
+    mine = [allinst[i] for i in parts[rank]]
+    return mine[:count] if count else mine
+
+
+def reference_text(config: str, text: str) -> str:
+    """The SFbox input of one instance with the bench's solver settings."""
+    w = WORKLOADS[config]
+    if config == "c4":
+        text = text.replace("start\n", f"newton : isaac : iterationlimit : {w['maxit']}\nstart\n")
+    return text
 
 
 # ---------------------------------------------------------------------------
@@ -105,84 +149,150 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(sample: int):
-    """The oracle (CPU restatement of SFbox's Pure_DIIS solve) on one core."""
-    from oracle.oracle import Oracle
-    insts = instances(0, sample)
-    t0 = time.perf_counter()
-    ok = 0
-    for spec, x0 in insts:
-        o = Oracle(spec)
-        _, rc, _, _ = o.solve_diis(x0, tol=TOL, maxit=MAXIT, m=DIIS_M, eta=DIIS_ETA)
-        ok += (rc == 0)
-    dt = time.perf_counter() - t0
-    return {"value": ok / dt, "unit": "solves/s", "cores": 1, "kind": "port",
-            "sample": f"{sample} seeded instances of the workload solved to 1e-7 by the oracle's Pure_DIIS "
-                      f"(m={DIIS_M}, eta={DIIS_ETA}) sequentially on one host core, {dt:.1f} s"}
+# CPU legs: SFbox itself (oracle/_ref/sfref) when built, else the oracle port
+def _sfbox_solve(args):
+    """One instance solved by SFbox's own Pure_DIIS in a child process; 1 if
+    it stopped on its tolerance test with finite numbers."""
+    text, x0_bytes = args
+    import numpy as np
+    with tempfile.TemporaryDirectory() as wd:
+        inp, xf, out = (os.path.join(wd, n) for n in ("c.in", "c.x", "c.out"))
+        with open(inp, "w") as f:
+            f.write(text)
+        with open(xf, "wb") as f:
+            f.write(x0_bytes)
+        r = subprocess.run([SFREF, "solve", inp, xf, out], capture_output=True, text=True, cwd=wd)
+        if r.returncode != 0:
+            return 0
+        its = [int(ln.split()[2]) for ln in r.stdout.splitlines() if ln.startswith("i = ")]
+        g = None
+        for line in open(out):
+            p = line.split()
+            if p[0] == "g":
+                g = np.array([float(v) for v in p[2:]])
+    maxit = int(text.split("iterationlimit : ")[1].split()[0]) if "iterationlimit : " in text else 5000
+    ok = g is not None and bool(np.all(np.isfinite(g))) and (not its or its[-1] < maxit)
+    return int(ok)
 
 
-def _ref_worker(args):
-    idx, = args
+def _port_solve(args):
+    """One instance solved by the oracle's Pure_DIIS (the CPU restatement)."""
+    text, x0_bytes = args
     sys.path.insert(0, ROOT)
-    from field_b200 import configs
+    import numpy as np
+    from field_b200.sfinput import build_system, parse_input
     from oracle.oracle import Oracle
-    spec, x0 = configs.cyl_micelle(seed=configs.BASE_SEED + 2 + idx)
-    o = Oracle(spec)
-    _, rc, _, _ = o.solve_diis(x0, tol=TOL, maxit=MAXIT, m=DIIS_M, eta=DIIS_ETA)
+    spec, st = build_system(parse_input(text)[0])
+    x0 = np.frombuffer(x0_bytes, dtype="<f8").copy()
+    _, rc, _, _ = Oracle(spec).solve_diis(x0, tol=st.tolerance, maxit=st.iterationlimit, m=st.m, eta=st.deltamax)
     return int(rc == 0)
 
 
+def _cpu_kind():
+    return "reference" if os.path.exists(SFREF) else "port"
+
+
+def _cpu_jobs(config, insts):
+    import numpy as np
+    return [(reference_text(config, t), np.ascontiguousarray(x, dtype="<f8").tobytes()) for _, x, t in insts]
+
+
+def cpu_baseline(config: str, sample: int):
+    """SFbox (or the port) on one host core over a bounded sample."""
+    insts = instances(config, 0, 1, 0)[:sample] if config == "c4" else instances(config, 0, 1, sample)
+    fn = _sfbox_solve if _cpu_kind() == "reference" else _port_solve
+    jobs = _cpu_jobs(config, insts)
+    t0 = time.perf_counter()
+    ok = sum(fn(j) for j in jobs)
+    dt = time.perf_counter() - t0
+    what = "SFbox built from its own sources (oracle/_ref/sfref), Pure_DIIS" if fn is _sfbox_solve else \
+        "the oracle's restatement of SFbox's Pure_DIIS"
+    w = WORKLOADS[config]
+    return {"value": ok / dt, "unit": "solves/s", "cores": 1, "kind": _cpu_kind(),
+            "sample": f"{len(jobs)} instances of the workload solved to 1e-7 by {what} (m={w['m']}, "
+                      f"eta={w['eta']}) sequentially on one host core, {dt:.1f} s, {ok} converged"}
+
+
 def run_reference(a, rank, world):
-    """--impl reference: the CPU restatement on all host cores (SFbox cannot
-    be built here: it needs the absent 'fenk' library and CLAPACK)."""
+    """--impl reference: SFbox itself on all host cores of rank 0."""
     import multiprocessing as mp
     if rank != 0:
         return None
     cores = os.cpu_count() or 1
+    kind = _cpu_kind()
+    fn = _sfbox_solve if kind == "reference" else _port_solve
+    if a.config == "c2":
+        def jobs_for(k):
+            from field_b200 import configs
+            w = WORKLOADS["c2"]
+            text = configs.cyl_micelle_input(m=w["m"], eta=w["eta"], tol=TOL, maxit=w["maxit"])
+            out = []
+            for i in range(cores):
+                _, x0 = configs.cyl_micelle(seed=configs.BASE_SEED + 2 + 1000 + k * cores + i)
+                out.append((text, x0.astype("<f8").tobytes()))
+            return out
+        per_step = cores
+    else:
+        # one step is the whole sweep, as the batched launch solves it
+        allj = _cpu_jobs("c4", instances("c4", 0, 1, 0))
+
+        def jobs_for(k):
+            return allj
+        per_step = len(allj)
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        per_step = cores
         for w in range(a.warmup):
-            pool.map(_ref_worker, [(i,) for i in range(per_step)])
+            pool.map(fn, jobs_for(10_000 + w))
         times, solved = [], 0
         for k in range(a.steps):
+            jobs = jobs_for(k)
             t0 = time.perf_counter()
-            solved += sum(pool.map(_ref_worker, [(1000 + k * per_step + i,) for i in range(per_step)]))
+            solved += sum(pool.map(fn, jobs))
             times.append(time.perf_counter() - t0)
     total = sum(times)
     value = solved / total
+    w = WORKLOADS[a.config]
+    what = "SFbox built from its own sources (oracle/_ref/sfref), one process per instance" if kind == "reference" \
+        else "the oracle's restatement of SFbox (oracle/_ref/sfref not built), one process per instance"
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1000 * total / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD, "instances_per_step": per_step, "method": "Pure_DIIS",
-                       "tolerance": TOL},
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
-                             "sample": f"{per_step} instances per step on {cores} spawned processes"},
+            "config": {"workload": w["name"], "instances_per_step": per_step,
+                       "method": "Pure_DIIS, m=%d, eta=%g" % (w["m"], w["eta"]), "tolerance": TOL},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": kind,
+                             "sample": f"{per_step} instances per step on {cores} spawned processes: {what}"},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return line
 
 
 # ---------------------------------------------------------------------------
-def plain_form(insts, stream, steps=1):
-    """Per-instance host-driven Pure_DIIS with one launch per propagator step
-    (the plain GPU form); returns solves/s."""
+def plain_form(config, insts, stream, steps=1):
+    """Per-instance host-driven GPU form: Pure_DIIS with one launch per
+    propagator step on the cylinder, SFbox's Newton iteration over the device
+    residual on the 1D instances.  Returns (solves/s, a System, iterations,
+    converged)."""
     import torch
     from field_b200.system import System
-    systems = [System(s) for s, _ in insts]
+    w = WORKLOADS[config]
+    systems = [System(s) for s, _, _ in insts]
     for s in systems:
         s.use_stream(stream.cuda_stream)
-    x_host = [torch.from_numpy(x0).pin_memory() for _, x0 in insts]
+    x_host = [torch.from_numpy(x0).pin_memory() for _, x0, _ in insts]
 
     def run():
         conv, iters = 0, 0
         for s, xh in zip(systems, x_host):
-            r = s.solve(xh.numpy(), tol=TOL, maxit=MAXIT, m=DIIS_M, eta=DIIS_ETA)
+            if config == "c4":
+                r = s.solve_newton(xh.numpy(), tol=TOL, maxit=w["maxit"])
+            else:
+                r = s.solve(xh.numpy(), tol=TOL, maxit=w["maxit"], m=w["m"], eta=w["eta"])
             conv += r.converged
             iters += r.iterations
         return conv, iters
-    run()
+    if config == "c2":
+        run()        # warm-up (the 1D Newton form is timed once: its solves take seconds)
     torch.cuda.synchronize()
     t = 0.0
     conv = iters = 0
@@ -195,7 +305,7 @@ def plain_form(insts, stream, steps=1):
         t += e0.elapsed_time(e1) / 1000.0
         conv += c
         iters += it
-    return conv / t, systems[0], iters
+    return conv / t, systems[0], iters, conv
 
 
 def run_ours(a, rank, world, local_rank):
@@ -204,11 +314,17 @@ def run_ours(a, rank, world, local_rank):
     import torch.distributed as dist
     from field_b200 import batch as fbatch
 
+    cfg = a.config
+    w = WORKLOADS[cfg]
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream()
-    B = a.batch or (fbatch.default_batch() if a.form == "chosen" else 4)
-    insts = instances(rank, B)
+    if cfg == "c2":
+        B = a.batch or (fbatch.default_batch() if a.form == "chosen" else 4)
+        insts = instances(cfg, rank, world, B)
+    else:
+        insts = instances(cfg, rank, world, a.batch)
+        B = len(insts)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > 126 MB L2
 
     def barrier():
@@ -217,14 +333,14 @@ def run_ours(a, rank, world, local_rank):
 
     solver = None
     if a.form == "chosen":
-        solver = fbatch.BatchSolver([s for s, _ in insts], method="diis", m=DIIS_M, eta=DIIS_ETA)
+        solver = fbatch.BatchSolver([s for s, _, _ in insts], method="diis", m=w["m"], eta=w["eta"])
         solver.use_stream(stream.cuda_stream)
-        x_all = np.concatenate([x for _, x in insts])
+        x_all = np.concatenate([x for _, x, _ in insts])
         x_pinned = torch.from_numpy(x_all).pin_memory()
         y_pinned = torch.empty_like(x_pinned).pin_memory()
         for _ in range(a.warmup):
             solver.load(x_all)
-            solver.solve_resident(TOL, MAXIT)
+            solver.solve_resident(TOL, w["maxit"])
             solver.results()
     torch.cuda.synchronize()
 
@@ -241,7 +357,7 @@ def run_ours(a, rank, world, local_rank):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            solver.solve_resident(TOL, MAXIT)
+            solver.solve_resident(TOL, w["maxit"])
             e1.record(stream)
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1000.0)
@@ -251,8 +367,7 @@ def run_ours(a, rank, world, local_rank):
             kms.append(solver.kernel_ms())
         last_iters = res.iterations
     else:
-        v, prof_sys, iters_total = plain_form(insts, stream, steps=a.steps)
-        conv_total = len(insts) * a.steps
+        v, prof_sys, iters_total, conv_total = plain_form(cfg, insts, stream, steps=a.steps)
         times = [conv_total / v]
     barrier()
     torch.cuda.synchronize()
@@ -262,7 +377,7 @@ def run_ours(a, rank, world, local_rank):
     value = solved_all / t_max
 
     # e2e through the public API: pinned host guesses in, iterates out, every step
-    h2d = sum(x.size for _, x in insts) * 8
+    h2d = sum(x.size for _, x, _ in insts) * 8
     if a.form == "chosen":
         et, econv = 0.0, 0
         for _ in range(a.steps):
@@ -270,7 +385,7 @@ def run_ours(a, rank, world, local_rank):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            r = solver.solve(x_pinned.numpy(), tol=TOL, maxit=MAXIT, out=y_pinned.numpy())
+            r = solver.solve(x_pinned.numpy(), tol=TOL, maxit=w["maxit"], out=y_pinned.numpy())
             e1.record(stream)
             torch.cuda.synchronize()
             et += e0.elapsed_time(e1) / 1000.0
@@ -280,40 +395,48 @@ def run_ours(a, rank, world, local_rank):
     else:
         e2e_value = value
     e2e = {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
-           "note": "sfgpu_batch_solve / sfgpu_solve_diis on pinned host arrays; copies inside every timed step"}
+           "note": "sfgpu_batch_solve / per-instance solves on pinned host arrays; copies inside every timed step"}
 
-    # plain GPU form on a few instances of the same workload, same run
+    # plain GPU form on a sample of the same workload, same run
     plain = None
     if a.form == "chosen":
-        pv, prof_sys, _ = plain_form(instances(rank, 2), stream, steps=1)
-        plain = {"value": pv, "unit": "solves/s", "instances": 2,
-                 "form": "per-instance host-driven Pure_DIIS, one launch per propagator step"}
+        ns = min(a.plain_sample, len(insts))
+        pv, prof_sys, _, pconv = plain_form(cfg, insts[:ns], stream, steps=1)
+        plain = {"value": pv, "unit": "solves/s", "instances": ns, "converged": int(pconv),
+                 "form": ("per-instance host-driven Pure_DIIS, one launch per propagator step" if cfg == "c2" else
+                          "per-instance SFbox Newton iteration (pseudohessian, Scheutjens step search) "
+                          "over the device residual, host-driven")}
         kp_bytes = solver.algorithmic_bytes(last_iters)
-        # DRAM traffic measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-        # on one launch of 148 instances of this workload, per instance and
-        # DIIS iteration, scaled to this launch's iterations
-        traffic = DRAM_BYTES_PER_INSTANCE_ITERATION * float(sum(int(i) + 1 for i in last_iters))
-        solver.kernel_profile = {"kernel": "batch_diis_kernel (persistent, one launch per batch solve)",
-                                 "bytes": kp_bytes, "ms": statistics.median(kms), "traffic": traffic,
-                                 "traffic_source": "ncu capture of 148 instances, scaled by residual evaluations"}
+        prof_k = {"kernel": "batch_diis_kernel (persistent, one launch per batch solve)",
+                  "bytes": kp_bytes, "ms": statistics.median(kms)}
+        if cfg == "c2":
+            # DRAM traffic measured by ncu (dram__bytes_read.sum +
+            # dram__bytes_write.sum) on one launch of 148 instances of this
+            # workload, per instance and DIIS iteration, scaled to this
+            # launch's iterations
+            prof_k["traffic"] = DRAM_BYTES_PER_INSTANCE_ITERATION_C2 * float(sum(int(i) + 1 for i in last_iters))
+            prof_k["traffic_source"] = "ncu capture of 148 instances, scaled by residual evaluations"
+        solver.kernel_profile = prof_k
     prof = prof_sys.profile_propagator(reps=400)
     roof = fbatch.roofline(prof, a.form, solver)
     if a.form == "chosen":
         roof["per_step_kernel"] = fbatch.roofline(prof, "plain", None)
 
     if rank == 0:
-        cpu = cpu_baseline(a.cpu_sample)
+        cpu = cpu_baseline(cfg, a.cpu_sample) if world == 1 else None
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": 1000 * t_max / a.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "form": a.form, "instances_per_rank_per_step": B,
-                           "method": "Pure_DIIS, m=%d, eta=%g" % (DIIS_M, DIIS_ETA),
-                           "tolerance": TOL, "converged": int(solved_all),
+                "config": {"workload": w["name"], "form": a.form, "instances_per_rank_per_step": B,
+                           "method": "Pure_DIIS, m=%d, eta=%g" % (w["m"], w["eta"]),
+                           "tolerance": TOL, "iteration_limit": w["maxit"], "converged": int(solved_all),
                            "mean_iterations": iters_total / max(1, conv_total),
                            "l2": "256 MB buffer written between timed steps",
                            "parallelism": f"instances x{world}"},
-                "e2e": e2e, "roofline": roof, "plain_gpu_form": plain, "cpu_baseline": cpu, "clocks": clocks,
-                "gpu_launches": fbatch.launch_count(a.form, iters_total, insts, solver)}
+                "e2e": e2e, "roofline": roof, "plain_gpu_form": plain,
+                "chosen_over_plain": (value / plain["value"]) if plain and plain["value"] > 0 else None,
+                "cpu_baseline": cpu, "clocks": clocks,
+                "gpu_launches": fbatch.launch_count(a.form, iters_total, [(s, x) for s, x, _ in insts], solver)}
         print(json.dumps(line), flush=True)
 
 

@@ -89,6 +89,43 @@ def cyl_micelle(nx=128, ny=128, nA=20, nB=20, phib=0.005, chi_aw=1.6, chi_bw=0.0
     return spec, x
 
 
+CYL_INPUT = """\
+lat : cyl : gradients : 2
+lat : cyl : geometry : cylindrical
+lat : cyl : n_layers_x : {nx}
+lat : cyl : n_layers_y : {ny}
+lat : cyl : lambda : 0.16666666666666667
+lat : cyl : lowerbound_x : mirror1
+lat : cyl : upperbound_x : mirror1
+lat : cyl : lowerbound_y : mirror1
+lat : cyl : upperbound_y : mirror1
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : {chi_aw!r}
+mon : B : chi - W : {chi_bw!r}
+mol : AB : composition : (A){nA}(B){nB}
+mol : AB : freedom : free
+mol : AB : phibulk : {phib!r}
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : m : {m}
+newton : isaac : deltamax : {eta!r}
+newton : isaac : tolerance : {tol!r}
+newton : isaac : iterationlimit : {maxit}
+start
+"""
+
+
+def cyl_micelle_input(nx=128, ny=128, nA=20, nB=20, phib=0.005, chi_aw=1.6, chi_bw=0.0, m=10, eta=0.1,
+                      tol=1e-7, maxit=2000):
+    """The SFbox input file of cyl_micelle's system (the iteration variables'
+    initial guess is cyl_micelle's x, passed separately)."""
+    return CYL_INPUT.format(nx=nx, ny=ny, nA=nA, nB=nB, phib=phib, chi_aw=chi_aw, chi_bw=chi_bw, m=m, eta=eta,
+                            tol=tol, maxit=maxit)
+
+
 def melt3d(n=128, nA=50, nB=50, chi_ab=0.2, amp=0.05, seed=BASE_SEED + 3):
     lat = Lattice(gradients=3, n_layers=[n, n, n], bound_lo=[BOUND_PERIODIC] * 3, bound_hi=[BOUND_PERIODIC] * 3)
     segs = [Segment("A"), Segment("B")]
