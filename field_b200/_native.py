@@ -19,6 +19,7 @@ PROTOTYPES = {
     "sfgpu_last_error": (C.c_char_p, []),
     "sfgpu_device_count": (i32, [ip]),
     "sfgpu_system_create": (i32, [vp, C.POINTER(vp)]),
+    "sfgpu_system_create_checkpointed": (i32, [vp, i32, C.POINTER(vp)]),
     "sfgpu_system_destroy": (i32, [vp]),
     "sfgpu_system_info": (i32, [vp, ip, ip, ip, ip]),
     "sfgpu_system_stream": (i32, [vp, C.POINTER(vp)]),
@@ -44,10 +45,12 @@ PROTOTYPES = {
     "sfgpu_lat_norm_phi_free": (i32, [vp, vp, f64]),
     "sfgpu_lat_norm_phi_restr": (i32, [vp, vp, vp, i32, f64]),
     "sfgpu_solve_diis": (i32, [vp, dp, f64, i32, i32, f64, ip, dp]),
+    "sfgpu_solve_diis_many": (i32, [i32, C.POINTER(vp), C.POINTER(dp), f64, i32, i32, f64, i32, ip, ip, dp]),
     "sfgpu_newton_default_settings": (i32, [vp]),
     "sfgpu_solve_newton": (i32, [vp, dp, vp, ip, ip, dp]),
     "sfgpu_profile_propagator": (i32, [vp, i32, dp, dp, dp, dp]),
     "sfgpu_system_set_tile": (i32, [vp, i32]),
+    "sfgpu_system_set_tile_pipelined": (i32, [vp, i32]),
     "sfgpu_jvp": (i32, [vp, vp, vp, vp, vp]),
     "sfgpu_jvp_host": (i32, [vp, dp, dp, dp, dp]),
     "sfgpu_solve_nk": (i32, [vp, dp, f64, i32, i32, ip, ip, dp]),

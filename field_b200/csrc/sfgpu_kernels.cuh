@@ -148,6 +148,93 @@ step3d_march(DLat L, const double *__restrict__ gin, const double *__restrict__ 
     }
 }
 
+// The same x-marching step software-pipelined: the loads of plane x+1 (the
+// column value two planes ahead, G, and for a composition phi and the other
+// propagator) are issued before plane x is computed, so every thread keeps a
+// plane's worth of loads in flight across the barrier, and the (z, y) tile is
+// double-buffered so one barrier per plane suffices (a thread writes buffer
+// b^1 for plane x+1 only after every thread passed plane x's barrier, i.e.
+// finished reading b^1 for plane x-1).  Same operands and operation order as
+// step3d_march, so the results are bit-identical.
+static __global__ void __launch_bounds__(kTZ * kTY)
+step3d_march_pf(DLat L, const double *__restrict__ gin, const double *__restrict__ G,
+                double *__restrict__ gout, const double *__restrict__ other, double *__restrict__ phi,
+                int mode, int xc) {
+    __shared__ double tile[2][kTY + 2][kTZ + 2];
+    const int nx = L.Md[0] - 2, ny = L.Md[1] - 2, nz = L.Md[2] - 2;
+    const int jx = L.st[0], jy = L.st[1];
+    const int tz = threadIdx.x % kTZ, ty = threadIdx.x / kTZ;
+    const int z = blockIdx.x * kTZ + tz + 1;
+    const int y = blockIdx.y * kTY + ty + 1;
+    const int x0 = blockIdx.z * xc + 1;
+    if (x0 > nx) return;
+    const int x1 = min(x0 + xc - 1, nx);
+    const bool act = (z <= nz) && (y <= ny);
+    const int zm = lat_mapc(L, 2, z - 1), zp = lat_mapc(L, 2, z + 1);
+    const int ym = lat_mapc(L, 1, y - 1), yp = lat_mapc(L, 1, y + 1);
+    const bool hz0 = (tz == 0), hz1 = (tz == kTZ - 1) || (z == nz);
+    const bool hy0 = (ty == 0), hy1 = (ty == kTY - 1) || (y == ny);
+    const int col = y * jy + z;
+    const bool acc_mode = (mode == COMP_ACC), centre = (mode == COMP_CENTRE);
+    // registers: column values of planes x-1, x, x+1; plane x's G, halos and
+    // composition operands
+    double vprev = 0, vcur = 0, vnext = 0, g = 0, hzl = 0, hzh = 0, hyl = 0, hyh = 0, ot = 0, ph = 0;
+    if (act) {
+        const int base = x0 * jx;
+        vprev = gin[lat_mapc(L, 0, x0 - 1) * jx + col];
+        vcur = gin[base + col];
+        vnext = gin[lat_mapc(L, 0, x0 + 1) * jx + col];
+        g = G[base + col];
+        if (hz0) hzl = gin[base + y * jy + zm];
+        if (hz1) hzh = gin[base + y * jy + zp];
+        if (hy0) hyl = gin[base + ym * jy + z];
+        if (hy1) hyh = gin[base + yp * jy + z];
+        if (acc_mode) { ot = other[base + col]; ph = phi[base + col]; }
+        else if (centre) ph = phi[base + col];
+    }
+    int b = 0;
+    for (int x = x0; x <= x1; x++) {
+        // loads of plane x+1, in flight while plane x is computed
+        double vn2 = 0, gn = 0, nzl = 0, nzh = 0, nyl = 0, nyh = 0, otn = 0, phn = 0;
+        const bool more = x < x1;
+        if (act && more) {
+            const int nb = (x + 1) * jx;
+            vn2 = gin[lat_mapc(L, 0, x + 2) * jx + col];
+            gn = G[nb + col];
+            if (hz0) nzl = gin[nb + y * jy + zm];
+            if (hz1) nzh = gin[nb + y * jy + zp];
+            if (hy0) nyl = gin[nb + ym * jy + z];
+            if (hy1) nyh = gin[nb + yp * jy + z];
+            if (acc_mode) { otn = other[nb + col]; phn = phi[nb + col]; }
+            else if (centre) phn = phi[nb + col];
+        }
+        if (act) {
+            tile[b][ty + 1][tz + 1] = vcur;
+            if (hz0) tile[b][ty + 1][0] = hzl;
+            if (hz1) tile[b][ty + 1][tz + 2] = hzh;
+            if (hy0) tile[b][0][tz + 1] = hyl;
+            if (hy1) tile[b][ty + 2][tz + 1] = hyh;
+        }
+        __syncthreads();
+        if (act) {
+            double acc = vprev * g;
+            acc += vnext * g;
+            acc += tile[b][ty][tz + 1] * g;
+            acc += tile[b][ty + 2][tz + 1] * g;
+            acc += tile[b][ty + 1][tz] * g;
+            acc += tile[b][ty + 1][tz + 2] * g;
+            const double out = acc * (1.0 / 6.0);
+            const int t = x * jx + col;
+            gout[t] = out;
+            if (acc_mode) phi[t] = ph + out * ot;
+            else if (centre) phi[t] = (ph + out * out) * 0.5;
+        }
+        vprev = vcur; vcur = vnext; vnext = vn2;
+        g = gn; hzl = nzl; hzh = nzh; hyl = nyl; hyh = nyh; ot = otn; ph = phn;
+        b ^= 1;
+    }
+}
+
 // One second-order step (Lat3D2ndO::PropagateF, Lat3D2ndO.cpp:65-152, and
 // PropagateB, :597-678) for the six direction components, with boundary
 // components swapped at mirrors (SetBx1(gz0,gz5)..., Lat3D2ndO.cpp:84-89) and

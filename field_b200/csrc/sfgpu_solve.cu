@@ -164,3 +164,42 @@ extern "C" int sfgpu_solve_diis(sfgpu_system *s, double *x_host, double tol, int
     if (rc == SFGPU_OK && !(err <= tol)) rc = SFGPU_ERR_NOTCONVERGED;
     return rc;
 }
+
+// Many systems solved concurrently: each by sfgpu_solve_diis on its own
+// stream, driven by its own host thread, so the device interleaves the
+// systems' kernels and each system's per-iteration host round trip hides
+// behind the others' work.  For instances large enough to fill the GPU one
+// step at a time (3D second order), where a block per instance would leave
+// most SMs idle.
+#include <atomic>
+#include <thread>
+
+extern "C" int sfgpu_solve_diis_many(int n, sfgpu_system *const *systems, double *const *x, double tol, int maxit,
+                                     int m, double eta, int threads, int *status, int *iterations, double *errors) {
+    if (n < 1 || !systems || !x || !status) return SFGPU_ERR_INVALID;
+    for (int i = 0; i < n; i++)
+        if (!systems[i] || !x[i]) return SFGPU_ERR_INVALID;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) { sfgpu_set_error(e, "cudaGetDevice", __FILE__, __LINE__); return SFGPU_ERR_CUDA; }
+    const int nt = std::max(1, std::min(threads > 0 ? threads : n, n));
+    std::atomic<int> next(0);
+    auto worker = [&]() {
+        cudaSetDevice(dev);
+        for (int i = next++; i < n; i = next++) {
+            int it = 0;
+            double err = 0;
+            status[i] = sfgpu_solve_diis(systems[i], x[i], tol, maxit, m, eta, &it, &err);
+            if (iterations) iterations[i] = it;
+            if (errors) errors[i] = err;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+    for (int i = 0; i < n; i++)
+        if (status[i] != SFGPU_OK && status[i] != SFGPU_ERR_NOTCONVERGED && status[i] != SFGPU_ERR_NONFINITE)
+            return status[i];
+    return SFGPU_OK;
+}

@@ -51,7 +51,10 @@ int sfgpu_system::launch_step1(const double *gin, const double *G, double *gout,
     const DLat &L = H.L;
     if (L.grad == 3 && !lat_twelve(L)) {
         dim3 grid((L.Md[2] - 2 + kTZ - 1) / kTZ, (L.Md[1] - 2 + kTY - 1) / kTY, (L.Md[0] - 2 + tile_xc - 1) / tile_xc);
-        step3d_march<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, tile_xc);
+        if (tile_pipelined)
+            step3d_march_pf<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, tile_xc);
+        else
+            step3d_march<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, tile_xc);
     } else {
         step1_rows<<<grid_rows(L), kBlock, 0, stream>>>(L, gin, G, gout, other, phi, mode);
     }
@@ -529,6 +532,10 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
         o.d_phi.assign(nseg, nullptr);
         for (int i : o.used) if ((rc = alloc_d(&o.d_phi[i], M))) return rc;
         size_t need = (o.type == 0) ? 0 : (size_t)(o.dend ? o.nshort : o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
+        if (primal_checkpointed(o)) {
+            const int k = primal_stride;
+            need = (size_t)((o.N + k - 1) / k + k) * K * M;   // checkpoints + one segment
+        }
         store = std::max(store, need);
     }
     if ((rc = alloc_d(&d_gi, store))) return rc;
@@ -877,61 +884,83 @@ int sfgpu_system::molecule_phi(int m) {
     }
     // full storage: copolymers and all second-order chains
     const int N = o.N;
-    replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[0]], d_gi);
-    if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, d_gi);
-    for (int t = 1; t < N; t++) {
+    // forward step into position t (SF_Copol1stO::Matrix1 / SF_Copol2ndO::Matrix1)
+    auto fwd = [&](int t, const double *in, double *out) {
         int sg = o.seg[t];
         if (K == 1 && o.force != 0)   // SF_Copol1stO.cpp:1207-1211: PropagateG(Gi, G, s, force)
-            step1_force_rows<<<grid_rows(L), kBlock, 0, s>>>(L, force_weights(L, o.force), d_gi + (size_t)(t - 1) * KM,
-                                                             d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
+            step1_force_rows<<<grid_rows(L), kBlock, 0, s>>>(L, force_weights(L, o.force), in, d_gseg[sg], out,
+                                                             nullptr, nullptr, COMP_NONE);
         else if (K == 1)
-            launch_step1(d_gi + (size_t)(t - 1) * KM, d_gseg[sg], d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE);
+            launch_step1(in, d_gseg[sg], out, nullptr, nullptr, COMP_NONE);
         else if (K == 6 && L.stiff) {
             // SF_Copol2ndO_stiff_range::Matrix1 (SF_Copol2ndO_stiff_range.cpp:211-217):
             // step s (1-based) takes Pf(s-1, s+1); the last one is isotropic
             const bool last = (t == N - 1);
             const double Sv = last ? 0.2 : pf[o.seg[t - 1] * nseg + o.seg[t + 1]];
-            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], Sv,
-                                       d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0,
+            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], Sv, out, nullptr, nullptr, COMP_NONE, 0,
                                        last ? STEP2_ISO : STEP2_STIFF);
         } else if (K == 6)
-            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
-                                       d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0);
+            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], out, nullptr,
+                                       nullptr, COMP_NONE, 0);
         else
-            step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * KM, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg],
-                                        d_gi + (size_t)t * KM, nullptr, nullptr, COMP_NONE, 0);
-    }
-    replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[N - 1]], ginv);
-    if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, ginv);
-    connect<<<g, kBlock, 0, s>>>(M, K, ginv, d_gi + (size_t)(N - 1) * KM, o.d_phi[o.seg[N - 1]]);
-    const bool ori = orient && K > 1;
-    if (ori) {
-        for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_ori[i], 0, sizeof(double) * mphi() * M, s));
-        orient_acc<<<g, kBlock, 0, s>>>(L, ginv, d_gi + (size_t)(N - 1) * KM, o.d_ori[o.seg[N - 1]]);
-    }
-    const double *cur = ginv;
-    std::swap(ginv, tmp);
-    for (int t = N - 2; t >= 0; t--) {
+            step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], out,
+                                        nullptr, nullptr, COMP_NONE, 0);
+    };
+    // backward step into position t with the composition phi += Gb(t) Gf(t)
+    auto bwd = [&](int t, const double *in, double *out, const double *gf) {
         int sg = o.seg[t];
         if (K == 1 && o.force != 0)   // backward steps with -force (SF_Copol1stO.cpp:1226-1230)
-            step1_force_rows<<<grid_rows(L), kBlock, 0, s>>>(L, force_weights(L, -o.force), cur, d_gseg[sg], ginv,
-                                                             d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
+            step1_force_rows<<<grid_rows(L), kBlock, 0, s>>>(L, force_weights(L, -o.force), in, d_gseg[sg], out, gf,
+                                                             o.d_phi[sg], COMP_ACC);
         else if (K == 1)
-            launch_step1(cur, d_gseg[sg], ginv, d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC);
+            launch_step1(in, d_gseg[sg], out, gf, o.d_phi[sg], COMP_ACC);
         else if (K == 6 && L.stiff) {
             // backward step s (1-based) takes Pf(s, s+2); the first one
             // (s = N-1) is isotropic (SF_Copol2ndO_stiff_range.cpp:229-234)
             const bool first = (t == N - 2);
             const double Sv = first ? 0.2 : pf[sg * nseg + o.seg[t + 2]];
-            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], Sv, ginv, d_gi + (size_t)t * KM, o.d_phi[sg],
-                                       COMP_ACC, 1, first ? STEP2_ISO : STEP2_STIFF);
+            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], Sv, out, gf, o.d_phi[sg], COMP_ACC, 1,
+                                       first ? STEP2_ISO : STEP2_STIFF);
         } else if (K == 6)
-            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv,
-                                       d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC, 1);
+            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], out, gf,
+                                       o.d_phi[sg], COMP_ACC, 1);
         else
-            step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, cur, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], ginv,
-                                        d_gi + (size_t)t * KM, o.d_phi[sg], COMP_ACC, 1);
-        if (ori) orient_acc<<<g, kBlock, 0, s>>>(L, ginv, d_gi + (size_t)t * KM, o.d_ori[sg]);
+            step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], out, gf,
+                                        o.d_phi[sg], COMP_ACC, 1);
+    };
+    const bool ori = orient && K > 1;
+    // storage: every slice, or checkpoints ck[q] = Gf(qk) plus one segment
+    // of slices seg[j] = Gf(qk + j), j = 1..k-1 (the forward sweep leaves the
+    // last segment there; the others are recomputed from their checkpoint)
+    const bool ckpt = primal_checkpointed(o);
+    const int kst = ckpt ? primal_stride : N;
+    const int nck = ckpt ? (N + kst - 1) / kst : 0;
+    double *segbuf = ckpt ? d_gi + (size_t)nck * KM : nullptr;
+    auto slot = [&](int t) -> double * {
+        if (!ckpt) return d_gi + (size_t)t * KM;
+        return (t % kst == 0) ? d_gi + (size_t)(t / kst) * KM : segbuf + (size_t)(t % kst) * KM;
+    };
+    replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[0]], slot(0));
+    if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, slot(0));
+    for (int t = 1; t < N; t++) fwd(t, slot(t - 1), slot(t));
+    replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[N - 1]], ginv);
+    if (K == 6) set_boundaries<<<g, kBlock, 0, s>>>(L, 6, ginv);
+    connect<<<g, kBlock, 0, s>>>(M, K, ginv, slot(N - 1), o.d_phi[o.seg[N - 1]]);
+    if (ori) {
+        for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_ori[i], 0, sizeof(double) * mphi() * M, s));
+        orient_acc<<<g, kBlock, 0, s>>>(L, ginv, slot(N - 1), o.d_ori[o.seg[N - 1]]);
+    }
+    const double *cur = ginv;
+    std::swap(ginv, tmp);
+    int seg_held = ckpt ? (N - 1) / kst : -1;   // segment whose slices segbuf holds
+    for (int t = N - 2; t >= 0; t--) {
+        if (ckpt && t % kst != 0 && t / kst != seg_held) {
+            const int q = t / kst;   // recompute Gf(qk+1 .. qk+k-1) from ck[q]
+            for (int u = q * kst + 1; u <= std::min(q * kst + kst - 1, N - 1); u++) fwd(u, slot(u - 1), slot(u));
+            seg_held = q;
+        }
+        bwd(t, cur, ginv, slot(t));
+        if (ori) orient_acc<<<g, kBlock, 0, s>>>(L, ginv, slot(t), o.d_ori[o.seg[t]]);
         cur = ginv; std::swap(ginv, tmp);
     }
     wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, cur, d_wgn, d_partial);
@@ -1037,8 +1066,15 @@ extern "C" int sfgpu_device_count(int *count) {
     return n > 0 ? SFGPU_OK : SFGPU_ERR_NODEVICE;
 }
 
-extern "C" int sfgpu_system_create(const sfgpu_system_desc *desc, sfgpu_system **out) {
+// the full-storage chains (copolymers, second-order chains; not dendrimers,
+// not symmetric homopolymers, which store half a chain) when a stride is set
+bool sfgpu_system::primal_checkpointed(const HMol &o) const {
+    return primal_stride > 0 && primal_stride < o.N && o.type != 0 && !o.dend && !o.sym && !logmode;
+}
+
+static int create_system(const sfgpu_system_desc *desc, int stride, sfgpu_system **out) {
     if (!desc || !out) return fail(SFGPU_ERR_INVALID, "null argument");
+    if (stride < 0) return fail(SFGPU_ERR_INVALID, "checkpoint stride must be >= 0");
     *out = nullptr;
     int n = 0;
     if (sfgpu_device_count(&n) != SFGPU_OK) return fail(SFGPU_ERR_NODEVICE, "no CUDA device");
@@ -1046,10 +1082,20 @@ extern "C" int sfgpu_system_create(const sfgpu_system_desc *desc, sfgpu_system *
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete s; sfgpu_set_error(e, "cudaStreamCreate", __FILE__, __LINE__); return SFGPU_ERR_CUDA; }
     s->own_stream = true;
+    // the log-space chains (overflow protection) keep every slice
+    s->primal_stride = desc->overflow_protection ? 0 : stride;
     int rc = s->setup(desc);
     if (rc) { delete s; return rc; }
     *out = s;
     return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_create(const sfgpu_system_desc *desc, sfgpu_system **out) {
+    return create_system(desc, 0, out);
+}
+
+extern "C" int sfgpu_system_create_checkpointed(const sfgpu_system_desc *desc, int stride, sfgpu_system **out) {
+    return create_system(desc, stride, out);
 }
 
 extern "C" int sfgpu_system_destroy(sfgpu_system *s) {
@@ -1395,10 +1441,10 @@ extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fw
     return SFGPU_OK;
 }
 
-// Pick the x-chunk depth of the 3D first-order step by timing each candidate
-// on this system's buffers (CUDA events, `reps` forward + backward steps
-// each); the fastest is kept for all later evaluations.  Other lattices have
-// nothing to tune.
+// Pick the x-chunk depth of the 3D first-order step, and whether the
+// software-pipelined form runs it, by timing each candidate on this system's
+// buffers (CUDA events, `reps` forward + backward steps each); the fastest is
+// kept for all later evaluations.  Other lattices have nothing to tune.
 extern "C" int sfgpu_system_autotune(sfgpu_system *s, int reps, int *chosen_xc, double *best_ms) {
     CHECK_SYS(s);
     if (reps < 1) return fail(SFGPU_ERR_INVALID, "reps must be positive");
@@ -1409,17 +1455,26 @@ extern "C" int sfgpu_system_autotune(sfgpu_system *s, int reps, int *chosen_xc, 
     }
     const int cand[] = {2, 4, 8, 16, 32};
     double best = 1e30;
-    int bestx = s->tile_xc;
-    for (int c : cand) {
-        s->tile_xc = c;
-        double f = 0, b = 0;
-        int rc = sfgpu_profile_propagator(s, reps, &f, &b, nullptr, nullptr);
-        if (rc) return rc;
-        if (f + b < best) { best = f + b; bestx = c; }
-    }
+    int bestx = s->tile_xc, bestp = s->tile_pipelined;
+    for (int pl = 0; pl < 2; pl++)
+        for (int c : cand) {
+            s->tile_xc = c;
+            s->tile_pipelined = pl;
+            double f = 0, b = 0;
+            int rc = sfgpu_profile_propagator(s, reps, &f, &b, nullptr, nullptr);
+            if (rc) return rc;
+            if (f + b < best) { best = f + b; bestx = c; bestp = pl; }
+        }
     s->tile_xc = bestx;
+    s->tile_pipelined = bestp;
     if (chosen_xc) *chosen_xc = bestx;
     if (best_ms) *best_ms = best;
+    return SFGPU_OK;
+}
+
+extern "C" int sfgpu_system_set_tile_pipelined(sfgpu_system *s, int enable) {
+    CHECK_SYS(s);
+    s->tile_pipelined = enable != 0;
     return SFGPU_OK;
 }
 

@@ -48,6 +48,12 @@ struct sfgpu_system {
     double *d_x = nullptr, *d_f = nullptr;
     int nblocks_red = 1;
     int tile_xc = 8;          // x planes per block of the 3D first-order step
+    int tile_pipelined = 1;   // 3D first-order step: software-pipelined form (step3d_march_pf)
+    // chain storage of residual evaluations: 0 keeps every forward slice,
+    // k > 0 keeps every k-th one and recomputes the others segment by
+    // segment during the backward sweep (set at creation)
+    int primal_stride = 0;
+    bool primal_checkpointed(const HMol &o) const;
     // bond-orientation profiles of second-order lattices (off by default)
     bool orient = false;
     double *d_ori_sum = nullptr;

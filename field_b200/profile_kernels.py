@@ -26,6 +26,8 @@ def main():
     ap.add_argument("--reps", type=int, default=50)
     ap.add_argument("--n", type=int, default=0, help="lattice size override")
     ap.add_argument("--tile", type=int, default=0, help="3D x-chunk depth (0: autotune)")
+    ap.add_argument("--form", default="pipelined", choices=["pipelined", "plain"],
+                    help="3D first-order step form when --tile is given")
     a = ap.parse_args()
     if a.case == "c2":
         spec, x = configs.cyl_micelle(**({"nx": a.n, "ny": a.n} if a.n else {}))
@@ -38,11 +40,13 @@ def main():
     tune = None
     if a.tile:
         s.set_tile(a.tile)
+        s.set_tile_pipelined(a.form == "pipelined")
     else:
         tune = s.autotune(reps=max(5, a.reps // 5))
     p = s.profile_propagator(reps=a.reps)
     peak, kind = measured_peaks()
-    out = {"case": a.case, "M": s.M, "K": s.K, "reps": a.reps, "tile": a.tile or tune, **p,
+    out = {"case": a.case, "M": s.M, "K": s.K, "reps": a.reps, "tile": a.tile or tune,
+           "form": a.form if a.tile else "autotuned", **p,
            "gbs_fwd": p["bytes_fwd"] / (p["ms_fwd"] / 1e3) / 1e9,
            "gbs_bwd": p["bytes_bwd"] / (p["ms_bwd"] / 1e3) / 1e9, "peak_gbs": peak, "peak_kind": kind}
     out["frac_fwd"] = out["gbs_fwd"] / peak

@@ -38,12 +38,19 @@ class SolveResult:
 
 
 class System:
-    def __init__(self, spec: SystemSpec):
+    def __init__(self, spec: SystemSpec, checkpoint_stride: int = 0):
+        """checkpoint_stride k > 0: residual evaluations keep every k-th
+        forward slice of a copolymer or second-order chain and recompute the
+        rest (sfgpu_system_create_checkpointed)."""
         self.lib = nat.load()
         self.spec = spec
         self._desc = spec.to_c()
         h = C.c_void_p()
-        nat.check(self.lib.sfgpu_system_create(C.byref(self._desc), C.byref(h)), "sfgpu_system_create")
+        if checkpoint_stride:
+            nat.check(self.lib.sfgpu_system_create_checkpointed(C.byref(self._desc), int(checkpoint_stride),
+                                                                 C.byref(h)), "sfgpu_system_create_checkpointed")
+        else:
+            nat.check(self.lib.sfgpu_system_create(C.byref(self._desc), C.byref(h)), "sfgpu_system_create")
         self.h = h
         M, nv, nc, ns = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         nat.check(self.lib.sfgpu_system_info(h, C.byref(M), C.byref(nv), C.byref(nc), C.byref(ns)), "info")
@@ -252,6 +259,9 @@ class System:
         nat.check(self.lib.sfgpu_system_autotune(self.h, reps, C.byref(x), C.byref(ms)), "sfgpu_system_autotune")
         return {"tile_xc": x.value, "ms_fwd_plus_bwd": ms.value}
 
+    def set_tile_pipelined(self, enable: bool):
+        nat.check(self.lib.sfgpu_system_set_tile_pipelined(self.h, int(bool(enable))), "set_tile_pipelined")
+
     def set_tile(self, xc: int):
         nat.check(self.lib.sfgpu_system_set_tile(self.h, xc), "sfgpu_system_set_tile")
 
@@ -330,3 +340,18 @@ class System:
         nat.check(self.lib.sfgpu_lat_lngn(self.h, C.c_void_p(g.data_ptr()), g.numel() // self.M, C.byref(v)),
                   "sfgpu_lat_lngn")
         return v.value
+
+
+def solve_diis_many(systems, x0s, tol=1e-7, maxit=5000, m=5, eta=0.1, threads=0):
+    """Pure_DIIS on many systems at once, one stream and host thread each
+    (sfgpu_solve_diis_many).  Returns a list of SolveResult."""
+    lib = nat.load()
+    n = len(systems)
+    xs = [np.ascontiguousarray(x, dtype=np.float64).copy() for x in x0s]
+    hs = (C.c_void_p * n)(*[s.h for s in systems])
+    xp = (C.POINTER(C.c_double) * n)(*[_d(x) for x in xs])
+    st = (C.c_int * n)()
+    it = (C.c_int * n)()
+    er = (C.c_double * n)()
+    nat.check(lib.sfgpu_solve_diis_many(n, hs, xp, tol, maxit, m, eta, threads, st, it, er), "sfgpu_solve_diis_many")
+    return [SolveResult(xs[i], st[i], it[i], er[i]) for i in range(n)]

@@ -195,6 +195,19 @@ int sfgpu_device_count(int *count);
  * path and of the per-call cudaMalloc of SF_Homopol1stO::CudaMatrix1
  * (SF_Homopol1stO.cpp:639-643): buffers are allocated once here. */
 int sfgpu_system_create(const sfgpu_system_desc *desc, sfgpu_system **out);
+/* The same with checkpointed chain storage for residual evaluations: the
+ * forward sweep of a copolymer or second-order chain keeps every stride-th
+ * propagator slice (Gf at positions 0, k, 2k, ...) and one segment of k
+ * slices; the backward sweep recomputes each earlier segment from its
+ * checkpoint with the same kernels before composing it.  Memory per chain
+ * (ceil(N/k) + k) K M doubles instead of N K M (a 96^3 second-order brush of
+ * N = 200 with k = 14: 1.3 GB instead of 9 GB), at the cost of about one
+ * extra forward sweep; residuals and profiles are bit-identical to full
+ * storage.  This is the memory-saving scheme SFbox selects with
+ * mol : X : save_memory (SF_Homopol1stO::Matrix1Long,
+ * SF_Homopol1stO.cpp:732-843), with the stride given here.  stride = 0 (or
+ * >= N) keeps every slice; overflow-protected systems keep every slice. */
+int sfgpu_system_create_checkpointed(const sfgpu_system_desc *desc, int stride, sfgpu_system **out);
 int sfgpu_system_destroy(sfgpu_system *sys);
 /* M (sites incl. boundaries), number of iteration variables, classes and
  * sites carrying iteration variables (SF_Solve.cpp:129-163). */
@@ -384,9 +397,27 @@ int sfgpu_profile_propagator(sfgpu_system *sys, int reps, double *ms_fwd, double
  * buffers and keep the fastest (reps forward + backward steps each; the
  * propagator contents are overwritten).  Other lattices ignore it. */
 int sfgpu_system_set_tile(sfgpu_system *sys, int xc);
+/* 1 (the default): the 3D first-order step runs software-pipelined (plane
+ * x+1's loads in flight while plane x is computed, double-buffered tile);
+ * 0: the plain x-marching form.  Results are bit-identical; the autotuner
+ * times both. */
+int sfgpu_system_set_tile_pipelined(sfgpu_system *sys, int enable);
 int sfgpu_system_autotune(sfgpu_system *sys, int reps, int *chosen_xc, double *best_ms);
 
 /* ---- iterations ------------------------------------------------------- */
+/* Many systems solved at once, each by sfgpu_solve_diis on its own stream
+ * from its own host thread (threads <= 0: one per system): the device
+ * interleaves the systems' kernels and every system's per-iteration host
+ * round trip hides behind the others' work.  The batched form for instances
+ * that fill the GPU one propagator step at a time (3D, second order), where
+ * the persistent one-block-per-instance solver (sfgpu_batch_*) would leave
+ * most SMs idle; a parameter sweep of such systems (Vary.cpp:127).  x[i]
+ * (host) is system i's start and receives its result; status[i] as
+ * sfgpu_solve_diis returns it.  Returns the first status other than OK,
+ * NOTCONVERGED or NONFINITE, else SFGPU_OK. */
+int sfgpu_solve_diis_many(int n, sfgpu_system *const *systems, double *const *x, double tol, int maxit, int m,
+                          double eta, int threads, int *status, int *iterations, double *errors);
+
 /* SFbox's Newton iteration (SFNewton::iterate, sfnewton.cpp:844-1143, with
  * Scheutjens' trust-region step search, :1946-2022) over this library's
  * residual: the "plain Newton form".  The Hessian is dense, single
