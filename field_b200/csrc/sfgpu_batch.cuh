@@ -26,6 +26,7 @@ struct InstDesc {
     DLat L;
     int M, nseg, nmol, nclass, nsites, solvent;
     int gstage;                     // G of the running segment staged in shared memory
+    int small1d;                    // 1D symmetric homopolymers: running slices and phi in shared memory too
     long long nvar;
     int freedom[SFGPU_MAX_SEG];
     int class_of[SFGPU_MAX_SEG];
@@ -184,6 +185,63 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
     }
     double *gi = I.gi;
     double *bufA = I.ginv0, *bufB = I.ginv1;
+    if (o.sym && I.small1d && I.gstage) {
+        // 1D lattices small enough to keep the whole step in shared memory:
+        // the running propagator slice (two buffers) and the molecule's phi
+        // sit next to the staged G, so a step reads only shared memory and
+        // the stored half chain (gi), and writes gi; each step costs a
+        // shared-memory round trip and a block barrier instead of an L2 one.
+        // Same operands and operation order as the path below.
+        const int sg = o.seg[0];
+        const double *G = gof(sg);
+        double *sa = g_stage + M, *sb = sa + M, *sphi = sb + M;
+        const int N = o.N, half = N / 2;
+        for (int r = threadIdx.x; r < M; r += blockDim.x) {
+            const double gv = G[r];
+            sa[r] = gv;
+            gi[r] = gv;
+            sb[r] = 0.0;
+            sphi[r] = 0.0;
+        }
+        __syncthreads();
+        for (int t = 1; t < half; t++) {
+            double *dst = gi + (size_t)t * M;
+            for_interior4(L, threadIdx.x, blockDim.x,
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, sa, G, k, nlast); },
+                [&](const RowInfo &R, int k, double v) { sb[R.base + k] = v; dst[R.base + k] = v; });
+            __syncthreads();
+            double *tt = sa; sa = sb; sb = tt;
+        }
+        if (N % 2 == 1) {
+            for_interior4(L, threadIdx.x, blockDim.x,
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, sa, G, k, nlast); },
+                [&](const RowInfo &R, int k, double out) {
+                    const int z = R.base + k;
+                    sb[z] = out;
+                    sphi[z] = (sphi[z] + out * out) * 0.5;
+                });
+            __syncthreads();
+            double *tt = sa; sa = sb; sb = tt;
+        }
+        for (int sp = (N + 3) / 2; sp <= N; sp++) {
+            const double *other = gi + (size_t)(N - sp) * M;
+            for_interior4_acc(L, threadIdx.x, blockDim.x, sphi, other,
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, sa, G, k, nlast); },
+                [&](const RowInfo &R, int k, double out, double ph, double ot) {
+                    const int z = R.base + k;
+                    sb[z] = out;
+                    sphi[z] = ph + out * ot;
+                });
+            __syncthreads();
+            double *tt = sa; sa = sb; sb = tt;
+        }
+        double *phi = o.phi[sg];
+        for (int r = threadIdx.x; r < M; r += blockDim.x) phi[r] = sphi[r];
+        __syncthreads();
+        finish_molecule(I, m, sa, sh);
+        __syncthreads();
+        return;
+    }
     if (o.sym) {
         const int sg = o.seg[0];
         const double *G = gof(sg);

@@ -156,7 +156,10 @@ step3d_march(DLat L, const double *__restrict__ gin, const double *__restrict__ 
 // b^1 for plane x+1 only after every thread passed plane x's barrier, i.e.
 // finished reading b^1 for plane x-1).  Same operands and operation order as
 // step3d_march, so the results are bit-identical.
-static __global__ void __launch_bounds__(kTZ * kTY)
+// kCompose = false compiles the composition-free (forward) step alone, whose
+// registers then leave room for more resident blocks.
+template <bool kCompose>
+static __global__ void __launch_bounds__(kTZ * kTY, kCompose ? 4 : 6)
 step3d_march_pf(DLat L, const double *__restrict__ gin, const double *__restrict__ G,
                 double *__restrict__ gout, const double *__restrict__ other, double *__restrict__ phi,
                 int mode, int xc) {
@@ -175,7 +178,7 @@ step3d_march_pf(DLat L, const double *__restrict__ gin, const double *__restrict
     const bool hz0 = (tz == 0), hz1 = (tz == kTZ - 1) || (z == nz);
     const bool hy0 = (ty == 0), hy1 = (ty == kTY - 1) || (y == ny);
     const int col = y * jy + z;
-    const bool acc_mode = (mode == COMP_ACC), centre = (mode == COMP_CENTRE);
+    const bool acc_mode = kCompose && (mode == COMP_ACC), centre = kCompose && (mode == COMP_CENTRE);
     // registers: column values of planes x-1, x, x+1; plane x's G, halos and
     // composition operands
     double vprev = 0, vcur = 0, vnext = 0, g = 0, hzl = 0, hzh = 0, hyl = 0, hyh = 0, ot = 0, ph = 0;

@@ -50,11 +50,15 @@ int sfgpu_system::launch_step1(const double *gin, const double *G, double *gout,
                                int mode) {
     const DLat &L = H.L;
     if (L.grad == 3 && !lat_twelve(L)) {
-        dim3 grid((L.Md[2] - 2 + kTZ - 1) / kTZ, (L.Md[1] - 2 + kTY - 1) / kTY, (L.Md[0] - 2 + tile_xc - 1) / tile_xc);
-        if (tile_pipelined)
-            step3d_march_pf<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, tile_xc);
+        const bool composing = mode != COMP_NONE;
+        const int xc = composing ? tile_xc_bwd : tile_xc;
+        dim3 grid((L.Md[2] - 2 + kTZ - 1) / kTZ, (L.Md[1] - 2 + kTY - 1) / kTY, (L.Md[0] - 2 + xc - 1) / xc);
+        if (composing && tile_pipelined_bwd)
+            step3d_march_pf<true><<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, xc);
+        else if (!composing && tile_pipelined)
+            step3d_march_pf<false><<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, xc);
         else
-            step3d_march<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, tile_xc);
+            step3d_march<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, xc);
     } else {
         step1_rows<<<grid_rows(L), kBlock, 0, stream>>>(L, gin, G, gout, other, phi, mode);
     }
@@ -1453,34 +1457,37 @@ extern "C" int sfgpu_system_autotune(sfgpu_system *s, int reps, int *chosen_xc, 
         if (best_ms) *best_ms = 0;
         return SFGPU_OK;
     }
+    // forward and backward steps are timed by the same profile call; each
+    // keeps its own fastest (depth, form)
     const int cand[] = {2, 4, 8, 16, 32};
-    double best = 1e30;
-    int bestx = s->tile_xc, bestp = s->tile_pipelined;
+    double bf = 1e30, bb = 1e30;
+    int fx = s->tile_xc, fp = s->tile_pipelined, bx = s->tile_xc_bwd, bp = s->tile_pipelined_bwd;
     for (int pl = 0; pl < 2; pl++)
         for (int c : cand) {
-            s->tile_xc = c;
-            s->tile_pipelined = pl;
+            s->tile_xc = s->tile_xc_bwd = c;
+            s->tile_pipelined = s->tile_pipelined_bwd = pl;
             double f = 0, b = 0;
             int rc = sfgpu_profile_propagator(s, reps, &f, &b, nullptr, nullptr);
             if (rc) return rc;
-            if (f + b < best) { best = f + b; bestx = c; bestp = pl; }
+            if (f < bf) { bf = f; fx = c; fp = pl; }
+            if (b < bb) { bb = b; bx = c; bp = pl; }
         }
-    s->tile_xc = bestx;
-    s->tile_pipelined = bestp;
-    if (chosen_xc) *chosen_xc = bestx;
-    if (best_ms) *best_ms = best;
+    s->tile_xc = fx; s->tile_pipelined = fp;
+    s->tile_xc_bwd = bx; s->tile_pipelined_bwd = bp;
+    if (chosen_xc) *chosen_xc = fx;
+    if (best_ms) *best_ms = bf + bb;
     return SFGPU_OK;
 }
 
 extern "C" int sfgpu_system_set_tile_pipelined(sfgpu_system *s, int enable) {
     CHECK_SYS(s);
-    s->tile_pipelined = enable != 0;
+    s->tile_pipelined = s->tile_pipelined_bwd = enable != 0;
     return SFGPU_OK;
 }
 
 extern "C" int sfgpu_system_set_tile(sfgpu_system *s, int xc) {
     CHECK_SYS(s);
     if (xc < 1 || xc > 1024) return fail(SFGPU_ERR_INVALID, "tile depth must be in 1..1024");
-    s->tile_xc = xc;
+    s->tile_xc = s->tile_xc_bwd = xc;
     return SFGPU_OK;
 }

@@ -47,8 +47,11 @@ struct sfgpu_system {
     double *d_partial = nullptr, *d_scal = nullptr, *d_phib = nullptr, *d_chib = nullptr, *d_misc = nullptr;
     double *d_x = nullptr, *d_f = nullptr;
     int nblocks_red = 1;
-    int tile_xc = 8;          // x planes per block of the 3D first-order step
-    int tile_pipelined = 1;   // 3D first-order step: software-pipelined form (step3d_march_pf)
+    // 3D first-order step, separately for the composition-free forward steps
+    // and the composing backward steps: x planes per block and whether the
+    // software-pipelined form (step3d_march_pf) runs it
+    int tile_xc = 4, tile_xc_bwd = 8;
+    int tile_pipelined = 0, tile_pipelined_bwd = 1;
     // chain storage of residual evaluations: 0 keeps every forward slice,
     // k > 0 keeps every k-th one and recomputes the others segment by
     // segment during the backward sweep (set at creation)

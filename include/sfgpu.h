@@ -397,10 +397,12 @@ int sfgpu_profile_propagator(sfgpu_system *sys, int reps, double *ms_fwd, double
  * buffers and keep the fastest (reps forward + backward steps each; the
  * propagator contents are overwritten).  Other lattices ignore it. */
 int sfgpu_system_set_tile(sfgpu_system *sys, int xc);
-/* 1 (the default): the 3D first-order step runs software-pipelined (plane
- * x+1's loads in flight while plane x is computed, double-buffered tile);
- * 0: the plain x-marching form.  Results are bit-identical; the autotuner
- * times both. */
+/* 1: the 3D first-order step runs software-pipelined (plane x+1's loads in
+ * flight while plane x is computed, double-buffered tile); 0: the plain
+ * x-marching form.  Results are bit-identical.  By default the composing
+ * backward steps run pipelined (x depth 8) and the forward steps plain (depth
+ * 4); the autotuner times both forms and depths for each kind of step.
+ * sfgpu_system_set_tile and this call set both kinds. */
 int sfgpu_system_set_tile_pipelined(sfgpu_system *sys, int enable);
 int sfgpu_system_autotune(sfgpu_system *sys, int reps, int *chosen_xc, double *best_ms);
 
