@@ -260,16 +260,18 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
             const size_t bytes = sizeof(double) * (size_t)b->sys[i]->M;
             b->desc_h[i].gstage = bytes <= room ? 1 : 0;
             if (bytes <= room) need = std::max(need, bytes);
-            // 1D symmetric homopolymers: G, two running slices and phi, when
-            // four lattice vectors fit in 24 KB (M <= 768), a budget that
-            // keeps several blocks resident per SM
+            // 1D symmetric homopolymers: G, two running slices, phi and the
+            // ring of stored slices, when these 4 + kRing lattice vectors fit
+            // in 48 KB (M <= 768), a budget that keeps several blocks
+            // resident per SM
             const auto *sy = b->sys[i];
             bool sym1d = sy->H.L.grad == 1;
             bool any_sym = false;
             for (const auto &o : sy->mols) any_sym |= o.sym != 0;
-            sym1d = sym1d && any_sym && 4 * bytes <= 24 * 1024 && 4 * bytes <= room;
+            const size_t vecs = (4 + sfb::kRing) * bytes;
+            sym1d = sym1d && any_sym && vecs <= 48 * 1024 && vecs <= room;
             b->desc_h[i].small1d = sym1d ? 1 : 0;
-            if (sym1d) need = std::max(need, 4 * bytes);
+            if (sym1d) need = std::max(need, vecs);
         }
         if (cudaMemcpy(b->d_desc, b->desc_h.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaFuncSetAttribute(batch_diis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) !=

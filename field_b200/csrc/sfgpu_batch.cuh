@@ -7,10 +7,12 @@
 // propagator steps and no host round trip.  Uneven instances of a parameter
 // sweep (Vary.cpp:127) therefore share the GPU without per-step launches.
 #pragma once
+#include <cuda_pipeline_primitives.h>
 #include "sfgpu_kernels.cuh"
 
 namespace sfb {
 
+constexpr int kRing = 4;            // stored slices in flight in the shared-memory 1D path
 constexpr int kMaxMol = SFGPU_MAX_SEG;
 constexpr int kMaxHist = 16;        // DIIS memory m supported by the batch path
 
@@ -26,7 +28,8 @@ struct InstDesc {
     DLat L;
     int M, nseg, nmol, nclass, nsites, solvent;
     int gstage;                     // G of the running segment staged in shared memory
-    int small1d;                    // 1D symmetric homopolymers: running slices and phi in shared memory too
+    int small1d;                    // 1D symmetric homopolymers: running slices, phi and a ring of
+                                    // kRing stored slices in shared memory too
     long long nvar;
     int freedom[SFGPU_MAX_SEG];
     int class_of[SFGPU_MAX_SEG];
@@ -223,18 +226,40 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
             __syncthreads();
             double *tt = sa; sa = sb; sb = tt;
         }
-        for (int sp = (N + 3) / 2; sp <= N; sp++) {
-            const double *other = gi + (size_t)(N - sp) * M;
-            for_interior4_acc(L, threadIdx.x, blockDim.x, sphi, other,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, sa, G, k, nlast); },
-                [&](const RowInfo &R, int k, double out, double ph, double ot) {
-                    const int z = R.base + k;
-                    sb[z] = out;
-                    sphi[z] = ph + out * ot;
-                });
+        // backward sweep: the stored slice each step composes with streams
+        // into a ring of kRing shared-memory slices by asynchronous copies
+        // issued kRing steps ahead, so its L2 latency hides behind the steps
+        // in between.  Every thread copies exactly the positions it later
+        // reads, so the copy group's completion (no barrier) makes them
+        // visible to it.
+        double *ring = sphi + M;
+        const int nlast = L.Md[0] - 2;
+        const RowInfo R0 = lat_row(L, 0);
+        const int sp0 = (N + 3) / 2, nsteps = N - sp0 + 1;
+        auto issue = [&](int j) {
+            if (j < nsteps) {
+                const double *src = gi + (size_t)(N - sp0 - j) * M;
+                double *dst = ring + (size_t)(j % kRing) * M;
+                for (int k = threadIdx.x + 1; k <= nlast; k += blockDim.x)
+                    __pipeline_memcpy_async(dst + k, src + k, sizeof(double));
+            }
+            __pipeline_commit();
+        };
+        for (int j = 0; j < kRing; j++) issue(j);
+        for (int j = 0; j < nsteps; j++) {
+            __pipeline_wait_prior(kRing - 1);
+            const double *ot = ring + (size_t)(j % kRing) * M;
+            for (int k = threadIdx.x + 1; k <= nlast; k += blockDim.x) {
+                const double ph = sphi[k], o2 = ot[k];
+                const double out = prop1_row<false>(L, R0, sa, G, k, nlast);
+                sb[k] = out;
+                sphi[k] = ph + out * o2;
+            }
             __syncthreads();
+            issue(j + kRing);
             double *tt = sa; sa = sb; sb = tt;
         }
+        __pipeline_wait_prior(0);
         double *phi = o.phi[sg];
         for (int r = threadIdx.x; r < M; r += blockDim.x) phi[r] = sphi[r];
         __syncthreads();
