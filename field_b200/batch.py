@@ -170,6 +170,29 @@ class BatchSolver:
         self.launches_in_last_solve_total += 1
         return BatchResult(y, st, it, er)
 
+    def set_launch(self, threads: int, stage: bool = True):
+        """Threads per block and shared-memory staging of the persistent
+        kernel (sfgpu_batch_set_launch)."""
+        nat.check(self.lib.sfgpu_batch_set_launch(self.h, int(threads), int(bool(stage))), "sfgpu_batch_set_launch")
+
+    def autotune(self, x0, tol=1e-7, maxit=2000, candidates=((1024, True), (512, True), (512, False),
+                                                             (256, True))):
+        """Time one solve per launch shape from x0 and keep the fastest;
+        returns {(threads, stage): ms}."""
+        times = {}
+        for th, stg in candidates:
+            try:
+                self.set_launch(th, stg)
+            except nat.SfgpuError:
+                continue
+            self.load(x0)
+            self.solve_resident(tol, maxit)
+            self.results()
+            times[(th, stg)] = self.kernel_ms()
+        best = min(times, key=times.get)
+        self.set_launch(*best)
+        return times
+
     def load(self, x0):
         x = np.ascontiguousarray(x0, dtype=np.float64)
         if x.size != self.total:

@@ -158,6 +158,46 @@ __global__ void __launch_bounds__(1024) batch_diis_kernel(const InstDesc *__rest
 }
 
 // ---------------------------------------------------------------------------
+// Shared-memory staging of each instance: G of the running segment where
+// the lattice fits next to the kernel's static shared memory, and on 1D
+// symmetric homopolymers also the running slices, phi and the ring of
+// stored slices.  allow = false stages nothing (more blocks per SM).
+static int configure_stage(sfgpu_batch *b, bool allow) {
+    int dev = 0, optin = 0;
+    cudaFuncAttributes fa;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, batch_diis_kernel) != cudaSuccess)
+        return SFGPU_ERR_CUDA;
+    const size_t fixed = fa.sharedSizeBytes + 1024;   // 1 KB the system reserves per block
+    const size_t room = (size_t)optin > fixed ? (size_t)optin - fixed : 0;
+    size_t need = 0;
+    const int n = (int)b->sys.size();
+    for (int i = 0; i < n; i++) {
+        const size_t bytes = sizeof(double) * (size_t)b->sys[i]->M;
+        b->desc_h[i].gstage = (allow && bytes <= room) ? 1 : 0;
+        if (b->desc_h[i].gstage) need = std::max(need, bytes);
+        // 1D symmetric homopolymers: G, two running slices, phi and the
+        // ring of stored slices, when these 4 + kRing lattice vectors fit
+        // in 48 KB (M <= 768), a budget that keeps several blocks
+        // resident per SM
+        const auto *sy = b->sys[i];
+        bool sym1d = allow && sy->H.L.grad == 1;
+        bool any_sym = false;
+        for (const auto &o : sy->mols) any_sym |= o.sym != 0;
+        const size_t vecs = (4 + sfb::kRing) * bytes;
+        sym1d = sym1d && any_sym && vecs <= 48 * 1024 && vecs <= room;
+        b->desc_h[i].small1d = sym1d ? 1 : 0;
+        if (sym1d) need = std::max(need, vecs);
+    }
+    if (cudaMemcpy(b->d_desc, b->desc_h.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaFuncSetAttribute(batch_diis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) !=
+            cudaSuccess)
+        return SFGPU_ERR_CUDA;
+    b->stage_bytes = need;
+    return SFGPU_OK;
+}
+
 extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, sfgpu_batch **out) {
     if (!out || !descs || n < 1) return SFGPU_ERR_INVALID;
     *out = nullptr;
@@ -242,45 +282,7 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
     if (!rc) rc = balloc(b, (void **)&b->d_err, sizeof(double) * n);
     if (rc) { delete b; return rc; }
     b->block = maxM >= 4096 ? 1024 : (maxM >= 1024 ? 512 : 256);
-    // stage G in shared memory for every instance whose lattice fits next to
-    // the static descriptor and reduction space
-    {
-        int dev = 0, optin = 0;
-        cudaFuncAttributes fa;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
-            cudaFuncGetAttributes(&fa, batch_diis_kernel) != cudaSuccess) {
-            delete b;
-            return SFGPU_ERR_CUDA;
-        }
-        const size_t fixed = fa.sharedSizeBytes + 1024;   // 1 KB the system reserves per block
-        const size_t room = (size_t)optin > fixed ? (size_t)optin - fixed : 0;
-        size_t need = 0;
-        for (int i = 0; i < n; i++) {
-            const size_t bytes = sizeof(double) * (size_t)b->sys[i]->M;
-            b->desc_h[i].gstage = bytes <= room ? 1 : 0;
-            if (bytes <= room) need = std::max(need, bytes);
-            // 1D symmetric homopolymers: G, two running slices, phi and the
-            // ring of stored slices, when these 4 + kRing lattice vectors fit
-            // in 48 KB (M <= 768), a budget that keeps several blocks
-            // resident per SM
-            const auto *sy = b->sys[i];
-            bool sym1d = sy->H.L.grad == 1;
-            bool any_sym = false;
-            for (const auto &o : sy->mols) any_sym |= o.sym != 0;
-            const size_t vecs = (4 + sfb::kRing) * bytes;
-            sym1d = sym1d && any_sym && vecs <= 48 * 1024 && vecs <= room;
-            b->desc_h[i].small1d = sym1d ? 1 : 0;
-            if (sym1d) need = std::max(need, vecs);
-        }
-        if (cudaMemcpy(b->d_desc, b->desc_h.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaFuncSetAttribute(batch_diis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) !=
-                cudaSuccess) {
-            delete b;
-            return SFGPU_ERR_CUDA;
-        }
-        b->stage_bytes = need;
-    }
+    if ((rc = configure_stage(b, true))) { delete b; return rc; }
     *out = b;
     return SFGPU_OK;
 }
@@ -308,6 +310,17 @@ extern "C" int sfgpu_batch_set_stream(sfgpu_batch *b, void *stream) {
     b->stream = (cudaStream_t)stream;
     for (auto *s : b->sys) s->stream = b->stream;
     return SFGPU_OK;
+}
+
+// Launch shape of the persistent kernel: threads per block (128..1024, a
+// multiple of 32) and whether instances stage G (and the 1D slices) in
+// shared memory.  By default 1024/512/256 threads by lattice size and
+// staging on.
+extern "C" int sfgpu_batch_set_launch(sfgpu_batch *b, int threads, int stage) {
+    if (!b || threads < 128 || threads > 1024 || threads % 32) return SFGPU_ERR_INVALID;
+    SFGPU_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    b->block = threads;
+    return configure_stage(b, stage != 0);
 }
 
 // Load the concatenated initial guesses (host) into the device iterate.
