@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "libsfgpu.so")
 SOURCES = ["sfgpu_system.cu", "sfgpu_solve.cu", "sfgpu_batch.cu", "sfgpu_tangent.cu", "sfgpu_adjoint.cu",
            "sfgpu_noalloc.cu", "sfgpu_newton.cu"]
 HEADERS = ["sfgpu_internal.cuh", "sfgpu_kernels.cuh", "sfgpu_system.h", "sfgpu_batch.cuh", "sfgpu_tangent.cuh",
-           "sfgpu_adjoint.cuh",
+           "sfgpu_adjoint.cuh", "sfgpu_newton.h",
            "../../include/sfgpu.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

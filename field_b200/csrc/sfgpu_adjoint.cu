@@ -176,7 +176,6 @@ int sfgpu_system::ensure_adjoint_misc() {
 
 int sfgpu_system::ensure_adjoint() {
     if (K == 3 || K == 5) return fail_unsupported("derivatives of the lumped 1D/2D second-order lattices");
-    if (H.L.ltype != SFGPU_LATTICE_STANDARD) return fail_unsupported("derivatives on the FCC, HEX and stencils 3D lattices");
     if (logmode) return fail_unsupported("derivatives with overflow protection");
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)

@@ -14,6 +14,29 @@ namespace sfa {
 using namespace sfk;
 using namespace sft;
 
+// neighbour i (0..11) of the twelve-neighbour steps, in step12's order
+__device__ __forceinline__ void twelve_offset(int ltype, int i, int &dx, int &dy, int &dz) {
+    // FCC (Lat3DFCC1stO.cpp:79-91) and HEX (Lat3DHEX1stO.cpp:79-91) bond sets
+    const signed char fcc[12][3] = {{-1, -1, 0}, {1, 1, 0},  {-1, 1, 0},  {1, -1, 0}, {0, -1, -1}, {0, 1, 1},
+                                    {0, -1, 1},  {0, 1, -1}, {-1, 0, -1}, {1, 0, 1},  {-1, 0, 1},  {1, 0, -1}};
+    const signed char hex[12][3] = {{-1, 0, 0}, {1, 0, 0},  {-1, 1, 0}, {0, 1, 0},  {0, -1, 0}, {1, -1, 0},
+                                    {0, 1, -1}, {0, 0, -1}, {1, 0, -1}, {-1, 0, 1}, {0, 0, 1},  {0, -1, 1}};
+    const signed char *o = (ltype == SFGPU_LATTICE_FCC) ? fcc[i] : hex[i];
+    dx = o[0];
+    dy = o[1];
+    dz = o[2];
+}
+
+// contact neighbour i (0..11) of the HEX lattice (side_fraction's set,
+// Lat3D.cpp:1733-1752)
+__device__ __forceinline__ void hex_side_offset(int i, int &dx, int &dy, int &dz) {
+    const signed char o[12][3] = {{1, 0, 0},  {-1, 0, 0}, {1, -1, 0}, {0, -1, 0}, {0, 1, 0},  {-1, 1, 0},
+                                  {0, -1, 1}, {0, 0, 1},  {-1, 0, 1}, {1, 0, -1}, {0, 0, -1}, {0, 1, -1}};
+    dx = o[i][0];
+    dy = o[i][1];
+    dz = o[i][2];
+}
+
 // out[map(n)] += c_n * y[t] for every site n the first-order stencil at
 // interior t reads (the transpose of the un-weighted stencil, raw1_row)
 __device__ __forceinline__ void scatter1(const DLat &L, const RowInfo &R, int k, int nlast, double y,
@@ -43,6 +66,20 @@ __device__ __forceinline__ void scatter1(const DLat &L, const RowInfo &R, int k,
         atomicAdd(out + t + R.dn, lp * y);
         atomicAdd(out + km, L.l1 * y);
         atomicAdd(out + kp, L.l1 * y);
+        return;
+    }
+    if (lat_twelve(L)) {
+        // transpose of the twelve-neighbour step (step12): 1/12 to each
+        // (mapped) neighbour it read
+        const double c12 = y * (1.0 / 12.0);
+        for (int i = 0; i < 12; i++) {
+            int dx, dy, dz;
+            twelve_offset(L.ltype, i, dx, dy, dz);
+            const int xo = dx < 0 ? R.up : (dx > 0 ? R.dn : 0);
+            const int yo = dy < 0 ? R.up2 : (dy > 0 ? R.dn2 : 0);
+            const int kk = dz < 0 ? km : (dz > 0 ? kp : t);
+            atomicAdd(out + kk + xo + yo, c12);
+        }
         return;
     }
     const double c = y * (1.0 / 6.0);
@@ -205,7 +242,7 @@ struct AdjResParam {
 };
 __device__ __forceinline__ void side_scatter(const DLat &L, int z, double y, double *__restrict__ out) {
     // transpose of side_fraction at an interior site (1D/2D: the contact
-    // stencil with lambda_chi; 3D: the six neighbours at 1/6)
+    // stencil with lambda_chi; 3D: the contact set of the lattice type)
     int c[3];
     lat_coords(L, z, c);
     auto at = [&](int cx, int cy, int cz) {
@@ -214,13 +251,34 @@ __device__ __forceinline__ void side_scatter(const DLat &L, int z, double y, dou
         return cc[0] * L.st[0] + cc[1] * L.st[1] + cc[2] * L.st[2];
     };
     if (L.grad == 3) {
-        const double q = y * (1.0 / 6.0);
-        atomicAdd(out + at(c[0] + 1, c[1], c[2]), q);
-        atomicAdd(out + at(c[0] - 1, c[1], c[2]), q);
-        atomicAdd(out + at(c[0], c[1] + 1, c[2]), q);
-        atomicAdd(out + at(c[0], c[1] - 1, c[2]), q);
-        atomicAdd(out + at(c[0], c[1], c[2] + 1), q);
-        atomicAdd(out + at(c[0], c[1], c[2] - 1), q);
+        if (L.ltype == SFGPU_LATTICE_STANDARD) {
+            const double q = y * (1.0 / 6.0);
+            atomicAdd(out + at(c[0] + 1, c[1], c[2]), q);
+            atomicAdd(out + at(c[0] - 1, c[1], c[2]), q);
+            atomicAdd(out + at(c[0], c[1] + 1, c[2]), q);
+            atomicAdd(out + at(c[0], c[1] - 1, c[2]), q);
+            atomicAdd(out + at(c[0], c[1], c[2] + 1), q);
+            atomicAdd(out + at(c[0], c[1], c[2] - 1), q);
+            return;
+        }
+        if (L.ltype == SFGPU_LATTICE_HEX) {
+            // the twelve HEX contact neighbours at 1/12 (side_fraction's set)
+            const double q = y * (1.0 / 12.0);
+            for (int i = 0; i < 12; i++) {
+                int dx, dy, dz;
+                hex_side_offset(i, dx, dy, dz);
+                atomicAdd(out + at(c[0] + dx, c[1] + dy, c[2] + dz), q);
+            }
+            return;
+        }
+        // FCC and stencils: the 27-site cube, weight by the offset's class
+        // (centre, face, edge, corner)
+        for (int dx = -1; dx <= 1; dx++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dz = -1; dz <= 1; dz++) {
+                    const double wgt = L.sl[abs(dx) + abs(dy) + abs(dz)];
+                    if (wgt != 0.0) atomicAdd(out + at(c[0] + dx, c[1] + dy, c[2] + dz), wgt * y);
+                }
         return;
     }
     const double l = L.l1chi;
@@ -322,12 +380,7 @@ __device__ inline void side_fraction_adj(const DLat &L, int z, double y, double 
     int c[3];
     lat_coords(L, z, c);
     if (L.grad == 3) {
-        if (!lat_interior(L, c)) return;
-        const int jx = L.st[0], jy = L.st[1];
-        const double q = y * (1.0 / 6.0);
-        side_put(L, z + jx, q, out); side_put(L, z - jx, q, out);
-        side_put(L, z + jy, q, out); side_put(L, z - jy, q, out);
-        side_put(L, z + 1, q, out);  side_put(L, z - 1, q, out);
+        if (lat_interior(L, c)) side_scatter(L, z, y, out);   // every 3D lattice type
         return;
     }
     const double l = L.l1chi;

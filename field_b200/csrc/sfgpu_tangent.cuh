@@ -56,6 +56,16 @@ __device__ __forceinline__ double raw1_row(const DLat &L, const RowInfo &R, cons
         double l0 = 1 - 4 * L.l1;
         return l0 * b + L.l1 * (a + c) + L.l1 * (u + dd);
     }
+    if (lat_twelve(L)) {
+        // FCC / HEX: the twelve neighbours of step12 at weight 1/12, mapped
+        // per coordinate as prop1_row maps them
+        return step12(L.ltype, 1.0, [&](int dx, int dy, int dz) {
+            const int xo = dx < 0 ? R.up : (dx > 0 ? R.dn : 0);
+            const int yo = dy < 0 ? R.up2 : (dy > 0 ? R.dn2 : 0);
+            const int kk = dz < 0 ? km : (dz > 0 ? kp : k);
+            return p[R.base + kk + xo + yo];
+        });
+    }
     return (p[t + R.up] + p[t + R.dn] + p[t + R.up2] + p[t + R.dn2] + a + c) * (1.0 / 6.0);
 }
 

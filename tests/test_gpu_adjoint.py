@@ -39,7 +39,8 @@ def test_dot_product_identity(gpu_lib, case):
     assert abs(lhs - rhs) <= 1e-10 * scale, (lhs, rhs)
 
 
-@pytest.mark.parametrize("case", ["1d_surface", "2d_cylinder", "3d_periodic_melt"])
+@pytest.mark.parametrize("case", ["1d_surface", "2d_cylinder", "3d_periodic_melt", "3d_fcc_colloid",
+                                  "3d_hex_colloid", "3d_stencils_melt"])
 def test_gradient_of_half_squared_norm(gpu_lib, case):
     spec = CASES[case]()
     s = System(spec)
@@ -55,11 +56,13 @@ def test_gradient_of_half_squared_norm(gpu_lib, case):
         assert abs(fd - g @ d) <= 1e-7 * np.linalg.norm(g) * np.linalg.norm(d), (fd, g @ d)
 
 
-def test_second_order_dot_product_and_gradient(gpu_lib):
-    """Second-order (six-direction) reverse sweep on the pinned 3D brush:
+@pytest.mark.parametrize("case", ["3d_2nd_brush", "3d_2nd_fcc_brush"])
+def test_second_order_dot_product_and_gradient(gpu_lib, case):
+    """Second-order (six-direction) reverse sweep on the pinned 3D brush (and
+    on the FCC lattice type, whose contact averages span the 27-site cube):
     <w, J v> = <J^T w, v> against the forward-mode tangent, and the gradient
     of |f|^2/2 against central differences."""
-    spec = CASES["3d_2nd_brush"]()
+    spec = CASES[case]()
     s = System(spec)
     x = random_x(spec, seed=71, scale=0.2)
     rng = np.random.default_rng(72)
@@ -124,7 +127,8 @@ def test_lbfgs_with_checkpoints_c1(gpu_lib):
     assert np.linalg.norm(Oracle(spec).residual(r.x)) < 1e-8
 
 
-@pytest.mark.parametrize("case", ["1d_surface", "2d_cylinder", "3d_mirror_mix", "3d_2nd_brush"])
+@pytest.mark.parametrize("case", ["1d_surface", "2d_cylinder", "3d_mirror_mix", "3d_2nd_brush", "3d_hex_colloid",
+                                  "3d_stencils_colloid"])
 def test_chi_gradient_against_differences(gpu_lib, case):
     """d(w.f)/d chi at fixed x against central differences of w.f with chi
     changed symmetrically (chi(a,b) = chi(b,a) += h).  f is linear in chi at
@@ -208,7 +212,8 @@ def test_auto_checkpoint_stride(gpu_lib):
 
 
 @pytest.mark.parametrize("case", ["1d_surface", "1d_lambda_chi", "1d_periodic_restricted", "2d_cylinder",
-                                  "2d_flat_surface", "3d_mirror_mix", "3d_2nd_brush"])
+                                  "2d_flat_surface", "3d_mirror_mix", "3d_2nd_brush", "3d_fcc_colloid",
+                                  "3d_hex_mirror", "3d_stencils_colloid"])
 def test_free_energy_gradient(gpu_lib, case):
     """dF/dx from the reverse sweep against central differences of F
     (h = 1e-5) along random directions; F itself equals sfgpu_free_energy
