@@ -180,6 +180,7 @@ int sfgpu_system::ensure_adjoint() {
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
         if (o.dend || o.force != 0) return fail_unsupported("derivatives of dendrimers and of the force ensemble");
+        else if (o.tree || o.ring) return fail_unsupported("derivatives of branched molecules and rings");
     int rc = ensure_adjoint_misc();
     if (rc) return rc;
     if (!a_store) {

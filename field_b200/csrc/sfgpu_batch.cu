@@ -215,8 +215,9 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
         if (descs[i].lattice.order != 1) { rc = fail_unsupported("batched second-order lattices"); break; }
         if (descs[i].overflow_protection) { rc = fail_unsupported("batched systems with overflow protection"); break; }
         for (int q = 0; q < descs[i].n_molecules && !rc; q++)
-            if (descs[i].molecules[q].n_generations > 0 || descs[i].molecules[q].force != 0)
-                rc = fail_unsupported("batched dendrimers and force ensembles");
+            if (descs[i].molecules[q].n_generations > 0 || descs[i].molecules[q].force != 0 ||
+                descs[i].molecules[q].bond_parent || descs[i].molecules[q].ring)
+                rc = fail_unsupported("batched dendrimers, branched molecules, rings and force ensembles");
         if (rc) break;
         if (descs[i].lattice.gradients == 3 && descs[i].lattice.lattice_type != SFGPU_LATTICE_STANDARD) {
             rc = fail_unsupported("batched FCC, HEX and stencils 3D lattices");

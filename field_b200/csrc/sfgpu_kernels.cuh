@@ -796,6 +796,65 @@ static __global__ void step1_force_rows(DLat L, ForceW w, const double *__restri
     });
 }
 
+// SF_HomoRing1stO::Matrix1 (SF_HomoRing1stO.cpp:110-160), the ring's
+// profile as a return weight: for every lattice site k (1-based) a walk
+// starts at k with weight G(k) and takes N/2 - 1 steps over the sites
+// 1 .. Mmax (beyond the lattice G = 1; site 0 stays 0), step s updating the
+// window [max(k - s, 1), min(k + s, Mmax)) from the previous values as
+// (a + 4 b + c) G / 6 after the top site has copied its lower neighbour;
+// phi(k) = phibulk sum_z Y(z)^2 / norm0.  One block per site, the walk in
+// two shared-memory buffers of Mmax + 1 values.
+static __global__ void ring_phi(int M, int N, int Mmax, const double *__restrict__ G, double phibulk,
+                                double norm0, double *__restrict__ phi) {
+    extern __shared__ double ring_sh[];
+    __shared__ double red[32];
+    double *Y = ring_sh, *Yn = ring_sh + (Mmax + 1);
+    for (int k = blockIdx.x + 1; k <= M; k += gridDim.x) {
+        for (int z = threadIdx.x; z <= Mmax; z += blockDim.x) Y[z] = (z == k) ? G[k - 1] : 0.0;
+        __syncthreads();
+        for (int st = 1; st < N / 2; st++) {
+            const int zmin = max(k - st, 1), zmax = min(k + st, Mmax);
+            const double ytop = Y[Mmax - 1];
+            for (int z = threadIdx.x; z <= Mmax; z += blockDim.x) {
+                double v = (z == Mmax) ? ytop : Y[z];
+                if (z >= zmin && z < zmax) {
+                    const double a = Y[z - 1], b = Y[z];
+                    const double c = (z + 1 == Mmax) ? ytop : Y[z + 1];
+                    const double gz = (z <= M) ? G[z - 1] / 6.0 : 1.0 / 6.0;
+                    v = gz * (a + 4 * b + c);
+                }
+                Yn[z] = v;
+            }
+            __syncthreads();
+            double *t = Y; Y = Yn; Yn = t;
+        }
+        double acc = 0;
+        for (int z = threadIdx.x + 1; z <= Mmax; z += blockDim.x) acc += Y[z] * Y[z];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w];
+            phi[k - 1] = v / norm0 * phibulk;
+        }
+        __syncthreads();
+    }
+}
+
+// a ring's molecule scalars: SF_HomoRing1stO::Matrix1 leaves lnGN and
+// ln Cb at their initial 0 (SF_Molecule.cpp:269), which the free energy
+// reads; the bulk fraction is the input's
+static __global__ void ring_scalars(int N, double phibulk, MolScal *__restrict__ scal, int self) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    MolScal v;
+    v.lngn = 0;
+    v.phibulk = phibulk;
+    v.lnc = 0;
+    v.norm = phibulk / N;
+    scal[self] = v;
+}
+
 // Dendrimer branch points (SF_Dend1stO.cpp:199-214, :245-253): out = a b / G
 // where G > 0, else 0 -- ConnectG into a zero vector, then CorrectDoubleCountG
 static __global__ void dend_combine(int M, const double *__restrict__ a, const double *__restrict__ b,

@@ -399,11 +399,30 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
             o.N = (int)L;
             o.dend = (L > 1);
         }
+        // branched molecules: the bond tree of the segments (SF_ParserBranched::
+        // FillLinks, SF_ParserBranched.cpp:43-60: every block's first segment
+        // bonds to the last segment of the nearest preceding block of lower
+        // or equal rank)
+        o.tree = 0;
+        o.parent.clear();
+        o.kids.clear();
+        if (md.bond_parent) {
+            if (o.dend) return fail(SFGPU_ERR_INVALID, "a molecule is either a dendrimer or branched");
+            if (K != 1) return fail(SFGPU_ERR_UNSUPPORTED, "branched molecules on second-order lattices");
+            if (md.bond_parent[0] != -1) return fail(SFGPU_ERR_INVALID, "bond_parent[0] must be -1");
+            o.parent.assign(md.bond_parent, md.bond_parent + o.N);
+            o.kids.assign(o.N, {});
+            for (int q = 1; q < o.N; q++) {
+                if (o.parent[q] < 0 || o.parent[q] >= q) return fail(SFGPU_ERR_INVALID, "bond_parent[s] must lie in [0, s)");
+                o.kids[o.parent[q]].push_back(q);
+            }
+            o.tree = (o.N > 1);
+        }
         o.used.clear();
         o.pinned = 0;
         for (int i = 0; i < nseg; i++)
             if (o.count[i]) { o.used.push_back(i); if (freedom[i] == SFGPU_SEG_PINNED) o.pinned = 1; }
-        o.type = (o.N == 1) ? 0 : (o.used.size() == 1 && !o.dend ? 1 : 2);
+        o.type = (o.N == 1) ? 0 : (o.used.size() == 1 && !o.dend && !o.tree ? 1 : 2);
         o.sym = (o.type == 1 && K == 1);
         o.freedom = md.freedom;
         o.phibulk = md.phibulk;
@@ -414,7 +433,7 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
         o.force = (o.type == 0) ? 0.0 : md.force;
         if (o.force != 0) {
             if (!(o.force >= -1000.0 && o.force <= 1000.0)) return fail(SFGPU_ERR_INVALID, "force must lie in [-1000, 1000]");
-            if (K != 1 || o.type != 2 || o.dend)
+            if (K != 1 || o.type != 2 || o.dend || o.tree)
                 return fail(SFGPU_ERR_UNSUPPORTED, "the force ensemble takes first-order linear copolymers");
             if (L.grad == 2 && !L.cyl) return fail(SFGPU_ERR_UNSUPPORTED, "no force ensemble on the 2D flat lattice");
             if (L.ltype != SFGPU_LATTICE_STANDARD) return fail(SFGPU_ERR_UNSUPPORTED, "force ensemble on FCC, HEX or stencils lattices");
@@ -428,6 +447,34 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
             if (!(o.phibulk > 0 && o.phibulk < 1)) return fail(SFGPU_ERR_INVALID, "free molecule needs 0 < phibulk < 1");
         } else {
             return fail(SFGPU_ERR_UNSUPPORTED, "molecule freedom");
+        }
+        // homopolymer ring (SF_MolList1stO.cpp:28-38, SF_HomoRing1stO::Matrix1)
+        o.ring = 0;
+        if (md.ring) {
+            if (o.type != 1 || o.tree) return fail(SFGPU_ERR_INVALID, "only linear homopolymers form rings (SF_MolList1stO.cpp:29-30)");
+            if (o.N % 2 != 0) return fail(SFGPU_ERR_INVALID, "rings have an even length (SF_HomoRing1stO.cpp:120)");
+            if (K != 1 || L.grad != 1 || L.cyl) return fail(SFGPU_ERR_UNSUPPORTED, "rings on lattices other than the 1D flat one");
+            if (o.freedom != SFGPU_MOL_FREE) return fail(SFGPU_ERR_UNSUPPORTED, "rings other than free ones (phibulk)");
+            if (o.pinned) return fail(SFGPU_ERR_UNSUPPORTED, "rings of pinned segments");
+            const int Mmax = (o.N / 2 > M) ? 2 * M : M + o.N / 2;
+            if ((size_t)2 * (Mmax + 1) * sizeof(double) > 200 * 1024) return fail(SFGPU_ERR_UNSUPPORTED, "ring walk larger than shared memory");
+            // NORM[0]: the free ring's return weight, the reference's own loop
+            // (SF_HomoRing1stO.cpp:123-135) on the host
+            const int h = o.N / 2;
+            std::vector<double> X(2 * h + 1, 0.0);
+            auto at = [&](int z) -> double & { return X[z + h]; };
+            at(0) = 1;
+            for (int st = 1; st < h; st++) {
+                double a = 0, b = at(-st - 1), c = at(-st);
+                for (int z = -st; z < st; z++) {
+                    a = b; b = c; c = at(z + 1);
+                    at(z) = (a + 4.0 * b + c) / 6.0;
+                }
+            }
+            double n0 = 0;
+            for (int z = -h; z < h; z++) n0 += at(z) * at(z);
+            o.ring_norm0 = n0;
+            o.ring = 1;
         }
         double cr = 0;   // SF_MolStructure.cpp:411-423
         for (int a : o.used) {
@@ -535,7 +582,8 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     for (auto &o : mols) {
         o.d_phi.assign(nseg, nullptr);
         for (int i : o.used) if ((rc = alloc_d(&o.d_phi[i], M))) return rc;
-        size_t need = (o.type == 0) ? 0 : (size_t)(o.dend ? o.nshort : o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
+        size_t need = (o.type == 0 || o.ring) ? 0
+                      : (size_t)(o.tree ? 3 * o.N : o.dend ? o.nshort : o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
         if (primal_checkpointed(o)) {
             const int k = primal_stride;
             need = (size_t)((o.N + k - 1) / k + k) * K * M;   // checkpoints + one segment
@@ -576,6 +624,7 @@ int sfgpu_system::setup_logspace() {
         return fail(SFGPU_ERR_UNSUPPORTED, "overflow protection needs a first-order 1D or 2D lattice");
     for (auto &o : mols) {
         if (o.dend) return fail(SFGPU_ERR_UNSUPPORTED, "dendrimers with overflow protection");
+        if (o.tree || o.ring) return fail(SFGPU_ERR_UNSUPPORTED, "branched molecules and rings with overflow protection");
         if (o.force != 0) return fail(SFGPU_ERR_UNSUPPORTED, "the force ensemble with overflow protection");
     }
     logmode = true;
@@ -838,9 +887,110 @@ int sfgpu_system::molecule_phi_dend(int m) {
     return SFGPU_OK;
 }
 
+// Branched molecules (SF_Branched1stO::Matrix1, SF_Branched1stO.cpp:1240-1310;
+// combs, SF_Comb1stO): for the bond tree rooted at segment 0,
+//   U(s) = G_s prod_(children c) A U(c)      (the subtree hanging from s,
+//                                             ends inwards, U(leaf) = G),
+//   Q(c) = G_p . A U(c)                       (child c's subtree seen from its
+//                                             parent p),
+//   D(0) = G_0,  D(c) = G_c . A [D(p) prod_(siblings c' != c) Q(c')]
+//                                             (the rest of the molecule seen
+//                                             from c),
+// every product over factors that each carry G_s once divided by G_s (where
+// G > 0, the reference's ConnectG + CorrectDoubleCountG pairs), and
+// phi += U(s) D(s) per segment before the division by G of finalize_phi.
+// lnGN comes from U(0), the whole molecule's propagator at its first
+// segment (Gzs[1][1], SF_Branched1stO.cpp:1269).  U, Q and D take 3 N
+// slices of the chain storage.
+int sfgpu_system::molecule_phi_tree(int m) {
+    HMol &o = mols[m];
+    const DLat &L = H.L;
+    const int g = grid_for(M), N = o.N;
+    cudaStream_t s = stream;
+    auto U = [&](int q) { return d_gi + (size_t)q * M; };
+    auto Q = [&](int q) { return d_gi + (size_t)(N + q) * M; };
+    auto D = [&](int q) { return d_gi + (size_t)(2 * N + q) * M; };
+    const size_t bytes = sizeof(double) * M;
+    for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_phi[i], 0, bytes, s));
+    // ends inwards
+    for (int q = N - 1; q >= 0; q--) {
+        const double *Gq = d_gseg[o.seg[q]];
+        const std::vector<int> &kids = o.kids[q];
+        if (kids.empty()) {
+            SFGPU_CUDA_TRY(cudaMemcpyAsync(U(q), Gq, bytes, cudaMemcpyDeviceToDevice, s));
+        } else if (kids.size() == 1) {
+            SFGPU_CUDA_TRY(cudaMemcpyAsync(U(q), Q(kids[0]), bytes, cudaMemcpyDeviceToDevice, s));
+        } else {
+            // the last product lands in U(q), earlier ones alternate between
+            // the two work slices (no kernel reads and writes one array)
+            const double *acc = Q(kids[0]);
+            int w = 0;
+            for (size_t c = 1; c < kids.size(); c++) {
+                double *dst = (c + 1 == kids.size()) ? U(q) : d_ginv[w];
+                dend_combine<<<g, kBlock, 0, s>>>(M, acc, Q(kids[c]), Gq, dst);
+                acc = dst;
+                w ^= 1;
+            }
+        }
+        if (q > 0) launch_step1(U(q), d_gseg[o.seg[o.parent[q]]], Q(q), nullptr, nullptr, COMP_NONE);
+    }
+    // from segment 0 outwards, composing every segment
+    SFGPU_CUDA_TRY(cudaMemcpyAsync(D(0), d_gseg[o.seg[0]], bytes, cudaMemcpyDeviceToDevice, s));
+    double *const tmp[2] = {d_ginv[0], d_ginv[1]};
+    for (int q = 0; q < N; q++) {
+        const double *Gq = d_gseg[o.seg[q]];
+        connect<<<g, kBlock, 0, s>>>(M, 1, U(q), D(q), o.d_phi[o.seg[q]]);
+        const std::vector<int> &kids = o.kids[q];
+        for (int c : kids) {
+            const double *acc = D(q);
+            int w = 0;
+            for (int c2 : kids) {
+                if (c2 == c) continue;
+                dend_combine<<<g, kBlock, 0, s>>>(M, acc, Q(c2), Gq, tmp[w]);
+                acc = tmp[w];
+                w ^= 1;
+            }
+            launch_step1(acc, d_gseg[o.seg[c]], D(c), nullptr, nullptr, COMP_NONE);
+        }
+    }
+    MolParam p;
+    p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = 0; p.K = 1;
+    p.pinned = o.pinned; p.solvent = (m == solvent); p.nmol = nmol;
+    p.phibulk_in = o.phibulk; p.theta = o.theta;
+    wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, 1, U(0), d_wgn, d_partial);
+    mol_scalars<<<1, 1, 0, s>>>(p, nblocks_red, d_partial, (MolScal *)d_scal, m);
+    for (int i : o.used) {
+        finalize_phi<<<g, kBlock, 0, s>>>(M, d_gseg[i], o.d_phi[i], (const MolScal *)d_scal, m, 0);
+        set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_phi[i]);
+    }
+    return SFGPU_OK;
+}
+
+// homopolymer ring (SF_HomoRing1stO::Matrix1): the profile of every site
+// from its own walk (ring_phi); the boundary layers then hold copies, as the
+// state profile has them once SF_SegmentList::PutSides has run
+// SetBoundaries on it (SF_SegmentList.cpp:524-525)
+int sfgpu_system::molecule_phi_ring(int m) {
+    HMol &o = mols[m];
+    cudaStream_t s = stream;
+    const int Mmax = (o.N / 2 > M) ? 2 * M : M + o.N / 2;
+    const size_t shm = (size_t)2 * (Mmax + 1) * sizeof(double);
+    if (shm > 48 * 1024)
+        SFGPU_CUDA_TRY(cudaFuncSetAttribute(ring_phi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    const int threads = Mmax + 1 >= 256 ? 256 : 64;
+    ring_phi<<<std::min(M, 148 * 8), threads, shm, s>>>(M, o.N, Mmax, d_gseg[o.seg[0]], o.phibulk, o.ring_norm0,
+                                                       o.d_phi[o.seg[0]]);
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    set_boundaries<<<grid_for(M), kBlock, 0, s>>>(H.L, 1, o.d_phi[o.seg[0]]);
+    ring_scalars<<<1, 1, 0, s>>>(o.N, o.phibulk, (MolScal *)d_scal, m);
+    return SFGPU_OK;
+}
+
 int sfgpu_system::molecule_phi(int m) {
     if (logmode) return molecule_phi_log(m);
     if (mols[m].dend) return molecule_phi_dend(m);
+    if (mols[m].tree) return molecule_phi_tree(m);
+    if (mols[m].ring) return molecule_phi_ring(m);
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_for(M);
@@ -1073,7 +1223,8 @@ extern "C" int sfgpu_device_count(int *count) {
 // the full-storage chains (copolymers, second-order chains; not dendrimers,
 // not symmetric homopolymers, which store half a chain) when a stride is set
 bool sfgpu_system::primal_checkpointed(const HMol &o) const {
-    return primal_stride > 0 && primal_stride < o.N && o.type != 0 && !o.dend && !o.sym && !logmode;
+    return primal_stride > 0 && primal_stride < o.N && o.type != 0 && !o.dend && !o.sym && !o.tree && !o.ring &&
+           !logmode;
 }
 
 static int create_system(const sfgpu_system_desc *desc, int stride, sfgpu_system **out) {

@@ -20,6 +20,13 @@ struct HMol {
     // from the centre to an end
     int dend = 0, nshort = 0;
     double force = 0;                 // mol : force (constant-force ensemble)
+    // branched molecule: parent[s] of every segment (parent[0] = -1,
+    // parent[s] < s) and the children of every segment in increasing order
+    int tree = 0;
+    std::vector<int> parent;
+    std::vector<std::vector<int>> kids;
+    int ring = 0;                     // homopolymer ring (SF_HomoRing1stO)
+    double ring_norm0 = 0;            // return weight of the free ring (NORM[0])
     std::vector<std::vector<int>> gen_seg;
     std::vector<int> gen_rep;
     std::vector<double *> d_phi;      // per segment (used ones)
@@ -112,6 +119,8 @@ struct sfgpu_system {
     int setup_logspace();
     int molecule_phi_log(int m);
     int molecule_phi_dend(int m);
+    int molecule_phi_tree(int m);
+    int molecule_phi_ring(int m);
     std::vector<void *> allocs;
 
     ~sfgpu_system();

@@ -29,6 +29,7 @@ int sfgpu_system::ensure_tangent() {
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
         if (o.dend || o.force != 0) return fail_unsupported("derivatives of dendrimers and of the force ensemble");
+        else if (o.tree || o.ring) return fail_unsupported("derivatives of branched molecules and rings");
     if (t_ready) return SFGPU_OK;
     int rc;
     dgfull.assign(nseg, nullptr); dgseg.assign(nseg, nullptr); dphi.assign(nseg, nullptr);

@@ -42,7 +42,7 @@ class MoleculeDesc(C.Structure):
                 ("block_length", C.POINTER(C.c_int)), ("freedom", C.c_int),
                 ("phibulk", C.c_double), ("theta", C.c_double), ("n_generations", C.c_int),
                 ("generation_blocks", C.POINTER(C.c_int)), ("generation_repeat", C.POINTER(C.c_int)),
-                ("force", C.c_double)]
+                ("force", C.c_double), ("bond_parent", C.POINTER(C.c_int)), ("ring", C.c_int)]
 
 
 class SystemDesc(C.Structure):
@@ -155,6 +155,10 @@ class Molecule:
     # functionality f); None for a linear chain
     generations: Optional[List[tuple]] = None
     force: float = 0.0                      # mol : force (constant-force ensemble)
+    # branched molecule: the segment each segment is bonded to on its way to
+    # segment 0 (-1 for segment 0), in the order of `blocks`; None if linear
+    bond_parent: Optional[List[int]] = None
+    ring: bool = False                      # mol : ring (homopolymer ring)
 
     def generation_blocks(self) -> List[List[tuple]]:
         out, b = [], 0
@@ -235,6 +239,15 @@ class SystemSpec:
             mols[m].block_segment, mols[m].block_length = iptr(bs), iptr(bl)
             mols[m].freedom, mols[m].phibulk, mols[m].theta = mol.freedom, mol.phibulk, mol.theta
             mols[m].force = float(mol.force)
+            mols[m].ring = int(bool(mol.ring))
+            if mol.bond_parent is not None:
+                bp = np.ascontiguousarray(mol.bond_parent, dtype=np.int32)
+                if bp.size != mol.N:
+                    raise ValueError(f"bond_parent of molecule {mol.name} has {bp.size} entries, chain has {mol.N}")
+                keep.append(bp)
+                mols[m].bond_parent = iptr(bp)
+            else:
+                mols[m].bond_parent = C.POINTER(C.c_int)()
             if mol.generations:
                 gb = np.array([g[0] for g in mol.generations], dtype=np.int32)
                 gr = np.array([g[1] for g in mol.generations], dtype=np.int32)

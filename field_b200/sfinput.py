@@ -77,6 +77,133 @@ def parse_composition(text: str) -> List[Tuple[str, int]]:
     return [(a, int(b)) for a, b in blocks]
 
 
+def _expand_branch_repeats(t: str) -> str:
+    """SF_ParserBranched::ExpandBrackets (SF_ParserBranched.cpp:94-122): the
+    first '[' that sits inside round brackets expands its enclosing group,
+    '((A)5[(B)1](C)5)2' -> '(A)5[(B)1](C)5(A)5[(B)1](C)5', until none is left."""
+    while True:
+        depth = 0
+        for i, ch in enumerate(t):
+            if ch == "(":
+                depth += 1
+            elif ch == ")":
+                depth -= 1
+            elif ch == "[" and depth > 0:
+                break
+        else:
+            return t
+        # the enclosing '(' to the left and its matching ')' to the right
+        d, lo = -1, i
+        while d < 0 and lo > 0:
+            lo -= 1
+            d += (t[lo] == "(") - (t[lo] == ")")
+        d, hi = 1, i
+        while d > 0 and hi < len(t) - 1:
+            hi += 1
+            d += (t[hi] == "(") - (t[hi] == ")")
+        if d != 0 or t[lo] != "(":
+            raise ValueError(f"composition '{t}': unbalanced brackets around a branch")
+        m = re.match(r"\d*", t[hi + 1:])
+        rep = int(m.group(0)) if m.group(0) else 1
+        t = t[:lo] + t[lo + 1:hi] * rep + t[hi + 1 + len(m.group(0)):]
+
+
+def parse_branched(text: str) -> Optional[Tuple[List[Tuple[str, int]], List[int]]]:
+    """Branched compositions with square brackets (SF_ParserBranched,
+    SF_ParserBranched.h:20-45): the linear fragments between brackets in
+    order, ranked from 1 ('[' raises the next fragment's rank, ']' lowers it,
+    a fragment after '][' takes the previous rank and the ranks before it
+    that are not lower move up by one), and every fragment's first segment
+    bonded to the last segment of the nearest preceding fragment of lower or
+    equal rank (FillLinks, SF_ParserBranched.cpp:43-60).  Returns the blocks
+    of all fragments in order and, per segment, the segment it is bonded to
+    towards segment 0 (-1 for segment 0); None without square brackets."""
+    t = text.replace(" ", "")
+    if "[" not in t and "]" not in t:
+        return None
+    t = _expand_branch_repeats(t)
+    if not t.startswith("["):
+        t = "[" + t + "]"
+    br = [(i, 1 if ch == "[" else -1) for i, ch in enumerate(t) if ch in "[]"]
+    if sum(b for _, b in br) != 0:
+        raise ValueError(f"composition '{text}': square brackets do not match")
+    frags, ranks = [], [0]
+    multi = False
+    for (p0, typ), (p1, _t1) in zip(br, br[1:]):
+        body = t[p0 + 1:p1]
+        if body:
+            if not multi:
+                r = ranks[-1] + typ
+                ranks.append(r)
+            else:
+                r = ranks[-1]
+                k = len(ranks) - 1
+                while k > 0 and ranks[k] >= r:
+                    ranks[k] += 1
+                    k -= 1
+                ranks.append(r)
+                multi = False
+            frags.append(parse_composition(body))
+        elif t[p0:p1 + 1] == "][":
+            multi = True
+        else:
+            raise ValueError(f"composition '{text}': unnecessary square brackets")
+    ranks = ranks[1:]
+    if sum(n for _, n in frags[0]) == 1:
+        raise ValueError(f"composition '{text}': the first linear fragment contains only one monomer")
+    blocks, parent, last = [], [], []
+    for b, fr in enumerate(frags):
+        n = sum(k for _, k in fr)
+        start = len(parent)
+        if b == 0:
+            parent.append(-1)
+        else:
+            i = b - 1
+            while i > 0 and ranks[i] > ranks[b]:
+                i -= 1
+            if ranks[i] > ranks[b]:
+                raise ValueError(f"composition '{text}': fragment {b + 1} has no fragment to branch from")
+            parent.append(last[i])
+        parent.extend(range(start, start + n - 1))
+        last.append(start + n - 1)
+        blocks.extend(fr)
+    return blocks, parent
+
+
+def parse_comb(text: str) -> Optional[Tuple[List[Tuple[str, int]], List[int]]]:
+    """Combs '@dend(NA. Main1, Spacer, Side, Main2)' = Main1-(Spacer-[Side])NA-Main2
+    (SF_MolStructure.cpp:167-181, :242-326; SF_Comb1stO::Matrix1,
+    SF_Comb1stO.cpp:636-760) with linear fragments: the backbone Main1, NA
+    spacers each carrying the side chain on its last segment, then Main2.
+    Returns the blocks in that order and the bond parent of every segment;
+    None for other compositions."""
+    t = text.replace(" ", "")
+    m = re.fullmatch(r"@dend\((\d+)\.(.*)\)", t)
+    if not m:
+        return None
+    na = int(m.group(1))
+    parts = m.group(2).split(",")
+    if na < 1 or len(parts) != 4 or any(("[" in q or "]" in q or ";" in q or "@" in q) for q in parts):
+        raise ValueError(f"composition '{text}': combs with linear main, spacer, side and end fragments only")
+    main1, spacer, side, main2 = (parse_composition(q) for q in parts)
+    blocks, parent = [], []
+
+    def chain(fr, attach):
+        start = len(parent)
+        n = sum(k for _, k in fr)
+        parent.append(attach)
+        parent.extend(range(start, start + n - 1))
+        blocks.extend(fr)
+        return start + n - 1
+
+    end = chain(main1, -1)
+    for _ in range(na):
+        end = chain(spacer, end)
+        chain(side, end)
+    chain(main2, end)
+    return blocks, parent
+
+
 def parse_dendrimer(text: str) -> Optional[List[Tuple[List[Tuple[str, int]], int]]]:
     """Symmetric dendrimer compositions '@dend(G, T1, f1, ..., TG, fG)'
     (SF_MolStructure.cpp:116-140, :348-359): per generation its linear block
@@ -89,7 +216,7 @@ def parse_dendrimer(text: str) -> Optional[List[Tuple[List[Tuple[str, int]], int
         raise ValueError(f"composition '{text}': only symmetric dendrimers @dend(G, T1, f1, ...) are on this path")
     args = m.group(1).split(",")
     if not args[0].isdigit():
-        raise ValueError(f"composition '{text}': asymmetric dendrimers and combs are not on this path")
+        raise ValueError(f"composition '{text}': asymmetric dendrimers are not on this path")
     G = int(args[0])
     if len(args) - 1 != 2 * G or G < 1:
         raise ValueError(f"composition '{text}': @dend(G, ...) needs G generations of (block, functionality)")
@@ -164,8 +291,6 @@ def _refuse_unbuilt(calc: Dict[Key, str]) -> None:
     here: refused by name instead of being ignored."""
     for (c, n, p), v in calc.items():
         lv = v.strip().lower()
-        if c == "mol" and p == "ring" and lv == "true":
-            raise ValueError(f"mol : {n} : ring : true -- ring chains (SF_HomoRing1stO) are not built")
         if c in ("mon", "state") and p == "valence" and float(v) != 0.0:
             raise ValueError(f"{c} : {n} : valence : {v} -- charges and electrostatics are not built")
         if c == "mon" and p.startswith("state"):
@@ -278,22 +403,34 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
     mols: List[Molecule] = []
     for mn in _names(calc, "mol"):
         ctext = _get(calc, "mol", mn, "composition")
-        dend = parse_dendrimer(ctext)
-        gens = None
-        if dend is not None:
-            comp = [b for blocks_i, _f in dend for b in blocks_i]
-            gens = [(len(blocks_i), f) for blocks_i, f in dend]
+        gens, parent = None, None
+        tree = parse_comb(ctext) or parse_branched(ctext)
+        if tree is not None:
+            comp, parent = tree
         else:
-            comp = parse_composition(ctext)
+            dend = parse_dendrimer(ctext)
+            if dend is not None:
+                comp = [b for blocks_i, _f in dend for b in blocks_i]
+                gens = [(len(blocks_i), f) for blocks_i, f in dend]
+            else:
+                comp = parse_composition(ctext)
         blocks = [(seg_names.index(a), n_) for a, n_ in comp]
         length = Molecule(mn, blocks, generations=gens).N
+        rv = _get(calc, "mol", mn, "ring", "false").strip().lower()
+        if rv not in ("true", "false"):
+            raise ValueError(f"mol : {mn} : ring : {rv} is not a boolean")
+        ring = rv == "true"
+        if ring and (parent is not None or gens or len({b[0] for b in blocks}) != 1):
+            raise ValueError(f"mol : {mn} : only homopolymer rings are implemented (SF_MolList1stO.cpp:29-30)")
+        if ring and length % 2:
+            raise ValueError(f"mol : {mn} : rings have an even length (SF_HomoRing1stO.cpp:120)")
         force = float(_get(calc, "mol", mn, "force", "0"))
         if not -1000.0 <= force <= 1000.0:   # SF_Molecule.cpp:42
             raise ValueError(f"mol : {mn} : force must lie in [-1000, 1000]")
         fr = _get(calc, "mol", mn, "freedom", "free")
         if fr == "free":
             mols.append(Molecule(mn, blocks, MOL_FREE, phibulk=float(_get(calc, "mol", mn, "phibulk")),
-                                 generations=gens, force=force))
+                                 generations=gens, force=force, bond_parent=parent, ring=ring))
         elif fr == "restricted":
             th = _get(calc, "mol", mn, "theta")
             if th is None:
@@ -301,10 +438,11 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
                 if nn is None:
                     raise ValueError(f"mol : {mn} needs theta or n")
                 th = float(nn) * length
-            mols.append(Molecule(mn, blocks, MOL_RESTRICTED, theta=float(th), generations=gens, force=force))
+            mols.append(Molecule(mn, blocks, MOL_RESTRICTED, theta=float(th), generations=gens, force=force,
+                                 bond_parent=parent, ring=ring))
         elif fr == "solvent":
-            if gens:
-                raise ValueError(f"mol : {mn} : a dendrimer cannot be the solvent here")
+            if gens or parent is not None or ring:
+                raise ValueError(f"mol : {mn} : a dendrimer, branched molecule or ring cannot be the solvent here")
             mols.append(Molecule(mn, blocks, MOL_SOLVENT))
         else:
             raise ValueError(f"mol : {mn} : freedom : {fr} is not on this path")

@@ -152,6 +152,20 @@ typedef struct {
      * Lat3D1stO.cpp:94-130); 0 for none.  Homopolymers, dendrimers, the 2D
      * flat lattice and overflow protection refuse it as SFbox does. */
     double     force;
+    /* branched first-order molecules: compositions with square brackets
+     * (SF_Branched1stO, parsed by SF_ParserBranched.cpp:3-255) and combs
+     * @dend(n. main1, spacer, side, main2) (SF_Comb1stO).  The bond tree of
+     * the chain's N segments, numbered in the order of the blocks above:
+     * bond_parent[s] (s = 1 .. N-1) is the segment that segment s is bonded
+     * to on its way to segment 0, bond_parent[s] < s, bond_parent[0] = -1.
+     * NULL for linear chains.  Not with dendrimer generations, the force
+     * ensemble, second-order lattices or overflow protection. */
+    const int *bond_parent;
+    /* homopolymer ring (mol : ring : true, SF_MolList1stO.cpp:28-38): the
+     * return-probability profile of SF_HomoRing1stO::Matrix1
+     * (SF_HomoRing1stO.cpp:110-160) -- free rings of even length on a 1D
+     * flat lattice; 0 for none */
+    int        ring;
 } sfgpu_molecule_desc;
 
 typedef struct {

@@ -763,6 +763,12 @@ typedef struct {
     int ngen, nshort;
     int *gen_len, *gen_rep, *gen_seg;   /* gen_seg: positions of all generations in order */
     double force;         /* mol : force, constant-force ensemble */
+    /* branched molecule: parent of every segment (parent[0] = -1) */
+    int tree;
+    int *parent;
+    /* homopolymer ring (SF_HomoRing1stO) and its free return weight NORM[0] */
+    int ring;
+    double ring_norm0;
 } omol;
 
 struct orc_system {
@@ -879,13 +885,46 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
             o->N = N;
             if (N == 1) o->ngen = 0;
         }
-        o->type = (N == 1) ? 0 : (o->nseg_used == 1 && !o->ngen ? 1 : 2);
+        if (md->bond_parent) {
+            /* branched: SF_ParserBranched::FillLinks (SF_ParserBranched.cpp:43-60) as a
+               parent per segment */
+            if (o->ngen || s->L.order != 1 || s->L.logmode) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
+            if (md->bond_parent[0] != -1) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+            o->parent = calloc(N, sizeof(int));
+            o->parent[0] = -1;
+            for (int q = 1; q < N; q++) {
+                if (md->bond_parent[q] < 0 || md->bond_parent[q] >= q) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+                o->parent[q] = md->bond_parent[q];
+            }
+            o->tree = (N > 1);
+        }
+        o->type = (N == 1) ? 0 : (o->nseg_used == 1 && !o->ngen && !o->tree ? 1 : 2);
         o->freedom = md->freedom; o->phibulk = md->phibulk; o->theta = md->theta;
+        if (md->ring) {
+            /* SF_MolList1stO.cpp:28-38; SF_HomoRing1stO.cpp:110-160 on the 1D flat
+               lattice, free rings of even length */
+            if (o->type != 1 || N % 2 || s->L.order != 1 || s->L.grad != 1 || s->L.cyl || s->L.logmode ||
+                o->freedom != SFGPU_MOL_FREE || o->pinned) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
+            int h = N / 2;
+            double *X = calloc(2 * h + 1, sizeof(double));
+            #define XAT(z) X[(z) + h]
+            XAT(0) = 1;
+            for (int st = 1; st < h; st++) {
+                double a = 0, b = XAT(-st - 1), c = XAT(-st);
+                for (int z = -st; z < st; z++) { a = b; b = c; c = XAT(z + 1); XAT(z) = (a + 4.0 * b + c) / 6.0; }
+            }
+            double n0 = 0;
+            for (int z = -h; z < h; z++) n0 += XAT(z) * XAT(z);
+            #undef XAT
+            free(X);
+            o->ring_norm0 = n0;
+            o->ring = 1;
+        }
         o->force = (o->type == 0) ? 0.0 : md->force;
         if (o->force != 0) {
             /* copolymers only (SF_Homopol1stO.cpp:24-27, SF_Dend1stO.cpp:11-14);
                no step on the 2D flat lattice (Lat2DFlat1stO.cpp:115-117) */
-            if (s->L.order != 1 || o->type != 2 || o->ngen || (s->L.grad == 2 && !s->L.cyl) ||
+            if (s->L.order != 1 || o->type != 2 || o->ngen || o->tree || (s->L.grad == 2 && !s->L.cyl) ||
                 s->L.ltype != SFGPU_LATTICE_STANDARD || s->L.logmode) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
         }
         if (o->freedom == SFGPU_MOL_SOLVENT) {
@@ -969,7 +1008,7 @@ void orc_destroy(orc_system *s) {
     olat_free(&s->L);
     for (int m = 0; m < s->nmol; m++) {
         free(s->mol[m].seg); free(s->mol[m].count); free(s->mol[m].used); free(s->mol[m].phi); free(s->mol[m].ori);
-        free(s->mol[m].gen_len); free(s->mol[m].gen_rep); free(s->mol[m].gen_seg);
+        free(s->mol[m].gen_len); free(s->mol[m].gen_rep); free(s->mol[m].gen_seg); free(s->mol[m].parent);
     }
     free(s->mol); free(s->freedom); free(s->range); free(s->chi); free(s->pf);
     free(s->stateQ); free(s->class_of); free(s->rep_of_class); free(s->sites);
@@ -1468,8 +1507,110 @@ static void molecule_phi_dend(orc_system *s, omol *o) {
     free(Gi); free(Ginv); free(tmp); free(add); free(gt);
 }
 
+/* Branched molecules (SF_Branched1stO::Matrix1, SF_Branched1stO.cpp:1240-1310)
+   on the bond tree rooted at segment 0: U(s) = G_s prod_c A U(c) from the ends
+   inwards, Q(c) = G_parent A U(c), D(0) = G_0, D(c) = G_c A [D(p) prod_(c' != c)
+   Q(c')], each product of factors that carry G_s once divided by G_s where
+   G > 0 (ConnectG then CorrectDoubleCountG); phi += U D before the division by
+   G; lnGN from U(0) (SF_Branched1stO.cpp:1269). */
+static void molecule_phi_tree(orc_system *s, omol *o) {
+    olat *L = &s->L;
+    int M = L->M, N = o->N;
+    double *U = calloc((size_t)M * N, sizeof(double)), *Q = calloc((size_t)M * N, sizeof(double));
+    double *D = calloc((size_t)M * N, sizeof(double)), *acc = malloc(sizeof(double) * M);
+    #define SL(A, q) ((A) + (size_t)(q) * M)
+    #define GOF(q) (s->swf + (size_t)o->seg[q] * M)
+    for (int q = N - 1; q >= 0; q--) {
+        const double *Gq = GOF(q);
+        int first = 1;
+        for (int c = q + 1; c < N; c++) {
+            if (o->parent[c] != q) continue;
+            if (first) { memcpy(SL(U, q), SL(Q, c), sizeof(double) * M); first = 0; continue; }
+            for (int z = 0; z < M; z++) SL(U, q)[z] = (Gq[z] > 0) ? (SL(U, q)[z] * SL(Q, c)[z]) / Gq[z] : 0;
+        }
+        if (first) memcpy(SL(U, q), Gq, sizeof(double) * M);
+        if (q > 0) olat_prop1(L, SL(U, q), GOF(o->parent[q]), SL(Q, q));
+    }
+    memcpy(SL(D, 0), GOF(0), sizeof(double) * M);
+    for (int q = 0; q < N; q++) {
+        const double *Gq = GOF(q);
+        double *phi = o->phi + (size_t)o->seg[q] * M;
+        for (int z = 0; z < M; z++) phi[z] += SL(U, q)[z] * SL(D, q)[z];
+        for (int c = q + 1; c < N; c++) {
+            if (o->parent[c] != q) continue;
+            memcpy(acc, SL(D, q), sizeof(double) * M);
+            for (int c2 = q + 1; c2 < N; c2++) {
+                if (o->parent[c2] != q || c2 == c) continue;
+                for (int z = 0; z < M; z++) acc[z] = (Gq[z] > 0) ? (acc[z] * SL(Q, c2)[z]) / Gq[z] : 0;
+            }
+            olat_prop1(L, acc, GOF(c), SL(D, c));
+        }
+    }
+    o->lngn = olat_lngn(L, SL(U, 0));
+    #undef SL
+    #undef GOF
+    for (int a = 0; a < o->nseg_used; a++) {
+        double *phi = o->phi + (size_t)o->used[a] * M;
+        const double *G1 = s->swf + (size_t)o->used[a] * M;
+        for (int z = 0; z < M; z++) { if (G1[z] > 0) phi[z] /= G1[z]; else phi[z] = 0; }
+    }
+    double norm;
+    if (o->freedom == SFGPU_MOL_RESTRICTED) {
+        o->lnc = log(o->theta) - o->lngn - log(1.0 * N);
+        o->phibulk = o->theta / exp(o->lngn);
+        norm = (o->theta / N) / exp(o->lngn);
+    } else {
+        o->lnc = log(o->phibulk / N);
+        norm = o->phibulk / N;
+    }
+    for (int a = 0; a < o->nseg_used; a++) {
+        double *phi = o->phi + (size_t)o->used[a] * M;
+        for (int z = 0; z < M; z++) phi[z] *= norm;
+        olat_set_boundaries(L, phi);
+    }
+    free(U); free(Q); free(D); free(acc);
+}
+
+/* SF_HomoRing1stO::Matrix1 (SF_HomoRing1stO.cpp:110-160) as the reference
+   loops it, 1-based: per site k a walk from k over sites 1 .. Mmax (G = 1
+   beyond the lattice, site 0 absorbing), phi(k) = NORM[k] / NORM[0] phibulk.
+   lnGN and ln Cb keep their initial 0 there (SF_Molecule.cpp:269), which the
+   free energy's entropy term then reads. */
+static void molecule_phi_ring(orc_system *s, omol *o) {
+    int M = s->L.M, N = o->N;
+    int Mmax = (N / 2 > M) ? 2 * M : M + N / 2;
+    const double *G0 = s->swf + (size_t)o->seg[0] * M;   /* 0-based */
+    double *phi = o->phi + (size_t)o->seg[0] * M;
+    double *Y = calloc(Mmax + 1, sizeof(double));
+    for (int k = 1; k <= M; k++) {
+        for (int z = 1; z <= Mmax; z++) Y[z] = (z == k) ? G0[z - 1] : 0;
+        for (int st = 1; st < N / 2; st++) {
+            int zmin = k - st; if (zmin < 1) zmin = 1;
+            int zmax = k + st; if (zmax > Mmax) zmax = Mmax;
+            double a, b = Y[zmin - 1], c = Y[zmin];
+            Y[Mmax] = Y[Mmax - 1];
+            for (int z = zmin; z < zmax; z++) {
+                a = b; b = c; c = Y[z + 1];
+                double gz = (z <= M) ? G0[z - 1] / 6.0 : 1.0 / 6.0;
+                Y[z] = gz * (a + 4 * b + c);
+            }
+        }
+        double nk = 0;
+        for (int z = 1; z <= Mmax; z++) nk += Y[z] * Y[z];
+        phi[k - 1] = nk / o->ring_norm0 * o->phibulk;
+    }
+    free(Y);
+    o->lngn = 0;
+    o->lnc = 0;
+}
+
 static void molecule_phi(orc_system *s, omol *o) {
     if (s->L.logmode) { molecule_phi_log(s, o); return; }
+    if (o->tree || o->ring) {
+        for (int a = 0; a < o->nseg_used; a++) memset(o->phi + (size_t)o->used[a] * s->L.M, 0, sizeof(double) * s->L.M);
+        if (o->tree) molecule_phi_tree(s, o); else molecule_phi_ring(s, o);
+        return;
+    }
     if (o->ngen) { for (int a = 0; a < o->nseg_used; a++) memset(o->phi + (size_t)o->used[a] * s->L.M, 0, sizeof(double) * s->L.M);
                    molecule_phi_dend(s, o); return; }
     olat *L = &s->L;

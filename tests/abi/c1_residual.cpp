@@ -55,8 +55,8 @@ int main(int argc, char **argv) {
     const int pol_seg[1] = {1}, pol_len[1] = {100};
     const int w_seg[1] = {2}, w_len[1] = {1};
     std::vector<sfgpu_molecule_desc> mols(2);
-    mols[0] = sfgpu_molecule_desc{1, pol_seg, pol_len, SFGPU_MOL_FREE, 0.01, 0.0, 0, nullptr, nullptr, 0.0};
-    mols[1] = sfgpu_molecule_desc{1, w_seg, w_len, SFGPU_MOL_SOLVENT, 0.0, 0.0, 0, nullptr, nullptr, 0.0};
+    mols[0] = sfgpu_molecule_desc{1, pol_seg, pol_len, SFGPU_MOL_FREE, 0.01, 0.0, 0, nullptr, nullptr, 0.0, nullptr, 0};
+    mols[1] = sfgpu_molecule_desc{1, w_seg, w_len, SFGPU_MOL_SOLVENT, 0.0, 0.0, 0, nullptr, nullptr, 0.0, nullptr, 0};
 
     sfgpu_system_desc D = {L, (int)segs.size(), segs.data(), chi.data(), nullptr,
                            (int)mols.size(), mols.data(), 0};

@@ -661,4 +661,145 @@ mol : tri : theta : 20
 newton : isaac : tolerance : 1e-12
 start
 """,
+    # branched copolymer (SF_Branched1stO) at an adsorbing surface: two
+    # branch points, one with two side fragments ('][')
+    "1d_branched": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 30
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.5
+mon : B : chi - W : 1.2
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)5[(B)3](A)4[(B)2][(A)3](B)6
+mol : pol : freedom : free
+mol : pol : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # a grafting-free restricted branched molecule next to a free linear one,
+    # with a repeated branched group ((..[..]..)2)
+    "1d_branched_restricted": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 24
+lat : flat : lambda : 0.25
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror2
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.2
+mon : A : chi - W : 0.4
+mon : B : chi - W : 0.9
+mol : br : composition : (A)3((A)2[(B)3](A)1)2(B)2
+mol : br : freedom : restricted
+mol : br : theta : 2.5
+mol : lin : composition : (B)6
+mol : lin : freedom : free
+mol : lin : phibulk : 0.005
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # a branched diblock in a 2D cylinder
+    "2d_branched": """lat : cyl : gradients : 2
+lat : cyl : geometry : cylindrical
+lat : cyl : n_layers_x : 14
+lat : cyl : n_layers_y : 10
+lat : cyl : lambda : 0.16666666666666667
+lat : cyl : lowerbound_x : mirror1
+lat : cyl : upperbound_x : mirror1
+lat : cyl : lowerbound_y : mirror1
+lat : cyl : upperbound_y : mirror1
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 1.4
+mon : B : chi - W : 0.0
+mol : AB : composition : (A)4[(A)3](B)5
+mol : AB : freedom : free
+mol : AB : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # a branched molecule around a 3D colloid
+    "3d_branched": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : n_layers_x : 7
+lat : box : n_layers_y : 6
+lat : box : n_layers_z : 6
+lat : box : lowerbound_x : mirror1
+lat : box : upperbound_x : mirror1
+lat : box : lowerbound_y : periodic
+lat : box : upperbound_y : periodic
+lat : box : lowerbound_z : mirror1
+lat : box : upperbound_z : mirror2
+mon : S : freedom : frozen
+mon : S : frozen_range : 1,1,1;2,2,3
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -1.0
+mon : A : chi - W : 0.6
+mon : B : chi - W : 0.3
+mol : br : composition : (A)3[(B)2][(B)2](A)3
+mol : br : freedom : free
+mol : br : phibulk : 0.02
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # comb @dend(NA. main1, spacer, side, main2) (SF_Comb1stO)
+    "1d_comb": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 30
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -0.8
+mon : A : chi - W : 0.3
+mon : B : chi - W : 0.8
+mol : comb : composition : @dend(3. (A)4, (A)3, (B)4, (A)5)
+mol : comb : freedom : free
+mol : comb : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # homopolymer ring (mol : ring, SF_HomoRing1stO) at an adsorbing surface
+    "1d_ring": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 30
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.5
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)20
+mol : pol : ring : true
+mol : pol : freedom : free
+mol : pol : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
 }

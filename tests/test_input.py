@@ -127,7 +127,7 @@ def test_overflow_protection_statement():
                                  "sys : noname : matrix_approach : second_order\nstart\n")[0])
 
 
-@pytest.mark.parametrize("extra", ["mol : pol : ring : true\n", "mon : A : valence : 1\n",
+@pytest.mark.parametrize("extra", ["mol : pol : ring : maybe\n", "mon : A : valence : 1\n",
                                    "mon : A : state1 : Ap\n", "reaction : r1 : equation : 2(A)=(B)\n",
                                    "lat : flat : n_layers_extended : 40\n"])
 def test_unbuilt_physics_is_refused(extra):
@@ -139,3 +139,45 @@ def test_unbuilt_physics_is_refused(extra):
         build_system(parse_input(base + extra + "start\n")[0])
     # statements without effect on this path are accepted
     build_system(parse_input(base + "mol : pol : save_memory : true\nmon : A : valence : 0\nstart\n")[0])
+
+
+def test_branched_compositions_as_bond_trees():
+    """SF_ParserBranched's rules (SF_ParserBranched.h:20-45): fragments between
+    square brackets, ranks, and every fragment's first segment bonded to the
+    last segment of the nearest preceding fragment of lower or equal rank."""
+    from field_b200.sfinput import parse_branched, parse_comb
+    assert parse_branched("(A)20(B)20") is None
+    blocks, parent = parse_branched("(A)3[(B)2](A)3")
+    assert blocks == [("A", 3), ("B", 2), ("A", 3)]
+    assert parent == [-1, 0, 1, 2, 3, 2, 5, 6]
+    # two side fragments at one point ('][')
+    _, parent = parse_branched("(A)3[(B)2][(C)2](A)3")
+    assert parent == [-1, 0, 1, 2, 3, 2, 5, 2, 7, 8]
+    # a branch inside a side fragment: (C) hangs from the end of (B)
+    _, parent = parse_branched("(A)2[(B)2[(C)1](B)1](A)1")
+    assert parent == [-1, 0, 1, 2, 3, 3, 1]
+    # repeated branched groups expand first (ExpandBrackets)
+    blocks, parent = parse_branched("((A)2[(B)1])2(A)1")
+    assert blocks == [("A", 2), ("B", 1), ("A", 2), ("B", 1), ("A", 1)]
+    assert parent == [-1, 0, 1, 1, 3, 4, 4]
+    for bad in ("(A)3[[(B)2]](A)3", "(A)3[(B)2](A)3]", "(A)1[(B)2](A)3", "(A)3[](A)3"):
+        with pytest.raises(ValueError):
+            parse_branched(bad)
+    # comb: Main1-(Spacer-[Side])NA-Main2
+    blocks, parent = parse_comb("@dend(2. (A)2, (A)1, (B)2, (A)1)")
+    assert blocks == [("A", 2), ("A", 1), ("B", 2), ("A", 1), ("B", 2), ("A", 1)]
+    assert parent == [-1, 0, 1, 2, 3, 2, 5, 6, 5]
+    assert parse_comb("@dend(2, (A)3, 3, (B)2, 2)") is None
+
+
+def test_rings_and_branched_molecules_in_input_files():
+    from field_b200 import configs
+    base = configs.C1_INPUT.format(n=20, N=10, phib=0.01, chi_aw=0.5, chi_as=-1.0).replace("start\n", "")
+    spec, _ = build_system(parse_input(base + "mol : pol : ring : true\nstart\n")[0])
+    assert spec.molecules[0].ring and spec.molecules[0].bond_parent is None
+    odd = configs.C1_INPUT.format(n=20, N=11, phib=0.01, chi_aw=0.5, chi_as=-1.0).replace("start\n", "")
+    with pytest.raises(ValueError):
+        build_system(parse_input(odd + "mol : pol : ring : true\nstart\n")[0])
+    text = base.replace("composition : (A)10", "composition : (A)4[(A)2](A)4") + "start\n"
+    spec, _ = build_system(parse_input(text)[0])
+    assert spec.molecules[0].N == 10 and spec.molecules[0].bond_parent == [-1, 0, 1, 2, 3, 4, 3, 6, 7, 8]
