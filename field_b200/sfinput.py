@@ -204,6 +204,64 @@ def parse_comb(text: str) -> Optional[Tuple[List[Tuple[str, int]], List[int]]]:
     return blocks, parent
 
 
+def _drop_first(fr: List[Tuple[str, int]]) -> List[Tuple[str, int]]:
+    """A linear fragment without its first segment."""
+    if not fr:
+        return []
+    (a, n), rest = fr[0], list(fr[1:])
+    return ([(a, n - 1)] if n > 1 else []) + rest
+
+
+def parse_asym_dendrimer(text: str) -> Optional[Tuple[List[Tuple[str, int]], List[int]]]:
+    """Asymmetric dendrimers '@dend(G; S11, S12, S21, S22, ..., SG1, SG2)'
+    (SF_MolStructure.cpp:141-160, :328-347: one ';' after G and 2G - 1
+    commas; the two fragments of a generation start with the same segment):
+    generation 1's shared first segment is the core with the two arms S11
+    and S12 (the rest of each fragment); every arm end of generation i - 1
+    carries a branch point of generation i, the shared first segment of
+    S_i1 and S_i2, with those two arms (SF_AsymDend1stO::ComputePhi,
+    SF_AsymDend1stO.cpp:206-300).  Returns the blocks in order of
+    construction and the bond parent of every segment; None for other
+    compositions."""
+    t = text.replace(" ", "")
+    m = re.fullmatch(r"@dend\((\d+);(.*)\)", t)
+    if not m:
+        return None
+    G = int(m.group(1))
+    parts = m.group(2).split(",")
+    if G < 1 or len(parts) != 2 * G:
+        raise ValueError(f"composition '{text}': @dend(G; ...) needs two fragments per generation")
+    gens = [(parse_composition(parts[2 * i]), parse_composition(parts[2 * i + 1])) for i in range(G)]
+    for f1, f2 in gens:
+        if f1[0][0] != f2[0][0]:
+            raise ValueError(f"composition '{text}': the two fragments of a generation must start with the same "
+                             "segment (SF_MolStructure.cpp:344-345)")
+    blocks, parent = [], []
+
+    def chain(fr, attach):
+        """append a linear fragment bonded to `attach`; its last segment (or
+        `attach` for an empty fragment)"""
+        n = sum(k for _, k in fr)
+        if n == 0:
+            return attach
+        start = len(parent)
+        parent.append(attach)
+        parent.extend(range(start, start + n - 1))
+        blocks.extend(fr)
+        return start + n - 1
+
+    def generation(f1, f2, attach):
+        first = len(parent)
+        e1 = chain(f1, attach)            # the branch point is f1's first segment
+        e2 = chain(_drop_first(f2), first)
+        return [e1, e2]
+
+    ends = generation(gens[0][0], gens[0][1], -1)
+    for f1, f2 in gens[1:]:
+        ends = [e for a in ends for e in generation(f1, f2, a)]
+    return blocks, parent
+
+
 def parse_dendrimer(text: str) -> Optional[List[Tuple[List[Tuple[str, int]], int]]]:
     """Symmetric dendrimer compositions '@dend(G, T1, f1, ..., TG, fG)'
     (SF_MolStructure.cpp:116-140, :348-359): per generation its linear block
@@ -404,7 +462,7 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
     for mn in _names(calc, "mol"):
         ctext = _get(calc, "mol", mn, "composition")
         gens, parent = None, None
-        tree = parse_comb(ctext) or parse_branched(ctext)
+        tree = parse_comb(ctext) or parse_asym_dendrimer(ctext) or parse_branched(ctext)
         if tree is not None:
             comp, parent = tree
         else:

@@ -802,4 +802,36 @@ mol : pol : phibulk : 0.01
 newton : isaac : tolerance : 1e-12
 start
 """,
+    # asymmetric dendrimer @dend(G; S11, S12, ..., SG1, SG2) (SF_AsymDend1stO);
+    # every generation's second fragment is (A)3 (see ASYM_MIXED below)
+    "1d_asym_dendrimer": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 30
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - W : 0.5
+mon : B : chi - W : 1.2
+mon : A : chi - S : -1.0
+mol : den : composition : @dend(3; (A)2, (A)3, (A)1(B)2, (A)3, (A)2(B)1, (A)3)
+mol : den : freedom : free
+mol : den : phibulk : 0.01
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
 }
+
+# An asymmetric dendrimer whose generations' second fragments differ: SFbox's
+# SF_AsymDend1stO::ComputePhi walks the second arm of generation i < G after
+# its recursive call for generation i + 1 has reassigned the member
+# SegBlock1 (SF_AsymDend1stO.cpp:218-219, :270-272), so those arms take the
+# segments of generation G's second fragment.  Its lnGN is the molecule's
+# partition function and agrees; its profiles do not describe the molecule.
+ASYM_MIXED = INPUTS["1d_asym_dendrimer"].replace(
+    "@dend(3; (A)2, (A)3, (A)1(B)2, (A)3, (A)2(B)1, (A)3)", "@dend(2; (A)3, (A)2, (B)2, (B)3)")

@@ -168,6 +168,15 @@ def test_branched_compositions_as_bond_trees():
     assert blocks == [("A", 2), ("A", 1), ("B", 2), ("A", 1), ("B", 2), ("A", 1)]
     assert parent == [-1, 0, 1, 2, 3, 2, 5, 6, 5]
     assert parse_comb("@dend(2, (A)3, 3, (B)2, 2)") is None
+    # asymmetric dendrimer: core = the shared first segment of generation 1,
+    # every arm end carries the next generation's pair of arms
+    from field_b200.sfinput import parse_asym_dendrimer
+    blocks, parent = parse_asym_dendrimer("@dend(2; (C)1(A)2, (C)1(A)1, (D)1(B)1, (D)1(B)2)")
+    assert sum(n for _, n in blocks) == 12
+    assert parent == [-1, 0, 1, 0, 2, 4, 4, 6, 3, 8, 8, 10]
+    with pytest.raises(ValueError):
+        parse_asym_dendrimer("@dend(2; (A)3, (A)2, (B)2, (A)2)")   # generation 2's fragments start differently
+    assert parse_asym_dendrimer("@dend(2, (A)3, 3, (B)2, 2)") is None
 
 
 def test_rings_and_branched_molecules_in_input_files():

@@ -28,7 +28,7 @@ import pytest
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
 
-from reference_inputs import INPUTS  # noqa: E402
+from reference_inputs import ASYM_MIXED, INPUTS  # noqa: E402
 from field_b200.sfinput import build_system, parse_input  # noqa: E402
 
 REFERENCE = os.path.join(HERE, "golden", "reference_cases.npz")
@@ -171,3 +171,30 @@ def test_gpu_converges_to_reference(gpu_lib, case):
             assert _rel(s.phi(i)[inner], want[i][inner]) <= 1e-10, (case, i)
     Fw = DATA[f"{case}/solve_F"][0]
     assert abs(s.free_energy() - Fw) <= 1e-9 * max(1.0, abs(Fw))
+
+
+@pytest.mark.skipif(not os.path.exists(SFREF), reason="SFbox not built (oracle/_ref/sfref)")
+def test_asym_dendrimer_with_differing_second_fragments_against_live_reference():
+    """Where the generations' second fragments differ, SFbox's profiles
+    follow the last generation's second fragment on every generation's
+    second arm (a member reassigned by the recursion,
+    SF_AsymDend1stO.cpp:218-219, :270-272): the partition function (lnGN)
+    still agrees to rounding, and in the bulk SFbox books one A of the
+    first generation's second arm as B -- A 3 and B 9 of N = 12 instead
+    of A 4 and B 8."""
+    from oracle.oracle import Oracle
+    spec = build_system(parse_input(ASYM_MIXED)[0])[0]
+    o = Oracle(spec)
+    x = np.random.default_rng(17).normal(0.0, 0.3, o.nvar)
+    with tempfile.TemporaryDirectory() as wd:
+        sys.path.insert(0, os.path.join(HERE, "golden"))
+        from make_reference_golden import run_sfref
+        d = run_sfref("eval", ASYM_MIXED, x, wd, "asym_mixed")
+        d0 = run_sfref("eval", ASYM_MIXED, np.zeros(o.nvar), wd, "asym_mixed0")
+    o.residual(x)
+    assert abs(o.lngn(0) - d["mol_den_lngn"][0]) <= 1e-13 * abs(d["mol_den_lngn"][0])
+    o.residual(np.zeros(o.nvar))
+    a, b = spec.segment_index("A"), spec.segment_index("B")
+    N, phib = spec.molecules[0].N, spec.molecules[0].phibulk
+    assert (N, round(o.phi(a)[-3] / phib * N, 9), round(o.phi(b)[-3] / phib * N, 9)) == (12, 4.0, 8.0)
+    assert (round(d0["state_A_phi"][-3] / phib * N, 9), round(d0["state_B_phi"][-3] / phib * N, 9)) == (3.0, 9.0)
