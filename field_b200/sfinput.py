@@ -183,9 +183,13 @@ def parse_comb(text: str) -> Optional[Tuple[List[Tuple[str, int]], List[int]]]:
         return None
     na = int(m.group(1))
     parts = m.group(2).split(",")
-    if na < 1 or len(parts) != 4 or any(("[" in q or "]" in q or ";" in q or "@" in q) for q in parts):
-        raise ValueError(f"composition '{text}': combs with linear main, spacer, side and end fragments only")
-    main1, spacer, side, main2 = (parse_composition(q) for q in parts)
+    if na < 1 or len(parts) != 4 or any(";" in q or "@" in q for q in parts) or \
+            any("[" in parts[i] or "]" in parts[i] for i in (0, 1, 3)):
+        raise ValueError(f"composition '{text}': combs of linear main, spacer and end fragments with a linear or "
+                         "branched side chain only")
+    main1, spacer, main2 = (parse_composition(parts[i]) for i in (0, 1, 3))
+    # a branched side chain hangs from its first segment (SF_Comb1stO.cpp:675-681)
+    side = parse_branched(parts[2]) or (parse_composition(parts[2]), None)
     blocks, parent = [], []
 
     def chain(fr, attach):
@@ -196,10 +200,19 @@ def parse_comb(text: str) -> Optional[Tuple[List[Tuple[str, int]], List[int]]]:
         blocks.extend(fr)
         return start + n - 1
 
+    def hang(tree, attach):
+        fr, par = tree
+        if par is None:
+            chain(fr, attach)
+            return
+        start = len(parent)
+        parent.extend([attach] + [p + start for p in par[1:]])
+        blocks.extend(fr)
+
     end = chain(main1, -1)
     for _ in range(na):
         end = chain(spacer, end)
-        chain(side, end)
+        hang(side, end)
     chain(main2, end)
     return blocks, parent
 

@@ -10,6 +10,28 @@ _SOLVENT_TAIL = """mol : water : composition : (W)1
 mol : water : freedom : solvent
 """
 
+INPUTS_COMB_BRANCHED_SIDE = """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 28
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : A : freedom : free
+mon : B : freedom : free
+mon : W : freedom : free
+mon : A : chi - S : -0.6
+mon : A : chi - W : 0.9
+mon : B : chi - W : 0.2
+mol : comb : composition : @dend(2. (A)2, (B)3, (A)3[(B)1][(B)2](A)1, (A)2)
+mol : comb : freedom : restricted
+mol : comb : theta : 1.5
+""" + _SOLVENT_TAIL + """newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+"""
+
 INPUTS = {
     # Lat1DFlat1stO, the C1 system at reduced size: surface, frozen S
     "1d_flat_surface": """lat : flat : gradients : 1
@@ -825,6 +847,8 @@ mol : den : phibulk : 0.01
 newton : isaac : tolerance : 1e-12
 start
 """,
+    # a comb whose side chains are branched (two fragments at one point)
+    "1d_comb_branched_side": INPUTS_COMB_BRANCHED_SIDE,
 }
 
 # An asymmetric dendrimer whose generations' second fragments differ: SFbox's
