@@ -67,7 +67,6 @@ PROTOTYPES = {
     "sfgpu_batch_info": (i32, [vp, ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "sfgpu_batch_set_stream": (i32, [vp, vp]),
     "sfgpu_batch_set_launch": (i32, [vp, i32, i32]),
-    "sfgpu_batch_set_walk": (i32, [vp, i32]),
     "sfgpu_batch_solve": (i32, [vp, dp, dp, f64, i32, f64, ip, ip, dp]),
     "sfgpu_batch_get_phi": (i32, [vp, i32, i32, dp]),
     "sfgpu_batch_load": (i32, [vp, dp]),

@@ -175,30 +175,22 @@ class BatchSolver:
         kernel (sfgpu_batch_set_launch)."""
         nat.check(self.lib.sfgpu_batch_set_launch(self.h, int(threads), int(bool(stage))), "sfgpu_batch_set_launch")
 
-    def set_walk(self, mode: int):
-        """Walk of the 2D propagator steps (sfgpu_batch_set_walk): 0 rows,
-        1, 2 or 4 the column march with that many 32-site chunks per warp."""
-        nat.check(self.lib.sfgpu_batch_set_walk(self.h, int(mode)), "sfgpu_batch_set_walk")
-
-    def autotune(self, x0, tol=1e-7, maxit=2000, candidates=((1024, True, 0), (1024, True, 2), (1024, True, 4),
-                                                             (512, True, 0), (512, False, 0), (256, True, 0))):
-        """Time one solve per launch shape (threads, staging, 2D walk) from
-        x0 and keep the fastest; returns {(threads, stage, walk): ms}."""
+    def autotune(self, x0, tol=1e-7, maxit=2000, candidates=((1024, True), (512, True), (512, False),
+                                                             (256, True))):
+        """Time one solve per launch shape from x0 and keep the fastest;
+        returns {(threads, stage): ms}."""
         times = {}
-        for cand in candidates:
-            th, stg, walk = (tuple(cand) + (0,))[:3]
+        for th, stg in candidates:
             try:
                 self.set_launch(th, stg)
-                self.set_walk(walk)
             except nat.SfgpuError:
                 continue
             self.load(x0)
             self.solve_resident(tol, maxit)
             self.results()
-            times[(th, stg, walk)] = self.kernel_ms()
+            times[(th, stg)] = self.kernel_ms()
         best = min(times, key=times.get)
-        self.set_launch(best[0], best[1])
-        self.set_walk(best[2])
+        self.set_launch(*best)
         return times
 
     def load(self, x0):

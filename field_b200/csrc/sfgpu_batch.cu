@@ -324,17 +324,6 @@ extern "C" int sfgpu_batch_set_launch(sfgpu_batch *b, int threads, int stage) {
     return configure_stage(b, stage != 0);
 }
 
-// Walk of the 2D propagator steps: 0 the row walk, U = 1, 2 or 4 the column
-// march with U 32-site chunks per warp (march2d).  Results are identical.
-extern "C" int sfgpu_batch_set_walk(sfgpu_batch *b, int mode) {
-    if (!b || !(mode == 0 || mode == 1 || mode == 2 || mode == 4)) return SFGPU_ERR_INVALID;
-    SFGPU_CUDA_TRY(cudaStreamSynchronize(b->stream));
-    for (auto &d : b->desc_h) d.walk2d = mode;
-    SFGPU_CUDA_TRY(cudaMemcpy(b->d_desc, b->desc_h.data(), sizeof(InstDesc) * b->desc_h.size(),
-                              cudaMemcpyHostToDevice));
-    return SFGPU_OK;
-}
-
 // Load the concatenated initial guesses (host) into the device iterate.
 extern "C" int sfgpu_batch_load(sfgpu_batch *b, const double *x) {
     if (!b || !x) return SFGPU_ERR_INVALID;

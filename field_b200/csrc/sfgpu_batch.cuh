@@ -30,8 +30,6 @@ struct InstDesc {
     int gstage;                     // G of the running segment staged in shared memory
     int small1d;                    // 1D symmetric homopolymers: running slices, phi and a ring of
                                     // kRing stored slices in shared memory too
-    int walk2d;                     // 2D steps: 0 row walk (for_interior4), U = 1, 2, 4 the column
-                                    // march of march2d with U 32-site chunks per warp
     long long nvar;
     int freedom[SFGPU_MAX_SEG];
     int class_of[SFGPU_MAX_SEG];
@@ -166,122 +164,6 @@ __device__ inline void finish_molecule(const InstDesc &I, int m, const double *c
 // lattice fits (I.gstage) it is copied once per run into the block's dynamic
 // shared memory and the steps read it there instead of streaming it from L2
 // in every step.
-// One first-order step on a 2D lattice as a column march: a warp owns U
-// consecutive 32-site chunks of a row (y) over a strip of consecutive rows
-// (x) and walks down the strip with rows x-1, x and x+1 of its chunks in
-// registers and row x+2 in flight, the y neighbours coming from the lanes
-// beside it by warp shuffles (loads only at the group's two outer edges).
-// Every source value is read about once per step instead of once per
-// stencil that uses it.  Same operands and operation order as prop1_row.
-// kAcc: the composing backward step, whose phi and other operands of row
-// x+1 are loaded while row x is computed; store(t, out[, phi, other]).
-template <int U, bool kAcc, class S>
-__device__ __forceinline__ void march2d(const DLat &L, int worker, int nworkers, const double *__restrict__ src,
-                                        const double *__restrict__ G, const double *__restrict__ pphi,
-                                        const double *__restrict__ pother, S &&store) {
-    constexpr unsigned kFull = 0xffffffffu;
-    const int MY = L.st[0], nx = L.Md[0] - 2, ny = L.Md[1] - 2;
-    const int lane = worker & 31, warp = worker >> 5, nw = nworkers >> 5;
-    const int nc = (ny + 31) >> 5;                  // 32-site chunks of a row
-    const int ng = (nc + U - 1) / U;                // groups of U chunks
-    int ns = nw / ng;                               // strips of rows
-    ns = ns < 1 ? 1 : (ns > nx ? nx : ns);
-    const int len = (nx + ns - 1) / ns;
-    for (int w = warp; w < ng * ns; w += nw) {
-        const int grp = w % ng, x0 = 1 + (w / ng) * len;
-        if (x0 > nx) continue;                      // warp-uniform
-        const int x1 = min(nx + 1, x0 + len);
-        int yc[U];
-        bool on[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int y = 1 + 32 * (grp * U + u) + lane;
-            on[u] = y <= ny;
-            yc[u] = on[u] ? y : ny;                 // in-range address for idle lanes
-        }
-        // outer edges of the group: the site before its first and after its
-        // last in-row site (mapped at the lattice's own edges)
-        const int yfirst = 1 + 32 * grp * U;
-        const int ylast = min(ny, 32 * (grp + 1) * U);
-        const int ylo = (yfirst == 1) ? L.map_lo[1] : yfirst - 1;
-        const int yhi = (ylast == ny) ? L.map_hi[1] : ylast + 1;
-        const int lastlane = (ylast - 1) & 31, lastu = (ylast - yfirst) >> 5;
-        auto rowof = [&](int x) { return lat_mapc(L, 0, x) * MY; };
-        double pr[U], cu[U], nx1[U], ph[U], ot[U];
-        {
-            const int rp = rowof(x0 - 1), rc = x0 * MY, rn = rowof(x0 + 1);
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                pr[u] = src[rp + yc[u]];
-                cu[u] = src[rc + yc[u]];
-                nx1[u] = src[rn + yc[u]];
-                if (kAcc) { ph[u] = pphi[rc + yc[u]]; ot[u] = pother[rc + yc[u]]; }
-            }
-        }
-        for (int x = x0; x < x1; x++) {
-            double nn[U], phn[U], otn[U];
-            const bool more = x + 1 < x1;           // warp-uniform
-            if (more) {
-                const int r2 = rowof(x + 2), r1 = (x + 1) * MY;
-#pragma unroll
-                for (int u = 0; u < U; u++) {
-                    nn[u] = src[r2 + yc[u]];
-                    if (kAcc) { phn[u] = pphi[r1 + yc[u]]; otn[u] = pother[r1 + yc[u]]; }
-                }
-            }
-            const int rx = x * MY;
-            const double elo = src[rx + ylo], ehi = src[rx + yhi];
-            const double lm = L.cyl ? L.lam_m[x] : 0.0, lp = L.cyl ? L.lam_p[x] : 0.0;
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                double a = __shfl_up_sync(kFull, cu[u], 1);
-                double c = __shfl_down_sync(kFull, cu[u], 1);
-                if (lane == 0) a = (u == 0) ? elo : 0.0;
-                if (lane == 31) c = (u + 1 < U) ? 0.0 : ehi;
-                // chunk seams inside the group: the neighbouring chunk's edge lane
-                if (u > 0) { const double v = __shfl_sync(kFull, cu[u > 0 ? u - 1 : 0], 31); if (lane == 0) a = v; }
-                if (u + 1 < U) { const double v = __shfl_sync(kFull, cu[u + 1 < U ? u + 1 : u], 0); if (lane == 31) c = v; }
-                if (u == lastu && lane == lastlane) c = ehi;
-                const double b = cu[u], uu = pr[u], dd = nx1[u];
-                const int t = rx + yc[u];
-                const double g = G[t];
-                double out;
-                if (L.cyl) {
-                    out = g * (b + lm * (uu - b) + lp * (dd - b) + L.l1 * (a + c - b - b));
-                } else {
-                    const double l0 = 1 - 4 * L.l1;
-                    out = g * (l0 * b + L.l1 * (a + c) + L.l1 * (uu + dd));
-                }
-                if (on[u]) {
-                    if constexpr (kAcc) store(t, out, ph[u], ot[u]);
-                    else store(t, out);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                pr[u] = cu[u];
-                cu[u] = nx1[u];
-                if (more) {
-                    nx1[u] = nn[u];
-                    if (kAcc) { ph[u] = phn[u]; ot[u] = otn[u]; }
-                }
-            }
-        }
-    }
-}
-
-// a 2D step by the walk the instance asks for (row walk or column march)
-template <bool kAcc, class S>
-__device__ __forceinline__ bool march2d_by(const InstDesc &I, const double *src, const double *G,
-                                           const double *pphi, const double *pother, S &&store) {
-    switch (I.walk2d) {
-        case 1: march2d<1, kAcc>(I.L, threadIdx.x, blockDim.x, src, G, pphi, pother, store); return true;
-        case 2: march2d<2, kAcc>(I.L, threadIdx.x, blockDim.x, src, G, pphi, pother, store); return true;
-        case 4: march2d<4, kAcc>(I.L, threadIdx.x, blockDim.x, src, G, pphi, pother, store); return true;
-        default: return false;
-    }
-}
-
 __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared &sh) {
     extern __shared__ double g_stage[];
     const IMol &o = I.mol[m];
@@ -395,10 +277,9 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         for (int t = 1; t < half; t++) {
             const double *src = gi + (size_t)(t - 1) * M;
             double *dst = gi + (size_t)t * M;
-            if (!march2d_by<false>(I, src, G, nullptr, nullptr, [&](int z, double v) { dst[z] = v; }))
-                for_interior4(L, threadIdx.x, blockDim.x,
-                    [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, src, G, k, nlast); },
-                    [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
+            for_interior4(L, threadIdx.x, blockDim.x,
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, src, G, k, nlast); },
+                [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
             __syncthreads();
         }
         const double *cur = gi + (size_t)(half - 1) * M;
@@ -417,17 +298,13 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         for (int sp = (N + 3) / 2; sp <= N; sp++) {
             const double *other = gi + (size_t)(N - sp) * M;
             double *dst = bufA;
-            if (!march2d_by<true>(I, cur, G, phi, other, [&](int z, double out, double ph, double ot) {
+            for_interior4_acc(L, threadIdx.x, blockDim.x, phi, other,
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
+                [&](const RowInfo &R, int k, double out, double ph, double ot) {
+                    const int z = R.base + k;
                     dst[z] = out;
                     phi[z] = ph + out * ot;
-                }))
-                for_interior4_acc(L, threadIdx.x, blockDim.x, phi, other,
-                    [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
-                    [&](const RowInfo &R, int k, double out, double ph, double ot) {
-                        const int z = R.base + k;
-                        dst[z] = out;
-                        phi[z] = ph + out * ot;
-                    });
+                });
             __syncthreads();
             cur = bufA; double *t = bufA; bufA = bufB; bufB = t;
         }
@@ -444,10 +321,9 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         const double *src = gi + (size_t)(t - 1) * M;
         double *dst = gi + (size_t)t * M;
         const double *G = gof(o.seg[t]);
-        if (!march2d_by<false>(I, src, G, nullptr, nullptr, [&](int z, double v) { dst[z] = v; }))
-            for_interior4(L, threadIdx.x, blockDim.x,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, src, G, k, nlast); },
-                [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
+        for_interior4(L, threadIdx.x, blockDim.x,
+            [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, src, G, k, nlast); },
+            [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
         __syncthreads();
     }
     {
@@ -470,17 +346,13 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         const double *gf = gi + (size_t)t * M;
         double *phi = o.phi[sg];
         double *dst = bufA;
-        if (!march2d_by<true>(I, cur, G, phi, gf, [&](int z, double out, double ph, double ot) {
+        for_interior4_acc(L, threadIdx.x, blockDim.x, phi, gf,
+            [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
+            [&](const RowInfo &R, int k, double out, double ph, double ot) {
+                const int z = R.base + k;
                 dst[z] = out;
                 phi[z] = ph + out * ot;
-            }))
-            for_interior4_acc(L, threadIdx.x, blockDim.x, phi, gf,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
-                [&](const RowInfo &R, int k, double out, double ph, double ot) {
-                    const int z = R.base + k;
-                    dst[z] = out;
-                    phi[z] = ph + out * ot;
-                });
+            });
         __syncthreads();
         cur = bufA; double *tt = bufA; bufA = bufB; bufB = tt;
     }

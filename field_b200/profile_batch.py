@@ -25,7 +25,6 @@ def main():
     ap.add_argument("--case", default="c2", choices=["c2", "c4"])
     ap.add_argument("--instances", type=int, default=16)
     ap.add_argument("--threads", type=int, default=0, help="threads per block (0: the library's default)")
-    ap.add_argument("--walk", type=int, default=-1, help="2D step walk: 0 rows, 1/2/4 column march (-1: default)")
     a = ap.parse_args()
     if a.case == "c2":
         insts = [configs.cyl_micelle(seed=sd) for sd in instance_seeds(0, a.instances, configs.BASE_SEED + 2)]
@@ -36,14 +35,12 @@ def main():
     bs = BatchSolver([s for s, _ in insts], m=m, eta=0.1)
     if a.threads:
         bs.set_launch(a.threads, True)
-    if a.walk >= 0:
-        bs.set_walk(a.walk)
     x = np.concatenate([x for _, x in insts])
     for _ in range(2):
         bs.load(x)
         bs.solve_resident(1e-7, maxit)
         r = bs.results()
-    print(json.dumps({"case": a.case, "instances": a.instances, "walk": a.walk, "kernel_ms": bs.kernel_ms(),
+    print(json.dumps({"case": a.case, "instances": a.instances, "kernel_ms": bs.kernel_ms(),
                       "converged": int(r.converged.sum()), "mean_iterations": float(np.mean(r.iterations))}))
 
 

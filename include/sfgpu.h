@@ -494,12 +494,6 @@ int sfgpu_batch_set_stream(sfgpu_batch *batch, void *stream);
  * Results do not depend on it; the autotuner of field_b200.batch times the
  * candidates. */
 int sfgpu_batch_set_launch(sfgpu_batch *batch, int threads, int stage);
-/* walk of the 2D propagator steps: 0 = rows (four positions per lane at a
- * time), 1, 2 or 4 = a column march in which a warp owns that many 32-site
- * chunks of a row over a strip of rows and keeps rows x-1, x, x+1 in
- * registers, reading each value of the source slice about once per step.
- * Results do not depend on it. */
-int sfgpu_batch_set_walk(sfgpu_batch *batch, int mode);
 /* Pure_DIIS (SFNewton::PlainLBFGSDIIS, sfnewton.cpp:566-664) on every
  * instance in one persistent kernel launch: thread blocks take instances
  * from a work queue and iterate them to |f| <= tol on the device.  x_in is

@@ -7,7 +7,6 @@ import os
 import numpy as np
 import pytest
 
-from cases import CASES, random_x
 from field_b200 import configs
 from field_b200.batch import BatchSolver
 from field_b200.system import System
@@ -126,27 +125,3 @@ def test_batch_reports_nonconvergence(gpu_lib):
     res = bs.solve(x0, tol=1e-12, maxit=3)
     assert (res.status == 5).all() and (res.iterations == 3).all()
 
-
-@pytest.mark.parametrize("walk", [1, 2, 4])
-def test_2d_column_march_equals_row_walk(gpu_lib, walk):
-    """The column march of the 2D steps (sfgpu_batch_set_walk) reads each
-    value once and takes y neighbours by warp shuffles; the iterates equal
-    the row walk's bit for bit -- on cylinders whose rows are not a multiple
-    of 32 sites, a flat square lattice with a surface, strips longer and
-    shorter than the warps, and a homopolymer (the half-chain path)."""
-    insts = [configs.cyl_micelle(nx=30, ny=24, nA=8, nB=8, radius=4, seed=300 + i) for i in range(3)]
-    insts += [configs.cyl_micelle(nx=9, ny=70, nA=5, nB=4, radius=3, seed=310)]
-    insts += [(CASES["2d_flat_surface"](), None), (CASES["2d_cylinder"](), None)]
-    specs = [s for s, _ in insts]
-    x0 = np.concatenate([x if x is not None else random_x(s, seed=11, scale=0.2) for s, x in insts])
-    ref = BatchSolver(specs, m=10, eta=0.1)
-    a = ref.solve(x0, tol=1e-9, maxit=40)
-    bs = BatchSolver(specs, m=10, eta=0.1)
-    bs.set_walk(walk)
-    b = bs.solve(x0, tol=1e-9, maxit=40)
-    assert np.array_equal(a.iterations, b.iterations)
-    assert np.array_equal(a.x, b.x)
-    for threads in (256, 512):
-        bs.set_launch(threads, True)
-        c = bs.solve(x0, tol=1e-9, maxit=40)
-        assert np.array_equal(a.x, c.x), threads
