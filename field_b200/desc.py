@@ -17,7 +17,7 @@ BOUND_SURFACE, BOUND_MIRROR1, BOUND_MIRROR2, BOUND_PERIODIC = 1, 2, 3, 4
 GEOM_FLAT, GEOM_CYLINDRICAL, GEOM_SPHERICAL = 0, 1, 2
 LATTICE_STANDARD, LATTICE_STENCILS, LATTICE_FCC, LATTICE_HEX = 0, 1, 2, 3
 SEG_FREE, SEG_FROZEN, SEG_PINNED = 0, 1, 2
-MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT = 0, 1, 2
+MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, MOL_NEUTRALIZER = 0, 1, 2, 3
 
 BOUND_NAMES = {"surface": BOUND_SURFACE, "mirror1": BOUND_MIRROR1,
                "mirror2": BOUND_MIRROR2, "periodic": BOUND_PERIODIC}
@@ -30,11 +30,12 @@ class LatticeDesc(C.Structure):
                 ("layer_adjustment", C.c_double), ("dimensions", C.c_double),
                 ("offset_first_layer", C.c_double), ("stiff_range", C.POINTER(C.c_double)),
                 ("lattice_type", C.c_int),
-                ("lambda_3d", C.c_double * 4)]
+                ("lambda_3d", C.c_double * 4), ("bondlength", C.c_double)]
 
 
 class SegmentDesc(C.Structure):
-    _fields_ = [("freedom", C.c_int), ("range", C.POINTER(C.c_double))]
+    _fields_ = [("freedom", C.c_int), ("range", C.POINTER(C.c_double)), ("valence", C.c_double),
+                ("epsilon", C.c_double)]
 
 
 class MoleculeDesc(C.Structure):
@@ -49,7 +50,8 @@ class SystemDesc(C.Structure):
     _fields_ = [("lattice", LatticeDesc), ("n_segments", C.c_int),
                 ("segments", C.POINTER(SegmentDesc)), ("chi", C.POINTER(C.c_double)),
                 ("pf", C.POINTER(C.c_double)), ("n_molecules", C.c_int),
-                ("molecules", C.POINTER(MoleculeDesc)), ("overflow_protection", C.c_int)]
+                ("molecules", C.POINTER(MoleculeDesc)), ("overflow_protection", C.c_int),
+                ("temperature", C.c_double)]
 
 
 class NewtonSettings(C.Structure):
@@ -85,6 +87,7 @@ class Lattice:
     lattice_type: int = LATTICE_STANDARD
     lambda_3d: Sequence[float] = (0.0, 0.0, 0.0, 0.0)
     stiff_range: Optional[np.ndarray] = None     # M values, 1 inside 'lat : stiff_range'
+    bondlength: float = 3e-10                    # lat : bondlength (m), charged systems
 
     @property
     def shape(self):
@@ -127,6 +130,7 @@ class Lattice:
         d.lattice_type = int(self.lattice_type)
         for k in range(4):
             d.lambda_3d[k] = float(self.lambda_3d[k])
+        d.bondlength = float(self.bondlength)
         if self.stiff_range is not None:
             self._stiff = np.ascontiguousarray(self.stiff_range, dtype=np.float64).reshape(-1)
             if self._stiff.size != self.M:
@@ -142,6 +146,8 @@ class Segment:
     name: str
     freedom: int = SEG_FREE
     range: Optional[np.ndarray] = None      # M range values (frozen/pinned)
+    valence: float = 0.0                    # mon : valence (elementary charges)
+    epsilon: float = 80.0                   # mon : epsilon (relative dielectric constant)
 
 
 @dataclass
@@ -202,6 +208,7 @@ class SystemSpec:
     molecules: List[Molecule]
     pf: Optional[np.ndarray] = None
     overflow_protection: bool = False
+    temperature: float = 298.15             # sys : temperature (K), electrostatic terms
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -220,6 +227,7 @@ class SystemSpec:
         segs = (SegmentDesc * ns)()
         for i, s in enumerate(self.segments):
             segs[i].freedom = s.freedom
+            segs[i].valence, segs[i].epsilon = float(s.valence), float(s.epsilon)
             if s.range is not None:
                 r = np.ascontiguousarray(s.range, dtype=np.float64)
                 if r.size != self.M:
@@ -272,6 +280,7 @@ class SystemSpec:
         d.n_molecules = len(self.molecules)
         d.molecules = C.cast(mols, C.POINTER(MoleculeDesc))
         d.overflow_protection = int(bool(self.overflow_protection))
+        d.temperature = float(self.temperature)
         keep += [segs, mols]
         self._keep = keep
         return d
@@ -327,5 +336,21 @@ class SystemSpec:
                 ok &= ~(np.asarray(s.range).reshape(-1) > 0.999)
         return np.nonzero(ok)[0].astype(np.int64)
 
+    @property
+    def charged(self) -> bool:
+        return any(s.valence != 0 for s in self.segments)
+
+    def potential_sites(self) -> np.ndarray:
+        """Sites whose electrostatic potential is an iteration variable in a
+        charged system (SF_Solve::PotItVar, SF_Solve.cpp:1761-1776): every
+        interior site and every site of a frozen segment's range."""
+        if not self.charged:
+            return np.zeros(0, dtype=np.int64)
+        ok = self.lattice.interior_mask().copy()
+        for s in self.segments:
+            if s.freedom == SEG_FROZEN and s.range is not None:
+                ok |= np.asarray(s.range).reshape(-1) > 0
+        return np.nonzero(ok)[0].astype(np.int64)
+
     def n_itvar(self) -> int:
-        return len(self.itvar_sites()) * self.class_layout()[1]
+        return len(self.itvar_sites()) * self.class_layout()[1] + len(self.potential_sites())

@@ -18,7 +18,8 @@ from typing import Dict, List, Optional, Tuple
 import numpy as np
 
 from .desc import (BOUND_NAMES, BOUND_MIRROR1, BOUND_PERIODIC, GEOM_CYLINDRICAL, GEOM_FLAT, GEOM_SPHERICAL,
-                   LATTICE_FCC, LATTICE_HEX, LATTICE_STANDARD, LATTICE_STENCILS, Lattice, Molecule, MOL_FREE, MOL_RESTRICTED, MOL_SOLVENT, Segment,
+                   LATTICE_FCC, LATTICE_HEX, LATTICE_STANDARD, LATTICE_STENCILS, Lattice, Molecule, MOL_FREE, MOL_NEUTRALIZER,
+                   MOL_RESTRICTED, MOL_SOLVENT, Segment,
                    SEG_FREE, SEG_FROZEN, SEG_PINNED, SystemSpec)
 
 Key = Tuple[str, str, str]
@@ -362,8 +363,8 @@ def _refuse_unbuilt(calc: Dict[Key, str]) -> None:
     here: refused by name instead of being ignored."""
     for (c, n, p), v in calc.items():
         lv = v.strip().lower()
-        if c in ("mon", "state") and p == "valence" and float(v) != 0.0:
-            raise ValueError(f"{c} : {n} : valence : {v} -- charges and electrostatics are not built")
+        if c == "state" and p == "valence" and float(v) != 0.0:
+            raise ValueError(f"{c} : {n} : valence : {v} -- multistate charges are not built")
         if c == "mon" and p.startswith("state"):
             raise ValueError(f"mon : {n} : {p} -- multistate segments are not built")
         if c in ("reaction", "state"):
@@ -460,7 +461,15 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
             segs.append(Segment(sn, SEG_PINNED, _range_mask(lat, _get(calc, "mon", sn, "pinned_range"))))
         else:
             raise ValueError(f"mon : {sn} : freedom : {fr} is not on this path")
+        # charges (SF_Segment.cpp:170-217): valence, relative dielectric constant
+        segs[-1].valence = float(_get(calc, "mon", sn, "valence", "0"))
+        segs[-1].epsilon = float(_get(calc, "mon", sn, "epsilon", "80"))
     ns = len(segs)
+    charged = any(sg.valence != 0 for sg in segs)
+    bl = _get(calc, "lat", ln, "bondlength", None)
+    if charged and bl is None:   # SF_Solve.cpp:169-170
+        raise ValueError(f"lat : {ln} : bondlength must be set in a system with charges")
+    lat.bondlength = float(bl) if bl is not None else 3e-10
     chi = np.zeros((ns, ns))
     pf = np.full((ns, ns), 0.2)
     for i, a in enumerate(seg_names):
@@ -511,6 +520,9 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
                 th = float(nn) * length
             mols.append(Molecule(mn, blocks, MOL_RESTRICTED, theta=float(th), generations=gens, force=force,
                                  bond_parent=parent, ring=ring))
+        elif fr == "neutralizer":
+            # SF_Molecule.cpp:110-126: its bulk fraction neutralises the bulk
+            mols.append(Molecule(mn, blocks, MOL_NEUTRALIZER, generations=gens, bond_parent=parent, ring=ring))
         elif fr == "solvent":
             if gens or parent is not None or ring:
                 raise ValueError(f"mol : {mn} : a dendrimer, branched molecule or ring cannot be the solvent here")
@@ -526,7 +538,11 @@ def build_system(calc: Dict[Key, str]) -> Tuple[SystemSpec, SolverSettings]:
         overflow |= v == "true"
     if overflow and (order != 1 or g == 3):
         raise ValueError("overflow_protection needs a first-order 1D or 2D lattice (SF_System.cpp:395, :478-481)")
-    spec = SystemSpec(lat, segs, chi, mols, pf=pf if order == 2 else None, overflow_protection=overflow)
+    temperature = 298.15
+    for sysname in _names(calc, "sys"):
+        temperature = float(_get(calc, "sys", sysname, "temperature", temperature))
+    spec = SystemSpec(lat, segs, chi, mols, pf=pf if order == 2 else None, overflow_protection=overflow,
+                      temperature=temperature)
     st = SolverSettings()
     for nn in _names(calc, "newton"):
         st.method = _get(calc, "newton", nn, "method", st.method)

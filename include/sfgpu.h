@@ -90,6 +90,9 @@ extern "C" {
 #define SFGPU_MOL_FREE       0
 #define SFGPU_MOL_RESTRICTED 1
 #define SFGPU_MOL_SOLVENT    2
+#define SFGPU_MOL_NEUTRALIZER 3   /* mol : freedom : neutralizer (SF_Molecule.cpp:51,
+                                     :110-126): its bulk fraction makes the bulk
+                                     electroneutral (SF_MolList1stO.cpp:250-266) */
 
 /* solver methods */
 #define SFGPU_METHOD_DIIS      1   /* SFNewton::PlainLBFGSDIIS, sfnewton.cpp:566-664 */
@@ -122,12 +125,23 @@ typedef struct {
                                   [0, 0.5], l0 + 6 l1 + 12 l2 + 8 l3 = 1 within
                                   DBL_EPSILON; lambda3 is then recomputed from
                                   the other three (Lat3D.cpp:246-259) */
+    double bondlength;         /* lat : bondlength in m (Lat1DFlat.cpp:123-137), the
+                                  site distance of the Poisson equation of charged
+                                  systems; 0 = SFbox's default 3e-10 */
 } sfgpu_lattice_desc;
 
 typedef struct {
     int           freedom;     /* SFGPU_SEG_* */
     const double *range;       /* host array of M range values for frozen and
                                   pinned segments (1 inside the range), else NULL */
+    /* charges (mon : X : valence / epsilon, SF_Segment.cpp:170-217): the
+     * valence in elementary charges and the relative dielectric constant
+     * (0 = SFbox's default 80).  Any nonzero valence makes the system
+     * charged: the electrostatic potential psi joins the iteration
+     * variables (SF_Solve.cpp:164-177) -- on the first-order 1D flat
+     * lattice; other lattices return SFGPU_ERR_UNSUPPORTED. */
+    double        valence;
+    double        epsilon;
 } sfgpu_segment_desc;
 
 typedef struct {
@@ -189,6 +203,9 @@ typedef struct {
                                   level propagate and lnGN calls then take and
                                   return logarithms; batches and derivatives
                                   return SFGPU_ERR_UNSUPPORTED. */
+    double                     temperature;
+                               /* sys : temperature in K (SF_System.cpp:68-69) for
+                                  the electrostatic terms; 0 = 298.15 */
 } sfgpu_system_desc;
 
 typedef struct sfgpu_system sfgpu_system;   /* opaque handle, owns device buffers */

@@ -793,7 +793,20 @@ struct orc_system {
     double *rho;          /* nseg*M */
     double *phib;         /* nseg */
     int evaluated;
+    /* charges (SF_Solve.cpp:164-177, :527-591, :794-852): valence and
+       relative dielectric constant per segment; psi joins the iteration
+       variables on the sites of PotItVar (SF_Solve.cpp:1761-1776) */
+    int charged, diffeps, neutralizer;
+    double *val, *eps;
+    double bondlength, temperature;
+    int *xu, *xp;         /* per site: offset of its first u / of its psi in x, -1 if none */
+    double *psi0, *psi, *esq, *lsites;
 };
+
+/* physical constants of SF_Box.h:37-43 */
+#define ORC_BOLTZMANN 1.38065812e-23
+#define ORC_EPS0 8.85418785e-12
+#define ORC_ELEM_CHARGE 1.6021773349e-19
 
 static int chi_rows_equal(const orc_system *s, int a, int b) {
     for (int i = 0; i < s->nseg; i++)
@@ -815,15 +828,30 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
     s->range = calloc((size_t)ns * M, sizeof(double));
     s->chi = calloc((size_t)ns * ns, sizeof(double));
     s->pf = calloc((size_t)ns * ns, sizeof(double));
+    s->val = calloc(ns, sizeof(double));
+    s->eps = calloc(ns, sizeof(double));
+    s->neutralizer = -1;
     for (int i = 0; i < ns; i++) {
         s->freedom[i] = d->segments[i].freedom;
         if (s->freedom[i] != SFGPU_SEG_FREE && d->segments[i].range)
             memcpy(s->range + (size_t)i * M, d->segments[i].range, sizeof(double) * M);
+        s->val[i] = d->segments[i].valence;
+        s->eps[i] = d->segments[i].epsilon != 0 ? d->segments[i].epsilon : 80.0;   /* SF_Segment.cpp:170 */
+        if (s->val[i] != 0) s->charged = 1;
         for (int j = 0; j < ns; j++) {
             s->chi[i * ns + j] = d->chi ? d->chi[i * ns + j] : 0.0;
             s->pf[i * ns + j] = d->pf ? d->pf[i * ns + j] : 0.2;
         }
     }
+    s->bondlength = d->lattice.bondlength > 0 ? d->lattice.bondlength : 3e-10;   /* Lat1DFlat.cpp:128 */
+    s->temperature = d->temperature > 0 ? d->temperature : 298.15;              /* SF_System.cpp:68 */
+    if (s->charged && (s->L.grad != 1 || s->L.cyl || s->L.order != 1 || s->L.logmode)) {
+        orc_destroy(s); return SFGPU_ERR_UNSUPPORTED;
+    }
+    for (int i = 0; i < ns; i++)   /* epsilon differs among liquid states (SF_Solve.cpp:154-162) */
+        for (int j = 0; j < ns; j++)
+            if (s->charged && s->freedom[i] != SFGPU_SEG_FROZEN && s->freedom[j] != SFGPU_SEG_FROZEN &&
+                s->eps[i] != s->eps[j]) s->diffeps = 1;
     /* molecules */
     s->nmol = d->n_molecules;
     s->mol = calloc(s->nmol, sizeof(omol));
@@ -931,6 +959,11 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
             if (s->solvent >= 0) { orc_destroy(s); return SFGPU_ERR_INVALID; }
             s->solvent = m;
         }
+        if (o->freedom == SFGPU_MOL_NEUTRALIZER) {
+            /* SF_Molecule.cpp:110-126; SF_MolList1stO.cpp:250-266 */
+            if (s->neutralizer >= 0 || !s->charged) { orc_destroy(s); return SFGPU_ERR_INVALID; }
+            s->neutralizer = m;
+        }
         /* chemIntRef, SF_MolStructure.cpp:411-423 */
         double cr = 0;
         for (int a = 0; a < o->nseg_used; a++) {
@@ -994,6 +1027,32 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
         if (ok) s->sites[s->nsites++] = z;
     }
     s->nvar = s->nsites * s->nclass;
+    /* charges: psi at every interior site and every site of a frozen
+       segment's range (PotItVar, SF_Solve.cpp:1761-1776), interleaved with
+       the u of the site in x (UpdateSWF, SF_Solve.cpp:797-810) */
+    s->xu = malloc(sizeof(int) * M);
+    s->xp = malloc(sizeof(int) * M);
+    for (int z = 0; z < M; z++) s->xu[z] = s->xp[z] = -1;
+    if (s->charged) {
+        int k = 0, j = 0;
+        for (int z = 0; z < M; z++) {
+            int pot = is_interior(&s->L, z);
+            for (int i = 0; i < ns; i++)
+                if (s->freedom[i] == SFGPU_SEG_FROZEN && s->range[(size_t)i * M + z] > 0) pot = 1;
+            if (pot) s->xp[z] = k++;
+            if (j < s->nsites && s->sites[j] == z) { s->xu[z] = k; k += s->nclass; j++; }
+        }
+        s->nvar = k;
+    } else {
+        for (int j = 0; j < s->nsites; j++) s->xu[s->sites[j]] = j * s->nclass;
+    }
+    s->psi0 = calloc(M, sizeof(double));
+    s->psi = calloc(M, sizeof(double));
+    s->esq = calloc(M, sizeof(double));
+    /* lattice sites per layer (MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269) */
+    s->lsites = malloc(sizeof(double) * M);
+    for (int z = 0; z < M; z++) s->lsites[z] = 1.0;
+    if (s->L.grad == 1 && M > 3) { s->lsites[1] *= s->L.ladj; s->lsites[M - 2] *= 2 - s->L.ladj; }
     s->swf_full = calloc((size_t)ns * M, sizeof(double));
     s->swf = calloc((size_t)ns * M, sizeof(double));
     s->phi = calloc((size_t)ns * M, sizeof(double));
@@ -1010,6 +1069,7 @@ void orc_destroy(orc_system *s) {
         free(s->mol[m].seg); free(s->mol[m].count); free(s->mol[m].used); free(s->mol[m].phi); free(s->mol[m].ori);
         free(s->mol[m].gen_len); free(s->mol[m].gen_rep); free(s->mol[m].gen_seg); free(s->mol[m].parent);
     }
+    free(s->val); free(s->eps); free(s->xu); free(s->xp); free(s->psi0); free(s->psi); free(s->esq); free(s->lsites);
     free(s->mol); free(s->freedom); free(s->range); free(s->chi); free(s->pf);
     free(s->stateQ); free(s->class_of); free(s->rep_of_class); free(s->sites);
     free(s->swf_full); free(s->swf); free(s->phi); free(s->rho); free(s->phib);
@@ -1024,14 +1084,85 @@ int orc_class_of_segment(const orc_system *s, int seg) { return s->class_of[seg]
 
 /* SF_Solve::UpdateSWF (SF_Solve.cpp:794-852) + SF_State/SF_MolState::UpdateSWF
    (SF_State.cpp:281-287, SF_MolState.cpp:147-151) */
+/* Lat1DFlat::ElectricPotential (Lat1DFlat.cpp:526-549): one Jacobi sweep of
+   the Poisson equation with the layer-averaged dielectric constant, 0-based;
+   a surface layer takes its own charge, other boundary layers copy */
+static void olat_poisson_flat(const olat *L, const double *psi0, const double *eps, const double *charge,
+                              double preFactor, double *psi) {
+    int M = L->M;
+    double pf = 2 * preFactor, epsmin, epsplus;
+    if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) {
+        epsmin = eps[M - 2] + eps[M - 1];
+        psi[M - 1] = psi0[M - 2] + pf * charge[M - 1] / epsmin;
+    } else {
+        psi[M - 1] = psi0[mapped_site(L, M - 1, NULL)];
+    }
+    epsplus = eps[0] + eps[1];
+    if (L->bc_lo[0] == SFGPU_BOUND_SURFACE) psi[0] = psi0[1] + pf * charge[0] / epsplus;
+    else psi[0] = psi0[mapped_site(L, 0, NULL)];
+    for (int z = 1; z < M - 1; z++) {
+        epsmin = epsplus;
+        epsplus = eps[z] + eps[z + 1];
+        psi[z] = (epsmin * psi0[z - 1] + pf * charge[z] + epsplus * psi0[z + 1]) / (epsmin + epsplus);
+    }
+}
+
+/* Lat1DFlat::ElectricFieldSquared (Lat1DFlat.cpp:551-570) */
+static void olat_esq_flat(const olat *L, const double *psi, double preFactor, double *esq) {
+    int M = L->M;
+    double pf = preFactor / 2, emin, eplus = psi[0] - psi[1];
+    eplus *= eplus;
+    if (L->bc_lo[0] == SFGPU_BOUND_SURFACE) esq[0] = pf * eplus;
+    for (int z = 1; z < M - 1; z++) {
+        emin = eplus;
+        eplus = psi[z] - psi[z + 1];
+        eplus *= eplus;
+        esq[z] = pf * (emin + eplus);
+    }
+    if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) esq[M - 1] = pf * eplus;
+}
+
+/* SF_SegmentList::GetCharge (SF_SegmentList.cpp:759-784): sum phi valence /
+   phi_T per layer, times the lattice sites of the layer */
+static void state_charge(const orc_system *s, double *charge) {
+    int M = s->L.M;
+    double *pt = calloc(M, sizeof(double));
+    for (int z = 0; z < M; z++) charge[z] = 0;
+    for (int i = 0; i < s->nseg; i++) {
+        const double *p = s->phi + (size_t)i * M;
+        for (int z = 0; z < M; z++) { charge[z] += p[z] * s->val[i]; pt[z] += p[z]; }
+    }
+    for (int z = 0; z < M; z++) charge[z] /= pt[z];
+    for (int z = 0; z < M; z++) charge[z] *= s->lsites[z];
+    free(pt);
+}
+
 static void update_swf(orc_system *s, const double *x) {
     int M = s->L.M, nc = s->nclass;
+    const double kT = ORC_BOLTZMANN * s->temperature;
+    if (s->charged) {
+        /* psi0 from x, its boundary copies and E^2 (SF_Solve.cpp:797-818) */
+        for (int z = 0; z < M; z++) if (s->xp[z] >= 0) s->psi0[z] = x[s->xp[z]];
+        olat_set_boundaries(&s->L, s->psi0);
+        olat_esq_flat(&s->L, s->psi0, (ORC_EPS0 * s->bondlength) / kT, s->esq);
+    }
     for (int i = 0; i < s->nseg; i++) {
         double *gf = s->swf_full + (size_t)i * M;
         memset(gf, 0, sizeof(double) * M);
         int c = s->class_of[i];
         if (c < 0) continue;
-        for (int j = 0; j < s->nsites; j++) gf[s->sites[j]] = exp(-x[j * nc + c]);
+        if (s->charged) {
+            /* exp(-x) times the electrostatic factors of the state
+               (SF_Solve.cpp:808, :819-834) */
+            for (int j = 0; j < s->nsites; j++) {
+                int z = s->sites[j];
+                gf[z] = exp(-x[s->xu[z] + c] - 0.0);
+                gf[z] *= exp(-s->val[i] * s->psi0[z] * ORC_ELEM_CHARGE / kT);
+                if (s->diffeps) gf[z] *= exp(0.5 * s->eps[i] * s->esq[z]);
+            }
+        } else {
+            for (int j = 0; j < s->nsites; j++) gf[s->sites[j]] = exp(-x[j * nc + c]);
+        }
         olat_set_boundaries(&s->L, gf);
         double *g = s->swf + (size_t)i * M;
         if (s->freedom[i] == SFGPU_SEG_PINNED) {
@@ -1773,16 +1904,33 @@ static void molecule_phi(orc_system *s, omol *o) {
 }
 
 /* SF_MolList1stO::ComputePhi (SF_MolList1stO.cpp:246-295) */
+/* SF_Molecule::GetBulkCharge (SF_Molecule.cpp:803-818): valence times the
+   number of each segment in one molecule */
+static double mol_bulk_charge(const orc_system *s, const omol *o) {
+    double q = 0;
+    for (int a = 0; a < o->nseg_used; a++) q += 1.0 * s->val[o->used[a]] * o->count[o->used[a]];
+    return q;
+}
+
 static void compute_phi(orc_system *s) {
     int M = s->L.M;
     double phib_solv = 1.0;
+    double bulkcharge = 0;
     for (int m = 0; m < s->nmol; m++) {
-        if (m == s->solvent) continue;
+        if (m == s->solvent || m == s->neutralizer) continue;
         omol *o = &s->mol[m];
         molecule_phi(s, o);
         if (o->pinned) o->phibulk = 0;   /* SF_Homopol1stO.cpp:124-125 */
-        phib_solv -= o->phibulk;
+        bulkcharge += mol_bulk_charge(s, o) * o->phibulk / o->N;
     }
+    if (s->neutralizer >= 0) {
+        /* SF_MolList1stO.cpp:250-266 */
+        omol *o = &s->mol[s->neutralizer];
+        o->phibulk = -bulkcharge * o->N / mol_bulk_charge(s, o);
+        molecule_phi(s, o);
+    }
+    for (int m = 0; m < s->nmol; m++)
+        if (m != s->solvent) phib_solv -= s->mol[m].phibulk;
     s->mol[s->solvent].phibulk = phib_solv;
     molecule_phi(s, &s->mol[s->solvent]);
     /* state phi and bulk values */
@@ -1809,8 +1957,47 @@ static void compute_phi(orc_system *s) {
    ChemIntBulk/GetPhiTotal (SF_SegmentList.cpp:512-744) */
 static void get_residuals(orc_system *s, double *f) {
     int M = s->L.M, ns = s->nseg, nc = s->nclass;
+    if (s->charged) {
+        /* SF_SegmentList::ComputeElectricPotential(psi0) (SF_SegmentList.cpp:
+           839-860) before PutSides, with the layer-averaged epsilon
+           (GetAverageEpsilon, :785-799) */
+        double *epsav = calloc(M, sizeof(double)), *charge = malloc(sizeof(double) * M);
+        for (int i = 0; i < ns; i++)
+            for (int z = 0; z < M; z++) epsav[z] += s->phi[(size_t)i * M + z] * s->eps[i];
+        state_charge(s, charge);
+        olat_poisson_flat(&s->L, s->psi0, epsav, charge, (ORC_ELEM_CHARGE / ORC_EPS0) / s->bondlength, s->psi);
+        free(epsav); free(charge);
+    }
     for (int i = 0; i < ns; i++) olat_side(&s->L, s->phi + (size_t)i * M, s->rho + (size_t)i * M);
     double *upr = malloc(sizeof(double) * nc);
+    if (s->charged) {
+        const double kT = ORC_BOLTZMANN * s->temperature;
+        for (int z = 0; z < M; z++) {
+            if (s->xp[z] >= 0) f[s->xp[z]] = s->psi0[z] - s->psi[z];
+            if (s->xu[z] < 0) continue;
+            double phit = 0;
+            for (int i = 0; i < ns; i++) phit += s->phi[(size_t)i * M + z];
+            double av = 0;
+            for (int c = 0; c < nc; c++) {
+                int st = s->rep_of_class[c];
+                double u = -log(s->swf_full[(size_t)st * M + z]);
+                double ci = 0, cb = 0;
+                for (int i = 0; i < ns; i++) {
+                    double x = s->chi[st * ns + i];
+                    if (x != 0) { ci += x * s->rho[(size_t)i * M + z]; cb += x * s->phib[i]; }
+                }
+                u -= ci / phit;
+                u += cb;
+                u -= s->val[st] * s->psi0[z] * ORC_ELEM_CHARGE / kT;
+                if (s->diffeps) u += 0.5 * s->eps[st] * s->esq[z];
+                upr[c] = u; av += u;
+            }
+            av /= nc;
+            for (int c = 0; c < nc; c++) f[s->xu[z] + c] = -1.0 + 1.0 / phit + upr[c] - av;
+        }
+        free(upr);
+        return;
+    }
     for (int j = 0; j < s->nsites; j++) {
         int z = s->sites[j];
         double phit = 0;
@@ -1861,10 +2048,25 @@ int orc_get_swf(const orc_system *s, int seg, double *g) {
 
 /* SF_MolList1stO::GetFreeEnergy (SF_MolList1stO.cpp:606-635) with
    GetEntropyProfile (:827-911) and GetContactInteractionsProfile (:914-940) */
+/* SF_MolList1stO::GetElectricInteractionsProfile (SF_MolList1stO.cpp:942-952):
+   1/2 psi q e / kT per layer, q = GetCharge / lattice sites, psi the
+   potential of the last Poisson sweep; NULL when the system has no charges */
+static double *elec_profile(const orc_system *s) {
+    if (!s->charged) return NULL;
+    int M = s->L.M;
+    double *q = malloc(sizeof(double) * M);
+    state_charge(s, q);
+    for (int z = 0; z < M; z++) q[z] /= s->lsites[z];
+    const double kT = ORC_BOLTZMANN * s->temperature;
+    for (int z = 0; z < M; z++) q[z] = 0.5 * s->psi[z] * q[z] * ORC_ELEM_CHARGE / kT;
+    return q;
+}
+
 double orc_free_energy(orc_system *s) {
     if (!s->evaluated) return NAN;
     int M = s->L.M, ns = s->nseg;
     double F = 0;
+    double *el = elec_profile(s);
     for (int z = 0; z < M; z++) {
         double w = s->L.w_f[z];
         if (w == 0) continue;
@@ -1892,8 +2094,9 @@ double orc_free_energy(orc_system *s) {
             }
             contact += 0.5 * s->phi[(size_t)i * M + z] * ci;
         }
-        F += w * (-entropy + contact);
+        F += w * (-entropy + contact + (el ? el[z] : 0.0));
     }
+    free(el);
     return F;
 }
 
@@ -1907,6 +2110,8 @@ int orc_thermo(orc_system *s, double *F, double *Omega, double *fe, double *gp) 
     if (!s->evaluated) return SFGPU_ERR_INVALID;
     int M = s->L.M, ns = s->nseg;
     double Ft = 0, Ot = 0;
+    double *el = elec_profile(s);
+    const double kT = ORC_BOLTZMANN * s->temperature;
     for (int z = 0; z < M; z++) {
         double entropy = 0, contact = 0, omega = 0;
         for (int m = 0; m < s->nmol; m++) {
@@ -1952,6 +2157,7 @@ int orc_thermo(orc_system *s, double *F, double *Omega, double *fe, double *gp) 
                 up = -log(G);
                 up -= ci;
                 up += cb;
+                if (s->charged) up -= s->val[i] * s->psi[z] * ORC_ELEM_CHARGE / kT;
             }
             omega -= up * s->phi[(size_t)i * M + z];
         }
@@ -1965,7 +2171,18 @@ int orc_thermo(orc_system *s, double *F, double *Omega, double *fe, double *gp) 
                 if (p1 > 0) omega += 0.5 * x * s->phib[i] * s->phib[j];
             }
         }
-        double f = -entropy + contact;
+        if (el) {
+            /* SF_MolList1stO.cpp:1074-1096: added on a frozen segment's
+               layers, subtracted elsewhere */
+            int surface = 0;
+            for (int i = 0; i < ns; i++)
+                if (s->freedom[i] == SFGPU_SEG_FROZEN && s->range[(size_t)i * M + z] > 0) surface = 1;
+            /* the electric profile arrives with its boundaries already
+               subtracted and the sum is subtracted once more (SF_MolList1stO.cpp:
+               952, :1098): mirror2 layers take it at 1/4 */
+            omega += surface ? el[z] * s->L.sb[z] : -el[z] * s->L.sb[z];
+        }
+        double f = -entropy + contact + (el ? el[z] : 0.0);
         Ft += s->L.w_f[z] * f;
         Ot += s->L.w_f[z] * omega;
         if (fe) fe[z] = f * s->L.sb[z];
@@ -1973,6 +2190,7 @@ int orc_thermo(orc_system *s, double *F, double *Omega, double *fe, double *gp) 
     }
     if (F) *F = Ft;
     if (Omega) *Omega = Ot;
+    free(el);
     return SFGPU_OK;
 }
 

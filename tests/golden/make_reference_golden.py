@@ -44,11 +44,11 @@ SOLVE_CASES = ["1d_flat_surface", "1d_flat_c1", "1d_flat_mirror2", "1d_flat_peri
                "1d_2nd_lumped", "2d_2nd_lumped", "1d_cyl_2nd", "1d_sphere_2nd", "2d_cyl_2nd", "1d_flat_overflow",
                "2d_cyl_overflow", "1d_dendrimer", "1d_force", "3d_2nd_stiff_range", "3d_2nd_palindrome",
                "1d_branched", "1d_branched_restricted", "2d_branched", "3d_branched", "1d_comb", "1d_ring",
-               "1d_asym_dendrimer", "1d_comb_branched_side"]
+               "1d_asym_dendrimer", "1d_comb_branched_side", "1d_charged", "1d_charged_eps"]
 
 
 NEWTON_CASES = ["1d_flat_c1", "1d_flat_surface", "1d_sphere_colloid", "2d_cylinder_core", "2d_flat_surface",
-                "1d_dendrimer", "1d_2nd_lumped", "1d_force"]
+                "1d_dendrimer", "1d_2nd_lumped", "1d_force", "1d_charged"]
 NEWTON_METHODS = ["pseudohessian", "hessian"]
 
 
@@ -111,7 +111,13 @@ def reference_arrays():
             data[f"{name}/Omega"] = d["Omega"]
             if name in SOLVE_CASES:
                 x0 = rng.normal(0.0, 0.1, spec.n_itvar())
+                if spec.charged:
+                    # a potential of 0.1 V is ~4 kT/e: from such a start SFbox's
+                    # Pure_DIIS overflows on its first step, so charged systems
+                    # start from x = 0
+                    x0 = np.zeros(spec.n_itvar())
                 s = run_sfref("solve", text, x0, wd, name + "_solve")
+                assert np.isfinite(s["g"]).all() and np.linalg.norm(s["g"]) <= 1e-10, name
                 data[f"{name}/solve_x0"] = x0
                 data[f"{name}/solve_x"] = s["x"]
                 data[f"{name}/solve_g"] = s["g"]

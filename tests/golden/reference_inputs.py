@@ -847,6 +847,81 @@ mol : den : phibulk : 0.01
 newton : isaac : tolerance : 1e-12
 start
 """,
+    # charges (SF_Solve.cpp:164-177): a polyelectrolyte at a charged surface
+    # with a 1:1 salt, the anion as neutralizer; Na and Cl share an iteration
+    # variable class (equal chi) and differ by valence
+    "1d_charged": """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 30
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+lat : flat : bondlength : 3e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : S : valence : -0.2
+mon : S : epsilon : 5
+mon : A : freedom : free
+mon : A : valence : 0.5
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - W : 0.5
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)20
+mol : pol : freedom : free
+mol : pol : phibulk : 0.001
+mol : Na : composition : (Na)1
+mol : Na : freedom : free
+mol : Na : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # charges with different dielectric constants of the liquid states
+    # (E^2 terms), a restricted polyelectrolyte, mirror2 above, T = 310 K
+    "1d_charged_eps": """sys : noname : temperature : 310
+lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 30
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror2
+lat : flat : bondlength : 6e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : S : valence : -0.4
+mon : S : epsilon : 5
+mon : A : freedom : free
+mon : A : valence : 0.5
+mon : A : epsilon : 20
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - W : 0.5
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)20
+mol : pol : freedom : restricted
+mol : pol : theta : 1.5
+mol : Na : composition : (Na)1
+mol : Na : freedom : free
+mol : Na : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
     # a comb whose side chains are branched (two fragments at one point)
     "1d_comb_branched_side": INPUTS_COMB_BRANCHED_SIDE,
 }
