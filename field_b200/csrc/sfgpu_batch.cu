@@ -214,6 +214,9 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
     for (int i = 0; i < n && !rc; i++) {
         if (descs[i].lattice.order != 1) { rc = fail_unsupported("batched second-order lattices"); break; }
         if (descs[i].overflow_protection) { rc = fail_unsupported("batched systems with overflow protection"); break; }
+        for (int q = 0; q < descs[i].n_segments && !rc; q++)
+            if (descs[i].segments[q].valence != 0) rc = fail_unsupported("batched charged systems");
+        if (rc) break;
         for (int q = 0; q < descs[i].n_molecules && !rc; q++)
             if (descs[i].molecules[q].n_generations > 0 || descs[i].molecules[q].force != 0 ||
                 descs[i].molecules[q].bond_parent || descs[i].molecules[q].ring)

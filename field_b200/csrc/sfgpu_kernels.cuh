@@ -692,6 +692,7 @@ static __global__ void wsum_partial(int M, int K, const double *__restrict__ g, 
 struct MolParam {
     int N, type, freedom, sym, K, pinned, solvent, nmol;
     double phibulk_in, theta;
+    const double *phib_dev = nullptr;   // device bulk fraction (a neutralizer's), else phibulk_in
 };
 static __global__ void mol_scalars(MolParam p, int nblocks, const double *__restrict__ partial,
                             MolScal *__restrict__ scal, int self) {
@@ -701,7 +702,7 @@ static __global__ void mol_scalars(MolParam p, int nblocks, const double *__rest
     if (p.K > 1) v /= 6.0;   // six bond directions (lumped or not)
     MolScal s;
     s.lngn = log(v);
-    double phib = p.phibulk_in;
+    double phib = p.phib_dev ? *p.phib_dev : p.phibulk_in;
     if (p.solvent) {
         phib = 1.0;
         for (int m = 0; m < p.nmol; m++)
@@ -965,7 +966,8 @@ struct FreeParam {
     double invN[SFGPU_MAX_SEG], lnN[SFGPU_MAX_SEG], chemintref[SFGPU_MAX_SEG];
 };
 static __global__ void free_energy_partial(DLat L, FreeParam fp, ChiTable ct, const double *__restrict__ wf,
-                                    const MolScal *__restrict__ scal, double *__restrict__ partial) {
+                                    const MolScal *__restrict__ scal, double *__restrict__ partial,
+                                    const double *__restrict__ el = nullptr) {
     __shared__ double sh[kBlock];
     double acc = 0;
     for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < L.M; z += gridDim.x * blockDim.x) {
@@ -996,7 +998,8 @@ static __global__ void free_energy_partial(DLat L, FreeParam fp, ChiTable ct, co
             }
             contact += 0.5 * fp.phi[i][z] * ci;
         }
-        acc += w * (-entropy + contact);
+        if (el) acc += w * (-entropy + contact + el[z]);   // charged: + electrostatic profile
+        else acc += w * (-entropy + contact);
     }
     sh[threadIdx.x] = acc;
     __syncthreads();
@@ -1022,6 +1025,10 @@ struct ThermoParam {
     const double *gseg[SFGPU_MAX_SEG], *gfull[SFGPU_MAX_SEG];
     int frozen[SFGPU_MAX_SEG];
     double invN[SFGPU_MAX_SEG], N[SFGPU_MAX_SEG], lnN[SFGPU_MAX_SEG], chemintref[SFGPU_MAX_SEG];
+    // charged systems (null el otherwise): the electrostatic profile, the
+    // potential psi, valences, e / kT and the layers of frozen segments
+    const double *el, *psi, *surf;
+    double val[SFGPU_MAX_SEG], ech, kT;
 };
 static __global__ void thermo_partial(DLat L, ThermoParam tp, ChiTable ct, const double *__restrict__ wf,
                                       const double *__restrict__ sb, const MolScal *__restrict__ scal,
@@ -1083,6 +1090,7 @@ static __global__ void thermo_partial(DLat L, ThermoParam tp, ChiTable ct, const
                 up = -log(G);
                 up -= ci;
                 up += cb;
+                if (tp.el) up -= tp.val[i] * tp.psi[z] * tp.ech / tp.kT;
             }
             omega -= up * tp.phi[i][z];
         }
@@ -1097,7 +1105,12 @@ static __global__ void thermo_partial(DLat L, ThermoParam tp, ChiTable ct, const
                 if (p1 > 0) omega += 0.5 * x * phib[i] * phib[j];
             }
         }
-        const double f = -entropy + contact;
+        if (tp.el) {
+            // SF_MolList1stO.cpp:1074-1096: added on frozen segments' layers,
+            // subtracted elsewhere, boundaries subtracted twice
+            omega += tp.surf[z] != 0 ? tp.el[z] * sb[z] : -tp.el[z] * sb[z];
+        }
+        const double f = tp.el ? -entropy + contact + tp.el[z] : -entropy + contact;
         const double w = wf[z];
         accF += w * f;
         accO += w * omega;

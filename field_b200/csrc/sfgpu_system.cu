@@ -445,7 +445,7 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
             if (!(o.theta > 0)) return fail(SFGPU_ERR_INVALID, "restricted molecule needs theta > 0");
         } else if (o.freedom == SFGPU_MOL_FREE) {
             if (!(o.phibulk > 0 && o.phibulk < 1)) return fail(SFGPU_ERR_INVALID, "free molecule needs 0 < phibulk < 1");
-        } else {
+        } else if (o.freedom != SFGPU_MOL_NEUTRALIZER) {   // checked with the charges
             return fail(SFGPU_ERR_UNSUPPORTED, "molecule freedom");
         }
         // homopolymer ring (SF_MolList1stO.cpp:28-38, SF_HomoRing1stO::Matrix1)
@@ -525,6 +525,7 @@ int sfgpu_system::setup(const sfgpu_system_desc *d) {
     nsites = (int)sites_h.size();
     nvar = (size_t)nsites * nclass;
     if (nsites == 0) return fail(SFGPU_ERR_INVALID, "no sites carry iteration variables");
+    if ((rc = setup_charges(d, jmap))) return rc;
 
     // device buffers
     if ((rc = alloc_d(&d_lam_m, M > 0 ? L.Md[0] : 1))) return rc;
@@ -999,6 +1000,7 @@ int sfgpu_system::molecule_phi(int m) {
     p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = o.sym; p.K = K;
     p.pinned = o.pinned; p.solvent = (m == solvent); p.nmol = nmol;
     p.phibulk_in = o.phibulk; p.theta = o.theta;
+    if (m == neutralizer) { p.freedom = SFGPU_MOL_FREE; p.phib_dev = d_neut_phib; }
     MolScal *scal = (MolScal *)d_scal;
     const size_t KM = (size_t)K * M;
     if (o.type == 0) {
@@ -1156,17 +1158,39 @@ int sfgpu_system::residual_async(const double *x, double *f) {
     const DLat &L = H.L;
     const int g = grid_for(M);
     cudaStream_t s = stream;
-    // segment weighting factors
+    // segment weighting factors; on a charged lattice psi0 and E^2 first
+    if (charged) {
+        q_psi0<<<g, kBlock, 0, s>>>(L, qp, x);
+        q_esq<<<g, kBlock, 0, s>>>(L, qp);
+    }
     for (int i = 0; i < nseg; i++) {
         if (freedom[i] == SFGPU_SEG_FROZEN) continue;
-        swf_update<<<g, kBlock, 0, s>>>(L, x, d_jmap, nclass, class_of[i], d_range[i],
-                                        freedom[i] == SFGPU_SEG_PINNED, d_gfull[i], d_gseg[i]);
+        if (charged)
+            swf_update_q<<<g, kBlock, 0, s>>>(L, qp, x, class_of[i], i, d_range[i], freedom[i] == SFGPU_SEG_PINNED,
+                                              d_gfull[i], d_gseg[i]);
+        else
+            swf_update<<<g, kBlock, 0, s>>>(L, x, d_jmap, nclass, class_of[i], d_range[i],
+                                            freedom[i] == SFGPU_SEG_PINNED, d_gfull[i], d_gseg[i]);
         if (logmode) make_safe<<<g, kBlock, 0, s>>>(M, logc, d_gseg[i], d_lgseg[i]);
     }
-    // molecules, solvent last (SF_MolList1stO.cpp:274-291)
+    // molecules, the neutralizer after the others, solvent last
+    // (SF_MolList1stO.cpp:246-295)
     for (int m = 0; m < nmol; m++) {
-        if (m == solvent) continue;
+        if (m == solvent || m == neutralizer) continue;
         int rc = molecule_phi(m);
+        if (rc) return rc;
+    }
+    if (neutralizer >= 0) {
+        NeutParam np;
+        np.nmol = nmol; np.solvent = solvent; np.self = neutralizer;
+        for (int m = 0; m < nmol; m++) {
+            double q = 0;
+            for (int i : mols[m].used) q += 1.0 * valence[i] * mols[m].count[i];
+            np.q[m] = q;
+            np.n[m] = mols[m].N;
+        }
+        q_neutralizer<<<1, 1, 0, s>>>(np, (const MolScal *)d_scal, d_neut_phib);
+        int rc = molecule_phi(neutralizer);
         if (rc) return rc;
     }
     int rc = molecule_phi(solvent);
@@ -1184,8 +1208,115 @@ int sfgpu_system::residual_async(const double *x, double *f) {
     rp.nsites = nsites; rp.nclass = nclass; rp.nseg = nseg;
     for (int c = 0; c < nclass; c++) { rp.rep[c] = rep_of_class[c]; rp.gfull[c] = d_gfull[rep_of_class[c]]; }
     for (int i = 0; i < nseg; i++) rp.phi[i] = d_phi[i];
-    residual<<<grid_for(nsites), kBlock, 0, s>>>(L, rp, ct, d_sites, d_chib, f);
+    if (charged) {
+        // the Poisson sweep from psi0 before the contact averages
+        // (SF_SegmentList::ComputeElectricPotential, SF_SegmentList.cpp:839-860)
+        PtrList all;
+        all.n = nseg;
+        for (int i = 0; i < nseg; i++) all.p[i] = d_phi[i];
+        q_eps_charge<<<g, kBlock, 0, s>>>(M, nseg, all, qp);
+        q_poisson<<<g, kBlock, 0, s>>>(L, qp);
+        residual_q<<<g, kBlock, 0, s>>>(L, rp, ct, qp, d_chib, f);
+    } else {
+        residual<<<grid_for(nsites), kBlock, 0, s>>>(L, rp, ct, d_sites, d_chib, f);
+    }
     SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
+}
+
+// Charges (SF_Solve.cpp:93-177; SF_Segment.cpp:170-217): valences and
+// dielectric constants, the neutralizer, and the iteration layout of SFbox
+// (per site its psi, then its class potentials: UpdateSWF, SF_Solve.cpp:
+// 797-810).  psi is an iteration variable on the interior sites and on
+// every site of a frozen segment's range (PotItVar, SF_Solve.cpp:1761-1776).
+int sfgpu_system::setup_charges(const sfgpu_system_desc *d, const std::vector<int> &jmap) {
+    const DLat &L = H.L;
+    int rc;
+    valence.assign(nseg, 0.0);
+    epsilon.assign(nseg, 80.0);
+    charged = false;
+    for (int i = 0; i < nseg; i++) {
+        valence[i] = d->segments[i].valence;
+        if (d->segments[i].epsilon != 0) epsilon[i] = d->segments[i].epsilon;
+        if (!std::isfinite(valence[i]) || !std::isfinite(epsilon[i])) return fail(SFGPU_ERR_INVALID, "valence and epsilon must be finite");
+        if (valence[i] != 0) charged = true;
+    }
+    neutralizer = -1;
+    for (int m = 0; m < nmol; m++)
+        if (mols[m].freedom == SFGPU_MOL_NEUTRALIZER) {
+            if (neutralizer >= 0) return fail(SFGPU_ERR_INVALID, "more than one neutralizer");
+            neutralizer = m;
+        }
+    if (!charged) {
+        if (neutralizer >= 0) return fail(SFGPU_ERR_INVALID, "a neutralizer needs charged segments");
+        return SFGPU_OK;
+    }
+    if (K != 1 || L.grad != 1 || L.cyl || logmode)
+        return fail(SFGPU_ERR_UNSUPPORTED, "charges on lattices other than the first-order 1D flat one");
+    auto bulk_charge = [&](const HMol &o) {
+        double q = 0;
+        for (int i : o.used) q += 1.0 * valence[i] * o.count[i];
+        return q;
+    };
+    if (neutralizer >= 0) {
+        const HMol &o = mols[neutralizer];
+        if (o.dend || o.tree || o.ring) return fail(SFGPU_ERR_UNSUPPORTED, "a branched neutralizer");
+        if (bulk_charge(o) == 0) return fail(SFGPU_ERR_INVALID, "the neutralizer carries no charge");
+    } else {
+        for (const auto &o : mols)   // SF_Solve.cpp:100-107
+            if (o.freedom == SFGPU_MOL_FREE && bulk_charge(o) != 0)
+                return fail(SFGPU_ERR_INVALID, "charged free molecules need a neutralizer molecule");
+    }
+    int diffeps = 0;   // SF_Solve.cpp:154-162
+    for (int i = 0; i < nseg; i++)
+        for (int j = 0; j < nseg; j++)
+            if (freedom[i] != SFGPU_SEG_FROZEN && freedom[j] != SFGPU_SEG_FROZEN && epsilon[i] != epsilon[j]) diffeps = 1;
+    // layout
+    std::vector<int> xu(M, -1), xp(M, -1);
+    std::vector<double> surf(M, 0.0);
+    long long k = 0;
+    for (int z = 0; z < M; z++) {
+        int c[3];
+        lat_coords(L, z, c);
+        bool pot = lat_interior(L, c);
+        for (int i = 0; i < nseg; i++)
+            if (freedom[i] == SFGPU_SEG_FROZEN && range_h[(size_t)i * M + z] > 0) { pot = true; surf[z] = 1.0; }
+        if (pot) xp[z] = (int)k++;
+        if (jmap[z] >= 0) { xu[z] = (int)k; k += nclass; }
+    }
+    nvar = (size_t)k;
+    // lattice sites per layer (Lat1DFlat::MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269)
+    const double ladj = d->lattice.layer_adjustment > 0 ? d->lattice.layer_adjustment : 1.0;
+    std::vector<double> ls(M, 1.0);
+    if (M > 3) { ls[1] *= ladj; ls[M - 2] *= 2 - ladj; }
+    memset(&qp, 0, sizeof(qp));
+    qp.diffeps = diffeps;
+    qp.surf_lo = L.bc_lo[0] == SFGPU_BOUND_SURFACE;
+    qp.surf_hi = L.bc_hi[0] == SFGPU_BOUND_SURFACE;
+    qp.map_lo = lat_map(L, 0);
+    qp.map_hi = lat_map(L, M - 1);
+    const double T = d->temperature > 0 ? d->temperature : 298.15;                      // SF_System.cpp:68
+    const double bl = d->lattice.bondlength > 0 ? d->lattice.bondlength : 3e-10;       // Lat1DFlat.cpp:128
+    qp.kT = sfk::kBoltzmann * T;
+    qp.pf_esq = (sfk::kEps0 * bl) / qp.kT;
+    qp.pf_psi = (sfk::kElemCharge / sfk::kEps0) / bl;
+    for (int i = 0; i < nseg; i++) { qp.val[i] = valence[i]; qp.eps[i] = epsilon[i]; }
+    int *dxu, *dxp;
+    double *dls;
+    if ((rc = alloc_i(&dxu, M)) || (rc = alloc_i(&dxp, M)) || (rc = alloc_d(&dls, M))) return rc;
+    if ((rc = alloc_d(&qp.psi0, M)) || (rc = alloc_d(&qp.psi, M)) || (rc = alloc_d(&qp.esq, M)) ||
+        (rc = alloc_d(&qp.epsav, M)) || (rc = alloc_d(&qp.charge, M)) || (rc = alloc_d(&d_el, M)) ||
+        (rc = alloc_d(&d_surf, M)) || (rc = alloc_d(&d_neut_phib, 1)))
+        return rc;
+    SFGPU_CUDA_TRY(cudaMemcpy(dxu, xu.data(), sizeof(int) * M, cudaMemcpyHostToDevice));
+    SFGPU_CUDA_TRY(cudaMemcpy(dxp, xp.data(), sizeof(int) * M, cudaMemcpyHostToDevice));
+    SFGPU_CUDA_TRY(cudaMemcpy(dls, ls.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+    SFGPU_CUDA_TRY(cudaMemcpy(d_surf, surf.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+    for (double *p : {qp.psi0, qp.psi, qp.esq, qp.epsav, qp.charge, d_el, d_neut_phib})
+        SFGPU_CUDA_TRY(cudaMemset(p, 0, sizeof(double) * (p == d_neut_phib ? 1 : M)));
+    qp.xu = dxu;
+    qp.xp = dxp;
+    qp.lsites = dls;
     return SFGPU_OK;
 }
 
@@ -1200,7 +1331,9 @@ int sfgpu_system::free_energy(double *F) {
         fp.chemintref[m] = mols[m].chemintref;
         for (int i : mols[m].used) fp.mphi[m * SFGPU_MAX_SEG + i] = mols[m].d_phi[i];
     }
-    free_energy_partial<<<nblocks_red, kBlock, 0, stream>>>(H.L, fp, ct, d_wf, (const MolScal *)d_scal, d_partial);
+    if (charged) q_elec<<<grid_for(M), kBlock, 0, stream>>>(M, qp, d_el);
+    free_energy_partial<<<nblocks_red, kBlock, 0, stream>>>(H.L, fp, ct, d_wf, (const MolScal *)d_scal, d_partial,
+                                                            charged ? d_el : nullptr);
     finish_sums<<<1, 32, 0, stream>>>(1, nblocks_red, d_partial, d_misc);
     SFGPU_CUDA_TRY(cudaMemcpyAsync(F, d_misc, sizeof(double), cudaMemcpyDeviceToHost, stream));
     SFGPU_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1383,6 +1516,15 @@ int sfgpu_system::thermo(double *F, double *Omega, double *fe, double *gp) {
         tp.lnN[m] = log((double)mols[m].N);
         tp.chemintref[m] = mols[m].chemintref;
         for (int i : mols[m].used) tp.mphi[m * SFGPU_MAX_SEG + i] = mols[m].d_phi[i];
+    }
+    if (charged) {
+        q_elec<<<grid_for(M), kBlock, 0, stream>>>(M, qp, d_el);
+        tp.el = d_el;
+        tp.psi = qp.psi;
+        tp.surf = d_surf;
+        for (int i = 0; i < nseg; i++) tp.val[i] = valence[i];
+        tp.ech = sfk::kElemCharge;
+        tp.kT = qp.kT;
     }
     double *dfe = (fe || gp) ? d_ginv[0] : nullptr, *dgp = (fe || gp) ? d_ginv[1] : nullptr;
     thermo_partial<<<nblocks_red, kBlock, 0, stream>>>(H.L, tp, ct, d_wf, d_sb, (const MolScal *)d_scal, d_phib,

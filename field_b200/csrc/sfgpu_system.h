@@ -2,6 +2,7 @@
 #pragma once
 #include <vector>
 #include "sfgpu_logspace.cuh"
+#include "sfgpu_charge.cuh"
 
 struct HostLat {
     DLat L;
@@ -121,6 +122,14 @@ struct sfgpu_system {
     int molecule_phi_dend(int m);
     int molecule_phi_tree(int m);
     int molecule_phi_ring(int m);
+    // charges (1D flat): valence and dielectric constant per segment, the
+    // neutralizer molecule, psi0/psi/E^2 and the iteration layout
+    bool charged = false;
+    int neutralizer = -1;
+    std::vector<double> valence, epsilon;
+    sfk::QParam qp;
+    double *d_neut_phib = nullptr, *d_el = nullptr, *d_surf = nullptr;
+    int setup_charges(const sfgpu_system_desc *d, const std::vector<int> &jmap);
     std::vector<void *> allocs;
 
     ~sfgpu_system();

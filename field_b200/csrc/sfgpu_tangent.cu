@@ -26,6 +26,7 @@ static int grid_rows_t(const DLat &L) {
 int sfgpu_system::ensure_tangent() {
     if (K == 3 || K == 5) return fail_unsupported("derivatives of the lumped 1D/2D second-order lattices");
     if (logmode) return fail_unsupported("derivatives with overflow protection");
+    if (charged) return fail_unsupported("derivatives of charged systems");
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
         if (o.dend || o.force != 0) return fail_unsupported("derivatives of dendrimers and of the force ensemble");
