@@ -1,11 +1,14 @@
-// sfgpu_charge.cuh -- charged systems on the first-order 1D flat lattice:
+// sfgpu_charge.cuh -- charged systems on the first-order 1D lattices (flat,
+// cylinder, sphere):
 // the electrostatic potential psi as iteration variables next to the
 // segment potentials (SF_Solve.cpp:164-177, :794-852), its Poisson sweep
 // (Lat1DFlat::ElectricPotential, Lat1DFlat.cpp:526-549) and field
 // (Lat1DFlat::ElectricFieldSquared, :551-570), the layer charge and
 // dielectric constant (SF_SegmentList.cpp:759-799), the residual rows of
 // psi and the electrostatic terms of u' (SF_Solve.cpp:527-591), and the
-// electrostatic free-energy profile (SF_MolList1stO.cpp:942-952).  All
+// electrostatic free-energy profile (SF_MolList1stO.cpp:942-952); the
+// curved lattices' sweeps and fields (Lat1DCylinder.cpp:178-240,
+// Lat1DSphere.cpp:76-131).  All
 // arithmetic keeps the reference's operation order; every kernel walks the
 // M sites of the lattice.
 #pragma once
@@ -17,6 +20,7 @@ namespace sfk {
 constexpr double kBoltzmann = 1.38065812e-23;
 constexpr double kEps0 = 8.85418785e-12;
 constexpr double kElemCharge = 1.6021773349e-19;
+constexpr double kPi = 3.141592653589793;   // PI = 4 atan(1) of SF_Box.h:35, as the host computes it
 
 struct QParam {
     int diffeps;                      // dielectric constants differ among liquid states
@@ -28,6 +32,8 @@ struct QParam {
     double val[SFGPU_MAX_SEG], eps[SFGPU_MAX_SEG];
     const int *xu, *xp;               // per site: offset of its first u / of its psi in x, -1 if none
     const double *lsites;             // lattice sites per layer (MultiplyWithLatticeSites)
+    int curved, sph;                  // 1D cylinder / sphere
+    double off1, ladj;                // offset_first_layer, layer adjustment
     double *psi0, *psi, *esq, *epsav, *charge;
 };
 
@@ -81,6 +87,42 @@ static __global__ void swf_update_q(DLat L, QParam q, const double *__restrict__
     }
 }
 
+// radius of layer z's outer edge in the curved sweeps: the reference starts
+// from z0 and adds 1 per layer (Z++), the same additions here
+__device__ __forceinline__ double q_radius(double z0, int z) {
+    double Z = z0;
+    for (int k = 0; k < z; k++) Z++;
+    return Z;
+}
+
+// E^2 on the 1D cylinder (Lat1DCylinder.cpp:211-240) and sphere
+// (Lat1DSphere.cpp:108-131), per layer from its two differences
+static __global__ void q_esq_curved(DLat L, QParam q) {
+    const int M = L.M;
+    const double *p = q.psi0;
+    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < M; z += gridDim.x * blockDim.x) {
+        if (q.sph) {
+            const double pf = q.pf_esq * kPi * 2, z0 = q.off1 + q.ladj - 1;
+            auto ep = [&](int k) { double e = q_radius(z0, k) * (p[k] - p[k + 1]); e *= e; return e; };
+            if (z == 0) { if (q.surf_lo) q.esq[0] = pf * ep(0) / q.lsites[0]; }
+            else if (z == M - 1) { if (q.surf_hi) q.esq[M - 1] = pf * ep(M - 2) / q.lsites[M - 1]; }
+            else q.esq[z] = pf * (ep(z - 1) + ep(z)) / q.lsites[z];
+            continue;
+        }
+        const double pf = q.pf_esq / 2, z0 = q.off1 + q.ladj - 1.5;
+        auto ep = [&](int k) { double e = p[k] - p[k + 1]; e *= (q_radius(z0, k) + 0.5) * e; return e; };
+        if (z == 0) {
+            if (q.off1 > 0 && q.surf_lo) q.esq[0] = pf * ep(0) / q_radius(z0, 0);
+        } else if (z == M - 1) {
+            if (q.surf_hi) q.esq[M - 1] = pf * ep(M - 2) / q_radius(z0, M - 2);
+        } else if (z == 1 && q.off1 <= 0) {
+            q.esq[1] = pf * ep(1) / q_radius(z0, 1);
+        } else {
+            q.esq[z] = pf * (ep(z - 1) + ep(z)) / q_radius(z0, z);
+        }
+    }
+}
+
 // layer dielectric constant sum_i phi_i eps_i and charge sum_i phi_i v_i /
 // phi_T times the layer's lattice sites, states in order
 static __global__ void q_eps_charge(int M, int nseg, PtrList phi, QParam q) {
@@ -112,6 +154,34 @@ static __global__ void q_poisson(DLat L, QParam q) {
         } else {
             const double epsmin = e[z - 1] + e[z], epsplus = e[z] + e[z + 1];
             q.psi[z] = (epsmin * p0[z - 1] + pf * q.charge[z] + epsplus * p0[z + 1]) / (epsmin + epsplus);
+        }
+    }
+}
+
+// the Poisson sweep on the 1D cylinder (Lat1DCylinder.cpp:178-210) and
+// sphere (Lat1DSphere.cpp:76-107): the dielectric sums weighted by the
+// radius (squared on the sphere) of each layer's outer edge; without an
+// offset the first interior layer takes only its outer neighbour; entries
+// the reference leaves unset keep their value
+static __global__ void q_poisson_curved(DLat L, QParam q) {
+    const int M = L.M;
+    const double pf = q.sph ? q.pf_psi / 2 / kPi : q.pf_psi / kPi;
+    const double z0 = q.off1 + q.ladj - 1;
+    const double *e = q.epsav, *p0 = q.psi0;
+    auto W = [&](int k) {
+        const double Z = q_radius(z0, k);
+        return (q.sph ? Z * Z : Z) * (e[k] + e[k + 1]);
+    };
+    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < M; z += gridDim.x * blockDim.x) {
+        if (z == 0) {
+            if (q.off1 > 0 && q.surf_lo) q.psi[0] = p0[1] + pf * q.charge[0] / W(0);
+        } else if (z == M - 1) {
+            if (q.surf_hi) q.psi[M - 1] = p0[M - 2] + pf * q.charge[M - 1] / W(M - 2);
+        } else if (z == 1 && q.off1 <= 0) {
+            q.psi[1] = p0[2] + pf * q.charge[1] / W(1);
+        } else {
+            const double epsmin = W(z - 1), epsplus = W(z);
+            q.psi[z] = (pf * q.charge[z] + p0[z - 1] * epsmin + p0[z + 1] * epsplus) / (epsmin + epsplus);
         }
     }
 }
@@ -162,7 +232,7 @@ static __global__ void residual_q(DLat L, ResParam rp, ChiTable ct, QParam q, co
 static __global__ void q_elec(int M, QParam q, double *__restrict__ el) {
     for (int z = blockIdx.x * blockDim.x + threadIdx.x; z < M; z += gridDim.x * blockDim.x) {
         double c = q.charge[z];
-        c /= q.lsites[z];
+        if (!q.curved || c != 0) c /= q.lsites[z];   // DivideByLatticeSites (curved: nonzero only)
         el[z] = 0.5 * q.psi[z] * c * kElemCharge / q.kT;
     }
 }

@@ -1161,7 +1161,8 @@ int sfgpu_system::residual_async(const double *x, double *f) {
     // segment weighting factors; on a charged lattice psi0 and E^2 first
     if (charged) {
         q_psi0<<<g, kBlock, 0, s>>>(L, qp, x);
-        q_esq<<<g, kBlock, 0, s>>>(L, qp);
+        if (qp.curved) q_esq_curved<<<g, kBlock, 0, s>>>(L, qp);
+        else q_esq<<<g, kBlock, 0, s>>>(L, qp);
     }
     for (int i = 0; i < nseg; i++) {
         if (freedom[i] == SFGPU_SEG_FROZEN) continue;
@@ -1215,7 +1216,8 @@ int sfgpu_system::residual_async(const double *x, double *f) {
         all.n = nseg;
         for (int i = 0; i < nseg; i++) all.p[i] = d_phi[i];
         q_eps_charge<<<g, kBlock, 0, s>>>(M, nseg, all, qp);
-        q_poisson<<<g, kBlock, 0, s>>>(L, qp);
+        if (qp.curved) q_poisson_curved<<<g, kBlock, 0, s>>>(L, qp);
+        else q_poisson<<<g, kBlock, 0, s>>>(L, qp);
         residual_q<<<g, kBlock, 0, s>>>(L, rp, ct, qp, d_chib, f);
     } else {
         residual<<<grid_for(nsites), kBlock, 0, s>>>(L, rp, ct, d_sites, d_chib, f);
@@ -1251,8 +1253,8 @@ int sfgpu_system::setup_charges(const sfgpu_system_desc *d, const std::vector<in
         if (neutralizer >= 0) return fail(SFGPU_ERR_INVALID, "a neutralizer needs charged segments");
         return SFGPU_OK;
     }
-    if (K != 1 || L.grad != 1 || L.cyl || logmode)
-        return fail(SFGPU_ERR_UNSUPPORTED, "charges on lattices other than the first-order 1D flat one");
+    if (K != 1 || L.grad != 1 || logmode)
+        return fail(SFGPU_ERR_UNSUPPORTED, "charges on lattices other than the first-order 1D ones");
     auto bulk_charge = [&](const HMol &o) {
         double q = 0;
         for (int i : o.used) q += 1.0 * valence[i] * o.count[i];
@@ -1288,13 +1290,18 @@ int sfgpu_system::setup_charges(const sfgpu_system_desc *d, const std::vector<in
     // lattice sites per layer (Lat1DFlat::MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269)
     const double ladj = d->lattice.layer_adjustment > 0 ? d->lattice.layer_adjustment : 1.0;
     std::vector<double> ls(M, 1.0);
-    if (M > 3) { ls[1] *= ladj; ls[M - 2] *= 2 - ladj; }
+    if (L.cyl) for (int z = 0; z < M; z++) ls[z] = H.Lx[z];   // Lat1DCylinder.cpp:127-132
+    else if (M > 3) { ls[1] *= ladj; ls[M - 2] *= 2 - ladj; }
     memset(&qp, 0, sizeof(qp));
     qp.diffeps = diffeps;
     qp.surf_lo = L.bc_lo[0] == SFGPU_BOUND_SURFACE;
     qp.surf_hi = L.bc_hi[0] == SFGPU_BOUND_SURFACE;
     qp.map_lo = lat_map(L, 0);
     qp.map_hi = lat_map(L, M - 1);
+    qp.curved = L.cyl;
+    qp.sph = d->lattice.geometry == SFGPU_GEOM_SPHERICAL;
+    qp.off1 = d->lattice.offset_first_layer;
+    qp.ladj = ladj;
     const double T = d->temperature > 0 ? d->temperature : 298.15;                      // SF_System.cpp:68
     const double bl = d->lattice.bondlength > 0 ? d->lattice.bondlength : 3e-10;       // Lat1DFlat.cpp:128
     qp.kT = sfk::kBoltzmann * T;

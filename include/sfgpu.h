@@ -138,8 +138,8 @@ typedef struct {
      * valence in elementary charges and the relative dielectric constant
      * (0 = SFbox's default 80).  Any nonzero valence makes the system
      * charged: the electrostatic potential psi joins the iteration
-     * variables (SF_Solve.cpp:164-177) -- on the first-order 1D flat
-     * lattice; other lattices return SFGPU_ERR_UNSUPPORTED. */
+     * variables (SF_Solve.cpp:164-177) -- on the first-order 1D lattices
+     * (flat, cylinder, sphere); other lattices return SFGPU_ERR_UNSUPPORTED. */
     double        valence;
     double        epsilon;
 } sfgpu_segment_desc;

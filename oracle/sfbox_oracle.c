@@ -41,6 +41,8 @@ typedef struct {
     int bc_lo[3], bc_hi[3];     /* SFGPU_BOUND_* */
     int map_lo[3], map_hi[3];   /* coordinate copied into 0 / Md-1 */
     double l1, l1chi, ladj;
+    int sph;           /* 1D curved: spherical (else cylindrical) */
+    double off1;       /* 1D curved: offset_first_layer */
     double *lam_m, *lam_p, *Lx; /* curved-lattice tables by 0-based x (0..MX-1) */
     double *lamc_m, *lamc_p;    /* 1D curved: contact tables with lambda_chi */
     double *w_gn;      /* weights of interior sites in lnGN sums */
@@ -219,6 +221,8 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
         const double PI_ = 4.0 * atan(1.0);
         int sph = d->geometry == SFGPU_GEOM_SPHERICAL;
         double off = d->offset_first_layer;
+        L->sph = sph;
+        L->off1 = off;
         if (off <= 0 && d->bound_lo[0] == SFGPU_BOUND_SURFACE) return SFGPU_ERR_INVALID;   /* Lat1DCylinder.cpp:50-53 */
         double dim = d->dimensions > 0 ? d->dimensions : 3.0;
         double D = sph ? dim : dim - 1;
@@ -845,7 +849,7 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
     }
     s->bondlength = d->lattice.bondlength > 0 ? d->lattice.bondlength : 3e-10;   /* Lat1DFlat.cpp:128 */
     s->temperature = d->temperature > 0 ? d->temperature : 298.15;              /* SF_System.cpp:68 */
-    if (s->charged && (s->L.grad != 1 || s->L.cyl || s->L.order != 1 || s->L.logmode)) {
+    if (s->charged && (s->L.grad != 1 || s->L.order != 1 || s->L.logmode)) {
         orc_destroy(s); return SFGPU_ERR_UNSUPPORTED;
     }
     for (int i = 0; i < ns; i++)   /* epsilon differs among liquid states (SF_Solve.cpp:154-162) */
@@ -1051,8 +1055,8 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
     s->esq = calloc(M, sizeof(double));
     /* lattice sites per layer (MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269) */
     s->lsites = malloc(sizeof(double) * M);
-    for (int z = 0; z < M; z++) s->lsites[z] = 1.0;
-    if (s->L.grad == 1 && M > 3) { s->lsites[1] *= s->L.ladj; s->lsites[M - 2] *= 2 - s->L.ladj; }
+    for (int z = 0; z < M; z++) s->lsites[z] = s->L.cyl ? s->L.Lx[z] : 1.0;   /* curved: Lat1DCylinder.cpp:127-132 */
+    if (s->L.grad == 1 && !s->L.cyl && M > 3) { s->lsites[1] *= s->L.ladj; s->lsites[M - 2] *= 2 - s->L.ladj; }
     s->swf_full = calloc((size_t)ns * M, sizeof(double));
     s->swf = calloc((size_t)ns * M, sizeof(double));
     s->phi = calloc((size_t)ns * M, sizeof(double));
@@ -1122,6 +1126,87 @@ static void olat_esq_flat(const olat *L, const double *psi, double preFactor, do
     if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) esq[M - 1] = pf * eplus;
 }
 
+/* Lat1DCylinder::ElectricPotential (Lat1DCylinder.cpp:178-210) and
+   Lat1DSphere::ElectricPotential (Lat1DSphere.cpp:76-107), 0-based: the
+   sweep weighted by the radius (cylinder) or its square (sphere) of the
+   outer edge of each layer; without an offset the first interior layer
+   takes only its outer neighbour.  Entries the reference leaves unset keep
+   their previous value.  The cylinder sets psi0's boundaries first. */
+static void olat_poisson_curved(const olat *L, double *psi0, const double *eps, const double *charge,
+                                double preFactor, double *psi) {
+    const double PI_ = 4.0 * atan(1.0);
+    int M = L->M, z;
+    double Z, pf, epsmin, epsplus;
+    if (!L->sph) olat_set_boundaries(L, psi0);
+    pf = L->sph ? preFactor / 2 / PI_ : preFactor / PI_;
+    Z = L->off1 + L->ladj - 1;
+    #define RW(Z) (L->sph ? (Z) * (Z) : (Z))
+    if (L->off1 <= 0) {
+        Z++;
+        epsplus = RW(Z) * (eps[1] + eps[2]);
+        psi[1] = psi0[2] + pf * charge[1] / epsplus;
+        z = 2;
+    } else {
+        epsplus = RW(Z) * (eps[0] + eps[1]);
+        if (L->bc_lo[0] == SFGPU_BOUND_SURFACE) psi[0] = psi0[1] + pf * charge[0] / epsplus;
+        z = 1;
+    }
+    for (; z < M - 1; z++) {
+        Z++;
+        epsmin = epsplus;
+        epsplus = RW(Z) * (eps[z] + eps[z + 1]);
+        psi[z] = (pf * charge[z] + psi0[z - 1] * epsmin + psi0[z + 1] * epsplus) / (epsmin + epsplus);
+    }
+    #undef RW
+    if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) psi[M - 1] = psi0[M - 2] + pf * charge[M - 1] / epsplus;
+}
+
+/* Lat1DCylinder::ElectricFieldSquared (Lat1DCylinder.cpp:211-240) and
+   Lat1DSphere::ElectricFieldSquared (Lat1DSphere.cpp:108-131), 0-based */
+static void olat_esq_curved(const olat *L, const double *psi, double preFactor, double *esq) {
+    const double PI_ = 4.0 * atan(1.0);
+    int M = L->M, z;
+    double Z, pf, emin, eplus;
+    if (L->sph) {
+        pf = preFactor * PI_ * 2;
+        Z = L->off1 + L->ladj - 1;
+        eplus = Z * (psi[0] - psi[1]);
+        eplus *= eplus;
+        if (L->bc_lo[0] == SFGPU_BOUND_SURFACE) esq[0] = pf * eplus / L->Lx[0];
+        for (z = 1; z < M - 1; z++) {
+            Z++;
+            emin = eplus;
+            eplus = Z * (psi[z] - psi[z + 1]);
+            eplus *= eplus;
+            esq[z] = pf * (emin + eplus) / L->Lx[z];
+        }
+        if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) esq[M - 1] = pf * eplus / L->Lx[M - 1];
+        return;
+    }
+    pf = preFactor / 2;
+    Z = L->off1 + L->ladj - 1.5;
+    if (L->off1 <= 0) {
+        Z++;
+        eplus = psi[1] - psi[2];
+        eplus *= (Z + 0.5) * eplus;
+        esq[1] = pf * eplus / Z;
+        z = 2;
+    } else {
+        eplus = psi[0] - psi[1];
+        eplus *= (Z + 0.5) * eplus;
+        if (L->bc_lo[0] == SFGPU_BOUND_SURFACE) esq[0] = pf * eplus / Z;
+        z = 1;
+    }
+    for (; z < M - 1; z++) {
+        Z++;
+        emin = eplus;
+        eplus = psi[z] - psi[z + 1];
+        eplus *= (Z + 0.5) * eplus;
+        esq[z] = pf * (emin + eplus) / Z;
+    }
+    if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) esq[M - 1] = pf * eplus / Z;
+}
+
 /* SF_SegmentList::GetCharge (SF_SegmentList.cpp:759-784): sum phi valence /
    phi_T per layer, times the lattice sites of the layer */
 static void state_charge(const orc_system *s, double *charge) {
@@ -1144,7 +1229,8 @@ static void update_swf(orc_system *s, const double *x) {
         /* psi0 from x, its boundary copies and E^2 (SF_Solve.cpp:797-818) */
         for (int z = 0; z < M; z++) if (s->xp[z] >= 0) s->psi0[z] = x[s->xp[z]];
         olat_set_boundaries(&s->L, s->psi0);
-        olat_esq_flat(&s->L, s->psi0, (ORC_EPS0 * s->bondlength) / kT, s->esq);
+        if (s->L.cyl) olat_esq_curved(&s->L, s->psi0, (ORC_EPS0 * s->bondlength) / kT, s->esq);
+        else olat_esq_flat(&s->L, s->psi0, (ORC_EPS0 * s->bondlength) / kT, s->esq);
     }
     for (int i = 0; i < s->nseg; i++) {
         double *gf = s->swf_full + (size_t)i * M;
@@ -1965,7 +2051,10 @@ static void get_residuals(orc_system *s, double *f) {
         for (int i = 0; i < ns; i++)
             for (int z = 0; z < M; z++) epsav[z] += s->phi[(size_t)i * M + z] * s->eps[i];
         state_charge(s, charge);
-        olat_poisson_flat(&s->L, s->psi0, epsav, charge, (ORC_ELEM_CHARGE / ORC_EPS0) / s->bondlength, s->psi);
+        if (s->L.cyl)
+            olat_poisson_curved(&s->L, s->psi0, epsav, charge, (ORC_ELEM_CHARGE / ORC_EPS0) / s->bondlength, s->psi);
+        else
+            olat_poisson_flat(&s->L, s->psi0, epsav, charge, (ORC_ELEM_CHARGE / ORC_EPS0) / s->bondlength, s->psi);
         free(epsav); free(charge);
     }
     for (int i = 0; i < ns; i++) olat_side(&s->L, s->phi + (size_t)i * M, s->rho + (size_t)i * M);
@@ -2056,7 +2145,8 @@ static double *elec_profile(const orc_system *s) {
     int M = s->L.M;
     double *q = malloc(sizeof(double) * M);
     state_charge(s, q);
-    for (int z = 0; z < M; z++) q[z] /= s->lsites[z];
+    for (int z = 0; z < M; z++)   /* DivideByLatticeSites: curved lattices skip zeros */
+        if (!s->L.cyl || q[z] != 0) q[z] /= s->lsites[z];
     const double kT = ORC_BOLTZMANN * s->temperature;
     for (int z = 0; z < M; z++) q[z] = 0.5 * s->psi[z] * q[z] * ORC_ELEM_CHARGE / kT;
     return q;

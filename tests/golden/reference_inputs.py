@@ -922,6 +922,76 @@ newton : isaac : method : Pure_DIIS
 newton : isaac : tolerance : 1e-12
 start
 """,
+    # charges on the 1D cylinder around its axis (a charged diblock, salt,
+    # the cation as neutralizer) and on a charged sphere with an offset
+    # (liquid states of different epsilon)
+    "1d_cyl_charged": """lat : l : gradients : 1
+lat : l : geometry : cylindrical
+lat : l : n_layers : 22
+lat : l : lambda : 0.16666666666666667
+lat : l : lowerbound : mirror1
+lat : l : upperbound : mirror1
+lat : l : bondlength : 4e-10
+mon : A : freedom : free
+mon : A : valence : -0.3
+mon : B : freedom : free
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - B : 0.3
+mon : A : chi - W : 1.4
+mon : B : chi - W : -0.1
+mol : AB : composition : (A)7(B)6
+mol : AB : freedom : free
+mol : AB : phibulk : 0.02
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : free
+mol : Cl : phibulk : 0.01
+mol : Na : composition : (Na)1
+mol : Na : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    "1d_sphere_charged": """lat : l : gradients : 1
+lat : l : geometry : spherical
+lat : l : n_layers : 18
+lat : l : offset_first_layer : 3
+lat : l : lambda : 0.16666666666666667
+lat : l : lowerbound : surface
+lat : l : upperbound : mirror2
+lat : l : bondlength : 5e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : S : valence : 0.3
+mon : A : freedom : free
+mon : A : valence : -0.5
+mon : A : epsilon : 40
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - S : -1.4
+mon : A : chi - W : 0.6
+mol : A : composition : (A)16
+mol : A : freedom : free
+mol : A : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : free
+mol : Cl : phibulk : 0.02
+mol : Na : composition : (Na)1
+mol : Na : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
     # a comb whose side chains are branched (two fragments at one point)
     "1d_comb_branched_side": INPUTS_COMB_BRANCHED_SIDE,
 }
