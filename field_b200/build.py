@@ -14,9 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsfgpu.so")
 SOURCES = ["sfgpu_system.cu", "sfgpu_solve.cu", "sfgpu_batch.cu", "sfgpu_tangent.cu", "sfgpu_adjoint.cu",
-           "sfgpu_noalloc.cu", "sfgpu_newton.cu"]
+           "sfgpu_noalloc.cu", "sfgpu_newton.cu", "sfgpu_batch_wide.cu"]
 HEADERS = ["sfgpu_internal.cuh", "sfgpu_kernels.cuh", "sfgpu_system.h", "sfgpu_batch.cuh", "sfgpu_tangent.cuh",
-           "sfgpu_adjoint.cuh", "sfgpu_newton.h",
+           "sfgpu_adjoint.cuh", "sfgpu_newton.h", "sfgpu_charge.cuh", "sfgpu_batch_kernel.cuh",
            "../../include/sfgpu.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -7,7 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <vector>
-#include "sfgpu_batch.cuh"
+#include "sfgpu_batch_kernel.cuh"
 #include "sfgpu_system.h"
 
 using namespace sfb;
@@ -22,6 +22,7 @@ struct sfgpu_batch {
     long long total = 0;
     int m = 10, block = 256;
     size_t stage_bytes = 0;         // dynamic shared memory per block (staged G)
+    bool wide = false;              // some instance needs batch_diis_kernel_t<true>
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -42,132 +43,21 @@ static int balloc(sfgpu_batch *b, void **p, size_t bytes) {
     return SFGPU_OK;
 }
 
-// status codes written per instance
-enum { ST_CONVERGED = 0, ST_NOTCONVERGED = SFGPU_ERR_NOTCONVERGED, ST_NONFINITE = SFGPU_ERR_NONFINITE };
-
-__global__ void __launch_bounds__(1024) batch_diis_kernel(const InstDesc *__restrict__ descs, int n,
-                                                          int *queue, int m, double eta, double tol,
-                                                          int maxit, int *status, int *iters, double *errs) {
-    __shared__ InstDesc I;
-    __shared__ BlockShared sh;
-    for (;;) {
-        if (threadIdx.x == 0) sh.inst = atomicAdd(queue, 1);
-        __syncthreads();
-        const int inst = sh.inst;
-        if (inst >= n) return;
-        {   // copy the descriptor into shared memory
-            const int *src = reinterpret_cast<const int *>(descs + inst);
-            int *dst = reinterpret_cast<int *>(&I);
-            for (int i = threadIdx.x; i < (int)(sizeof(InstDesc) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
-        }
-        __syncthreads();
-        const long long iv = I.nvar;
-        double *x = I.x, *x0 = I.x0, *g = I.g, *XR = I.XR, *XX0 = I.XX0;
-        // first step: x = -eta * g(x_initial)  (sfnewton.cpp:578-584)
-        residual_block(I, x, g, sh);
-        double acc = 0;
-        for (long long r = threadIdx.x; r < iv; r += blockDim.x) {
-            double xi = x[r];
-            double v = 0.0 - g[r] * eta;
-            x0[r] = xi;
-            x[r] = v;
-            XR[r] = v;
-            XX0[r] = v - xi;
-            acc += g[r] * g[r];
-        }
-        block_sum1(acc, sh);
-        double err = sqrt(sh.val[0]);
-        int k = 0, it = 0, kd = 1, st = ST_CONVERGED;
-        if (threadIdx.x == 0)
-            for (int i = 0; i < kMaxHist * kMaxHist; i++) sh.gram[i] = 0;
-        __syncthreads();
-        while (tol < err && it < maxit) {
-            it++;
-            for (long long r = threadIdx.x; r < iv; r += blockDim.x) x0[r] = x[r];
-            __syncthreads();
-            residual_block(I, x, g, sh);
-            k = it % m;
-            kd++;
-            if (kd > m) kd = m;
-            double *xr = XR + (size_t)k * iv, *xx = XX0 + (size_t)k * iv;
-            // x -= eta*g; XR[k] = x; XX0[k] = x - x0; Gram row and |g|^2 in one pass
-            double part[kMaxHist + 1];
-            int slot[kMaxHist + 1];
-#pragma unroll
-            for (int i = 0; i <= kMaxHist; i++) {
-                part[i] = 0;
-                slot[i] = (i < kd) ? i : (i == kMaxHist ? kd : -1);
-            }
-            for (long long r = threadIdx.x; r < iv; r += blockDim.x) {
-                const double v = x[r] - g[r] * eta;
-                const double d = v - x0[r];
-                x[r] = v; xr[r] = v; xx[r] = d;
-                part[kMaxHist] += g[r] * g[r];
-#pragma unroll
-                for (int i = 0; i < kMaxHist; i++) {
-                    if (i >= kd) continue;
-                    int posi = k - kd + 1 + i;
-                    if (posi < 0) posi += m;
-                    part[i] += XX0[(size_t)posi * iv + r] * d;
-                }
-            }
-            block_sums_slots<kMaxHist + 1>(part, slot, sh);
-            if (threadIdx.x == 0) {
-                // shift out the oldest row/column when the memory is full
-                // (sfnewton.cpp:624-628), then write the new row
-                if (it >= m) {
-                    for (int i = 1; i < m; i++)
-                        for (int j = 1; j < m; j++) sh.gram[m * (i - 1) + j - 1] = sh.gram[m * i + j];
-                }
-                for (int i = 0; i < kd; i++) sh.gram[i + m * (kd - 1)] = sh.gram[kd - 1 + m * i] = sh.val[i];
-            }
-            __syncthreads();
-            if (threadIdx.x < 32) {
-                for (int e = threadIdx.x; e < kd * kd; e += 32) sh.A[e] = sh.gram[(e % kd) + m * (e / kd)];
-                __syncwarp();
-                diis_coeff_warp(kd, sh.A, sh.Q, sh.coef);
-                if (threadIdx.x == 0) {
-                    double nc = 0;
-                    for (int i = 0; i < kd; i++) nc += sh.coef[i];
-                    for (int i = 0; i < kd; i++) {
-                        sh.coef[i] = sh.coef[i] / nc;
-                        int posi = k - kd + 1 + i;
-                        if (posi < 0) posi += m;
-                        sh.pos[i] = posi;
-                    }
-                }
-            }
-            __syncthreads();
-            for (long long r = threadIdx.x; r < iv; r += blockDim.x) {
-                double v = sh.coef[0] * XR[(size_t)sh.pos[0] * iv + r];
-                for (int i = 1; i < kd; i++) v += sh.coef[i] * XR[(size_t)sh.pos[i] * iv + r];
-                x[r] = v;
-            }
-            err = sqrt(sh.val[kd]);
-            if (!isfinite(err)) { st = ST_NONFINITE; break; }
-            __syncthreads();
-        }
-        if (st == ST_CONVERGED && !(err <= tol)) st = ST_NOTCONVERGED;
-        if (threadIdx.x == 0) {
-            status[inst] = st;
-            iters[inst] = it;
-            errs[inst] = err;
-        }
-        __syncthreads();
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Shared-memory staging of each instance: G of the running segment where
 // the lattice fits next to the kernel's static shared memory, and on 1D
 // symmetric homopolymers also the running slices, phi and the ring of
 // stored slices.  allow = false stages nothing (more blocks per SM).
+static BatchKernel batch_kernel(const sfgpu_batch *b) {
+    return b->wide ? batch_kernel_wide() : batch_diis_kernel_t<false>;
+}
+
 static int configure_stage(sfgpu_batch *b, bool allow) {
     int dev = 0, optin = 0;
     cudaFuncAttributes fa;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
-        cudaFuncGetAttributes(&fa, batch_diis_kernel) != cudaSuccess)
+        cudaFuncGetAttributes(&fa, batch_kernel(b)) != cudaSuccess)
         return SFGPU_ERR_CUDA;
     const size_t fixed = fa.sharedSizeBytes + 1024;   // 1 KB the system reserves per block
     const size_t room = (size_t)optin > fixed ? (size_t)optin - fixed : 0;
@@ -191,7 +81,7 @@ static int configure_stage(sfgpu_batch *b, bool allow) {
         if (sym1d) need = std::max(need, vecs);
     }
     if (cudaMemcpy(b->d_desc, b->desc_h.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaFuncSetAttribute(batch_diis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) !=
+        cudaFuncSetAttribute(batch_kernel(b), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) !=
             cudaSuccess)
         return SFGPU_ERR_CUDA;
     b->stage_bytes = need;
@@ -217,15 +107,14 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
         for (int q = 0; q < descs[i].n_segments && !rc; q++)
             if (descs[i].segments[q].valence != 0) rc = fail_unsupported("batched charged systems");
         if (rc) break;
-        for (int q = 0; q < descs[i].n_molecules && !rc; q++)
-            if (descs[i].molecules[q].n_generations > 0 || descs[i].molecules[q].force != 0 ||
-                descs[i].molecules[q].bond_parent || descs[i].molecules[q].ring)
-                rc = fail_unsupported("batched dendrimers, branched molecules, rings and force ensembles");
-        if (rc) break;
-        if (descs[i].lattice.gradients == 3 && descs[i].lattice.lattice_type != SFGPU_LATTICE_STANDARD) {
-            rc = fail_unsupported("batched FCC, HEX and stencils 3D lattices");
-            break;
+        for (int q = 0; q < descs[i].n_molecules && !rc; q++) {
+            if (descs[i].molecules[q].n_generations > 0 || descs[i].molecules[q].bond_parent ||
+                descs[i].molecules[q].ring)
+                rc = fail_unsupported("batched dendrimers, branched molecules and rings");
+            if (descs[i].molecules[q].force != 0) b->wide = true;
         }
+        if (rc) break;
+        if (descs[i].lattice.gradients == 3 && descs[i].lattice.lattice_type != SFGPU_LATTICE_STANDARD) b->wide = true;
         sfgpu_system *s = new sfgpu_system();
         s->stream = b->stream;
         rc = s->setup(&descs[i]);
@@ -271,6 +160,25 @@ extern "C" int sfgpu_batch_create(int n, const sfgpu_system_desc *descs, int m, 
             im.seg = dseg;
         }
         if (rc) break;
+        {   // force ensembles: step weights per molecule
+            std::vector<sfk::ForceW> fw(2 * s->nmol);
+            I.fmask = 0;
+            for (int q = 0; q < s->nmol; q++)
+                if (s->mols[q].force != 0) {
+                    I.fmask |= 1 << q;
+                    fw[2 * q] = force_weights(s->H.L, s->mols[q].force);
+                    fw[2 * q + 1] = force_weights(s->H.L, -s->mols[q].force);
+                }
+            sfk::ForceW *dfw = nullptr;
+            if (I.fmask) {
+                if ((rc = balloc(b, (void **)&dfw, sizeof(sfk::ForceW) * fw.size()))) break;
+                if (cudaMemcpy(dfw, fw.data(), sizeof(sfk::ForceW) * fw.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+                    rc = SFGPU_ERR_CUDA;
+                    break;
+                }
+            }
+            I.fw = dfw;
+        }
         I.gi = s->d_gi; I.ginv0 = s->d_ginv[0]; I.ginv1 = s->d_ginv[1];
         const size_t iv = s->nvar;
         I.x = b->d_xall + b->offset[i];
@@ -347,14 +255,14 @@ extern "C" int sfgpu_batch_solve_resident(sfgpu_batch *b, double tol, int maxit,
     SFGPU_CUDA_TRY(cudaGetDevice(&dev));
     SFGPU_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     int per_sm = 1;
-    SFGPU_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_diis_kernel, b->block, b->stage_bytes));
+    SFGPU_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel(b), b->block, b->stage_bytes));
     int grid = std::max(1, std::min(n, nsm * std::max(1, per_sm)));
     if (!b->ev0) {
         SFGPU_CUDA_TRY(cudaEventCreate(&b->ev0));
         SFGPU_CUDA_TRY(cudaEventCreate(&b->ev1));
     }
     SFGPU_CUDA_TRY(cudaEventRecord(b->ev0, st));
-    batch_diis_kernel<<<grid, b->block, b->stage_bytes, st>>>(b->d_desc, n, b->d_queue, b->m, eta, tol, maxit,
+    batch_kernel(b)<<<grid, b->block, b->stage_bytes, st>>>(b->d_desc, n, b->d_queue, b->m, eta, tol, maxit,
                                                   b->d_status, b->d_iters, b->d_err);
     SFGPU_CUDA_TRY(cudaGetLastError());
     SFGPU_CUDA_TRY(cudaEventRecord(b->ev1, st));

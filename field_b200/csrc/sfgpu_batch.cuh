@@ -44,6 +44,10 @@ struct InstDesc {
     double *gi, *ginv0, *ginv1;
     // iteration work
     double *x, *x0, *g, *XR, *XX0;
+    // mol : force (wide kernel): bit m of fmask marks molecule m, whose
+    // forward and backward step weights are fw[2m], fw[2m + 1]
+    int fmask;
+    const sfk::ForceW *fw;
 };
 
 struct BlockShared {
@@ -89,7 +93,7 @@ __device__ __forceinline__ void block_sum1(double v, BlockShared &sh) {
     block_sums_slots<1>(a, sl, sh);
 }
 
-__device__ inline void mol_scalars_block(const InstDesc &I, int m, double wsum, BlockShared &sh) {
+__device__ __forceinline__ void mol_scalars_block(const InstDesc &I, int m, double wsum, BlockShared &sh) {
     const IMol &o = I.mol[m];
     sfk::MolScal s;
     s.lngn = log(wsum);
@@ -119,7 +123,7 @@ __device__ inline void mol_scalars_block(const InstDesc &I, int m, double wsum, 
 
 // lnGN sum, scalars and normalised phi of molecule m; cur = end-point
 // distribution (Gi_inv after the backward pass)
-__device__ inline void finish_molecule(const InstDesc &I, int m, const double *cur, BlockShared &sh) {
+__device__ __forceinline__ void finish_molecule(const InstDesc &I, int m, const double *cur, BlockShared &sh) {
     const IMol &o = I.mol[m];
     double acc = 0;
     for (int r = threadIdx.x; r < I.M; r += blockDim.x) {
@@ -164,6 +168,16 @@ __device__ inline void finish_molecule(const InstDesc &I, int m, const double *c
 // lattice fits (I.gstage) it is copied once per run into the block's dynamic
 // shared memory and the steps read it there instead of streaming it from L2
 // in every step.
+// One step of a linear chain in the wide kernel: the constant-force step
+// where the molecule has a force (forward +f, backward -f weights), else the
+// first-order step of any lattice type.
+__device__ __forceinline__ double chain_step_wide(const DLat &L, const InstDesc &I, int m, const RowInfo &R,
+                                                  const double *src, const double *G, int k, int nlast, bool fwd) {
+    if ((I.fmask >> m) & 1) return force_row(L, R, src, G, k, nlast, I.fw[2 * m + (fwd ? 0 : 1)]);
+    return prop1_row<true>(L, R, src, G, k, nlast);
+}
+
+template <bool kWide>
 __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared &sh) {
     extern __shared__ double g_stage[];
     const IMol &o = I.mol[m];
@@ -278,7 +292,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
             const double *src = gi + (size_t)(t - 1) * M;
             double *dst = gi + (size_t)t * M;
             for_interior4(L, threadIdx.x, blockDim.x,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, src, G, k, nlast); },
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<kWide>(L, R, src, G, k, nlast); },
                 [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
             __syncthreads();
         }
@@ -286,7 +300,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         if (N % 2 == 1) {
             double *dst = bufA;
             for_interior4(L, threadIdx.x, blockDim.x,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<kWide>(L, R, cur, G, k, nlast); },
                 [&](const RowInfo &R, int k, double out) {
                     const int z = R.base + k;
                     dst[z] = out;
@@ -299,7 +313,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
             const double *other = gi + (size_t)(N - sp) * M;
             double *dst = bufA;
             for_interior4_acc(L, threadIdx.x, blockDim.x, phi, other,
-                [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
+                [&](const RowInfo &R, int k, int nlast) { return prop1_row<kWide>(L, R, cur, G, k, nlast); },
                 [&](const RowInfo &R, int k, double out, double ph, double ot) {
                     const int z = R.base + k;
                     dst[z] = out;
@@ -322,7 +336,10 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         double *dst = gi + (size_t)t * M;
         const double *G = gof(o.seg[t]);
         for_interior4(L, threadIdx.x, blockDim.x,
-            [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, src, G, k, nlast); },
+            [&](const RowInfo &R, int k, int nlast) {
+                if constexpr (kWide) return chain_step_wide(L, I, m, R, src, G, k, nlast, true);
+                else return prop1_row<false>(L, R, src, G, k, nlast);
+            },
             [&](const RowInfo &R, int k, double v) { dst[R.base + k] = v; });
         __syncthreads();
     }
@@ -347,7 +364,10 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
         double *phi = o.phi[sg];
         double *dst = bufA;
         for_interior4_acc(L, threadIdx.x, blockDim.x, phi, gf,
-            [&](const RowInfo &R, int k, int nlast) { return prop1_row<false>(L, R, cur, G, k, nlast); },
+            [&](const RowInfo &R, int k, int nlast) {
+                if constexpr (kWide) return chain_step_wide(L, I, m, R, cur, G, k, nlast, false);
+                else return prop1_row<false>(L, R, cur, G, k, nlast);
+            },
             [&](const RowInfo &R, int k, double out, double ph, double ot) {
                 const int z = R.base + k;
                 dst[z] = out;
@@ -365,6 +385,7 @@ __device__ inline void molecule_phi_block(const InstDesc &I, int m, BlockShared 
 // contact averages and potentials stay in registers; the sums run in the
 // same order as the single-system kernel.
 constexpr int kResMax = 8;
+template <bool kWide>
 __device__ __forceinline__ void site_residual(const InstDesc &I, const BlockShared &sh, int j, double *f) {
     const DLat &L = I.L;
     const int z = I.sites[j];
@@ -381,7 +402,7 @@ __device__ __forceinline__ void site_residual(const InstDesc &I, const BlockShar
         if (i >= nseg) continue;
         bool need = false;
         for (int c = 0; c < ncl; c++) need |= I.ct.chi[I.rep[c] * SFGPU_MAX_SEG + i] != 0;
-        if (need) rho[i] = side_fraction<false>(L, I.phi[i], z);
+        if (need) rho[i] = side_fraction<kWide>(L, I.phi[i], z);
     }
     double u[kResMax];
     double av = 0;
@@ -410,6 +431,7 @@ __device__ __forceinline__ void site_residual(const InstDesc &I, const BlockShar
 }
 
 // x -> f for one instance (SF_Solve::residuals, SF_Solve.cpp:647-651)
+template <bool kWide>
 __device__ inline void residual_block(const InstDesc &I, const double *x, double *f, BlockShared &sh) {
     const DLat &L = I.L;
     const int M = I.M;
@@ -430,10 +452,10 @@ __device__ inline void residual_block(const InstDesc &I, const double *x, double
     __syncthreads();
     for (int m = 0; m < I.nmol; m++) {
         if (m == I.solvent) continue;
-        molecule_phi_block(I, m, sh);
+        molecule_phi_block<kWide>(I, m, sh);
         __syncthreads();
     }
-    molecule_phi_block(I, I.solvent, sh);
+    molecule_phi_block<kWide>(I, I.solvent, sh);
     __syncthreads();
     for (int i = 0; i < I.nseg; i++) {
         if (I.freedom[i] == SFGPU_SEG_FROZEN) continue;
@@ -464,7 +486,7 @@ __device__ inline void residual_block(const InstDesc &I, const double *x, double
         }
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < I.nsites; j += blockDim.x) site_residual(I, sh, j, f);
+    for (int j = threadIdx.x; j < I.nsites; j += blockDim.x) site_residual<kWide>(I, sh, j, f);
     __syncthreads();
 }
 
@@ -474,7 +496,7 @@ __device__ inline void residual_block(const InstDesc &I, const double *x, double
 // in shared memory: lane k owns row / column k of each rotation, lane 0 takes
 // the convergence sums in the serial order, so the result is bit-identical
 // to the serial form (n <= kMaxHist <= 32).
-__device__ inline void diis_coeff_warp(int n, double *A, double *Q, double *c) {
+__device__ __forceinline__ void diis_coeff_warp(int n, double *A, double *Q, double *c) {
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
     for (int i = lane; i < n * n; i += 32) Q[i] = (i / n == i % n);

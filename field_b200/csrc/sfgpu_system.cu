@@ -788,7 +788,7 @@ int sfgpu_system::molecule_phi_log(int m) {
 }
 
 // weights of a constant-force step with force f (see force_row)
-static ForceW force_weights(const DLat &L, double f) {
+ForceW force_weights(const DLat &L, double f) {
     ForceW w;
     const double l1 = L.l1;
     if (L.grad == 1 && !L.cyl) {

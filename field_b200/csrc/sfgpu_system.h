@@ -11,6 +11,8 @@ struct HostLat {
     std::vector<double> stiff; // 'lat : stiff_range' mask (3D second order), empty if none
 };
 int sfgpu_build_lattice(const sfgpu_lattice_desc *d, HostLat *H);
+// weights of a constant-force step with force f (see sfk::force_row)
+sfk::ForceW force_weights(const DLat &L, double f);
 
 struct HMol {
     int N = 0, type = 0, sym = 0, freedom = 0, pinned = 0;

@@ -174,13 +174,13 @@ def sweep_calculations(calc: Dict[Key, str]) -> Tuple[Optional[Variation], List[
 
 def batchable(spec) -> bool:
     """Whether the batched persistent kernel takes this system: first order,
-    the standard lattice type in 3D, no overflow protection, and linear
-    chains without a force (dendrimers and the force ensemble run on the
-    single-system path)."""
-    from .desc import LATTICE_STANDARD
-    return (spec.lattice.order == 1 and spec.lattice.lattice_type == LATTICE_STANDARD
-            and not getattr(spec, "overflow_protection", False)
-            and all(not m.generations and m.force == 0 for m in spec.molecules))
+    no overflow protection, no charges, and linear chains (the FCC, HEX and
+    stencils lattice types and the force ensemble run in the kernel's wide
+    instantiation; dendrimers, branched molecules, rings and charged systems
+    on the single-system path)."""
+    return (spec.lattice.order == 1 and not getattr(spec, "overflow_protection", False)
+            and not getattr(spec, "charged", False)
+            and all(not m.generations and m.bond_parent is None and not m.ring for m in spec.molecules))
 
 
 @dataclass

@@ -125,3 +125,36 @@ def test_batch_reports_nonconvergence(gpu_lib):
     res = bs.solve(x0, tol=1e-12, maxit=3)
     assert (res.status == 5).all() and (res.iterations == 3).all()
 
+
+
+def test_wide_batch_meets_sfbox(gpu_lib):
+    """The wide instantiation of the batched kernel (FCC, HEX and stencils
+    lattice types, the force ensemble) next to standard instances in one
+    launch: every instance's Pure_DIIS from SFbox's start reaches SFbox's own
+    solution (tests/golden/reference_cases.npz) -- interior phi to 1e-10,
+    the same tolerance as the single-system path."""
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    from reference_inputs import INPUTS
+    from field_b200.sfinput import build_system, parse_input
+    data = np.load(os.path.join(here, "golden", "reference_cases.npz"))
+    cases = ["3d_fcc_colloid", "3d_hex_colloid", "3d_stencils_colloid", "1d_force", "1d_flat_c1", "2d_cylinder"]
+    specs, x0s = [], []
+    for c in cases:
+        spec, st = build_system(parse_input(INPUTS[c])[0])
+        assert (st.m, st.deltamax) == (5, 0.1), c
+        specs.append(spec)
+        x0s.append(data[f"{c}/solve_x0"])
+    bs = BatchSolver(specs, m=5, eta=0.1)
+    res = bs.solve(np.concatenate(x0s), tol=1e-12, maxit=20000)
+    assert res.converged.all(), res.status
+    for i, (c, spec) in enumerate(zip(cases, specs)):
+        inner = spec.lattice.interior_mask()
+        want = data[f"{c}/solve_phi"]
+        for seg in range(len(spec.segments)):
+            w = want[seg][inner]
+            if np.max(np.abs(w)) == 0:
+                continue
+            got = bs.phi(i, seg)[inner]
+            assert np.max(np.abs(got - w)) <= 1e-10 * np.max(np.abs(w)), (c, seg)

@@ -77,9 +77,10 @@ def test_batchable_routes_special_systems_to_the_single_system_path():
     sys.path.insert(0, os.path.dirname(__file__))
     from cases import CASES
     from field_b200.sweep import batchable
-    assert batchable(CASES["1d_surface"]())
-    for k in ("1d_dendrimer", "1d_force", "3d_fcc_colloid", "3d_2nd_brush"):
-        assert not batchable(CASES[k]())
+    for k in ("1d_surface", "1d_force", "3d_fcc_colloid", "3d_hex_colloid", "3d_stencils_melt"):
+        assert batchable(CASES[k]()), k   # the wide kernel takes the lattice types and the force
+    for k in ("1d_dendrimer", "3d_2nd_brush", "2d_2nd_lumped"):
+        assert not batchable(CASES[k]()), k
     spec = CASES["1d_surface"]()
     spec.overflow_protection = True
     assert not batchable(spec)
