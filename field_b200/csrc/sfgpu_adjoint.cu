@@ -180,7 +180,7 @@ int sfgpu_system::ensure_adjoint() {
     if (charged) return fail_unsupported("derivatives of charged systems");
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
-        if (o.dend || o.force != 0) return fail_unsupported("derivatives of dendrimers and of the force ensemble");
+        if (o.dend) return fail_unsupported("derivatives of dendrimers");
         else if (o.tree || o.ring) return fail_unsupported("derivatives of branched molecules and rings");
     int rc = ensure_adjoint_misc();
     if (rc) return rc;
@@ -246,7 +246,10 @@ void sfgpu_system::adj_start(const double *G, double *dst) {
 void sfgpu_system::adj_fstep(const HMol &o, int t, const double *src, double *dst) {
     const DLat &L = H.L;
     const int sg = o.seg[t];
-    if (K == 1)
+    if (K == 1 && o.force != 0)   // SF_Copol1stO.cpp:1207-1211
+        step1_force_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, force_weights(L, o.force), src, d_gseg[sg], dst,
+                                                                nullptr, nullptr, COMP_NONE);
+    else if (K == 1)
         step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, nullptr, nullptr, COMP_NONE);
     else
         step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], dst,
@@ -257,7 +260,10 @@ void sfgpu_system::adj_bstep(const HMol &o, int t, const double *src, double *ds
     const DLat &L = H.L;
     const int sg = o.seg[t];
     const int mode = other ? COMP_ACC : COMP_NONE;
-    if (K == 1)
+    if (K == 1 && o.force != 0)   // SF_Copol1stO.cpp:1226-1230
+        step1_force_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, force_weights(L, -o.force), src, d_gseg[sg], dst,
+                                                                other, phi, mode);
+    else if (K == 1)
         step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, other, phi, mode);
     else
         step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], dst,
@@ -433,7 +439,10 @@ int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
     // one reverse step: gbar(seg t) += cot . A p; nxt += A^T (G_t cot)
     auto rstep = [&](int t, const double *p, double S, int backward) {
         const int sg = o.seg[t];
-        if (K == 1)
+        if (K == 1 && o.force != 0)   // the forward recursion's +force, the backward one's -force
+            adj_chain_step_force<<<gr, kBlock, 0, s>>>(L, force_weights(L, backward ? -o.force : o.force), cot,
+                                                       d_gseg[sg], p, a_gbar[sg], nxt);
+        else if (K == 1)
             adj_chain_step<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[sg], p, a_gbar[sg], nxt);
         else
             adj_step2<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[sg], p, S, backward, a_gbar[sg], nxt);

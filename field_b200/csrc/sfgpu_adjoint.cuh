@@ -91,6 +91,59 @@ __device__ __forceinline__ void scatter1(const DLat &L, const RowInfo &R, int k,
     atomicAdd(out + kp, c);
 }
 
+// transpose of the bare constant-force stencil (force_row_g with g = 1):
+// y spread to the sites the step read with their weights
+__device__ __forceinline__ void scatter_force(const DLat &L, const RowInfo &R, int k, int nlast, double y,
+                                              const ForceW &w, double *__restrict__ out) {
+    const int d = L.grad - 1;
+    const int t = R.base + k;
+    const int km = R.base + ((k == 1) ? L.map_lo[d] : k - 1);
+    const int kp = R.base + ((k == nlast) ? L.map_hi[d] : k + 1);
+    if (L.grad == 1 && !L.cyl) {   // b + a1 (a - b) + a2 (c - b)
+        atomicAdd(out + t, (1.0 - w.a1 - w.a2) * y);
+        atomicAdd(out + km, w.a1 * y);
+        atomicAdd(out + kp, w.a2 * y);
+        return;
+    }
+    if (L.grad == 1) {             // f-1 a + f0 b + f1 c
+        atomicAdd(out + km, L.lam_m[t] * w.a2 * y);
+        atomicAdd(out + t, (1 - L.lam_p[t] - L.lam_m[t]) / w.a3 * y);
+        atomicAdd(out + kp, L.lam_p[t] * w.a1 * y);
+        return;
+    }
+    if (L.grad == 2) {             // (b + lm (u - b) + lp (d - b) + l1 (a a1 + c a2 - 2 b)) / a3
+        const double lm = L.lam_m[R.x], lp = L.lam_p[R.x], yy = y / w.a3;
+        atomicAdd(out + t, (1.0 - lm - lp - 2.0 * L.l1) * yy);
+        atomicAdd(out + t + R.up, lm * yy);
+        atomicAdd(out + t + R.dn, lp * yy);
+        atomicAdd(out + km, L.l1 * w.a1 * yy);
+        atomicAdd(out + kp, L.l1 * w.a2 * yy);
+        return;
+    }
+    const double c = y * w.a3;     // (x-, x+, y-, y+, z- a1, z+ a2) a3
+    atomicAdd(out + t + R.up, c);
+    atomicAdd(out + t + R.dn, c);
+    atomicAdd(out + t + R.up2, c);
+    atomicAdd(out + t + R.dn2, c);
+    atomicAdd(out + km, c * w.a1);
+    atomicAdd(out + kp, c * w.a2);
+}
+
+// one reverse constant-force step: Gbar[t] += cot[t] * A_f p and
+// out += A_f^T (G * cot)
+static __global__ void adj_chain_step_force(DLat L, ForceW w, const double *__restrict__ cot,
+                                            const double *__restrict__ G, const double *__restrict__ p,
+                                            double *__restrict__ gbar, double *__restrict__ out) {
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const int t = R.base + k;
+        const double c = cot[t];
+        if (c == 0.0) return;
+        gbar[t] += c * force_row_g(L, R, p, 1.0, k, nlast, w);
+        scatter_force(L, R, k, nlast, G[t] * c, w, out);
+    });
+}
+
 // one reverse chain step: Gbar[t] += cot[t] * A p (p = the neighbouring
 // propagator slice), and out += A^T (G * cot)
 static __global__ void adj_chain_step(DLat L, const double *__restrict__ cot, const double *__restrict__ G,

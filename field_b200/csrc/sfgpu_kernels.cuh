@@ -759,13 +759,14 @@ static __global__ void finalize_phi(int M, const double *__restrict__ G, double 
 //  3D        (Lat3D1stO.cpp:94-130): (x-, x+, y-, y+ times g, z- g a1, z+ g a2) a3,
 //            a1 = e^f, a2 = e^-f, a3 = 1 / (4 + e^f + e^-f)
 struct ForceW { double a1, a2, a3; };
-__device__ __forceinline__ double force_row(const DLat &L, const RowInfo &R, const double *__restrict__ gin,
-                                            const double *__restrict__ G, int k, int nlast, const ForceW &w) {
+// the step with the weight g of the target site given (force_row: g = G[t];
+// the derivative kernels take g = 1 for the bare stencil)
+__device__ __forceinline__ double force_row_g(const DLat &L, const RowInfo &R, const double *__restrict__ gin,
+                                              double g, int k, int nlast, const ForceW &w) {
     const int d = L.grad - 1;
     const int t = R.base + k;
     const int km = (k == 1) ? L.map_lo[d] : k - 1;
     const int kp = (k == nlast) ? L.map_hi[d] : k + 1;
-    const double g = G[t];
     const double a = gin[R.base + km], b = gin[t], c = gin[R.base + kp];
     if (L.grad == 1 && !L.cyl) return g * (b + w.a1 * (a - b) + w.a2 * (c - b));
     if (L.grad == 1) {
@@ -783,6 +784,10 @@ __device__ __forceinline__ double force_row(const DLat &L, const RowInfo &R, con
     acc += a * g * w.a1;
     acc += c * g * w.a2;
     return acc * w.a3;
+}
+__device__ __forceinline__ double force_row(const DLat &L, const RowInfo &R, const double *__restrict__ gin,
+                                            const double *__restrict__ G, int k, int nlast, const ForceW &w) {
+    return force_row_g(L, R, gin, G[R.base + k], k, nlast, w);
 }
 
 static __global__ void step1_force_rows(DLat L, ForceW w, const double *__restrict__ gin, const double *__restrict__ G,

@@ -29,7 +29,7 @@ int sfgpu_system::ensure_tangent() {
     if (charged) return fail_unsupported("derivatives of charged systems");
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
-        if (o.dend || o.force != 0) return fail_unsupported("derivatives of dendrimers and of the force ensemble");
+        if (o.dend) return fail_unsupported("derivatives of dendrimers");
         else if (o.tree || o.ring) return fail_unsupported("derivatives of branched molecules and rings");
     if (t_ready) return SFGPU_OK;
     int rc;
@@ -125,7 +125,10 @@ int sfgpu_system::molecule_phi_t(int m) {
             int sg = o.seg[t];
             const double *src = d_gi + (size_t)(t - 1) * KM, *dsrc = d_dgi + (size_t)(t - 1) * KM;
             double *dst = d_gi + (size_t)t * KM, *ddst = d_dgi + (size_t)t * KM;
-            if (K == 1)
+            if (K == 1 && o.force != 0)   // forward steps with +force
+                step1_force_rows_t<<<gr, kBlock, 0, s>>>(L, force_weights(L, o.force), src, dsrc, d_gseg[sg], dgseg[sg],
+                                                         dst, ddst, nullptr, nullptr, nullptr, nullptr, COMP_NONE);
+            else if (K == 1)
                 step1_rows_t<<<gr, kBlock, 0, s>>>(L, src, dsrc, d_gseg[sg], dgseg[sg], dst, ddst, nullptr, nullptr,
                                                    nullptr, nullptr, COMP_NONE);
             else
@@ -140,7 +143,11 @@ int sfgpu_system::molecule_phi_t(int m) {
         std::swap(ginv, tmp); std::swap(dginv, dtmp);
         for (int t = N - 2; t >= 0; t--) {
             int sg = o.seg[t];
-            if (K == 1)
+            if (K == 1 && o.force != 0)   // backward steps with -force
+                step1_force_rows_t<<<gr, kBlock, 0, s>>>(L, force_weights(L, -o.force), cur, dcur, d_gseg[sg],
+                                                         dgseg[sg], ginv, dginv, d_gi + (size_t)t * KM,
+                                                         d_dgi + (size_t)t * KM, o.d_phi[sg], o.d_dphi[sg], COMP_ACC);
+            else if (K == 1)
                 step1_rows_t<<<gr, kBlock, 0, s>>>(L, cur, dcur, d_gseg[sg], dgseg[sg], ginv, dginv,
                                                    d_gi + (size_t)t * KM, d_dgi + (size_t)t * KM, o.d_phi[sg],
                                                    o.d_dphi[sg], COMP_ACC);

@@ -92,6 +92,30 @@ static __global__ void step1_rows_t(DLat L, const double *__restrict__ gin, cons
     });
 }
 
+// primal constant-force step (as step1_force_rows) plus its tangent: the
+// step is linear in gin with the weights of force_row, so d(out) =
+// dG * stencil(gin) + G * stencil(dgin) with the bare (g = 1) stencil
+static __global__ void step1_force_rows_t(DLat L, ForceW w, const double *__restrict__ gin,
+                                          const double *__restrict__ dgin, const double *__restrict__ G,
+                                          const double *__restrict__ dG, double *__restrict__ gout,
+                                          double *__restrict__ dgout, const double *__restrict__ other,
+                                          const double *__restrict__ dother, double *__restrict__ phi,
+                                          double *__restrict__ dphi, int mode) {
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const int t = R.base + k;
+        const double out = force_row(L, R, gin, G, k, nlast, w);
+        const double dout = dG[t] * force_row_g(L, R, gin, 1.0, k, nlast, w) +
+                            G[t] * force_row_g(L, R, dgin, 1.0, k, nlast, w);
+        gout[t] = out;
+        dgout[t] = dout;
+        if (mode == COMP_ACC) {
+            phi[t] += out * other[t];
+            dphi[t] += dout * other[t] + out * dother[t];
+        }
+    });
+}
+
 // primal second-order step (as step2_rows) plus its tangent
 static __global__ void step2_rows_t(DLat L, const double *__restrict__ gin, const double *__restrict__ dgin,
                                     const double *__restrict__ G, const double *__restrict__ dG, double S,

@@ -311,8 +311,8 @@ CASES = {
 }
 
 # cases whose derivatives (forward and reverse mode) are implemented: not the
-# lumped second-order lattices, dendrimers, stiff ranges or the force ensemble
-NOT_DIFFERENTIABLE = ("lumped", "dendrimer", "stiff", "force")
+# lumped second-order lattices, dendrimers or stiff ranges
+NOT_DIFFERENTIABLE = ("lumped", "dendrimer", "stiff")
 DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFERENTIABLE))
 
 
