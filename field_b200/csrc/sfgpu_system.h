@@ -76,6 +76,10 @@ struct sfgpu_system {
     bool t_ready = false;
     std::vector<double *> dgfull, dgseg, dphi;
     double *d_dgi = nullptr, *d_dginv[2] = {nullptr, nullptr};
+    // the tangent's chain storage (every position): the primal's d_gi, or a
+    // buffer of its own when the primal keeps checkpoints only; two work
+    // slices for the steps whose tangent is formed from two primal steps
+    double *t_gi = nullptr, *t_w[2] = {nullptr, nullptr};
     double *d_tscal = nullptr, *d_dpartial = nullptr, *d_dphib = nullptr, *d_dchib = nullptr;
     double *d_v = nullptr, *d_jv = nullptr;
     int ensure_tangent();

@@ -24,10 +24,8 @@ static int grid_rows_t(const DLat &L) {
 }
 
 int sfgpu_system::ensure_tangent() {
-    if (K == 3 || K == 5) return fail_unsupported("derivatives of the lumped 1D/2D second-order lattices");
     if (logmode) return fail_unsupported("derivatives with overflow protection");
     if (charged) return fail_unsupported("derivatives of charged systems");
-    if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
         if (o.dend) return fail_unsupported("derivatives of dendrimers");
         else if (o.tree || o.ring) return fail_unsupported("derivatives of branched molecules and rings");
@@ -51,6 +49,17 @@ int sfgpu_system::ensure_tangent() {
         store = std::max(store, need);
     }
     if ((rc = alloc_d(&d_dgi, store))) return rc;
+    // checkpointed primal storage holds fewer slices than the tangent sweeps write
+    bool ck = false;
+    for (auto &o : mols) ck |= primal_checkpointed(o);
+    t_gi = d_gi;
+    if (ck) {
+        if ((rc = alloc_d(&t_gi, store))) return rc;
+        SFGPU_CUDA_TRY(cudaMemset(t_gi, 0, sizeof(double) * std::max<size_t>(store, 1)));
+    }
+    if ((rc = alloc_d(&t_w[0], (size_t)K * M)) || (rc = alloc_d(&t_w[1], (size_t)K * M))) return rc;
+    SFGPU_CUDA_TRY(cudaMemset(t_w[0], 0, sizeof(double) * K * M));
+    SFGPU_CUDA_TRY(cudaMemset(t_w[1], 0, sizeof(double) * K * M));
     if ((rc = alloc_d(&d_dginv[0], (size_t)K * M)) || (rc = alloc_d(&d_dginv[1], (size_t)K * M))) return rc;
     SFGPU_CUDA_TRY(cudaMemset(d_dgi, 0, sizeof(double) * std::max<size_t>(store, 1)));
     SFGPU_CUDA_TRY(cudaMemset(d_dginv[0], 0, sizeof(double) * K * M));
@@ -97,13 +106,13 @@ int sfgpu_system::molecule_phi_t(int m) {
         const double *G = d_gseg[i], *dG = dgseg[i];
         const int N = o.N, half = N / 2;
         double *phi = o.d_phi[i], *dph = o.d_dphi[i];
-        SFGPU_CUDA_TRY(cudaMemcpyAsync(d_gi, G, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
+        SFGPU_CUDA_TRY(cudaMemcpyAsync(t_gi, G, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
         SFGPU_CUDA_TRY(cudaMemcpyAsync(d_dgi, dG, sizeof(double) * M, cudaMemcpyDeviceToDevice, s));
         for (int t = 1; t < half; t++)
-            step1_rows_t<<<gr, kBlock, 0, s>>>(L, d_gi + (size_t)(t - 1) * M, d_dgi + (size_t)(t - 1) * M, G, dG,
-                                               d_gi + (size_t)t * M, d_dgi + (size_t)t * M, nullptr, nullptr,
+            step1_rows_t<<<gr, kBlock, 0, s>>>(L, t_gi + (size_t)(t - 1) * M, d_dgi + (size_t)(t - 1) * M, G, dG,
+                                               t_gi + (size_t)t * M, d_dgi + (size_t)t * M, nullptr, nullptr,
                                                nullptr, nullptr, COMP_NONE);
-        cur = d_gi + (size_t)(half - 1) * M;
+        cur = t_gi + (size_t)(half - 1) * M;
         dcur = d_dgi + (size_t)(half - 1) * M;
         if (N % 2 == 1) {
             step1_rows_t<<<gr, kBlock, 0, s>>>(L, cur, dcur, G, dG, ginv, dginv, nullptr, nullptr, phi, dph, COMP_CENTRE);
@@ -112,20 +121,47 @@ int sfgpu_system::molecule_phi_t(int m) {
         }
         for (int sp = (N + 3) / 2; sp <= N; sp++) {
             int sinv = N - sp + 1;
-            step1_rows_t<<<gr, kBlock, 0, s>>>(L, cur, dcur, G, dG, ginv, dginv, d_gi + (size_t)(sinv - 1) * M,
+            step1_rows_t<<<gr, kBlock, 0, s>>>(L, cur, dcur, G, dG, ginv, dginv, t_gi + (size_t)(sinv - 1) * M,
                                                d_dgi + (size_t)(sinv - 1) * M, phi, dph, COMP_ACC);
             cur = ginv; dcur = dginv;
             std::swap(ginv, tmp); std::swap(dginv, dtmp);
         }
     } else {
         const int N = o.N;
-        replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[0]], d_gi);
+        // lumped second-order lattices and stiff ranges: a step is bilinear
+        // in (propagator, G), so its tangent is step(d in, G) + step(in, dG),
+        // two more launches of the primal step with the primal's parameters
+        // (molecule_phi: SF_Copol2ndO_stiff_range.cpp:211-234 for the stiff
+        // range's Pf(s-1, s+1) and isotropic end steps)
+        const bool pair = (K == 3 || K == 5) || (K == 6 && L.stiff);
+        auto prim = [&](int t, bool backward, const double *in, const double *G, double *out) {
+            const int sg = o.seg[t];
+            if (K == 6) {
+                const bool iso = backward ? (t == N - 2) : (t == N - 1);
+                const double Sv = iso ? 0.2 : (backward ? pf[sg * nseg + o.seg[t + 2]] : pf[o.seg[t - 1] * nseg + o.seg[t + 1]]);
+                step2_rows<<<gr, kBlock, 0, s>>>(L, in, G, Sv, out, nullptr, nullptr, COMP_NONE, backward ? 1 : 0,
+                                                 iso ? STEP2_ISO : STEP2_STIFF);
+            } else {
+                const double Sv = backward ? pf[sg * nseg + o.seg[t + 1]] : pf[o.seg[t - 1] * nseg + sg];
+                step2l_rows<<<gr, kBlock, 0, s>>>(L, in, G, Sv, out, nullptr, nullptr, COMP_NONE, backward ? 1 : 0);
+            }
+        };
+        auto pair_step = [&](int t, bool backward, const double *in, const double *din, double *out, double *dout) {
+            const int sg = o.seg[t];
+            prim(t, backward, in, d_gseg[sg], out);
+            prim(t, backward, din, d_gseg[sg], t_w[0]);
+            prim(t, backward, in, dgseg[sg], t_w[1]);
+            sum2<<<g, kBlock, 0, s>>>(KM, t_w[0], t_w[1], dout);
+        };
+        replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[0]], t_gi);
         replicate<<<g, kBlock, 0, s>>>(M, K, dgseg[o.seg[0]], d_dgi);
         for (int t = 1; t < N; t++) {
             int sg = o.seg[t];
-            const double *src = d_gi + (size_t)(t - 1) * KM, *dsrc = d_dgi + (size_t)(t - 1) * KM;
-            double *dst = d_gi + (size_t)t * KM, *ddst = d_dgi + (size_t)t * KM;
-            if (K == 1 && o.force != 0)   // forward steps with +force
+            const double *src = t_gi + (size_t)(t - 1) * KM, *dsrc = d_dgi + (size_t)(t - 1) * KM;
+            double *dst = t_gi + (size_t)t * KM, *ddst = d_dgi + (size_t)t * KM;
+            if (pair)
+                pair_step(t, false, src, dsrc, dst, ddst);
+            else if (K == 1 && o.force != 0)   // forward steps with +force
                 step1_force_rows_t<<<gr, kBlock, 0, s>>>(L, force_weights(L, o.force), src, dsrc, d_gseg[sg], dgseg[sg],
                                                          dst, ddst, nullptr, nullptr, nullptr, nullptr, COMP_NONE);
             else if (K == 1)
@@ -137,23 +173,27 @@ int sfgpu_system::molecule_phi_t(int m) {
         }
         replicate<<<g, kBlock, 0, s>>>(M, K, d_gseg[o.seg[N - 1]], ginv);
         replicate<<<g, kBlock, 0, s>>>(M, K, dgseg[o.seg[N - 1]], dginv);
-        connect_t<<<g, kBlock, 0, s>>>(M, K, ginv, dginv, d_gi + (size_t)(N - 1) * KM, d_dgi + (size_t)(N - 1) * KM,
+        connect_t<<<g, kBlock, 0, s>>>(M, K, ginv, dginv, t_gi + (size_t)(N - 1) * KM, d_dgi + (size_t)(N - 1) * KM,
                                        o.d_phi[o.seg[N - 1]], o.d_dphi[o.seg[N - 1]]);
         cur = ginv; dcur = dginv;
         std::swap(ginv, tmp); std::swap(dginv, dtmp);
         for (int t = N - 2; t >= 0; t--) {
             int sg = o.seg[t];
-            if (K == 1 && o.force != 0)   // backward steps with -force
+            if (pair) {
+                pair_step(t, true, cur, dcur, ginv, dginv);
+                compose2_t<<<g, kBlock, 0, s>>>(L, K, ginv, dginv, t_gi + (size_t)t * KM, d_dgi + (size_t)t * KM,
+                                                o.d_phi[sg], o.d_dphi[sg]);
+            } else if (K == 1 && o.force != 0)   // backward steps with -force
                 step1_force_rows_t<<<gr, kBlock, 0, s>>>(L, force_weights(L, -o.force), cur, dcur, d_gseg[sg],
-                                                         dgseg[sg], ginv, dginv, d_gi + (size_t)t * KM,
+                                                         dgseg[sg], ginv, dginv, t_gi + (size_t)t * KM,
                                                          d_dgi + (size_t)t * KM, o.d_phi[sg], o.d_dphi[sg], COMP_ACC);
             else if (K == 1)
                 step1_rows_t<<<gr, kBlock, 0, s>>>(L, cur, dcur, d_gseg[sg], dgseg[sg], ginv, dginv,
-                                                   d_gi + (size_t)t * KM, d_dgi + (size_t)t * KM, o.d_phi[sg],
+                                                   t_gi + (size_t)t * KM, d_dgi + (size_t)t * KM, o.d_phi[sg],
                                                    o.d_dphi[sg], COMP_ACC);
             else
                 step2_rows_t<<<gr, kBlock, 0, s>>>(L, cur, dcur, d_gseg[sg], dgseg[sg], pf[sg * nseg + o.seg[t + 1]],
-                                                   ginv, dginv, d_gi + (size_t)t * KM, d_dgi + (size_t)t * KM,
+                                                   ginv, dginv, t_gi + (size_t)t * KM, d_dgi + (size_t)t * KM,
                                                    o.d_phi[sg], o.d_dphi[sg], COMP_ACC, 1);
             cur = ginv; dcur = dginv;
             std::swap(ginv, tmp); std::swap(dginv, dtmp);

@@ -209,6 +209,36 @@ static __global__ void step2_rows_t(DLat L, const double *__restrict__ gin, cons
     });
 }
 
+// composition of a second-order backward step on interior sites, phi +=
+// sum_k mu_k out_k gf_k with the lumped multiplicities, and its tangent
+static __global__ void compose2_t(DLat L, int K, const double *__restrict__ out, const double *__restrict__ dout,
+                                  const double *__restrict__ gf, const double *__restrict__ dgf,
+                                  double *__restrict__ phi, double *__restrict__ dphi) {
+    const int M = L.M;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+        int c[3];
+        lat_coords(L, r, c);
+        if (!lat_interior(L, c)) continue;
+        double p = phi[r], dp = dphi[r];
+        for (int k = 0; k < K; k++) {
+            const size_t q = (size_t)k * M + r;
+            const double mu = comp_mult(K, k);
+            const double a = out[q] * gf[q], da = dout[q] * gf[q] + out[q] * dgf[q];
+            p += (mu == 1.0) ? a : a * mu;
+            dp += (mu == 1.0) ? da : da * mu;
+        }
+        phi[r] = p;
+        dphi[r] = dp;
+    }
+}
+
+// out = a + b
+static __global__ void sum2(size_t n, const double *__restrict__ a, const double *__restrict__ b,
+                            double *__restrict__ out) {
+    for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n; r += (size_t)gridDim.x * blockDim.x)
+        out[r] = a[r] + b[r];
+}
+
 static __global__ void connect_t(int M, int K, const double *__restrict__ a, const double *__restrict__ da,
                                  const double *__restrict__ b, const double *__restrict__ db,
                                  double *__restrict__ phi, double *__restrict__ dphi) {
@@ -216,8 +246,10 @@ static __global__ void connect_t(int M, int K, const double *__restrict__ a, con
         double p = phi[r], dp = dphi[r];
         for (int k = 0; k < K; k++) {
             size_t q = (size_t)k * M + r;
-            p += a[q] * b[q];
-            dp += da[q] * b[q] + a[q] * db[q];
+            const double mu = comp_mult(K, k);   // lumped multiplicities (1 otherwise)
+            const double v = a[q] * b[q], dv = da[q] * b[q] + a[q] * db[q];
+            p += (mu == 1.0) ? v : v * mu;
+            dp += (mu == 1.0) ? dv : dv * mu;
         }
         phi[r] = p;
         dphi[r] = dp;

@@ -132,3 +132,16 @@ def test_newton_krylov_agrees_with_pure_diis_on_sweep(gpu_lib):
             np.testing.assert_allclose(phi_nk[k], o.phi(k), rtol=1e-6, atol=1e-10 * np.max(o.phi(k)))
         checked += 1
     assert checked >= 15
+
+
+@pytest.mark.parametrize("case,stride", [("3d_2nd_brush", 4), ("2d_cylinder", 3), ("1d_2nd_lumped", 5)])
+def test_jvp_on_checkpointed_system(gpu_lib, case, stride):
+    """A system created with checkpointed chain storage keeps every slice of
+    the tangent sweeps in a buffer of their own: J.v equals the full-storage
+    system's bit for bit."""
+    spec = CASES[case]()
+    x = random_x(spec, seed=21, scale=0.2)
+    v = np.random.default_rng(22).normal(size=spec.n_itvar())
+    f1, jv1 = System(spec).jvp(x, v)
+    f2, jv2 = System(spec, checkpoint_stride=stride).jvp(x, v)
+    assert np.array_equal(f1, f2) and np.array_equal(jv1, jv2)
