@@ -57,6 +57,7 @@ PROTOTYPES = {
     "sfgpu_vjp": (i32, [vp, vp, vp, vp, vp]),
     "sfgpu_vjp_host": (i32, [vp, dp, dp, dp, dp]),
     "sfgpu_system_set_checkpoint": (i32, [vp, i32]),
+    "sfgpu_system_autotune_checkpoint": (i32, [vp, dp, i32, C.c_double, ip, dp]),
     "sfgpu_vjp_chi": (i32, [vp, dp, dp, dp]),
     "sfgpu_free_energy_grad": (i32, [vp, dp, dp, dp]),
     "sfgpu_phi_sensitivity_chi": (i32, [vp, dp, dp, dp, f64, i32, i32, dp]),

@@ -752,6 +752,60 @@ extern "C" int sfgpu_vjp_host(sfgpu_system *s, const double *x, const double *w,
     return SFGPU_OK;
 }
 
+// Checkpoint stride of the reverse sweep by measurement: every candidate
+// (full storage; k = ceil(sqrt(N)) and k/2, 2k, N/4 of the longest chain)
+// whose storage fits max_bytes (<= 0: no limit) is timed on `reps` reverse
+// sweeps at x (host) with CUDA events on the system's stream after one
+// untimed sweep; the fastest stays set.  Storage: 2N slices of K*M doubles
+// in full, 2 ceil(N/k) + 2k + 1 with checkpoints.
+extern "C" int sfgpu_system_autotune_checkpoint(sfgpu_system *s, const double *x, int reps, double max_bytes,
+                                                int *stride, double *best_ms) {
+    if (!s || !x || reps < 1) return SFGPU_ERR_INVALID;
+    int nmax = 1;
+    for (auto &o : s->mols) if (o.type != 0) nmax = std::max(nmax, o.N);
+    const double slice = 8.0 * s->K * s->M;
+    auto bytes = [&](int k) {
+        if (k == 0) return 2.0 * nmax * slice;
+        const double nq = (double)((nmax + k - 1) / k);
+        return (2 * nq + 2.0 * k + 1) * slice;
+    };
+    const int r = std::max(1, (int)std::ceil(std::sqrt((double)nmax)));
+    std::vector<int> cand = {0, r, std::max(1, r / 2), 2 * r, std::max(1, nmax / 4)};
+    std::sort(cand.begin(), cand.end());
+    cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    cudaEvent_t e0, e1;
+    SFGPU_CUDA_TRY(cudaEventCreate(&e0));
+    SFGPU_CUDA_TRY(cudaEventCreate(&e1));
+    int best = -1, rc = SFGPU_OK;
+    double best_t = 0;
+    for (int k : cand) {
+        if (k >= nmax && k != 0) continue;
+        if (max_bytes > 0 && bytes(k) > max_bytes) continue;
+        if ((rc = s->set_checkpoint(k)) || (rc = s->ensure_adjoint())) break;
+        if (cudaMemcpyAsync(s->d_x, x, sizeof(double) * s->nvar, cudaMemcpyHostToDevice, s->stream) != cudaSuccess) {
+            rc = SFGPU_ERR_CUDA;
+            break;
+        }
+        if ((rc = s->vjp_async(s->d_x, nullptr, s->d_f, s->a_xbar))) break;
+        cudaEventRecord(e0, s->stream);
+        for (int i = 0; i < reps && !rc; i++) rc = s->vjp_async(s->d_x, nullptr, s->d_f, s->a_xbar);
+        cudaEventRecord(e1, s->stream);
+        if (rc || cudaEventSynchronize(e1) != cudaSuccess) { if (!rc) rc = SFGPU_ERR_CUDA; break; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double t = ms / reps;
+        if (best < 0 || t < best_t) { best = k; best_t = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (best < 0) { sfgpu_set_error(cudaErrorMemoryAllocation, "no checkpoint stride fits max_bytes", __FILE__, __LINE__); return SFGPU_ERR_NOMEM; }
+    if ((rc = s->set_checkpoint(best))) return rc;
+    if (stride) *stride = best;
+    if (best_ms) *best_ms = best_t;
+    return SFGPU_OK;
+}
+
 // ---------------------------------------------------------------------------
 // L-BFGS on Phi(x) = |f(x)|^2 / 2, gradient J^T f from the adjoint sweep
 // ---------------------------------------------------------------------------

@@ -262,7 +262,7 @@ static __global__ void mol_scalars_t(MolParam p, int nblocks, const double *__re
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double dv = 0;
     for (int b = 0; b < nblocks; b++) dv += dpartial[b];
-    if (p.K == 6) dv /= 6.0;
+    if (p.K > 1) dv /= 6.0;   // six bond directions, lumped or not (as mol_scalars)
     const MolScal s = scal[self];
     MolScalT t;
     t.pad = 0;

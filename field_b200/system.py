@@ -226,6 +226,15 @@ class System:
         every k positions and recomputes segments (sfgpu_system_set_checkpoint)."""
         nat.check(self.lib.sfgpu_system_set_checkpoint(self.h, int(stride)), "sfgpu_system_set_checkpoint")
 
+    def autotune_checkpoint(self, x, reps: int = 3, max_bytes: float = 0.0):
+        """Checkpoint stride of the reverse sweep by timing candidate strides
+        at x (sfgpu_system_autotune_checkpoint); returns (stride, ms)."""
+        k, ms = C.c_int(), C.c_double()
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        nat.check(self.lib.sfgpu_system_autotune_checkpoint(self.h, _d(x), int(reps), float(max_bytes), C.byref(k),
+                                                             C.byref(ms)), "sfgpu_system_autotune_checkpoint")
+        return k.value, ms.value
+
     def solve_lbfgs(self, x0=None, tol=1e-7, maxit=2000, m=10) -> SolveResult:
         """L-BFGS on |f|^2/2 with the adjoint gradient (sfgpu_solve_lbfgs)."""
         x = np.zeros(self.nvar) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()

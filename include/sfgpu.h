@@ -384,6 +384,12 @@ int sfgpu_vjp_host(sfgpu_system *sys, const double *x, const double *w, double *
  * every stride (the recomputed slices are computed by the same kernels).
  * The storage is reallocated at the next sfgpu_vjp. */
 int sfgpu_system_set_checkpoint(sfgpu_system *sys, int stride);
+/* The checkpoint stride by measurement: full storage and strides around
+ * sqrt(N) of the longest chain (k/2, k, 2k, N/4), each whose storage fits
+ * max_bytes (<= 0: no limit), timed on `reps` reverse sweeps at the host
+ * vector x; the fastest is set and returned with its time per sweep. */
+int sfgpu_system_autotune_checkpoint(sfgpu_system *sys, const double *x, int reps, double max_bytes, int *stride,
+                                     double *best_ms);
 /* Sensitivity of the residual to the Flory-Huggins parameters at fixed x
  * (first and second order): dchi[a * nseg + i] = d (w . f(x)) / d chi(a, i)
  * over the entries the residual reads (a = the representative state of a

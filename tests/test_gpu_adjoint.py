@@ -303,3 +303,25 @@ def test_c3_full_size_gradient_at_64_sites(gpu_lib):
         _, jv = s.jvp(x0, e)
         fd_jv = (fp - fm) / (2 * h)
         assert np.max(np.abs(jv - fd_jv)) <= 1e-6 * max(np.max(np.abs(fd_jv)), 1e-12), i
+
+
+def test_checkpoint_stride_by_measurement(gpu_lib):
+    """The measured checkpoint stride (sfgpu_system_autotune_checkpoint)
+    respects the memory bound it is given and leaves J^T w unchanged."""
+    spec = CASES["3d_mirror_mix"]()
+    s = System(spec)
+    x = random_x(spec, seed=61, scale=0.2)
+    w = np.random.default_rng(62).normal(size=s.nvar)
+    f0, g0 = s.vjp(x, w)
+    k, ms = s.autotune_checkpoint(x, reps=2)
+    assert k >= 0 and ms > 0
+    f1, g1 = s.vjp(x, w)
+    assert np.array_equal(f0, f1)
+    np.testing.assert_allclose(g1, g0, rtol=0, atol=1e-12 * np.max(np.abs(g0)))
+    # a bound below full storage forces checkpoints
+    N = max(m.N for m in spec.molecules)
+    slice_bytes = 8.0 * spec.M
+    k2, _ = s.autotune_checkpoint(x, reps=1, max_bytes=N * slice_bytes)
+    assert k2 > 0
+    nq = -(-N // k2)
+    assert (2 * nq + 2 * k2 + 1) * slice_bytes <= N * slice_bytes
