@@ -28,7 +28,6 @@ int sfgpu_system::ensure_tangent() {
     if (charged) return fail_unsupported("derivatives of charged systems");
     for (auto &o : mols)
         if (o.dend) return fail_unsupported("derivatives of dendrimers");
-        else if (o.tree || o.ring) return fail_unsupported("derivatives of branched molecules and rings");
     if (t_ready) return SFGPU_OK;
     int rc;
     dgfull.assign(nseg, nullptr); dgseg.assign(nseg, nullptr); dphi.assign(nseg, nullptr);
@@ -45,7 +44,7 @@ int sfgpu_system::ensure_tangent() {
     }
     size_t store = 0;
     for (auto &o : mols) {
-        size_t need = (o.type == 0) ? 0 : (size_t)(o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
+        size_t need = (o.type == 0 || o.ring) ? 0 : (size_t)(o.tree ? 3 * o.N : o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
         store = std::max(store, need);
     }
     if ((rc = alloc_d(&d_dgi, store))) return rc;
@@ -95,12 +94,94 @@ int sfgpu_system::molecule_phi_t(int m) {
         finalize_phi_t<<<g, kBlock, 0, s>>>(M, d_gseg[i], dgseg[i], o.d_phi[i], o.d_dphi[i], scal, tscal, m, 1);
         return SFGPU_OK;
     }
+    if (o.ring) {
+        // the ring's walk with its tangent; lnGN, ln C and phibulk are
+        // constants of the ring (ring_scalars), their tangents 0
+        const int Mmax = (o.N / 2 > M) ? 2 * M : M + o.N / 2;
+        const size_t shm = (size_t)4 * (Mmax + 1) * sizeof(double);
+        if (shm > 200 * 1024) return fail_unsupported("the tangent of a ring walk larger than shared memory");
+        if (shm > 48 * 1024)
+            SFGPU_CUDA_TRY(cudaFuncSetAttribute(ring_phi_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        const int sg = o.seg[0];
+        ring_phi_t<<<std::min(M, 148 * 8), Mmax + 1 >= 256 ? 256 : 64, shm, s>>>(
+            M, o.N, Mmax, d_gseg[sg], dgseg[sg], o.phibulk, o.ring_norm0, o.d_phi[sg], o.d_dphi[sg]);
+        SFGPU_CUDA_TRY(cudaGetLastError());
+        set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_phi[sg]);
+        set_boundaries<<<g, kBlock, 0, s>>>(L, 1, o.d_dphi[sg]);
+        ring_scalars<<<1, 1, 0, s>>>(o.N, o.phibulk, scal, m);
+        SFGPU_CUDA_TRY(cudaMemsetAsync(tscal + m, 0, sizeof(MolScalT), s));
+        return SFGPU_OK;
+    }
+    const double *cur = nullptr, *dcur = nullptr;
+    if (o.tree) {
+        // the bond-tree recursion of molecule_phi_tree with tangents: steps
+        // by step1_rows_t, products by combine_t, compositions by connect_t
+        const int N = o.N;
+        auto U = [&](int q) { return t_gi + (size_t)q * M; };
+        auto Q = [&](int q) { return t_gi + (size_t)(N + q) * M; };
+        auto D = [&](int q) { return t_gi + (size_t)(2 * N + q) * M; };
+        auto dU = [&](int q) { return d_dgi + (size_t)q * M; };
+        auto dQ = [&](int q) { return d_dgi + (size_t)(N + q) * M; };
+        auto dD = [&](int q) { return d_dgi + (size_t)(2 * N + q) * M; };
+        const size_t bytes = sizeof(double) * M;
+        for (int i : o.used) {
+            SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_phi[i], 0, bytes, s));
+            SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_dphi[i], 0, bytes, s));
+        }
+        auto stepT = [&](const double *in, const double *din, int sgq, double *out, double *dout) {
+            step1_rows_t<<<gr, kBlock, 0, s>>>(L, in, din, d_gseg[sgq], dgseg[sgq], out, dout, nullptr, nullptr,
+                                               nullptr, nullptr, COMP_NONE);
+        };
+        for (int q = N - 1; q >= 0; q--) {
+            const int sq = o.seg[q];
+            const std::vector<int> &kids = o.kids[q];
+            if (kids.empty()) {
+                SFGPU_CUDA_TRY(cudaMemcpyAsync(U(q), d_gseg[sq], bytes, cudaMemcpyDeviceToDevice, s));
+                SFGPU_CUDA_TRY(cudaMemcpyAsync(dU(q), dgseg[sq], bytes, cudaMemcpyDeviceToDevice, s));
+            } else if (kids.size() == 1) {
+                SFGPU_CUDA_TRY(cudaMemcpyAsync(U(q), Q(kids[0]), bytes, cudaMemcpyDeviceToDevice, s));
+                SFGPU_CUDA_TRY(cudaMemcpyAsync(dU(q), dQ(kids[0]), bytes, cudaMemcpyDeviceToDevice, s));
+            } else {
+                const double *acc = Q(kids[0]), *dacc = dQ(kids[0]);
+                int w = 0;
+                for (size_t c = 1; c < kids.size(); c++) {
+                    const bool last = c + 1 == kids.size();
+                    double *dst = last ? U(q) : d_ginv[w], *ddst = last ? dU(q) : d_dginv[w];
+                    combine_t<<<g, kBlock, 0, s>>>(M, acc, dacc, Q(kids[c]), dQ(kids[c]), d_gseg[sq], dgseg[sq], dst,
+                                                   ddst);
+                    acc = dst; dacc = ddst;
+                    w ^= 1;
+                }
+            }
+            if (q > 0) stepT(U(q), dU(q), o.seg[o.parent[q]], Q(q), dQ(q));
+        }
+        SFGPU_CUDA_TRY(cudaMemcpyAsync(D(0), d_gseg[o.seg[0]], bytes, cudaMemcpyDeviceToDevice, s));
+        SFGPU_CUDA_TRY(cudaMemcpyAsync(dD(0), dgseg[o.seg[0]], bytes, cudaMemcpyDeviceToDevice, s));
+        for (int q = 0; q < N; q++) {
+            const int sq = o.seg[q];
+            connect_t<<<g, kBlock, 0, s>>>(M, 1, U(q), dU(q), D(q), dD(q), o.d_phi[sq], o.d_dphi[sq]);
+            const std::vector<int> &kids = o.kids[q];
+            for (int c : kids) {
+                const double *acc = D(q), *dacc = dD(q);
+                int w = 0;
+                for (int c2 : kids) {
+                    if (c2 == c) continue;
+                    combine_t<<<g, kBlock, 0, s>>>(M, acc, dacc, Q(c2), dQ(c2), d_gseg[sq], dgseg[sq], d_ginv[w],
+                                                   d_dginv[w]);
+                    acc = d_ginv[w]; dacc = d_dginv[w];
+                    w ^= 1;
+                }
+                stepT(acc, dacc, o.seg[c], D(c), dD(c));
+            }
+        }
+        cur = U(0);
+        dcur = dU(0);
+    } else {
     for (int i : o.used) {
         SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_phi[i], 0, sizeof(double) * M, s));
         SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_dphi[i], 0, sizeof(double) * M, s));
     }
     double *ginv = d_ginv[0], *tmp = d_ginv[1], *dginv = d_dginv[0], *dtmp = d_dginv[1];
-    const double *cur, *dcur;
     if (o.sym) {
         const int i = o.seg[0];
         const double *G = d_gseg[i], *dG = dgseg[i];
@@ -198,6 +279,7 @@ int sfgpu_system::molecule_phi_t(int m) {
             cur = ginv; dcur = dginv;
             std::swap(ginv, tmp); std::swap(dginv, dtmp);
         }
+    }
     }
     wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, cur, d_wgn, d_partial);
     wsum_partial<<<nblocks_red, kBlock, 0, s>>>(M, K, dcur, d_wgn, d_dpartial);

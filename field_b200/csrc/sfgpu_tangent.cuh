@@ -232,6 +232,76 @@ static __global__ void compose2_t(DLat L, int K, const double *__restrict__ out,
     }
 }
 
+// a b / G where G > 0, else 0 (dend_combine) and its tangent
+static __global__ void combine_t(int M, const double *__restrict__ a, const double *__restrict__ da,
+                                 const double *__restrict__ b, const double *__restrict__ db,
+                                 const double *__restrict__ G, const double *__restrict__ dG,
+                                 double *__restrict__ out, double *__restrict__ dout) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+        const double g = G[r];
+        if (g > 0) {
+            const double o = (a[r] * b[r]) / g;
+            out[r] = o;
+            dout[r] = (da[r] * b[r] + a[r] * db[r]) / g - o * dG[r] / g;
+        } else {
+            out[r] = 0;
+            dout[r] = 0;
+        }
+    }
+}
+
+// the ring's return walk (ring_phi, SF_HomoRing1stO.cpp:110-160) carrying
+// the walk's tangent dY beside Y: phi(k) = phib sum Y^2 / norm0, dphi(k) =
+// phib 2 sum Y dY / norm0; four shared-memory buffers of Mmax + 1 values
+static __global__ void ring_phi_t(int M, int N, int Mmax, const double *__restrict__ G, const double *__restrict__ dG,
+                                  double phibulk, double norm0, double *__restrict__ phi, double *__restrict__ dphi) {
+    extern __shared__ double ring_t_sh[];
+    __shared__ double red[32], dred[32];
+    double *Y = ring_t_sh, *Yn = Y + (Mmax + 1), *dY = Yn + (Mmax + 1), *dYn = dY + (Mmax + 1);
+    for (int k = blockIdx.x + 1; k <= M; k += gridDim.x) {
+        for (int z = threadIdx.x; z <= Mmax; z += blockDim.x) {
+            Y[z] = (z == k) ? G[k - 1] : 0.0;
+            dY[z] = (z == k) ? dG[k - 1] : 0.0;
+        }
+        __syncthreads();
+        for (int st = 1; st < N / 2; st++) {
+            const int zmin = max(k - st, 1), zmax = min(k + st, Mmax);
+            const double ytop = Y[Mmax - 1], dytop = dY[Mmax - 1];
+            for (int z = threadIdx.x; z <= Mmax; z += blockDim.x) {
+                double v = (z == Mmax) ? ytop : Y[z], dv = (z == Mmax) ? dytop : dY[z];
+                if (z >= zmin && z < zmax) {
+                    const double a = Y[z - 1], b = Y[z], c = (z + 1 == Mmax) ? ytop : Y[z + 1];
+                    const double da = dY[z - 1], db = dY[z], dc = (z + 1 == Mmax) ? dytop : dY[z + 1];
+                    const double gz = (z <= M) ? G[z - 1] / 6.0 : 1.0 / 6.0;
+                    const double dgz = (z <= M) ? dG[z - 1] / 6.0 : 0.0;
+                    v = gz * (a + 4 * b + c);
+                    dv = dgz * (a + 4 * b + c) + gz * (da + 4 * db + dc);
+                }
+                Yn[z] = v;
+                dYn[z] = dv;
+            }
+            __syncthreads();
+            double *t = Y; Y = Yn; Yn = t;
+            t = dY; dY = dYn; dYn = t;
+        }
+        double acc = 0, dacc = 0;
+        for (int z = threadIdx.x + 1; z <= Mmax; z += blockDim.x) { acc += Y[z] * Y[z]; dacc += 2 * Y[z] * dY[z]; }
+        for (int o = 16; o > 0; o >>= 1) {
+            acc += __shfl_down_sync(0xffffffffu, acc, o);
+            dacc += __shfl_down_sync(0xffffffffu, dacc, o);
+        }
+        if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = acc; dred[threadIdx.x >> 5] = dacc; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = 0, dv = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) { v += red[w]; dv += dred[w]; }
+            phi[k - 1] = v / norm0 * phibulk;
+            dphi[k - 1] = dv / norm0 * phibulk;
+        }
+        __syncthreads();
+    }
+}
+
 // out = a + b
 static __global__ void sum2(size_t n, const double *__restrict__ a, const double *__restrict__ b,
                             double *__restrict__ out) {

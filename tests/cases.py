@@ -310,9 +310,27 @@ CASES = {
     "2d_cyl_2nd_lumped": _cyl2d_2nd,
 }
 
+def _from_input(name):
+    """A system of the SFbox fixture inputs (tests/golden/reference_inputs.py)."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from reference_inputs import INPUTS
+    from field_b200.sfinput import build_system, parse_input
+    return build_system(parse_input(INPUTS[name])[0])[0]
+
+
+CASES.update({
+    "1d_branched": lambda: _from_input("1d_branched"),
+    "2d_branched": lambda: _from_input("2d_branched"),
+    "3d_branched": lambda: _from_input("3d_branched"),
+    "1d_comb_branched": lambda: _from_input("1d_comb_branched_side"),
+    "1d_ring": lambda: _from_input("1d_ring"),
+})
+
 # cases with forward-mode derivatives (all but dendrimers); the reverse mode
-# also leaves out the second-order lumped lattices and stiff ranges, which
-# the adjoint tests do not take ("2nd" cases are listed there by name)
+# also leaves out the second-order lumped lattices and stiff ranges (the
+# adjoint tests list "2nd" cases by name), branched molecules and rings
 NOT_DIFFERENTIABLE = ("dendrimer",)
 DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFERENTIABLE))
 
@@ -320,3 +338,5 @@ DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFEREN
 def random_x(spec, seed=7, scale=0.3):
     rng = np.random.default_rng(seed)
     return rng.normal(0.0, scale, spec.n_itvar())
+
+REVERSE_EXCLUDED = ("2nd", "branched", "ring", "comb")
