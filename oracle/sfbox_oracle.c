@@ -1816,6 +1816,7 @@ static void molecule_phi_ring(orc_system *s, omol *o) {
         for (int z = 1; z <= Mmax; z++) nk += Y[z] * Y[z];
         phi[k - 1] = nk / o->ring_norm0 * o->phibulk;
     }
+    olat_set_boundaries(&s->L, phi);   /* SF_SegmentList.cpp:524-525, as the contact averages read it */
     free(Y);
     o->lngn = 0;
     o->lnc = 0;
