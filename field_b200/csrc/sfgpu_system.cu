@@ -1161,8 +1161,16 @@ int sfgpu_system::residual_async(const double *x, double *f) {
     // segment weighting factors; on a charged lattice psi0 and E^2 first
     if (charged) {
         q_psi0<<<g, kBlock, 0, s>>>(L, qp, x);
-        if (qp.curved) q_esq_curved<<<g, kBlock, 0, s>>>(L, qp);
-        else q_esq<<<g, kBlock, 0, s>>>(L, qp);
+        if (L.grad == 3) {
+            q_esq_3d<<<g, kBlock, 0, s>>>(L, qp);
+            q_copy_boundaries<<<g, kBlock, 0, s>>>(L, qp.esq);
+        } else if (L.grad == 2) {
+            q_esq_2d<<<g, kBlock, 0, s>>>(L, qp);
+        } else if (qp.curved) {
+            q_esq_curved<<<g, kBlock, 0, s>>>(L, qp);
+        } else {
+            q_esq<<<g, kBlock, 0, s>>>(L, qp);
+        }
     }
     for (int i = 0; i < nseg; i++) {
         if (freedom[i] == SFGPU_SEG_FROZEN) continue;
@@ -1216,8 +1224,16 @@ int sfgpu_system::residual_async(const double *x, double *f) {
         all.n = nseg;
         for (int i = 0; i < nseg; i++) all.p[i] = d_phi[i];
         q_eps_charge<<<g, kBlock, 0, s>>>(M, nseg, all, qp);
-        if (qp.curved) q_poisson_curved<<<g, kBlock, 0, s>>>(L, qp);
-        else q_poisson<<<g, kBlock, 0, s>>>(L, qp);
+        if (L.grad == 3) {
+            q_poisson_3d<<<g, kBlock, 0, s>>>(L, qp);
+            q_copy_boundaries<<<g, kBlock, 0, s>>>(L, qp.psi);
+        } else if (L.grad == 2) {
+            q_poisson_2d<<<g, kBlock, 0, s>>>(L, qp);
+        } else if (qp.curved) {
+            q_poisson_curved<<<g, kBlock, 0, s>>>(L, qp);
+        } else {
+            q_poisson<<<g, kBlock, 0, s>>>(L, qp);
+        }
         residual_q<<<g, kBlock, 0, s>>>(L, rp, ct, qp, d_chib, f);
     } else {
         residual<<<grid_for(nsites), kBlock, 0, s>>>(L, rp, ct, d_sites, d_chib, f);
@@ -1253,8 +1269,8 @@ int sfgpu_system::setup_charges(const sfgpu_system_desc *d, const std::vector<in
         if (neutralizer >= 0) return fail(SFGPU_ERR_INVALID, "a neutralizer needs charged segments");
         return SFGPU_OK;
     }
-    if (K != 1 || L.grad != 1 || logmode)
-        return fail(SFGPU_ERR_UNSUPPORTED, "charges on lattices other than the first-order 1D ones");
+    if (K != 1 || logmode)
+        return fail(SFGPU_ERR_UNSUPPORTED, "charges on second-order or overflow-protected lattices");
     auto bulk_charge = [&](const HMol &o) {
         double q = 0;
         for (int i : o.used) q += 1.0 * valence[i] * o.count[i];
@@ -1285,28 +1301,50 @@ int sfgpu_system::setup_charges(const sfgpu_system_desc *d, const std::vector<in
             if (freedom[i] == SFGPU_SEG_FROZEN && range_h[(size_t)i * M + z] > 0) { pot = true; surf[z] = 1.0; }
         if (pot) xp[z] = (int)k++;
         if (jmap[z] >= 0) { xu[z] = (int)k; k += nclass; }
+        // the 3D sweep leaves boundary layers to SetBoundaries (Lat3D.cpp:1966):
+        // a psi there would be a copy, not a variable
+        if (pot && L.grad == 3 && !lat_interior(L, c))
+            return fail(SFGPU_ERR_UNSUPPORTED, "3D charges with frozen segments on a boundary layer");
     }
     nvar = (size_t)k;
     // lattice sites per layer (Lat1DFlat::MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269)
     const double ladj = d->lattice.layer_adjustment > 0 ? d->lattice.layer_adjustment : 1.0;
     std::vector<double> ls(M, 1.0);
-    if (L.cyl) for (int z = 0; z < M; z++) ls[z] = H.Lx[z];   // Lat1DCylinder.cpp:127-132
-    else if (M > 3) { ls[1] *= ladj; ls[M - 2] *= 2 - ladj; }
+    if (L.cyl) {   // Lat1DCylinder.cpp:127-132, Lat2DCylinder.cpp:156-164: the sites of the row
+        for (int z = 0; z < M; z++) {
+            int c[3];
+            lat_coords(L, z, c);
+            ls[z] = H.Lx[c[0]];
+        }
+    } else if (L.grad == 1 && M > 3) {
+        ls[1] *= ladj;
+        ls[M - 2] *= 2 - ladj;
+    }
     memset(&qp, 0, sizeof(qp));
     qp.diffeps = diffeps;
     qp.surf_lo = L.bc_lo[0] == SFGPU_BOUND_SURFACE;
     qp.surf_hi = L.bc_hi[0] == SFGPU_BOUND_SURFACE;
     qp.map_lo = lat_map(L, 0);
     qp.map_hi = lat_map(L, M - 1);
-    qp.curved = L.cyl;
+    qp.curved = L.cyl && L.grad == 1;
+    qp.cyl2 = L.cyl && L.grad == 2;
+    if (L.grad >= 2) {
+        qp.surf_ylo = L.bc_lo[1] == SFGPU_BOUND_SURFACE;
+        qp.surf_yhi = L.bc_hi[1] == SFGPU_BOUND_SURFACE;
+    }
+    if (qp.cyl2) qp.z0c = H.Lx[2] / 2 / sfk::kPi - 2;   // Lat2DCylinder.cpp:337
     qp.sph = d->lattice.geometry == SFGPU_GEOM_SPHERICAL;
     qp.off1 = d->lattice.offset_first_layer;
     qp.ladj = ladj;
     const double T = d->temperature > 0 ? d->temperature : 298.15;                      // SF_System.cpp:68
     const double bl = d->lattice.bondlength > 0 ? d->lattice.bondlength : 3e-10;       // Lat1DFlat.cpp:128
+    // the site distance: bondlength / sqrt(2 dimensions lambda) on the 1D and 2D
+    // lattices (Lat1DFlat.cpp:129, Lat2DFlat.cpp:209), the bondlength in 3D (Lat3D.cpp:263)
+    const double dims = d->lattice.dimensions > 0 ? d->lattice.dimensions : 3.0;
+    const double sd = L.grad == 3 ? bl : bl / sqrt(2 * dims * L.l1);
     qp.kT = sfk::kBoltzmann * T;
-    qp.pf_esq = (sfk::kEps0 * bl) / qp.kT;
-    qp.pf_psi = (sfk::kElemCharge / sfk::kEps0) / bl;
+    qp.pf_esq = (sfk::kEps0 * sd) / qp.kT;
+    qp.pf_psi = (sfk::kElemCharge / sfk::kEps0) / sd;
     for (int i = 0; i < nseg; i++) { qp.val[i] = valence[i]; qp.eps[i] = epsilon[i]; }
     int *dxu, *dxp;
     double *dls;

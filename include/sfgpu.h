@@ -125,9 +125,12 @@ typedef struct {
                                   [0, 0.5], l0 + 6 l1 + 12 l2 + 8 l3 = 1 within
                                   DBL_EPSILON; lambda3 is then recomputed from
                                   the other three (Lat3D.cpp:246-259) */
-    double bondlength;         /* lat : bondlength in m (Lat1DFlat.cpp:123-137), the
-                                  site distance of the Poisson equation of charged
-                                  systems; 0 = SFbox's default 3e-10 */
+    double bondlength;         /* lat : bondlength in m (Lat1DFlat.cpp:123-137); the
+                                  Poisson equation of charged systems uses the site
+                                  distance bondlength / sqrt(2 dimensions lambda) on
+                                  the 1D and 2D lattices (Lat1DFlat.cpp:129,
+                                  Lat2DFlat.cpp:209), the bondlength in 3D
+                                  (Lat3D.cpp:263); 0 = SFbox's default 3e-10 */
 } sfgpu_lattice_desc;
 
 typedef struct {
@@ -138,8 +141,10 @@ typedef struct {
      * valence in elementary charges and the relative dielectric constant
      * (0 = SFbox's default 80).  Any nonzero valence makes the system
      * charged: the electrostatic potential psi joins the iteration
-     * variables (SF_Solve.cpp:164-177) -- on the first-order 1D lattices
-     * (flat, cylinder, sphere); other lattices return SFGPU_ERR_UNSUPPORTED. */
+     * variables (SF_Solve.cpp:164-177) -- on the first-order lattices (1D
+     * flat, cylinder, sphere; 2D flat, cylinder; 3D, where no frozen segment
+     * may lie on a boundary layer); second-order and overflow-protected
+     * lattices return SFGPU_ERR_UNSUPPORTED. */
     double        valence;
     double        epsilon;
 } sfgpu_segment_desc;

@@ -4,6 +4,8 @@
 //
 //   sfref eval  <input.in> <x.bin|-> <out.txt>    one residual evaluation
 //   sfref solve <input.in> <x0.bin|-> <out.txt>   SF_Solve::Iterate from x0
+//   sfref poisson <input.in> <in.bin> <out.txt>   the lattice's Poisson sweep
+//                                                  and E^2 on given profiles
 //
 // x.bin holds the iteration variables as raw little-endian doubles in
 // SF_Solve's packing; "-" keeps SFbox's own initial guess
@@ -16,6 +18,7 @@
 // printed with 17 significant digits (exact round trip):
 //   nvar, x, g (residual at x), iterations, accuracy, F, Omega,
 //   state_<name>_phi, state_<name>_swf, mol_<name>_lngn, mol_<name>_phibulk,
+//   (charged systems) psi, charge, epsav,
 //   mol_<name>_theta, mol_<name>_phi, mol_<name>_seg_<segname>_phi
 // standard and fenk headers first, so only the reference's classes see the
 // access override that lets this driver read SF_Solve's iterate
@@ -76,7 +79,7 @@ static std::vector<double> read_x(const char *path) {
 
 int main(int argc, char **argv) {
     if (argc != 5) {
-        fprintf(stderr, "usage: sfref eval|solve <input.in> <x.bin|-> <out.txt>\n");
+        fprintf(stderr, "usage: sfref eval|solve|poisson <input.in> <x.bin|-> <out.txt>\n");
         return 2;
     }
     const std::string mode = argv[1];
@@ -106,6 +109,39 @@ int main(int argc, char **argv) {
     Sys->SetInitialGuess(Sys, Sys->GetLattice());
     SF_Solve *Solve = Sys->GetSolve();
     const int n = Solve->GetNumItVar();
+    if (mode == "poisson") {
+        // the lattice's Poisson sweep and field alone: x.bin holds psi0, the
+        // dielectric profile and the charge (M values each); out.txt gets
+        // psi (from zeros) and E^2 (from zeros) with the preFactors
+        // SF_SegmentList::ComputeElectricPotential(psi0) and
+        // SF_Solve::UpdateSWF pass
+        Lattice *Lat = Sys->GetLattice();
+        const int M = Lat->GetTotalNumLayers();
+        std::vector<double> in = read_x(argv[3]);
+        if ((int)in.size() != 3 * M) {
+            fprintf(stderr, "sfref: poisson wants %d values, %s holds %zu\n", 3 * M, argv[3], in.size());
+            return 2;
+        }
+        Vector psi0(1, M), psi0b(1, M), eps(1, M), charge(1, M), psi(1, M), esq(1, M);
+        for (int z = 1; z <= M; z++) {
+            psi0[z] = psi0b[z] = in[z - 1];
+            eps[z] = in[M + z - 1];
+            charge[z] = in[2 * M + z - 1];
+        }
+        const double pfp = (ELEM_CHARGE / EPS0) / Lat->GetSiteDistance();
+        const double pfe = (EPS0 * Lat->GetSiteDistance()) / (BOLTZMANN * TEMPERATURE);
+        Lat->ElectricPotential(psi, psi0, eps, charge, pfp);
+        Lat->ElectricFieldSquared(esq, psi0b, pfe);
+        g_out = fopen(argv[4], "w");
+        if (!g_out) return 2;
+        putv("psi", psi);
+        putv("esq", esq);
+        Vector sites(1, M);
+        for (int z = 1; z <= M; z++) sites[z] = Lat->GetNumLatticeSites(z);
+        putv("sites", sites);
+        fclose(g_out);
+        return 0;
+    }
     if (std::string(argv[3]) != "-") {
         std::vector<double> x0 = read_x(argv[3]);
         if ((int)x0.size() != n) {
@@ -157,6 +193,11 @@ int main(int argc, char **argv) {
     }
     put1("F", MolQ->GetFreeEnergy());
     put1("Omega", MolQ->GetGrandPotential());
+    if (SegQ->Charged()) {
+        putv("psi", SegQ->GetElectricPotential());
+        putv("charge", SegQ->GetCharge());
+        putv("epsav", SegQ->GetAverageEpsilon());
+    }
     fclose(g_out);
     return 0;
 }

@@ -261,6 +261,7 @@ static int olat_init(olat *L, const sfgpu_lattice_desc *d) {
         double off = d->offset_first_layer;
         double D = (d->dimensions > 0 ? d->dimensions : 3.0) - 1;
         double ladj = 1.0;
+        L->off1 = off;
         double *V = calloc(MX + 1, sizeof(double)), *S = calloc(MX + 1, sizeof(double));
         double *lm = calloc(MX + 1, sizeof(double)), *lp = calloc(MX + 1, sizeof(double));
         double *LL = calloc(MX + 1, sizeof(double));
@@ -802,7 +803,7 @@ struct orc_system {
        variables on the sites of PotItVar (SF_Solve.cpp:1761-1776) */
     int charged, diffeps, neutralizer;
     double *val, *eps;
-    double bondlength, temperature;
+    double bondlength, sitedist, temperature;
     int *xu, *xp;         /* per site: offset of its first u / of its psi in x, -1 if none */
     double *psi0, *psi, *esq, *lsites;
 };
@@ -848,8 +849,14 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
         }
     }
     s->bondlength = d->lattice.bondlength > 0 ? d->lattice.bondlength : 3e-10;   /* Lat1DFlat.cpp:128 */
+    {   /* the site distance: bondlength / sqrt(2 dimensions lambda) on the 1D and
+           2D lattices (Lat1DFlat.cpp:129, Lat2DFlat.cpp:209), the bondlength in
+           3D (Lat3D.cpp:263) */
+        const double dims = d->lattice.dimensions > 0 ? d->lattice.dimensions : 3.0;
+        s->sitedist = s->L.grad == 3 ? s->bondlength : s->bondlength / sqrt(2 * dims * s->L.l1);
+    }
     s->temperature = d->temperature > 0 ? d->temperature : 298.15;              /* SF_System.cpp:68 */
-    if (s->charged && (s->L.grad != 1 || s->L.order != 1 || s->L.logmode)) {
+    if (s->charged && (s->L.order != 1 || s->L.logmode)) {
         orc_destroy(s); return SFGPU_ERR_UNSUPPORTED;
     }
     for (int i = 0; i < ns; i++)   /* epsilon differs among liquid states (SF_Solve.cpp:154-162) */
@@ -1045,6 +1052,9 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
                 if (s->freedom[i] == SFGPU_SEG_FROZEN && s->range[(size_t)i * M + z] > 0) pot = 1;
             if (pot) s->xp[z] = k++;
             if (j < s->nsites && s->sites[j] == z) { s->xu[z] = k; k += s->nclass; j++; }
+            /* the 3D sweep leaves boundary layers to SetBoundaries: a psi
+               there would be a copy, not a variable */
+            if (pot && s->L.grad == 3 && !is_interior(&s->L, z)) { orc_destroy(s); return SFGPU_ERR_UNSUPPORTED; }
         }
         s->nvar = k;
     } else {
@@ -1055,7 +1065,10 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
     s->esq = calloc(M, sizeof(double));
     /* lattice sites per layer (MultiplyWithLatticeSites, Lat1DFlat.cpp:266-269) */
     s->lsites = malloc(sizeof(double) * M);
-    for (int z = 0; z < M; z++) s->lsites[z] = s->L.cyl ? s->L.Lx[z] : 1.0;   /* curved: Lat1DCylinder.cpp:127-132 */
+    for (int z = 0; z < M; z++) {   /* curved: Lat1DCylinder.cpp:127-132, Lat2DCylinder.cpp:156-164 */
+        int c[3]; coords(&s->L, z, c);
+        s->lsites[z] = s->L.cyl ? s->L.Lx[c[0]] : 1.0;
+    }
     if (s->L.grad == 1 && !s->L.cyl && M > 3) { s->lsites[1] *= s->L.ladj; s->lsites[M - 2] *= 2 - s->L.ladj; }
     s->swf_full = calloc((size_t)ns * M, sizeof(double));
     s->swf = calloc((size_t)ns * M, sizeof(double));
@@ -1207,6 +1220,395 @@ static void olat_esq_curved(const olat *L, const double *psi, double preFactor, 
     if (L->bc_hi[0] == SFGPU_BOUND_SURFACE) esq[M - 1] = pf * eplus / Z;
 }
 
+/* The 2D sweeps and fields below walk the lattice as the reference does,
+   1-based (site k of the reference is index k - 1 here; MY sites per row x):
+   the lower x row first, then the rows x = 2..MX-1 from y = 1 to MY, then the
+   upper x row.  A boundary row or column is updated only where its bound is
+   a surface; the other entries keep their previous value.  Two-term sums are
+   exact under commutation, so only longer sums keep the reference's order,
+   and the reference's own choices are kept where they look like slips (the
+   first site of the lower x row takes the running y-sum of the corner, the
+   upper y corner of the lower row the charge of site 1, the upper corner of
+   the upper row the dielectric sum eps[M-MY] + eps[M]). */
+#define R1(a, k) (a)[(k) - 1]
+
+/* Lat2DFlat::ElectricPotential (Lat2DFlat.cpp:1116-1207) */
+static void olat_poisson_2dflat(const olat *L, double *psi0, const double *eps, const double *charge,
+                                double preFactor, double *psi) {
+    const int MX = L->Md[0], MY = L->Md[1], M = MX * MY;
+    const int sx1 = L->bc_lo[0] == SFGPU_BOUND_SURFACE, sx2 = L->bc_hi[0] == SFGPU_BOUND_SURFACE;
+    const int sy1 = L->bc_lo[1] == SFGPU_BOUND_SURFACE, sy2 = L->bc_hi[1] == SFGPU_BOUND_SURFACE;
+    const double pf = 2 * preFactor;
+    double exm, exp_, eym = 0, eyp;
+    int z;
+    olat_set_boundaries(L, psi0);
+    if (sx1) {
+        eyp = R1(eps, 1) + R1(eps, 2);
+        if (sy1) {
+            exp_ = R1(eps, 1) + R1(eps, MY + 1);
+            R1(psi, 1) = (pf * R1(charge, 1) + exp_ * R1(psi0, MY + 1) + eyp * R1(psi0, 2)) / (exp_ + eyp);
+        }
+        for (z = MY - 1; z > 1; z--) {
+            eym = eyp;
+            exp_ = R1(eps, z) + R1(eps, z + MY);
+            eyp = R1(eps, z) + R1(eps, z + 1);
+            R1(psi, z) = (pf * R1(charge, z) + exp_ * R1(psi0, z + MY) + eym * R1(psi0, z - 1) + eyp * R1(psi0, z + 1)) /
+                         (exp_ + eym + eyp);
+        }
+        if (sy2) {
+            exp_ = R1(eps, MY) + R1(eps, MY + MY);
+            R1(psi, MY) = (pf * R1(charge, z) + exp_ * R1(psi0, MY + MY) + eyp * R1(psi0, MY - 1)) / (exp_ + eyp);
+        }
+    }
+    z = MY + 1;
+    for (int x = 2; x < MX; x++) {
+        eyp = R1(eps, z) + R1(eps, z + 1);
+        if (sy1) {
+            exm = R1(eps, z) + R1(eps, z - MY);
+            exp_ = R1(eps, z) + R1(eps, z + MY);
+            R1(psi, z) = (pf * R1(charge, z) + exm * R1(psi0, z - MY) + exp_ * R1(psi0, z + MY) + eyp * R1(psi0, z + 1)) /
+                         (exm + exp_ + eyp);
+        }
+        z++;
+        for (int y = 2; y < MY; y++, z++) {
+            eym = eyp;
+            exm = R1(eps, z) + R1(eps, z - MY);
+            exp_ = R1(eps, z) + R1(eps, z + MY);
+            eyp = R1(eps, z) + R1(eps, z + 1);
+            R1(psi, z) = (pf * R1(charge, z) + exm * R1(psi0, z - MY) + exp_ * R1(psi0, z + MY) + eym * R1(psi0, z - 1) +
+                          eyp * R1(psi0, z + 1)) / (exm + exp_ + eym + eyp);
+        }
+        if (sy2) {
+            exm = R1(eps, z) + R1(eps, z - MY);
+            exp_ = R1(eps, z) + R1(eps, z + MY);
+            R1(psi, z) = (pf * R1(charge, z) + exm * R1(psi0, z - MY) + exp_ * R1(psi0, z + MY) + eyp * R1(psi0, z - 1)) /
+                         (exm + exp_ + eyp);
+        }
+        z++;
+    }
+    if (sx2) {
+        eyp = R1(eps, M - MY + 1) + R1(eps, M - MY + 2);
+        if (sy1) {
+            exm = R1(eps, M - MY + 1) + R1(eps, M - MY - MY + 1);
+            R1(psi, M - MY + 1) = (pf * R1(charge, M - MY + 1) + exm * R1(psi0, M - MY - MY + 1) + eyp * R1(psi0, M - MY + 2)) /
+                                  (exm + eyp);
+        }
+        for (z = M - MY + 2; z < M; z++) {
+            eym = eyp;
+            exm = R1(eps, z) + R1(eps, z - MY);
+            eyp = R1(eps, z) + R1(eps, z + 1);
+            R1(psi, z) = (pf * R1(charge, z) + exm * R1(psi0, z - MY) + eym * R1(psi0, z - 1) + eyp * R1(psi0, z + 1)) /
+                         (exm + eym + eyp);
+        }
+        if (sy2) {
+            exm = R1(eps, M - MY) + R1(eps, M);
+            R1(psi, M) = (pf * R1(charge, M) + exm * R1(psi0, M - MY) + eyp * R1(psi0, M - 1)) / (exm + eyp);
+        }
+    }
+}
+
+/* Lat2DFlat::ElectricFieldSquared (Lat2DFlat.cpp:1209-1272) */
+static void olat_esq_2dflat(const olat *L, const double *psi, double preFactor, double *esq) {
+    const int MX = L->Md[0], MY = L->Md[1], M = MX * MY;
+    const int sx1 = L->bc_lo[0] == SFGPU_BOUND_SURFACE, sx2 = L->bc_hi[0] == SFGPU_BOUND_SURFACE;
+    const int sy1 = L->bc_lo[1] == SFGPU_BOUND_SURFACE, sy2 = L->bc_hi[1] == SFGPU_BOUND_SURFACE;
+    const double pf = preFactor / 2;
+    double exm, exp_, eym, eyp;
+    int z;
+    #define SQ(v) ((v) * (v))
+    if (sx1) {
+        eym = SQ(R1(psi, MY - 1) - R1(psi, MY));
+        for (z = MY - 1; z > 1; z--) {
+            eyp = eym;
+            eym = SQ(R1(psi, z) - R1(psi, z - 1));
+            exp_ = SQ(R1(psi, z) - R1(psi, z + MY));
+            R1(esq, z) = pf * (exp_ + eym + eyp);
+        }
+    }
+    z = MY + 1;
+    for (int x = 2; x < MX; x++) {
+        eyp = SQ(R1(psi, z) - R1(psi, z + 1));
+        if (sy1) {
+            exm = SQ(R1(psi, z) - R1(psi, z - MY));
+            exp_ = SQ(R1(psi, z) - R1(psi, z + MY));
+            R1(esq, z) = pf * (exm + exp_ + eyp);
+        }
+        z++;
+        for (int y = 2; y < MY; y++, z++) {
+            eym = eyp;
+            eyp = SQ(R1(psi, z) - R1(psi, z + 1));
+            exm = SQ(R1(psi, z) - R1(psi, z - MY));
+            exp_ = SQ(R1(psi, z) - R1(psi, z + MY));
+            R1(esq, z) = pf * (exm + exp_ + eym + eyp);
+        }
+        if (sy2) {
+            exm = SQ(R1(psi, z) - R1(psi, z - MY));
+            exp_ = SQ(R1(psi, z) - R1(psi, z + MY));
+            R1(esq, z) = pf * (exm + exp_ + eyp);
+        }
+        z++;
+    }
+    if (sx2) {
+        eyp = SQ(R1(psi, M - MY + 2) - R1(psi, M - MY + 1));
+        for (z = M - MY + 2; z < M; z++) {
+            eym = eyp;
+            eyp = SQ(R1(psi, z) - R1(psi, z + 1));
+            exm = SQ(R1(psi, z) - R1(psi, z - MY));
+            R1(esq, z) = pf * (exm + eym + eyp);
+        }
+    }
+}
+
+/* radius to the centre of the first layer of the 2D cylinder, L[3]/2/PI - 2
+   (Lat2DCylinder.cpp:337) */
+static double cyl2d_z0(const olat *L) {
+    const double PI_ = 4.0 * atan(1.0);
+    return L->Lx[2] / 2 / PI_ - 2;
+}
+
+/* Lat2DCylinder::ElectricPotential (Lat2DCylinder.cpp:323-450): the
+   dielectric sums across rows weighted by 1 -+ 1/(2Z), the charge term by
+   1/(PI Z); without an offset the first interior row has no inner
+   neighbour and is walked from y = MY down */
+static void olat_poisson_2dcyl(const olat *L, double *psi0, const double *eps, const double *charge,
+                               double preFactor, double *psi) {
+    const double PI_ = 4.0 * atan(1.0);
+    const int MX = L->Md[0], MY = L->Md[1], M = MX * MY;
+    const int sx1 = L->bc_lo[0] == SFGPU_BOUND_SURFACE, sx2 = L->bc_hi[0] == SFGPU_BOUND_SURFACE;
+    const int sy1 = L->bc_lo[1] == SFGPU_BOUND_SURFACE, sy2 = L->bc_hi[1] == SFGPU_BOUND_SURFACE;
+    double Z = cyl2d_z0(L), pf, xm, xp, exm, exp_, eym, eyp = 0;
+    int x, z;
+    olat_set_boundaries(L, psi0);
+    if (L->off1 <= 0) {
+        Z++;
+        pf = preFactor / PI_ / Z;
+        xp = 1 + 0.5 / Z;
+        z = MY + MY;
+        eym = R1(eps, z) + R1(eps, z - 1);
+        if (sy2) {
+            exp_ = xp * (R1(eps, z) + R1(eps, z + MY));
+            R1(psi, z) = (pf * R1(charge, z) + eym * R1(psi0, z - 1) + exp_ * R1(psi0, z + MY)) / (eym + exp_);
+        }
+        for (z = 2 * MY - 1; z > MY + 1; z--) {
+            eyp = eym;
+            eym = R1(eps, z) + R1(eps, z - 1);
+            exp_ = xp * (R1(eps, z) + R1(eps, z + MY));
+            R1(psi, z) = (pf * R1(charge, z) + exp_ * R1(psi0, z + MY) + eym * R1(psi0, z - 1) + eyp * R1(psi0, z + 1)) /
+                         (exp_ + eym + eyp);
+        }
+        if (sy1) {
+            exp_ = xp * (R1(eps, z) + R1(eps, z + MY));
+            R1(psi, z) = (pf * R1(charge, z) + exp_ * R1(psi0, z + MY) + eym * R1(psi0, z + 1)) / (exp_ + eym);
+        }
+        x = 3;
+        z = MY + MY + 1;
+    } else {
+        if (sx1) {
+            pf = preFactor / PI_ / Z;
+            xp = 1 + 0.5 / Z;
+            eym = R1(eps, MY) + R1(eps, MY - 1);
+            if (sy2) {
+                exp_ = xp * (R1(eps, MY) + R1(eps, MY + MY));
+                R1(psi, MY) = (pf * R1(charge, MY) + eym * R1(psi0, MY - 1) + exp_ * R1(psi0, MY + MY)) / (eym + exp_);
+            }
+            for (z = MY - 1; z > 1; z--) {
+                eyp = eym;
+                eym = R1(eps, z) + R1(eps, z - 1);
+                exp_ = xp * (R1(eps, z) + R1(eps, z + MY));
+                R1(psi, z) = (pf * R1(charge, z) + exp_ * R1(psi0, z + MY) + eym * R1(psi0, z - 1) + eyp * R1(psi0, z + 1)) /
+                             (exp_ + eym + eyp);
+            }
+            if (sy1) {
+                exp_ = xp * (R1(eps, 1) + R1(eps, MY + 1));
+                R1(psi, 1) = (pf * R1(charge, 1) + exp_ * R1(psi0, MY + 1) + eym * R1(psi0, 2)) / (exp_ + eym);
+            }
+        }
+        x = 2;
+        z = MY + 1;
+    }
+    for (; x < MX; x++) {
+        Z++;
+        pf = preFactor / PI_ / Z;
+        xm = 1 - 0.5 / Z;
+        xp = 1 + 0.5 / Z;
+        eyp = R1(eps, z) + R1(eps, z + 1);
+        if (sy1) {
+            exm = xm * (R1(eps, z - MY) + R1(eps, z));
+            exp_ = xp * (R1(eps, z) + R1(eps, z + MY));
+            R1(psi, z) = (pf * R1(charge, z) + exm * R1(psi0, z - MY) + exp_ * R1(psi0, z + MY) + eyp * R1(psi0, z + 1)) /
+                         (exm + exp_ + eyp);
+        }
+        z++;
+        for (int y = 2; y < MY; y++, z++) {
+            eym = eyp;
+            eyp = R1(eps, z) + R1(eps, z + 1);
+            exm = xm * (R1(eps, z - MY) + R1(eps, z));
+            exp_ = xp * (R1(eps, z) + R1(eps, z + MY));
+            R1(psi, z) = (pf * R1(charge, z) + exm * R1(psi0, z - MY) + exp_ * R1(psi0, z + MY) + eym * R1(psi0, z - 1) +
+                          eyp * R1(psi0, z + 1)) / (exm + exp_ + eym + eyp);
+        }
+        if (sy2) {
+            exm = xm * (R1(eps, z - MY) + R1(eps, z));
+            exp_ = xp * (R1(eps, z) + R1(eps, z + MY));
+            R1(psi, z) = (pf * R1(charge, z) + exm * R1(psi0, z - MY) + exp_ * R1(psi0, z + MY) + eyp * R1(psi0, z - 1)) /
+                         (exm + exp_ + eyp);
+        }
+        z++;
+    }
+    if (sx2) {
+        Z++;
+        pf = preFactor / PI_ / Z;
+        xm = 1 - 0.5 / Z;
+        eyp = R1(eps, M - MY + 1) + R1(eps, M - MY + 2);
+        if (sy1) {
+            exm = xm * (R1(eps, M - MY - MY + 1) + R1(eps, M - MY + 1));
+            R1(psi, M - MY + 1) = (pf * R1(charge, M - MY + 1) + exm * R1(psi0, M - MY - MY + 1) + eyp * R1(psi0, M - MY + 2)) /
+                                  (exm + eyp);
+        }
+        for (z = M - MY + 2; z < M; z++) {
+            eym = eyp;
+            eyp = R1(eps, z) + R1(eps, z + 1);
+            exm = xm * (R1(eps, z - MY) + R1(eps, z));
+            R1(psi, z) = (pf * R1(charge, z) + exm * R1(psi0, z - MY) + eym * R1(psi0, z - 1) + eyp * R1(psi0, z + 1)) /
+                         (exm + eym + eyp);
+        }
+        if (sy2) {
+            exm = xm * (R1(eps, M) + R1(eps, M - MY));
+            R1(psi, M) = (pf * R1(charge, M) + exm * R1(psi0, M - MY) + eyp * R1(psi0, M - 1)) / (exm + eyp);
+        }
+    }
+}
+
+/* Lat2DCylinder::ElectricFieldSquared (Lat2DCylinder.cpp:452-541) */
+static void olat_esq_2dcyl(const olat *L, const double *psi, double preFactor, double *esq) {
+    const int MX = L->Md[0], MY = L->Md[1], M = MX * MY;
+    const int sx1 = L->bc_lo[0] == SFGPU_BOUND_SURFACE, sx2 = L->bc_hi[0] == SFGPU_BOUND_SURFACE;
+    const int sy1 = L->bc_lo[1] == SFGPU_BOUND_SURFACE, sy2 = L->bc_hi[1] == SFGPU_BOUND_SURFACE;
+    const double pf = preFactor / 2;
+    double Z = cyl2d_z0(L), xm, xp, exm, exp_, eym, eyp;
+    int x, z;
+    if (L->off1 <= 0) {
+        Z++;
+        xp = 1 + 0.5 / Z;
+        eym = SQ(R1(psi, MY + MY) - R1(psi, MY + MY - 1));
+        for (z = 2 * MY - 1; z > MY + 1; z--) {
+            eyp = eym;
+            eym = SQ(R1(psi, z) - R1(psi, z - 1));
+            exp_ = R1(psi, z) - R1(psi, z + MY);
+            exp_ *= xp * exp_;
+            R1(esq, z) = pf * (exp_ + eym + eyp);
+        }
+        x = 3;
+        z = MY + MY + 1;
+    } else {
+        if (sx1) {
+            xp = 1 + 0.5 / Z;
+            eym = SQ(R1(psi, MY) - R1(psi, MY - 1));
+            for (z = MY - 1; z > 1; z--) {
+                eyp = eym;
+                eym = SQ(R1(psi, z) - R1(psi, z - 1));
+                exp_ = R1(psi, z) - R1(psi, z + MY);
+                exp_ *= xp * exp_;
+                R1(esq, z) = pf * (exp_ + eym + eyp);
+            }
+        }
+        x = 2;
+        z = MY + 1;
+    }
+    for (; x < MX; x++) {
+        Z++;
+        xm = 1 - 0.5 / Z;
+        xp = 1 + 0.5 / Z;
+        eyp = SQ(R1(psi, z) - R1(psi, z + 1));
+        if (sy1) {
+            exm = R1(psi, z) - R1(psi, z - MY);
+            exm *= xm * exm;
+            exp_ = R1(psi, z) - R1(psi, z + MY);
+            exp_ *= xp * exp_;
+            R1(esq, z) = pf * (exm + exp_ + eyp);
+        }
+        z++;
+        for (int y = 2; y < MY; y++, z++) {
+            eym = eyp;
+            eyp = SQ(R1(psi, z) - R1(psi, z + 1));
+            exm = R1(psi, z) - R1(psi, z - MY);
+            exm *= xm * exm;
+            exp_ = R1(psi, z) - R1(psi, z + MY);
+            exp_ *= xp * exp_;
+            R1(esq, z) = pf * (exm + exp_ + eym + eyp);
+        }
+        if (sy2) {
+            exm = R1(psi, z) - R1(psi, z - MY);
+            exm *= xm * exm;
+            exp_ = R1(psi, z) - R1(psi, z + MY);
+            exp_ *= xp * exp_;
+            R1(esq, z) = pf * (exm + exp_ + eyp);
+        }
+        z++;
+    }
+    if (sx2) {
+        Z++;
+        xm = 1 - 0.5 / Z;
+        eyp = SQ(R1(psi, M - MY + 2) - R1(psi, M - MY + 1));
+        for (z = M - MY + 2; z < M; z++) {
+            eym = eyp;
+            eyp = SQ(R1(psi, z) - R1(psi, z + 1));
+            exm = R1(psi, z) - R1(psi, z - MY);
+            exm *= xm * exm;
+            R1(esq, z) = pf * (exm + eym + eyp);
+        }
+    }
+    (void)sy1; (void)sy2;
+}
+
+/* Lat3D::ElectricPotential (Lat3D.cpp:1937-1969): boundaries of psi0 and
+   of the dielectric profile first, then per site the six neighbour terms in
+   the order -x, +x, -y, +y, -z, +z, the charge term, the division by the
+   summed dielectric weights (0 where they are not positive), and the
+   boundaries of psi.  Only interior sites are computed here: the
+   reference's shifted vector operations leave boundary entries to
+   SetBoundaries (no psi site lies on a boundary layer of a 3D lattice). */
+static void olat_poisson_3d(const olat *L, double *psi0, const double *eps_in, const double *charge,
+                            double preFactor, double *psi) {
+    const int M = L->M, jx = L->st[0], jy = L->st[1];
+    double *eps = malloc(sizeof(double) * M);
+    memcpy(eps, eps_in, sizeof(double) * M);
+    olat_set_boundaries(L, psi0);
+    olat_set_boundaries(L, eps);
+    const int off[6] = {-jx, jx, -jy, jy, -1, 1};
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(L, z)) continue;
+        double tot = 0, acc = 0;
+        for (int k = 0; k < 6; k++) {
+            const double w = eps[z + off[k]] + eps[z];
+            if (k == 0) { tot = w; acc = w * psi0[z + off[k]]; }
+            else { tot += w; acc += w * psi0[z + off[k]]; }
+        }
+        acc += charge[z] * (2 * preFactor);
+        psi[z] = (tot > 0) ? acc / tot : 0.0;
+    }
+    olat_set_boundaries(L, psi);
+    free(eps);
+}
+
+/* Lat3D::ElectricFieldSquared (Lat3D.cpp:1979-2005): the six squared
+   differences in the same order, times preFactor / 2 */
+static void olat_esq_3d(const olat *L, double *psi, double preFactor, double *esq) {
+    const int M = L->M, jx = L->st[0], jy = L->st[1];
+    const int off[6] = {-jx, jx, -jy, jy, -1, 1};
+    olat_set_boundaries(L, psi);
+    const double pf = preFactor / 2;
+    for (int z = 0; z < M; z++) {
+        if (!is_interior(L, z)) continue;
+        double e = SQ(psi[z] - psi[z + off[0]]);
+        for (int k = 1; k < 6; k++) e += SQ(psi[z] - psi[z + off[k]]);
+        esq[z] = e * pf;
+    }
+    olat_set_boundaries(L, esq);
+}
+#undef SQ
+#undef R1
+
 /* SF_SegmentList::GetCharge (SF_SegmentList.cpp:759-784): sum phi valence /
    phi_T per layer, times the lattice sites of the layer */
 static void state_charge(const orc_system *s, double *charge) {
@@ -1229,8 +1631,12 @@ static void update_swf(orc_system *s, const double *x) {
         /* psi0 from x, its boundary copies and E^2 (SF_Solve.cpp:797-818) */
         for (int z = 0; z < M; z++) if (s->xp[z] >= 0) s->psi0[z] = x[s->xp[z]];
         olat_set_boundaries(&s->L, s->psi0);
-        if (s->L.cyl) olat_esq_curved(&s->L, s->psi0, (ORC_EPS0 * s->bondlength) / kT, s->esq);
-        else olat_esq_flat(&s->L, s->psi0, (ORC_EPS0 * s->bondlength) / kT, s->esq);
+        const double pfe = (ORC_EPS0 * s->sitedist) / kT;
+        if (s->L.grad == 3) olat_esq_3d(&s->L, s->psi0, pfe, s->esq);
+        else if (s->L.grad == 2 && s->L.cyl) olat_esq_2dcyl(&s->L, s->psi0, pfe, s->esq);
+        else if (s->L.grad == 2) olat_esq_2dflat(&s->L, s->psi0, pfe, s->esq);
+        else if (s->L.cyl) olat_esq_curved(&s->L, s->psi0, pfe, s->esq);
+        else olat_esq_flat(&s->L, s->psi0, pfe, s->esq);
     }
     for (int i = 0; i < s->nseg; i++) {
         double *gf = s->swf_full + (size_t)i * M;
@@ -2052,10 +2458,12 @@ static void get_residuals(orc_system *s, double *f) {
         for (int i = 0; i < ns; i++)
             for (int z = 0; z < M; z++) epsav[z] += s->phi[(size_t)i * M + z] * s->eps[i];
         state_charge(s, charge);
-        if (s->L.cyl)
-            olat_poisson_curved(&s->L, s->psi0, epsav, charge, (ORC_ELEM_CHARGE / ORC_EPS0) / s->bondlength, s->psi);
-        else
-            olat_poisson_flat(&s->L, s->psi0, epsav, charge, (ORC_ELEM_CHARGE / ORC_EPS0) / s->bondlength, s->psi);
+        const double pfp = (ORC_ELEM_CHARGE / ORC_EPS0) / s->sitedist;
+        if (s->L.grad == 3) olat_poisson_3d(&s->L, s->psi0, epsav, charge, pfp, s->psi);
+        else if (s->L.grad == 2 && s->L.cyl) olat_poisson_2dcyl(&s->L, s->psi0, epsav, charge, pfp, s->psi);
+        else if (s->L.grad == 2) olat_poisson_2dflat(&s->L, s->psi0, epsav, charge, pfp, s->psi);
+        else if (s->L.cyl) olat_poisson_curved(&s->L, s->psi0, epsav, charge, pfp, s->psi);
+        else olat_poisson_flat(&s->L, s->psi0, epsav, charge, pfp, s->psi);
         free(epsav); free(charge);
     }
     for (int i = 0; i < ns; i++) olat_side(&s->L, s->phi + (size_t)i * M, s->rho + (size_t)i * M);
@@ -2146,8 +2554,11 @@ static double *elec_profile(const orc_system *s) {
     int M = s->L.M;
     double *q = malloc(sizeof(double) * M);
     state_charge(s, q);
-    for (int z = 0; z < M; z++)   /* DivideByLatticeSites: curved lattices skip zeros */
-        if (!s->L.cyl || q[z] != 0) q[z] /= s->lsites[z];
+    for (int z = 0; z < M; z++) {   /* DivideByLatticeSites: the 1D curved lattices skip zero
+                                       entries, the 2D cylinder rows without sites */
+        if (s->L.grad == 2 && s->L.cyl) { if (s->lsites[z] != 0) q[z] /= s->lsites[z]; }
+        else if (!s->L.cyl || q[z] != 0) q[z] /= s->lsites[z];
+    }
     const double kT = ORC_BOLTZMANN * s->temperature;
     for (int z = 0; z < M; z++) q[z] = 0.5 * s->psi[z] * q[z] * ORC_ELEM_CHARGE / kT;
     return q;

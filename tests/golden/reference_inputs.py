@@ -994,6 +994,217 @@ start
 """,
     # a comb whose side chains are branched (two fragments at one point)
     "1d_comb_branched_side": INPUTS_COMB_BRANCHED_SIDE,
+    # charges on the 2D flat lattice (Lat2DFlat::ElectricPotential): a
+    # charged surface row at lower x, mirrors elsewhere
+    "2d_flat_charged": """lat : sq : gradients : 2
+lat : sq : geometry : flat
+lat : sq : n_layers_x : 14
+lat : sq : n_layers_y : 11
+lat : sq : lambda : 0.16666666666666667
+lat : sq : lowerbound_x : surface
+lat : sq : upperbound_x : mirror1
+lat : sq : lowerbound_y : mirror2
+lat : sq : upperbound_y : mirror1
+lat : sq : bondlength : 3e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : 0,1;0,11
+mon : S : valence : -0.2
+mon : S : epsilon : 5
+mon : A : freedom : free
+mon : A : valence : 0.5
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - W : 0.5
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)12
+mol : pol : freedom : free
+mol : pol : phibulk : 0.002
+mol : Na : composition : (Na)1
+mol : Na : freedom : free
+mol : Na : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # a charged corner: surfaces at lower x (row S) and lower y (column T),
+    # the upper x row a surface too (U), different dielectric constants of
+    # the liquid states; square, because SFbox checks the upper x surface
+    # row at sites y + M - MX (Lat2DFlat.cpp:876-881)
+    "2d_flat_charged_walls": """lat : sq : gradients : 2
+lat : sq : geometry : flat
+lat : sq : n_layers_x : 11
+lat : sq : n_layers_y : 11
+lat : sq : lambda : 0.16666666666666667
+lat : sq : lowerbound_x : surface
+lat : sq : upperbound_x : surface
+lat : sq : lowerbound_y : surface
+lat : sq : upperbound_y : mirror1
+lat : sq : bondlength : 3e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : 0,0;0,11
+mon : S : valence : -0.1
+mon : S : epsilon : 5
+mon : T : freedom : frozen
+mon : T : frozen_range : 1,0;11,0
+mon : T : valence : 0.05
+mon : T : epsilon : 10
+mon : U : freedom : frozen
+mon : U : frozen_range : 12,0;12,11
+mon : A : freedom : free
+mon : A : valence : -0.3
+mon : A : epsilon : 60
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - W : 0.6
+mon : A : chi - S : -0.5
+mon : A : chi - T : -0.3
+mol : pol : composition : (A)8
+mol : pol : freedom : free
+mol : pol : phibulk : 0.003
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : free
+mol : Cl : phibulk : 0.01
+mol : Na : composition : (Na)1
+mol : Na : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # charges on the 2D cylinder with an offset (Lat2DCylinder::
+    # ElectricPotential): a charged core surface at lower x
+    "2d_cyl_charged": """lat : cyl : gradients : 2
+lat : cyl : geometry : cylindrical
+lat : cyl : n_layers_x : 14
+lat : cyl : n_layers_y : 11
+lat : cyl : offset_first_layer_x : 2
+lat : cyl : lambda : 0.2
+lat : cyl : lowerbound_x : surface
+lat : cyl : upperbound_x : mirror1
+lat : cyl : lowerbound_y : mirror1
+lat : cyl : upperbound_y : mirror2
+lat : cyl : bondlength : 3e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : 0,1;0,11
+mon : S : valence : -0.1
+mon : A : freedom : free
+mon : A : valence : 0.4
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - W : 0.6
+mon : A : chi - S : -0.8
+mol : a : composition : (A)10
+mol : a : freedom : free
+mol : a : phibulk : 0.002
+mol : Na : composition : (Na)1
+mol : Na : freedom : free
+mol : Na : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # the 2D cylinder from its axis (no offset): the first interior row has
+    # no inner neighbour; a charged diblock, salt, a surface at upper y
+    "2d_cyl_charged_axis": """lat : cyl : gradients : 2
+lat : cyl : geometry : cylindrical
+lat : cyl : n_layers_x : 12
+lat : cyl : n_layers_y : 10
+lat : cyl : lambda : 0.16666666666666667
+lat : cyl : lowerbound_x : mirror1
+lat : cyl : upperbound_x : mirror1
+lat : cyl : lowerbound_y : mirror1
+lat : cyl : upperbound_y : surface
+lat : cyl : bondlength : 4e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : 1,11;12,11
+mon : S : valence : 0.1
+mon : S : epsilon : 8
+mon : A : freedom : free
+mon : A : valence : -0.3
+mon : B : freedom : free
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - B : 0.3
+mon : A : chi - W : 1.2
+mon : B : chi - S : -0.6
+mol : AB : composition : (A)6(B)5
+mol : AB : freedom : free
+mol : AB : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : free
+mol : Cl : phibulk : 0.01
+mol : Na : composition : (Na)1
+mol : Na : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # charges on the 3D lattice (Lat3D::ElectricPotential): a charged
+    # colloid inside a mirror / periodic box
+    "3d_charged_colloid": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : n_layers_x : 8
+lat : box : n_layers_y : 7
+lat : box : n_layers_z : 6
+lat : box : lowerbound_x : mirror1
+lat : box : upperbound_x : mirror2
+lat : box : lowerbound_y : mirror2
+lat : box : upperbound_y : mirror1
+lat : box : lowerbound_z : periodic
+lat : box : upperbound_z : periodic
+lat : box : bondlength : 3e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : 1,1,2;2,2,4
+mon : S : valence : -0.3
+mon : S : epsilon : 5
+mon : A : freedom : free
+mon : A : valence : 0.2
+mon : B : freedom : free
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - S : -1.5
+mon : A : chi - W : 0.7
+mon : B : chi - W : 0.2
+mol : AB : composition : (A)5(B)4
+mol : AB : freedom : free
+mol : AB : phibulk : 0.02
+mol : Na : composition : (Na)1
+mol : Na : freedom : free
+mol : Na : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
 }
 
 # An asymmetric dendrimer whose generations' second fragments differ: SFbox's
