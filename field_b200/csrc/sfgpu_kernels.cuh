@@ -8,6 +8,17 @@
 
 namespace sfk {
 
+// Programmatic dependent launch (PTX griddepcontrol, sm_90+): a step launched
+// with programmatic stream serialization may be scheduled while the step
+// before it drains; it waits here for that step's completion and memory
+// before touching global memory, then lets the next step be scheduled.  In
+// a launch without the attribute both are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+
 constexpr int kBlock = 256;
 
 struct MolScal {            // per-molecule device scalars
@@ -55,6 +66,7 @@ static __global__ void step1(DLat L, const double *__restrict__ gin, const doubl
 static __global__ void step1_rows(DLat L, const double *__restrict__ gin, const double *__restrict__ G,
                                   double *__restrict__ gout, const double *__restrict__ other,
                                   double *__restrict__ phi, int mode) {
+    pdl_enter();
     const int worker = blockIdx.x * blockDim.x + threadIdx.x;
     if (mode == COMP_ACC) {
         for_interior4_acc(L, worker, gridDim.x * blockDim.x, phi, other,
@@ -89,6 +101,7 @@ step3d_march(DLat L, const double *__restrict__ gin, const double *__restrict__ 
              double *__restrict__ gout, const double *__restrict__ other, double *__restrict__ phi,
              int mode, int xc) {
     __shared__ double tile[kTY + 2][kTZ + 2];
+    pdl_enter();
     const int nx = L.Md[0] - 2, ny = L.Md[1] - 2, nz = L.Md[2] - 2;
     const int jx = L.st[0], jy = L.st[1];
     const int tz = threadIdx.x % kTZ, ty = threadIdx.x / kTZ;
@@ -164,6 +177,7 @@ step3d_march_pf(DLat L, const double *__restrict__ gin, const double *__restrict
                 double *__restrict__ gout, const double *__restrict__ other, double *__restrict__ phi,
                 int mode, int xc) {
     __shared__ double tile[2][kTY + 2][kTZ + 2];
+    pdl_enter();
     const int nx = L.Md[0] - 2, ny = L.Md[1] - 2, nz = L.Md[2] - 2;
     const int jx = L.st[0], jy = L.st[1];
     const int tz = threadIdx.x % kTZ, ty = threadIdx.x / kTZ;
@@ -234,6 +248,104 @@ step3d_march_pf(DLat L, const double *__restrict__ gin, const double *__restrict
         }
         vprev = vcur; vcur = vnext; vnext = vn2;
         g = gn; hzl = nzl; hzh = nzh; hyl = nyl; hyh = nyh; ot = otn; ph = phn;
+        b ^= 1;
+    }
+}
+
+// The composition-free (forward) step of step3d_march_pf with two y rows
+// per thread: a block owns a 32 (z) x 16 (y) tile, thread (tz, ty) the
+// columns y and y + 8, so every thread keeps two columns' loads of plane x+1
+// in flight (the forward step moves half the bytes of a composing one, and
+// one column per thread leaves its reads latency-bound).  Same operands and
+// operation order, bit-identical results.
+constexpr int kTY2 = 2 * kTY;
+static __global__ void __launch_bounds__(kTZ * kTY, 3)
+step3d_march_pf2(DLat L, const double *__restrict__ gin, const double *__restrict__ G, double *__restrict__ gout,
+                 int xc) {
+    __shared__ double tile[2][kTY2 + 2][kTZ + 2];
+    pdl_enter();
+    const int nx = L.Md[0] - 2, ny = L.Md[1] - 2, nz = L.Md[2] - 2;
+    const int jx = L.st[0], jy = L.st[1];
+    const int tz = threadIdx.x % kTZ, ty = threadIdx.x / kTZ;
+    const int z = blockIdx.x * kTZ + tz + 1;
+    const int x0 = blockIdx.z * xc + 1;
+    if (x0 > nx) return;
+    const int x1 = min(x0 + xc - 1, nx);
+    const int zm = lat_mapc(L, 2, z - 1), zp = lat_mapc(L, 2, z + 1);
+    const bool hz0 = (tz == 0), hz1 = (tz == kTZ - 1) || (z == nz);
+    int yr[2], ymr[2], ypr[2], colr[2];
+    bool act[2], hy0[2], hy1[2];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        yr[r] = blockIdx.y * kTY2 + ty + kTY * r + 1;
+        act[r] = (z <= nz) && (yr[r] <= ny);
+        ymr[r] = lat_mapc(L, 1, yr[r] - 1);
+        ypr[r] = lat_mapc(L, 1, yr[r] + 1);
+        colr[r] = yr[r] * jy + z;
+        hy0[r] = (r == 0) && (ty == 0);
+        hy1[r] = (r == 1 && ty == kTY - 1) || (yr[r] == ny);
+    }
+    double vprev[2], vcur[2], vnext[2], g[2], hzl[2], hzh[2], hyl[2], hyh[2];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        vprev[r] = vcur[r] = vnext[r] = g[r] = hzl[r] = hzh[r] = hyl[r] = hyh[r] = 0;
+        if (act[r]) {
+            const int base = x0 * jx;
+            vprev[r] = gin[lat_mapc(L, 0, x0 - 1) * jx + colr[r]];
+            vcur[r] = gin[base + colr[r]];
+            vnext[r] = gin[lat_mapc(L, 0, x0 + 1) * jx + colr[r]];
+            g[r] = G[base + colr[r]];
+            if (hz0) hzl[r] = gin[base + yr[r] * jy + zm];
+            if (hz1) hzh[r] = gin[base + yr[r] * jy + zp];
+            if (hy0[r]) hyl[r] = gin[base + ymr[r] * jy + z];
+            if (hy1[r]) hyh[r] = gin[base + ypr[r] * jy + z];
+        }
+    }
+    int b = 0;
+    for (int x = x0; x <= x1; x++) {
+        double vn2[2], gn[2], nzl[2], nzh[2], nyl[2], nyh[2];
+        const bool more = x < x1;
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            vn2[r] = gn[r] = nzl[r] = nzh[r] = nyl[r] = nyh[r] = 0;
+            if (act[r] && more) {
+                const int nb = (x + 1) * jx;
+                vn2[r] = gin[lat_mapc(L, 0, x + 2) * jx + colr[r]];
+                gn[r] = G[nb + colr[r]];
+                if (hz0) nzl[r] = gin[nb + yr[r] * jy + zm];
+                if (hz1) nzh[r] = gin[nb + yr[r] * jy + zp];
+                if (hy0[r]) nyl[r] = gin[nb + ymr[r] * jy + z];
+                if (hy1[r]) nyh[r] = gin[nb + ypr[r] * jy + z];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            if (!act[r]) continue;
+            const int tr = ty + kTY * r + 1;
+            tile[b][tr][tz + 1] = vcur[r];
+            if (hz0) tile[b][tr][0] = hzl[r];
+            if (hz1) tile[b][tr][tz + 2] = hzh[r];
+            if (hy0[r]) tile[b][0][tz + 1] = hyl[r];
+            if (hy1[r]) tile[b][tr + 1][tz + 1] = hyh[r];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            if (!act[r]) continue;
+            const int tr = ty + kTY * r + 1;
+            double acc = vprev[r] * g[r];
+            acc += vnext[r] * g[r];
+            acc += tile[b][tr - 1][tz + 1] * g[r];
+            acc += tile[b][tr + 1][tz + 1] * g[r];
+            acc += tile[b][tr][tz] * g[r];
+            acc += tile[b][tr][tz + 2] * g[r];
+            gout[x * jx + colr[r]] = acc * (1.0 / 6.0);
+        }
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            vprev[r] = vcur[r]; vcur[r] = vnext[r]; vnext[r] = vn2[r];
+            g[r] = gn[r]; hzl[r] = nzl[r]; hzh[r] = nzh[r]; hyl[r] = nyl[r]; hyh[r] = nyh[r];
+        }
         b ^= 1;
     }
 }

@@ -44,8 +44,26 @@ static int grid_rows(const DLat &L) {
     return (int)std::max(1L, std::min(b, 148L * 32));
 }
 
+// a step launch with programmatic stream serialization: the kernel may be
+// scheduled while the previous one drains and waits for it in pdl_enter()
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // first-order step inside a residual evaluation: x-marching tiles on the
-// six-neighbour 3D lattices, row-wise otherwise
+// six-neighbour 3D lattices (launched as programmatic dependents of the
+// step before), row-wise otherwise
 int sfgpu_system::launch_step1(const double *gin, const double *G, double *gout, const double *other, double *phi,
                                int mode) {
     const DLat &L = H.L;
@@ -53,14 +71,23 @@ int sfgpu_system::launch_step1(const double *gin, const double *G, double *gout,
         const bool composing = mode != COMP_NONE;
         const int xc = composing ? tile_xc_bwd : tile_xc;
         dim3 grid((L.Md[2] - 2 + kTZ - 1) / kTZ, (L.Md[1] - 2 + kTY - 1) / kTY, (L.Md[0] - 2 + xc - 1) / xc);
-        if (composing && tile_pipelined_bwd)
-            step3d_march_pf<true><<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, xc);
-        else if (!composing && tile_pipelined)
-            step3d_march_pf<false><<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, xc);
-        else
-            step3d_march<<<grid, kTZ * kTY, 0, stream>>>(L, gin, G, gout, other, phi, mode, xc);
+        const dim3 block(kTZ * kTY);
+        cudaError_t e;
+        if (!composing && tile_pipelined == 2) {
+            grid.y = (L.Md[1] - 2 + kTY2 - 1) / kTY2;
+            e = launch_pdl(step3d_march_pf2, grid, block, stream, L, gin, G, gout, xc);
+        } else if (composing && tile_pipelined_bwd) {
+            e = launch_pdl(step3d_march_pf<true>, grid, block, stream, L, gin, G, gout, other, phi, mode, xc);
+        } else if (!composing && tile_pipelined) {
+            e = launch_pdl(step3d_march_pf<false>, grid, block, stream, L, gin, G, gout, other, phi, mode, xc);
+        } else {
+            e = launch_pdl(step3d_march, grid, block, stream, L, gin, G, gout, other, phi, mode, xc);
+        }
+        if (e != cudaSuccess) { sfgpu_set_error(e, "cudaLaunchKernelEx", __FILE__, __LINE__); return SFGPU_ERR_CUDA; }
     } else {
-        step1_rows<<<grid_rows(L), kBlock, 0, stream>>>(L, gin, G, gout, other, phi, mode);
+        const cudaError_t e = launch_pdl(step1_rows, dim3(grid_rows(L)), dim3(kBlock), stream, L, gin, G, gout, other, phi,
+                                         mode);
+        if (e != cudaSuccess) { sfgpu_set_error(e, "cudaLaunchKernelEx", __FILE__, __LINE__); return SFGPU_ERR_CUDA; }
     }
     return SFGPU_OK;
 }
@@ -1797,18 +1824,21 @@ extern "C" int sfgpu_system_autotune(sfgpu_system *s, int reps, int *chosen_xc, 
     }
     // forward and backward steps are timed by the same profile call; each
     // keeps its own fastest (depth, form)
+    // forms: 0 plain, 1 pipelined, 2 (forward only) pipelined with two y rows
+    // per thread
     const int cand[] = {2, 4, 8, 16, 32};
     double bf = 1e30, bb = 1e30;
     int fx = s->tile_xc, fp = s->tile_pipelined, bx = s->tile_xc_bwd, bp = s->tile_pipelined_bwd;
-    for (int pl = 0; pl < 2; pl++)
+    for (int pl = 0; pl < 3; pl++)
         for (int c : cand) {
             s->tile_xc = s->tile_xc_bwd = c;
-            s->tile_pipelined = s->tile_pipelined_bwd = pl;
+            s->tile_pipelined = pl;
+            s->tile_pipelined_bwd = pl != 0;
             double f = 0, b = 0;
             int rc = sfgpu_profile_propagator(s, reps, &f, &b, nullptr, nullptr);
             if (rc) return rc;
             if (f < bf) { bf = f; fx = c; fp = pl; }
-            if (b < bb) { bb = b; bx = c; bp = pl; }
+            if (pl < 2 && b < bb) { bb = b; bx = c; bp = pl; }
         }
     s->tile_xc = fx; s->tile_pipelined = fp;
     s->tile_xc_bwd = bx; s->tile_pipelined_bwd = bp;
@@ -1819,7 +1849,9 @@ extern "C" int sfgpu_system_autotune(sfgpu_system *s, int reps, int *chosen_xc, 
 
 extern "C" int sfgpu_system_set_tile_pipelined(sfgpu_system *s, int enable) {
     CHECK_SYS(s);
-    s->tile_pipelined = s->tile_pipelined_bwd = enable != 0;
+    if (enable < 0 || enable > 2) return fail(SFGPU_ERR_INVALID, "the step form is 0, 1 or 2");
+    s->tile_pipelined = enable;
+    s->tile_pipelined_bwd = enable != 0;
     return SFGPU_OK;
 }
 

@@ -26,7 +26,7 @@ def main():
     ap.add_argument("--reps", type=int, default=50)
     ap.add_argument("--n", type=int, default=0, help="lattice size override")
     ap.add_argument("--tile", type=int, default=0, help="3D x-chunk depth (0: autotune)")
-    ap.add_argument("--form", default="pipelined", choices=["pipelined", "plain"],
+    ap.add_argument("--form", default="pipelined", choices=["pipelined", "plain", "pipelined2"],
                     help="3D first-order step form when --tile is given")
     a = ap.parse_args()
     if a.case == "c2":
@@ -40,7 +40,7 @@ def main():
     tune = None
     if a.tile:
         s.set_tile(a.tile)
-        s.set_tile_pipelined(a.form == "pipelined")
+        s.set_tile_pipelined({"plain": 0, "pipelined": 1, "pipelined2": 2}[a.form])
     else:
         tune = s.autotune(reps=max(5, a.reps // 5))
     p = s.profile_propagator(reps=a.reps)

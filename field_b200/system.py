@@ -268,8 +268,10 @@ class System:
         nat.check(self.lib.sfgpu_system_autotune(self.h, reps, C.byref(x), C.byref(ms)), "sfgpu_system_autotune")
         return {"tile_xc": x.value, "ms_fwd_plus_bwd": ms.value}
 
-    def set_tile_pipelined(self, enable: bool):
-        nat.check(self.lib.sfgpu_system_set_tile_pipelined(self.h, int(bool(enable))), "set_tile_pipelined")
+    def set_tile_pipelined(self, enable):
+        """Form of the 3D first-order step: False/0 plain, True/1 pipelined,
+        2 pipelined with two y rows per thread in the forward steps."""
+        nat.check(self.lib.sfgpu_system_set_tile_pipelined(self.h, int(enable)), "set_tile_pipelined")
 
     def set_tile(self, xc: int):
         nat.check(self.lib.sfgpu_system_set_tile(self.h, xc), "sfgpu_system_set_tile")

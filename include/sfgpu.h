@@ -441,10 +441,11 @@ int sfgpu_profile_propagator(sfgpu_system *sys, int reps, double *ms_fwd, double
 int sfgpu_system_set_tile(sfgpu_system *sys, int xc);
 /* 1: the 3D first-order step runs software-pipelined (plane x+1's loads in
  * flight while plane x is computed, double-buffered tile); 0: the plain
- * x-marching form.  Results are bit-identical.  By default the composing
- * backward steps run pipelined (x depth 8) and the forward steps plain (depth
- * 4); the autotuner times both forms and depths for each kind of step.
- * sfgpu_system_set_tile and this call set both kinds. */
+ * x-marching form; 2: pipelined, the forward (composition-free) steps with
+ * two y rows of columns per thread.  Results are bit-identical.  By default
+ * the composing backward steps run pipelined (x depth 8) and the forward
+ * steps plain (depth 4); the autotuner times the forms and depths for each
+ * kind of step.  sfgpu_system_set_tile and this call set both kinds. */
 int sfgpu_system_set_tile_pipelined(sfgpu_system *sys, int enable);
 int sfgpu_system_autotune(sfgpu_system *sys, int reps, int *chosen_xc, double *best_ms);
 

@@ -121,26 +121,30 @@ def test_c5_adjoint_gradient_against_differences_96(gpu_lib):
 
 
 @pytest.mark.parametrize("xc", [1, 3, 8, 32])
-def test_pipelined_3d_step_bit_identical(gpu_lib, xc):
-    """The software-pipelined 3D first-order step gives the plain x-marching
-    step's results bit for bit, for chunk depths that do and do not divide
-    the lattice (composition-free forward steps and composing backward steps
-    both run inside a residual)."""
+@pytest.mark.parametrize("form", [1, 2])
+def test_pipelined_3d_step_bit_identical(gpu_lib, xc, form):
+    """The software-pipelined 3D first-order step (form 1; form 2 with two y
+    rows per thread in the forward steps) gives the plain x-marching step's
+    results bit for bit, for chunk depths that do and do not divide the
+    lattice and y extents that do and do not fill the last tile
+    (composition-free forward steps and composing backward steps both run
+    inside a residual)."""
     for case in ("3d_periodic_melt", "3d_mirror_mix", "3d_2nd_brush"):
         spec = CASES[case]()
         x = random_x(spec, seed=9, scale=0.2)
         a, b = System(spec), System(spec)
         a.set_tile(xc)
         b.set_tile(xc)
-        a.set_tile_pipelined(True)
-        b.set_tile_pipelined(False)
+        a.set_tile_pipelined(form)
+        b.set_tile_pipelined(0)
         assert np.array_equal(a.residual(x), b.residual(x)), case
         for i in range(len(spec.segments)):
             assert np.array_equal(a.phi(i), b.phi(i)), (case, i)
-    spec, x0 = configs.melt3d(n=40, nA=10, nB=10)
-    a, b = System(spec), System(spec)
-    a.set_tile(xc)
-    b.set_tile(xc)
-    a.set_tile_pipelined(True)
-    b.set_tile_pipelined(False)
-    assert np.array_equal(a.residual(x0), b.residual(x0))
+    for n in (40, 21):
+        spec, x0 = configs.melt3d(n=n, nA=10, nB=10)
+        a, b = System(spec), System(spec)
+        a.set_tile(xc)
+        b.set_tile(xc)
+        a.set_tile_pipelined(form)
+        b.set_tile_pipelined(0)
+        assert np.array_equal(a.residual(x0), b.residual(x0)), n
