@@ -425,9 +425,11 @@ __device__ __forceinline__ bool is_mirror(int bc) {
 // (:250-344, :765-850), whose forward -y component reads +z twice and -y
 // never (Lat3D2ndO.cpp:308-313).
 enum { STEP2_PLAIN = 0, STEP2_STIFF = 1, STEP2_ISO = 2 };
-static __global__ void step2_rows(DLat L, const double *__restrict__ gin, const double *__restrict__ G, double S,
-                                  double *__restrict__ gout, const double *__restrict__ other,
-                                  double *__restrict__ phi, int mode, int backward, int wmode = STEP2_PLAIN) {
+static __global__ void __launch_bounds__(kBlock, 4)
+step2_rows(DLat L, const double *__restrict__ gin, const double *__restrict__ G, double S,
+           double *__restrict__ gout, const double *__restrict__ other,
+           double *__restrict__ phi, int mode, int backward, int wmode = STEP2_PLAIN) {
+    pdl_enter();
     const int M = L.M;
     const double Lw = (1.0 - S) / 4.0;
     const int nx = L.Md[0] - 2, ny = L.Md[1] - 2;

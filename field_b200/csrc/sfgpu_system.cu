@@ -1080,11 +1080,13 @@ int sfgpu_system::molecule_phi(int m) {
             // step s (1-based) takes Pf(s-1, s+1); the last one is isotropic
             const bool last = (t == N - 1);
             const double Sv = last ? 0.2 : pf[o.seg[t - 1] * nseg + o.seg[t + 1]];
-            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], Sv, out, nullptr, nullptr, COMP_NONE, 0,
-                                       last ? STEP2_ISO : STEP2_STIFF);
+            launch_pdl(step2_rows, dim3(grid_rows(L)), dim3(kBlock), s, L, in, (const double *)d_gseg[sg], Sv, out,
+                       (const double *)nullptr, (double *)nullptr, (int)COMP_NONE, 0,
+                       (int)(last ? STEP2_ISO : STEP2_STIFF));
         } else if (K == 6)
-            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], out, nullptr,
-                                       nullptr, COMP_NONE, 0);
+            launch_pdl(step2_rows, dim3(grid_rows(L)), dim3(kBlock), s, L, in, (const double *)d_gseg[sg],
+                       pf[o.seg[t - 1] * nseg + sg], out, (const double *)nullptr, (double *)nullptr, (int)COMP_NONE, 0,
+                       (int)STEP2_PLAIN);
         else
             step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], out,
                                         nullptr, nullptr, COMP_NONE, 0);
@@ -1102,11 +1104,11 @@ int sfgpu_system::molecule_phi(int m) {
             // (s = N-1) is isotropic (SF_Copol2ndO_stiff_range.cpp:229-234)
             const bool first = (t == N - 2);
             const double Sv = first ? 0.2 : pf[sg * nseg + o.seg[t + 2]];
-            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], Sv, out, gf, o.d_phi[sg], COMP_ACC, 1,
-                                       first ? STEP2_ISO : STEP2_STIFF);
+            launch_pdl(step2_rows, dim3(grid_rows(L)), dim3(kBlock), s, L, in, (const double *)d_gseg[sg], Sv, out, gf,
+                       o.d_phi[sg], (int)COMP_ACC, 1, (int)(first ? STEP2_ISO : STEP2_STIFF));
         } else if (K == 6)
-            step2_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], out, gf,
-                                       o.d_phi[sg], COMP_ACC, 1);
+            launch_pdl(step2_rows, dim3(grid_rows(L)), dim3(kBlock), s, L, in, (const double *)d_gseg[sg],
+                       pf[sg * nseg + o.seg[t + 1]], out, gf, o.d_phi[sg], (int)COMP_ACC, 1, (int)STEP2_PLAIN);
         else
             step2l_rows<<<grid_rows(L), kBlock, 0, s>>>(L, in, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], out, gf,
                                         o.d_phi[sg], COMP_ACC, 1);
@@ -1785,7 +1787,9 @@ extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fw
         if (K == 1)
             s->launch_step1(s->d_gi + (t - 1) * KM, G, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE);
         else
-            step2_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, s->d_gi + (t - 1) * KM, G, 0.2, s->d_gi + t * KM, nullptr, nullptr, COMP_NONE, 0);
+            launch_pdl(step2_rows, dim3(grid_rows(s->H.L)), dim3(kBlock), s->stream, s->H.L,
+                       (const double *)(s->d_gi + (t - 1) * KM), G, 0.2, s->d_gi + t * KM, (const double *)nullptr,
+                       (double *)nullptr, (int)COMP_NONE, 0, (int)STEP2_PLAIN);
     }
     SFGPU_CUDA_TRY(cudaEventRecord(e1, s->stream));
     for (int r = 0; r < reps; r++) {
@@ -1795,7 +1799,8 @@ extern "C" int sfgpu_profile_propagator(sfgpu_system *s, int reps, double *ms_fw
         if (K == 1)
             s->launch_step1(src, G, dst, s->d_gi + t * KM, phi, COMP_ACC);
         else
-            step2_rows<<<grid_rows(s->H.L), kBlock, 0, s->stream>>>(s->H.L, src, G, 0.2, dst, s->d_gi + t * KM, phi, COMP_ACC, 1);
+            launch_pdl(step2_rows, dim3(grid_rows(s->H.L)), dim3(kBlock), s->stream, s->H.L, src, G, 0.2, dst,
+                       (const double *)(s->d_gi + t * KM), phi, (int)COMP_ACC, 1, (int)STEP2_PLAIN);
     }
     SFGPU_CUDA_TRY(cudaEventRecord(e2, s->stream));
     SFGPU_CUDA_TRY(cudaEventSynchronize(e2));
