@@ -181,9 +181,30 @@ int sfgpu_system::ensure_adjoint() {
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
         if (o.dend) return fail_unsupported("derivatives of dendrimers");
-        else if (o.tree || o.ring) return fail_unsupported("derivatives of branched molecules and rings");
+        else if (o.tree) return fail_unsupported("the reverse mode of branched molecules");
     int rc = ensure_adjoint_misc();
     if (rc) return rc;
+    // rings: one set of walk levels per block of ring_phi_adj
+    size_t ring_need = 0;
+    for (auto &o : mols) {
+        if (!o.ring) continue;
+        const int Mmax = (o.N / 2 > M) ? 2 * M : M + o.N / 2;
+        if ((size_t)3 * (Mmax + 1) * sizeof(double) > 200 * 1024)
+            return fail_unsupported("the reverse mode of a ring walk larger than shared memory");
+        ring_need = std::max(ring_need, (size_t)std::min(M, kRingAdjBlocks) * (o.N / 2) * (Mmax + 1));
+    }
+    if (ring_need > a_ring_doubles) {
+        if (a_ring) cudaFree(a_ring);
+        a_ring = nullptr;
+        a_ring_doubles = 0;
+        cudaError_t e = cudaMalloc((void **)&a_ring, sizeof(double) * ring_need);
+        if (e != cudaSuccess) {
+            a_ring = nullptr;
+            sfgpu_set_error(e, "cudaMalloc (ring walk levels)", __FILE__, __LINE__);
+            return SFGPU_ERR_NOMEM;
+        }
+        a_ring_doubles = ring_need;
+    }
     if (!a_store) {
         int nmax = 1;
         for (auto &o : mols) if (o.type != 0) nmax = std::max(nmax, o.N);
@@ -372,6 +393,7 @@ int sfgpu_system::molecule_phi_store(int m) {
     p.pinned = o.pinned; p.solvent = (m == solvent); p.nmol = nmol;
     p.phibulk_in = o.phibulk; p.theta = o.theta;
     MolScal *scal = (MolScal *)d_scal;
+    if (o.ring) return molecule_phi_ring(m);
     if (o.type == 0) {
         int i = o.seg[0];
         MolParam p1 = p;
@@ -406,6 +428,17 @@ int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
     p.phibulk_in = o.phibulk; p.theta = o.theta;
     MolScal *scal = (MolScal *)d_scal;
     AdjScal *as = (AdjScal *)a_scal;
+    if (o.ring) {
+        const int Mmax = (o.N / 2 > M) ? 2 * M : M + o.N / 2;
+        const size_t shm = (size_t)3 * (Mmax + 1) * sizeof(double);
+        if (shm > 48 * 1024)
+            SFGPU_CUDA_TRY(cudaFuncSetAttribute(ring_phi_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        const int sg = o.seg[0];
+        ring_phi_adj<<<std::min(M, kRingAdjBlocks), Mmax + 1 >= 256 ? 256 : 64, shm, s>>>(
+            L, M, o.N, Mmax, d_gseg[sg], phibar_src[sg], o.phibulk, o.ring_norm0, a_ring, a_gbar[sg]);
+        SFGPU_CUDA_TRY(cudaGetLastError());
+        return SFGPU_OK;
+    }
     // C-bar: sum over the molecule's segments of phibar . phi
     const int np = nblocks_red;
     for (size_t a = 0; a < o.used.size(); a++) {
@@ -540,14 +573,14 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
     // molecules in reverse order of the primal (the solvent first).  The
     // chain storage holds one molecule: the last polymer the primal
     // propagated keeps its chains, every other polymer is propagated again.
-    int held = (mols[solvent].type != 0) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring) held = m;
     if ((rc = molecule_adjoint(solvent, a_phibar.data()))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }
@@ -610,14 +643,14 @@ int sfgpu_system::free_energy_grad(const double *x, double *F, double *xbar) {
                                                o.chemintref, scal, m, a_phibar_m[i]);
         return molecule_adjoint(m, a_phibar_m.data());
     };
-    int held = (mols[solvent].type != 0) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring) held = m;
     if ((rc = mol_adj(solvent))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }
@@ -651,14 +684,14 @@ int sfgpu_system::phi_vjp_async(const double *x, const double *const *omega, dou
         SFGPU_CUDA_TRY(cudaMemsetAsync(a_gbar[i], 0, sizeof(double) * M, s));
     }
     fe_zero_scal<<<1, 1, 0, s>>>(nmol, (AdjScal *)a_scal);
-    int held = (mols[solvent].type != 0) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring) held = m;
     if ((rc = molecule_adjoint(solvent, a_phibar.data()))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }

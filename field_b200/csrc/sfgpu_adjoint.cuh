@@ -572,4 +572,105 @@ static __global__ void fe_gbar(int M, const double *__restrict__ q, const double
     }
 }
 
+// Reverse sweep of the ring's return walk (ring_phi, SF_HomoRing1stO.cpp:
+// 110-160): for every interior site k the walk is run forward again with its
+// levels Y_0 .. Y_{N/2-1} kept in `levels` (Mmax + 1 values each, one set per
+// block), then walked back with the cotangent Ybar, from
+// Ybar = 2 Y phibar(k) phib / norm0 (phi(k) = phib sum_z Y(z)^2 / norm0).  A
+// step maps Y to Y'(z) = g_z (Y(z-1) + 4 Y(z) + Y(z+1)) on the window
+// zmin <= z < zmax (g_z = G(z-1) / 6 up to M, 1/6 beyond), copies Y(Mmax-1)
+// into Y(Mmax) before it, and keeps Y elsewhere; its transpose gathers, for
+// every j, the window's three terms, the untouched value, and at Mmax - 1
+// the copy.  G's cotangent collects Ybar'(z) (Y(z-1) + 4 Y(z) + Y(z+1)) / 6
+// per step and Ybar_0(k) at the start in shared memory, then goes to Gbar
+// with one atomic add per site; a boundary layer's share goes to the site it
+// copies (a surface layer's G is a constant).  The ring's scalars (lnGN 0,
+// its phibulk the input's) carry no cotangent.  Boundary sites' profiles
+// are copies whose cotangents arrive folded into their mapped sites.
+constexpr int kRingAdjBlocks = 148 * 4;   // blocks of ring_phi_adj (each keeps one set of levels)
+static __global__ void ring_phi_adj(DLat L, int M, int N, int Mmax, const double *__restrict__ G,
+                                    const double *__restrict__ phibar, double phibulk, double norm0,
+                                    double *__restrict__ levels, double *__restrict__ gbar) {
+    extern __shared__ double ring_a_sh[];
+    double *Yb = ring_a_sh, *Ybn = Yb + (Mmax + 1), *gacc = Ybn + (Mmax + 1);
+    const int W = Mmax + 1, nlev = N / 2;
+    double *lev = levels + (size_t)blockIdx.x * nlev * W;
+    for (int k = blockIdx.x + 1; k <= M; k += gridDim.x) {
+        int ck[3];
+        lat_coords(L, k - 1, ck);
+        if (!lat_interior(L, ck)) continue;   // block-uniform
+        const double pb = phibar[k - 1];
+        if (pb == 0.0) continue;               // block-uniform
+        // forward walk, every level kept
+        for (int z = threadIdx.x; z <= Mmax; z += blockDim.x) {
+            lev[z] = (z == k) ? G[k - 1] : 0.0;
+            gacc[z] = 0.0;
+        }
+        __syncthreads();
+        for (int st = 1; st < nlev; st++) {
+            const double *Y = lev + (size_t)(st - 1) * W;
+            double *Yn = lev + (size_t)st * W;
+            const int zmin = max(k - st, 1), zmax = min(k + st, Mmax);
+            const double ytop = Y[Mmax - 1];
+            for (int z = threadIdx.x; z <= Mmax; z += blockDim.x) {
+                double v = (z == Mmax) ? ytop : Y[z];
+                if (z >= zmin && z < zmax) {
+                    const double a = Y[z - 1], b = Y[z], c = (z + 1 == Mmax) ? ytop : Y[z + 1];
+                    const double gz = (z <= M) ? G[z - 1] / 6.0 : 1.0 / 6.0;
+                    v = gz * (a + 4 * b + c);
+                }
+                Yn[z] = v;
+            }
+            __syncthreads();
+        }
+        // cotangent of the last level
+        const double *Yl = lev + (size_t)(nlev - 1) * W;
+        const double sc = 2.0 * pb * phibulk / norm0;
+        for (int z = threadIdx.x; z <= Mmax; z += blockDim.x) Yb[z] = (z >= 1) ? sc * Yl[z] : 0.0;
+        __syncthreads();
+        for (int st = nlev - 1; st >= 1; st--) {
+            const double *Y = lev + (size_t)(st - 1) * W;   // the step's input
+            const int zmin = max(k - st, 1), zmax = min(k + st, Mmax);
+            const double ytop = Y[Mmax - 1];
+            auto in_win = [&](int z) { return z >= zmin && z < zmax; };
+            auto gz = [&](int z) { return (z <= M) ? G[z - 1] / 6.0 : 1.0 / 6.0; };
+            for (int j = threadIdx.x; j <= Mmax; j += blockDim.x) {
+                double v = 0.0;
+                if (j >= 1 && j < Mmax) {
+                    if (!in_win(j)) v += Yb[j];
+                    if (in_win(j + 1)) v += gz(j + 1) * Yb[j + 1];
+                    if (in_win(j)) v += 4.0 * gz(j) * Yb[j];
+                    if (j - 1 >= 1 && in_win(j - 1)) v += gz(j - 1) * Yb[j - 1];
+                    if (j == Mmax - 1) {
+                        v += Yb[Mmax];
+                        if (in_win(Mmax - 1)) v += gz(Mmax - 1) * Yb[Mmax - 1];
+                    }
+                }
+                Ybn[j] = v;
+                if (in_win(j) && j <= M) {
+                    const double a = Y[j - 1], b = Y[j], c = (j + 1 == Mmax) ? ytop : Y[j + 1];
+                    gacc[j] += Yb[j] * ((a + 4 * b + c) / 6.0);
+                }
+            }
+            __syncthreads();
+            double *t = Yb; Yb = Ybn; Ybn = t;
+        }
+        if (threadIdx.x == 0) gacc[k] += Yb[k];   // Y_0(k) = G(k - 1)
+        __syncthreads();
+        for (int z = threadIdx.x + 1; z <= M; z += blockDim.x) {
+            const double v = gacc[z];
+            if (v == 0.0) continue;
+            int c[3];
+            lat_coords(L, z - 1, c);
+            int t = z - 1;
+            if (!lat_interior(L, c)) {
+                t = lat_map(L, z - 1);
+                if (t == z - 1) continue;      // surface layer: G there is a constant
+            }
+            atomicAdd(gbar + t, v);
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace sfa

@@ -93,6 +93,8 @@ struct sfgpu_system {
     int a_stride = 0;
     bool a_misc = false;
     double *a_store = nullptr;
+    double *a_ring = nullptr;               // ring walk levels of the reverse sweep (ring_phi_adj)
+    size_t a_ring_doubles = 0;
     double *a_ckF = nullptr, *a_ckB = nullptr, *a_bufF = nullptr, *a_bufB = nullptr;
     int a_qseg = -1;                        // segment held in a_bufF / a_bufB
     std::vector<double *> a_phibar, a_gbar, a_phibar_raw;
