@@ -181,9 +181,29 @@ int sfgpu_system::ensure_adjoint() {
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
         if (o.dend) return fail_unsupported("derivatives of dendrimers");
-        else if (o.tree) return fail_unsupported("the reverse mode of branched molecules");
     int rc = ensure_adjoint_misc();
     if (rc) return rc;
+    // branched molecules: the cotangents of every U, Q, D slice and a pool
+    // for the products a node's combinations pass through
+    size_t tree_need = 0;
+    for (auto &o : mols) {
+        if (!o.tree) continue;
+        size_t kmax = 1;
+        for (auto &k : o.kids) kmax = std::max(kmax, k.size());
+        tree_need = std::max(tree_need, (3 * (size_t)o.N + kmax + 3) * M);
+    }
+    if (tree_need > a_tree_doubles) {
+        if (a_tree) cudaFree(a_tree);
+        a_tree = nullptr;
+        a_tree_doubles = 0;
+        cudaError_t e = cudaMalloc((void **)&a_tree, sizeof(double) * tree_need);
+        if (e != cudaSuccess) {
+            a_tree = nullptr;
+            sfgpu_set_error(e, "cudaMalloc (bond-tree cotangents)", __FILE__, __LINE__);
+            return SFGPU_ERR_NOMEM;
+        }
+        a_tree_doubles = tree_need;
+    }
     // rings: one set of walk levels per block of ring_phi_adj
     size_t ring_need = 0;
     for (auto &o : mols) {
@@ -394,6 +414,7 @@ int sfgpu_system::molecule_phi_store(int m) {
     p.phibulk_in = o.phibulk; p.theta = o.theta;
     MolScal *scal = (MolScal *)d_scal;
     if (o.ring) return molecule_phi_ring(m);
+    if (o.tree) return molecule_phi_tree(m);
     if (o.type == 0) {
         int i = o.seg[0];
         MolParam p1 = p;
@@ -455,6 +476,7 @@ int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
         adj_axpy_interior<<<g, kBlock, 0, s>>>(L, 1, d_wgn, a_qbar, 1.0, a_gbar[o.seg[0]]);
         return SFGPU_OK;
     }
+    if (o.tree) return molecule_adjoint_tree(m);
     const int N = o.N;
     double *cot = a_cot[0], *nxt = a_cot[1];
     // slices of position t: stored, or recomputed segment by segment
@@ -508,6 +530,114 @@ int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
     }
     adj_add_interior<<<g, kBlock, 0, s>>>(L, K, cot, a_gbar[o.seg[N - 1]]);
     return rcs;
+}
+
+// Reverse sweep of a branched molecule (molecule_phi_tree's bond-tree
+// recursion).  The primal's slices U(q), Q(q), D(q) are computed again into
+// the chain scratch; the cotangents Ubar, Qbar, Dbar then run back through
+// the outward pass (segments N-1 .. 0: the composition U D, every child's
+// D(c) = step(D(q) prod_{siblings} Q / G_q, G_c)) and through the inward
+// pass (segments 0 .. N-1: Q(q) = step(U(q), G_parent), U(q) = G_q at a leaf,
+// Q of its only child, or the product of its children's Q over G_q).  The
+// composition's cotangent phibar_raw and the lnGN term (qbar w into Ubar(0))
+// are set up as for linear chains; every product a node's combinations pass
+// through is formed again in a pool before it is reversed.
+int sfgpu_system::molecule_adjoint_tree(int m) {
+    HMol &o = mols[m];
+    const DLat &L = H.L;
+    const int g = grid_a(M), gr = grid_rows_a(L), N = o.N;
+    cudaStream_t s = stream;
+    const size_t bytes = sizeof(double) * M;
+    int rc = molecule_phi_tree(m);   // U, Q, D of this molecule (the profiles come out unchanged)
+    if (rc) return rc;
+    auto U = [&](int q) { return d_gi + (size_t)q * M; };
+    auto Q = [&](int q) { return d_gi + (size_t)(N + q) * M; };
+    auto D = [&](int q) { return d_gi + (size_t)(2 * N + q) * M; };
+    auto Ub = [&](int q) { return a_tree + (size_t)q * M; };
+    auto Qb = [&](int q) { return a_tree + (size_t)(N + q) * M; };
+    auto Db = [&](int q) { return a_tree + (size_t)(2 * N + q) * M; };
+    size_t kmax = 1;
+    for (auto &k : o.kids) kmax = std::max(kmax, k.size());
+    double *pool = a_tree + (size_t)3 * N * M;            // kmax slices of products
+    double *cb[2] = {pool + kmax * M, pool + (kmax + 1) * M};
+    double *accbar = pool + (kmax + 2) * M;
+    SFGPU_CUDA_TRY(cudaMemsetAsync(a_tree, 0, sizeof(double) * 3 * N * M, s));
+    AdjScal *as = (AdjScal *)a_scal;
+    adj_qbar_scale<<<1, 1, 0, s>>>(as, m, a_qbar);
+    adj_axpy_interior<<<g, kBlock, 0, s>>>(L, 1, d_wgn, a_qbar, 1.0, Ub(0));
+    // reverse a chain of combinations acc_j = acc_{j-1} b_j / Gq (j = 1..n,
+    // acc_0 = first, the products in pool[0..n-1]) from the cotangent of
+    // acc_n in cb[0]; returns the buffer with the cotangent of acc_0
+    auto reverse_products = [&](const double *first, const std::vector<const double *> &bs,
+                                const std::vector<double *> &bbars, const double *Gq, double *gbq) -> double * {
+        const int n = (int)bs.size();
+        // products again
+        const double *acc = first;
+        for (int j = 0; j < n; j++) {
+            dend_combine<<<g, kBlock, 0, s>>>(M, acc, bs[j], Gq, pool + (size_t)j * M);
+            acc = pool + (size_t)j * M;
+        }
+        int w = 0;
+        for (int j = n - 1; j >= 0; j--) {
+            const double *a = (j == 0) ? first : pool + (size_t)(j - 1) * M;
+            tree_adj_combine<<<g, kBlock, 0, s>>>(L, cb[w], a, bs[j], Gq, pool + (size_t)j * M, cb[w ^ 1], bbars[j],
+                                                  gbq);
+            w ^= 1;
+        }
+        return cb[w];
+    };
+    // outward pass reversed
+    for (int q = N - 1; q >= 0; q--) {
+        const int sq = o.seg[q];
+        const double *Gq = d_gseg[sq];
+        tree_adj_connect<<<g, kBlock, 0, s>>>(L, a_phibar_raw[sq], U(q), D(q), Ub(q), Db(q));
+        const std::vector<int> &kids = o.kids[q];
+        for (int ci = (int)kids.size() - 1; ci >= 0; ci--) {
+            const int c = kids[ci];
+            std::vector<const double *> bs;
+            std::vector<double *> bbars;
+            for (int c2 : kids) if (c2 != c) { bs.push_back(Q(c2)); bbars.push_back(Qb(c2)); }
+            // the step's input: D(q) times the siblings' Q over G_q
+            const double *in = D(q);
+            for (size_t j = 0; j < bs.size(); j++) {
+                dend_combine<<<g, kBlock, 0, s>>>(M, in, bs[j], Gq, pool + j * M);
+                in = pool + j * M;
+            }
+            SFGPU_CUDA_TRY(cudaMemsetAsync(accbar, 0, bytes, s));
+            adj_chain_step<<<gr, kBlock, 0, s>>>(L, Db(c), d_gseg[o.seg[c]], in, a_gbar[o.seg[c]], accbar);
+            if (bs.empty()) {
+                adj_add_interior<<<g, kBlock, 0, s>>>(L, 1, accbar, Db(q));
+            } else {
+                SFGPU_CUDA_TRY(cudaMemcpyAsync(cb[0], accbar, bytes, cudaMemcpyDeviceToDevice, s));
+                double *d0 = reverse_products(D(q), bs, bbars, Gq, a_gbar[sq]);
+                adj_add_interior<<<g, kBlock, 0, s>>>(L, 1, d0, Db(q));
+            }
+        }
+    }
+    adj_add_interior<<<g, kBlock, 0, s>>>(L, 1, Db(0), a_gbar[o.seg[0]]);   // D(0) = G_0
+    // inward pass reversed
+    for (int q = 0; q < N; q++) {
+        const int sq = o.seg[q];
+        if (q > 0) {
+            const int sp = o.seg[o.parent[q]];
+            adj_chain_step<<<gr, kBlock, 0, s>>>(L, Qb(q), d_gseg[sp], U(q), a_gbar[sp], Ub(q));
+        }
+        const std::vector<int> &kids = o.kids[q];
+        if (kids.empty()) {
+            adj_add_interior<<<g, kBlock, 0, s>>>(L, 1, Ub(q), a_gbar[sq]);
+        } else if (kids.size() == 1) {
+            adj_add_interior<<<g, kBlock, 0, s>>>(L, 1, Ub(q), Qb(kids[0]));
+        } else {
+            std::vector<const double *> bs;
+            std::vector<double *> bbars;
+            for (size_t j = 1; j < kids.size(); j++) { bs.push_back(Q(kids[j])); bbars.push_back(Qb(kids[j])); }
+            SFGPU_CUDA_TRY(cudaMemcpyAsync(cb[0], Ub(q), bytes, cudaMemcpyDeviceToDevice, s));
+            double *q0 = reverse_products(Q(kids[0]), bs, bbars, d_gseg[sq], a_gbar[sq]);
+            adj_add_interior<<<g, kBlock, 0, s>>>(L, 1, q0, Qb(kids[0]));
+        }
+    }
+    SFGPU_CUDA_TRY(cudaGetLastError());
+    return SFGPU_OK;
 }
 
 // primal residual evaluation that keeps what the reverse sweep reads:
@@ -573,14 +703,14 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
     // molecules in reverse order of the primal (the solvent first).  The
     // chain storage holds one molecule: the last polymer the primal
     // propagated keeps its chains, every other polymer is propagated again.
-    int held = (mols[solvent].type != 0 && !mols[solvent].ring) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0 && !mols[m].ring) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree) held = m;
     if ((rc = molecule_adjoint(solvent, a_phibar.data()))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && !mols[m].ring && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }
@@ -643,14 +773,14 @@ int sfgpu_system::free_energy_grad(const double *x, double *F, double *xbar) {
                                                o.chemintref, scal, m, a_phibar_m[i]);
         return molecule_adjoint(m, a_phibar_m.data());
     };
-    int held = (mols[solvent].type != 0 && !mols[solvent].ring) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0 && !mols[m].ring) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree) held = m;
     if ((rc = mol_adj(solvent))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && !mols[m].ring && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }
@@ -684,14 +814,14 @@ int sfgpu_system::phi_vjp_async(const double *x, const double *const *omega, dou
         SFGPU_CUDA_TRY(cudaMemsetAsync(a_gbar[i], 0, sizeof(double) * M, s));
     }
     fe_zero_scal<<<1, 1, 0, s>>>(nmol, (AdjScal *)a_scal);
-    int held = (mols[solvent].type != 0 && !mols[solvent].ring) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0 && !mols[m].ring) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree) held = m;
     if ((rc = molecule_adjoint(solvent, a_phibar.data()))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && !mols[m].ring && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }

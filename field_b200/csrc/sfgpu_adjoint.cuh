@@ -587,6 +587,39 @@ static __global__ void fe_gbar(int M, const double *__restrict__ q, const double
 // copies (a surface layer's G is a constant).  The ring's scalars (lnGN 0,
 // its phibulk the input's) carry no cotangent.  Boundary sites' profiles
 // are copies whose cotangents arrive folded into their mapped sites.
+// Reverse of the bond tree's composition phi_raw += U D (connect, K = 1) on
+// interior sites: Ubar += pr D, Dbar += pr U
+static __global__ void tree_adj_connect(DLat L, const double *__restrict__ pr, const double *__restrict__ U,
+                                        const double *__restrict__ D, double *__restrict__ Ubar,
+                                        double *__restrict__ Dbar) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < L.M; r += gridDim.x * blockDim.x) {
+        int c[3];
+        lat_coords(L, r, c);
+        if (!lat_interior(L, c)) continue;
+        const double v = pr[r];
+        Ubar[r] += v * D[r];
+        Dbar[r] += v * U[r];
+    }
+}
+
+// Reverse of dst = a b / G (dend_combine; 0 where G <= 0) on interior sites:
+// abar = dstbar b / G (written), bbar += dstbar a / G, Gbar -= dstbar dst / G
+static __global__ void tree_adj_combine(DLat L, const double *__restrict__ dstbar, const double *__restrict__ a,
+                                        const double *__restrict__ b, const double *__restrict__ G,
+                                        const double *__restrict__ dst, double *__restrict__ abar,
+                                        double *__restrict__ bbar, double *__restrict__ gbar) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < L.M; r += gridDim.x * blockDim.x) {
+        int c[3];
+        lat_coords(L, r, c);
+        const double g = G[r];
+        if (!lat_interior(L, c) || !(g > 0)) { abar[r] = 0.0; continue; }
+        const double v = dstbar[r];
+        abar[r] = v * b[r] / g;
+        bbar[r] += v * a[r] / g;
+        gbar[r] -= v * dst[r] / g;
+    }
+}
+
 constexpr int kRingAdjBlocks = 148 * 4;   // blocks of ring_phi_adj (each keeps one set of levels)
 static __global__ void ring_phi_adj(DLat L, int M, int N, int Mmax, const double *__restrict__ G,
                                     const double *__restrict__ phibar, double phibulk, double norm0,

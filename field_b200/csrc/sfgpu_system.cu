@@ -321,6 +321,7 @@ static bool chi_cols_equal(const std::vector<double> &chi, int ns, int a, int b)
 sfgpu_system::~sfgpu_system() {
     if (a_store) cudaFree(a_store);
     if (a_ring) cudaFree(a_ring);
+    if (a_tree) cudaFree(a_tree);
     for (void *p : allocs) cudaFree(p);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }

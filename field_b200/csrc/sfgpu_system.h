@@ -95,6 +95,9 @@ struct sfgpu_system {
     double *a_store = nullptr;
     double *a_ring = nullptr;               // ring walk levels of the reverse sweep (ring_phi_adj)
     size_t a_ring_doubles = 0;
+    double *a_tree = nullptr;               // bond-tree cotangents (molecule_adjoint_tree)
+    size_t a_tree_doubles = 0;
+    int molecule_adjoint_tree(int m);
     double *a_ckF = nullptr, *a_ckB = nullptr, *a_bufF = nullptr, *a_bufB = nullptr;
     int a_qseg = -1;                        // segment held in a_bufF / a_bufB
     std::vector<double *> a_phibar, a_gbar, a_phibar_raw;

@@ -330,7 +330,7 @@ CASES.update({
 
 # cases with forward-mode derivatives (all but dendrimers); the reverse mode
 # also leaves out the second-order lumped lattices and stiff ranges (the
-# adjoint tests list "2nd" cases by name) and branched molecules
+# adjoint tests list "2nd" cases by name)
 NOT_DIFFERENTIABLE = ("dendrimer",)
 DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFERENTIABLE))
 
@@ -339,4 +339,4 @@ def random_x(spec, seed=7, scale=0.3):
     rng = np.random.default_rng(seed)
     return rng.normal(0.0, scale, spec.n_itvar())
 
-REVERSE_EXCLUDED = ("2nd", "branched", "comb")
+REVERSE_EXCLUDED = ("2nd",)
