@@ -180,16 +180,32 @@ int sfgpu_system::ensure_adjoint() {
     if (charged) return fail_unsupported("derivatives of charged systems");
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
-        if (o.dend) return fail_unsupported("derivatives of dendrimers");
+        if (o.dend) build_dend_tree(o);
     int rc = ensure_adjoint_misc();
     if (rc) return rc;
+    // dendrimers run the tree recursion in the reverse sweep: 3N slices
+    size_t dend_need = 0;
+    for (auto &o : mols)
+        if (o.dend) dend_need = std::max(dend_need, (size_t)3 * o.N * M);
+    if (dend_need > a_dend_gi_doubles) {
+        if (a_dend_gi) cudaFree(a_dend_gi);
+        a_dend_gi = nullptr;
+        a_dend_gi_doubles = 0;
+        cudaError_t e = cudaMalloc((void **)&a_dend_gi, sizeof(double) * dend_need);
+        if (e != cudaSuccess) {
+            a_dend_gi = nullptr;
+            sfgpu_set_error(e, "cudaMalloc (dendrimer tree slices)", __FILE__, __LINE__);
+            return SFGPU_ERR_NOMEM;
+        }
+        a_dend_gi_doubles = dend_need;
+    }
     // branched molecules: the cotangents of every U, Q, D slice and a pool
     // for the products a node's combinations pass through
     size_t tree_need = 0;
     for (auto &o : mols) {
-        if (!o.tree) continue;
+        if (!o.tree && !o.dend) continue;
         size_t kmax = 1;
-        for (auto &k : o.kids) kmax = std::max(kmax, k.size());
+        for (auto &k : (o.dend ? o.tkids : o.kids)) kmax = std::max(kmax, k.size());
         tree_need = std::max(tree_need, (3 * (size_t)o.N + kmax + 3) * M);
     }
     if (tree_need > a_tree_doubles) {
@@ -404,6 +420,14 @@ int sfgpu_system::load_segment(int m, int q) {
 
 // primal evaluation of molecule m through store_chains
 int sfgpu_system::molecule_phi_store(int m) {
+    if (mols[m].dend) {   // the tree recursion on the dendrimer's tree form
+        dend_view(mols[m], true);
+        tree_gi = a_dend_gi;
+        const int rc = molecule_phi_store(m);
+        tree_gi = nullptr;
+        dend_view(mols[m], false);
+        return rc;
+    }
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_a(M);
@@ -439,6 +463,14 @@ int sfgpu_system::molecule_phi_store(int m) {
 
 // reverse sweep of one molecule; state phi cotangents in a_phibar
 int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
+    if (mols[m].dend) {
+        dend_view(mols[m], true);
+        tree_gi = a_dend_gi;
+        const int rc = molecule_adjoint(m, phibar_src);
+        tree_gi = nullptr;
+        dend_view(mols[m], false);
+        return rc;
+    }
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_a(M), gr = grid_rows_a(L);
@@ -550,9 +582,10 @@ int sfgpu_system::molecule_adjoint_tree(int m) {
     const size_t bytes = sizeof(double) * M;
     int rc = molecule_phi_tree(m);   // U, Q, D of this molecule (the profiles come out unchanged)
     if (rc) return rc;
-    auto U = [&](int q) { return d_gi + (size_t)q * M; };
-    auto Q = [&](int q) { return d_gi + (size_t)(N + q) * M; };
-    auto D = [&](int q) { return d_gi + (size_t)(2 * N + q) * M; };
+    double *const base = tree_gi ? tree_gi : d_gi;
+    auto U = [&](int q) { return base + (size_t)q * M; };
+    auto Q = [&](int q) { return base + (size_t)(N + q) * M; };
+    auto D = [&](int q) { return base + (size_t)(2 * N + q) * M; };
     auto Ub = [&](int q) { return a_tree + (size_t)q * M; };
     auto Qb = [&](int q) { return a_tree + (size_t)(N + q) * M; };
     auto Db = [&](int q) { return a_tree + (size_t)(2 * N + q) * M; };
@@ -703,14 +736,14 @@ int sfgpu_system::vjp_async(const double *x, const double *w, double *f, double 
     // molecules in reverse order of the primal (the solvent first).  The
     // chain storage holds one molecule: the last polymer the primal
     // propagated keeps its chains, every other polymer is propagated again.
-    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree && !mols[solvent].dend) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree && !mols[m].dend) held = m;
     if ((rc = molecule_adjoint(solvent, a_phibar.data()))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && !mols[m].dend && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }
@@ -773,14 +806,14 @@ int sfgpu_system::free_energy_grad(const double *x, double *F, double *xbar) {
                                                o.chemintref, scal, m, a_phibar_m[i]);
         return molecule_adjoint(m, a_phibar_m.data());
     };
-    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree && !mols[solvent].dend) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree && !mols[m].dend) held = m;
     if ((rc = mol_adj(solvent))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && !mols[m].dend && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }
@@ -814,14 +847,14 @@ int sfgpu_system::phi_vjp_async(const double *x, const double *const *omega, dou
         SFGPU_CUDA_TRY(cudaMemsetAsync(a_gbar[i], 0, sizeof(double) * M, s));
     }
     fe_zero_scal<<<1, 1, 0, s>>>(nmol, (AdjScal *)a_scal);
-    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree) ? solvent : -1;
+    int held = (mols[solvent].type != 0 && !mols[solvent].ring && !mols[solvent].tree && !mols[solvent].dend) ? solvent : -1;
     if (held < 0)
         for (int m = nmol - 1; m >= 0 && held < 0; m--)
-            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree) held = m;
+            if (m != solvent && mols[m].type != 0 && !mols[m].ring && !mols[m].tree && !mols[m].dend) held = m;
     if ((rc = molecule_adjoint(solvent, a_phibar.data()))) return rc;
     for (int m = nmol - 1; m >= 0; m--) {
         if (m == solvent) continue;
-        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && m != held) {
+        if (mols[m].type != 0 && !mols[m].ring && !mols[m].tree && !mols[m].dend && m != held) {
             if ((rc = store_chains(m, false, nullptr))) return rc;
             held = m;
         }

@@ -322,6 +322,7 @@ sfgpu_system::~sfgpu_system() {
     if (a_store) cudaFree(a_store);
     if (a_ring) cudaFree(a_ring);
     if (a_tree) cudaFree(a_tree);
+    if (a_dend_gi) cudaFree(a_dend_gi);
     for (void *p : allocs) cudaFree(p);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -932,14 +933,58 @@ int sfgpu_system::molecule_phi_dend(int m) {
 // lnGN comes from U(0), the whole molecule's propagator at its first
 // segment (Gzs[1][1], SF_Branched1stO.cpp:1269).  U, Q and D take 3 N
 // slices of the chain storage.
+// A symmetric dendrimer as its bond tree, in the order SF_Dend1stO's
+// generations nest (SF_MolStructure.cpp:552-595): generation i is a branch
+// point (its first segment) with f_i copies of the rest of its segments,
+// each continued by generation i + 1; segment 0 is the centre and every
+// parent precedes its children.
+void sfgpu_system::build_dend_tree(HMol &o) {
+    if (!o.tseg.empty()) return;
+    const int G = (int)o.gen_seg.size();
+    std::vector<int> seg, par;
+    // iterative expansion: (generation, parent index) work items
+    std::vector<std::pair<int, int>> todo{{0, -1}};
+    while (!todo.empty()) {
+        const auto [i, p] = todo.back();
+        todo.pop_back();
+        const int root = (int)seg.size();
+        seg.push_back(o.gen_seg[i][0]);
+        par.push_back(p);
+        for (int r = 0; r < o.gen_rep[i]; r++) {
+            int prev = root;
+            for (size_t j = 1; j < o.gen_seg[i].size(); j++) {
+                seg.push_back(o.gen_seg[i][j]);
+                par.push_back(prev);
+                prev = (int)seg.size() - 1;
+            }
+            if (i + 1 < G) todo.push_back({i + 1, prev});
+        }
+    }
+    o.tseg = seg;
+    o.tparent = par;
+    o.tkids.assign(seg.size(), {});
+    for (size_t q = 1; q < seg.size(); q++) o.tkids[par[q]].push_back((int)q);
+}
+
+// swap a dendrimer's tree form in (on) or out: the tree recursion then reads
+// seg, parent, kids and tree as for a branched molecule; N is the same
+void sfgpu_system::dend_view(HMol &o, bool on) {
+    std::swap(o.seg, o.tseg);
+    std::swap(o.parent, o.tparent);
+    std::swap(o.kids, o.tkids);
+    o.tree = on ? 1 : 0;
+    o.dend = on ? 0 : 1;
+}
+
 int sfgpu_system::molecule_phi_tree(int m) {
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_for(M), N = o.N;
     cudaStream_t s = stream;
-    auto U = [&](int q) { return d_gi + (size_t)q * M; };
-    auto Q = [&](int q) { return d_gi + (size_t)(N + q) * M; };
-    auto D = [&](int q) { return d_gi + (size_t)(2 * N + q) * M; };
+    double *const base = tree_gi ? tree_gi : d_gi;
+    auto U = [&](int q) { return base + (size_t)q * M; };
+    auto Q = [&](int q) { return base + (size_t)(N + q) * M; };
+    auto D = [&](int q) { return base + (size_t)(2 * N + q) * M; };
     const size_t bytes = sizeof(double) * M;
     for (int i : o.used) SFGPU_CUDA_TRY(cudaMemsetAsync(o.d_phi[i], 0, bytes, s));
     // ends inwards

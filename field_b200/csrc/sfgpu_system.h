@@ -28,6 +28,10 @@ struct HMol {
     int tree = 0;
     std::vector<int> parent;
     std::vector<std::vector<int>> kids;
+    // a symmetric dendrimer written out as its bond tree (tseg, tparent,
+    // tkids; built by the derivatives, which run the tree recursion on it)
+    std::vector<int> tseg, tparent;
+    std::vector<std::vector<int>> tkids;
     int ring = 0;                     // homopolymer ring (SF_HomoRing1stO)
     double ring_norm0 = 0;            // return weight of the free ring (NORM[0])
     std::vector<std::vector<int>> gen_seg;
@@ -98,6 +102,13 @@ struct sfgpu_system {
     double *a_tree = nullptr;               // bond-tree cotangents (molecule_adjoint_tree)
     size_t a_tree_doubles = 0;
     int molecule_adjoint_tree(int m);
+    // slices of the bond-tree recursion: d_gi, or while a dendrimer runs as
+    // its tree in the reverse sweep (3N slices) a_dend_gi
+    double *tree_gi = nullptr;
+    double *a_dend_gi = nullptr;
+    size_t a_dend_gi_doubles = 0;
+    void build_dend_tree(HMol &o);
+    void dend_view(HMol &o, bool on);
     double *a_ckF = nullptr, *a_ckB = nullptr, *a_bufF = nullptr, *a_bufB = nullptr;
     int a_qseg = -1;                        // segment held in a_bufF / a_bufB
     std::vector<double *> a_phibar, a_gbar, a_phibar_raw;

@@ -27,7 +27,7 @@ int sfgpu_system::ensure_tangent() {
     if (logmode) return fail_unsupported("derivatives with overflow protection");
     if (charged) return fail_unsupported("derivatives of charged systems");
     for (auto &o : mols)
-        if (o.dend) return fail_unsupported("derivatives of dendrimers");
+        if (o.dend) build_dend_tree(o);
     if (t_ready) return SFGPU_OK;
     int rc;
     dgfull.assign(nseg, nullptr); dgseg.assign(nseg, nullptr); dphi.assign(nseg, nullptr);
@@ -44,13 +44,15 @@ int sfgpu_system::ensure_tangent() {
     }
     size_t store = 0;
     for (auto &o : mols) {
-        size_t need = (o.type == 0 || o.ring) ? 0 : (size_t)(o.tree ? 3 * o.N : o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
+        size_t need = (o.type == 0 || o.ring) ? 0
+                      : (size_t)((o.tree || o.dend) ? 3 * o.N : o.sym ? std::max(1, o.N / 2) : o.N) * K * M;
         store = std::max(store, need);
     }
     if ((rc = alloc_d(&d_dgi, store))) return rc;
     // checkpointed primal storage holds fewer slices than the tangent sweeps write
+    // (and a dendrimer's primal keeps one path, its tree three slices per segment)
     bool ck = false;
-    for (auto &o : mols) ck |= primal_checkpointed(o);
+    for (auto &o : mols) ck |= primal_checkpointed(o) || o.dend;
     t_gi = d_gi;
     if (ck) {
         if ((rc = alloc_d(&t_gi, store))) return rc;
@@ -73,6 +75,14 @@ int sfgpu_system::ensure_tangent() {
 }
 
 int sfgpu_system::molecule_phi_t(int m) {
+    if (mols[m].dend) {
+        // a dendrimer's derivatives: the bond-tree recursion on its tree form
+        build_dend_tree(mols[m]);
+        dend_view(mols[m], true);
+        const int rc = molecule_phi_t(m);
+        dend_view(mols[m], false);
+        return rc;
+    }
     HMol &o = mols[m];
     const DLat &L = H.L;
     const int g = grid_n(M), gr = grid_rows_t(L);

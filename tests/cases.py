@@ -328,11 +328,10 @@ CASES.update({
     "1d_ring": lambda: _from_input("1d_ring"),
 })
 
-# cases with forward-mode derivatives (all but dendrimers); the reverse mode
-# also leaves out the second-order lumped lattices and stiff ranges (the
-# adjoint tests list "2nd" cases by name)
-NOT_DIFFERENTIABLE = ("dendrimer",)
-DIFFERENTIABLE = sorted(k for k in CASES if not any(t in k for t in NOT_DIFFERENTIABLE))
+# cases with forward-mode derivatives (all); the reverse mode leaves out the
+# second-order lumped lattices and stiff ranges (the adjoint tests list "2nd"
+# cases by name)
+DIFFERENTIABLE = sorted(CASES)
 
 
 def random_x(spec, seed=7, scale=0.3):

@@ -41,7 +41,8 @@ def test_dot_product_identity(gpu_lib, case):
 
 @pytest.mark.parametrize("case", ["1d_surface", "2d_cylinder", "3d_periodic_melt", "3d_fcc_colloid",
                                   "3d_hex_colloid", "3d_stencils_melt", "1d_branched", "2d_branched",
-                                  "3d_branched", "1d_comb_branched", "1d_ring"])
+                                  "3d_branched", "1d_comb_branched", "1d_ring", "1d_dendrimer",
+                                  "2d_dendrimer"])
 def test_gradient_of_half_squared_norm(gpu_lib, case):
     spec = CASES[case]()
     s = System(spec)
@@ -215,7 +216,7 @@ def test_auto_checkpoint_stride(gpu_lib):
 @pytest.mark.parametrize("case", ["1d_surface", "1d_lambda_chi", "1d_periodic_restricted", "2d_cylinder",
                                   "2d_flat_surface", "3d_mirror_mix", "3d_2nd_brush", "3d_fcc_colloid",
                                   "3d_hex_mirror", "3d_stencils_colloid", "1d_branched", "3d_branched",
-                                  "1d_comb_branched", "1d_ring"])
+                                  "1d_comb_branched", "1d_ring", "1d_dendrimer"])
 def test_free_energy_gradient(gpu_lib, case):
     """dF/dx from the reverse sweep against central differences of F
     (h = 1e-5) along random directions; F itself equals sfgpu_free_energy

@@ -34,7 +34,12 @@ def test_jvp_matches_central_differences(gpu_lib, case):
     x = random_x(spec, seed=21, scale=0.2)
     v = np.random.default_rng(22).normal(0.0, 1.0, s.nvar)
     f, jv = s.jvp(x, v)
-    assert np.array_equal(f, s.residual(x)), "primal of the tangent sweep differs from the residual"
+    if "dendrimer" in case:
+        # the derivatives run a dendrimer as its bond tree: the same molecule
+        # through the tree recursion, equal to the generation walk up to rounding
+        np.testing.assert_allclose(f, s.residual(x), rtol=0, atol=1e-12 * np.max(np.abs(f)))
+    else:
+        assert np.array_equal(f, s.residual(x)), "primal of the tangent sweep differs from the residual"
     ref = fd_jv(s, x, v)
     err = np.max(np.abs(jv - ref)) / max(np.max(np.abs(ref)), 1e-300)
     assert err < TOL_FD, err
