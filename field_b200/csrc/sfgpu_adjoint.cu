@@ -175,7 +175,6 @@ int sfgpu_system::ensure_adjoint_misc() {
 }
 
 int sfgpu_system::ensure_adjoint() {
-    if (K == 3 || K == 5) return fail_unsupported("derivatives of the lumped 1D/2D second-order lattices");
     if (logmode) return fail_unsupported("derivatives with overflow protection");
     if (charged) return fail_unsupported("derivatives of charged systems");
     if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
@@ -308,9 +307,12 @@ void sfgpu_system::adj_fstep(const HMol &o, int t, const double *src, double *ds
                                                                 nullptr, nullptr, COMP_NONE);
     else if (K == 1)
         step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, nullptr, nullptr, COMP_NONE);
-    else
+    else if (K == 6)
         step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], dst,
                                                           nullptr, nullptr, COMP_NONE, 0);
+    else
+        step2l_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], dst,
+                                                           nullptr, nullptr, COMP_NONE, 0);
 }
 void sfgpu_system::adj_bstep(const HMol &o, int t, const double *src, double *dst, const double *other,
                              double *phi) {
@@ -322,9 +324,12 @@ void sfgpu_system::adj_bstep(const HMol &o, int t, const double *src, double *ds
                                                                 other, phi, mode);
     else if (K == 1)
         step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, other, phi, mode);
-    else
+    else if (K == 6)
         step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], dst,
                                                           other, phi, mode, 1);
+    else
+        step2l_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], dst,
+                                                           other, phi, mode, 1);
 }
 
 // Gf and Gb of every position of molecule m's chain (full chains, also for
@@ -531,8 +536,10 @@ int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
                                                        d_gseg[sg], p, a_gbar[sg], nxt);
         else if (K == 1)
             adj_chain_step<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[sg], p, a_gbar[sg], nxt);
-        else
+        else if (K == 6)
             adj_step2<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[sg], p, S, backward, a_gbar[sg], nxt);
+        else
+            adj_step2l<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[sg], p, S, backward, a_gbar[sg], nxt);
     };
     // descending sweep over the forward recursion (step t used S(t-1, t))
     {
@@ -542,22 +549,23 @@ int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
     for (int t = N - 1; t >= 1; t--) {
         const int j = at(t - 1);
         adj_init<<<g, kBlock, 0, s>>>(L, K, a_phibar_raw[o.seg[t - 1]], GB(j), nxt);
-        rstep(t, GF(j), K == 6 ? pf[o.seg[t - 1] * nseg + o.seg[t]] : 0.0, 0);
+        rstep(t, GF(j), K > 1 ? pf[o.seg[t - 1] * nseg + o.seg[t]] : 0.0, 0);
         std::swap(cot, nxt);
     }
     adj_add_interior<<<g, kBlock, 0, s>>>(L, K, cot, a_gbar[o.seg[0]]);
     // ascending sweep over the backward recursion (step t used S(t, t+1));
-    // lnGN = ln(sum w sum_k Gb_k(1) / K) adds qbar / K * w to every component
+    // lnGN = ln(sum w sum_k mu_k Gb_k(1) / 6) (mu_k the lumped multiplicities,
+    // 1 in 3D; 1 and no division on first order) adds qbar mu_k / 6 * w
     {
         const int j = at(0);
         adj_init<<<g, kBlock, 0, s>>>(L, K, a_phibar_raw[o.seg[0]], GF(j), cot);
     }
     adj_qbar_scale<<<1, 1, 0, s>>>(as, m, a_qbar);
-    adj_axpy_interior<<<g, kBlock, 0, s>>>(L, K, d_wgn, a_qbar, 1.0 / K, cot);
+    adj_axpy_interior<<<g, kBlock, 0, s>>>(L, K, d_wgn, a_qbar, K > 1 ? 1.0 / 6.0 : 1.0, cot);
     for (int t = 0; t < N - 1; t++) {
         const int j = at(t + 1);
         adj_init<<<g, kBlock, 0, s>>>(L, K, a_phibar_raw[o.seg[t + 1]], GF(j), nxt);
-        rstep(t, GB(j), K == 6 ? pf[o.seg[t] * nseg + o.seg[t + 1]] : 0.0, 1);
+        rstep(t, GB(j), K > 1 ? pf[o.seg[t] * nseg + o.seg[t + 1]] : 0.0, 1);
         std::swap(cot, nxt);
     }
     adj_add_interior<<<g, kBlock, 0, s>>>(L, K, cot, a_gbar[o.seg[N - 1]]);

@@ -166,8 +166,11 @@ static __global__ void adj_init(DLat L, int K, const double *__restrict__ phibar
         int c[3];
         lat_coords(L, r, c);
         const bool in = lat_interior(L, c);
-        for (int k = 0; k < K; k++)
-            out[(size_t)k * L.M + r] = in ? phibar_raw[r] * q[(size_t)k * L.M + r] : 0.0;
+        for (int k = 0; k < K; k++) {
+            // lumped components carry their multiplicity in the composition
+            const double mu = comp_mult(K, k), v = phibar_raw[r] * q[(size_t)k * L.M + r];
+            out[(size_t)k * L.M + r] = in ? ((mu == 1.0) ? v : v * mu) : 0.0;
+        }
     }
 }
 
@@ -192,8 +195,88 @@ static __global__ void adj_axpy_interior(DLat L, int K, const double *__restrict
         int c[3];
         lat_coords(L, r, c);
         if (!lat_interior(L, c)) continue;
-        for (int k = 0; k < K; k++) out[(size_t)k * L.M + r] += s * w[r];
+        for (int k = 0; k < K; k++) {
+            const double mu = comp_mult(K, k), v = s * w[r];   // lumped: the lnGN sum weighs components
+            out[(size_t)k * L.M + r] += (mu == 1.0) ? v : v * mu;
+        }
     }
+}
+
+// One reverse step of the lumped 1D/2D second-order lattices (the transpose
+// of step2l_rows, flat and curved): gbar[t] += sum_k cot[k][t] (A p)[k][t]
+// and out += A^T (G cot), every read of the forward step (its mapped site,
+// its component after boundary swaps, the curved lattices' mixture
+// f read + (1 - f) reflected component at t) scattered with its weight.
+static __global__ void adj_step2l(DLat L, const double *__restrict__ cot, const double *__restrict__ G,
+                                  const double *__restrict__ p, double S, int backward, double *__restrict__ gbar,
+                                  double *__restrict__ out) {
+    const int M = L.M;
+    const Lump2 q = lump2_of(L.grad);
+    const double Lw = (1.0 - S) / 4.0;
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const int t = R.base + k;
+        const int x = (L.grad == 1) ? k : R.x, y = (L.grad == 1) ? 0 : k;
+        double c[5];
+        bool any = false;
+        for (int kk = 0; kk < q.K; kk++) {
+            c[kk] = cot[(size_t)kk * M + t];
+            any |= c[kk] != 0.0;
+        }
+        if (!any) return;
+        const double g = G[t];
+        double gb = 0;
+        if (!backward) {
+            for (int kk = 0; kk < q.K; kk++) {
+                int src = t, sm = 0;
+                if (q.axis[kk] >= 0) src = lump2_nb(L, x, y, q.axis[kk], -q.sgn[kk], sm);
+                const bool mix = L.cyl && q.axis[kk] == 0;
+                const double f = mix ? 6 * ((-q.sgn[kk] > 0) ? L.lam_p[x] : L.lam_m[x]) : 1.0;
+                const double y0 = g * c[kk];
+                double acc = 0;
+                for (int kp = 0; kp < q.K; kp++) {
+                    const double w = lump2_w(q, kk, kp, S, Lw);
+                    if (w == 0.0) continue;
+                    const int ci = lump2_read(q, kp, q.axis[kk], sm);
+                    double r = p[(size_t)ci * M + src];
+                    if (mix) {
+                        const int refl = lump2_read(q, kp, 0, 1);
+                        r = f * r + (1.0 - f) * p[(size_t)refl * M + t];
+                        atomicAdd(out + (size_t)ci * M + src, y0 * w * f);
+                        atomicAdd(out + (size_t)refl * M + t, y0 * w * (1.0 - f));
+                    } else {
+                        atomicAdd(out + (size_t)ci * M + src, y0 * w);
+                    }
+                    acc += w * r;
+                }
+                gb += c[kk] * acc;
+            }
+        } else {
+            for (int kp = 0; kp < q.K; kp++) {
+                int src = t, sm = 0;
+                if (q.axis[kp] >= 0) src = lump2_nb(L, x, y, q.axis[kp], q.sgn[kp], sm);
+                const int ci = lump2_read(q, kp, q.axis[kp], sm);
+                const bool mixed = L.cyl && q.axis[kp] == 0 && (L.grad == 1 || q.sgn[kp] < 0);
+                const double f = mixed ? 6 * ((q.sgn[kp] > 0) ? L.lam_p[x] : L.lam_m[x]) : 1.0;
+                double v = p[(size_t)ci * M + src];
+                if (mixed) v = f * v + (1.0 - f) * p[(size_t)lump2_swap(q, kp) * M + t];
+                double wc = 0;   // sum_kq w(kq, kp) cot[kq]
+                for (int kq = 0; kq < q.K; kq++) {
+                    const double w = lump2_w(q, kq, kp, S, Lw);
+                    if (w != 0.0) wc += w * c[kq];
+                }
+                const double vb = g * wc;
+                if (mixed) {
+                    atomicAdd(out + (size_t)ci * M + src, vb * f);
+                    atomicAdd(out + (size_t)lump2_swap(q, kp) * M + t, vb * (1.0 - f));
+                } else {
+                    atomicAdd(out + (size_t)ci * M + src, vb);
+                }
+                gb += wc * v;
+            }
+        }
+        gbar[t] += gb;
+    });
 }
 
 // One reverse second-order step (the transpose of step2_rows): with

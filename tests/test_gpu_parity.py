@@ -195,21 +195,6 @@ def test_lumped_second_order_converged_parity(gpu_lib, case):
     assert abs(sys_.free_energy() - o.free_energy()) <= 1e-9 * max(1.0, abs(o.free_energy()))
 
 
-def test_lumped_reverse_mode_reports_unsupported(gpu_lib):
-    """The reverse mode of the lumped lattices is outside the implemented
-    path (their forward mode exists): J^T.w returns SFGPU_ERR_UNSUPPORTED
-    instead of a number, and the primal path stays usable afterwards."""
-    from field_b200._native import SfgpuError
-    spec = CASES["1d_2nd_lumped"]()
-    sys_ = System(spec)
-    x = random_x(spec)
-    assert np.all(np.isfinite(sys_.jvp(x, x)))
-    with pytest.raises(SfgpuError) as e:
-        sys_.vjp(x, x)
-    assert e.value.code == 7
-    assert np.all(np.isfinite(sys_.residual(x)))
-
-
 @pytest.mark.parametrize("case", ["3d_2nd_brush", "1d_2nd_lumped", "2d_2nd_lumped", "2d_2nd_lumped_periodic",
                                   "1d_cyl_2nd_lumped", "2d_cyl_2nd_lumped"])
 def test_bond_orientation(gpu_lib, case):
