@@ -177,7 +177,6 @@ int sfgpu_system::ensure_adjoint_misc() {
 int sfgpu_system::ensure_adjoint() {
     if (logmode) return fail_unsupported("derivatives with overflow protection");
     if (charged) return fail_unsupported("derivatives of charged systems");
-    if (H.L.stiff) return fail_unsupported("derivatives with a stiff range");
     for (auto &o : mols)
         if (o.dend) build_dend_tree(o);
     int rc = ensure_adjoint_misc();
@@ -307,7 +306,13 @@ void sfgpu_system::adj_fstep(const HMol &o, int t, const double *src, double *ds
                                                                 nullptr, nullptr, COMP_NONE);
     else if (K == 1)
         step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, nullptr, nullptr, COMP_NONE);
-    else if (K == 6)
+    else if (K == 6 && L.stiff) {   // SF_Copol2ndO_stiff_range.cpp:211-217, the last step isotropic
+        const bool last = (t == o.N - 1);
+        step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg],
+                                                          last ? 0.2 : pf[o.seg[t - 1] * nseg + o.seg[t + 1]], dst,
+                                                          nullptr, nullptr, COMP_NONE, 0,
+                                                          last ? STEP2_ISO : STEP2_STIFF);
+    } else if (K == 6)
         step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[o.seg[t - 1] * nseg + sg], dst,
                                                           nullptr, nullptr, COMP_NONE, 0);
     else
@@ -324,7 +329,12 @@ void sfgpu_system::adj_bstep(const HMol &o, int t, const double *src, double *ds
                                                                 other, phi, mode);
     else if (K == 1)
         step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, other, phi, mode);
-    else if (K == 6)
+    else if (K == 6 && L.stiff) {   // :229-234, the first backward step isotropic
+        const bool first = (t == o.N - 2);
+        step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg],
+                                                          first ? 0.2 : pf[sg * nseg + o.seg[t + 2]], dst, other,
+                                                          phi, mode, 1, first ? STEP2_ISO : STEP2_STIFF);
+    } else if (K == 6)
         step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], pf[sg * nseg + o.seg[t + 1]], dst,
                                                           other, phi, mode, 1);
     else
@@ -531,6 +541,15 @@ int sfgpu_system::molecule_adjoint(int m, double *const *phibar_src) {
     // one reverse step: gbar(seg t) += cot . A p; nxt += A^T (G_t cot)
     auto rstep = [&](int t, const double *p, double S, int backward) {
         const int sg = o.seg[t];
+        if (K == 6 && L.stiff) {
+            // the stiff-range chain's steps: forward into t with Pf(t-1, t+1),
+            // backward into t with Pf(t, t+2), isotropic at the chain's end
+            const bool iso = backward ? (t == N - 2) : (t == N - 1);
+            const double Sv = iso ? 0.2 : (backward ? pf[sg * nseg + o.seg[t + 2]] : pf[o.seg[t - 1] * nseg + o.seg[t + 1]]);
+            adj_step2v<<<gr, kBlock, 0, s>>>(L, cot, d_gseg[sg], p, Sv, backward, iso ? STEP2_ISO : STEP2_STIFF,
+                                             a_gbar[sg], nxt);
+            return;
+        }
         if (K == 1 && o.force != 0)   // the forward recursion's +force, the backward one's -force
             adj_chain_step_force<<<gr, kBlock, 0, s>>>(L, force_weights(L, backward ? -o.force : o.force), cot,
                                                        d_gseg[sg], p, a_gbar[sg], nxt);

@@ -202,6 +202,104 @@ static __global__ void adj_axpy_interior(DLat L, int K, const double *__restrict
     }
 }
 
+// One reverse step of the 3D second-order stiff-range steps (the transpose
+// of step2_rows with STEP2_STIFF or STEP2_ISO): every read of the forward
+// step (the mapped, component-swapped source) scattered with its weight --
+// per site S inside the range and 0.2 outside, taken at the index the
+// forward step takes it, or G/6 for the isotropic steps (whose forward -y
+// component reads +z twice and -y never) -- and G's cotangent from the
+// unweighted sums.
+static __global__ void adj_step2v(DLat L, const double *__restrict__ cot, const double *__restrict__ G,
+                                  const double *__restrict__ p, double S, int backward, int wmode,
+                                  double *__restrict__ gbar, double *__restrict__ out) {
+    const int M = L.M;
+    const int nx = L.Md[0] - 2, ny = L.Md[1] - 2;
+    const int worker = blockIdx.x * blockDim.x + threadIdx.x;
+    for_interior(L, worker, gridDim.x * blockDim.x, [&](const RowInfo &R, int k, int nlast) {
+        const int t = R.base + k;
+        double c[6];
+        bool any = false;
+#pragma unroll
+        for (int kk = 0; kk < 6; kk++) {
+            c[kk] = cot[(size_t)kk * M + t];
+            any |= c[kk] != 0.0;
+        }
+        if (!any) return;
+        const int zm = (k == 1) ? L.map_lo[2] : k - 1;
+        const int zp = (k == nlast) ? L.map_hi[2] : k + 1;
+        const int off[6] = {R.up, R.dn, R.up2, R.dn2, zm - k, zp - k};
+        const bool sw[6] = {R.x == 1 && is_mirror(L.bc_lo[0]), R.x == nx && is_mirror(L.bc_hi[0]),
+                            R.y == 1 && is_mirror(L.bc_lo[1]), R.y == ny && is_mirror(L.bc_hi[1]),
+                            k == 1 && is_mirror(L.bc_lo[2]), k == nlast && is_mirror(L.bc_hi[2])};
+        const int raw[6] = {L.st[0], L.st[1], 1, 1, L.st[1], L.st[0]};
+        auto ps_at = [&](int i) { return (L.stiff[i] != 0) ? S : 0.2; };
+        const double g = G[t];
+        double gb = 0;
+        if (!backward) {
+            const int dir_of[6] = {0, 2, 4, 5, 3, 1};
+            for (int kk = 0; kk < 6; kk++) {
+                const int dd = dir_of[kk];
+                const int src = t + off[dd];
+                const int axis = dd >> 1;
+                const bool sflag = sw[dd];
+                auto cidx = [&](int kp) {
+                    int cc = kp;
+                    if (sflag) {
+                        if (axis == 0 && (kp == 0 || kp == 5)) cc = 5 - kp;
+                        if (axis == 1 && (kp == 1 || kp == 4)) cc = 5 - kp;
+                        if (axis == 2 && (kp == 2 || kp == 3)) cc = 5 - kp;
+                    }
+                    return cc;
+                };
+                double acc = 0;
+                if (wmode == STEP2_ISO) {
+                    const int seq4[6] = {0, 2, 2, 3, 4, 5};
+                    for (int q = 0; q < 6; q++) {
+                        const int cc = cidx(kk == 4 ? seq4[q] : q);
+                        acc += p[(size_t)cc * M + src] * (1.0 / 6.0);
+                        atomicAdd(out + (size_t)cc * M + src, c[kk] * g * (1.0 / 6.0));
+                    }
+                } else {
+                    const int pi = (kk < 3) ? t - raw[kk] : t;
+                    const double ps = ps_at(pi), pl = (1.0 - ps) / 4.0;
+                    for (int kp = 0; kp < 6; kp++) {
+                        if (kp == 5 - kk) continue;
+                        const double w = (kp == kk) ? ps : pl;
+                        const int cc = cidx(kp);
+                        acc += p[(size_t)cc * M + src] * w;
+                        atomicAdd(out + (size_t)cc * M + src, c[kk] * g * w);
+                    }
+                }
+                gb += c[kk] * acc;
+            }
+        } else {
+            const int dir_of[6] = {1, 3, 5, 4, 2, 0};
+            for (int kp = 0; kp < 6; kp++) {
+                const int dd = dir_of[kp];
+                const int cc = sw[dd] ? 5 - kp : kp;
+                const int src = t + off[dd];
+                const double v = p[(size_t)cc * M + src];
+                double wc = 0;   // sum_kq w(kq, kp) cot[kq], w without G
+                for (int kq = 0; kq < 6; kq++) {
+                    double w;
+                    if (wmode == STEP2_ISO) {
+                        w = 1.0 / 6.0;
+                    } else {
+                        if (kp == 5 - kq) continue;
+                        const int pi = (kp >= 3) ? t - raw[kp] : t;
+                        const double ps = ps_at(pi), pl = (1.0 - ps) / 4.0;
+                        w = (kp == kq) ? ps : pl;
+                    }
+                    wc += w * c[kq];
+                }
+                atomicAdd(out + (size_t)cc * M + src, g * wc);
+                gb += wc * v;
+            }
+        }
+        gbar[t] += gb;
+    });
+}
+
 // One reverse step of the lumped 1D/2D second-order lattices (the transpose
 // of step2l_rows, flat and curved): gbar[t] += sum_k cot[k][t] (A p)[k][t]
 // and out += A^T (G cot), every read of the forward step (its mapped site,

@@ -60,7 +60,7 @@ def test_gradient_of_half_squared_norm(gpu_lib, case):
 
 @pytest.mark.parametrize("case", ["3d_2nd_brush", "3d_2nd_fcc_brush", "1d_2nd_lumped", "2d_2nd_lumped",
                                   "2d_2nd_lumped_periodic", "1d_cyl_2nd_lumped", "1d_sphere_2nd_lumped",
-                                  "2d_cyl_2nd_lumped"])
+                                  "2d_cyl_2nd_lumped", "3d_2nd_stiff_copol"])
 def test_second_order_dot_product_and_gradient(gpu_lib, case):
     """Second-order (six-direction) reverse sweep on the pinned 3D brush (and
     on the FCC lattice type, whose contact averages span the 27-site cube):

@@ -296,17 +296,13 @@ def test_dendrimer_converged_parity(gpu_lib, case):
 
 def test_stiff_range_refusals(gpu_lib):
     """A stiff range takes copolymers only (SF_MolList2ndO.cpp:39-47); bond
-    orientation and the reverse mode are not built for it."""
+    orientation is not built for it."""
     from field_b200._native import SfgpuError
     from field_b200.desc import Molecule, MOL_FREE
     spec = CASES["3d_2nd_stiff_copol"]()
     s = System(spec)
     with pytest.raises(SfgpuError) as e:
         s.set_bond_orientation(True)
-    assert e.value.code == 7
-    x = random_x(spec)
-    with pytest.raises(SfgpuError) as e:
-        s.vjp(x, x)
     assert e.value.code == 7
     spec.molecules[0] = Molecule("A9", [(1, 9)], MOL_FREE, phibulk=0.03)
     with pytest.raises(SfgpuError) as e:
