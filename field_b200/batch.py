@@ -176,7 +176,7 @@ class BatchSolver:
         nat.check(self.lib.sfgpu_batch_set_launch(self.h, int(threads), int(bool(stage))), "sfgpu_batch_set_launch")
 
     def autotune(self, x0, tol=1e-7, maxit=2000, candidates=((1024, True), (512, True), (512, False),
-                                                             (256, True))):
+                                                             (384, True), (256, True))):
         """Time one solve per launch shape from x0 and keep the fastest;
         returns {(threads, stage): ms}."""
         times = {}

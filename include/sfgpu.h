@@ -516,8 +516,8 @@ int sfgpu_batch_destroy(sfgpu_batch *batch);
  * instance in the concatenated x vector */
 int sfgpu_batch_info(sfgpu_batch *batch, int *n, long long *total_nvar, long long *offsets);
 int sfgpu_batch_set_stream(sfgpu_batch *batch, void *stream);
-/* launch shape of the persistent kernel: threads per block (128..1024, a
- * multiple of 32; default 1024, 512 or 256 by lattice size) and whether G of
+/* launch shape of the persistent kernel: threads per block (32..1024, a
+ * multiple of 32; default 1024, 512, 384 or 256 by lattice size) and whether G of
  * the running segment (and on 1D symmetric homopolymers the running slices,
  * phi and a ring of stored slices) is staged in shared memory (default 1).
  * Results do not depend on it; the autotuner of field_b200.batch times the
