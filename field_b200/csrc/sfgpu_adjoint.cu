@@ -305,7 +305,7 @@ void sfgpu_system::adj_fstep(const HMol &o, int t, const double *src, double *ds
         step1_force_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, force_weights(L, o.force), src, d_gseg[sg], dst,
                                                                 nullptr, nullptr, COMP_NONE);
     else if (K == 1)
-        step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, nullptr, nullptr, COMP_NONE);
+        launch_step1(src, d_gseg[sg], dst, nullptr, nullptr, COMP_NONE);   // the residual's step (3D: x-marching)
     else if (K == 6 && L.stiff) {   // SF_Copol2ndO_stiff_range.cpp:211-217, the last step isotropic
         const bool last = (t == o.N - 1);
         step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg],
@@ -328,7 +328,7 @@ void sfgpu_system::adj_bstep(const HMol &o, int t, const double *src, double *ds
         step1_force_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, force_weights(L, -o.force), src, d_gseg[sg], dst,
                                                                 other, phi, mode);
     else if (K == 1)
-        step1_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg], dst, other, phi, mode);
+        launch_step1(src, d_gseg[sg], dst, other, phi, mode);
     else if (K == 6 && L.stiff) {   // :229-234, the first backward step isotropic
         const bool first = (t == o.N - 2);
         step2_rows<<<grid_rows_a(L), kBlock, 0, stream>>>(L, src, d_gseg[sg],
