@@ -1,5 +1,5 @@
-// sfgpu_charge.cuh -- charged systems on the first-order lattices (1D flat,
-// cylinder, sphere; 2D flat and cylinder; 3D):
+// sfgpu_charge.cuh -- charged systems on every lattice (1D flat,
+// cylinder, sphere; 2D flat and cylinder; 3D; first or second order):
 // the electrostatic potential psi as iteration variables next to the
 // segment potentials (SF_Solve.cpp:164-177, :794-852), its Poisson sweep
 // (Lat1DFlat::ElectricPotential, Lat1DFlat.cpp:526-549) and field

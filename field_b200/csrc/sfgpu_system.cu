@@ -1345,8 +1345,7 @@ int sfgpu_system::setup_charges(const sfgpu_system_desc *d, const std::vector<in
         if (neutralizer >= 0) return fail(SFGPU_ERR_INVALID, "a neutralizer needs charged segments");
         return SFGPU_OK;
     }
-    if (K != 1 || logmode)
-        return fail(SFGPU_ERR_UNSUPPORTED, "charges on second-order or overflow-protected lattices");
+    if (logmode) return fail(SFGPU_ERR_UNSUPPORTED, "charges on overflow-protected lattices");
     auto bulk_charge = [&](const HMol &o) {
         double q = 0;
         for (int i : o.used) q += 1.0 * valence[i] * o.count[i];

@@ -141,9 +141,9 @@ typedef struct {
      * valence in elementary charges and the relative dielectric constant
      * (0 = SFbox's default 80).  Any nonzero valence makes the system
      * charged: the electrostatic potential psi joins the iteration
-     * variables (SF_Solve.cpp:164-177) -- on the first-order lattices (1D
-     * flat, cylinder, sphere; 2D flat, cylinder; 3D, where no frozen segment
-     * may lie on a boundary layer); second-order and overflow-protected
+     * variables (SF_Solve.cpp:164-177) -- on every lattice (1D flat,
+     * cylinder, sphere; 2D flat, cylinder; 3D, where no frozen segment may
+     * lie on a boundary layer), first or second order; overflow-protected
      * lattices return SFGPU_ERR_UNSUPPORTED. */
     double        valence;
     double        epsilon;

@@ -1162,6 +1162,84 @@ newton : isaac : method : Pure_DIIS
 newton : isaac : tolerance : 1e-12
 start
 """,
+    # charges with second-order propagators (Lat1D2ndO): a charged surface,
+    # a semiflexible polyelectrolyte with salt and a neutralizer
+    "1d_2nd_charged": """lat : l : gradients : 1
+lat : l : geometry : flat
+lat : l : n_layers : 24
+lat : l : lambda : 0.16666666666666667
+lat : l : lowerbound : surface
+lat : l : upperbound : mirror2
+lat : l : bondlength : 3e-10
+sys : noname : matrix_approach : second_order
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : S : valence : -0.2
+mon : A : freedom : free
+mon : A : valence : 0.3
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - S : -1.2
+mon : A : chi - W : 0.6
+mon : A : Pf - A : 0.5
+mol : A : composition : (A)15
+mol : A : freedom : free
+mol : A : phibulk : 0.002
+mol : Na : composition : (Na)1
+mol : Na : freedom : free
+mol : Na : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
+    # charges with the six-direction 3D second-order propagators (Lat3D2ndO)
+    "3d_2nd_charged": """lat : box : gradients : 3
+lat : box : geometry : flat
+lat : box : n_layers_x : 6
+lat : box : n_layers_y : 5
+lat : box : n_layers_z : 6
+lat : box : lowerbound_x : mirror1
+lat : box : upperbound_x : mirror1
+lat : box : lowerbound_y : periodic
+lat : box : upperbound_y : periodic
+lat : box : lowerbound_z : mirror2
+lat : box : upperbound_z : mirror1
+lat : box : bondlength : 3e-10
+sys : noname : matrix_approach : second_order
+mon : S : freedom : frozen
+mon : S : frozen_range : 2,2,2;3,3,3
+mon : S : valence : 0.3
+mon : A : freedom : free
+mon : A : valence : -0.2
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - S : -0.8
+mon : A : chi - W : 0.5
+mon : A : Pf - A : 0.4
+mol : A : composition : (A)8
+mol : A : freedom : free
+mol : A : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : free
+mol : Cl : phibulk : 0.01
+mol : Na : composition : (Na)1
+mol : Na : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+""",
     # charges on the 3D lattice (Lat3D::ElectricPotential): a charged
     # colloid inside a mirror / periodic box
     "3d_charged_colloid": """lat : box : gradients : 3
