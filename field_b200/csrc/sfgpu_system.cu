@@ -1345,7 +1345,6 @@ int sfgpu_system::setup_charges(const sfgpu_system_desc *d, const std::vector<in
         if (neutralizer >= 0) return fail(SFGPU_ERR_INVALID, "a neutralizer needs charged segments");
         return SFGPU_OK;
     }
-    if (logmode) return fail(SFGPU_ERR_UNSUPPORTED, "charges on overflow-protected lattices");
     auto bulk_charge = [&](const HMol &o) {
         double q = 0;
         for (int i : o.used) q += 1.0 * valence[i] * o.count[i];

@@ -143,8 +143,8 @@ typedef struct {
      * charged: the electrostatic potential psi joins the iteration
      * variables (SF_Solve.cpp:164-177) -- on every lattice (1D flat,
      * cylinder, sphere; 2D flat, cylinder; 3D, where no frozen segment may
-     * lie on a boundary layer), first or second order; overflow-protected
-     * lattices return SFGPU_ERR_UNSUPPORTED. */
+     * lie on a boundary layer), first or second order, with or without
+     * overflow protection. */
     double        valence;
     double        epsilon;
 } sfgpu_segment_desc;

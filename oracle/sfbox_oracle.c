@@ -856,9 +856,6 @@ int orc_create(const sfgpu_system_desc *d, orc_system **out) {
         s->sitedist = s->L.grad == 3 ? s->bondlength : s->bondlength / sqrt(2 * dims * s->L.l1);
     }
     s->temperature = d->temperature > 0 ? d->temperature : 298.15;              /* SF_System.cpp:68 */
-    if (s->charged && s->L.logmode) {
-        orc_destroy(s); return SFGPU_ERR_UNSUPPORTED;
-    }
     for (int i = 0; i < ns; i++)   /* epsilon differs among liquid states (SF_Solve.cpp:154-162) */
         for (int j = 0; j < ns; j++)
             if (s->charged && s->freedom[i] != SFGPU_SEG_FROZEN && s->freedom[j] != SFGPU_SEG_FROZEN &&

@@ -46,7 +46,8 @@ SOLVE_CASES = ["1d_flat_surface", "1d_flat_c1", "1d_flat_mirror2", "1d_flat_peri
                "1d_branched", "1d_branched_restricted", "2d_branched", "3d_branched", "1d_comb", "1d_ring",
                "1d_asym_dendrimer", "1d_comb_branched_side", "1d_charged", "1d_charged_eps",
                "1d_cyl_charged", "1d_sphere_charged", "2d_flat_charged", "2d_flat_charged_walls", "2d_cyl_charged",
-               "2d_cyl_charged_axis", "3d_charged_colloid", "1d_2nd_charged", "3d_2nd_charged"]
+               "2d_cyl_charged_axis", "3d_charged_colloid", "1d_2nd_charged", "3d_2nd_charged",
+               "1d_charged_overflow"]
 
 
 NEWTON_CASES = ["1d_flat_c1", "1d_flat_surface", "1d_sphere_colloid", "2d_cylinder_core", "2d_flat_surface",

@@ -32,6 +32,41 @@ newton : isaac : tolerance : 1e-12
 start
 """
 
+INPUTS_CHARGED_1D = """lat : flat : gradients : 1
+lat : flat : geometry : flat
+lat : flat : n_layers : 30
+lat : flat : lambda : 0.16666666666666667
+lat : flat : lowerbound : surface
+lat : flat : upperbound : mirror1
+lat : flat : bondlength : 3e-10
+mon : S : freedom : frozen
+mon : S : frozen_range : lowerbound
+mon : S : valence : -0.2
+mon : S : epsilon : 5
+mon : A : freedom : free
+mon : A : valence : 0.5
+mon : W : freedom : free
+mon : Na : freedom : free
+mon : Na : valence : 1
+mon : Cl : freedom : free
+mon : Cl : valence : -1
+mon : A : chi - W : 0.5
+mon : A : chi - S : -1.0
+mol : pol : composition : (A)20
+mol : pol : freedom : free
+mol : pol : phibulk : 0.001
+mol : Na : composition : (Na)1
+mol : Na : freedom : free
+mol : Na : phibulk : 0.01
+mol : Cl : composition : (Cl)1
+mol : Cl : freedom : neutralizer
+mol : water : composition : (W)1
+mol : water : freedom : solvent
+newton : isaac : method : Pure_DIIS
+newton : isaac : tolerance : 1e-12
+start
+"""
+
 INPUTS = {
     # Lat1DFlat1stO, the C1 system at reduced size: surface, frozen S
     "1d_flat_surface": """lat : flat : gradients : 1
@@ -850,40 +885,8 @@ start
     # charges (SF_Solve.cpp:164-177): a polyelectrolyte at a charged surface
     # with a 1:1 salt, the anion as neutralizer; Na and Cl share an iteration
     # variable class (equal chi) and differ by valence
-    "1d_charged": """lat : flat : gradients : 1
-lat : flat : geometry : flat
-lat : flat : n_layers : 30
-lat : flat : lambda : 0.16666666666666667
-lat : flat : lowerbound : surface
-lat : flat : upperbound : mirror1
-lat : flat : bondlength : 3e-10
-mon : S : freedom : frozen
-mon : S : frozen_range : lowerbound
-mon : S : valence : -0.2
-mon : S : epsilon : 5
-mon : A : freedom : free
-mon : A : valence : 0.5
-mon : W : freedom : free
-mon : Na : freedom : free
-mon : Na : valence : 1
-mon : Cl : freedom : free
-mon : Cl : valence : -1
-mon : A : chi - W : 0.5
-mon : A : chi - S : -1.0
-mol : pol : composition : (A)20
-mol : pol : freedom : free
-mol : pol : phibulk : 0.001
-mol : Na : composition : (Na)1
-mol : Na : freedom : free
-mol : Na : phibulk : 0.01
-mol : Cl : composition : (Cl)1
-mol : Cl : freedom : neutralizer
-mol : water : composition : (W)1
-mol : water : freedom : solvent
-newton : isaac : method : Pure_DIIS
-newton : isaac : tolerance : 1e-12
-start
-""",
+    "1d_charged": INPUTS_CHARGED_1D,
+
     # charges with different dielectric constants of the liquid states
     # (E^2 terms), a restricted polyelectrolyte, mirror2 above, T = 310 K
     "1d_charged_eps": """sys : noname : temperature : 310
@@ -1240,6 +1243,9 @@ newton : isaac : method : Pure_DIIS
 newton : isaac : tolerance : 1e-12
 start
 """,
+    # charges with overflow protection (the log-space Lat1DFlat1stOS)
+    "1d_charged_overflow": INPUTS_CHARGED_1D.replace("lat : flat : bondlength : 3e-10\n",
+                                                      "lat : flat : bondlength : 3e-10\nsys : noname : overflow_protection : true\n"),
     # charges on the 3D lattice (Lat3D::ElectricPotential): a charged
     # colloid inside a mirror / periodic box
     "3d_charged_colloid": """lat : box : gradients : 3
