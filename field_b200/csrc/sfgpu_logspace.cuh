@@ -213,7 +213,7 @@ static __global__ void mol_scalars_log(MolParam p, const double *__restrict__ ln
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     MolScal s;
     s.lngn = *lngn;
-    double phib = p.phibulk_in;
+    double phib = p.phib_dev ? *p.phib_dev : p.phibulk_in;   // a neutralizer's from the device
     if (p.solvent) {
         phib = 1.0;
         for (int m = 0; m < p.nmol; m++)

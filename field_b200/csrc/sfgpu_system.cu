@@ -754,6 +754,7 @@ int sfgpu_system::molecule_phi_log(int m) {
     p.N = o.N; p.type = o.type; p.freedom = o.freedom; p.sym = o.sym; p.K = 1;
     p.pinned = o.pinned; p.solvent = (m == solvent); p.nmol = nmol;
     p.phibulk_in = o.phibulk; p.theta = o.theta;
+    if (m == neutralizer) { p.freedom = SFGPU_MOL_FREE; p.phib_dev = d_neut_phib; }
     MolScal *scal = (MolScal *)d_scal;
     const int restr = (o.freedom == SFGPU_MOL_RESTRICTED);
     const double N = (double)o.N;
