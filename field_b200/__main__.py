@@ -5,7 +5,7 @@ Runs an SFbox input file the way ``sfbox input.in`` does for the SCF path
 ``var :`` sweep in order, each point started from the previous point's
 result (``newton : initial_guess : previous_result``, the default), and
 ``ana`` / ``kal`` output files written after every point
-(field_b200.output).  ``vtk`` files are written one per
+(field_b200.output).  ``vtk`` and ``profiles`` files are written one per
 calculation under numbered names.  Sweeps of first-order systems are solved as batched
 instances (field_b200.sweep): ``--waves`` sets how many batched launches the
 sweep is split into (default: one per point, SFbox's chain).  Solver: the
@@ -31,7 +31,7 @@ def main(argv=None) -> int:
     ap.add_argument("--waves", type=int, default=0, help="batched launches per sweep (0: one per point)")
     a = ap.parse_args(argv)
     from .output import (numbered_filename, output_lines, output_requests, read_template, write_ana, write_kal,
-                         write_vtk)
+                         write_profiles, write_vtk)
     from .desc import LATTICE_HEX
     from .sfinput import build_system, parse_input
     from .sweep import batchable, solve_sweep, sweep_calculations
@@ -92,8 +92,13 @@ def main(argv=None) -> int:
                     tmpl = read_template(os.path.join(indir, tmpl)) if tmpl else None
                     vpath = os.path.join(outdir, numbered_filename(name, ci, len(calcs), var,
                                                                    var.values[pi] if var else None))
-                    write_vtk(vpath, lines, spec.lattice.shape, tmpl,
-                              spec.lattice.gradients == 3 and spec.lattice.lattice_type == LATTICE_HEX)
+                    if kind == "profiles":
+                        write_profiles(vpath, lines, spec.lattice.shape, tmpl,
+                                       params.get("write_bounds", "true") != "false",
+                                       params.get("write_blank_lines", "true") != "false")
+                    else:
+                        write_vtk(vpath, lines, spec.lattice.shape, tmpl,
+                                  spec.lattice.gradients == 3 and spec.lattice.lattice_type == LATTICE_HEX)
                 written.add(path)
             print(f"calculation {calc_number}: {'converged' if status == 0 else 'NOT converged'} "
                   f"in {its} iterations, |f| = {err:.3g}", flush=True)

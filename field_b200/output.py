@@ -19,10 +19,13 @@ The keys are SFbox's.  Two writers:
   one row of values per calculation.
 * ``vtk`` (Output::OutputVtkProfiles, Output.cpp:727-905): one file per
   calculation (numbered names) with the profiles a template selects.
+* ``profiles`` (Output::OutputProfiles, Output.cpp:998-1196): one file per
+  calculation (numbered names), the selected profiles as columns beside the
+  site coordinates.
 
-Scalars are printed with ``accuracy`` significant digits (default
-int(-log10(tolerance) + 0.5), SF_Box.cpp:93); profile values with six, as a
-default C++ stream prints them.
+Reals -- scalars and profile values -- are printed as SFbox's output streams
+print them: scientific with ``accuracy`` significant digits (default
+int(-log10(tolerance) + 0.5), SF_Box.cpp:93; Output.cpp:1398-1410).
 """
 from __future__ import annotations
 
@@ -47,6 +50,7 @@ class OutputLine:
     key: str
     value: str
     profile: Optional[np.ndarray] = None
+    acc: int = 12                     # significant digits of the profile values
 
 
 def _names(calc: Dict[Key, str], cls: str, default: str) -> str:
@@ -57,7 +61,9 @@ def _names(calc: Dict[Key, str], cls: str, default: str) -> str:
 
 
 def _real(v: float, acc: int) -> str:
-    return f"{v:.{acc}g}"
+    """A real as SFbox's output streams print it: scientific, acc - 1 digits
+    after the point, the point always shown (Output::open, Output.cpp:1398-1410)."""
+    return f"{v:.{max(acc - 1, 0)}e}"
 
 
 def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: int, error: float,
@@ -72,7 +78,7 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
     out: List[OutputLine] = []
     R = lambda c, n, k, v: out.append(OutputLine(c, n, k, _real(float(v), acc)))
     T = lambda c, n, k, v: out.append(OutputLine(c, n, k, str(v)))
-    P = lambda c, n, k, p: out.append(OutputLine(c, n, k, "profile", np.asarray(p, dtype=float)))
+    P = lambda c, n, k, p: out.append(OutputLine(c, n, k, "profile", np.asarray(p, dtype=float), acc))
     sname = _names(calc, "sys", "noname")
     T("sys", sname, "calculation number", calc_number)
     T("sys", sname, "matrix_approach", "second_order" if spec.lattice.order == 2 else "first_order")
@@ -92,34 +98,10 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
         T("lat", lname, "lowerbound" + a, _BOUND_TEXT.get(lat.bound_lo[d], "?"))
         T("lat", lname, "upperbound" + a, _BOUND_TEXT.get(lat.bound_hi[d], "?"))
     R("lat", lname, "lambda", lat.lam)
-    # chi list, then the segments (SF_SegmentList::GetOutput, SF_SegmentList.cpp:387-405;
-    # SF_Segment::GetOutput, SF_Segment.cpp:345-402)
-    ns = len(spec.segments)
-    chi = np.asarray(spec.chi, dtype=float).reshape(ns, ns)
-    for i in range(ns):
-        for j in range(ns):
-            if i != j:
-                R("chi list", spec.segments[i].name, "chi - " + spec.segments[j].name, chi[i, j])
     sites = float(w_sum.sum())
     mols = spec.molecules
     N = [m.N for m in mols]
     phib_m = [sys_.mol_scalars(m)["phibulk"] for m in range(len(mols))]
-    for i, seg in enumerate(spec.segments):
-        fr = {SEG_FROZEN: "frozen", SEG_PINNED: "pinned"}.get(seg.freedom, "free")
-        T("mon", seg.name, "freedom", fr)
-        phi = sys_.phi(i)
-        pb = 0.0
-        if seg.freedom != SEG_FROZEN:
-            for m, mol in enumerate(mols):
-                cnt = mol.count(i)
-                pb += phib_m[m] * cnt / N[m]
-        R("mon", seg.name, "phibulk", pb)
-        theta = float((w_sum * phi).sum())
-        R("mon", seg.name, "theta", theta)
-        R("mon", seg.name, "theta excess", theta - sites * pb)
-        P("mon", seg.name, "phi", phi)
-        if seg.freedom != SEG_FROZEN:
-            P("mon", seg.name, "G", sys_.swf(i))
     # molecules (SF_Molecule::GetOutput, SF_Molecule.cpp:355-465)
     for m, mol in enumerate(mols):
         sc = sys_.mol_scalars(m)
@@ -149,6 +131,31 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
         R("mol", mol.name, "force", getattr(mol, "force", 0.0))
         R("mol", mol.name, "ln(norm_restricted)" if mol.freedom == MOL_RESTRICTED else "ln(norm_free)", sc["lnc"])
         P("mol", mol.name, "phi", phi)
+    # chi list, then the segments (SF_SegmentList::GetOutput, SF_SegmentList.cpp:387-405;
+    # SF_Segment::GetOutput, SF_Segment.cpp:345-402), after the molecules as SFbox
+    # writes them
+    ns = len(spec.segments)
+    chi = np.asarray(spec.chi, dtype=float).reshape(ns, ns)
+    for i in range(ns):
+        for j in range(ns):
+            if i != j:
+                R("chi list", spec.segments[i].name, "chi - " + spec.segments[j].name, chi[i, j])
+    for i, seg in enumerate(spec.segments):
+        fr = {SEG_FROZEN: "frozen", SEG_PINNED: "pinned"}.get(seg.freedom, "free")
+        T("mon", seg.name, "freedom", fr)
+        phi = sys_.phi(i)
+        pb = 0.0
+        if seg.freedom != SEG_FROZEN:
+            for m, mol in enumerate(mols):
+                cnt = mol.count(i)
+                pb += phib_m[m] * cnt / N[m]
+        R("mon", seg.name, "phibulk", pb)
+        theta = float((w_sum * phi).sum())
+        R("mon", seg.name, "theta", theta)
+        R("mon", seg.name, "theta excess", theta - sites * pb)
+        P("mon", seg.name, "phi", phi)
+        if seg.freedom != SEG_FROZEN:
+            P("mon", seg.name, "G", sys_.swf(i))
     nname = _names(calc, "newton", "noname")
     T("newton", nname, "iterations", int(iterations))
     T("newton", nname, "iterationlimit", int(iterationlimit))
@@ -173,7 +180,7 @@ def write_ana(path: str, lines: List[OutputLine], first: bool, write_bounds: boo
             f.write(f"{ln.cls} : {ln.name} : {ln.key} : {ln.value}\n")
             if ln.profile is not None:
                 vals = ln.profile if interior is None else ln.profile[interior]
-                f.write("".join(f"{v:g}\n" for v in vals))
+                f.write("".join(_real(v, ln.acc) + "\n" for v in vals))
         f.write("system delimiter\n\n")
 
 
@@ -253,6 +260,7 @@ def write_vtk(path: str, lines: List[OutputLine], lattice_shape: Tuple[int, ...]
     1..n-1 (0-based), in 2D the template's first profile at (x, y-1) for
     y = 1..n_y, x = 1..n_x, in 3D at (x, y, z) with x fastest."""
     prof = [ln for ln in lines if ln.profile is not None and (template is None or in_template(template, ln))]
+    acc = prof[0].acc if prof else 12
     n = [int(s) - 2 for s in lattice_shape]
     g = len(n)
     out = ["# vtk DataFile Version 3.0", "vtk output", "ASCII",
@@ -269,7 +277,8 @@ def write_vtk(path: str, lines: List[OutputLine], lattice_shape: Tuple[int, ...]
             for i in range(n[2]):
                 for j in range(n[1]):
                     for k in range(n[0]):
-                        out.append(f"{k + 0.5 * j + 0.5 * i:g} {yc1 * j + yc2 * i:g} {0.75 * i:g}")
+                        out.append(" ".join(_real(v, acc) for v in (k + 0.5 * j + 0.5 * i, yc1 * j + yc2 * i,
+                                                                         0.75 * i)))
         else:
             out += ["SPACING 1 1 1", "ORIGIN 0 0 0"]
         out.append(f"POINT_DATA {n[0] * n[1] * n[2]}")
@@ -277,7 +286,7 @@ def write_vtk(path: str, lines: List[OutputLine], lattice_shape: Tuple[int, ...]
     out.append("LOOKUP_TABLE default ")
     if g == 1:
         for z in range(1, n[0]):
-            out.append("".join(f"{ln.profile[z]:g}" for ln in prof))
+            out.append("".join(_real(ln.profile[z], ln.acc) for ln in prof))
     else:
         sel = None
         for ln in lines:
@@ -290,12 +299,59 @@ def write_vtk(path: str, lines: List[OutputLine], lattice_shape: Tuple[int, ...]
         if g == 2:
             for y in range(1, n[1] + 1):
                 for x in range(1, n[0] + 1):
-                    out.append(f"{p[x, y - 1]:g}")
+                    out.append(_real(p[x, y - 1], sel.acc))
         else:
             for z in range(1, n[2] + 1):
                 for y in range(1, n[1] + 1):
                     for x in range(1, n[0] + 1):
-                        out.append(f"{p[x, y, z]:g}")
+                        out.append(_real(p[x, y, z], sel.acc))
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+
+
+def write_profiles(path: str, lines: List[OutputLine], lattice_shape: Tuple[int, ...], template=None,
+                   write_bounds: bool = True, blank_lines: bool = True) -> None:
+    """Output::OutputProfiles (Output.cpp:998-1196): one file per calculation
+    (numbered names, as vtk files), a header row -- 'layer' (1D), 'layer x',
+    'layer y' (2D) or also 'layer z' (3D), then 'c : n : k' of every profile
+    line the template selects -- and one row per site with its 0-based
+    coordinates and those profiles' values, every field followed by a tab.
+    Boundary sites are written only with write_bounds (1D, 2D; never in 3D);
+    in 2D each x row ends with a blank line and the file with one more
+    (write_blank_lines)."""
+    prof = [ln for ln in lines if ln.profile is not None and (template is None or in_template(template, ln))]
+    g = len(lattice_shape)
+    head = {1: ["layer"], 2: ["layer x", "layer y"], 3: ["layer x", "layer y", "layer z"]}[g]
+    out = ["".join(h + "\t" for h in head) + "".join(f"{ln.cls} : {ln.name} : {ln.key}\t" for ln in prof)]
+    vals = [np.asarray(ln.profile, dtype=float) for ln in prof]
+
+    def row(coords, z):
+        return "".join(f"{c}\t" for c in coords) + "".join(_real(v[z], ln.acc) + "\t" for v, ln in zip(vals, prof))
+
+    n = [int(s) for s in lattice_shape]
+    if g == 1:
+        for z in range(n[0]):
+            if write_bounds or 0 < z < n[0] - 1:
+                out.append(row((z,), z))
+    elif g == 2:
+        z = 0
+        for x in range(n[0]):
+            for y in range(n[1]):
+                if write_bounds or (0 < x < n[0] - 1 and 0 < y < n[1] - 1):
+                    out.append(row((x, y), z))
+                z += 1
+            if blank_lines:
+                out.append("")
+        if blank_lines:
+            out.append("")
+    else:
+        z = 0
+        for x in range(n[0]):
+            for y in range(n[1]):
+                for w in range(n[2]):
+                    if 0 < x < n[0] - 1 and 0 < y < n[1] - 1 and 0 < w < n[2] - 1:
+                        out.append(row((x, y, w), z))
+                    z += 1
     with open(path, "w") as f:
         f.write("\n".join(out) + "\n")
 
@@ -310,7 +366,7 @@ def output_requests(calc: Dict[Key, str]) -> List[Tuple[str, str, Dict[str, str]
     for n in names:
         params = {p: v for (c, nn, p), v in calc.items() if c == "output" and nn == n}
         t = params.get("type")
-        if t not in ("ana", "kal", "vtk"):
-            raise ValueError(f"output : {n} : type : {t} is not written here (ana, kal and vtk are)")
+        if t not in ("ana", "kal", "vtk", "profiles"):
+            raise ValueError(f"output : {n} : type : {t} is not written here (ana, kal, vtk and profiles are)")
         out.append((n, t, params))
     return out

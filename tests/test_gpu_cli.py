@@ -54,3 +54,50 @@ def test_cli_sweep_writes_ana_and_kal(gpu_lib, tmp_path):
     ana = (tmp_path / "run.ana").read_text().splitlines()
     assert ana.count("system delimiter") == 1 + 4
     assert sum(l.startswith("mon : A : phi : profile") for l in ana) == 4
+
+
+SFBOX = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "sfbox")
+
+
+def _read_profiles(path):
+    rows = [l.split("\t") for l in open(path).read().splitlines() if l.strip()]
+    head = [h for h in rows[0] if h]
+    data = {}
+    for r in rows[1:]:
+        vals = [v for v in r if v != ""]
+        ncoord = sum(h.startswith("layer") for h in head)
+        key = tuple(int(v) for v in vals[:ncoord])
+        data[key] = dict(zip(head[ncoord:], (float(v) for v in vals[ncoord:])))
+    return head, data
+
+
+@pytest.mark.skipif(not os.path.exists(SFBOX), reason="oracle/_ref/sfbox is built where the reference sources are")
+@pytest.mark.parametrize("case", ["1d_flat_surface", "2d_flat_surface"])
+def test_cli_profiles_file_meets_sfbox(gpu_lib, tmp_path, case):
+    """The profiles file of `python -m field_b200` against the one SFbox
+    itself writes for the same input: the same coordinates and, for every
+    profile both write, the same values (both converged to 1e-12); SFbox
+    also writes density profiles this library leaves out."""
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from reference_inputs import INPUTS
+    text = INPUTS[case].replace("start\n", "output : prof : type : profiles\nstart\n")
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    ours.mkdir()
+    ref.mkdir()
+    (ours / "a.in").write_text(text)
+    (ref / "a.in").write_text(text)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-m", "field_b200", str(ours / "a.in")], capture_output=True, text=True,
+                       timeout=600, cwd=root)
+    assert r.returncode == 0, r.stdout + r.stderr
+    r2 = subprocess.run([SFBOX, "a.in"], capture_output=True, text=True, timeout=600, cwd=str(ref))
+    assert r2.returncode == 0, r2.stdout[-2000:]
+    h1, d1 = _read_profiles(ours / "prof")
+    h2, d2 = _read_profiles(ref / "prof")
+    assert set(d1) == set(d2)
+    common = [h for h in h1 if h in h2 and not h.startswith("layer")]
+    assert any(h.endswith(": phi") for h in common) and len(common) >= 4, common
+    for h in common:
+        a = np.array([d1[k][h] for k in sorted(d1)])
+        b = np.array([d2[k][h] for k in sorted(d2)])
+        assert np.max(np.abs(a - b)) <= 1e-8 * max(np.max(np.abs(b)), 1e-300) + 1e-11, h

@@ -20,12 +20,13 @@ def test_ana_blocks_and_profiles(tmp_path):
     assert text[0] == "system delimiter" and text[1] == ""
     assert text[2] == "sys : noname : free energy : -1.25"
     assert text[3] == "sys : noname : free energy density : profile"
-    assert text[4:8] == ["0", "1.5", "2.25", "0"]
+    # reals as SFbox's streams print them: scientific, accuracy - 1 decimals
+    assert text[4:8] == ["0.00000000000e+00", "1.50000000000e+00", "2.25000000000e+00", "0.00000000000e+00"]
     assert text.count("system delimiter") == 3
     assert "sys : noname : free energy : -2.5" in text
     write_ana(p, _lines(-1.0), first=True, write_bounds=False, lattice_shape=(4,))
     text = open(p).read().splitlines()
-    assert text[4:6] == ["1.5", "2.25"] and text[6] == "mol : pol : theta : 3.5"
+    assert text[4:6] == ["1.50000000000e+00", "2.25000000000e+00"] and text[6] == "mol : pol : theta : 3.5"
 
 
 def test_kal_header_once_then_rows(tmp_path):
@@ -44,6 +45,7 @@ def test_output_requests():
     assert [(n, t) for n, t, _ in req] == [("run.ana", "ana"), ("run.kal", "kal")]
     with pytest.raises(ValueError):
         output_requests(parse_input("output : x.ave : type : ave\n")[0])
+    assert output_requests(parse_input("output : x.prf : type : profiles\n")[0])[0][1] == "profiles"
 
 
 class _OracleSystem:
@@ -94,7 +96,13 @@ def test_output_lines_keys_and_sums():
     lines = output_lines(calc, spec, sys_, x, it, err, st.tolerance, st.iterationlimit, 1)
     d = {(l.cls, l.name, l.key): l for l in lines}
     assert [l.cls for l in lines][:2] == ["sys", "sys"]
-    assert d[("sys", "noname", "free energy")].value == f"{sys_.o.thermo()[0]:.7g}"
+    acc = int(-np.log10(st.tolerance) + 0.5)
+    assert d[("sys", "noname", "free energy")].value == f"{sys_.o.thermo()[0]:.{acc - 1}e}"
+    order = []
+    for l in lines:
+        if not order or order[-1] != l.cls:
+            order.append(l.cls)
+    assert order == ["sys", "lat", "mol", "chi list", "mon", "newton"]   # SFbox's class order
     assert float(d[("chi list", "A", "chi - W")].value) == 0.5
     assert float(d[("chi list", "A", "chi - S")].value) == -1.0
     phiA = sys_.o.phi(1)
@@ -124,7 +132,7 @@ def test_vtk_1d_and_2d_layout(tmp_path):
     assert text[:4] == ["# vtk DataFile Version 3.0", "vtk output", "ASCII", "DATASET STRUCTURED_POINTS"]
     assert text[4] == "DIMENSIONS5" and text[7] == "POINT_DATA 5"
     assert text[8] == "SCALARS SFBox_profile double" and text[9] == "LOOKUP_TABLE default "
-    assert text[10:] == ["1", "2", "3", "4"]
+    assert text[10:] == [f"{v:.11e}" for v in (1.0, 2.0, 3.0, 4.0)]
     grid = np.arange(5 * 4, dtype=float).reshape(5, 4)   # nx = 3, ny = 2
     lines2 = [OutputLine("mon", "A", "phi", "profile", grid.ravel()),
               OutputLine("mon", "B", "phi", "profile", -grid.ravel())]
@@ -160,3 +168,33 @@ def test_template_wildcards():
     assert in_template([("mon", "*", "phi")], ln)
     assert in_template([("m*", "A", "p*")], ln)
     assert not in_template([("mol", "*", "phi")], ln)
+
+
+def test_profiles_layout(tmp_path):
+    """OutputProfiles as SFbox writes it: a header of the coordinate names and
+    'c : n : k' of each profile, then one row per site, every field followed
+    by a tab; boundary sites only with write_bounds; in 2D a blank line after
+    each x row and one more at the end; in 3D interior sites only."""
+    from field_b200.output import write_profiles
+    a, b = np.arange(5, dtype=float), -np.arange(5, dtype=float)
+    lines = [OutputLine("sys", "noname", "free energy", "1"), OutputLine("mon", "A", "phi", "profile", a),
+             OutputLine("mol", "m", "phi", "profile", b)]
+    p = str(tmp_path / "p")
+    write_profiles(p, lines, (5,))
+    t = open(p).read().split("\n")
+    assert t[0] == "layer\tmon : A : phi\tmol : m : phi\t"
+    assert t[1] == f"0\t{0.0:.11e}\t{-0.0:.11e}\t" and t[5].startswith("4\t") and t[6] == ""
+    write_profiles(p, lines, (5,), write_bounds=False, template=[("mol", "*", "*")])
+    t = open(p).read().split("\n")
+    assert t[0] == "layer\tmol : m : phi\t" and [r.split("\t")[0] for r in t[1:4]] == ["1", "2", "3"]
+    g2 = np.arange(12, dtype=float)                     # (4, 3)
+    write_profiles(p, [OutputLine("mon", "A", "phi", "profile", g2)], (4, 3), write_bounds=False)
+    t = open(p).read().split("\n")
+    assert t[0] == "layer x\tlayer y\tmon : A : phi\t"
+    # interior (1, 1) and (2, 1); each of the four x rows closed by a blank
+    # line, one more at the end
+    assert t[1:] == ["", f"1\t1\t{4.0:.11e}\t", "", f"2\t1\t{7.0:.11e}\t", "", "", "", ""]
+    g3 = np.arange(27, dtype=float)                     # (3, 3, 3): one interior site
+    write_profiles(p, [OutputLine("mon", "A", "phi", "profile", g3)], (3, 3, 3))
+    t = open(p).read().split("\n")
+    assert t == ["layer x\tlayer y\tlayer z\tmon : A : phi\t", f"1\t1\t1\t{13.0:.11e}\t", ""]
