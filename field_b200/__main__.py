@@ -76,7 +76,10 @@ def main(argv=None) -> int:
             all_ok &= status == 0
             sys_ = System(spec)
             err = float(np.linalg.norm(sys_.residual(x)))
-            lines = output_lines(p, spec, sys_, x, its, err, stp.tolerance, stp.iterationlimit, calc_number)
+            # SFbox's Pure_DIIS counts its iterations on the console only: the
+            # newton iterations line of its output stays 0 (sfnewton.cpp:566-664)
+            lines = output_lines(p, spec, sys_, x, its if newton else 0, err, stp.tolerance, stp.iterationlimit,
+                                 calc_number)
             for name, kind, params in output_requests(p):
                 path = os.path.join(outdir, name)
                 first = path not in written

@@ -91,6 +91,8 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
     lname = _names(calc, "lat", "lat")
     T("lat", lname, "gradients", lat.gradients)
     geom = {GEOM_CYLINDRICAL: "cylindrical", GEOM_SPHERICAL: "spherical"}.get(lat.geometry, "flat")
+    if lat.gradients > 1:
+        geom = "flat"   # what Lat2DCylinder::GetOutput writes for the cylinder too (Lat2DCylinder.cpp:91)
     T("lat", lname, "geometry", geom)
     axes = [""] if lat.gradients == 1 else ["_x", "_y", "_z"][:lat.gradients]
     for d, a in enumerate(axes):

@@ -101,3 +101,48 @@ def test_cli_profiles_file_meets_sfbox(gpu_lib, tmp_path, case):
         a = np.array([d1[k][h] for k in sorted(d1)])
         b = np.array([d2[k][h] for k in sorted(d2)])
         assert np.max(np.abs(a - b)) <= 1e-8 * max(np.max(np.abs(b)), 1e-300) + 1e-11, h
+
+
+def _read_ana(path):
+    out = {}
+    for l in open(path).read().splitlines():
+        parts = l.split(" : ")
+        if len(parts) == 4 and parts[3] != "profile":
+            out[tuple(parts[:3])] = parts[3]
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(SFBOX), reason="oracle/_ref/sfbox is built where the reference sources are")
+@pytest.mark.parametrize("case", ["1d_flat_surface", "2d_cylinder_core"])
+def test_cli_ana_lines_meet_sfbox(gpu_lib, tmp_path, case):
+    """Every scalar line this library writes to an ana file against the same
+    line of the ana file SFbox itself writes for the input: the same key,
+    the same text, or the same number to 1e-8 (both converged to 1e-12)."""
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from reference_inputs import INPUTS
+    text = INPUTS[case].replace("start\n", "output : out.ana : type : ana\nstart\n")
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    ours.mkdir()
+    ref.mkdir()
+    (ours / "a.in").write_text(text)
+    (ref / "a.in").write_text(text)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-m", "field_b200", str(ours / "a.in")], capture_output=True, text=True,
+                       timeout=600, cwd=root)
+    assert r.returncode == 0, r.stdout + r.stderr
+    r2 = subprocess.run([SFBOX, "a.in"], capture_output=True, text=True, timeout=600, cwd=str(ref))
+    assert r2.returncode == 0, r2.stdout[-2000:]
+    a, b = _read_ana(ours / "out.ana"), _read_ana(ref / "out.ana")
+    bad = []
+    for k, v in a.items():
+        if k not in b:
+            bad.append((k, v, None))
+            continue
+        try:
+            x, y = float(v), float(b[k])
+            ok = abs(x - y) <= 1e-8 * max(abs(y), 1.0)
+        except ValueError:
+            ok = v == b[k]
+        if not ok:
+            bad.append((k, v, b[k]))
+    assert not bad, bad
