@@ -155,6 +155,9 @@ def output_lines(calc: Dict[Key, str], spec, sys_, x: np.ndarray, iterations: in
         theta = float((w_sum * phi).sum())
         R("mon", seg.name, "theta", theta)
         R("mon", seg.name, "theta excess", theta - sites * pb)
+        R("mon", seg.name, "valence", getattr(seg, "valence", 0.0))
+        R("mon", seg.name, "epsilon", getattr(seg, "epsilon", 80.0) or 80.0)
+        R("mon", seg.name, "int.free energy", 0.0)   # internal states: none without reactions
         P("mon", seg.name, "phi", phi)
         if seg.freedom != SEG_FROZEN:
             P("mon", seg.name, "G", sys_.swf(i))
